@@ -1,0 +1,958 @@
+/*
+ * hecmw33_oracle.c -- CPU restatement (C + OpenMP) of FrontISTR 5.9's 3x3-block
+ * CG solve path.  TEST INFRASTRUCTURE ONLY: the parity checker and the CPU
+ * baseline, never part of the product.
+ *
+ * Reference files restated here (paths inside the FrontISTR tree):
+ *   hecmw1/src/solver/main/hecmw_solver.f90:9-88                 (hecmw_solve)
+ *   hecmw1/src/solver/iterative/hecmw_solver_Iterative.f90:13-187,255-323
+ *   hecmw1/src/solver/iterative/hecmw_solver_CG.f90:19-320        (hecmw_solve_CG)
+ *   hecmw1/src/solver/las/hecmw_solver_las_33.F90:120-435         (matvec/matresid/rel_resid)
+ *   hecmw1/src/solver/communication/hecmw_solver_misc.F90:46-201  (dot/axpy/xpay)
+ *   hecmw1/src/solver/precond/hecmw_precond.f90:30-172            (setup/apply dispatch)
+ *   hecmw1/src/solver/precond/ssor/hecmw_precond_SSOR_33.F90:57-415
+ *   hecmw1/src/solver/precond/bilu/hecmw_precond_BILU_33.f90:34-362,1493-1596
+ *   hecmw1/src/solver/precond/diag/hecmw_precond_DIAG_33.F90:27-149
+ *   hecmw1/src/solver/matrix/hecmw_matrix_ordering_CM.f90:18-245  (RCM)
+ *   hecmw1/src/solver/matrix/hecmw_matrix_ordering_MC.f90:15-72   (multicolouring)
+ *   hecmw1/src/solver/matrix/hecmw_matrix_reorder.f90:20-314
+ *   hecmw1/src/solver/matrix/hecmw_matrix_misc.F90:858-877        (precond recycling)
+ *
+ * Floating-point expressions keep the reference's operand order; build with
+ * -ffp-contract=off so no FMA contraction changes the rounding.
+ */
+#include "hecmw33_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* hecmw1/src/solver/init/hecmw_solve_error.f90:9-16 */
+enum {
+  ERR_INCONS_PC = 1001,
+  ERR_ZERO_DIAG = 2001,
+  ERR_ZERO_RHS = 2002,
+  ERR_NOCONV_MAXIT = 3001,
+  ERR_DIVERGE_MAT = 3002,
+  ERR_DIVERGE_PC = 3003,
+  ERR_DIVERGE_NAN = 3004,
+  /* not a reference code: FORM_ILU0_33/ILU1a33 stop the program on a zero pivot
+   * (hecmw_precond_BILU_33.f90:1510-1513); the oracle returns this instead. */
+  ERR_ILU_ZERO_PIVOT = 9001
+};
+
+static double now_s(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+int o33_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+/* ------------------------------------------------------------------------ */
+/* hecmw_matvec_33_inner, CPU branch: hecmw_solver_las_33.F90:279-311.
+ * Row i: D block first, then L blocks in ascending order, then U blocks. */
+void o33_matvec(const o33_matrix *A, const double *X, double *Y) {
+  const int N = A->N;
+  const int *indexL = A->indexL, *indexU = A->indexU;
+  const int *itemL = A->itemL, *itemU = A->itemU;
+  const double *D = A->D, *AL = A->AL, *AU = A->AU;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < N; i++) {
+    double X1 = X[3 * i], X2 = X[3 * i + 1], X3 = X[3 * i + 2];
+    const double *d = D + 9 * (size_t)i;
+    double YV1 = d[0] * X1 + d[1] * X2 + d[2] * X3;
+    double YV2 = d[3] * X1 + d[4] * X2 + d[5] * X3;
+    double YV3 = d[6] * X1 + d[7] * X2 + d[8] * X3;
+    for (int j = indexL[i]; j < indexL[i + 1]; j++) {
+      const int in = itemL[j] - 1;
+      X1 = X[3 * in];
+      X2 = X[3 * in + 1];
+      X3 = X[3 * in + 2];
+      const double *a = AL + 9 * (size_t)j;
+      YV1 = YV1 + a[0] * X1 + a[1] * X2 + a[2] * X3;
+      YV2 = YV2 + a[3] * X1 + a[4] * X2 + a[5] * X3;
+      YV3 = YV3 + a[6] * X1 + a[7] * X2 + a[8] * X3;
+    }
+    for (int j = indexU[i]; j < indexU[i + 1]; j++) {
+      const int in = itemU[j] - 1;
+      X1 = X[3 * in];
+      X2 = X[3 * in + 1];
+      X3 = X[3 * in + 2];
+      const double *a = AU + 9 * (size_t)j;
+      YV1 = YV1 + a[0] * X1 + a[1] * X2 + a[2] * X3;
+      YV2 = YV2 + a[3] * X1 + a[4] * X2 + a[5] * X3;
+      YV3 = YV3 + a[6] * X1 + a[7] * X2 + a[8] * X3;
+    }
+    Y[3 * i] = YV1;
+    Y[3 * i + 1] = YV2;
+    Y[3 * i + 2] = YV3;
+  }
+}
+
+/* hecmw_matresid_33: hecmw_solver_las_33.F90:367-399 */
+void o33_matresid(const o33_matrix *A, const double *X, const double *B, double *R) {
+  o33_matvec(A, X, R);
+  const int n = 3 * A->N;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) R[i] = B[i] - R[i];
+}
+
+/* hecmw_InnerProduct_R CPU branch: serial loop, hecmw_solver_misc.F90:61-68 */
+double o33_dot(int n, const double *x, const double *y) {
+  double sum = 0.0;
+  for (int i = 0; i < n; i++) sum = sum + x[i] * y[i];
+  return sum;
+}
+
+/* hecmw_rel_resid_L2_33: hecmw_solver_las_33.F90:406-435 */
+double o33_rel_resid_L2(const o33_matrix *A, const double *X, const double *B) {
+  const int n = 3 * A->N;
+  double *r = (double *)malloc(sizeof(double) * 3 * (size_t)A->NP);
+  double bnorm2 = o33_dot(n, B, B);
+  if (bnorm2 == 0.0) bnorm2 = 1.0;
+  o33_matresid(A, X, B, r);
+  double rnorm2 = o33_dot(n, r, r);
+  free(r);
+  return sqrt(rnorm2 / bnorm2);
+}
+
+/* hecmw_axpy_R: y = alpha*x + y  (hecmw_solver_misc.F90:156-158) */
+static void axpy(int n, double alpha, const double *x, double *y) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) y[i] = alpha * x[i] + y[i];
+}
+/* hecmw_xpay_R: y = x + alpha*y  (hecmw_solver_misc.F90:191-193) */
+static void xpay(int n, double alpha, const double *x, double *y) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) y[i] = x[i] + alpha * y[i];
+}
+
+/* ------------------------------------------------------------------------ */
+/* Orderings.  Arrays named with a trailing "1" are used with 1-based indices
+ * (element 0 unused) to follow the Fortran text. */
+
+/* sort_nodes_by_degree: hecmw_matrix_ordering_CM.f90:207-233 (recursive
+ * middle-pivot Hoare quicksort; not stable, so equal-degree order depends on it) */
+static void sort_nodes_by_degree(int *lv_item1, int istart, int iend, const int *degs1) {
+  if (istart >= iend) return;
+  const int pivot = degs1[lv_item1[(istart + iend) / 2]];
+  int left = istart, right = iend;
+  for (;;) {
+    while (degs1[lv_item1[left]] < pivot) left++;
+    while (pivot < degs1[lv_item1[right]]) right--;
+    if (left >= right) break;
+    const int t = lv_item1[left];
+    lv_item1[left] = lv_item1[right];
+    lv_item1[right] = t;
+    left++;
+    right--;
+  }
+  sort_nodes_by_degree(lv_item1, istart, left - 1, degs1);
+  sort_nodes_by_degree(lv_item1, right + 1, iend, degs1);
+}
+
+/* ordering_CM_inner: hecmw_matrix_ordering_CM.f90:88-147 */
+static int ordering_cm_inner(int N, const int *indexL, const int *itemL, const int *indexU,
+                             const int *itemU, const int *degs1, int nstart, int *lv_index,
+                             int *lv_item1) {
+  int *iwk1 = (int *)calloc((size_t)N + 1, sizeof(int));
+  int nlevel = 1;
+  lv_index[0] = 0;
+  iwk1[nstart] = 1;
+  int cntall = 1;
+  lv_item1[1] = nstart;
+  lv_index[1] = 1;
+  for (int level = 2; level <= N; level++) {
+    int cnt = 0;
+    for (int j = lv_index[level - 2] + 1; j <= lv_index[level - 1]; j++) {
+      const int jnode = lv_item1[j];
+      for (int k = indexL[jnode - 1]; k < indexL[jnode]; k++) {
+        const int knode = itemL[k];
+        if (iwk1[knode] == 0) {
+          iwk1[knode] = level;
+          cnt++;
+          cntall++;
+          lv_item1[cntall] = knode;
+        }
+      }
+      for (int k = indexU[jnode - 1]; k < indexU[jnode]; k++) {
+        const int knode = itemU[k];
+        if (knode > N) continue;
+        if (iwk1[knode] == 0) {
+          iwk1[knode] = level;
+          cnt++;
+          cntall++;
+          lv_item1[cntall] = knode;
+        }
+      }
+    }
+    if (cnt == 0) {
+      for (int knode = 1; knode <= N; knode++) {
+        if (iwk1[knode] == 0) {
+          iwk1[knode] = level;
+          cnt++;
+          cntall++;
+          lv_item1[cntall] = knode;
+          break;
+        }
+      }
+    }
+    lv_index[level] = cntall;
+    sort_nodes_by_degree(lv_item1, lv_index[level - 1] + 1, lv_index[level], degs1);
+    if (cntall == N) {
+      nlevel = level;
+      break;
+    }
+  }
+  free(iwk1);
+  return nlevel;
+}
+
+/* hecmw_matrix_ordering_CM + reverse_ordering: hecmw_matrix_ordering_CM.f90:18-86,235-245 */
+void o33_ordering_rcm(int N, const int *indexL, const int *itemL, const int *indexU,
+                      const int *itemU, int *perm, int *iperm) {
+  enum { NMINMAX = 5 };
+  int *degs1 = (int *)malloc(sizeof(int) * ((size_t)N + 1));
+  /* count_degrees: :167-179 */
+  for (int i = 1; i <= N; i++) {
+    degs1[i] = indexL[i] - indexL[i - 1];
+    for (int j = indexU[i - 1]; j < indexU[i]; j++)
+      if (itemU[j] <= N) degs1[i]++;
+  }
+  /* find_minimum_degrees: :181-205 */
+  int mins1[NMINMAX + 1];
+  int degmin = N, nmin = 0;
+  for (int i = 1; i <= N; i++) {
+    if (degs1[i] == 0) continue;
+    if (degs1[i] < degmin) {
+      degmin = degs1[i];
+      nmin = 1;
+      mins1[1] = i;
+    } else if (degs1[i] == degmin) {
+      nmin++;
+      if (nmin <= NMINMAX) mins1[nmin] = i;
+    }
+  }
+  if (nmin > NMINMAX) nmin = NMINMAX;
+  /* Degenerate graph without edges: the reference reads an unset seed here; the
+   * oracle starts from node 1 (a documented deviation for an undefined case). */
+  if (nmin == 0) {
+    nmin = 1;
+    mins1[1] = 1;
+  }
+  int *nlevel = (int *)malloc(sizeof(int) * (size_t)nmin);
+  int **lv_item = (int **)malloc(sizeof(int *) * (size_t)nmin);
+#pragma omp parallel for schedule(static, 1)
+  for (int s = 0; s < nmin; s++) {
+    int *lv_index = (int *)malloc(sizeof(int) * ((size_t)N + 1));
+    lv_item[s] = (int *)malloc(sizeof(int) * ((size_t)N + 1));
+    nlevel[s] = ordering_cm_inner(N, indexL, itemL, indexU, itemU, degs1, mins1[s + 1], lv_index,
+                                  lv_item[s]);
+    free(lv_index);
+  }
+  int nlevel_max = nlevel[0], max_id = 0;
+  for (int s = 1; s < nmin; s++)
+    if (nlevel[s] > nlevel_max) {
+      nlevel_max = nlevel[s];
+      max_id = s;
+    }
+  for (int i = 1; i <= N; i++) {
+    perm[i - 1] = lv_item[max_id][i];
+    iperm[perm[i - 1] - 1] = i;
+  }
+  for (int s = 0; s < nmin; s++) free(lv_item[s]);
+  free(lv_item);
+  free(nlevel);
+  free(degs1);
+  /* reverse_ordering */
+  const int N1 = N + 1;
+  for (int i = 1; i <= N; i++) {
+    iperm[i - 1] = N1 - iperm[i - 1];
+    perm[iperm[i - 1] - 1] = i;
+  }
+}
+
+/* hecmw_matrix_ordering_MC: hecmw_matrix_ordering_MC.f90:15-72 */
+int o33_ordering_mc(int N, const int *indexL, const int *itemL, const int *indexU,
+                    const int *itemU, const int *perm_cur, int ncolor_in, int *colorindex,
+                    int *perm, int *iperm) {
+  int *iwk1 = (int *)calloc((size_t)N + 1, sizeof(int));
+  if (ncolor_in < 1) ncolor_in = 1;
+  const int nn_color = N / ncolor_in;
+  int cntall = 0, ncolor_out = 0;
+  colorindex[0] = 0;
+  for (int color = 1; color <= N; color++) {
+    int cnt = 0;
+    for (int i = 1; i <= N; i++) {
+      const int inode = perm_cur[i - 1];
+      if (iwk1[inode] > 0 || iwk1[inode] == -1) continue;
+      iwk1[inode] = color;
+      cntall++;
+      perm[cntall - 1] = inode;
+      cnt++;
+      if (cnt == nn_color) break;
+      if (cntall == N) break;
+      for (int j = indexL[inode - 1]; j < indexL[inode]; j++) {
+        const int jnode = itemL[j];
+        if (iwk1[jnode] == 0) iwk1[jnode] = -1;
+      }
+      for (int j = indexU[inode - 1]; j < indexU[inode]; j++) {
+        const int jnode = itemU[j];
+        if (jnode > N) continue;
+        if (iwk1[jnode] == 0) iwk1[jnode] = -1;
+      }
+    }
+    colorindex[color] = cntall;
+    if (cntall == N) {
+      ncolor_out = color;
+      break;
+    }
+    for (int i = 1; i <= N; i++)
+      if (iwk1[i] == -1) iwk1[i] = 0;
+  }
+  free(iwk1);
+  for (int i = 1; i <= N; i++) iperm[perm[i - 1] - 1] = i;
+  return ncolor_out;
+}
+
+static int cmp_int(const void *a, const void *b) {
+  const int x = *(const int *)a, y = *(const int *)b;
+  return (x > y) - (x < y);
+}
+
+/* hecmw_bsearch_int_array over item[is..ie) (0-based); returns position or -1 */
+static int bsearch_pos(const int *item, int is, int ie, int key) {
+  int lo = is, hi = ie - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) / 2;
+    if (item[mid] == key) return mid;
+    if (item[mid] < key) lo = mid + 1;
+    else hi = mid - 1;
+  }
+  return -1;
+}
+
+/* In-place LU of a sigma-scaled 3x3 block with reciprocal pivots:
+ * hecmw_precond_SSOR_33.F90:157-208 (and DIAG_33:67-102, ILU1a33 with sigma=1). */
+static int lu33(double *a, double sigma) {
+  double T[3][3] = {{a[0] * sigma, a[1], a[2]}, {a[3], a[4] * sigma, a[5]}, {a[6], a[7], a[8] * sigma}};
+  double PW[3];
+  int zero = 0;
+  for (int k = 0; k < 3; k++) {
+    if (T[k][k] == 0.0) zero = 1;
+    T[k][k] = 1.0 / T[k][k];
+    for (int i = k + 1; i < 3; i++) {
+      T[i][k] = T[i][k] * T[k][k];
+      for (int j = k + 1; j < 3; j++) PW[j] = T[i][j] - T[i][k] * T[k][j];
+      for (int j = k + 1; j < 3; j++) T[i][j] = PW[j];
+    }
+  }
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) a[3 * r + c] = T[r][c];
+  return zero;
+}
+
+/* forward/backward substitution with the reciprocal-pivot LU block:
+ * hecmw_precond_SSOR_33.F90:332-338 */
+static inline void lu33_solve(const double *alu, double *X1, double *X2, double *X3) {
+  double x1 = *X1, x2 = *X2, x3 = *X3;
+  x2 = x2 - alu[3] * x1;
+  x3 = x3 - alu[6] * x1 - alu[7] * x2;
+  x3 = alu[8] * x3;
+  x2 = alu[4] * (x2 - alu[5] * x3);
+  x1 = alu[0] * (x1 - alu[2] * x3 - alu[1] * x2);
+  *X1 = x1;
+  *X2 = x2;
+  *X3 = x3;
+}
+
+/* ------------------------------------------------------------------------ */
+struct o33_precond {
+  int kind; /* 1 SSOR, 3 DIAG, 10 BILU0 */
+  int N, NP;
+  /* SSOR: reordered profile (items renumbered to old 1-based ids) */
+  int ncolor;
+  int *colorindex, *perm, *iperm;
+  int *indexL, *indexU, *itemL, *itemU;
+  double *AL, *AU, *ALU;
+  /* BILU0 */
+  double *Dlu0, *ALlu0, *AUlu0;
+  const int *inL, *inU, *iaL, *iaU; /* borrowed from the matrix (copied) */
+  int *own_inL, *own_inU, *own_iaL, *own_iaU;
+};
+
+static o33_precond *ssor_setup(const o33_matrix *A, int ncolor_in, double sigma_diag,
+                               int coloured) {
+  const int N = A->N;
+  o33_precond *P = (o33_precond *)calloc(1, sizeof(o33_precond));
+  P->kind = 1;
+  P->N = N;
+  P->NP = A->NP;
+  P->perm = (int *)malloc(sizeof(int) * (size_t)N);
+  P->iperm = (int *)malloc(sizeof(int) * (size_t)N);
+  /* hecmw_precond_SSOR_33.F90:93-128 */
+  if (!coloured) {
+    P->ncolor = 1;
+    P->colorindex = (int *)malloc(sizeof(int) * 2);
+    P->colorindex[0] = 0;
+    P->colorindex[1] = N;
+    for (int i = 0; i < N; i++) P->perm[i] = P->iperm[i] = i + 1;
+  } else {
+    P->colorindex = (int *)malloc(sizeof(int) * ((size_t)N + 1));
+    int *perm_tmp = (int *)malloc(sizeof(int) * (size_t)N);
+    o33_ordering_rcm(N, A->indexL, A->itemL, A->indexU, A->itemU, perm_tmp, P->iperm);
+    P->ncolor = o33_ordering_mc(N, A->indexL, A->itemL, A->indexU, A->itemU, perm_tmp, ncolor_in,
+                                P->colorindex, P->perm, P->iperm);
+    free(perm_tmp);
+  }
+  /* allocation sizes: :130-139 */
+  int NPL = 0;
+  for (int i = 0; i < N; i++)
+    for (int j = A->indexU[i]; j < A->indexU[i + 1]; j++) {
+      if (A->itemU[j] > N) break;
+      NPL++;
+    }
+  if (A->indexL[N] > NPL) NPL = A->indexL[N];
+  const int NPU = A->indexU[N];
+  P->indexL = (int *)malloc(sizeof(int) * ((size_t)N + 1));
+  P->indexU = (int *)malloc(sizeof(int) * ((size_t)N + 1));
+  P->itemL = (int *)malloc(sizeof(int) * ((size_t)NPL + 1));
+  P->itemU = (int *)malloc(sizeof(int) * ((size_t)NPU + 1));
+  /* hecmw_matrix_reorder_profile: hecmw_matrix_reorder.f90:20-66 */
+  int cntL = 0, cntU = 0;
+  P->indexL[0] = P->indexU[0] = 0;
+  for (int inew = 1; inew <= N; inew++) {
+    const int iold = P->perm[inew - 1];
+    for (int j = A->indexL[iold - 1]; j < A->indexL[iold]; j++) {
+      const int jnew = P->iperm[A->itemL[j] - 1];
+      if (jnew < inew) P->itemL[cntL++] = jnew;
+      else P->itemU[cntU++] = jnew;
+    }
+    for (int j = A->indexU[iold - 1]; j < A->indexU[iold]; j++) {
+      const int jold = A->itemU[j];
+      if (jold > N) continue;
+      const int jnew = P->iperm[jold - 1];
+      if (jnew < inew) P->itemL[cntL++] = jnew;
+      else P->itemU[cntU++] = jnew;
+    }
+    P->indexL[inew] = cntL;
+    P->indexU[inew] = cntU;
+    qsort(P->itemL + P->indexL[inew - 1], (size_t)(cntL - P->indexL[inew - 1]), sizeof(int), cmp_int);
+    qsort(P->itemU + P->indexU[inew - 1], (size_t)(cntU - P->indexU[inew - 1]), sizeof(int), cmp_int);
+  }
+  /* hecmw_matrix_reorder_values (reorder_diag2 + reorder_off_diag2): :68-97,182-314 */
+  double *Dp = (double *)calloc(9 * (size_t)N, sizeof(double));
+  P->AL = (double *)calloc(9 * ((size_t)NPL + 1), sizeof(double));
+  P->AU = (double *)calloc(9 * ((size_t)NPU + 1), sizeof(double));
+  for (int iold = 1; iold <= N; iold++) {
+    const int inew = P->iperm[iold - 1];
+    memcpy(Dp + 9 * (size_t)(inew - 1), A->D + 9 * (size_t)(iold - 1), 9 * sizeof(double));
+  }
+  for (int pass = 0; pass < 2; pass++) {
+    const int *indexX = pass == 0 ? A->indexL : A->indexU;
+    const int *itemX = pass == 0 ? A->itemL : A->itemU;
+    const double *AX = pass == 0 ? A->AL : A->AU;
+#pragma omp parallel for schedule(static)
+    for (int iold = 1; iold <= N; iold++) {
+      const int inew = P->iperm[iold - 1];
+      for (int jold = indexX[iold - 1]; jold < indexX[iold]; jold++) {
+        const int kold = itemX[jold];
+        if (kold > N) continue;
+        const int knew = P->iperm[kold - 1];
+        if (knew < inew) {
+          const int jnew = bsearch_pos(P->itemL, P->indexL[inew - 1], P->indexL[inew], knew);
+          memcpy(P->AL + 9 * (size_t)jnew, AX + 9 * (size_t)jold, 9 * sizeof(double));
+        } else {
+          const int jnew = bsearch_pos(P->itemU, P->indexU[inew - 1], P->indexU[inew], knew);
+          memcpy(P->AU + 9 * (size_t)jnew, AX + 9 * (size_t)jold, 9 * sizeof(double));
+        }
+      }
+    }
+  }
+  /* hecmw_matrix_reorder_renum_item: :143-158 (new column -> old id) */
+  for (int j = 0; j < cntL; j++) P->itemL[j] = P->perm[P->itemL[j] - 1];
+  for (int j = 0; j < cntU; j++) P->itemU[j] = P->perm[P->itemU[j] - 1];
+  /* diagonal LU with reciprocal pivots: :157-208 */
+  P->ALU = Dp;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < N; i++) lu33(P->ALU + 9 * (size_t)i, sigma_diag);
+  return P;
+}
+
+/* hecmw_precond_SSOR_33_apply: hecmw_precond_SSOR_33.F90:273-415 */
+static void ssor_apply(const o33_precond *P, double *ZP) {
+  for (int ic = 1; ic <= P->ncolor; ic++) {
+#pragma omp parallel for schedule(static) if (P->ncolor > 1)
+    for (int i = P->colorindex[ic - 1] + 1; i <= P->colorindex[ic]; i++) {
+      const int iold = P->perm[i - 1];
+      double SW1 = ZP[3 * (iold - 1)], SW2 = ZP[3 * (iold - 1) + 1], SW3 = ZP[3 * (iold - 1) + 2];
+      for (int j = P->indexL[i - 1]; j < P->indexL[i]; j++) {
+        const int k = P->itemL[j];
+        const double X1 = ZP[3 * (k - 1)], X2 = ZP[3 * (k - 1) + 1], X3 = ZP[3 * (k - 1) + 2];
+        const double *a = P->AL + 9 * (size_t)j;
+        SW1 = SW1 - a[0] * X1 - a[1] * X2 - a[2] * X3;
+        SW2 = SW2 - a[3] * X1 - a[4] * X2 - a[5] * X3;
+        SW3 = SW3 - a[6] * X1 - a[7] * X2 - a[8] * X3;
+      }
+      lu33_solve(P->ALU + 9 * (size_t)(i - 1), &SW1, &SW2, &SW3);
+      ZP[3 * (iold - 1)] = SW1;
+      ZP[3 * (iold - 1) + 1] = SW2;
+      ZP[3 * (iold - 1) + 2] = SW3;
+    }
+  }
+  for (int ic = P->ncolor; ic >= 1; ic--) {
+#pragma omp parallel for schedule(static) if (P->ncolor > 1)
+    for (int i = P->colorindex[ic]; i >= P->colorindex[ic - 1] + 1; i--) {
+      double SW1 = 0.0, SW2 = 0.0, SW3 = 0.0;
+      for (int j = P->indexU[i] - 1; j >= P->indexU[i - 1]; j--) {
+        const int k = P->itemU[j];
+        const double X1 = ZP[3 * (k - 1)], X2 = ZP[3 * (k - 1) + 1], X3 = ZP[3 * (k - 1) + 2];
+        const double *a = P->AU + 9 * (size_t)j;
+        SW1 = SW1 + a[0] * X1 + a[1] * X2 + a[2] * X3;
+        SW2 = SW2 + a[3] * X1 + a[4] * X2 + a[5] * X3;
+        SW3 = SW3 + a[6] * X1 + a[7] * X2 + a[8] * X3;
+      }
+      lu33_solve(P->ALU + 9 * (size_t)(i - 1), &SW1, &SW2, &SW3);
+      const int iold = P->perm[i - 1];
+      ZP[3 * (iold - 1)] = ZP[3 * (iold - 1)] - SW1;
+      ZP[3 * (iold - 1) + 1] = ZP[3 * (iold - 1) + 1] - SW2;
+      ZP[3 * (iold - 1) + 2] = ZP[3 * (iold - 1) + 2] - SW3;
+    }
+  }
+}
+
+/* hecmw_precond_DIAG_33_setup/apply: hecmw_precond_DIAG_33.F90:27-136 */
+static o33_precond *diag_setup(const o33_matrix *A, double sigma_diag) {
+  o33_precond *P = (o33_precond *)calloc(1, sizeof(o33_precond));
+  P->kind = 3;
+  P->N = A->N;
+  P->NP = A->NP;
+  P->ALU = (double *)calloc(9 * (size_t)A->NP, sizeof(double));
+  memcpy(P->ALU, A->D, 9 * (size_t)A->N * sizeof(double));
+  for (int i = 0; i < A->N; i++) lu33(P->ALU + 9 * (size_t)i, sigma_diag);
+  return P;
+}
+
+static void diag_apply(const o33_precond *P, double *WW) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < P->N; i++) lu33_solve(P->ALU + 9 * (size_t)i, &WW[3 * i], &WW[3 * i + 1], &WW[3 * i + 2]);
+}
+
+/* ILU1b33: RHS = Aik * Dk^-1 * Akj  (hecmw_precond_BILU_33.f90:1538-1596) */
+static void ilu1b33(double *RHS, const double *DkINV, const double *Aik, const double *Akj) {
+  for (int c = 0; c < 3; c++) {
+    double X1 = Akj[c], X2 = Akj[3 + c], X3 = Akj[6 + c];
+    X2 = X2 - DkINV[3] * X1;
+    X3 = X3 - DkINV[6] * X1 - DkINV[7] * X2;
+    X3 = DkINV[8] * X3;
+    X2 = DkINV[4] * (X2 - DkINV[5] * X3);
+    X1 = DkINV[0] * (X1 - DkINV[2] * X3 - DkINV[1] * X2);
+    RHS[c] = Aik[0] * X1 + Aik[1] * X2 + Aik[2] * X3;
+    RHS[3 + c] = Aik[3] * X1 + Aik[4] * X2 + Aik[5] * X3;
+    RHS[6 + c] = Aik[6] * X1 + Aik[7] * X2 + Aik[8] * X3;
+  }
+}
+
+/* FORM_ILU0_33: hecmw_precond_BILU_33.f90:185-362.  The reference clears its
+ * IW1/IW2 marker arrays in full for every row (O(NP^2)); clearing only the
+ * entries that were set gives the same markers.  As in the reference, j == i
+ * never matches a marker (a row's own id is in neither of its L/U lists), so
+ * the diagonal blocks are not updated by the elimination. */
+static o33_precond *bilu0_setup(const o33_matrix *A, double sigma_diag, int *ierr) {
+  const int NP = A->NP, NPL = A->NPL, NPU = A->NPU;
+  o33_precond *P = (o33_precond *)calloc(1, sizeof(o33_precond));
+  P->kind = 10;
+  P->N = A->N;
+  P->NP = NP;
+  P->Dlu0 = (double *)malloc(sizeof(double) * 9 * (size_t)NP);
+  P->ALlu0 = (double *)malloc(sizeof(double) * 9 * ((size_t)NPL + 1));
+  P->AUlu0 = (double *)malloc(sizeof(double) * 9 * ((size_t)NPU + 1));
+  memcpy(P->Dlu0, A->D, sizeof(double) * 9 * (size_t)NP);
+  memcpy(P->ALlu0, A->AL, sizeof(double) * 9 * (size_t)NPL);
+  memcpy(P->AUlu0, A->AU, sizeof(double) * 9 * (size_t)NPU);
+  P->own_inL = (int *)malloc(sizeof(int) * ((size_t)NP + 1));
+  P->own_inU = (int *)malloc(sizeof(int) * ((size_t)NP + 1));
+  P->own_iaL = (int *)malloc(sizeof(int) * ((size_t)NPL + 1));
+  P->own_iaU = (int *)malloc(sizeof(int) * ((size_t)NPU + 1));
+  memcpy(P->own_inL, A->indexL, sizeof(int) * ((size_t)NP + 1));
+  memcpy(P->own_inU, A->indexU, sizeof(int) * ((size_t)NP + 1));
+  memcpy(P->own_iaL, A->itemL, sizeof(int) * (size_t)NPL);
+  memcpy(P->own_iaU, A->itemU, sizeof(int) * (size_t)NPU);
+  P->inL = P->own_inL;
+  P->inU = P->own_inU;
+  P->iaL = P->own_iaL;
+  P->iaU = P->own_iaU;
+  *ierr = 0;
+  for (int i = 0; i < NP; i++) {
+    P->Dlu0[9 * i + 0] = P->Dlu0[9 * i + 0] * sigma_diag;
+    P->Dlu0[9 * i + 4] = P->Dlu0[9 * i + 4] * sigma_diag;
+    P->Dlu0[9 * i + 8] = P->Dlu0[9 * i + 8] * sigma_diag;
+  }
+  if (lu33(P->Dlu0, 1.0)) *ierr = ERR_ILU_ZERO_PIVOT;
+  int *IW1 = (int *)calloc((size_t)NP + 1, sizeof(int));
+  int *IW2 = (int *)calloc((size_t)NP + 1, sizeof(int));
+  double RHS[9];
+  for (int i = 2; i <= NP && !*ierr; i++) {
+    for (int k = P->inL[i - 1]; k < P->inL[i]; k++) IW1[P->iaL[k]] = k + 1;
+    for (int k = P->inU[i - 1]; k < P->inU[i]; k++) IW2[P->iaU[k]] = k + 1;
+    for (int kk = A->indexL[i - 1]; kk < A->indexL[i]; kk++) {
+      const int k = A->itemL[kk];
+      const double *DkINV = P->Dlu0 + 9 * (size_t)(k - 1);
+      double Aik[9];
+      memcpy(Aik, P->ALlu0 + 9 * (size_t)kk, sizeof(Aik));
+      for (int jj = A->indexU[k - 1]; jj < A->indexU[k]; jj++) {
+        const int j = A->itemU[jj];
+        if (IW1[j] == 0 && IW2[j] == 0) continue;
+        ilu1b33(RHS, DkINV, Aik, P->AUlu0 + 9 * (size_t)jj);
+        double *dst = NULL;
+        if (j == i) dst = P->Dlu0 + 9 * (size_t)(i - 1);
+        if (j < i) dst = P->ALlu0 + 9 * (size_t)(IW1[j] - 1);
+        if (j > i) dst = P->AUlu0 + 9 * (size_t)(IW2[j] - 1);
+        for (int e = 0; e < 9; e++) dst[e] = dst[e] - RHS[e];
+      }
+    }
+    if (lu33(P->Dlu0 + 9 * (size_t)(i - 1), 1.0)) *ierr = ERR_ILU_ZERO_PIVOT;
+    for (int k = P->inL[i - 1]; k < P->inL[i]; k++) IW1[P->iaL[k]] = 0;
+    for (int k = P->inU[i - 1]; k < P->inU[i]; k++) IW2[P->iaU[k]] = 0;
+  }
+  free(IW1);
+  free(IW2);
+  return P;
+}
+
+/* hecmw_precond_BILU_33_apply: hecmw_precond_BILU_33.f90:90-157 (serial) */
+static void bilu0_apply(const o33_precond *P, double *WW) {
+  const int N = P->N;
+  for (int i = 1; i <= N; i++) {
+    double SW1 = WW[3 * (i - 1)], SW2 = WW[3 * (i - 1) + 1], SW3 = WW[3 * (i - 1) + 2];
+    for (int j = P->inL[i - 1]; j < P->inL[i]; j++) {
+      const int k = P->iaL[j];
+      const double X1 = WW[3 * (k - 1)], X2 = WW[3 * (k - 1) + 1], X3 = WW[3 * (k - 1) + 2];
+      const double *a = P->ALlu0 + 9 * (size_t)j;
+      SW1 = SW1 - a[0] * X1 - a[1] * X2 - a[2] * X3;
+      SW2 = SW2 - a[3] * X1 - a[4] * X2 - a[5] * X3;
+      SW3 = SW3 - a[6] * X1 - a[7] * X2 - a[8] * X3;
+    }
+    lu33_solve(P->Dlu0 + 9 * (size_t)(i - 1), &SW1, &SW2, &SW3);
+    WW[3 * (i - 1)] = SW1;
+    WW[3 * (i - 1) + 1] = SW2;
+    WW[3 * (i - 1) + 2] = SW3;
+  }
+  for (int i = N; i >= 1; i--) {
+    double SW1 = 0.0, SW2 = 0.0, SW3 = 0.0;
+    for (int j = P->inU[i] - 1; j >= P->inU[i - 1]; j--) {
+      const int k = P->iaU[j];
+      const double X1 = WW[3 * (k - 1)], X2 = WW[3 * (k - 1) + 1], X3 = WW[3 * (k - 1) + 2];
+      const double *a = P->AUlu0 + 9 * (size_t)j;
+      SW1 = SW1 + a[0] * X1 + a[1] * X2 + a[2] * X3;
+      SW2 = SW2 + a[3] * X1 + a[4] * X2 + a[5] * X3;
+      SW3 = SW3 + a[6] * X1 + a[7] * X2 + a[8] * X3;
+    }
+    lu33_solve(P->Dlu0 + 9 * (size_t)(i - 1), &SW1, &SW2, &SW3);
+    WW[3 * (i - 1)] = WW[3 * (i - 1)] - SW1;
+    WW[3 * (i - 1) + 1] = WW[3 * (i - 1) + 1] - SW2;
+    WW[3 * (i - 1) + 2] = WW[3 * (i - 1) + 2] - SW3;
+  }
+}
+
+o33_precond *o33_precond_setup(const o33_matrix *A, int kind, int ncolor_in, double sigma_diag,
+                               int ssor_coloured, int *ierr) {
+  *ierr = 0;
+  switch (kind) {
+    case 1:
+    case 2:
+      return ssor_setup(A, ncolor_in, sigma_diag, ssor_coloured);
+    case 3:
+      return diag_setup(A, sigma_diag);
+    case 10: {
+      o33_precond *P = bilu0_setup(A, sigma_diag, ierr);
+      return P;
+    }
+    default:
+      *ierr = ERR_INCONS_PC;
+      return NULL;
+  }
+}
+
+void o33_precond_free(o33_precond *P) {
+  if (!P) return;
+  free(P->colorindex);
+  free(P->perm);
+  free(P->iperm);
+  free(P->indexL);
+  free(P->indexU);
+  free(P->itemL);
+  free(P->itemU);
+  free(P->AL);
+  free(P->AU);
+  free(P->ALU);
+  free(P->Dlu0);
+  free(P->ALlu0);
+  free(P->AUlu0);
+  free(P->own_inL);
+  free(P->own_inU);
+  free(P->own_iaL);
+  free(P->own_iaU);
+  free(P);
+}
+
+void o33_precond_sweep(const o33_precond *P, double *zp) {
+  switch (P->kind) {
+    case 1: ssor_apply(P, zp); break;
+    case 3: diag_apply(P, zp); break;
+    case 10: bilu0_apply(P, zp); break;
+    default: break;
+  }
+}
+
+int o33_precond_ncolor(const o33_precond *P) { return P->kind == 1 ? P->ncolor : 0; }
+
+void o33_precond_ordering(const o33_precond *P, int *colorindex, int *perm, int *iperm) {
+  if (P->kind != 1) return;
+  memcpy(colorindex, P->colorindex, sizeof(int) * ((size_t)P->ncolor + 1));
+  memcpy(perm, P->perm, sizeof(int) * (size_t)P->N);
+  memcpy(iperm, P->iperm, sizeof(int) * (size_t)P->N);
+}
+
+/* hecmw_precond_apply: hecmw_precond.f90:86-172 (ZP is a work vector of 3*NP) */
+void o33_precond_apply(const o33_precond *P, const o33_matrix *A, int iterpremax, const double *R,
+                       double *Z, double *ZP) {
+  const int NN = 3 * A->N, NPN = 3 * A->NP;
+  if (iterpremax <= 0 || P == NULL) {
+    for (int i = 0; i < NN; i++) Z[i] = R[i];
+    return;
+  }
+  for (int i = 0; i < NN; i++) ZP[i] = R[i];
+  for (int i = NN; i < NPN; i++) ZP[i] = 0.0;
+  for (int i = 0; i < NPN; i++) Z[i] = 0.0;
+  for (int it = 1; it <= iterpremax; it++) {
+    o33_precond_sweep(P, ZP);
+    for (int i = 0; i < NN; i++) Z[i] = Z[i] + ZP[i];
+    if (it == iterpremax) break;
+    o33_matresid(A, Z, R, ZP);
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* hecmw_solve_CG: hecmw_solver_CG.f90:77-279 (scaling off, no JAD, no ESTCOND) */
+enum { N_ITER_RECOMPUTE_R = 50 };
+
+int o33_cg(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
+           const double *B, double *X, int *iter_out, double *resid_out, double *resid_hist) {
+  const int NP = A->NP, NN = 3 * A->N;
+  const size_t len = 3 * (size_t)NP;
+  double *R = (double *)calloc(len, sizeof(double));
+  double *Z = (double *)calloc(len, sizeof(double)); /* Z and Q share storage */
+  double *Pv = (double *)calloc(len, sizeof(double));
+  double *WK = (double *)calloc(len, sizeof(double));
+  int error = 0, n_indef_precond = 0, iter;
+  double RHO1 = 0.0, BETA = 0.0, RESID = 0.0;
+
+  o33_matresid(A, X, B, R);
+  const double BNRM2 = o33_dot(NN, B, B);
+  if (BNRM2 == 0.0) {
+    maxit = 0;
+    RESID = 0.0;
+    for (size_t i = 0; i < len; i++) X[i] = 0.0;
+  }
+  for (iter = 1; iter <= maxit; iter++) {
+    o33_precond_apply(P, A, iterpremax, R, Z, WK);
+    const double RHO = o33_dot(NN, R, Z);
+    if (RHO == 0.0) break;
+    else if (iter > 1 && RHO * RHO1 <= 0) {
+      n_indef_precond++;
+      if (n_indef_precond >= 3) {
+        error = ERR_DIVERGE_PC;
+        break;
+      }
+    } else if (RHO != RHO) {
+      error = ERR_DIVERGE_NAN;
+      break;
+    }
+    if (iter == 1) memcpy(Pv, Z, sizeof(double) * (size_t)NN);
+    else {
+      BETA = RHO / RHO1;
+      xpay(NN, BETA, Z, Pv);
+    }
+    o33_matvec(A, Pv, Z); /* Q = A P  (Q shares Z) */
+    const double C1 = o33_dot(NN, Pv, Z);
+    if (C1 <= 0) {
+      error = ERR_DIVERGE_MAT;
+      break;
+    } else if (C1 != C1) {
+      error = ERR_DIVERGE_NAN;
+      break;
+    }
+    const double ALPHA = RHO / C1;
+    axpy(NN, ALPHA, Pv, X);
+    if (iter % N_ITER_RECOMPUTE_R == 0) o33_matresid(A, X, B, R);
+    else axpy(NN, -ALPHA, Z, R);
+    double DNRM2 = o33_dot(NN, R, R);
+    RESID = sqrt(DNRM2 / BNRM2);
+    if (resid_hist) resid_hist[iter - 1] = RESID;
+    if (RESID <= tol) {
+      if (iter % N_ITER_RECOMPUTE_R == 0) break;
+      o33_matresid(A, X, B, R);
+      DNRM2 = o33_dot(NN, R, R);
+      RESID = sqrt(DNRM2 / BNRM2);
+      if (RESID <= tol) break;
+    }
+    if (iter == maxit) error = ERR_NOCONV_MAXIT;
+    RHO1 = RHO;
+  }
+  /* a Fortran DO loop that runs to completion leaves ITER = MAXIT+1 */
+  *iter_out = iter;
+  *resid_out = RESID;
+  free(R);
+  free(Z);
+  free(Pv);
+  free(WK);
+  return error;
+}
+
+double o33_cg_fixed_iters(const o33_matrix *A, const o33_precond *P, int iterpremax, int n,
+                          const double *B, double *X) {
+  const int NP = A->NP, NN = 3 * A->N;
+  const size_t len = 3 * (size_t)NP;
+  double *R = (double *)calloc(len, sizeof(double));
+  double *Z = (double *)calloc(len, sizeof(double));
+  double *Pv = (double *)calloc(len, sizeof(double));
+  double *WK = (double *)calloc(len, sizeof(double));
+  double RHO1 = 1.0;
+  const double t0 = now_s();
+  o33_matresid(A, X, B, R);
+  const double BNRM2 = o33_dot(NN, B, B);
+  for (int iter = 1; iter <= n; iter++) {
+    o33_precond_apply(P, A, iterpremax, R, Z, WK);
+    const double RHO = o33_dot(NN, R, Z);
+    if (iter == 1) memcpy(Pv, Z, sizeof(double) * (size_t)NN);
+    else xpay(NN, RHO / RHO1, Z, Pv);
+    o33_matvec(A, Pv, Z);
+    const double C1 = o33_dot(NN, Pv, Z);
+    const double ALPHA = RHO / C1;
+    axpy(NN, ALPHA, Pv, X);
+    if (iter % N_ITER_RECOMPUTE_R == 0) o33_matresid(A, X, B, R);
+    else axpy(NN, -ALPHA, Z, R);
+    volatile double resid = sqrt(o33_dot(NN, R, R) / BNRM2);
+    (void)resid;
+    RHO1 = RHO;
+  }
+  const double t1 = now_s();
+  free(R);
+  free(Z);
+  free(Pv);
+  free(WK);
+  return t1 - t0;
+}
+
+/* hecmw_mat_recycle_precond_setting: hecmw_matrix_misc.F90:858-877 */
+static void recycle_precond_setting(int *Iarray) {
+  int *nrecycle = &Iarray[95], *numfact = &Iarray[96];
+  const int symbfact = Iarray[97], maxrecycle = Iarray[34];
+  if (symbfact >= 1) {
+    *numfact = 1;
+    *nrecycle = 0;
+  } else if (*numfact > 1) {
+    *nrecycle = 0;
+    *numfact = 1;
+  } else if (*numfact == 1) {
+    if (*nrecycle < maxrecycle) {
+      *numfact = 0;
+      (*nrecycle)++;
+    } else {
+      *nrecycle = 0;
+    }
+  }
+}
+
+int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, double *Rarray,
+              int ssor_coloured, o33_precond **cache, int *iter_out, double *resid_out,
+              double *resid_true_out) {
+  const int N = A->N, NP = A->NP;
+  *iter_out = 0;
+  *resid_out = 0.0;
+  *resid_true_out = 0.0;
+  /* hecmw_solve_check_zerorhs: hecmw_solver_Iterative.f90:284-323 (no MPC) */
+  double rhs = 0.0;
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < 3; j++) rhs = rhs + B[3 * i + j] * B[3 * i + j];
+  if (rhs == 0.0) {
+    for (size_t i = 0; i < 3 * (size_t)NP; i++) X[i] = 0.0;
+    Iarray[80] = 1;
+    Iarray[81] = 0;
+    return ERR_ZERO_RHS;
+  }
+  const int METHOD = Iarray[1], PRECOND = Iarray[2], iterPREmax = Iarray[4];
+  const int MAXIT = Iarray[0], NCOLOR_IN = Iarray[33];
+  const double TOL = Rarray[0];
+  double SIGMA_DIAG = Rarray[1];
+  int auto_sigma_diag = 0;
+  if (SIGMA_DIAG < 0.0) {
+    auto_sigma_diag = 1;
+    SIGMA_DIAG = 1.0;
+  }
+  /* hecmw_solve_check_zerodiag: :255-282 */
+  int zdiag = 0;
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < 3; j++)
+      if (fabs(A->D[9 * i + 4 * j]) == 0.0) zdiag = ERR_ZERO_DIAG;
+  if (zdiag && PRECOND < 10 && iterPREmax > 0) return ERR_ZERO_DIAG;
+  if (METHOD != 1) return ERR_INCONS_PC;
+  recycle_precond_setting(Iarray);
+
+  int error = 0, iter = 0;
+  double resid = 0.0;
+  for (;;) {
+    Iarray[80] = 0;
+    Iarray[81] = 0;
+    o33_precond *P = NULL;
+    if (iterPREmax > 0) {
+      const int need = (cache == NULL || *cache == NULL || (*cache)->kind != (PRECOND == 2 ? 1 : PRECOND) ||
+                        Iarray[97] == 1 || Iarray[96] == 1);
+      if (need) {
+        if (cache && *cache) {
+          o33_precond_free(*cache);
+          *cache = NULL;
+        }
+        int perr = 0;
+        P = o33_precond_setup(A, PRECOND, NCOLOR_IN, SIGMA_DIAG, ssor_coloured, &perr);
+        if (perr) {
+          o33_precond_free(P);
+          return perr;
+        }
+        if (cache) *cache = P;
+        Iarray[97] = 0;
+        Iarray[96] = 0;
+      } else {
+        P = *cache;
+      }
+    }
+    error = o33_cg(A, P, iterPREmax, MAXIT, TOL, B, X, &iter, &resid, NULL);
+    if (!cache) o33_precond_free(P);
+    if (error == ERR_DIVERGE_PC || error == ERR_DIVERGE_MAT || error == ERR_DIVERGE_NAN) {
+      Iarray[81] = 1;
+      if (PRECOND >= 10 && PRECOND < 20 && auto_sigma_diag == 1 && SIGMA_DIAG < 2.0) {
+        SIGMA_DIAG = SIGMA_DIAG + 0.1;
+        continue;
+      }
+    }
+    break;
+  }
+  const double resid2 = o33_rel_resid_L2(A, X, B);
+  if (resid2 < TOL) Iarray[80] = 1;
+  *iter_out = iter;
+  *resid_out = resid;
+  *resid_true_out = resid2;
+  return error;
+}

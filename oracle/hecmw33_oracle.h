@@ -1,0 +1,96 @@
+/*
+ * hecmw33_oracle.h -- CPU restatement of FrontISTR's 3x3-block CG solve path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the parity checker for the
+ * CUDA solver in frontistr_b200/.  Only tests/, __graft_entry__.smoke() and
+ * the CPU-baseline leg of bench.py may load it.  It is never part of the
+ * product path.
+ *
+ * Every function restates the cited reference Fortran line by line, keeping
+ * the reference's summation order, so that its results can be compared with
+ * the reference's own outputs (the golden vectors of tests/solver/CG) and
+ * with the GPU solver.
+ *
+ * Matrix layout (hecmwST_matrix, hecmw1/src/common/hecmw_util_f.F90:458-470):
+ *   indexL/indexU : NP+1 entries, index[0] = 0
+ *   itemL/itemU   : 1-based node ids, sorted ascending within each row
+ *   D  : 9*NP  row-major 3x3 blocks  (r1c1, r1c2, r1c3, r2c1, ...)
+ *   AL : 9*NPL, AU : 9*NPU
+ * Vectors have 3*NP entries.  Iarray/Rarray follow the index map of
+ * hecmw1/src/solver/matrix/hecmw_matrix_misc.F90:107-150 (1-based there,
+ * so Iarray[k-1] here holds Fortran Iarray(k)).
+ */
+#ifndef HECMW33_ORACLE_H
+#define HECMW33_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int N, NP, NPL, NPU;
+  const int *indexL, *itemL, *indexU, *itemU;
+  const double *D, *AL, *AU;
+} o33_matrix;
+
+/* ---- kernels of hecmw1/src/solver/las/hecmw_solver_las_33.F90 ---- */
+void o33_matvec(const o33_matrix *A, const double *x, double *y);
+void o33_matresid(const o33_matrix *A, const double *x, const double *b, double *r);
+double o33_rel_resid_L2(const o33_matrix *A, const double *x, const double *b);
+
+/* ---- hecmw1/src/solver/communication/hecmw_solver_misc.F90 ---- */
+double o33_dot(int n, const double *x, const double *y);
+
+/* ---- orderings (hecmw1/src/solver/matrix/hecmw_matrix_ordering_CM.f90, _MC.f90) ----
+ * perm[new-1] = old (1-based), iperm[old-1] = new (1-based). */
+void o33_ordering_rcm(int N, const int *indexL, const int *itemL,
+                      const int *indexU, const int *itemU, int *perm, int *iperm);
+/* colorindex must hold N+1 entries; returns NColor */
+int o33_ordering_mc(int N, const int *indexL, const int *itemL,
+                    const int *indexU, const int *itemU, const int *perm_cur,
+                    int ncolor_in, int *colorindex, int *perm, int *iperm);
+
+/* ---- preconditioners ---- */
+typedef struct o33_precond o33_precond;
+/* kind: 1,2 = SSOR, 3 = DIAG, 10 = BILU(0).
+ * ssor_coloured: 1 = RCM + multicolour ordering (the reference's OpenMP
+ * (>1 thread) and OpenACC path), 0 = natural order, one colour (1 thread). */
+o33_precond *o33_precond_setup(const o33_matrix *A, int kind, int ncolor_in,
+                               double sigma_diag, int ssor_coloured, int *ierr);
+void o33_precond_free(o33_precond *P);
+/* one sweep of the preconditioner, in place on zp (3*NP) */
+void o33_precond_sweep(const o33_precond *P, double *zp);
+/* hecmw_precond_apply: z = M^-1 r with iterPREmax outer passes */
+void o33_precond_apply(const o33_precond *P, const o33_matrix *A, int iterpremax,
+                       const double *r, double *z, double *zp);
+/* SSOR ordering queries */
+int o33_precond_ncolor(const o33_precond *P);
+void o33_precond_ordering(const o33_precond *P, int *colorindex, int *perm, int *iperm);
+
+/* ---- hecmw_solve (hecmw1/src/solver/main/hecmw_solver.f90:9-88) restricted to
+ * METHOD=1 (CG), PRECOND in {1,2,3,10}.  X holds x0 on entry and the solution on
+ * return.  Iarray flags 81/82/96/97/98 are updated as the reference does.
+ * Returns the solver error code (0, 2001, 2002, 3001..3004, 1001).  The
+ * preconditioner may be kept between calls through *cache (NULL to disable);
+ * the recycle policy of hecmw_mat_recycle_precond_setting decides reuse. */
+int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray,
+              double *Rarray, int ssor_coloured, o33_precond **cache,
+              int *iter_out, double *resid_out, double *resid_true_out);
+
+/* CG iterations only (hecmw_solve_CG), given a ready preconditioner.
+ * resid_hist (optional, length >= maxit) receives RESID per iteration. */
+int o33_cg(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit,
+           double tol, const double *B, double *X, int *iter_out, double *resid_out,
+           double *resid_hist);
+
+/* run exactly n CG iterations (no convergence exit) and return elapsed seconds;
+ * used for the bounded CPU-baseline sample. */
+double o33_cg_fixed_iters(const o33_matrix *A, const o33_precond *P, int iterpremax,
+                          int n, const double *B, double *X);
+
+int o33_max_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
