@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 3x3-block CG drop-in (FrontISTR hecmw_solve, METHOD=CG).
+
+Workload (default): the 100x100x100 HEX8 linear-elastic cantilever cube --
+1,030,301 nodes, 3,090,903 DOF, 27,270,901 3x3 FP64 blocks (~2 GB of values) --
+E=210000, nu=0.3, 2x2x2 Gauss, face z=0 clamped, -1.0 y-load on every node of
+face z=100, assembled on the host like fistr1 (synthetic input; there is no
+public dataset).  One step = one solve to relative residual 1e-8 with CG + SSOR
+(PRECOND=1, iterPREmax=1, ncolor_in=10, sigma_diag=1), X0 = 0.
+
+  value        seconds per solve with B, X and the matrix resident in HBM
+               (device events around the one-graph CG solve), max over ranks
+  e2e          seconds per solve through the drop-in C-ABI call with host buffers
+               (hecmw33_gpu_solve: matrix values + B + X uploaded, numeric
+               preconditioner rebuild, solve, X downloaded), wall clock
+  roofline     the plain FP64 SpMV (spmv_kernel) against measured HBM bandwidth
+  cpu_baseline the CPU oracle (C restatement of the reference's CG + SSOR,
+               OpenMP over all host cores) on a bounded sample of iterations,
+               extrapolated to this run's iteration count
+
+The path does not shard (one GPU domain): with --gpus N, N independent replicas
+run, one per GPU (torch.distributed only for the barrier and the max).
+`--impl reference` times the CPU oracle alone (the reference's own CPU path is
+Fortran and cannot be built on this image).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s to rel-res 1e-8, 3M-DOF HEX8 elasticity: learned+mixed vs FP64 CG on 1 B200"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mesh", default="100,100,100", help="nx,ny,nz HEX8 elements")
+    ap.add_argument("--precond", type=int, default=1)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--spmv-only", type=int, default=0,
+                    help="only build the system and run this many SpMV launches (profiling)")
+    return ap.parse_args()
+
+
+def pin_local_gpu():
+    """One process per GPU: expose only this rank's GPU before CUDA initialises."""
+    lr = os.environ.get("LOCAL_RANK")
+    if lr is None:
+        return
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    ids = vis.split(",") if vis else None
+    os.environ["CUDA_VISIBLE_DEVICES"] = ids[int(lr)] if ids else lr
+
+
+class Clocks:
+    """Samples nvidia-smi every 200 ms while the timed region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid, self.proc, self.lines = uuid, None, []
+
+    def start(self):
+        try:
+            cmd = ["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.uuid:
+                cmd += ["-i", self.uuid]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax = max(smax, float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def spmv_traffic_from_profile(tag):
+    """Per-launch DRAM bytes of the SpMV from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "spmv_kernel_%s.txt" % tag)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_launch_full:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def build_system(nx, ny, nz):
+    from frontistr_b200.mesh import box_system
+    m = box_system(nx, ny, nz)
+    return m
+
+
+def solver_flags(m, precond, tol, maxit=20000):
+    m.set_precond(precond)
+    m.set_iter(maxit)
+    m.set_resid(tol)
+    return m
+
+
+def cpu_oracle_sample(m, precond, iters_full, budget_s, steps=1):
+    """Times the CPU oracle (test infrastructure) on a bounded sample of iterations."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import numpy as np
+    import oracle_ctypes
+    oracle_ctypes.build()
+    L = oracle_ctypes.lib()
+    orc = oracle_ctypes.Oracle(m)
+    t0 = time.time()
+    pc = orc.precond(precond, 10, 1.0, 1)
+    t_setup = time.time() - t0
+    X = np.zeros(3 * m.NP)
+    import ctypes
+    # calibrate with 3 iterations, then size the sample to the time budget
+    t3 = L.o33_cg_fixed_iters(ctypes.byref(orc.mat), pc.h, 1, 3, oracle_ctypes._dp(m.B), oracle_ctypes._dp(X))
+    n = int(max(5, min(iters_full, budget_s / max(t3 / 3.0, 1e-6))))
+    per_iter = []
+    for _ in range(steps):
+        X[:] = 0.0
+        t = L.o33_cg_fixed_iters(ctypes.byref(orc.mat), pc.h, 1, n, oracle_ctypes._dp(m.B), oracle_ctypes._dp(X))
+        per_iter.append(t / n)
+    cores = L.o33_max_threads()
+    return per_iter, n, cores, t_setup
+
+
+def iterations_for(nx, ny, nz, precond):
+    """Iteration count of the oracle's full solve for the reference arm (no GPU there)."""
+    p = os.path.join(ROOT, "tests", "golden", "oracle_iterations.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        key = "%d,%d,%d/%d" % (nx, ny, nz, precond)
+        if key in d:
+            return int(d[key]), "oracle full solve (tests/golden/oracle_iterations.json)"
+    return None, None
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    nx, ny, nz = (int(v) for v in args.mesh.split(","))
+    m = solver_flags(build_system(nx, ny, nz), args.precond, args.tol)
+    iters, src = iterations_for(nx, ny, nz, args.precond)
+    if iters is None:
+        print(json.dumps({"impl": "reference", "unavailable": "no recorded oracle iteration count for this mesh"}))
+        return
+    budget = max(5.0, min(args.cpu_sample_s, 150.0 / max(1, args.steps + args.warmup)))
+    per_iter, n, cores, t_setup = cpu_oracle_sample(m, args.precond, iters, budget,
+                                                    steps=args.steps + args.warmup)
+    timed = per_iter[args.warmup:] or per_iter
+    value = statistics.mean(timed) * iters
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(timed) * n * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_dict(nx, ny, nz, m, args),
+        "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port",
+                         "sample": "%d CG+SSOR iterations per step of the C oracle (OpenMP, serial dots as the "
+                                   "reference), per-iteration time x %d iterations (%s); setup %.2f s not included"
+                                   % (n, iters, src, t_setup)},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def config_dict(nx, ny, nz, m, args):
+    return {"workload": "HEX8 cantilever %dx%dx%d elements (%d nodes, %d DOF, %d blocks), CG+%s to %g"
+                        % (nx, ny, nz, m.N, 3 * m.N, m.NZ, {1: "SSOR", 3: "DIAG", 10: "ILU(0)"}.get(args.precond),
+                           args.tol),
+            "nodes": m.N, "dof": 3 * m.N, "blocks": m.NZ, "precond": args.precond, "tol": args.tol,
+            "solver": "plain FP64 CG (drop-in)", "l2": "inputs larger than L2 (matrix ~2 GB)",
+            "parallelism": "replicas"}
+
+
+def main():
+    args = parse()
+    pin_local_gpu()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(0)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from frontistr_b200.solver import GpuSolver
+
+    nx, ny, nz = (int(v) for v in args.mesh.split(","))
+    m = solver_flags(build_system(nx, ny, nz), args.precond, args.tol)
+    solver = GpuSolver()
+    if args.spmv_only:
+        solver.set_matrix(m)
+        solver.time_spmv(args.spmv_only)
+        torch.cuda.synchronize()
+        return
+
+    # first drop-in call: symbolic setup, preconditioner, graph
+    first = m.copy()
+    info0 = solver.solve(first)
+    if info0["error"] != 0:
+        raise SystemExit("solve failed: %r" % info0)
+    ia, ra = first.Iarray.copy(), first.Rarray.copy()  # flags 97/98 now 0: reuse
+    dev = torch.device("cuda", 0)
+    dB = torch.from_numpy(m.B).to(dev)
+    dX = torch.zeros_like(dB)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(0).uuid)
+    except Exception:
+        pass
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def step():
+        dX.zero_()
+        torch.cuda.synchronize()
+        rec = solver.solve_resident_device(dB.data_ptr(), dX.data_ptr(), ia.copy(), ra.copy())
+        if rec["error"] != 0:
+            raise SystemExit("solve failed: %r" % rec)
+        return rec
+
+    for _ in range(args.warmup):
+        step()
+    clocks = Clocks(uuid)
+    barrier()
+    clocks.start()
+    t0 = time.perf_counter()
+    recs = [step() for _ in range(args.steps)]
+    barrier()
+    wall = (time.perf_counter() - t0) / args.steps
+    clk = clocks.stop()
+    dev_s = statistics.mean(r["t_solve"] for r in recs)
+    info = solver.last_solve_info()
+    iters = recs[-1]["iter"]
+
+    # SpMV roofline, live: device events over back-to-back launches on the solver's stream
+    spmv_ms = solver.time_spmv(20)
+    peak, peak_kind = measured_peaks()
+    achieved = info["spmv_bytes"] / (spmv_ms * 1e-3) / 1e9
+    iter_s = dev_s / max(iters, 1)
+
+    # end-to-end through the drop-in call with host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e_t = []
+        for i in range(max(1, min(args.steps, 3)) + 1):
+            mm = m.copy()
+            mm.Iarray[97] = 0  # structure unchanged (flag 98)
+            mm.Iarray[96] = 2  # numerical preconditioner rebuild forced (flag 97), as a new Newton increment
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            rec = solver.solve(mm)
+            e2e_t.append(time.perf_counter() - t)
+            assert rec["error"] == 0
+        e2e_t = e2e_t[1:]
+        h2d = 8 * 9 * m.NZ + 2 * 8 * 3 * m.N
+        d2h = 8 * 3 * m.N
+        e2e = {"value": statistics.mean(e2e_t), "unit": "s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h}
+
+    vals = torch.tensor([dev_s, wall, e2e["value"] if e2e else 0.0], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    dev_s, wall = float(vals[0]), float(vals[1])
+    if e2e:
+        e2e["value"] = float(vals[2])
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        per_iter, n, cores, t_setup = cpu_oracle_sample(m, args.precond, iters, args.cpu_sample_s)
+        cpu = {"value": per_iter[0] * iters, "unit": "s", "cores": cores, "kind": "port",
+               "sample": "%d CG+SSOR iterations of the C oracle (OpenMP over %d threads, serial dots as the "
+                         "reference), per-iteration time x %d GPU iterations; oracle setup %.2f s not included"
+                         % (n, cores, iters, t_setup)}
+
+    if rank == 0:
+        tag = "%dcube" % nx if nx == ny == nz else "%dx%dx%d" % (nx, ny, nz)
+        line = {
+            "metric": METRIC, "value": dev_s, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_s * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(nx, ny, nz, m, args),
+            "iterations": iters, "wall_s_per_step": wall, "ms_per_iteration": iter_s * 1e3,
+            "iteration_GBps": info["iter_bytes"] / iter_s / 1e9,
+            "setup_s_first_call": info0["t_setup"],
+            "roofline": {"bound": "hbm", "kernel": "spmv_kernel (plain FP64 SpMV, y = A x)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": spmv_traffic_from_profile(tag),
+                         "algorithmic_bytes": info["spmv_bytes"], "ms_per_launch": spmv_ms},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": info["kernels"] * args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    solver.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,36 @@
+"""ctypes signatures of include/hecmw33_gpu.h (every argument by pointer)."""
+import ctypes
+
+_i = ctypes.POINTER(ctypes.c_int)
+_d = ctypes.POINTER(ctypes.c_double)
+_v = ctypes.c_void_p
+
+SIGNATURES = {
+    "hecmw33_gpu_create": [_i, _i],
+    "hecmw33_gpu_destroy": [_i, _i],
+    "hecmw33_gpu_set_matrix": [_i, _i, _i, _i, _i, _i, _i, _i, _i, _d, _d, _d, _i, _i],
+    "hecmw33_gpu_solve_resident": [_i, _d, _d, _i, _d, _i, _d, _d, _i],
+    "hecmw33_gpu_solve_resident_device": [_i, _v, _v, _i, _d, _i, _d, _d, _i],
+    "hecmw33_gpu_solve": [_i, _i, _i, _i, _i, _i, _i, _i, _i, _d, _d, _d, _d, _d, _i, _d, _i, _d,
+                          _d, _i],
+    "hecmw33_gpu_matvec": [_i, _d, _d, _i],
+    "hecmw33_gpu_precond_apply": [_i, _d, _d, _i, _d, _i],
+    "hecmw33_gpu_get_colouring": [_i, _i, _i, _i, _i],
+    "hecmw33_gpu_colour_schedule": [_i, _i, _i, _i, _i, _i, _i, _i, _i, _i],
+    "hecmw33_gpu_last_solve_info": [_i, _i, _d, _i],
+    "hecmw33_gpu_time_spmv": [_i, _i, _d, _i],
+    "hecmw33_gpu_last_error": [ctypes.c_char_p, ctypes.c_int],
+}
+
+RESTYPES = {"hecmw33_gpu_last_error": ctypes.c_int}
+
+
+def declare(lib):
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = RESTYPES.get(name, None)
+
+
+def exported_names():
+    return sorted(SIGNATURES)

@@ -41,7 +41,7 @@ def _stale(target, sources):
 
 def gpu_sources():
     srcs = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))
-            if f.endswith((".cu", ".cuh", ".h", ".hpp"))]
+            if f.endswith((".cu", ".cuh", ".h", ".hpp")) or f.startswith("h33_")]
     srcs.append(os.path.join(ROOT, "include", "hecmw33_gpu.h"))
     return srcs
 
@@ -49,13 +49,15 @@ def gpu_sources():
 def build_gpu(force=False, verbose_ptxas=False):
     os.makedirs(LIB, exist_ok=True)
     target = os.path.join(LIB, "libhecmw33_gpu.so")
-    cu = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith(".cu")]
+    cu = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))
+          if f.endswith(".cu") or (f.startswith("h33_") and f.endswith(".cpp"))]
     if not force and not _stale(target, gpu_sources()):
         return target
     cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "-ccbin", shutil.which("g++") or "g++",
            "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           "--expt-relaxed-constexpr", "-o", target, *cu, "-lcudart"]
+           "-Xcompiler", "-fopenmp", "--expt-relaxed-constexpr", "-o", target, *cu,
+           "-lcudart", "-lgomp"]
     if verbose_ptxas:
         cmd.insert(1, "-Xptxas=-v")
     _run(cmd)

@@ -1,0 +1,413 @@
+// h33_setup.cpp -- host-side symbolic setup of the B200 3x3 solver.
+//
+// The orderings must reproduce the reference's colour schedule exactly (the same
+// permutation and COLORindex), so their steps follow the reference algorithms:
+//   RCM   hecmw1/src/solver/matrix/hecmw_matrix_ordering_CM.f90:18-245
+//   MC    hecmw1/src/solver/matrix/hecmw_matrix_ordering_MC.f90:15-72
+//   reorder hecmw1/src/solver/matrix/hecmw_matrix_reorder.f90:20-158
+//   ILU(0) hecmw1/src/solver/precond/bilu/hecmw_precond_BILU_33.f90:185-362,1493-1596
+// Everything here is 0-based; node ids in the input profile are 1-based.
+#include "h33_setup.h"
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <stdexcept>
+
+namespace h33 {
+
+namespace {
+
+// Degree = lower neighbours + upper neighbours inside the domain (count_degrees).
+std::vector<int> degrees(const Profile &p) {
+  std::vector<int> deg(p.N);
+  for (int i = 0; i < p.N; i++) {
+    int d = p.indexL[i + 1] - p.indexL[i];
+    for (int j = p.indexU[i]; j < p.indexU[i + 1]; j++)
+      if (p.itemU[j] <= p.N) d++;
+    deg[i] = d;
+  }
+  return deg;
+}
+
+// Middle-pivot Hoare partition sort of a level by degree (sort_nodes_by_degree).
+// Unstable; the order of equal degrees is part of the reference's result.
+void sort_level(int *item, int lo, int hi, const std::vector<int> &deg) {
+  while (lo < hi) {
+    const int pivot = deg[item[(lo + hi) / 2]];
+    int l = lo, r = hi;
+    for (;;) {
+      while (deg[item[l]] < pivot) l++;
+      while (pivot < deg[item[r]]) r--;
+      if (l >= r) break;
+      std::swap(item[l], item[r]);
+      l++;
+      r--;
+    }
+    // recurse into the left part, iterate on the right part (same order of work)
+    sort_level(item, lo, l - 1, deg);
+    lo = r + 1;
+  }
+}
+
+// One Cuthill-McKee sweep from `seed`; returns the number of levels and fills order.
+int cm_from_seed(const Profile &p, const std::vector<int> &deg, int seed, std::vector<int> &order) {
+  const int N = p.N;
+  std::vector<int> level_of(N, 0);
+  order.assign(N, 0);
+  int prev_begin = 0, prev_end = 1, count = 1;
+  order[0] = seed;
+  level_of[seed] = 1;
+  if (count == N) return 1;
+  for (int level = 2; level <= N; level++) {
+    const int begin = count;
+    for (int j = prev_begin; j < prev_end; j++) {
+      const int node = order[j];
+      for (int k = p.indexL[node]; k < p.indexL[node + 1]; k++) {
+        const int nb = p.itemL[k] - 1;
+        if (level_of[nb] == 0) {
+          level_of[nb] = level;
+          order[count++] = nb;
+        }
+      }
+      for (int k = p.indexU[node]; k < p.indexU[node + 1]; k++) {
+        const int nb1 = p.itemU[k];
+        if (nb1 > N) continue;
+        const int nb = nb1 - 1;
+        if (level_of[nb] == 0) {
+          level_of[nb] = level;
+          order[count++] = nb;
+        }
+      }
+    }
+    if (count == begin) {  // disconnected: start the next component at the lowest id
+      for (int nb = 0; nb < N; nb++)
+        if (level_of[nb] == 0) {
+          level_of[nb] = level;
+          order[count++] = nb;
+          break;
+        }
+    }
+    sort_level(order.data(), begin, count - 1, deg);
+    if (count == N) return level;
+    prev_begin = begin;
+    prev_end = count;
+  }
+  return N;
+}
+
+}  // namespace
+
+void ordering_rcm(const Profile &p, std::vector<int> &perm, std::vector<int> &iperm) {
+  const int N = p.N;
+  const std::vector<int> deg = degrees(p);
+  // up to five minimum-degree seeds in index order (find_minimum_degrees)
+  std::vector<int> seeds;
+  int degmin = N, nmin = 0;
+  for (int i = 0; i < N; i++) {
+    if (deg[i] == 0) continue;
+    if (deg[i] < degmin) {
+      degmin = deg[i];
+      nmin = 1;
+      seeds.assign(1, i);
+    } else if (deg[i] == degmin) {
+      nmin++;
+      if (nmin <= 5) seeds.push_back(i);
+    }
+  }
+  if (seeds.empty()) seeds.push_back(0);  // no edges at all: start from node 0
+  std::vector<std::vector<int>> orders(seeds.size());
+  std::vector<int> nlevel(seeds.size());
+#pragma omp parallel for schedule(static, 1)
+  for (int s = 0; s < int(seeds.size()); s++) nlevel[s] = cm_from_seed(p, deg, seeds[s], orders[s]);
+  size_t best = 0;
+  for (size_t s = 1; s < seeds.size(); s++)
+    if (nlevel[s] > nlevel[best]) best = s;
+  // reverse the chosen Cuthill-McKee order
+  perm.assign(N, 0);
+  iperm.assign(N, 0);
+  for (int pos = 0; pos < N; pos++) {
+    const int node = orders[best][pos];
+    const int rpos = N - 1 - pos;
+    iperm[node] = rpos;
+    perm[rpos] = node;
+  }
+}
+
+int ordering_mc(const Profile &p, const std::vector<int> &perm_cur, int ncolor_in,
+                std::vector<int> &colorindex, std::vector<int> &perm, std::vector<int> &iperm) {
+  const int N = p.N;
+  if (ncolor_in < 1) ncolor_in = 1;
+  const int per_colour = N / ncolor_in;  // colour size cap (0 = no cap)
+  std::vector<int> mark(N, 0);           // >0 colour, -1 neighbour of this colour
+  perm.assign(N, 0);
+  colorindex.assign(1, 0);
+  int done = 0, ncolor = 0;
+  for (int colour = 1; colour <= N; colour++) {
+    int taken = 0;
+    for (int i = 0; i < N; i++) {
+      const int node = perm_cur[i];
+      if (mark[node] != 0) continue;
+      mark[node] = colour;
+      perm[done++] = node;
+      taken++;
+      if (taken == per_colour || done == N) break;
+      for (int k = p.indexL[node]; k < p.indexL[node + 1]; k++) {
+        const int nb = p.itemL[k] - 1;
+        if (mark[nb] == 0) mark[nb] = -1;
+      }
+      for (int k = p.indexU[node]; k < p.indexU[node + 1]; k++) {
+        const int nb1 = p.itemU[k];
+        if (nb1 > N) continue;
+        if (mark[nb1 - 1] == 0) mark[nb1 - 1] = -1;
+      }
+    }
+    colorindex.push_back(done);
+    if (done == N) {
+      ncolor = colour;
+      break;
+    }
+    for (int i = 0; i < N; i++)
+      if (mark[i] == -1) mark[i] = 0;
+  }
+  iperm.assign(N, 0);
+  for (int i = 0; i < N; i++) iperm[perm[i]] = i;
+  return ncolor;
+}
+
+void unified_rows(const Profile &p, BlockRows &out) {
+  const int N = p.N, NPL = p.NPL();
+  const int64_t nz = int64_t(N) + NPL + p.NPU();
+  out.ptr.assign(size_t(N) + 1, 0);
+  out.col.resize(size_t(nz));
+  out.src.resize(size_t(nz));
+  for (int i = 0; i < N; i++)
+    out.ptr[i + 1] = out.ptr[i] + (p.indexL[i + 1] - p.indexL[i]) + 1 + (p.indexU[i + 1] - p.indexU[i]);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < N; i++) {
+    int64_t w = out.ptr[i];
+    for (int j = p.indexL[i]; j < p.indexL[i + 1]; j++) {
+      out.col[w] = p.itemL[j] - 1;
+      out.src[w++] = N + j;
+    }
+    out.col[w] = i;
+    out.src[w++] = i;
+    for (int j = p.indexU[i]; j < p.indexU[i + 1]; j++) {
+      out.col[w] = p.itemU[j] - 1;
+      out.src[w++] = N + NPL + j;
+    }
+  }
+}
+
+void reordered_rows(const Profile &p, const std::vector<int> &perm, const std::vector<int> &iperm,
+                    BlockRows &lower, BlockRows &upper) {
+  const int N = p.N, NPL = p.NPL();
+  lower.ptr.assign(size_t(N) + 1, 0);
+  upper.ptr.assign(size_t(N) + 1, 0);
+  // counts per new row
+  for (int inew = 0; inew < N; inew++) {
+    const int iold = perm[inew];
+    int nl = 0, nu = 0;
+    for (int j = p.indexL[iold]; j < p.indexL[iold + 1]; j++)
+      (iperm[p.itemL[j] - 1] < inew ? nl : nu)++;
+    for (int j = p.indexU[iold]; j < p.indexU[iold + 1]; j++) {
+      if (p.itemU[j] > N) continue;
+      (iperm[p.itemU[j] - 1] < inew ? nl : nu)++;
+    }
+    lower.ptr[inew + 1] = lower.ptr[inew] + nl;
+    upper.ptr[inew + 1] = upper.ptr[inew] + nu;
+  }
+  lower.col.resize(size_t(lower.ptr[N]));
+  lower.src.resize(size_t(lower.ptr[N]));
+  upper.col.resize(size_t(upper.ptr[N]));
+  upper.src.resize(size_t(upper.ptr[N]));
+#pragma omp parallel
+  {
+    std::vector<std::pair<int, int>> lo, up;  // (new column, raw block)
+#pragma omp for schedule(static)
+    for (int inew = 0; inew < N; inew++) {
+      const int iold = perm[inew];
+      lo.clear();
+      up.clear();
+      for (int j = p.indexL[iold]; j < p.indexL[iold + 1]; j++) {
+        const int jnew = iperm[p.itemL[j] - 1];
+        (jnew < inew ? lo : up).emplace_back(jnew, N + j);
+      }
+      for (int j = p.indexU[iold]; j < p.indexU[iold + 1]; j++) {
+        if (p.itemU[j] > N) continue;
+        const int jnew = iperm[p.itemU[j] - 1];
+        (jnew < inew ? lo : up).emplace_back(jnew, N + NPL + j);
+      }
+      std::sort(lo.begin(), lo.end());
+      std::sort(up.begin(), up.end());
+      int64_t w = lower.ptr[inew];
+      for (auto &e : lo) {
+        lower.col[w] = perm[e.first];  // column renumbered to the old node id
+        lower.src[w++] = e.second;
+      }
+      w = upper.ptr[inew];
+      for (auto &e : up) {
+        upper.col[w] = perm[e.first];
+        upper.src[w++] = e.second;
+      }
+    }
+  }
+}
+
+void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out) {
+  out = SellLayout();
+  const int ngroups = int(group_rows.size()) - 1;
+  out.group_slice.assign(size_t(ngroups) + 1, 0);
+  for (int g = 0; g < ngroups; g++) {
+    for (int r0 = group_rows[g]; r0 < group_rows[g + 1]; r0 += 32) {
+      const int nr = std::min(32, group_rows[g + 1] - r0);
+      int len = 0;
+      for (int l = 0; l < nr; l++) len = std::max<int>(len, int(rows.ptr[r0 + l + 1] - rows.ptr[r0 + l]));
+      out.row0.push_back(r0);
+      out.nrows.push_back(nr);
+      out.slot0.push_back(int(out.nslots));
+      out.len.push_back(len);
+      out.nslots += len;
+      if (out.nslots > (int64_t(1) << 31) / 32 / 9)
+        throw std::runtime_error("matrix too large for 32-bit slot offsets");
+    }
+    out.group_slice[g + 1] = int(out.row0.size());
+  }
+  out.nslices = int(out.row0.size());
+  out.rowlen.assign(size_t(out.nslices) * 32, 0);
+  out.col.assign(size_t(out.nslots) * 32, 0);
+  out.src.assign(size_t(out.nslots) * 32, -1);
+#pragma omp parallel for schedule(static)
+  for (int s = 0; s < out.nslices; s++) {
+    for (int l = 0; l < out.nrows[s]; l++) {
+      const int r = out.row0[s] + l;
+      const int64_t b = rows.ptr[r];
+      const int n = int(rows.ptr[r + 1] - b);
+      out.rowlen[size_t(s) * 32 + l] = n;
+      for (int k = 0; k < n; k++) {
+        const size_t at = (size_t(out.slot0[s]) + k) * 32 + l;
+        out.col[at] = rows.col[b + k];
+        out.src[at] = rows.src[b + k];
+      }
+    }
+  }
+}
+
+namespace {
+
+// In-place 3x3 LU with reciprocal pivots (the reference's ALU / ILU1a33 form).
+bool lu33_inplace(double *a) {
+  double T[3][3] = {{a[0], a[1], a[2]}, {a[3], a[4], a[5]}, {a[6], a[7], a[8]}};
+  bool zero = false;
+  for (int k = 0; k < 3; k++) {
+    if (T[k][k] == 0.0) zero = true;
+    T[k][k] = 1.0 / T[k][k];
+    for (int i = k + 1; i < 3; i++) {
+      T[i][k] = T[i][k] * T[k][k];
+      double PW[3];
+      for (int j = k + 1; j < 3; j++) PW[j] = T[i][j] - T[i][k] * T[k][j];
+      for (int j = k + 1; j < 3; j++) T[i][j] = PW[j];
+    }
+  }
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) a[3 * r + c] = T[r][c];
+  return zero;
+}
+
+// RHS = Aik * Dk^-1 * Akj with Dk in reciprocal-pivot LU form (ILU1b33).
+void aik_dinv_akj(double *RHS, const double *Dk, const double *Aik, const double *Akj) {
+  for (int c = 0; c < 3; c++) {
+    double x1 = Akj[c], x2 = Akj[3 + c], x3 = Akj[6 + c];
+    x2 = x2 - Dk[3] * x1;
+    x3 = x3 - Dk[6] * x1 - Dk[7] * x2;
+    x3 = Dk[8] * x3;
+    x2 = Dk[4] * (x2 - Dk[5] * x3);
+    x1 = Dk[0] * (x1 - Dk[2] * x3 - Dk[1] * x2);
+    RHS[c] = Aik[0] * x1 + Aik[1] * x2 + Aik[2] * x3;
+    RHS[3 + c] = Aik[3] * x1 + Aik[4] * x2 + Aik[5] * x3;
+    RHS[6 + c] = Aik[6] * x1 + Aik[7] * x2 + Aik[8] * x3;
+  }
+}
+
+}  // namespace
+
+int factor_bilu0(const Profile &p, const double *D, const double *AL, const double *AU,
+                 double sigma_diag, std::vector<double> &Dlu0, std::vector<double> &ALlu0,
+                 std::vector<double> &AUlu0) {
+  const int N = p.N, NPL = p.NPL(), NPU = p.NPU();
+  Dlu0.assign(D, D + 9 * size_t(N));
+  ALlu0.assign(AL, AL + 9 * size_t(NPL));
+  AUlu0.assign(AU, AU + 9 * size_t(NPU));
+  for (int i = 0; i < N; i++) {
+    Dlu0[9 * size_t(i)] *= sigma_diag;
+    Dlu0[9 * size_t(i) + 4] *= sigma_diag;
+    Dlu0[9 * size_t(i) + 8] *= sigma_diag;
+  }
+  if (N > 0 && lu33_inplace(Dlu0.data())) return 9001;
+  // position markers of row i's lower / upper entries (0 = absent)
+  std::vector<int> posL(N, 0), posU(N, 0);
+  double RHS[9];
+  for (int i = 1; i < N; i++) {
+    for (int k = p.indexL[i]; k < p.indexL[i + 1]; k++) posL[p.itemL[k] - 1] = k + 1;
+    for (int k = p.indexU[i]; k < p.indexU[i + 1]; k++)
+      if (p.itemU[k] <= N) posU[p.itemU[k] - 1] = k + 1;
+    for (int kk = p.indexL[i]; kk < p.indexL[i + 1]; kk++) {
+      const int k = p.itemL[kk] - 1;
+      double Aik[9];
+      std::memcpy(Aik, &ALlu0[9 * size_t(kk)], sizeof(Aik));
+      const double *Dk = &Dlu0[9 * size_t(k)];
+      for (int jj = p.indexU[k]; jj < p.indexU[k + 1]; jj++) {
+        const int j = p.itemU[jj] - 1;
+        if (j >= N) continue;
+        // a row's own id is in neither of its lists, so j == i never passes here and
+        // the diagonal block is left as it is (as in the reference)
+        if (posL[j] == 0 && posU[j] == 0) continue;
+        aik_dinv_akj(RHS, Dk, Aik, &AUlu0[9 * size_t(jj)]);
+        double *dst = j < i ? &ALlu0[9 * size_t(posL[j] - 1)] : &AUlu0[9 * size_t(posU[j] - 1)];
+        for (int e = 0; e < 9; e++) dst[e] = dst[e] - RHS[e];
+      }
+    }
+    if (lu33_inplace(&Dlu0[9 * size_t(i)])) return 9001;
+    for (int k = p.indexL[i]; k < p.indexL[i + 1]; k++) posL[p.itemL[k] - 1] = 0;
+    for (int k = p.indexU[i]; k < p.indexU[i + 1]; k++)
+      if (p.itemU[k] <= N) posU[p.itemU[k] - 1] = 0;
+  }
+  return 0;
+}
+
+void level_schedule(const Profile &p, bool lower, std::vector<int> &order,
+                    std::vector<int> &level_ptr) {
+  const int N = p.N;
+  std::vector<int> lev(N, 0);
+  int maxlev = 0;
+  if (lower) {
+    for (int i = 0; i < N; i++) {
+      int l = 0;
+      for (int k = p.indexL[i]; k < p.indexL[i + 1]; k++) l = std::max(l, lev[p.itemL[k] - 1] + 1);
+      lev[i] = l;
+      maxlev = std::max(maxlev, l);
+    }
+  } else {
+    for (int i = N - 1; i >= 0; i--) {
+      int l = 0;
+      for (int k = p.indexU[i]; k < p.indexU[i + 1]; k++) {
+        if (p.itemU[k] > N) continue;
+        l = std::max(l, lev[p.itemU[k] - 1] + 1);
+      }
+      lev[i] = l;
+      maxlev = std::max(maxlev, l);
+    }
+  }
+  level_ptr.assign(size_t(maxlev) + 2, 0);
+  for (int i = 0; i < N; i++) level_ptr[lev[i] + 1]++;
+  for (int l = 0; l <= maxlev; l++) level_ptr[l + 1] += level_ptr[l];
+  order.assign(N, 0);
+  std::vector<int> fill(level_ptr.begin(), level_ptr.end() - 1);
+  for (int i = 0; i < N; i++) order[fill[lev[i]]++] = i;
+  if (!lower) {
+    // the backward sweep visits higher ids first inside a level; keep descending ids
+    for (int l = 0; l <= maxlev; l++) std::reverse(order.begin() + level_ptr[l], order.begin() + level_ptr[l + 1]);
+  }
+}
+
+}  // namespace h33

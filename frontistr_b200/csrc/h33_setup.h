@@ -1,0 +1,73 @@
+// h33_setup.h -- host-side symbolic setup of the B200 3x3 solver: orderings, reordered
+// profiles, block ILU(0) factorisation and the sliced block-ELL layouts.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace h33 {
+
+// Borrowed hecmwST_matrix profile (indexX[0..N], itemX 1-based ids).
+struct Profile {
+  int N;
+  const int *indexL, *itemL, *indexU, *itemU;
+  int NPL() const { return indexL[N]; }
+  int NPU() const { return indexU[N]; }
+};
+
+// Raw block numbering used on the device: blocks of D are 0..N-1, AL blocks
+// N..N+NPL-1 and AU blocks N+NPL..N+NPL+NPU-1 (the order of the upload buffer).
+
+// Reverse Cuthill-McKee (hecmw_matrix_ordering_CM.f90:18-245).
+// perm[new] = old, iperm[old] = new (0-based here).
+void ordering_rcm(const Profile &p, std::vector<int> &perm, std::vector<int> &iperm);
+
+// Greedy multicolouring in the order perm_cur (hecmw_matrix_ordering_MC.f90:15-72).
+// colorindex has ncolor+1 entries; returns ncolor.
+int ordering_mc(const Profile &p, const std::vector<int> &perm_cur, int ncolor_in,
+                std::vector<int> &colorindex, std::vector<int> &perm, std::vector<int> &iperm);
+
+// A row-wise list of blocks: for row r, entries [ptr[r], ptr[r+1]) of (col, src),
+// col = 0-based node index gathered by the kernel, src = raw block id.
+struct BlockRows {
+  std::vector<int64_t> ptr;
+  std::vector<int> col, src;
+};
+
+// Rows of the unified matrix (L, D, U per row, ascending column; raw ids).
+void unified_rows(const Profile &p, BlockRows &out);
+
+// SSOR reordering (hecmw_matrix_reorder.f90:20-158): rows in the new order, the
+// lower (new col < new row) and upper parts sorted by new column, columns
+// renumbered to old node ids, src = raw block id of the value.
+void reordered_rows(const Profile &p, const std::vector<int> &perm, const std::vector<int> &iperm,
+                    BlockRows &lower, BlockRows &upper);
+
+// Host-side sliced block-ELL layout; rows are taken in groups (a group never
+// shares a slice with another group), 32 consecutive rows per slice.
+struct SellLayout {
+  int nslices = 0;
+  int64_t nslots = 0;
+  std::vector<int> row0, nrows, slot0, len;  // per slice
+  std::vector<int> rowlen;                    // per slice*32 + lane
+  std::vector<int> col, src;                  // per slot*32 + lane (pad: col 0, src -1)
+  std::vector<int> group_slice;               // group g -> slices [group_slice[g], group_slice[g+1])
+};
+// group_rows: row boundaries of the groups (size ngroups+1, rows 0..nrows-1).
+void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out);
+
+// Block ILU(0) in natural order (FORM_ILU0_33, hecmw_precond_BILU_33.f90:185-362),
+// computed on the host from the hecmwST arrays.  Outputs the factor blocks in the
+// layout of the input (Dlu0 9N, ALlu0 9NPL, AUlu0 9NPU).  Returns 0 or 9001 on a
+// zero pivot.
+int factor_bilu0(const Profile &p, const double *D, const double *AL, const double *AU,
+                 double sigma_diag, std::vector<double> &Dlu0, std::vector<double> &ALlu0,
+                 std::vector<double> &AUlu0);
+
+// Level schedule of the natural-order lower (or upper) triangular solve:
+// level[i] = 1 + max level over dependencies.  rows sorted by level -> order,
+// boundaries in level_ptr.
+void level_schedule(const Profile &p, bool lower, std::vector<int> &order,
+                    std::vector<int> &level_ptr);
+
+}  // namespace h33

@@ -1,0 +1,200 @@
+"""Host-side mirror of FrontISTR's solver interface on top of the CUDA C ABI.
+
+``hecmw_solve(hecMAT)`` follows hecmw_solve (hecmw1/src/solver/main/hecmw_solver.f90:9-88)
+for METHOD=1: it updates hecMAT.X and the converged / diverged flags in
+hecMAT.Iarray(81)/(82), consumes the preconditioner flags 97/98 and returns the
+iteration record.  Error behaviour follows hecmw_solve_error
+(hecmw1/src/solver/init/hecmw_solve_error.f90:20-93): 1001 and 2001 abort the
+reference (here: HecmwSolverError is raised), 2002 and 3001 are warnings, and
+3002-3004 set the diverged flag.  There is no CPU fallback: every call goes to
+libhecmw33_gpu.so.
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import gpu_lib
+from .matrix import HecMatrix  # noqa: F401
+
+FATAL = {1001, 2001, 9001, 9100, 9101, 9102, 9103, 9104}
+
+
+class HecmwSolverError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__("HEC-MW-SOLVER-E-%d: %s" % (code, message))
+        self.code = code
+
+
+def _i(v):
+    return ctypes.byref(ctypes.c_int(int(v)))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def last_error():
+    lib = gpu_lib()
+    buf = ctypes.create_string_buffer(4096)
+    lib.hecmw33_gpu_last_error(buf, 4096)
+    return buf.value.decode(errors="replace")
+
+
+class GpuSolver:
+    """One solver handle (its own CUDA stream and device buffers)."""
+
+    def __init__(self):
+        self.lib = gpu_lib()
+        h, err = ctypes.c_int(0), ctypes.c_int(0)
+        self.lib.hecmw33_gpu_create(ctypes.byref(h), ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+        self.handle = h
+        self.N = None
+
+    def close(self):
+        if getattr(self, "handle", None) is not None:
+            err = ctypes.c_int(0)
+            self.lib.hecmw33_gpu_destroy(ctypes.byref(self.handle), ctypes.byref(err))
+            self.handle = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, code, fatal_only=True):
+        if code == 0:
+            return
+        if code in FATAL or not fatal_only:
+            raise HecmwSolverError(code, last_error())
+
+    # ---- matrix ------------------------------------------------------------
+    def set_matrix(self, m, Iarray=None):
+        err = ctypes.c_int(0)
+        ia = None if Iarray is None else np.ascontiguousarray(Iarray, dtype=np.int32)
+        self.lib.hecmw33_gpu_set_matrix(
+            ctypes.byref(self.handle), _i(m.N), _i(m.NP), _i(m.NPL), _i(m.NPU),
+            _ip(m.indexL), _ip(m.itemL), _ip(m.indexU), _ip(m.itemU), _dp(m.D), _dp(m.AL), _dp(m.AU),
+            _ip(ia) if ia is not None else None, ctypes.byref(err))
+        self._check(err.value)
+        self.N = m.N
+
+    def matvec(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_matvec(ctypes.byref(self.handle), _dp(x), _dp(y), ctypes.byref(err))
+        self._check(err.value)
+        return y
+
+    def precond_apply(self, r, Iarray, Rarray):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty_like(r)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_precond_apply(ctypes.byref(self.handle), _dp(r), _dp(z), _ip(Iarray),
+                                           _dp(Rarray), ctypes.byref(err))
+        self._check(err.value)
+        return z
+
+    def colouring(self):
+        n = self.N
+        nc = ctypes.c_int(0)
+        ci = np.zeros(n + 1, np.int32)
+        perm = np.zeros(n, np.int32)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_get_colouring(ctypes.byref(self.handle), ctypes.byref(nc), _ip(ci), _ip(perm),
+                                           ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+        return ci[:nc.value + 1].copy(), perm
+
+    # ---- solves ------------------------------------------------------------
+    def _record(self, err, it, res, times):
+        return dict(error=err, iter=it.value, resid=res.value, t_setup=times[0], t_solve=times[1],
+                    t_comm=times[2])
+
+    def solve(self, m):
+        """The drop-in hecmw_solve: matrix upload + solve; updates m.X and m.Iarray."""
+        err, it, res = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+        times = np.zeros(3)
+        self.lib.hecmw33_gpu_solve(
+            ctypes.byref(self.handle), _i(m.N), _i(m.NP), _i(m.NPL), _i(m.NPU),
+            _ip(m.indexL), _ip(m.itemL), _ip(m.indexU), _ip(m.itemU), _dp(m.D), _dp(m.AL), _dp(m.AU),
+            _dp(m.B), _dp(m.X), _ip(m.Iarray), _dp(m.Rarray), ctypes.byref(it), ctypes.byref(res),
+            _dp(times), ctypes.byref(err))
+        self.N = m.N
+        self._check(err.value)
+        return self._record(err.value, it, res, times)
+
+    def solve_resident(self, B, X, Iarray, Rarray):
+        """Solve on the matrix already uploaded; X (host) is updated in place."""
+        err, it, res = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+        times = np.zeros(3)
+        self.lib.hecmw33_gpu_solve_resident(ctypes.byref(self.handle), _dp(B), _dp(X), _ip(Iarray),
+                                            _dp(Rarray), ctypes.byref(it), ctypes.byref(res), _dp(times),
+                                            ctypes.byref(err))
+        self._check(err.value)
+        return self._record(err.value, it, res, times)
+
+    def solve_resident_device(self, dB_ptr, dX_ptr, Iarray, Rarray):
+        """Solve with B and X in device memory (raw device pointers, e.g. tensor.data_ptr())."""
+        err, it, res = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+        times = np.zeros(3)
+        self.lib.hecmw33_gpu_solve_resident_device(ctypes.byref(self.handle), ctypes.c_void_p(dB_ptr),
+                                                   ctypes.c_void_p(dX_ptr), _ip(Iarray), _dp(Rarray),
+                                                   ctypes.byref(it), ctypes.byref(res), _dp(times),
+                                                   ctypes.byref(err))
+        self._check(err.value)
+        return self._record(err.value, it, res, times)
+
+    def last_solve_info(self):
+        info = np.zeros(8, np.int32)
+        dinfo = np.zeros(8)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_last_solve_info(ctypes.byref(self.handle), _ip(info), _dp(dinfo), ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+        return dict(iter=int(info[0]), kernels=int(info[1]), sweep_groups=int(info[2]),
+                    kernels_per_iter=int(info[3]), nz_blocks=int(info[4]), spmv_slices=int(info[5]),
+                    spmv_slots=int(info[6]), t_solve=float(dinfo[0]), t_setup=float(dinfo[1]),
+                    spmv_bytes=float(dinfo[2]), iter_bytes=float(dinfo[3]), device_bytes=float(dinfo[4]))
+
+    def time_spmv(self, reps=20):
+        ms = ctypes.c_double(0)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_time_spmv(ctypes.byref(self.handle), _i(reps), ctypes.byref(ms), ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+        return ms.value
+
+
+_default = None
+
+
+def hecmw_solve(hecMAT, solver=None):
+    """hecmw_solve(hecMESH, hecMAT) for one GPU domain: updates hecMAT.X and flags."""
+    global _default
+    if solver is None:
+        if _default is None:
+            _default = GpuSolver()
+        solver = _default
+    return solver.solve(hecMAT)
+
+
+def colour_schedule(m, ncolor_in=10):
+    """Host-only SSOR colour schedule (RCM + multicolouring) of a HecMatrix profile."""
+    lib = gpu_lib()
+    n = m.N
+    nc = ctypes.c_int(0)
+    ci = np.zeros(n + 1, np.int32)
+    perm = np.zeros(n, np.int32)
+    err = ctypes.c_int(0)
+    lib.hecmw33_gpu_colour_schedule(_i(n), _ip(m.indexL), _ip(m.itemL), _ip(m.indexU), _ip(m.itemU),
+                                    _i(ncolor_in), ctypes.byref(nc), _ip(ci), _ip(perm), ctypes.byref(err))
+    if err.value:
+        raise HecmwSolverError(err.value, last_error())
+    return ci[:nc.value + 1].copy(), perm

@@ -1,0 +1,154 @@
+/*
+ * hecmw33_gpu.h -- C ABI of the B200 (sm_100a) 3x3-block CG solver, a drop-in for
+ * FrontISTR's hecmw_solve on a hecmwST_matrix with NDOF = 3 and METHOD = 1 (CG).
+ *
+ * Reference interfaces replaced (paths inside the FrontISTR tree):
+ *   hecmw_solve(hecMESH, hecMAT)          hecmw1/src/solver/main/hecmw_solver.f90:9
+ *   hecmw_solve_iterative(hecMESH, hecMAT) hecmw1/src/solver/iterative/hecmw_solver_Iterative.f90:13
+ *   hecmw_solve_CG(hecMESH, hecMAT, ITER, RESID, error, Tset, Tsol, Tcomm)
+ *                                          hecmw1/src/solver/iterative/hecmw_solver_CG.f90:19-20
+ *   hecmw_matvec / hecmw_matvec_33         hecmw1/src/solver/las/hecmw_solver_las.f90:42,
+ *                                          hecmw1/src/solver/las/hecmw_solver_las_33.F90:34
+ *   hecmw_precond_setup / _apply           hecmw1/src/solver/precond/hecmw_precond.f90:30,86
+ *   (C-side plugin precedent: hecmw_ML_wrapper_setup/apply/clear,
+ *    hecmw1/src/solver/precond/ml/hecmw_ML_wrapper.c:320,546,571)
+ *
+ * Conventions (all arguments by pointer, Fortran-callable; see the mangled
+ * aliases at the end):
+ *   - Matrix arrays use the hecmwST_matrix layout: indexL/indexU have NP+1 entries
+ *     (index[0] = 0); itemL/itemU hold 1-based node ids sorted ascending per row;
+ *     D has 9*NP, AL 9*NPL, AU 9*NPU doubles of row-major 3x3 blocks.
+ *   - Vectors B and X have 3*NP doubles.  Iarray[100]/Rarray[100] are hecMAT%Iarray
+ *     /Rarray (Iarray[k-1] is Fortran Iarray(k)); map in
+ *     hecmw1/src/solver/matrix/hecmw_matrix_misc.F90:107-150.
+ *   - Host pointers are borrowed for the duration of the call only.  Device buffers
+ *     belong to the handle.  One host thread per handle; every call is synchronous.
+ *   - One GPU domain: N == NP is required (no halo; hecmw_update_R is a no-op).
+ *   - *ierr receives 0 or an error code: the reference's codes (1001, 2001, 2002,
+ *     3001-3004; hecmw1/src/solver/init/hecmw_solve_error.f90:9-16) or the
+ *     HECMW33_ERR_* codes below.  1001 and 2001 are fatal in the reference
+ *     (hecmw_abort); 2002 and 3001 are warnings; 3002-3004 set the diverged flag.
+ */
+#ifndef HECMW33_GPU_H
+#define HECMW33_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define HECMW33_API __attribute__((visibility("default")))
+#else
+#define HECMW33_API
+#endif
+
+/* reference error codes (hecmw_solve_error.f90:9-16) */
+#define HECMW33_ERR_INCONS_PC 1001
+#define HECMW33_ERR_ZERO_DIAG 2001
+#define HECMW33_ERR_ZERO_RHS 2002
+#define HECMW33_ERR_NOCONV_MAXIT 3001
+#define HECMW33_ERR_DIVERGE_MAT 3002
+#define HECMW33_ERR_DIVERGE_PC 3003
+#define HECMW33_ERR_DIVERGE_NAN 3004
+/* codes of this library (no counterpart in the reference) */
+#define HECMW33_ERR_ILU_ZERO_PIVOT 9001 /* the reference stops the program here */
+#define HECMW33_ERR_CUDA 9100           /* CUDA runtime error; see hecmw33_gpu_last_error */
+#define HECMW33_ERR_BAD_INPUT 9101      /* inconsistent sizes, indices out of range, NP != N */
+#define HECMW33_ERR_BAD_HANDLE 9102
+#define HECMW33_ERR_TIMEOUT 9103        /* a bounded device-side wait gave up */
+#define HECMW33_ERR_NO_MATRIX 9104      /* solve/matvec before set_matrix */
+
+/* Create a solver handle bound to the current CUDA device (its own stream).
+ * Counterpart of the integer id table of hecmw1/src/solver/matrix/hecmw_mat_id.f90:21-72. */
+HECMW33_API void hecmw33_gpu_create(int *handle, int *ierr);
+
+/* Release every device buffer of the handle (hecmw_precond_clear + deallocation). */
+HECMW33_API void hecmw33_gpu_destroy(const int *handle, int *ierr);
+
+/* Upload the matrix.  Symbolic setup (device layout, SSOR ordering) runs when the
+ * handle has no matrix, when N/NP/NPL/NPU change, or when Iarray(98) != 0
+ * (hecMAT%Iarray(98): symbolic factorisation flag); otherwise only the values are
+ * copied and the device layout is reused.  Iarray may be NULL (= symbolic setup).
+ * Does not build the preconditioner (hecmw33_gpu_solve does, per flags 97/98). */
+HECMW33_API void hecmw33_gpu_set_matrix(const int *handle, const int *N, const int *NP,
+                                        const int *NPL, const int *NPU, const int *indexL,
+                                        const int *itemL, const int *indexU, const int *itemU,
+                                        const double *D, const double *AL, const double *AU,
+                                        const int *Iarray, int *ierr);
+
+/* hecmw_solve (hecmw_solver.f90:9-88) for METHOD=1 on the resident matrix:
+ * zero-RHS check, zero-diagonal check, preconditioner recycle policy
+ * (hecmw_matrix_misc.F90:858-877), preconditioner setup (PRECOND 1,2 = SSOR with the
+ * reference's RCM + multicolour ordering, 3 = DIAG, 10 = block ILU(0)), CG to
+ * Rarray(1), true relative residual, converged/diverged flags Iarray(81)/(82).
+ * B, X: host arrays of 3*NP (X: initial guess in, solution out).
+ * iter, resid: ITER and RESID as hecmw_solve_CG returns them.
+ * times[3]: set-up, solve and communication seconds (Tset, Tsol, Tcomm = 0). */
+HECMW33_API void hecmw33_gpu_solve_resident(const int *handle, const double *B, double *X,
+                                            int *Iarray, double *Rarray, int *iter,
+                                            double *resid, double *times, int *ierr);
+
+/* As hecmw33_gpu_solve_resident, with B and X in device memory (3*NP doubles each,
+ * on the handle's device).  Used when the caller keeps its vectors in HBM. */
+HECMW33_API void hecmw33_gpu_solve_resident_device(const int *handle, const double *dB,
+                                                   double *dX, int *Iarray, double *Rarray,
+                                                   int *iter, double *resid, double *times,
+                                                   int *ierr);
+
+/* The drop-in for hecmw_solve(hecMESH, hecMAT): set_matrix + solve_resident. */
+HECMW33_API void hecmw33_gpu_solve(const int *handle, const int *N, const int *NP,
+                                   const int *NPL, const int *NPU, const int *indexL,
+                                   const int *itemL, const int *indexU, const int *itemU,
+                                   const double *D, const double *AL, const double *AU,
+                                   const double *B, double *X, int *Iarray, double *Rarray,
+                                   int *iter, double *resid, double *times, int *ierr);
+
+/* y = A x on the resident matrix (hecmw_matvec_33), host vectors of 3*NP. */
+HECMW33_API void hecmw33_gpu_matvec(const int *handle, const double *X, double *Y, int *ierr);
+
+/* z = M^-1 r (hecmw_precond_apply, hecmw_precond.f90:86-172): builds the preconditioner
+ * selected by Iarray/Rarray if needed (same recycle rules as solve), then applies
+ * Iarray(5) = iterPREmax passes.  Host vectors of 3*NP. */
+HECMW33_API void hecmw33_gpu_precond_apply(const int *handle, const double *R, double *Z,
+                                           int *Iarray, double *Rarray, int *ierr);
+
+/* The SSOR colour schedule of the current preconditioner: *ncolor, colorindex[0..ncolor]
+ * (COLORindex) and perm[0..N-1] (new -> old, 1-based), as hecmw_precond_SSOR_33_setup
+ * builds them (hecmw_precond_SSOR_33.F90:93-128).  colorindex needs N+1 entries. */
+HECMW33_API void hecmw33_gpu_get_colouring(const int *handle, int *ncolor, int *colorindex,
+                                           int *perm, int *ierr);
+
+/* Host-only (no GPU needed): the SSOR colour schedule that hecmw33_gpu_solve would
+ * build for this profile with Iarray(34) = ncolor_in: RCM (hecmw_matrix_ordering_CM.f90)
+ * followed by multicolouring (hecmw_matrix_ordering_MC.f90).  Outputs as
+ * hecmw33_gpu_get_colouring (colorindex needs N+1 entries, perm N, 1-based ids). */
+HECMW33_API void hecmw33_gpu_colour_schedule(const int *N, const int *indexL, const int *itemL,
+                                             const int *indexU, const int *itemU,
+                                             const int *ncolor_in, int *ncolor, int *colorindex,
+                                             int *perm, int *ierr);
+
+/* Record of the last solve on this handle, the counterpart of the reference's
+ * TIMELOG summary and matvec bandwidth model (hecmw_solver_Iterative.f90:170-254):
+ *   info[0] iterations, info[1] kernels launched by the last solve (prologue +
+ *   iterations + epilogue), info[2] preconditioner sweep groups (colours or levels,
+ *   forward + backward), info[3] kernels per iteration, info[4] NZ (blocks),
+ *   info[5] SpMV slices, info[6] padded SpMV slots;
+ *   dinfo[0] solve seconds (device events), dinfo[1] setup seconds,
+ *   dinfo[2] algorithmic SpMV bytes (reference model: 72 NZ + 4 (NPL+NPU)
+ *   + 8 (N+1) + 24 N + 24 NP), dinfo[3] algorithmic bytes of one iteration,
+ *   dinfo[4] device bytes held by the handle.  info/dinfo need 8 entries each. */
+HECMW33_API void hecmw33_gpu_last_solve_info(const int *handle, int *info, double *dinfo, int *ierr);
+
+/* Times `reps` back-to-back launches of the plain SpMV y = A x on the resident
+ * matrix (x taken from the last solve) with device events on the handle's stream;
+ * *ms_per_launch receives the average.  For bandwidth measurements. */
+HECMW33_API void hecmw33_gpu_time_spmv(const int *handle, const int *reps, double *ms_per_launch,
+                                       int *ierr);
+
+/* Copies the message of the last error of the calling thread into buf; returns its length. */
+HECMW33_API int hecmw33_gpu_last_error(char *buf, int len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HECMW33_GPU_H */

@@ -159,14 +159,16 @@ class OraclePrecond:
         self.orc.L.o33_precond_ordering(self.h, _ip(ci), _ip(perm), _ip(iperm))
         return ci, perm, iperm
 
-    def cg(self, B, maxit=20000, tol=1e-8, iterpremax=1, X=None, hist=False):
-        m = self.orc.m
+    def cg(self, B, maxit=20000, tol=1e-8, iterpremax=1, X=None, hist=False, on=None):
+        """CG with this preconditioner; `on` (an Oracle) selects another matrix."""
+        orc = self.orc if on is None else on
+        m = orc.m
         B = np.ascontiguousarray(B, dtype=np.float64)
         X = np.zeros(3 * m.NP) if X is None else np.ascontiguousarray(X, dtype=np.float64).copy()
         it = ctypes.c_int(0)
         res = ctypes.c_double(0)
         h = np.zeros(maxit) if hist else None
-        err = self.orc.L.o33_cg(ctypes.byref(self.orc.mat), self.h, iterpremax, maxit, tol, _dp(B),
+        err = orc.L.o33_cg(ctypes.byref(orc.mat), self.h, iterpremax, maxit, tol, _dp(B),
                                 _dp(X), ctypes.byref(it), ctypes.byref(res),
                                 _dp(h) if hist else None)
         out = dict(X=X, error=err, iter=it.value, resid=res.value)

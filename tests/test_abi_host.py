@@ -1,0 +1,99 @@
+"""CPU-only checks of the C ABI library: it loads, exports every symbol that
+include/hecmw33_gpu.h declares, and its host-side colour schedule (RCM +
+multicolouring) is identical to the oracle's restatement of
+hecmw_matrix_ordering_CM.f90 / _MC.f90.  No GPU compute is called here."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from frontistr_b200 import _abi
+from frontistr_b200._lib import gpu_lib
+from frontistr_b200.matrix import HecMatrix
+from frontistr_b200.mesh import box_system
+from frontistr_b200.solver import HecmwSolverError, colour_schedule
+from oracle_ctypes import Oracle
+from test_oracle_golden import golden_system
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", fn)).read()
+            names |= set(re.findall(r"HECMW33_API\s+[\w\s\*]+?\b(hecmw33_\w+)\s*\(", txt))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = gpu_lib()
+    names = declared_symbols()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(lib, n), n
+    # and the Python declarations cover the header
+    assert names == set(_abi.exported_names())
+
+
+def oracle_schedule(m, ncolor_in):
+    orc = Oracle(m)
+    pc = orc.precond(1, ncolor_in=ncolor_in, coloured=1)
+    ci, perm, _ = pc.ordering()
+    return ci, perm
+
+
+@pytest.mark.parametrize("case", ["tet4", "box1", "box_small", "box_flat"])
+@pytest.mark.parametrize("ncolor_in", [10, 3, 50])
+def test_colour_schedule_matches_oracle(case, ncolor_in):
+    if case == "tet4":
+        _, m = golden_system()
+    elif case == "box1":
+        m = box_system(16, 16, 64)
+    elif case == "box_small":
+        m = box_system(3, 4, 5)
+    else:
+        m = box_system(9, 7, 1)
+    ci, perm = colour_schedule(m, ncolor_in)
+    ci_o, perm_o = oracle_schedule(m, ncolor_in)
+    assert np.array_equal(ci, ci_o)
+    assert np.array_equal(perm, perm_o)
+    # colours are independent sets (check_ordering, hecmw_precond_SSOR_33.F90:476-513)
+    colour = np.empty(m.N, np.int64)
+    for c in range(len(ci) - 1):
+        colour[perm[ci[c]:ci[c + 1]] - 1] = c
+    rows = np.repeat(np.arange(m.N), np.diff(m.indexU))
+    cols = m.itemU[:m.NPU] - 1
+    assert not np.any(colour[rows] == colour[cols])
+
+
+def test_colour_schedule_rejects_bad_profile():
+    m = box_system(2, 2, 2)
+    bad = m.copy()
+    bad.itemU[0] = bad.N + 5  # out of range
+    with pytest.raises(HecmwSolverError) as e:
+        colour_schedule(bad)
+    assert e.value.code == 9101
+
+
+def test_single_node_and_disconnected_profiles():
+    # one node, no neighbours
+    m = HecMatrix(1, 1, [0, 0], [0], [0, 0], [0], np.eye(3).ravel(), np.zeros(9), np.zeros(9))
+    ci, perm = colour_schedule(m)
+    assert list(ci) == [0, 1] and list(perm) == [1]
+    # two disconnected 2x2x2 boxes side by side in one profile
+    a = box_system(1, 1, 1)
+    n = a.N
+    indexL = np.concatenate([a.indexL, a.indexL[1:] + a.NPL])
+    indexU = np.concatenate([a.indexU, a.indexU[1:] + a.NPU])
+    itemL = np.concatenate([a.itemL[:a.NPL], a.itemL[:a.NPL] + n])
+    itemU = np.concatenate([a.itemU[:a.NPU], a.itemU[:a.NPU] + n])
+    D = np.concatenate([a.D, a.D])
+    m2 = HecMatrix(2 * n, 2 * n, indexL, itemL, indexU, itemU, D, np.concatenate([a.AL, a.AL]),
+                   np.concatenate([a.AU, a.AU]))
+    ci, perm = colour_schedule(m2)
+    ci_o, perm_o = oracle_schedule(m2, 10)
+    assert np.array_equal(ci, ci_o) and np.array_equal(perm, perm_o)

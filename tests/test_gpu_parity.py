@@ -1,0 +1,229 @@
+"""GPU parity of the CUDA solver against the CPU oracle, through the C ABI.
+
+Bars (from the drop-in contract):
+  * SpMV: within 1e-14 relative (to the row-sum of |A||x|, the scale that
+    bounds rounding of a dot product) of the oracle's hecmw_matvec_33.
+  * SSOR colour schedule: identical COLORindex and permutation.
+  * Preconditioner application: within 1e-12 relative of the oracle's sweep
+    (same operations, different summation order inside a row).
+  * CG: iteration count within +-2 of the oracle, solution within 1e-8
+    relative, true relative residual at or below the requested tolerance.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from frontistr_b200.matrix import HecMatrix
+from frontistr_b200.mesh import box_system
+from frontistr_b200.solver import GpuSolver, HecmwSolverError
+from oracle_ctypes import Oracle
+from test_oracle_golden import golden_system
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def solver():
+    s = GpuSolver()
+    yield s
+    s.close()
+
+
+def systems():
+    _, tet = golden_system()
+    return {
+        "tet4_golden": tet,
+        "box_16x16x64": box_system(16, 16, 64),
+        "box_jitter_10": box_system(10, 9, 11, jitter=0.2, sigma_E=1.0, nu_range=(0.25, 0.40), seed=7),
+        "box_3x4x5": box_system(3, 4, 5),
+    }
+
+
+SYSTEMS = systems()
+
+
+def mv_scale(m, x):
+    A = abs(m.to_scipy())
+    return A @ np.abs(x)
+
+
+@pytest.mark.parametrize("name", list(SYSTEMS))
+def test_spmv_matches_oracle(solver, name):
+    m = SYSTEMS[name]
+    solver.set_matrix(m)
+    rng = np.random.default_rng(1)
+    for _ in range(2):
+        x = rng.standard_normal(3 * m.NP)
+        y = solver.matvec(x)
+        y_ref = Oracle(m).matvec(x)
+        scale = mv_scale(m, x)
+        assert np.all(np.abs(y - y_ref) <= 1e-14 * scale + 1e-300)
+
+
+@pytest.mark.parametrize("name", ["tet4_golden", "box_16x16x64", "box_jitter_10"])
+@pytest.mark.parametrize("precond", [1, 3, 10])
+def test_precond_apply_matches_oracle(solver, name, precond):
+    m = SYSTEMS[name].copy()
+    m.set_precond(precond)
+    solver.set_matrix(m)
+    rng = np.random.default_rng(2)
+    r = rng.standard_normal(3 * m.NP)
+    ia, ra = m.Iarray.copy(), m.Rarray.copy()
+    z = solver.precond_apply(r, ia, ra)
+    pc = Oracle(m).precond(precond, ncolor_in=int(ia[33]), coloured=1)
+    z_ref = pc.apply(r, iterpremax=1)
+    assert np.linalg.norm(z - z_ref) <= 1e-12 * np.linalg.norm(z_ref)
+    if precond == 1:
+        ci, perm = solver.colouring()
+        ci_o, perm_o, _ = pc.ordering()
+        assert np.array_equal(ci, ci_o) and np.array_equal(perm, perm_o)
+
+
+@pytest.mark.parametrize("iterpremax", [0, 2])
+def test_precond_iterpremax(solver, iterpremax):
+    m = SYSTEMS["box_3x4x5"].copy()
+    solver.set_matrix(m)
+    m.set_iterpremax(iterpremax)
+    r = np.random.default_rng(3).standard_normal(3 * m.NP)
+    z = solver.precond_apply(r, m.Iarray.copy(), m.Rarray.copy())
+    z_ref = Oracle(m).precond(1).apply(r, iterpremax=iterpremax)
+    assert np.linalg.norm(z - z_ref) <= 1e-12 * np.linalg.norm(z_ref)
+
+
+def run_both(solver, m, precond, tol=1e-8, maxit=20000):
+    m = m.copy()
+    m.set_precond(precond)
+    m.set_iter(maxit)
+    m.set_resid(tol)
+    orc = Oracle(m).solve(coloured=1)
+    g = m.copy()
+    info = solver.solve(g)
+    return orc, info, g
+
+
+@pytest.mark.parametrize("name", ["tet4_golden", "box_16x16x64", "box_jitter_10"])
+@pytest.mark.parametrize("precond", [1, 3, 10])
+def test_cg_matches_oracle(solver, name, precond):
+    m = SYSTEMS[name]
+    orc, info, g = run_both(solver, m, precond)
+    assert orc["error"] == 0 and info["error"] == 0
+    assert abs(info["iter"] - orc["iter"]) <= 2, (info["iter"], orc["iter"])
+    assert np.linalg.norm(g.X - orc["X"]) <= 1e-8 * np.linalg.norm(orc["X"])
+    assert g.get_flag_converged() == 1 and g.get_flag_diverged() == 0
+    true_res = Oracle(m).rel_resid(g.X, m.B)
+    assert true_res <= 1e-8
+    assert info["resid"] <= 1e-8
+
+
+def test_cg_golden_displacement(solver):
+    g, m = golden_system()
+    for precond in (1, 10, 3):
+        mm = m.copy()
+        mm.set_precond(precond)
+        mm.set_iter(10000)
+        solver.solve(mm)
+        ref = np.array(g["displacement"][str(precond)])
+        assert np.abs(mm.X.reshape(-1, 3) - ref).max() <= 1e-9 * np.abs(ref).max()
+
+
+def test_cg_deterministic(solver):
+    m = SYSTEMS["box_16x16x64"]
+    a, b = m.copy(), m.copy()
+    ia = solver.solve(a)
+    ib = solver.solve(b)
+    assert ia["iter"] == ib["iter"]
+    assert np.array_equal(a.X, b.X)
+
+
+# ---- error contract (hecmw_solve_error.f90:9-16) ------------------------------
+def test_zero_rhs(solver):
+    m = SYSTEMS["box_3x4x5"].copy()
+    m.B[:] = 0.0
+    m.X[:] = 1.0
+    info = solver.solve(m)
+    assert info["error"] == 2002
+    assert np.all(m.X == 0.0) and m.get_flag_converged() == 1
+
+
+def test_zero_diagonal_is_fatal(solver):
+    m = SYSTEMS["box_3x4x5"].copy()
+    m.D[9 * 5 + 4] = 0.0
+    with pytest.raises(HecmwSolverError) as e:
+        solver.solve(m)
+    assert e.value.code == 2001
+
+
+def test_nan_rhs_diverges(solver):
+    m = SYSTEMS["box_3x4x5"].copy()
+    m.B[7] = np.nan
+    orc = Oracle(m).solve()
+    info = solver.solve(m)
+    assert info["error"] == orc["error"] == 3004
+    assert m.get_flag_diverged() == 1
+
+
+def test_indefinite_matrix(solver):
+    m = SYSTEMS["box_3x4x5"].copy()
+    m.D *= -1.0
+    m.AL *= -1.0
+    m.AU *= -1.0
+    m.set_precond(3)
+    orc = Oracle(m).solve()
+    info = solver.solve(m)
+    assert info["error"] == orc["error"]
+    assert info["error"] in (3002, 3003)
+    assert m.get_flag_diverged() == 1
+
+
+def test_maxit(solver):
+    m = SYSTEMS["box_16x16x64"].copy()
+    m.set_iter(5)
+    orc = Oracle(m).solve()
+    info = solver.solve(m)
+    assert info["error"] == orc["error"] == 3001
+    assert info["iter"] == orc["iter"] == 6  # a completed DO loop leaves MAXIT+1
+    assert m.get_flag_converged() == 0
+    assert np.linalg.norm(m.X - orc["X"]) <= 1e-10 * np.linalg.norm(orc["X"])
+
+
+def test_unsupported_method_is_fatal(solver):
+    m = SYSTEMS["box_3x4x5"].copy()
+    m.set_method(2)
+    with pytest.raises(HecmwSolverError) as e:
+        solver.solve(m)
+    assert e.value.code == 1001
+
+
+def test_recycle_policy_matches_oracle(solver):
+    """Newton-style reuse: the preconditioner of the first matrix is kept (flags 97/98
+    and maxrecycle), so the second solve runs on a stale SSOR like the reference."""
+    m1 = SYSTEMS["box_16x16x64"].copy()
+    m2 = m1.copy()
+    m2.D *= 1.3
+    m2.AL *= 1.3
+    m2.AU *= 1.3
+    ia = m1.Iarray.copy()
+    ra = m1.Rarray.copy()
+    s = GpuSolver()
+    try:
+        a = m1.copy()
+        a.Iarray, a.Rarray = ia, ra
+        s.solve(a)
+        assert ia[96] == 0 and ia[97] == 0
+        ia[96] = 1  # Newton iteration > 1: numerical setup requested, recycle decides
+        b = m2.copy()
+        b.Iarray, b.Rarray = ia, ra
+        info = s.solve(b)
+        assert ia[96] == 0 and ia[95] == 1  # recycled once
+        # oracle: keep the first matrix's SSOR, solve the second matrix
+        orc = Oracle(m2)
+        pc = Oracle(m1).precond(1)
+        ref = pc.cg(m2.B, maxit=20000, on=orc)
+        orc_res = orc.rel_resid(ref["X"], m2.B)
+        assert orc_res <= 1e-8
+        assert abs(info["iter"] - ref["iter"]) <= 2
+        assert np.linalg.norm(b.X - ref["X"]) <= 1e-8 * np.linalg.norm(ref["X"])
+    finally:
+        s.close()
