@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--spmv-only", type=int, default=0,
                     help="only build the system and run this many SpMV launches (profiling)")
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="one solve capped at 5 CG iterations, nothing printed (profiling)")
     return ap.parse_args()
 
 
@@ -248,6 +250,13 @@ def main():
         solver.set_matrix(m)
         solver.time_spmv(args.spmv_only)
         torch.cuda.synchronize()
+        return
+    if args.profile_solve:
+        mm = m.copy()
+        mm.set_iter(5)
+        rec = solver.solve(mm)
+        if rec["error"] not in (0, 3001):
+            raise SystemExit("solve failed: %r" % rec)
         return
 
     # first drop-in call: symbolic setup, preconditioner, graph

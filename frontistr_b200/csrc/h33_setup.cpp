@@ -398,6 +398,11 @@ void level_schedule(const Profile &p, bool lower, std::vector<int> &order,
       maxlev = std::max(maxlev, l);
     }
   }
+  // The backward sweep walks its groups from the last to the first (as the SSOR
+  // backward sweep walks the colours), so the upper schedule numbers its groups
+  // from the highest level down: group maxlev - l holds level l.
+  if (!lower)
+    for (int i = 0; i < N; i++) lev[i] = maxlev - lev[i];
   level_ptr.assign(size_t(maxlev) + 2, 0);
   for (int i = 0; i < N; i++) level_ptr[lev[i] + 1]++;
   for (int l = 0; l <= maxlev; l++) level_ptr[l + 1] += level_ptr[l];

@@ -65,8 +65,9 @@ int factor_bilu0(const Profile &p, const double *D, const double *AL, const doub
                  std::vector<double> &AUlu0);
 
 // Level schedule of the natural-order lower (or upper) triangular solve:
-// level[i] = 1 + max level over dependencies.  rows sorted by level -> order,
-// boundaries in level_ptr.
+// level[i] = 1 + max level over dependencies.  Rows sorted by group -> order,
+// group boundaries in level_ptr.  Lower: group = level (walked first to last).
+// Upper: group = maxlevel - level (walked last to first by the backward sweep).
 void level_schedule(const Profile &p, bool lower, std::vector<int> &order,
                     std::vector<int> &level_ptr);
 

@@ -14,9 +14,11 @@
 //      iteration; the device decides when the loop ends (cudaGraphSetConditional).
 //   5. true relative residual and the converged/diverged flags (Iterative.f90:131-157).
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -34,6 +36,21 @@ namespace h33 {
 namespace {
 
 thread_local std::string g_last_error;
+
+// NVTX range for profilers (no-op without a tool attached).
+struct Range {
+  explicit Range(const char *name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+};
+
+// HECMW33_GRAPH=0 selects stream mode: the same kernels launched from the host in
+// chunks of kStreamChunk iterations, the host reading the done flag in between
+// (used by profilers that replay single launches).
+bool graph_mode() {
+  const char *e = std::getenv("HECMW33_GRAPH");
+  return !(e && e[0] == '0');
+}
+constexpr int kStreamChunk = 16;
 
 double wall() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -118,6 +135,7 @@ struct Solver {
   cudaGraphExec_t exec = nullptr;
   int graph_key[4] = {-1, -1, -1, -1};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int build_counter = 0;  // monotonic id of preconditioner builds (graph cache key)
   // last-solve record
   int last_iter = 0, last_kernels = 0, kernels_per_iter = 0, prologue_kernels = 0;
   double last_solve_s = 0.0, last_setup_s = 0.0;
@@ -415,8 +433,11 @@ void precond_setup(Solver &S, int precond, int ncolor_in, double sigma, int *Iar
   S.sync();
   (void)err;  // a zero pivot in SSOR/DIAG gives Inf entries, as in the reference (no check there)
   P.valid = true;
-  P.generation++;
-  S.drop_graph();
+  if (symbolic) {
+    // new device buffers: graphs that captured the old ones must go
+    P.generation = ++S.build_counter;
+    S.drop_graph();
+  }
   Iarray[97] = 0;
   Iarray[96] = 0;
 }
@@ -600,11 +621,16 @@ int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *re
   if (METHOD != 1)
     throw Failure(HECMW33_ERR_INCONS_PC, "METHOD " + std::to_string(METHOD) + ": the GPU drop-in implements CG (1)");
   recycle_precond_setting(Iarray);
-  if (iterPREmax > 0) precond_setup(S, PRECOND, NCOLOR_IN, sigma, Iarray);
-  build_graph(S, iterPREmax);
+  {
+    Range rg("hecmw33_precond_setup");
+    if (iterPREmax > 0) precond_setup(S, PRECOND, NCOLOR_IN, sigma, Iarray);
+    if (graph_mode()) build_graph(S, iterPREmax);
+  }
+  Range rs("hecmw33_solve");
   const double t1 = wall();
   int error = 0;
   float ms_total = 0.0f;
+  const bool use_graph = graph_mode();
   for (;;) {
     Iarray[80] = 0;
     Iarray[81] = 0;
@@ -613,10 +639,23 @@ int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *re
     S.h_params->iterpremax = iterPREmax;
     H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, S.stream));
     H33_CUDA(cudaEventRecord(S.ev0, S.stream));
-    H33_CUDA(cudaGraphLaunch(S.exec, S.stream));
-    H33_CUDA(cudaEventRecord(S.ev1, S.stream));
-    H33_CUDA(cudaMemcpyAsync(S.h_state, S.state.p, sizeof(CgState), cudaMemcpyDeviceToHost, S.stream));
-    S.sync();
+    if (use_graph) {
+      H33_CUDA(cudaGraphLaunch(S.exec, S.stream));
+      H33_CUDA(cudaEventRecord(S.ev1, S.stream));
+      H33_CUDA(cudaMemcpyAsync(S.h_state, S.state.p, sizeof(CgState), cudaMemcpyDeviceToHost, S.stream));
+      S.sync();
+    } else {
+      launch_prologue(S, 0, 0);
+      for (int done = 0, it = 0; !done && it <= MAXIT + kStreamChunk; it += kStreamChunk) {
+        for (int k = 0; k < kStreamChunk; k++) launch_iteration(S, iterPREmax, 0, 0);
+        H33_CUDA(cudaGetLastError());
+        H33_CUDA(cudaMemcpyAsync(S.h_state, S.state.p, sizeof(CgState), cudaMemcpyDeviceToHost, S.stream));
+        S.sync();
+        done = S.h_state->done;
+      }
+      H33_CUDA(cudaEventRecord(S.ev1, S.stream));
+      S.sync();
+    }
     float ms = 0.0f;
     H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
     ms_total += ms;
