@@ -90,6 +90,18 @@ struct CgState {
   double rr_true;
   int iter, maxit, done, error, n_indef, recompute, converged, zero_rhs;
   int guard;  // body executions of this solve (fail-safe bound on the device loop)
+  int inner;  // inner solve of the mixed-precision refinement: no true-residual refresh
+  // flexible CG with the learned preconditioner
+  int flexible;   // BETA = z.(r - r_old) / RHO_old
+  int use_gnn;    // the network is applied after SSOR (cleared by the fallback)
+  int restart;    // next BETA is 0 (after a fallback)
+  int fallback;   // iteration at which the SSOR-CG fallback took over (0 = never)
+  double resid_mark;
+  float gamma;    // RMS of the SSOR output, the network's input/output scale
+  // mixed precision with reliable updates: FP32 CG whose solution and residual are
+  // folded into FP64 each time the FP32 residual falls by ru_delta
+  int reliable, ru_pending, ru_count;
+  double ru_delta, ru_mark;
   unsigned int ticket[8];
 };
 
@@ -98,6 +110,11 @@ struct CgParams {
   double tol;
   int maxit;
   int iterpremax;
+  int inner;  // 1: stop on the recursive residual (the outer FP64 loop checks the true one)
+  int flexible;  // 1: flexible CG (BETA of Polak-Ribiere form)
+  int use_gnn;   // 1: learned preconditioner active at the start of the solve
+  int reliable;  // 1: FP32 CG with FP64 reliable updates
+  double ru_delta;
 };
 
 }  // namespace h33

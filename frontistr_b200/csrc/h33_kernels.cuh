@@ -11,6 +11,8 @@
 // hecmw_solve_CG decisions (hecmw_solver_CG.f90:164-279).
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "h33_common.cuh"
 
 namespace h33 {
@@ -64,6 +66,37 @@ __device__ __forceinline__ void reduce_finish(double v, double *partials, int pa
   }
 }
 
+// As reduce_finish for two values at once (partials[part] and partials[total + part]).
+template <class Fin>
+__device__ __forceinline__ void reduce_finish2(double v1, double v2, double *partials, int part, int total,
+                                               unsigned int *ticket, Fin fin) {
+  __shared__ double sh[32];
+  __shared__ int is_last;
+  v1 = block_sum(v1, sh);
+  v2 = block_sum(v2, sh);
+  if (threadIdx.x == 0) {
+    partials[part] = v1;
+    partials[total + part] = v2;
+    __threadfence();
+    const unsigned int t = atomicAdd(ticket, 1u);
+    is_last = (t == unsigned(total) - 1u);
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  double s1 = 0.0, s2 = 0.0;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    s1 += __ldcg(&partials[i]);
+    s2 += __ldcg(&partials[total + i]);
+  }
+  s1 = block_sum(s1, sh);
+  s2 = block_sum(s2, sh);
+  if (threadIdx.x == 0) {
+    fin(s1, s2);
+    *ticket = 0u;
+  }
+}
+
 // ---- CG decisions (hecmw_solver_CG.f90) ------------------------------------
 __device__ __forceinline__ void set_loop(cudaGraphConditionalHandle h, int use_cond, int go) {
   if (use_cond) cudaGraphSetConditional(h, go ? 1u : 0u);
@@ -108,7 +141,56 @@ __device__ __forceinline__ void fin_pq(CgState *st, double c1) {
 __device__ __forceinline__ void fin_rr(CgState *st, double rr) {
   st->rr = rr;
   st->resid = sqrt(rr / st->bnrm2);
+  if (st->reliable) {
+    // FP32 recursive residual: ask for an FP64 reliable update when it has fallen
+    // by ru_delta since the last one, or reached the tolerance
+    if (st->resid <= st->ru_delta * st->ru_mark || st->resid <= st->tol) st->ru_pending = 1;
+    st->recompute = 0;
+    return;
+  }
+  if (st->inner) {
+    // inner solve of the refinement: the recursive residual decides; the outer
+    // FP64 loop recomputes the true residual itself
+    if (st->resid <= st->tol) {
+      st->done = 1;
+      st->converged = 1;
+    }
+    st->recompute = 0;
+    return;
+  }
   st->recompute = st->resid <= st->tol ? 1 : 0;
+}
+
+// Flexible CG: RHO = z.r, DELTA = z.r_old, BETA = (RHO - DELTA) / RHO_old (the
+// Polak-Ribiere form that keeps CG convergent with a preconditioner that changes
+// from one iteration to the next).  A non-positive RHO while the network is active
+// means the learned step points away from the error: the network is switched off
+// (SSOR-CG fallback) and the recurrence restarts.
+__device__ __forceinline__ void fin_rho_flex(CgState *st, double rho, double delta) {
+  st->rho = rho;
+  if (rho == 0.0) {
+    st->done = 1;
+    return;
+  }
+  if (rho != rho) {
+    st->error = HECMW33_ERR_DIVERGE_NAN;
+    st->done = 1;
+    return;
+  }
+  if (rho < 0.0 && st->use_gnn) {
+    st->use_gnn = 0;
+    st->fallback = st->iter;
+    st->restart = 1;
+  } else if (st->iter > 1 && !st->restart && rho * st->rho1 <= 0) {
+    st->n_indef++;
+    if (st->n_indef >= 3) {
+      st->error = HECMW33_ERR_DIVERGE_PC;
+      st->done = 1;
+      return;
+    }
+  }
+  st->beta = (st->iter == 1 || st->restart) ? 0.0 : (rho - delta) / st->rho1;
+  st->restart = 0;
 }
 
 // End of one iteration: MAXIT test (:275) and the loop condition.  Only this
@@ -118,6 +200,16 @@ __device__ __forceinline__ void loop_ctl(CgState *st, cudaGraphConditionalHandle
   if (!st->done && st->guard > st->maxit + 1) {
     st->error = HECMW33_ERR_TIMEOUT;
     st->done = 1;
+  }
+  // learned preconditioner: less than 20 % residual reduction over 25 iterations
+  // counts as stagnation and hands over to SSOR-CG (restarted)
+  if (!st->done && st->use_gnn && (st->iter % 25) == 0) {
+    if (st->iter > 25 && st->resid > 0.8 * st->resid_mark) {
+      st->use_gnn = 0;
+      st->fallback = st->iter;
+      st->restart = 1;
+    }
+    st->resid_mark = st->resid;
   }
   if (!st->done) {
     if (st->iter == st->maxit) {
@@ -135,12 +227,12 @@ __device__ __forceinline__ void loop_ctl(CgState *st, cudaGraphConditionalHandle
 // ---- 3x3 helpers -----------------------------------------------------------
 // Forward/backward substitution with a reciprocal-pivot LU block stored SoA:
 // entry e of position `row` at alu[e*stride + row] (hecmw_precond_SSOR_33.F90:332-338).
-template <class T>
-__device__ __forceinline__ void lu_solve(const T *__restrict__ alu, int stride, int row, double &x1,
-                                         double &x2, double &x3) {
-  const double a0 = alu[0 * stride + row], a1 = alu[1 * stride + row], a2 = alu[2 * stride + row];
-  const double a3 = alu[3 * stride + row], a4 = alu[4 * stride + row], a5 = alu[5 * stride + row];
-  const double a6 = alu[6 * stride + row], a7 = alu[7 * stride + row], a8 = alu[8 * stride + row];
+template <class TA, class R>
+__device__ __forceinline__ void lu_solve(const TA *__restrict__ alu, int stride, int row, R &x1, R &x2,
+                                         R &x3) {
+  const R a0 = R(alu[0 * stride + row]), a1 = R(alu[1 * stride + row]), a2 = R(alu[2 * stride + row]);
+  const R a3 = R(alu[3 * stride + row]), a4 = R(alu[4 * stride + row]), a5 = R(alu[5 * stride + row]);
+  const R a6 = R(alu[6 * stride + row]), a7 = R(alu[7 * stride + row]), a8 = R(alu[8 * stride + row]);
   x2 = x2 - a3 * x1;
   x3 = x3 - a6 * x1 - a7 * x2;
   x3 = a8 * x3;
@@ -148,32 +240,54 @@ __device__ __forceinline__ void lu_solve(const T *__restrict__ alu, int stride, 
   x1 = a0 * (x1 - a2 * x3 - a1 * x2);
 }
 
-template <class T>
-__device__ __forceinline__ T ld_stream(const T *p) {
-  return __ldcs(p);
+// Streaming (evict-first) load of a stored matrix value, widened to the working
+// precision R.  Values may be stored in FP64, FP32 or BF16.
+template <class R, class T>
+__device__ __forceinline__ R ld_val(const T *p) {
+  return R(__ldcs(p));
+}
+template <>
+__device__ __forceinline__ double ld_val<double, __nv_bfloat16>(const __nv_bfloat16 *p) {
+  const unsigned short u = __ldcs(reinterpret_cast<const unsigned short *>(p));
+  return double(__uint_as_float(unsigned(u) << 16));
+}
+template <>
+__device__ __forceinline__ float ld_val<float, __nv_bfloat16>(const __nv_bfloat16 *p) {
+  const unsigned short u = __ldcs(reinterpret_cast<const unsigned short *>(p));
+  return __uint_as_float(unsigned(u) << 16);
 }
 
-// y(row) = sum over the row's blocks of A_blk * x(col), ascending columns.
-// SIGN = +1 accumulates, -1 subtracts (forward sweep).  BACKWARD walks the
-// slots in descending order (the reference's backward-sweep order).
-template <class T, bool BACKWARD>
-__device__ __forceinline__ void row_gemv(const SellView<T> &A, int s, int lane, int len,
-                                         const double *__restrict__ x, double &y0, double &y1,
-                                         double &y2) {
+// Partial sums of one row of a sliced layout whose rows are spread over K lanes
+// (SellLayout: block k of a row sits in slot k/K at lane offset k%K): this lane
+// accumulates blocks sub, sub+K, sub+2K, ... of the row in the working precision
+// R (matrix values, vectors and accumulators alike).  BACKWARD walks them in
+// descending order (the reference's backward-sweep order when K == 1).
+template <class R, class TV, int K, bool BACKWARD>
+__device__ __forceinline__ void row_gemv(const SellView<TV> &A, int s, int lane, int rowlen,
+                                         const R *__restrict__ x, R &y0, R &y1, R &y2) {
+  const int sub = lane & (K - 1);
+  const int nb = rowlen > sub ? (rowlen - sub + K - 1) / K : 0;
   const int slot0 = A.slot0[s];
-#pragma unroll 2
-  for (int kk = 0; kk < len; kk++) {
-    const int k = BACKWARD ? len - 1 - kk : kk;
+#pragma unroll 4
+  for (int kk = 0; kk < nb; kk++) {
+    const int k = BACKWARD ? nb - 1 - kk : kk;
     const int sl = slot0 + k;
     const int c = __ldg(&A.col[sl * 32 + lane]);
-    const T *v = A.val + sl * 288 + lane;
-    const double x0 = __ldg(&x[3 * c]), x1 = __ldg(&x[3 * c + 1]), x2 = __ldg(&x[3 * c + 2]);
-    const double v0 = ld_stream(v), v1 = ld_stream(v + 32), v2 = ld_stream(v + 64);
-    const double v3 = ld_stream(v + 96), v4 = ld_stream(v + 128), v5 = ld_stream(v + 160);
-    const double v6 = ld_stream(v + 192), v7 = ld_stream(v + 224), v8 = ld_stream(v + 256);
+    const TV *v = A.val + sl * 288 + lane;
+    const R x0 = __ldg(&x[3 * c]), x1 = __ldg(&x[3 * c + 1]), x2 = __ldg(&x[3 * c + 2]);
+    const R v0 = ld_val<R>(v), v1 = ld_val<R>(v + 32), v2 = ld_val<R>(v + 64);
+    const R v3 = ld_val<R>(v + 96), v4 = ld_val<R>(v + 128), v5 = ld_val<R>(v + 160);
+    const R v6 = ld_val<R>(v + 192), v7 = ld_val<R>(v + 224), v8 = ld_val<R>(v + 256);
     y0 = fma(v2, x2, fma(v1, x1, fma(v0, x0, y0)));
     y1 = fma(v5, x2, fma(v4, x1, fma(v3, x0, y1)));
     y2 = fma(v8, x2, fma(v7, x1, fma(v6, x0, y2)));
+  }
+  // combine the K lanes of the row (aligned groups of K lanes)
+#pragma unroll
+  for (int o = K / 2; o > 0; o >>= 1) {
+    y0 += __shfl_xor_sync(0xffffffffu, y0, o);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, o);
+    y2 += __shfl_xor_sync(0xffffffffu, y2, o);
   }
 }
 
@@ -226,11 +340,10 @@ __global__ void alu_kernel(const double *__restrict__ blocks, const int *__restr
 
 // y = A x (MODE 0), r = b - A x (MODE 1); MODE 2: q = A p with the {p}{q} partial
 // and the ALPHA finisher.
-template <class T, int MODE>
-__global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<T> A, const double *__restrict__ x,
-                                                        double *__restrict__ y,
-                                                        const double *__restrict__ b, CgState *st,
-                                                        double *partials) {
+template <class R, int MODE>
+__global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<R> A, const R *__restrict__ x,
+                                                        R *__restrict__ y, const R *__restrict__ b,
+                                                        CgState *st, double *partials) {
   if (MODE == 2 && st->done) return;
   const int lane = threadIdx.x & 31;
   const int warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -240,8 +353,8 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<T> A, const dou
     const bool active = lane < A.nrows[s];
     const int row = A.row0[s] + lane;
     const int len = active ? A.rowlen[s * 32 + lane] : 0;
-    double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-    row_gemv<T, false>(A, s, lane, len, x, y0, y1, y2);
+    R y0 = 0, y1 = 0, y2 = 0;
+    row_gemv<R, R, 1, false>(A, s, lane, len, x, y0, y1, y2);
     if (active) {
       if (MODE == 1) {
         y0 = b[3 * row] - y0;
@@ -251,65 +364,76 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<T> A, const dou
       y[3 * row] = y0;
       y[3 * row + 1] = y1;
       y[3 * row + 2] = y2;
-      if (MODE == 2) dot += x[3 * row] * y0 + x[3 * row + 1] * y1 + x[3 * row + 2] * y2;
+      if (MODE == 2)
+        dot += double(x[3 * row]) * double(y0) + double(x[3 * row + 1]) * double(y1) +
+               double(x[3 * row + 2]) * double(y2);
     }
   }
   if (MODE == 2) reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[1], [&](double v) { fin_pq(st, v); });
 }
 
-// Forward sweep over the slices [sbeg, send) of one colour / level:
-// z(node) = LU^-1 ( r(node) - sum_lower A z(col) )   (hecmw_precond_SSOR_33.F90:309-345)
-template <class T>
-__global__ void __launch_bounds__(kThreads) sweep_fwd_kernel(SellView<T> L, const int *__restrict__ perm,
-                                                             const T *__restrict__ alu, int npos,
-                                                             const double *__restrict__ r,
-                                                             double *__restrict__ z, int sbeg,
-                                                             int send, const CgState *st) {
+// Forward sweep over the slices [sbeg, send) of one colour / level, each row spread
+// over K lanes:  z(node) = LU^-1 ( r(node) - sum_lower A z(col) )
+// (hecmw_precond_SSOR_33.F90:309-345)
+template <class R, class TV, class TA, int K>
+__global__ void __launch_bounds__(kThreads) sweep_fwd_kernel(SellView<TV> L, const int *__restrict__ perm,
+                                                             const TA *__restrict__ alu, int npos,
+                                                             const R *__restrict__ r, R *__restrict__ z,
+                                                             int sbeg, int send, const CgState *st) {
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
+  const int roff = lane / K;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
-    if (lane >= L.nrows[s]) continue;
-    const int row = L.row0[s] + lane;
-    const int node = perm[row];
-    const int len = L.rowlen[s * 32 + lane];
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    row_gemv<T, false>(L, s, lane, len, z, a0, a1, a2);
-    double x1 = r[3 * node] - a0, x2 = r[3 * node + 1] - a1, x3 = r[3 * node + 2] - a2;
-    lu_solve(alu, npos, row, x1, x2, x3);
-    z[3 * node] = x1;
-    z[3 * node + 1] = x2;
-    z[3 * node + 2] = x3;
+    const bool active = roff < L.nrows[s];
+    const int row = L.row0[s] + roff;
+    const int len = active ? L.rowlen[s * 32 + roff] : 0;
+    R a0 = 0, a1 = 0, a2 = 0;
+    row_gemv<R, TV, K, false>(L, s, lane, len, z, a0, a1, a2);
+    if (active && (lane & (K - 1)) == 0) {
+      const int node = perm[row];
+      R x1 = r[3 * node] - a0, x2 = r[3 * node + 1] - a1, x3 = r[3 * node + 2] - a2;
+      lu_solve(alu, npos, row, x1, x2, x3);
+      z[3 * node] = x1;
+      z[3 * node + 1] = x2;
+      z[3 * node + 2] = x3;
+    }
   }
 }
 
-// Backward sweep over [sbeg, send): z(node) -= LU^-1 ( sum_upper A z(col) )
-// (hecmw_precond_SSOR_33.F90:353-405).  FUSE_RHO accumulates {r}{z} of the
-// finished rows; the last launch's last CTA runs the RHO finisher.
-template <class T, bool FUSE_RHO>
-__global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<T> U, const int *__restrict__ perm,
-                                                             const T *__restrict__ alu, int npos,
-                                                             const double *__restrict__ r,
-                                                             double *__restrict__ z, int sbeg,
-                                                             int send, CgState *st, double *partials,
-                                                             int part_base, int part_total) {
+// Backward sweep over [sbeg, send), rows spread over K lanes:
+// z(node) -= LU^-1 ( sum_upper A z(col) )   (hecmw_precond_SSOR_33.F90:353-405).
+// FUSE_RHO accumulates {r}{z} of the finished rows; the last launch's last CTA
+// runs the RHO finisher.
+template <class R, class TV, class TA, int K, bool FUSE_RHO>
+__global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, const int *__restrict__ perm,
+                                                             const TA *__restrict__ alu, int npos,
+                                                             const R *__restrict__ r, R *__restrict__ z,
+                                                             int sbeg, int send, CgState *st,
+                                                             double *partials, int part_base,
+                                                             int part_total) {
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
+  const int roff = lane / K;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double dot = 0.0;
   for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
-    if (lane >= U.nrows[s]) continue;
-    const int row = U.row0[s] + lane;
-    const int node = perm[row];
-    const int len = U.rowlen[s * 32 + lane];
-    double x1 = 0.0, x2 = 0.0, x3 = 0.0;
-    row_gemv<T, true>(U, s, lane, len, z, x1, x2, x3);
-    lu_solve(alu, npos, row, x1, x2, x3);
-    const double z0 = z[3 * node] - x1, z1 = z[3 * node + 1] - x2, z2 = z[3 * node + 2] - x3;
-    z[3 * node] = z0;
-    z[3 * node + 1] = z1;
-    z[3 * node + 2] = z2;
-    if (FUSE_RHO) dot += r[3 * node] * z0 + r[3 * node + 1] * z1 + r[3 * node + 2] * z2;
+    const bool active = roff < U.nrows[s];
+    const int row = U.row0[s] + roff;
+    const int len = active ? U.rowlen[s * 32 + roff] : 0;
+    R x1 = 0, x2 = 0, x3 = 0;
+    row_gemv<R, TV, K, true>(U, s, lane, len, z, x1, x2, x3);
+    if (active && (lane & (K - 1)) == 0) {
+      const int node = perm[row];
+      lu_solve(alu, npos, row, x1, x2, x3);
+      const R z0 = z[3 * node] - x1, z1 = z[3 * node + 1] - x2, z2 = z[3 * node + 2] - x3;
+      z[3 * node] = z0;
+      z[3 * node + 1] = z1;
+      z[3 * node + 2] = z2;
+      if (FUSE_RHO)
+        dot += double(r[3 * node]) * double(z0) + double(r[3 * node + 1]) * double(z1) +
+               double(r[3 * node + 2]) * double(z2);
+    }
   }
   if (FUSE_RHO)
     reduce_finish(dot, partials, part_base + blockIdx.x, part_total, &st->ticket[0],
@@ -318,52 +442,105 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<T> U, cons
 
 // Block-diagonal preconditioner z = ALU^-1 r (hecmw_precond_DIAG_33.F90:116-136),
 // optionally with the fused {r}{z} partial.
-template <class T, bool FUSE_RHO>
-__global__ void __launch_bounds__(kThreads) diag_kernel(const T *__restrict__ alu, int n,
-                                                        const double *__restrict__ r,
-                                                        double *__restrict__ z, CgState *st,
-                                                        double *partials) {
+template <class R, class TA, bool FUSE_RHO>
+__global__ void __launch_bounds__(kThreads) diag_kernel(const TA *__restrict__ alu, int n,
+                                                        const R *__restrict__ r, R *__restrict__ z,
+                                                        CgState *st, double *partials) {
   if (st && st->done) return;
   double dot = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double x1 = r[3 * i], x2 = r[3 * i + 1], x3 = r[3 * i + 2];
+    R x1 = r[3 * i], x2 = r[3 * i + 1], x3 = r[3 * i + 2];
     lu_solve(alu, n, i, x1, x2, x3);
     z[3 * i] = x1;
     z[3 * i + 1] = x2;
     z[3 * i + 2] = x3;
-    if (FUSE_RHO) dot += r[3 * i] * x1 + r[3 * i + 1] * x2 + r[3 * i + 2] * x3;
+    if (FUSE_RHO)
+      dot += double(r[3 * i]) * double(x1) + double(r[3 * i + 1]) * double(x2) +
+             double(r[3 * i + 2]) * double(x3);
   }
   if (FUSE_RHO) reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[0], [&](double v) { fin_rho(st, v); });
 }
 
+// RHO and DELTA of flexible CG in one pass, with the fin_rho_flex decisions.
+template <class R>
+__global__ void __launch_bounds__(kThreads) fcg_rho_kernel(const R *__restrict__ z, const R *__restrict__ r,
+                                                           const R *__restrict__ r_old, int n3, CgState *st,
+                                                           double *partials) {
+  if (st->done) return;
+  double a = 0.0, b = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+    const double zi = double(z[i]);
+    a += zi * double(r[i]);
+    b += zi * double(r_old[i]);
+  }
+  reduce_finish2(a, b, partials, blockIdx.x, gridDim.x, &st->ticket[0],
+                 [&](double rho, double delta) { fin_rho_flex(st, rho, delta); });
+}
+
+// Flexible CG update: r_old = r, then as update_xr_kernel.
+template <class R>
+__global__ void __launch_bounds__(kThreads) update_xr_flex_kernel(R *__restrict__ x, const R *__restrict__ p,
+                                                                  R *__restrict__ r, R *__restrict__ r_old,
+                                                                  const R *__restrict__ q, int n3, CgState *st,
+                                                                  double *partials) {
+  if (st->done) return;
+  const R alpha = R(st->alpha);
+  const bool refresh = !st->inner && (st->iter % kIterRecomputeR) == 0;
+  double dot = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+    x[i] = alpha * p[i] + x[i];
+    const R ri = r[i];
+    r_old[i] = ri;
+    if (!refresh) {
+      const R rn = -alpha * q[i] + ri;
+      r[i] = rn;
+      dot += double(rn) * double(rn);
+    }
+  }
+  if (!refresh) reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[2], [&](double v) { fin_rr(st, v); });
+}
+
+// gamma = sqrt(mean(zs^2)), the learned preconditioner's scale (skipped when off)
+template <class R>
+__global__ void __launch_bounds__(kThreads) gamma_kernel(const R *__restrict__ zs, int n3, CgState *st,
+                                                         double *partials) {
+  if (st->done || !st->use_gnn) return;
+  double a = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
+    a += double(zs[i]) * double(zs[i]);
+  reduce_finish(a, partials, blockIdx.x, gridDim.x, &st->ticket[7], [&](double v) {
+    const double g2 = v / double(n3);
+    st->gamma = g2 > 0.0 ? float(sqrt(g2)) : 1.0f;
+  });
+}
+
 // {p} = {z} (first iteration) or {z} + BETA {p}  (hecmw_solver_CG.f90:202-207)
-__global__ void __launch_bounds__(kThreads) update_p_kernel(const double *__restrict__ z,
-                                                            double *__restrict__ p, int n3,
-                                                            const CgState *st) {
+template <class R>
+__global__ void __launch_bounds__(kThreads) update_p_kernel(const R *__restrict__ z, R *__restrict__ p,
+                                                            int n3, const CgState *st) {
   if (st->done) return;
   const bool first = st->iter == 1;
-  const double beta = st->beta;
+  const R beta = R(st->beta);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
     p[i] = first ? z[i] : z[i] + beta * p[i];
 }
 
 // {x} += ALPHA {p}; {r} -= ALPHA {q} with the DNRM2 partial, except on every
 // 50th iteration where r is recomputed from b - A x instead (:240-246).
-__global__ void __launch_bounds__(kThreads) update_xr_kernel(double *__restrict__ x,
-                                                             const double *__restrict__ p,
-                                                             double *__restrict__ r,
-                                                             const double *__restrict__ q, int n3,
-                                                             CgState *st, double *partials) {
+template <class R>
+__global__ void __launch_bounds__(kThreads) update_xr_kernel(R *__restrict__ x, const R *__restrict__ p,
+                                                             R *__restrict__ r, const R *__restrict__ q,
+                                                             int n3, CgState *st, double *partials) {
   if (st->done) return;
-  const double alpha = st->alpha;
-  const bool refresh = (st->iter % kIterRecomputeR) == 0;
+  const R alpha = R(st->alpha);
+  const bool refresh = !st->inner && (st->iter % kIterRecomputeR) == 0;
   double dot = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
     x[i] = alpha * p[i] + x[i];
     if (!refresh) {
-      const double ri = -alpha * q[i] + r[i];
+      const R ri = -alpha * q[i] + r[i];
       r[i] = ri;
-      dot += ri * ri;
+      dot += double(ri) * double(ri);
     }
   }
   if (!refresh) reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[2], [&](double v) { fin_rr(st, v); });
@@ -372,13 +549,12 @@ __global__ void __launch_bounds__(kThreads) update_xr_kernel(double *__restrict_
 // End of an iteration: when a true residual is due (every 50th iteration, or
 // RESID <= TOL, :242-274) r = b - A x and RESID are recomputed; then the loop
 // control.  Exactly one thread runs loop_ctl per iteration.
-template <class T>
-__global__ void __launch_bounds__(kThreads) resid_ctl_kernel(SellView<T> A, const double *__restrict__ x,
-                                                             double *__restrict__ r,
-                                                             const double *__restrict__ b, CgState *st,
-                                                             double *partials,
+template <class R>
+__global__ void __launch_bounds__(kThreads) resid_ctl_kernel(SellView<R> A, const R *__restrict__ x,
+                                                             R *__restrict__ r, const R *__restrict__ b,
+                                                             CgState *st, double *partials,
                                                              cudaGraphConditionalHandle h, int use_cond) {
-  const bool need = !st->done && ((st->iter % kIterRecomputeR) == 0 || st->recompute);
+  const bool need = !st->done && ((!st->inner && (st->iter % kIterRecomputeR) == 0) || st->recompute);
   if (!need) {
     if (blockIdx.x == 0 && threadIdx.x == 0) loop_ctl(st, h, use_cond);
     return;
@@ -391,8 +567,8 @@ __global__ void __launch_bounds__(kThreads) resid_ctl_kernel(SellView<T> A, cons
     const bool active = lane < A.nrows[s];
     const int row = A.row0[s] + lane;
     const int len = active ? A.rowlen[s * 32 + lane] : 0;
-    double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-    row_gemv<T, false>(A, s, lane, len, x, y0, y1, y2);
+    R y0 = 0, y1 = 0, y2 = 0;
+    row_gemv<R, R, 1, false>(A, s, lane, len, x, y0, y1, y2);
     if (active) {
       y0 = b[3 * row] - y0;
       y1 = b[3 * row + 1] - y1;
@@ -400,7 +576,7 @@ __global__ void __launch_bounds__(kThreads) resid_ctl_kernel(SellView<T> A, cons
       r[3 * row] = y0;
       r[3 * row + 1] = y1;
       r[3 * row + 2] = y2;
-      dot += y0 * y0 + y1 * y1 + y2 * y2;
+      dot += double(y0) * double(y0) + double(y1) * double(y1) + double(y2) * double(y2);
     }
   }
   reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[3], [&](double v) {
@@ -414,18 +590,104 @@ __global__ void __launch_bounds__(kThreads) resid_ctl_kernel(SellView<T> A, cons
   });
 }
 
+// ---- mixed precision with reliable updates --------------------------------
+// Start: r32 = float(r64) (r64 = b - A x64 computed by the FP64 SpMV), x32 = 0,
+// ru_mark = ||r64|| / ||b||; a start already within the tolerance ends the loop.
+__global__ void __launch_bounds__(kThreads) ru_init_kernel(const double *__restrict__ r64, float *__restrict__ r32,
+                                                           float *__restrict__ x32, int n3, CgState *st,
+                                                           double *partials, cudaGraphConditionalHandle h,
+                                                           int use_cond) {
+  double dot = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+    const double v = r64[i];
+    r32[i] = float(v);
+    x32[i] = 0.0f;
+    dot += v * v;
+  }
+  reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[6], [&](double v) {
+    if (st->bnrm2 > 0.0) {
+      st->ru_mark = sqrt(v / st->bnrm2);
+      st->resid = st->ru_mark;
+      if (st->ru_mark <= st->tol) {
+        st->done = 1;
+        st->converged = 1;
+      }
+    }
+    set_loop(h, use_cond, !st->done);
+  });
+}
+
+// Reliable update, part 1 (only when pending): x64 += x32, x32 = 0.
+__global__ void __launch_bounds__(kThreads) ru_update_x_kernel(double *__restrict__ x64, float *__restrict__ x32,
+                                                               int n3, const CgState *st) {
+  if (st->done || !st->ru_pending) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+    x64[i] = x64[i] + double(x32[i]);
+    x32[i] = 0.0f;
+  }
+}
+
+// Reliable update, part 2 and the end of the iteration: when pending, the FP64 true
+// residual r64 = b - A x64 replaces the FP32 one (r32 = float(r64)) and decides
+// convergence on ||r64|| / ||b||; then the loop control.
+__global__ void __launch_bounds__(kThreads) ru_resid_kernel(SellView<double> A, const double *__restrict__ x64,
+                                                            double *__restrict__ r64, const double *__restrict__ b64,
+                                                            float *__restrict__ r32, CgState *st, double *partials,
+                                                            cudaGraphConditionalHandle h, int use_cond) {
+  const bool need = !st->done && st->ru_pending;
+  if (!need) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) loop_ctl(st, h, use_cond);
+    return;
+  }
+  const int lane = threadIdx.x & 31;
+  const int warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double dot = 0.0;
+  for (int s = warp0; s < A.nslices; s += nwarps) {
+    const bool active = lane < A.nrows[s];
+    const int row = A.row0[s] + lane;
+    const int len = active ? A.rowlen[s * 32 + lane] : 0;
+    double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+    row_gemv<double, double, 1, false>(A, s, lane, len, x64, y0, y1, y2);
+    if (active) {
+      y0 = b64[3 * row] - y0;
+      y1 = b64[3 * row + 1] - y1;
+      y2 = b64[3 * row + 2] - y2;
+      r64[3 * row] = y0;
+      r64[3 * row + 1] = y1;
+      r64[3 * row + 2] = y2;
+      r32[3 * row] = float(y0);
+      r32[3 * row + 1] = float(y1);
+      r32[3 * row + 2] = float(y2);
+      dot += y0 * y0 + y1 * y1 + y2 * y2;
+    }
+  }
+  reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[3], [&](double v) {
+    st->rr = v;
+    st->resid = sqrt(v / st->bnrm2);
+    st->ru_pending = 0;
+    st->ru_count++;
+    st->ru_mark = st->resid;
+    if (st->resid <= st->tol) {
+      st->done = 1;
+      st->converged = 1;
+    }
+    loop_ctl(st, h, use_cond);
+  });
+}
+
 // Generic dot with a selectable finisher:
 //   WHICH 0: BNRM2 at the start of a solve (also decides whether the loop runs)
 //   WHICH 1: RHO (unfused preconditioner paths)
 //   WHICH 2: plain result into st->rr_true
-template <int WHICH>
-__global__ void __launch_bounds__(kThreads) dot_kernel(const double *__restrict__ a,
-                                                       const double *__restrict__ b, int n3,
-                                                       CgState *st, double *partials,
+template <class R, int WHICH>
+__global__ void __launch_bounds__(kThreads) dot_kernel(const R *__restrict__ a, const R *__restrict__ b,
+                                                       int n3, CgState *st, double *partials,
                                                        cudaGraphConditionalHandle h, int use_cond) {
   if (WHICH == 1 && st->done) return;
   double dot = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) dot += a[i] * b[i];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
+    dot += double(a[i]) * double(b[i]);
   reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[4 + WHICH], [&](double v) {
     if (WHICH == 0) {
       st->bnrm2 = v;
@@ -466,21 +728,52 @@ __global__ void cg_init_kernel(CgState *st, const CgParams *prm) {
   st->converged = 0;
   st->zero_rhs = 0;
   st->guard = 0;
+  st->inner = prm->inner;
+  st->flexible = prm->flexible;
+  st->use_gnn = prm->use_gnn;
+  st->restart = 0;
+  st->fallback = 0;
+  st->resid_mark = 1.0;
+  st->gamma = 1.0f;
+  st->reliable = prm->reliable;
+  st->ru_pending = 0;
+  st->ru_count = 0;
+  st->ru_delta = prm->ru_delta;
+  st->ru_mark = 1.0;
   for (int i = 0; i < 8; i++) st->ticket[i] = 0u;
 }
 
-// Vector helpers for the unfused preconditioner paths (iterPREmax != 1).
-__global__ void copy_kernel(const double *__restrict__ a, double *__restrict__ b, int n, const CgState *st) {
+// Vector helpers for the unfused preconditioner paths (iterPREmax != 1) and the
+// precision conversions of the mixed-precision refinement.
+template <class R>
+__global__ void copy_kernel(const R *__restrict__ a, R *__restrict__ b, int n, const CgState *st) {
   if (st && st->done) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
-__global__ void add_kernel(const double *__restrict__ a, double *__restrict__ b, int n, const CgState *st) {
+template <class R>
+__global__ void add_kernel(const R *__restrict__ a, R *__restrict__ b, int n, const CgState *st) {
   if (st && st->done) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = b[i] + a[i];
 }
-__global__ void zero_kernel(double *__restrict__ b, int n, const CgState *st) {
-  if (st && st->done) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = 0.0;
+// b = float(a) (inner right-hand side from the FP64 residual)
+__global__ void narrow_kernel(const double *__restrict__ a, float *__restrict__ b, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = float(a[i]);
+}
+// x += double(d) (FP64 correction of the outer refinement)
+__global__ void widen_add_kernel(const float *__restrict__ d, double *__restrict__ x, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = x[i] + double(d[i]);
+}
+// b = R(a) for value arrays (FP32 copies of the matrix / preconditioner values)
+template <class R>
+__global__ void convert_kernel(const double *__restrict__ a, R *__restrict__ b, size_t n) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    b[i] = R(a[i]);
+}
+// BF16 copies of stored values (round to nearest even)
+__global__ void convert_bf16_kernel(const double *__restrict__ a, __nv_bfloat16 *__restrict__ b, size_t n) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    b[i] = __float2bfloat16_rn(float(a[i]));
 }
 
 }  // namespace h33

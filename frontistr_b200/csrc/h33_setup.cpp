@@ -254,15 +254,21 @@ void reordered_rows(const Profile &p, const std::vector<int> &perm, const std::v
   }
 }
 
-void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out) {
+void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out, int lanes) {
+  if (lanes < 1 || lanes > 32 || (32 % lanes) != 0) throw std::runtime_error("lanes per row must divide 32");
   out = SellLayout();
+  out.lanes = lanes;
+  const int per_slice = 32 / lanes;
   const int ngroups = int(group_rows.size()) - 1;
   out.group_slice.assign(size_t(ngroups) + 1, 0);
   for (int g = 0; g < ngroups; g++) {
-    for (int r0 = group_rows[g]; r0 < group_rows[g + 1]; r0 += 32) {
-      const int nr = std::min(32, group_rows[g + 1] - r0);
+    for (int r0 = group_rows[g]; r0 < group_rows[g + 1]; r0 += per_slice) {
+      const int nr = std::min(per_slice, group_rows[g + 1] - r0);
       int len = 0;
-      for (int l = 0; l < nr; l++) len = std::max<int>(len, int(rows.ptr[r0 + l + 1] - rows.ptr[r0 + l]));
+      for (int l = 0; l < nr; l++) {
+        const int n = int(rows.ptr[r0 + l + 1] - rows.ptr[r0 + l]);
+        len = std::max(len, (n + lanes - 1) / lanes);
+      }
       out.row0.push_back(r0);
       out.nrows.push_back(nr);
       out.slot0.push_back(int(out.nslots));
@@ -277,15 +283,16 @@ void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellL
   out.rowlen.assign(size_t(out.nslices) * 32, 0);
   out.col.assign(size_t(out.nslots) * 32, 0);
   out.src.assign(size_t(out.nslots) * 32, -1);
+  // block k of the row at offset r of slice s sits in slot k / lanes, lane r*lanes + k % lanes
 #pragma omp parallel for schedule(static)
   for (int s = 0; s < out.nslices; s++) {
-    for (int l = 0; l < out.nrows[s]; l++) {
-      const int r = out.row0[s] + l;
-      const int64_t b = rows.ptr[r];
-      const int n = int(rows.ptr[r + 1] - b);
-      out.rowlen[size_t(s) * 32 + l] = n;
+    for (int r = 0; r < out.nrows[s]; r++) {
+      const int row = out.row0[s] + r;
+      const int64_t b = rows.ptr[row];
+      const int n = int(rows.ptr[row + 1] - b);
+      out.rowlen[size_t(s) * 32 + r] = n;
       for (int k = 0; k < n; k++) {
-        const size_t at = (size_t(out.slot0[s]) + k) * 32 + l;
+        const size_t at = (size_t(out.slot0[s]) + k / lanes) * 32 + size_t(r) * lanes + k % lanes;
         out.col[at] = rows.col[b + k];
         out.src[at] = rows.src[b + k];
       }

@@ -44,17 +44,22 @@ void reordered_rows(const Profile &p, const std::vector<int> &perm, const std::v
                     BlockRows &lower, BlockRows &upper);
 
 // Host-side sliced block-ELL layout; rows are taken in groups (a group never
-// shares a slice with another group), 32 consecutive rows per slice.
+// shares a slice with another group).  Each row is spread over `lanes` lanes of
+// a warp (lanes divides 32), so a slice holds 32/lanes consecutive rows: block k
+// of the row at offset r sits in slot k/lanes at lane r*lanes + k%lanes, and every
+// load of one entry of a slot is 32 consecutive values.
 struct SellLayout {
   int nslices = 0;
+  int lanes = 1;
   int64_t nslots = 0;
   std::vector<int> row0, nrows, slot0, len;  // per slice
-  std::vector<int> rowlen;                    // per slice*32 + lane
+  std::vector<int> rowlen;                    // per slice*32 + row offset (blocks in the row)
   std::vector<int> col, src;                  // per slot*32 + lane (pad: col 0, src -1)
   std::vector<int> group_slice;               // group g -> slices [group_slice[g], group_slice[g+1])
 };
 // group_rows: row boundaries of the groups (size ngroups+1, rows 0..nrows-1).
-void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out);
+void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out,
+                int lanes = 1);
 
 // Block ILU(0) in natural order (FORM_ILU0_33, hecmw_precond_BILU_33.f90:185-362),
 // computed on the host from the hecmwST arrays.  Outputs the factor blocks in the

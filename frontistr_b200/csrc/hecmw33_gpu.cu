@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "h33_common.cuh"
+#include "h33_gnn.cuh"
 #include "h33_kernels.cuh"
 #include "h33_setup.h"
 
@@ -52,6 +53,16 @@ bool graph_mode() {
 }
 constexpr int kStreamChunk = 16;
 
+// Lanes per row of the preconditioner sweep layouts (HECMW33_SWEEP_LANES overrides;
+// 1, 2, 4, 8, 16 or 32).  Several lanes per row shorten each row's dependent load
+// chain and multiply the warps of a colour, which the sweeps need: a colour holds
+// a tenth of the rows, too few one-lane rows to cover HBM latency.
+int sweep_lanes() {
+  const char *e = std::getenv("HECMW33_SWEEP_LANES");
+  const int k = e ? std::atoi(e) : 8;
+  return (k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32) ? k : 8;
+}
+
 double wall() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -62,10 +73,14 @@ struct DevSell {
   int nslices = 0, nslots = 0;
   DevArray<int> row0, nrows, slot0, len, rowlen, col, src;
   DevArray<T> val;
+  DevArray<float> val32;  // FP32 copy of val (mixed precision), same layout
+  DevArray<__nv_bfloat16> val16;  // BF16 copy of val (low-precision preconditioner), same layout
   std::vector<int> group_slice;
 
+  int lanes = 1;
   void upload(const SellLayout &L, cudaStream_t s) {
     nslices = L.nslices;
+    lanes = L.lanes;
     nslots = int(L.nslots);
     row0.upload(L.row0, s);
     nrows.upload(L.nrows, s);
@@ -80,6 +95,12 @@ struct DevSell {
   SellView<T> view() const {
     return SellView<T>{nslices, row0.p, nrows.p, slot0.p, len.p, rowlen.p, col.p, val.p};
   }
+  SellView<float> view32() const {
+    return SellView<float>{nslices, row0.p, nrows.p, slot0.p, len.p, rowlen.p, col.p, val32.p};
+  }
+  SellView<__nv_bfloat16> view16() const {
+    return SellView<__nv_bfloat16>{nslices, row0.p, nrows.p, slot0.p, len.p, rowlen.p, col.p, val16.p};
+  }
   void pack(const double *raw, cudaStream_t s, int nsm) {
     if (nslots == 0) return;
     const int total = nslots * 32;
@@ -89,7 +110,7 @@ struct DevSell {
   }
   size_t bytes() const {
     return row0.bytes() + nrows.bytes() + slot0.bytes() + len.bytes() + rowlen.bytes() + col.bytes() +
-           src.bytes() + val.bytes();
+           src.bytes() + val.bytes() + val32.bytes() + val16.bytes();
   }
 };
 
@@ -106,6 +127,49 @@ struct Precond {
   int ncolor = 0;
   std::vector<int> colorindex, perm;  // SSOR: host copies (0-based)
   DevArray<double> ilu_raw;           // ILU(0) factor blocks, raw numbering
+  DevArray<float> alu32_fwd, alu32_bwd;
+  int numeric_version = 0, fp32_version = -1, lowp_version = -1;
+};
+
+// The learned preconditioner: node graph of the matrix, weights, activations and
+// the (r, e) pairs recorded from earlier solves (training data).
+struct Learned {
+  int graph_generation = -1, feat_version = -1;
+  int n = 0, nedges = 0;
+  DevArray<int> ptr, col, rev, src;
+  DevArray<float> feat, s;
+  bool have_weights = false;
+  int weights_version = 0;
+  int adam_step = 0;
+  DevArray<float> theta, m1, m2, grad, gacc;
+  DevArray<__nv_bfloat16> theta_bf16;
+  DevArray<int> row_of;
+  int built_for = -1, w_version = -1;
+  DevArray<float> w, x, h[4], m[3], gm, dh, dhp, part;
+  int nparts = 0, stride = 0;
+  DevArray<float> t_z, t_zs, t_d, t_q, t_dz;  // training scratch (3N)
+  // recorded pairs (FP32): r_k, e_k, SSOR(r_k) and e_k.r_k
+  bool recording = false;
+  int max_pairs = 16;
+  std::vector<DevArray<float>> pr, pe, pzs;
+  std::vector<double> per;
+  DevArray<double> losses;
+  GnnGraph graph() const { return GnnGraph{n, nedges, ptr.p, col.p, rev.p, feat.p, s.p}; }
+};
+
+// One instantiated CG graph and the key of the device buffers it captured.
+struct GraphSlot {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int key[5] = {-1, -1, -1, -1, -1};
+  int kernels_per_iter = 0, prologue_kernels = 0;
+  void drop() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    key[0] = -1;
+  }
 };
 
 struct Solver {
@@ -130,23 +194,29 @@ struct Solver {
   CgState *h_state = nullptr;
   DevArray<int> d_err;
   Precond pc;
-  // graph
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  int graph_key[4] = {-1, -1, -1, -1};
+  // FP32 copies for the mixed-precision refinement
+  DevArray<float> bf, xf, rf, zf, pf, qf, wf, zpf;
+  // flexible CG buffers (SSOR output and previous residual) and the learned preconditioner
+  DevArray<double> zs, rold;
+  DevArray<float> zsf, roldf;
+  Learned L;
+  int values_version = 0, a32_version = -1;
+  double bnrm2 = 0.0;
+  // graphs (FP64 drop-in, FP32 inner solve)
+  GraphSlot g64, g32;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int build_counter = 0;  // monotonic id of preconditioner builds (graph cache key)
   // last-solve record
-  int last_iter = 0, last_kernels = 0, kernels_per_iter = 0, prologue_kernels = 0;
-  double last_solve_s = 0.0, last_setup_s = 0.0;
+  int last_iter = 0, last_outer = 0, last_kernels = 0, last_learned = 0, last_fallback = 0;
+  double last_solve_s = 0.0, last_setup_s = 0.0, last_true_resid = 0.0;
 
   Solver() {
     H33_CUDA(cudaGetDevice(&device));
     H33_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     H33_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_spmv, spmv_kernel<double, 2>, kThreads, 0));
-    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep, sweep_bwd_kernel<double, true>, kThreads, 0));
-    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_vec, update_xr_kernel, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep, sweep_bwd_kernel<double, double, double, 8, true>, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_vec, update_xr_kernel<double>, kThreads, 0));
     occ_spmv = std::max(occ_spmv, 1);
     occ_sweep = std::max(occ_sweep, 1);
     occ_vec = std::max(occ_vec, 1);
@@ -170,11 +240,8 @@ struct Solver {
     }
   }
   void drop_graph() {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    exec = nullptr;
-    graph = nullptr;
-    graph_key[0] = -1;
+    g64.drop();
+    g32.drop();
   }
   int n3() const { return 3 * N; }
   int grid_vec() const { return std::max(1, std::min((n3() + kThreads - 1) / kThreads, nsm * occ_vec)); }
@@ -280,6 +347,7 @@ void set_matrix(Solver &S, int N, int NP, int NPL, int NPU, const int *indexL, c
     H33_CUDA(cudaMemcpyAsync(S.raw.p + 9 * (size_t(N) + NPL), AU, sizeof(double) * 9 * NPU,
                              cudaMemcpyHostToDevice, S.stream));
   S.A.pack(S.raw.p, S.stream, S.nsm);
+  S.values_version++;
   S.zero_diag = false;
   for (int i = 0; i < N && !S.zero_diag; i++)
     for (int j = 0; j < 3; j++)
@@ -309,8 +377,8 @@ void setup_ssor(Solver &S, int ncolor_in, double sigma, bool symbolic) {
     BlockRows lower, upper;
     reordered_rows(prof, perm, iperm, lower, upper);
     SellLayout lo, up;
-    build_sell(lower, colorindex, lo);
-    build_sell(upper, colorindex, up);
+    build_sell(lower, colorindex, lo, sweep_lanes());
+    build_sell(upper, colorindex, up, sweep_lanes());
     P.lo.upload(lo, S.stream);
     P.up.upload(up, S.stream);
     P.perm_fwd.upload(perm, S.stream);
@@ -359,8 +427,8 @@ void setup_bilu0(Solver &S, double sigma, bool symbolic) {
       }
     }
     SellLayout lo, up;
-    build_sell(lower, lev_f, lo);
-    build_sell(upper, lev_b, up);
+    build_sell(lower, lev_f, lo, sweep_lanes());
+    build_sell(upper, lev_b, up, sweep_lanes());
     P.lo.upload(lo, S.stream);
     P.up.upload(up, S.stream);
     P.perm_fwd.upload(ord_f, S.stream);
@@ -433,6 +501,7 @@ void precond_setup(Solver &S, int precond, int ncolor_in, double sigma, int *Iar
   S.sync();
   (void)err;  // a zero pivot in SSOR/DIAG gives Inf entries, as in the reference (no check there)
   P.valid = true;
+  P.numeric_version = ++S.build_counter;
   if (symbolic) {
     // new device buffers: graphs that captured the old ones must go
     P.generation = ++S.build_counter;
@@ -443,26 +512,53 @@ void precond_setup(Solver &S, int precond, int ncolor_in, double sigma, int *Iar
 }
 
 // ---------------------------------------------------------------------------
-// Launch sequences (captured into graphs or run directly)
+// Launch sequences (captured into graphs or run directly), for the working
+// precision R: double (the drop-in) or float (the inner solves of the
+// mixed-precision refinement, on FP32 copies of the same sliced layouts).
 
-// z = M^-1 r, one pass; FUSE_RHO adds the RHO reduction + finisher.
-template <bool FUSE_RHO>
-void launch_sweep(Solver &S, const double *rin, double *zout, CgState *st) {
+template <class R>
+struct Views {
+  SellView<R> A, lo, up;
+  const R *alu_f, *alu_b;
+  R *b, *x, *r, *z, *p, *q, *w, *zp, *zs, *rold;
+  // low-precision preconditioner (lowp = 1): BF16 sweep values, FP32 diagonal LU,
+  // arithmetic still in R
+  int lowp;
+  SellView<__nv_bfloat16> lo16, up16;
+  const float *alu32_f, *alu32_b;
+};
+
+Views<double> views(Solver &S, double, int lowp = 0) {
+  Precond &P = S.pc;
+  return Views<double>{S.A.view(),   P.lo.view(),   P.up.view(), P.alu_fwd.p,
+                       P.alu_shared ? P.alu_fwd.p : P.alu_bwd.p,
+                       S.b.p, S.x.p, S.r.p, S.z.p, S.p.p, S.q.p, S.w.p, S.zp.p, S.zs.p, S.rold.p,
+                       lowp, P.lo.view16(), P.up.view16(), P.alu32_fwd.p,
+                       P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p};
+}
+Views<float> views(Solver &S, float, int lowp = 0) {
+  Precond &P = S.pc;
+  return Views<float>{S.A.view32(),   P.lo.view32(),   P.up.view32(), P.alu32_fwd.p,
+                      P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p,
+                      S.bf.p, S.xf.p, S.rf.p, S.zf.p, S.pf.p, S.qf.p, S.wf.p, S.zpf.p, S.zsf.p, S.roldf.p,
+                      lowp, P.lo.view16(), P.up.view16(), P.alu32_fwd.p,
+                      P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p};
+}
+
+// z = M^-1 r, one pass; FUSE_RHO adds the RHO reduction + finisher.  K = lanes per
+// row of the sweep layouts.
+template <class R, class TV, class TA, bool FUSE_RHO, int K>
+void launch_sweep_k(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f, const TA *alu_b,
+                    const R *rin, R *zout, CgState *st) {
   Precond &P = S.pc;
   cudaStream_t s = S.stream;
-  if (P.kind == 3) {
-    diag_kernel<double, FUSE_RHO><<<S.grid_vec(), kThreads, 0, s>>>(P.alu_fwd.p, S.N, rin, zout, st, S.partials.p);
-    return;
-  }
-  const SellView<double> L = P.lo.view(), U = P.up.view();
-  const double *alu_b = P.alu_shared ? P.alu_fwd.p : P.alu_bwd.p;
   const int *perm_b = P.alu_shared ? P.perm_fwd.p : P.perm_bwd.p;
   const int gf = int(P.lo.group_slice.size()) - 1;
   for (int g = 0; g < gf; g++) {
     const int sb = P.lo.group_slice[g], se = P.lo.group_slice[g + 1];
     if (se <= sb) continue;
-    sweep_fwd_kernel<double><<<S.grid_sweep(se - sb), kThreads, 0, s>>>(L, P.perm_fwd.p, P.alu_fwd.p, S.N, rin,
-                                                                        zout, sb, se, st);
+    sweep_fwd_kernel<R, TV, TA, K><<<S.grid_sweep(se - sb), kThreads, 0, s>>>(lo, P.perm_fwd.p, alu_f, S.N, rin,
+                                                                              zout, sb, se, st);
   }
   const int gb = int(P.up.group_slice.size()) - 1;
   int total = 0;
@@ -476,73 +572,196 @@ void launch_sweep(Solver &S, const double *rin, double *zout, CgState *st) {
     const int grid = S.grid_sweep(std::max(se - sb, 1));
     // a group without slices still launches (one idle CTA) so that the reduction
     // ticket count stays exact
-    sweep_bwd_kernel<double, FUSE_RHO><<<grid, kThreads, 0, s>>>(U, perm_b, alu_b, S.N, rin, zout, sb, se, st,
-                                                                 S.partials.p, base, total);
+    sweep_bwd_kernel<R, TV, TA, K, FUSE_RHO><<<grid, kThreads, 0, s>>>(up, perm_b, alu_b, S.N, rin, zout, sb, se,
+                                                                       st, S.partials.p, base, total);
     base += grid;
   }
+}
+
+template <class R, class TV, class TA, bool FUSE_RHO>
+void launch_sweep_t(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f, const TA *alu_b,
+                    const R *rin, R *zout, CgState *st) {
+  Precond &P = S.pc;
+  if (P.kind == 3) {
+    diag_kernel<R, TA, FUSE_RHO><<<S.grid_vec(), kThreads, 0, S.stream>>>(alu_f, S.N, rin, zout, st, S.partials.p);
+    return;
+  }
+  switch (P.lo.lanes) {
+    case 1: return launch_sweep_k<R, TV, TA, FUSE_RHO, 1>(S, lo, up, alu_f, alu_b, rin, zout, st);
+    case 2: return launch_sweep_k<R, TV, TA, FUSE_RHO, 2>(S, lo, up, alu_f, alu_b, rin, zout, st);
+    case 4: return launch_sweep_k<R, TV, TA, FUSE_RHO, 4>(S, lo, up, alu_f, alu_b, rin, zout, st);
+    case 16: return launch_sweep_k<R, TV, TA, FUSE_RHO, 16>(S, lo, up, alu_f, alu_b, rin, zout, st);
+    case 32: return launch_sweep_k<R, TV, TA, FUSE_RHO, 32>(S, lo, up, alu_f, alu_b, rin, zout, st);
+    default: return launch_sweep_k<R, TV, TA, FUSE_RHO, 8>(S, lo, up, alu_f, alu_b, rin, zout, st);
+  }
+}
+
+template <class R, bool FUSE_RHO>
+void launch_sweep(Solver &S, const Views<R> &V, const R *rin, R *zout, CgState *st) {
+  if (V.lowp)
+    launch_sweep_t<R, __nv_bfloat16, float, FUSE_RHO>(S, V.lo16, V.up16, V.alu32_f, V.alu32_b, rin, zout, st);
+  else
+    launch_sweep_t<R, R, R, FUSE_RHO>(S, V.lo, V.up, V.alu_f, V.alu_b, rin, zout, st);
 }
 
 // hecmw_precond_apply (hecmw_precond.f90:86-172): z = M^-1 r with iterPREmax passes.
 // When st is given and iterPREmax == 1 the RHO reduction is fused into the sweep;
 // otherwise (st given) RHO is computed by a separate dot.
-void launch_precond(Solver &S, int iterpremax, const double *r, double *z, CgState *st) {
+template <class R>
+void launch_precond(Solver &S, const Views<R> &V, int iterpremax, const R *r, R *z, CgState *st) {
   cudaStream_t s = S.stream;
   const int n3 = S.n3();
   if (iterpremax <= 0) {
-    copy_kernel<<<S.grid_vec(), kThreads, 0, s>>>(r, z, n3, st);
-    if (st) dot_kernel<1><<<S.grid_vec(), kThreads, 0, s>>>(r, z, n3, st, S.partials.p, 0, 0);
+    copy_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(r, z, n3, st);
+    if (st) dot_kernel<R, 1><<<S.grid_vec(), kThreads, 0, s>>>(r, z, n3, st, S.partials.p, 0, 0);
     return;
   }
   if (iterpremax == 1) {
-    if (st) launch_sweep<true>(S, r, z, st);
-    else launch_sweep<false>(S, r, z, nullptr);
+    if (st) launch_sweep<R, true>(S, V, r, z, st);
+    else launch_sweep<R, false>(S, V, r, z, nullptr);
     return;
   }
-  const double *in = r;
+  const R *in = r;
   for (int it = 1; it <= iterpremax; it++) {
-    launch_sweep<false>(S, in, S.zp.p, st);
-    if (it == 1) copy_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.zp.p, z, n3, st);
-    else add_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.zp.p, z, n3, st);
+    launch_sweep<R, false>(S, V, in, V.zp, st);
+    if (it == 1) copy_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.zp, z, n3, st);
+    else add_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.zp, z, n3, st);
     if (it == iterpremax) break;
-    spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), z, S.w.p, r, nullptr, nullptr);
-    in = S.w.p;
+    spmv_kernel<R, 1><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, z, V.w, r, nullptr, nullptr);
+    in = V.w;
   }
-  if (st) dot_kernel<1><<<S.grid_vec(), kThreads, 0, s>>>(r, z, n3, st, S.partials.p, 0, 0);
+  if (st) dot_kernel<R, 1><<<S.grid_vec(), kThreads, 0, s>>>(r, z, n3, st, S.partials.p, 0, 0);
 }
 
-void launch_prologue(Solver &S, cudaGraphConditionalHandle h, int use_cond) {
+template <class R>
+void launch_prologue(Solver &S, const Views<R> &V, cudaGraphConditionalHandle h, int use_cond) {
   cudaStream_t s = S.stream;
   CgState *st = S.state.p;
   cg_init_kernel<<<1, 32, 0, s>>>(st, S.params.p);
-  spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.r.p, S.b.p, nullptr, nullptr);
-  dot_kernel<0><<<S.grid_vec(), kThreads, 0, s>>>(S.b.p, S.b.p, S.n3(), st, S.partials.p, h, use_cond);
+  spmv_kernel<R, 1><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.x, V.r, V.b, nullptr, nullptr);
+  dot_kernel<R, 0><<<S.grid_vec(), kThreads, 0, s>>>(V.b, V.b, S.n3(), st, S.partials.p, h, use_cond);
 }
 
-void launch_iteration(Solver &S, int iterpremax, cudaGraphConditionalHandle h, int use_cond) {
+template <class R>
+void launch_iteration(Solver &S, const Views<R> &V, int iterpremax, cudaGraphConditionalHandle h, int use_cond) {
   cudaStream_t s = S.stream;
   CgState *st = S.state.p;
   const int n3 = S.n3();
   iter_begin_kernel<<<1, 32, 0, s>>>(st, h, use_cond);
-  launch_precond(S, iterpremax, S.r.p, S.z.p, st);
-  update_p_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.z.p, S.p.p, n3, st);
-  spmv_kernel<double, 2><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.p.p, S.q.p, nullptr, st, S.partials.p);
-  update_xr_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.x.p, S.p.p, S.r.p, S.q.p, n3, st, S.partials.p);
-  resid_ctl_kernel<double><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.r.p, S.b.p, st, S.partials.p,
-                                                              h, use_cond);
+  launch_precond<R>(S, V, iterpremax, V.r, V.z, st);
+  update_p_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.z, V.p, n3, st);
+  spmv_kernel<R, 2><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.p, V.q, nullptr, st, S.partials.p);
+  update_xr_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.x, V.p, V.r, V.q, n3, st, S.partials.p);
+  resid_ctl_kernel<R><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.x, V.r, V.b, st, S.partials.p, h, use_cond);
 }
 
-void build_graph(Solver &S, int iterpremax) {
-  const int key[4] = {S.generation, S.pc.generation, S.pc.kind, iterpremax};
-  if (S.exec && std::equal(key, key + 4, S.graph_key)) return;
-  S.drop_graph();
+// Network application z = zs + gamma W_out h3 (or z = zs when it is off), R-precision
+// vectors, BF16 weights, FP32 activations.
+template <class R>
+void launch_gnn(Solver &S, const R *zs, const R *r, R *z, CgState *st, bool bf16_weights) {
+  Learned &L = S.L;
+  cudaStream_t s = S.stream;
+  const GnnGraph g = L.graph();
+  const int gw = std::max(1, std::min((S.N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8));
+  const int gt = S.grid_vec();
+  gamma_kernel<R><<<gt, kThreads, 0, s>>>(zs, S.n3(), st, S.partials.p);
+  if (bf16_weights) {
+    const __nv_bfloat16 *th = L.theta_bf16.p;
+    gnn_encode_kernel<R, __nv_bfloat16><<<gt, kThreads, 0, s>>>(g, th, zs, r, &st->gamma, nullptr, L.h[0].p, st);
+    for (int l = 0; l < kGnnLayers; l++)
+      gnn_layer_kernel<__nv_bfloat16><<<gw, kThreads, 0, s>>>(g, th, l, L.w.p, L.h[l].p, nullptr, L.h[l + 1].p, st);
+    gnn_decode_kernel<R, __nv_bfloat16><<<gt, kThreads, 0, s>>>(S.N, th, L.h[3].p, zs, &st->gamma, z, st);
+  } else {
+    const float *th = L.theta.p;
+    gnn_encode_kernel<R, float><<<gt, kThreads, 0, s>>>(g, th, zs, r, &st->gamma, nullptr, L.h[0].p, st);
+    for (int l = 0; l < kGnnLayers; l++)
+      gnn_layer_kernel<float><<<gw, kThreads, 0, s>>>(g, th, l, L.w.p, L.h[l].p, nullptr, L.h[l + 1].p, st);
+    gnn_decode_kernel<R, float><<<gt, kThreads, 0, s>>>(S.N, th, L.h[3].p, zs, &st->gamma, z, st);
+  }
+}
+
+// One flexible-CG iteration with the learned preconditioner after SSOR
+// (iterPREmax = 1).  The network may be switched off on the device (fallback);
+// its kernels then only copy the SSOR output.
+template <class R>
+void launch_iteration_flex(Solver &S, const Views<R> &V, cudaGraphConditionalHandle h, int use_cond) {
+  cudaStream_t s = S.stream;
+  CgState *st = S.state.p;
+  const int n3 = S.n3();
+  iter_begin_kernel<<<1, 32, 0, s>>>(st, h, use_cond);
+  launch_sweep<R, false>(S, V, V.r, V.zs, st);
+  launch_gnn<R>(S, V.zs, V.r, V.z, st, true);
+  fcg_rho_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.z, V.r, V.rold, n3, st, S.partials.p);
+  update_p_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.z, V.p, n3, st);
+  spmv_kernel<R, 2><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.p, V.q, nullptr, st, S.partials.p);
+  update_xr_flex_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.x, V.p, V.r, V.rold, V.q, n3, st, S.partials.p);
+  resid_ctl_kernel<R><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.x, V.r, V.b, st, S.partials.p, h, use_cond);
+}
+
+// Mixed precision with reliable updates (graph body in FP32, FP64 pieces inside).
+// Prologue: r64 = b - A x64, ||b||^2 (FP64), r32 = float(r64), x32 = 0.
+void launch_prologue_reliable(Solver &S, cudaGraphConditionalHandle h, int use_cond) {
+  cudaStream_t s = S.stream;
+  CgState *st = S.state.p;
+  cg_init_kernel<<<1, 32, 0, s>>>(st, S.params.p);
+  spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.r.p, S.b.p, nullptr, nullptr);
+  dot_kernel<double, 0><<<S.grid_vec(), kThreads, 0, s>>>(S.b.p, S.b.p, S.n3(), st, S.partials.p, h, use_cond);
+  ru_init_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.r.p, S.rf.p, S.xf.p, S.n3(), st, S.partials.p, h, use_cond);
+}
+
+// One FP32 CG (or flexible CG with the network) iteration followed by the FP64
+// reliable update when due.
+void launch_iteration_reliable(Solver &S, int iterpremax, bool learned, cudaGraphConditionalHandle h,
+                               int use_cond) {
+  cudaStream_t s = S.stream;
+  CgState *st = S.state.p;
+  const int n3 = S.n3();
+  const Views<float> V = views(S, 0.0f);
+  iter_begin_kernel<<<1, 32, 0, s>>>(st, h, use_cond);
+  if (learned) {
+    launch_sweep<float, false>(S, V, V.r, V.zs, st);
+    launch_gnn<float>(S, V.zs, V.r, V.z, st, true);
+    fcg_rho_kernel<float><<<S.grid_vec(), kThreads, 0, s>>>(V.z, V.r, V.rold, n3, st, S.partials.p);
+  } else {
+    launch_precond<float>(S, V, iterpremax, V.r, V.z, st);
+  }
+  update_p_kernel<float><<<S.grid_vec(), kThreads, 0, s>>>(V.z, V.p, n3, st);
+  spmv_kernel<float, 2><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.p, V.q, nullptr, st, S.partials.p);
+  if (learned)
+    update_xr_flex_kernel<float><<<S.grid_vec(), kThreads, 0, s>>>(V.x, V.p, V.r, V.rold, V.q, n3, st, S.partials.p);
+  else
+    update_xr_kernel<float><<<S.grid_vec(), kThreads, 0, s>>>(V.x, V.p, V.r, V.q, n3, st, S.partials.p);
+  ru_update_x_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.x.p, S.xf.p, n3, st);
+  ru_resid_kernel<<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.r.p, S.b.p, S.rf.p, st, S.partials.p, h,
+                                                     use_cond);
+}
+
+template <class R>
+GraphSlot &slot_of(Solver &S) {
+  return sizeof(R) == sizeof(double) ? S.g64 : S.g32;
+}
+
+// mode bit 1: flexible CG with the learned preconditioner; bit 2: FP32 CG with FP64
+// reliable updates (R = float)
+template <class R>
+void build_graph(Solver &S, int iterpremax, int mode = 0) {
+  GraphSlot &G = slot_of<R>(S);
+  const int flexible = mode & 1;
+  const int lowp = (mode & 4) ? 1 : 0;
+  const int key[5] = {S.generation, S.pc.generation, S.pc.kind, iterpremax,
+                      mode + (flexible ? S.L.graph_generation * 4 : 0)};
+  if (G.exec && std::equal(key, key + 5, G.key)) return;
+  G.drop();
+  const Views<R> V = views(S, R(), lowp);
   cudaGraph_t g = nullptr;
   H33_CUDA(cudaGraphCreate(&g, 0));
-  S.graph = g;
+  G.graph = g;
   cudaGraphConditionalHandle h;
   H33_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
   // prologue
   H33_CUDA(cudaStreamBeginCaptureToGraph(S.stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  launch_prologue(S, h, 1);
+  if (mode & 2) launch_prologue_reliable(S, h, 1);
+  else launch_prologue<R>(S, V, h, 1);
   cudaStreamCaptureStatus cs;
   const cudaGraphNode_t *deps = nullptr;
   size_t ndeps = 0;
@@ -560,16 +779,72 @@ void build_graph(Solver &S, int iterpremax) {
   H33_CUDA(cudaGraphAddNode(&cnode, g, dep.data(), dep.size(), &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   H33_CUDA(cudaStreamBeginCaptureToGraph(S.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  launch_iteration(S, iterpremax, h, 1);
+  if (mode & 2) launch_iteration_reliable(S, iterpremax, flexible != 0, h, 1);
+  else if (flexible) launch_iteration_flex<R>(S, V, h, 1);
+  else launch_iteration<R>(S, V, iterpremax, h, 1);
   cudaGraph_t b2 = nullptr;
   H33_CUDA(cudaStreamEndCapture(S.stream, &b2));
-  H33_CUDA(cudaGraphInstantiate(&S.exec, g, 0));
-  std::copy(key, key + 4, S.graph_key);
+  H33_CUDA(cudaGraphInstantiate(&G.exec, g, 0));
+  std::copy(key, key + 5, G.key);
   size_t nbody = 0, nall = 0;
   H33_CUDA(cudaGraphGetNodes(body, nullptr, &nbody));
   H33_CUDA(cudaGraphGetNodes(g, nullptr, &nall));
-  S.kernels_per_iter = int(nbody);
-  S.prologue_kernels = int(nall) - 1;  // minus the conditional node
+  G.kernels_per_iter = int(nbody);
+  G.prologue_kernels = int(nall) - 1;  // minus the conditional node
+}
+
+// One CG run on the device in precision R (graph or stream mode); returns the final
+// state in S.h_state and the device time in ms; counts launched kernels.
+template <class R>
+float run_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels, int inner = 0, int learned = 0,
+             int reliable = 0, double ru_delta = 1e-4, int lowp = 0) {
+  const Views<R> V = views(S, R(), lowp);
+  const int mode = (learned ? 1 : 0) | (reliable ? 2 : 0) | (lowp ? 4 : 0);
+  S.h_params->tol = tol;
+  S.h_params->maxit = maxit;
+  S.h_params->iterpremax = iterpremax;
+  S.h_params->inner = inner || reliable;
+  S.h_params->flexible = learned;
+  S.h_params->use_gnn = learned;
+  S.h_params->reliable = reliable;
+  S.h_params->ru_delta = ru_delta;
+  H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, S.stream));
+  H33_CUDA(cudaEventRecord(S.ev0, S.stream));
+  if (graph_mode()) {
+    build_graph<R>(S, iterpremax, mode);
+    H33_CUDA(cudaGraphLaunch(slot_of<R>(S).exec, S.stream));
+    H33_CUDA(cudaEventRecord(S.ev1, S.stream));
+    H33_CUDA(cudaMemcpyAsync(S.h_state, S.state.p, sizeof(CgState), cudaMemcpyDeviceToHost, S.stream));
+    S.sync();
+    const GraphSlot &G = slot_of<R>(S);
+    const int executed = std::max(std::min(S.h_state->guard, maxit + 1), 0);
+    if (kernels) *kernels += G.prologue_kernels + executed * G.kernels_per_iter;
+  } else {
+    if (reliable) launch_prologue_reliable(S, 0, 0);
+    else launch_prologue<R>(S, V, 0, 0);
+    int launched = 0;
+    for (int done = 0, it = 0; !done && it <= maxit + kStreamChunk; it += kStreamChunk) {
+      for (int k = 0; k < kStreamChunk; k++) {
+        if (reliable) launch_iteration_reliable(S, iterpremax, learned != 0, 0, 0);
+        else if (learned) launch_iteration_flex<R>(S, V, 0, 0);
+        else launch_iteration<R>(S, V, iterpremax, 0, 0);
+      }
+      launched += kStreamChunk;
+      H33_CUDA(cudaGetLastError());
+      H33_CUDA(cudaMemcpyAsync(S.h_state, S.state.p, sizeof(CgState), cudaMemcpyDeviceToHost, S.stream));
+      S.sync();
+      done = S.h_state->done;
+    }
+    H33_CUDA(cudaEventRecord(S.ev1, S.stream));
+    S.sync();
+    (void)launched;
+  }
+  float ms = 0.0f;
+  H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+  const CgState &st = *S.h_state;
+  if (!st.done && !st.zero_rhs)
+    throw Failure(HECMW33_ERR_TIMEOUT, "device CG loop ended without a decision (internal error)");
+  return ms;
 }
 
 // Relative residual ||b - A x|| / ||b|| on the device (hecmw_rel_resid_L2_33).
@@ -577,98 +852,453 @@ double rel_resid_device(Solver &S) {
   cudaStream_t s = S.stream;
   CgState *st = S.state.p;
   spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.w.p, S.b.p, nullptr, nullptr);
-  dot_kernel<2><<<S.grid_vec(), kThreads, 0, s>>>(S.w.p, S.w.p, S.n3(), st, S.partials.p, 0, 0);
+  dot_kernel<double, 2><<<S.grid_vec(), kThreads, 0, s>>>(S.w.p, S.w.p, S.n3(), st, S.partials.p, 0, 0);
   double rr = 0.0;
   H33_CUDA(cudaMemcpyAsync(&rr, &st->rr_true, sizeof(double), cudaMemcpyDeviceToHost, s));
   S.sync();
-  double bb = S.h_state->bnrm2;
+  double bb = S.bnrm2;
   if (bb == 0.0) bb = 1.0;
   return std::sqrt(rr / bb);
 }
 
-double dot_device(Solver &S, const double *a, const double *b) {
+double dot_device_f(Solver &S, const float *a, const float *b) {
   CgState *st = S.state.p;
-  dot_kernel<2><<<S.grid_vec(), kThreads, 0, S.stream>>>(a, b, S.n3(), st, S.partials.p, 0, 0);
+  dot_kernel<float, 2><<<S.grid_vec(), kThreads, 0, S.stream>>>(a, b, S.n3(), st, S.partials.p, 0, 0);
   double v = 0.0;
   H33_CUDA(cudaMemcpyAsync(&v, &st->rr_true, sizeof(double), cudaMemcpyDeviceToHost, S.stream));
   S.sync();
   return v;
 }
 
-// The hecmw_solve / hecmw_solve_iterative sequence on resident B (S.b) and X (S.x).
-int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
+double dot_device(Solver &S, const double *a, const double *b) {
+  CgState *st = S.state.p;
+  dot_kernel<double, 2><<<S.grid_vec(), kThreads, 0, S.stream>>>(a, b, S.n3(), st, S.partials.p, 0, 0);
+  double v = 0.0;
+  H33_CUDA(cudaMemcpyAsync(&v, &st->rr_true, sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+  S.sync();
+  return v;
+}
+
+// FP32 copies of the matrix and preconditioner values (same sliced layouts),
+// refreshed when the FP64 values changed.
+void ensure_fp32(Solver &S) {
+  auto conv = [&](const double *a, float *b, size_t n) {
+    if (n == 0) return;
+    const int grid = int(std::min<size_t>((n + kThreads - 1) / kThreads, size_t(S.nsm) * 16));
+    convert_kernel<float><<<grid, kThreads, 0, S.stream>>>(a, b, n);
+    H33_CUDA(cudaGetLastError());
+  };
+  if (S.a32_version != S.values_version) {
+    S.A.val32.alloc(S.A.val.n);
+    conv(S.A.val.p, S.A.val32.p, S.A.val.n);
+    S.a32_version = S.values_version;
+  }
+  Precond &P = S.pc;
+  if (P.fp32_version != P.numeric_version) {
+    for (auto *d : {&P.lo, &P.up}) {
+      d->val32.alloc(d->val.n);
+      conv(d->val.p, d->val32.p, d->val.n);
+    }
+    P.alu32_fwd.alloc(P.alu_fwd.n);
+    conv(P.alu_fwd.p, P.alu32_fwd.p, P.alu_fwd.n);
+    if (!P.alu_shared) {
+      P.alu32_bwd.alloc(P.alu_bwd.n);
+      conv(P.alu_bwd.p, P.alu32_bwd.p, P.alu_bwd.n);
+    }
+    P.fp32_version = P.numeric_version;
+  }
+  const size_t n3 = size_t(S.n3());
+  for (auto *v : {&S.bf, &S.xf, &S.rf, &S.zf, &S.pf, &S.qf, &S.wf, &S.zpf}) v->alloc(n3);
+}
+
+// ---------------------------------------------------------------------------
+// Learned preconditioner (host side)
+
+// Node graph of the matrix (CSR of off-diagonal neighbours, reverse edges, raw
+// block ids) and the scaled features; rebuilt when the profile / values change.
+void learned_graph(Solver &S) {
+  Learned &L = S.L;
+  const int N = S.N;
+  if (L.graph_generation < 0 || L.built_for != S.generation) {
+    const int NPL = S.NPL;
+    std::vector<int> ptr(size_t(N) + 1, 0), col, src, row_of, rev;
+    col.reserve(size_t(S.NPL) + S.NPU);
+    for (int i = 0; i < N; i++) {
+      for (int j = S.indexL[i]; j < S.indexL[i + 1]; j++) {
+        col.push_back(S.itemL[j] - 1);
+        src.push_back(N + j);
+        row_of.push_back(i);
+      }
+      for (int j = S.indexU[i]; j < S.indexU[i + 1]; j++) {
+        col.push_back(S.itemU[j] - 1);
+        src.push_back(N + NPL + j);
+        row_of.push_back(i);
+      }
+      ptr[i + 1] = int(col.size());
+    }
+    const int ne = int(col.size());
+    rev.assign(size_t(ne), 0);
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < ne; e++) {
+      const int i = row_of[e], j = col[e];
+      const int *b = col.data() + ptr[j], *en = col.data() + ptr[j + 1];
+      const int *f = std::lower_bound(b, en, i);
+      rev[e] = (f != en && *f == i) ? int(f - col.data()) : e;
+    }
+    L.n = N;
+    L.nedges = ne;
+    L.ptr.upload(ptr, S.stream);
+    L.col.upload(col, S.stream);
+    L.src.upload(src, S.stream);
+    L.row_of.upload(row_of, S.stream);
+    L.rev.upload(rev, S.stream);
+    L.feat.alloc(size_t(9) * std::max(ne, 1));
+    L.s.alloc(size_t(N));
+    L.w.alloc(size_t(kGnnLayers) * std::max(ne, 1));
+    for (auto &h : L.h) h.alloc(size_t(N) * kGnnWidth);
+    L.built_for = S.generation;
+    L.graph_generation = ++S.build_counter;
+    L.feat_version = -1;
+  }
+  if (L.feat_version != S.values_version) {
+    const int grid = std::max(1, std::min((N + kThreads - 1) / kThreads, S.nsm * 8));
+    gnn_node_scale_kernel<<<grid, kThreads, 0, S.stream>>>(S.raw.p, N, L.s.p);
+    const int ge = std::max(1, std::min((L.nedges + kThreads - 1) / kThreads, S.nsm * 16));
+    gnn_edge_feat_kernel<<<ge, kThreads, 0, S.stream>>>(L.graph(), L.row_of.p, L.src.p, S.raw.p, L.feat.p);
+    H33_CUDA(cudaGetLastError());
+    L.feat_version = S.values_version;
+    L.w_version = -1;
+  }
+}
+
+// Edge weights of the current weights (BF16 copy for inference, FP32 for training).
+void learned_edge_weights(Solver &S, bool bf16) {
+  Learned &L = S.L;
+  const int ge = std::max(1, std::min((L.nedges + kThreads - 1) / kThreads, S.nsm * 16));
+  if (bf16) gnn_edge_weights_kernel<__nv_bfloat16><<<ge, kThreads, 0, S.stream>>>(L.graph(), L.theta_bf16.p, L.w.p);
+  else gnn_edge_weights_kernel<float><<<ge, kThreads, 0, S.stream>>>(L.graph(), L.theta.p, L.w.p);
+  H33_CUDA(cudaGetLastError());
+  L.w_version = bf16 ? L.weights_version : -1;
+}
+
+void learned_set_weights(Solver &S, const float *theta_host, bool reset_adam) {
+  Learned &L = S.L;
+  const int n = GnnOffsets::make().total;
+  L.theta.upload(theta_host, size_t(n), S.stream);
+  std::vector<__nv_bfloat16> b(static_cast<size_t>(n));
+  for (int k = 0; k < n; k++) b[size_t(k)] = __float2bfloat16(theta_host[k]);
+  L.theta_bf16.upload(b.data(), b.size(), S.stream);
+  if (reset_adam || L.m1.n != size_t(n)) {
+    L.m1.alloc(size_t(n));
+    L.m2.alloc(size_t(n));
+    L.m1.zero(S.stream);
+    L.m2.zero(S.stream);
+    L.adam_step = 0;
+  }
+  L.grad.alloc(size_t(n));
+  L.gacc.alloc(size_t(n));
+  L.have_weights = true;
+  L.weights_version++;
+  S.sync();
+}
+
+// Deterministic initial weights (scaled Gaussian; the output layer starts small so
+// that the untrained network is close to plain SSOR).
+void learned_init_weights(Solver &S, uint64_t seed) {
+  const GnnOffsets o = GnnOffsets::make();
+  std::vector<float> th(size_t(o.total), 0.0f);
+  uint64_t st = seed * 0x9E3779B97F4A7C15ull + 1;
+  auto normal = [&]() {
+    auto next = [&]() {
+      uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      return double((z ^ (z >> 31)) >> 11) * (1.0 / 9007199254740992.0);
+    };
+    double u1 = next(), u2 = next();
+    if (u1 < 1e-300) u1 = 1e-300;
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+  };
+  for (int k = 0; k < kGnnWidth * 6; k++) th[size_t(o.W_in + k)] = float(normal() / std::sqrt(6.0));
+  for (int l = 0; l < kGnnLayers; l++) {
+    for (int k = 0; k < 9; k++) th[size_t(o.u[l] + k)] = float(0.3 * normal());
+    th[size_t(o.c[l])] = 0.5f;
+    for (int k = 0; k < kGnnWidth * kGnnWidth; k++) {
+      th[size_t(o.Ws[l] + k)] = float(normal() / std::sqrt(double(kGnnWidth)));
+      th[size_t(o.Wm[l] + k)] = float(normal() / std::sqrt(double(kGnnWidth)) / 8.0);
+    }
+  }
+  for (int k = 0; k < 3 * kGnnWidth; k++) th[size_t(o.W_out + k)] = float(0.01 * normal());
+  learned_set_weights(S, th.data(), true);
+}
+
+// Ready for inference inside a solve: graph, features, BF16 edge weights.
+void learned_prepare_inference(Solver &S) {
+  Learned &L = S.L;
+  if (!L.have_weights) throw Failure(HECMW33_ERR_INCONS_PC, "learned preconditioner requested but not trained");
+  if (!(S.pc.valid && S.pc.kind == 1))
+    throw Failure(HECMW33_ERR_INCONS_PC, "the learned preconditioner works after SSOR (PRECOND 1 or 2)");
+  learned_graph(S);
+  if (L.w_version != L.weights_version) learned_edge_weights(S, true);
+  const size_t n3 = size_t(S.n3());
+  S.zs.alloc(n3);
+  S.rold.alloc(n3);
+  S.zsf.alloc(n3);
+  S.roldf.alloc(n3);
+}
+
+// Training buffers (activations saved for the backward pass).
+void learned_train_buffers(Solver &S) {
+  Learned &L = S.L;
+  const size_t nw = size_t(S.N) * kGnnWidth;
+  for (auto &m : L.m) m.alloc(nw);
+  L.x.alloc(size_t(S.N) * 6);
+  L.gm.alloc(nw);
+  L.dh.alloc(nw);
+  L.dhp.alloc(nw);
+  const size_t n3 = size_t(S.n3());
+  for (auto *v : {&L.t_z, &L.t_zs, &L.t_d, &L.t_q, &L.t_dz}) v->alloc(n3);
+  L.nparts = std::max(1, std::min((S.N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 4));
+  L.stride = GnnOffsets::make().total;
+  L.part.alloc(size_t(L.nparts) * L.stride);
+}
+
+// Forward (FP32 weights, activations kept) + energy loss + backward for one pair
+// (r, e) with zs = SSOR(r) precomputed; adds coef * grad into gacc.  Returns the
+// loss value through the device (read by the caller after a sync).
+void learned_pair_grad(Solver &S, const float *r, const float *e, const float *zs, double er, float coef,
+                       double *loss_slot) {
+  Learned &L = S.L;
+  cudaStream_t s = S.stream;
+  CgState *st = S.state.p;
+  const GnnGraph g = L.graph();
+  const int n3 = S.n3();
+  const int gw = std::max(1, std::min((S.N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8));
+  const int gt = S.grid_vec();
+  gnn_state_kernel<<<1, 32, 0, s>>>(st);
+  gamma_kernel<float><<<gt, kThreads, 0, s>>>(zs, n3, st, S.partials.p);
+  gnn_encode_kernel<float, float><<<gt, kThreads, 0, s>>>(g, L.theta.p, zs, r, &st->gamma, L.x.p, L.h[0].p, st);
+  for (int l = 0; l < kGnnLayers; l++)
+    gnn_layer_kernel<float><<<gw, kThreads, 0, s>>>(g, L.theta.p, l, L.w.p, L.h[l].p, L.m[l].p, L.h[l + 1].p, st);
+  gnn_decode_kernel<float, float><<<gt, kThreads, 0, s>>>(S.N, L.theta.p, L.h[3].p, zs, &st->gamma, L.t_z.p, st);
+  // d = z - e, q = A d (FP32), loss = d.q / e.r, dz = 2 q / e.r
+  sub_kernel<<<gt, kThreads, 0, s>>>(L.t_z.p, e, L.t_d.p, n3);
+  spmv_kernel<float, 0><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view32(), L.t_d.p, L.t_q.p, nullptr, nullptr, nullptr);
+  dot_kernel<float, 2><<<gt, kThreads, 0, s>>>(L.t_d.p, L.t_q.p, n3, st, S.partials.p, 0, 0);
+  H33_CUDA(cudaMemcpyAsync(loss_slot, &st->rr_true, sizeof(double), cudaMemcpyDeviceToDevice, s));
+  scale_kernel<<<gt, kThreads, 0, s>>>(L.t_q.p, float(2.0 / er), L.t_dz.p, n3);
+  // backward
+  const int np = L.nparts, stride = L.stride;
+  gnn_decode_bwd_kernel<<<np, kThreads, 0, s>>>(S.N, L.theta.p, L.h[3].p, L.t_dz.p, &st->gamma, L.dh.p, L.part.p,
+                                                stride);
+  for (int l = kGnnLayers - 1; l >= 0; l--) {
+    gnn_layer_bwd_kernel<<<np, kThreads, 0, s>>>(g, L.theta.p, l, L.w.p, L.h[l].p, L.h[l + 1].p, L.m[l].p, L.dh.p,
+                                                 L.gm.p, L.dhp.p, L.part.p, stride);
+    gnn_layer_bwd_gather_kernel<<<gw, kThreads, 0, s>>>(g, l, L.w.p, L.gm.p, L.dhp.p);
+    std::swap(L.dh, L.dhp);
+  }
+  gnn_encode_bwd_kernel<<<np, kThreads, 0, s>>>(S.N, L.x.p, L.dh.p, L.part.p, stride);
+  gnn_reduce_grads_kernel<<<(stride + 255) / 256, 256, 0, s>>>(L.part.p, np, stride, L.grad.p, stride);
+  accum_kernel<<<(stride + 255) / 256, 256, 0, s>>>(L.grad.p, coef, L.gacc.p, stride);
+  H33_CUDA(cudaGetLastError());
+  (void)er;
+}
+
+// FP64 CG in stream mode, one iteration per host step, keeping x at iterations
+// 1, 2, 4, 8, ... (x_0 = the start); after convergence every kept x_k gives a
+// training pair (r_k = b - A x_k, e_k = x* - x_k) for the learned preconditioner.
+float record_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels) {
+  Learned &L = S.L;
+  const Views<double> V = views(S, 0.0);
+  const size_t n3 = size_t(S.n3());
+  S.h_params->tol = tol;
+  S.h_params->maxit = maxit;
+  S.h_params->iterpremax = iterpremax;
+  S.h_params->inner = 0;
+  S.h_params->flexible = 0;
+  S.h_params->use_gnn = 0;
+  S.h_params->reliable = 0;
+  S.h_params->ru_delta = 1.0;
+  H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, S.stream));
+  H33_CUDA(cudaEventRecord(S.ev0, S.stream));
+  launch_prologue<double>(S, V, 0, 0);
+  std::vector<DevArray<double>> snaps;
+  int next = 1;
+  for (int it = 1; it <= maxit + 1; it++) {
+    if (it == next && snaps.size() < 24) {
+      snaps.emplace_back();
+      snaps.back().alloc(n3);
+      H33_CUDA(cudaMemcpyAsync(snaps.back().p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, S.stream));
+      next *= 2;
+    }
+    launch_iteration<double>(S, V, iterpremax, 0, 0);
+    H33_CUDA(cudaGetLastError());
+    H33_CUDA(cudaMemcpyAsync(S.h_state, S.state.p, sizeof(CgState), cudaMemcpyDeviceToHost, S.stream));
+    S.sync();
+    if (S.h_state->done) break;
+  }
+  H33_CUDA(cudaEventRecord(S.ev1, S.stream));
+  S.sync();
+  float ms = 0.0f;
+  H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+  if (kernels) *kernels += 3 + S.h_state->iter * 40;
+  if (S.h_state->error == 0 && S.h_state->converged) {
+    const int gt = S.grid_vec();
+    for (auto &x : snaps) {
+      DevArray<float> pr, pe;
+      pr.alloc(n3);
+      pe.alloc(n3);
+      spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, S.stream>>>(S.A.view(), x.p, S.w.p, S.b.p, nullptr,
+                                                                        nullptr);
+      narrow_kernel<<<gt, kThreads, 0, S.stream>>>(S.w.p, pr.p, int(n3));
+      diff_narrow_kernel<<<gt, kThreads, 0, S.stream>>>(S.x.p, x.p, pe.p, int(n3));
+      H33_CUDA(cudaGetLastError());
+      // e.r of the stored FP32 pair (FP64 accumulation) -- the normaliser of its loss
+      const double er = dot_device_f(S, pe.p, pr.p);
+      if (!(er > 0.0)) continue;
+      L.pr.push_back(std::move(pr));
+      L.pe.push_back(std::move(pe));
+      L.pzs.emplace_back();
+      L.per.push_back(er);
+      while (int(L.pr.size()) > L.max_pairs) {
+        L.pr.erase(L.pr.begin());
+        L.pe.erase(L.pe.begin());
+        L.pzs.erase(L.pzs.begin());
+        L.per.erase(L.per.begin());
+      }
+    }
+    S.sync();
+  }
+  return ms;
+}
+
+// Trains the network on the recorded pairs: Adam on the mean energy-norm loss.
+// loss[0] = mean loss before the first step, loss[1] = after the last.
+void learned_train(Solver &S, int steps, double lr, double *loss) {
+  Learned &L = S.L;
+  const int np = int(L.pr.size());
+  if (np == 0) throw Failure(HECMW33_ERR_BAD_INPUT, "no recorded pairs: enable recording and solve first");
+  if (!(S.pc.valid && S.pc.kind == 1))
+    throw Failure(HECMW33_ERR_INCONS_PC, "training needs the SSOR preconditioner of the matrix");
+  ensure_fp32(S);
+  learned_graph(S);
+  learned_train_buffers(S);
+  if (!L.have_weights) learned_init_weights(S, 12345);
+  const Views<float> V = views(S, 0.0f);
+  const size_t n3 = size_t(S.n3());
+  for (int k = 0; k < np; k++)
+    if (L.pzs[size_t(k)].n != n3) {
+      L.pzs[size_t(k)].alloc(n3);
+      launch_sweep<float, false>(S, V, L.pr[size_t(k)].p, L.pzs[size_t(k)].p, nullptr);
+    }
+  L.losses.alloc(size_t(np));
+  std::vector<double> lh(static_cast<size_t>(np));
+  const int nparam = GnnOffsets::make().total;
+  auto eval_pass = [&](bool update) {
+    learned_edge_weights(S, false);
+    L.gacc.zero(S.stream);
+    for (int k = 0; k < np; k++)
+      learned_pair_grad(S, L.pr[size_t(k)].p, L.pe[size_t(k)].p, L.pzs[size_t(k)].p, L.per[size_t(k)],
+                        1.0f / float(np), L.losses.p + k);
+    if (update) {
+      L.adam_step++;
+      gnn_adam_kernel<<<(nparam + 255) / 256, 256, 0, S.stream>>>(L.theta.p, L.gacc.p, L.m1.p, L.m2.p, nparam,
+                                                                  float(lr), 0.9f, 0.999f, 1e-8f, L.adam_step, 1.0f,
+                                                                  L.theta_bf16.p);
+      H33_CUDA(cudaGetLastError());
+    }
+    H33_CUDA(cudaMemcpyAsync(lh.data(), L.losses.p, sizeof(double) * size_t(np), cudaMemcpyDeviceToHost, S.stream));
+    S.sync();
+    double m = 0.0;
+    for (int k = 0; k < np; k++) m += lh[size_t(k)] / L.per[size_t(k)];
+    return m / np;
+  };
+  loss[0] = eval_pass(false);
+  for (int it = 0; it < steps; it++) eval_pass(true);
+  loss[1] = eval_pass(false);
+  L.weights_version++;
+}
+
+// BF16 copies of the preconditioner's sweep values and FP32 copies of its diagonal
+// LU (same layouts), refreshed when the preconditioner's values changed.
+void ensure_lowp(Solver &S) {
+  Precond &P = S.pc;
+  if (P.lowp_version == P.numeric_version) return;
+  auto grid = [&](size_t n) { return int(std::max<size_t>(1, std::min<size_t>((n + kThreads - 1) / kThreads, size_t(S.nsm) * 16))); };
+  for (auto *d : {&P.lo, &P.up}) {
+    d->val16.alloc(d->val.n);
+    if (d->val.n) convert_bf16_kernel<<<grid(d->val.n), kThreads, 0, S.stream>>>(d->val.p, d->val16.p, d->val.n);
+  }
+  P.alu32_fwd.alloc(P.alu_fwd.n);
+  if (P.alu_fwd.n) convert_kernel<float><<<grid(P.alu_fwd.n), kThreads, 0, S.stream>>>(P.alu_fwd.p, P.alu32_fwd.p, P.alu_fwd.n);
+  if (!P.alu_shared) {
+    P.alu32_bwd.alloc(P.alu_bwd.n);
+    convert_kernel<float><<<grid(P.alu_bwd.n), kThreads, 0, S.stream>>>(P.alu_bwd.p, P.alu32_bwd.p, P.alu_bwd.n);
+  }
+  H33_CUDA(cudaGetLastError());
+  P.lowp_version = P.numeric_version;
+  P.fp32_version = -1;  // the FP32 ALU copy now follows the low-precision path
+}
+
+// Checks and preconditioner setup shared by the FP64 and mixed solves
+// (hecmw_solve + hecmw_solve_iterative up to the CG call).  Returns 0 to go on,
+// or the code to return (2002 with X = 0, 2001).
+int prepare_solve(Solver &S, int *Iarray, double *Rarray, double *sigma, bool *auto_sigma) {
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_set_matrix first");
-  const double t0 = wall();
-  *iter = 0;
-  *resid = 0.0;
-  if (times) times[0] = times[1] = times[2] = 0.0;
   // zero right-hand side (hecmw_solver.f90:32-37)
-  const double bb = dot_device(S, S.b.p, S.b.p);
-  if (bb == 0.0) {
+  S.bnrm2 = dot_device(S, S.b.p, S.b.p);
+  if (S.bnrm2 == 0.0) {
     H33_CUDA(cudaMemsetAsync(S.x.p, 0, sizeof(double) * S.n3(), S.stream));
     S.sync();
     Iarray[80] = 1;
     Iarray[81] = 0;
     return HECMW33_ERR_ZERO_RHS;
   }
-  const int MAXIT = Iarray[0], METHOD = Iarray[1], PRECOND = Iarray[2], iterPREmax = Iarray[4];
-  const int NCOLOR_IN = Iarray[33];
-  const double TOL = Rarray[0];
-  double sigma = Rarray[1];
-  const bool auto_sigma = sigma < 0.0;
-  if (auto_sigma) sigma = 1.0;
+  const int METHOD = Iarray[1], PRECOND = Iarray[2], iterPREmax = Iarray[4];
+  *sigma = Rarray[1];
+  *auto_sigma = *sigma < 0.0;
+  if (*auto_sigma) *sigma = 1.0;
   if (S.zero_diag && PRECOND < 10 && iterPREmax > 0) return HECMW33_ERR_ZERO_DIAG;
   if (METHOD != 1)
     throw Failure(HECMW33_ERR_INCONS_PC, "METHOD " + std::to_string(METHOD) + ": the GPU drop-in implements CG (1)");
   recycle_precond_setting(Iarray);
-  {
-    Range rg("hecmw33_precond_setup");
-    if (iterPREmax > 0) precond_setup(S, PRECOND, NCOLOR_IN, sigma, Iarray);
-    if (graph_mode()) build_graph(S, iterPREmax);
-  }
+  Range rg("hecmw33_precond_setup");
+  if (iterPREmax > 0) precond_setup(S, PRECOND, Iarray[33], *sigma, Iarray);
+  return 0;
+}
+
+// The hecmw_solve / hecmw_solve_iterative sequence on resident B (S.b) and X (S.x),
+// FP64 throughout (the drop-in).
+int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times, int lowp = 0) {
+  const double t0 = wall();
+  *iter = 0;
+  *resid = 0.0;
+  if (times) times[0] = times[1] = times[2] = 0.0;
+  double sigma;
+  bool auto_sigma;
+  const int pre = prepare_solve(S, Iarray, Rarray, &sigma, &auto_sigma);
+  if (pre) return pre;
+  const int MAXIT = Iarray[0], PRECOND = Iarray[2], iterPREmax = Iarray[4];
+  const double TOL = Rarray[0];
+  const int learned = Iarray[42] == 1 ? 1 : 0;
+  if (learned) learned_prepare_inference(S);
+  if (lowp && iterPREmax > 0) ensure_lowp(S);
+  else lowp = 0;
+  const bool record = S.L.recording && !learned;
+  if (graph_mode() && !record) build_graph<double>(S, iterPREmax, learned | (lowp ? 4 : 0));
   Range rs("hecmw33_solve");
   const double t1 = wall();
-  int error = 0;
+  int error = 0, kernels = 1;
   float ms_total = 0.0f;
-  const bool use_graph = graph_mode();
   for (;;) {
     Iarray[80] = 0;
     Iarray[81] = 0;
-    S.h_params->tol = TOL;
-    S.h_params->maxit = MAXIT;
-    S.h_params->iterpremax = iterPREmax;
-    H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, S.stream));
-    H33_CUDA(cudaEventRecord(S.ev0, S.stream));
-    if (use_graph) {
-      H33_CUDA(cudaGraphLaunch(S.exec, S.stream));
-      H33_CUDA(cudaEventRecord(S.ev1, S.stream));
-      H33_CUDA(cudaMemcpyAsync(S.h_state, S.state.p, sizeof(CgState), cudaMemcpyDeviceToHost, S.stream));
-      S.sync();
-    } else {
-      launch_prologue(S, 0, 0);
-      for (int done = 0, it = 0; !done && it <= MAXIT + kStreamChunk; it += kStreamChunk) {
-        for (int k = 0; k < kStreamChunk; k++) launch_iteration(S, iterPREmax, 0, 0);
-        H33_CUDA(cudaGetLastError());
-        H33_CUDA(cudaMemcpyAsync(S.h_state, S.state.p, sizeof(CgState), cudaMemcpyDeviceToHost, S.stream));
-        S.sync();
-        done = S.h_state->done;
-      }
-      H33_CUDA(cudaEventRecord(S.ev1, S.stream));
-      S.sync();
-    }
-    float ms = 0.0f;
-    H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
-    ms_total += ms;
+    if (record) ms_total += record_cg(S, iterPREmax, TOL, MAXIT, &kernels);
+    else ms_total += run_cg<double>(S, iterPREmax, TOL, MAXIT, &kernels, 0, learned, 0, 1e-4, lowp);
     const CgState &st = *S.h_state;
     error = st.error;
-    if (!st.done && !st.zero_rhs)
-      throw Failure(HECMW33_ERR_TIMEOUT, "device CG loop ended without a decision (internal error)");
     *iter = st.iter;
     *resid = st.resid;
-    if (st.zero_rhs) {  // not reached after the host-side test, kept for completeness
-      *iter = 0;
-      *resid = 0.0;
-    }
     if (error == HECMW33_ERR_DIVERGE_PC || error == HECMW33_ERR_DIVERGE_MAT || error == HECMW33_ERR_DIVERGE_NAN) {
       Iarray[81] = 1;
       // Iterative.f90:133-137; the reference's retry reuses the factorisation
@@ -682,16 +1312,14 @@ int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *re
   }
   const double resid2 = rel_resid_device(S);
   if (resid2 < TOL) Iarray[80] = 1;
-  {
-    // launches: zero-RHS dot, per graph launch the prologue plus one body per
-    // executed iteration (iterations that stopped early still launched the body),
-    // and the true-residual SpMV + dot
-    const int executed = std::min(S.h_state->iter, MAXIT);
-    S.last_iter = *iter;
-    S.last_kernels = 1 + S.prologue_kernels + std::max(executed, 0) * S.kernels_per_iter + 2;
-    S.last_solve_s = ms_total * 1e-3;
-    S.last_setup_s = t1 - t0;
-  }
+  S.last_learned = learned;
+  S.last_fallback = S.h_state->fallback;
+  S.last_iter = *iter;
+  S.last_outer = 1;
+  S.last_kernels = kernels + 2;
+  S.last_solve_s = ms_total * 1e-3;
+  S.last_setup_s = t1 - t0;
+  S.last_true_resid = resid2;
   if (times) {
     times[0] = t1 - t0;
     times[1] = ms_total * 1e-3;
@@ -699,6 +1327,166 @@ int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *re
   }
   return error;
 }
+
+// Mixed precision (selected by Iarray(42) = 1): FP64 iterative refinement around
+// FP32 preconditioned CG.  Matrix and preconditioner are FP32 copies of the FP64
+// ones; inner CG vectors are FP32 while every dot product (RHO, C1, DNRM2) is
+// accumulated in FP64, so ALPHA/BETA are FP64 values; the outer true residual
+// r = b - A x, its norm and the correction x += d are FP64.  The inner solve stops
+// at a relative residual of Rarray(42) (default 1e-4); the outer loop stops at
+// Rarray(1) on the FP64 true residual.  ITER reports the total inner iterations.
+int solve_mixed_restart(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
+  const double t0 = wall();
+  *iter = 0;
+  *resid = 0.0;
+  if (times) times[0] = times[1] = times[2] = 0.0;
+  double sigma;
+  bool auto_sigma;
+  const int pre = prepare_solve(S, Iarray, Rarray, &sigma, &auto_sigma);
+  if (pre) return pre;
+  const int MAXIT = Iarray[0], iterPREmax = Iarray[4];
+  const double TOL = Rarray[0];
+  const double TOL_IN = Rarray[41] > 0.0 ? Rarray[41] : 1e-4;
+  ensure_fp32(S);
+  if (graph_mode()) build_graph<float>(S, iterPREmax);
+  Range rs("hecmw33_solve_mixed");
+  const double t1 = wall();
+  Iarray[80] = 0;
+  Iarray[81] = 0;
+  const int n3 = S.n3();
+  cudaStream_t s = S.stream;
+  cudaEvent_t e0, e1;
+  H33_CUDA(cudaEventCreate(&e0));
+  H33_CUDA(cudaEventCreate(&e1));
+  H33_CUDA(cudaEventRecord(e0, s));
+  int kernels = 1, total_inner = 0, outer = 0, error = 0;
+  // r = b - A x in FP64
+  spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.r.p, S.b.p, nullptr, nullptr);
+  double rr = dot_device(S, S.r.p, S.r.p);
+  kernels += 2;
+  double res = std::sqrt(rr / S.bnrm2);
+  constexpr int kMaxOuter = 60;
+  while (!(res <= TOL)) {
+    if (res != res) {
+      error = HECMW33_ERR_DIVERGE_NAN;
+      break;
+    }
+    if (outer >= kMaxOuter || total_inner >= MAXIT) {
+      error = HECMW33_ERR_NOCONV_MAXIT;
+      break;
+    }
+    narrow_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.r.p, S.bf.p, n3);
+    H33_CUDA(cudaMemsetAsync(S.xf.p, 0, sizeof(float) * n3, s));
+    run_cg<float>(S, iterPREmax, TOL_IN, MAXIT - total_inner, &kernels, 1);
+    const CgState st = *S.h_state;
+    const int inner = std::min(st.iter, MAXIT - total_inner);
+    total_inner += std::max(inner, 0);
+    if (st.error == HECMW33_ERR_DIVERGE_PC || st.error == HECMW33_ERR_DIVERGE_MAT ||
+        st.error == HECMW33_ERR_DIVERGE_NAN) {
+      error = st.error;
+      Iarray[81] = 1;
+      break;
+    }
+    widen_add_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.xf.p, S.x.p, n3);
+    spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.r.p, S.b.p, nullptr, nullptr);
+    rr = dot_device(S, S.r.p, S.r.p);
+    kernels += 4;
+    res = std::sqrt(rr / S.bnrm2);
+    outer++;
+  }
+  H33_CUDA(cudaEventRecord(e1, s));
+  S.sync();
+  float ms = 0.0f;
+  H33_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *iter = total_inner;
+  *resid = res;
+  if (res < TOL) Iarray[80] = 1;
+  S.last_iter = total_inner;
+  S.last_outer = outer;
+  S.last_kernels = kernels;
+  S.last_solve_s = ms * 1e-3;
+  S.last_setup_s = t1 - t0;
+  S.last_true_resid = res;
+  if (times) {
+    times[0] = t1 - t0;
+    times[1] = ms * 1e-3;
+    times[2] = 0.0;
+  }
+  return error;
+}
+
+// Mixed precision with reliable updates (Iarray(42) = 1): FP32 CG + SSOR (FP32
+// matrix and preconditioner copies, FP64 dot products) whose solution and residual
+// are folded into FP64 -- x64 += x32, r64 = b - A x64 (FP64 SpMV), r32 = float(r64)
+// -- each time the FP32 residual has fallen by Rarray(42) (default 1e-4) since the
+// last update, and at the tolerance.  Convergence is decided on the FP64 true
+// residual; the FP32 recurrence keeps its search direction across updates, so the
+// iteration count stays close to the FP64 solve's.  With Iarray(43) = 1 the
+// learned preconditioner runs after the FP32 SSOR (flexible CG).
+int solve_mixed_reliable(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
+  const double t0 = wall();
+  *iter = 0;
+  *resid = 0.0;
+  if (times) times[0] = times[1] = times[2] = 0.0;
+  double sigma;
+  bool auto_sigma;
+  const int pre = prepare_solve(S, Iarray, Rarray, &sigma, &auto_sigma);
+  if (pre) return pre;
+  const int MAXIT = Iarray[0], iterPREmax = Iarray[4];
+  const double TOL = Rarray[0];
+  const double DELTA = Rarray[41] > 0.0 ? Rarray[41] : 0.1;
+  const int learned = Iarray[42] == 1 ? 1 : 0;
+  ensure_fp32(S);
+  if (learned) learned_prepare_inference(S);
+  if (graph_mode()) build_graph<float>(S, iterPREmax, 2 | learned);
+  Range rs("hecmw33_solve_mixed");
+  const double t1 = wall();
+  Iarray[80] = 0;
+  Iarray[81] = 0;
+  int kernels = 1;
+  const float ms = run_cg<float>(S, iterPREmax, TOL, MAXIT, &kernels, 0, learned, 1, DELTA);
+  const CgState st = *S.h_state;
+  // fold a correction not yet carried into x64 (a stop between reliable updates)
+  widen_add_kernel<<<S.grid_vec(), kThreads, 0, S.stream>>>(S.xf.p, S.x.p, S.n3());
+  const int error = st.error;
+  *iter = st.iter;
+  *resid = st.resid;
+  if (error == HECMW33_ERR_DIVERGE_PC || error == HECMW33_ERR_DIVERGE_MAT || error == HECMW33_ERR_DIVERGE_NAN)
+    Iarray[81] = 1;
+  const double resid2 = rel_resid_device(S);
+  if (resid2 < TOL) Iarray[80] = 1;
+  S.last_learned = learned;
+  S.last_fallback = st.fallback;
+  S.last_iter = *iter;
+  S.last_outer = st.ru_count;
+  S.last_kernels = kernels + 3;
+  S.last_solve_s = ms * 1e-3;
+  S.last_setup_s = t1 - t0;
+  S.last_true_resid = resid2;
+  if (times) {
+    times[0] = t1 - t0;
+    times[1] = ms * 1e-3;
+    times[2] = 0.0;
+  }
+  return error;
+}
+
+int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
+  switch (Iarray[41]) {
+    case 1: return solve_fp64(S, Iarray, Rarray, iter, resid, times, 1);
+    case 2: return solve_mixed_restart(S, Iarray, Rarray, iter, resid, times);
+    case 3: return solve_mixed_reliable(S, Iarray, Rarray, iter, resid, times);
+    default: return solve_fp64(S, Iarray, Rarray, iter, resid, times, 0);
+  }
+}
+
+}  // namespace
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+namespace {
 
 void fail(int *ierr, int code, const char *msg) {
   g_last_error = msg;
@@ -855,7 +1643,7 @@ HECMW33_API void hecmw33_gpu_precond_apply(const int *handle, const double *R, d
   if (iterPREmax > 0) precond_setup(S, Iarray[2], Iarray[33], sigma, Iarray);
   const size_t bytes = sizeof(double) * S.n3();
   H33_CUDA(cudaMemcpyAsync(S.r.p, R, bytes, cudaMemcpyHostToDevice, S.stream));
-  launch_precond(S, iterPREmax, S.r.p, S.z.p, nullptr);
+  launch_precond<double>(S, views(S, 0.0), iterPREmax, S.r.p, S.z.p, nullptr);
   H33_CUDA(cudaGetLastError());
   H33_CUDA(cudaMemcpyAsync(Z, S.z.p, bytes, cudaMemcpyDeviceToHost, S.stream));
   S.sync();
@@ -894,14 +1682,18 @@ HECMW33_API void hecmw33_gpu_last_solve_info(const int *handle, int *info, doubl
   if (ierr) *ierr = 0;
   H33_ENTRY_BEGIN
   Solver &S = get(handle);
-  for (int i = 0; i < 8; i++) {
+  for (int i = 0; i < 16; i++) {
     info[i] = 0;
     dinfo[i] = 0.0;
   }
+  info[8] = S.last_learned;
+  info[9] = S.last_fallback;
+  info[10] = int(S.L.pr.size());
   info[0] = S.last_iter;
   info[1] = S.last_kernels;
   info[2] = S.pc.valid ? int(S.pc.lo.group_slice.size() + S.pc.up.group_slice.size()) - 2 : 0;
-  info[3] = S.kernels_per_iter;
+  info[3] = S.g64.kernels_per_iter ? S.g64.kernels_per_iter : S.g32.kernels_per_iter;
+  info[7] = S.last_outer;
   const double N = S.N, NPL = S.NPL, NPU = S.NPU, NZ = N + NPL + NPU;
   info[4] = int(NZ);
   info[5] = S.A.nslices;
@@ -919,7 +1711,10 @@ HECMW33_API void hecmw33_gpu_last_solve_info(const int *handle, int *info, doubl
   size_t held = S.raw.bytes() + S.A.bytes() + S.pc.lo.bytes() + S.pc.up.bytes() + S.pc.alu_fwd.bytes() +
                 S.pc.alu_bwd.bytes() + S.pc.ilu_raw.bytes();
   for (auto *v : {&S.b, &S.x, &S.r, &S.z, &S.p, &S.q, &S.w, &S.zp}) held += v->bytes();
+  held += S.pc.alu32_fwd.bytes() + S.pc.alu32_bwd.bytes();
+  for (auto *v : {&S.bf, &S.xf, &S.rf, &S.zf, &S.pf, &S.qf, &S.wf, &S.zpf}) held += v->bytes();
   dinfo[4] = double(held);
+  dinfo[5] = S.last_true_resid;
   H33_ENTRY_END
 }
 
@@ -941,6 +1736,101 @@ HECMW33_API void hecmw33_gpu_time_spmv(const int *handle, const int *reps, doubl
   float ms = 0.0f;
   H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
   *ms_per_launch = double(ms) / n;
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_learn_record(const int *handle, const int *enable, const int *max_pairs,
+                                          int *npairs, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  S.L.recording = enable && *enable != 0;
+  if (max_pairs && *max_pairs > 0) S.L.max_pairs = *max_pairs;
+  if (enable && *enable < 0) {  // forget the recorded pairs
+    S.L.pr.clear();
+    S.L.pe.clear();
+    S.L.pzs.clear();
+    S.L.per.clear();
+    S.L.recording = false;
+  }
+  if (npairs) *npairs = int(S.L.pr.size());
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_learn_train(const int *handle, const int *steps, const double *lr, double *loss,
+                                         int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  double l2[2] = {0.0, 0.0};
+  learned_train(S, steps ? *steps : 100, lr ? *lr : 1e-3, l2);
+  if (loss) {
+    loss[0] = l2[0];
+    loss[1] = l2[1];
+  }
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_learn_weights(const int *handle, const int *mode, float *theta, int *n, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  const int total = GnnOffsets::make().total;
+  if (*mode == 1) {
+    if (*n != total) throw Failure(HECMW33_ERR_BAD_INPUT, "expected " + std::to_string(total) + " weights");
+    learned_set_weights(S, theta, true);
+  } else {
+    if (theta && *n >= total && S.L.have_weights) {
+      H33_CUDA(cudaMemcpyAsync(theta, S.L.theta.p, sizeof(float) * size_t(total), cudaMemcpyDeviceToHost, S.stream));
+      S.sync();
+    }
+    *n = S.L.have_weights ? total : 0;
+    if (!S.L.have_weights && *mode == 0) *n = total == 0 ? 0 : -total;
+  }
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_learn_eval(const int *handle, const float *theta, const double *R, const double *E,
+                                        double *Z, double *loss, float *grad, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix");
+  if (!(S.pc.valid && S.pc.kind == 1)) throw Failure(HECMW33_ERR_INCONS_PC, "build the SSOR preconditioner first");
+  const int total = GnnOffsets::make().total;
+  ensure_fp32(S);
+  learned_graph(S);
+  learned_train_buffers(S);
+  learned_set_weights(S, theta, false);
+  const size_t n3 = size_t(S.n3());
+  std::vector<float> rf(n3), ef(n3), zf(n3);
+  for (size_t i = 0; i < n3; i++) {
+    rf[i] = float(R[i]);
+    ef[i] = float(E[i]);
+  }
+  DevArray<float> dr, de, dzs;
+  dr.upload(rf, S.stream);
+  de.upload(ef, S.stream);
+  dzs.alloc(n3);
+  const Views<float> V = views(S, 0.0f);
+  launch_sweep<float, false>(S, V, dr.p, dzs.p, nullptr);
+  const double er = dot_device_f(S, de.p, dr.p);
+  learned_edge_weights(S, false);
+  S.L.gacc.zero(S.stream);
+  S.L.losses.alloc(1);
+  learned_pair_grad(S, dr.p, de.p, dzs.p, er, 1.0f, S.L.losses.p);
+  double dq = 0.0;
+  H33_CUDA(cudaMemcpyAsync(&dq, S.L.losses.p, sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+  H33_CUDA(cudaMemcpyAsync(zf.data(), S.L.t_z.p, sizeof(float) * n3, cudaMemcpyDeviceToHost, S.stream));
+  if (grad)
+    H33_CUDA(cudaMemcpyAsync(grad, S.L.gacc.p, sizeof(float) * size_t(total), cudaMemcpyDeviceToHost, S.stream));
+  S.sync();
+  for (size_t i = 0; i < n3; i++) Z[i] = zf[i];
+  if (loss) *loss = dq / er;
+  S.L.weights_version++;
   H33_ENTRY_END
 }
 

@@ -154,15 +154,68 @@ class GpuSolver:
         return self._record(err.value, it, res, times)
 
     def last_solve_info(self):
-        info = np.zeros(8, np.int32)
-        dinfo = np.zeros(8)
+        info = np.zeros(16, np.int32)
+        dinfo = np.zeros(16)
         err = ctypes.c_int(0)
         self.lib.hecmw33_gpu_last_solve_info(ctypes.byref(self.handle), _ip(info), _dp(dinfo), ctypes.byref(err))
         self._check(err.value, fatal_only=False)
         return dict(iter=int(info[0]), kernels=int(info[1]), sweep_groups=int(info[2]),
                     kernels_per_iter=int(info[3]), nz_blocks=int(info[4]), spmv_slices=int(info[5]),
-                    spmv_slots=int(info[6]), t_solve=float(dinfo[0]), t_setup=float(dinfo[1]),
-                    spmv_bytes=float(dinfo[2]), iter_bytes=float(dinfo[3]), device_bytes=float(dinfo[4]))
+                    spmv_slots=int(info[6]), outer=int(info[7]), t_solve=float(dinfo[0]),
+                    t_setup=float(dinfo[1]), spmv_bytes=float(dinfo[2]), iter_bytes=float(dinfo[3]),
+                    device_bytes=float(dinfo[4]), true_resid=float(dinfo[5]), learned=int(info[8]),
+                    fallback=int(info[9]), pairs=int(info[10]))
+
+    # ---- learned preconditioner (hecmw33_gpu_learn_*) -------------------------
+    def learn_record(self, enable=1, max_pairs=0):
+        n, err = ctypes.c_int(0), ctypes.c_int(0)
+        self.lib.hecmw33_gpu_learn_record(ctypes.byref(self.handle), _i(enable), _i(max_pairs), ctypes.byref(n),
+                                          ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+        return n.value
+
+    def learn_train(self, steps=100, lr=1e-3):
+        loss = np.zeros(2)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_learn_train(ctypes.byref(self.handle), _i(steps), ctypes.byref(ctypes.c_double(lr)),
+                                         _dp(loss), ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+        return float(loss[0]), float(loss[1])
+
+    def learn_get_weights(self):
+        n, err = ctypes.c_int(0), ctypes.c_int(0)
+        self.lib.hecmw33_gpu_learn_weights(ctypes.byref(self.handle), _i(0), None, ctypes.byref(n), ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+        if n.value <= 0:
+            return None
+        th = np.zeros(n.value, np.float32)
+        self.lib.hecmw33_gpu_learn_weights(ctypes.byref(self.handle), _i(0),
+                                           th.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(n),
+                                           ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+        return th
+
+    def learn_set_weights(self, theta):
+        th = np.ascontiguousarray(theta, dtype=np.float32)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_learn_weights(ctypes.byref(self.handle), _i(1),
+                                           th.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                           ctypes.byref(ctypes.c_int(th.size)), ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+
+    def learn_eval(self, theta, R, E):
+        th = np.ascontiguousarray(theta, dtype=np.float32)
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        E = np.ascontiguousarray(E, dtype=np.float64)
+        Z = np.zeros_like(R)
+        grad = np.zeros(th.size, np.float32)
+        loss = ctypes.c_double(0)
+        err = ctypes.c_int(0)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self.lib.hecmw33_gpu_learn_eval(ctypes.byref(self.handle), th.ctypes.data_as(fp), _dp(R), _dp(E), _dp(Z),
+                                        ctypes.byref(loss), grad.ctypes.data_as(fp), ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+        return Z, loss.value, grad
 
     def time_spmv(self, reps=20):
         ms = ctypes.c_double(0)

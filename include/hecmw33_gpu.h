@@ -24,6 +24,22 @@
  *   - Host pointers are borrowed for the duration of the call only.  Device buffers
  *     belong to the handle.  One host thread per handle; every call is synchronous.
  *   - One GPU domain: N == NP is required (no halo; hecmw_update_R is a no-op).
+ *   - Options of this library in the SOLVER_OPT block of Iarray/Rarray (41-50,
+ *     hecmw_matrix_misc.F90:137-147), unused by the reference's CG:
+ *       Iarray(42) = 0  FP64 CG (the drop-in, default)
+ *                  = 1  mixed precision, low-precision preconditioner: FP64 CG whose
+ *                       preconditioner sweeps read BF16-stored factors (FP32 diagonal
+ *                       LU) and compute in FP64; matrix, vectors, dots and residuals
+ *                       stay FP64, so the convergence test is the reference's
+ *                  = 2  mixed precision, restarted refinement: inner FP32 CG (FP32
+ *                       matrix and preconditioner copies, FP64 dot products) from zero
+ *                       to Rarray(42) relative (0 -> 1e-4), FP64 correction and true
+ *                       residual
+ *                  = 3  mixed precision, reliable updates: FP32 CG whose solution and
+ *                       residual are folded into FP64 (x64 += x32, r = b - A x in FP64)
+ *                       each time the FP32 residual has fallen by Rarray(42) (0 -> 0.1)
+ *       Rarray(42)      inner tolerance (mode 2) / refinement factor (mode 3)
+ *       Iarray(43) = 1  learned preconditioner after SSOR (see hecmw33_gpu_learn_*)
  *   - *ierr receives 0 or an error code: the reference's codes (1001, 2001, 2002,
  *     3001-3004; hecmw1/src/solver/init/hecmw_solve_error.f90:9-16) or the
  *     HECMW33_ERR_* codes below.  1001 and 2001 are fatal in the reference
@@ -127,16 +143,56 @@ HECMW33_API void hecmw33_gpu_colour_schedule(const int *N, const int *indexL, co
                                              const int *ncolor_in, int *ncolor, int *colorindex,
                                              int *perm, int *ierr);
 
+/* ---- learned preconditioner (no counterpart in the reference) -------------------
+ * Selected by Iarray(43) = 1 (with SSOR, PRECOND 1/2, iterPREmax 1): after the SSOR
+ * sweep, a 3-layer message-passing network over the matrix graph (width 32, BF16
+ * weights, FP32 accumulation) adds a correction; the solve becomes flexible CG
+ * (BETA = z.(r - r_old)/RHO_old).  The network is switched off on the device --
+ * SSOR-CG takes over, restarted -- when RHO <= 0 or when the residual falls by
+ * less than 20 % over 25 iterations.  Works in FP64 (Iarray(42) = 0) and inside
+ * mixed precision (Iarray(42) = 1).  Training data are (r, e) pairs recorded from
+ * earlier FP64 SSOR-CG solves on the same handle (e.g. earlier Newton or load
+ * increments): r_k = b - A x_k and e_k = x* - x_k at iterations 1, 2, 4, 8, ...
+ *
+ * enable: 1 record pairs during the following FP64 solves, 0 stop, -1 forget them;
+ * max_pairs (optional, >0): keep the newest max_pairs pairs; *npairs: pairs held. */
+HECMW33_API void hecmw33_gpu_learn_record(const int *handle, const int *enable, const int *max_pairs,
+                                          int *npairs, int *ierr);
+
+/* Trains the network on the recorded pairs with the handle's GPU kernels (forward,
+ * backward, Adam; FP32 master weights), minimising the mean energy-norm error of the
+ * preconditioned step, (z - e)^T A (z - e) / (e^T r).  loss[0]/loss[1]: mean loss
+ * before the first and after the last of `steps` steps (learning rate lr). */
+HECMW33_API void hecmw33_gpu_learn_train(const int *handle, const int *steps, const double *lr, double *loss,
+                                         int *ierr);
+
+/* mode 0: copy the FP32 weights out (theta may be NULL; *n receives the count, or
+ * minus the count when there are no weights yet); mode 1: load *n weights (the count
+ * must match) and reset the optimiser.  Used to save and restore trained networks. */
+HECMW33_API void hecmw33_gpu_learn_weights(const int *handle, const int *mode, float *theta, int *n, int *ierr);
+
+/* One evaluation of the network for checking: with weights theta (FP32), residual R
+ * and error E (host, 3*NP), returns z = SSOR(R) + network correction (Z), the loss
+ * (z - E)^T A (z - E) / (E^T R) and its gradient with respect to theta (grad, may be
+ * NULL), all in FP32 on the GPU.  Needs the SSOR preconditioner already built. */
+HECMW33_API void hecmw33_gpu_learn_eval(const int *handle, const float *theta, const double *R, const double *E,
+                                        double *Z, double *loss, float *grad, int *ierr);
+
 /* Record of the last solve on this handle, the counterpart of the reference's
  * TIMELOG summary and matvec bandwidth model (hecmw_solver_Iterative.f90:170-254):
  *   info[0] iterations, info[1] kernels launched by the last solve (prologue +
  *   iterations + epilogue), info[2] preconditioner sweep groups (colours or levels,
  *   forward + backward), info[3] kernels per iteration, info[4] NZ (blocks),
- *   info[5] SpMV slices, info[6] padded SpMV slots;
+ *   info[5] SpMV slices, info[6] padded SpMV slots, info[7] outer refinement
+ *   steps (1 for the FP64 solve);
  *   dinfo[0] solve seconds (device events), dinfo[1] setup seconds,
  *   dinfo[2] algorithmic SpMV bytes (reference model: 72 NZ + 4 (NPL+NPU)
- *   + 8 (N+1) + 24 N + 24 NP), dinfo[3] algorithmic bytes of one iteration,
- *   dinfo[4] device bytes held by the handle.  info/dinfo need 8 entries each. */
+ *   + 8 (N+1) + 24 N + 24 NP), dinfo[3] algorithmic bytes of one FP64 iteration,
+ *   dinfo[4] device bytes held by the handle, dinfo[5] final FP64 true relative
+ *   residual ||b - A x|| / ||b||;
+ *   info[8] learned preconditioner used (1/0), info[9] iteration at which its
+ *   SSOR-CG fallback took over (0 = none), info[10] training pairs held.
+ *   info/dinfo need 16 entries each. */
 HECMW33_API void hecmw33_gpu_last_solve_info(const int *handle, int *info, double *dinfo, int *ierr);
 
 /* Times `reps` back-to-back launches of the plain SpMV y = A x on the resident
