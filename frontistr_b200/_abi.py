@@ -24,6 +24,7 @@ SIGNATURES = {
     "hecmw33_gpu_learn_weights": [_i, _i, ctypes.POINTER(ctypes.c_float), _i, _i],
     "hecmw33_gpu_learn_eval": [_i, ctypes.POINTER(ctypes.c_float), _d, _d, _d, _d, ctypes.POINTER(ctypes.c_float),
                                _i],
+    "hecmw33_gpu_rel_resid_noalloc": [_i, _v, _v, _v, _v, _v, _v, _v, _v, _v, _d, _i],
     "hecmw33_gpu_last_error": [ctypes.c_char_p, ctypes.c_int],
 }
 

@@ -201,6 +201,24 @@ HECMW33_API void hecmw33_gpu_last_solve_info(const int *handle, int *info, doubl
 HECMW33_API void hecmw33_gpu_time_spmv(const int *handle, const int *reps, double *ms_per_launch,
                                        int *ierr);
 
+/* No counterpart in the reference.  For callers that cannot allocate GPU memory
+ * (their device memory is owned in full by another allocator, or allocation is
+ * forbidden between their solves): the relative residual ||b - A x|| / ||b|| of
+ * hecmw_rel_resid_L2_33 for a matrix, x and b that the caller already holds in
+ * device memory, in the hecmwST_matrix layout (d_indexL/d_indexU: N+1 ints,
+ * 1-based items, row-major 3x3 blocks, vectors of 3N doubles).  No handle, no
+ * device or pinned allocation: the scratch space is a static 131 kB array in the
+ * library, held by every GPU that loads it.  N is limited to 2,097,152 block rows
+ * (larger N: HECMW33_ERR_BAD_INPUT, nothing runs).  *resid is a host double; the
+ * call returns when it is written.  Calls share the scratch array: calls that
+ * overlap on the GPU race and must be serialised.  The first call on a device looks
+ * up the array's address there; make it before any stream capture. */
+HECMW33_API void hecmw33_gpu_rel_resid_noalloc(const int *N, const int *d_indexL, const int *d_itemL,
+                                               const int *d_indexU, const int *d_itemU,
+                                               const double *d_D, const double *d_AL,
+                                               const double *d_AU, const double *d_X,
+                                               const double *d_B, double *resid, int *ierr);
+
 /* Copies the message of the last error of the calling thread into buf; returns its length. */
 HECMW33_API int hecmw33_gpu_last_error(char *buf, int len);
 
