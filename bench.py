@@ -309,6 +309,9 @@ def main():
         train = {"pairs": npairs, "record_s": t1 - t0, "train_s": t2 - t1, "steps": args.train_steps,
                  "loss_before": loss0, "loss_after": loss1}
 
+    class VariantFailed(Exception):
+        pass
+
     def step(mode, learned=0):
         dX.zero_()
         torch.cuda.synchronize()
@@ -317,7 +320,9 @@ def main():
         iam[42] = learned
         rec = solver.solve_resident_device(dB.data_ptr(), dX.data_ptr(), iam, ra.copy())
         if rec["error"] != 0:
-            raise SystemExit("solve failed: %r" % rec)
+            if mode == 0 and learned == 0:
+                raise SystemExit("solve failed: %r" % rec)
+            raise VariantFailed(rec)
         return rec
 
     variants = {}
@@ -326,14 +331,22 @@ def main():
         modes += [("learned_fp64", 0, 1), ("learned_mixed", 1, 1)]
     clocks = Clocks(uuid)
     sols = {}
+    failed = {}
+    clocks.start()  # sampled over every variant's solves, the headline's among them
     for name, mode, learned in modes:
-        for _ in range(args.warmup):
-            step(mode, learned)
-        barrier()
-        if name == modes[-1][0]:
-            clocks.start()
-        t0 = time.perf_counter()
-        recs = [step(mode, learned) for _ in range(args.steps)]
+        # every rank runs the same steps; a variant that fails (non-FP64 only) is
+        # reported and left out of the headline
+        try:
+            for _ in range(args.warmup):
+                step(mode, learned)
+            barrier()
+            t0 = time.perf_counter()
+            recs = [step(mode, learned) for _ in range(args.steps)]
+        except VariantFailed as exc:
+            barrier()
+            r = exc.args[0]
+            failed[name] = {"error": int(r["error"]), "iter": int(r["iter"]), "resid": float(r["resid"])}
+            continue
         barrier()
         wall = (time.perf_counter() - t0) / args.steps
         info = solver.last_solve_info()
@@ -343,12 +356,13 @@ def main():
                           "true_resid": info["true_resid"], "kernels": info["kernels"],
                           "fallback_iter": info["fallback"]}
     clk = clocks.stop()
-    for name in variants:
+    for name in sols:
         variants[name]["rel_err_vs_fp64"] = float(np.linalg.norm(sols[name] - sols["fp64"]) /
                                                   np.linalg.norm(sols["fp64"]))
     # headline: the fastest variant whose FP64 true residual meets the tolerance
     ok = [k for k, v in variants.items() if v["true_resid"] <= args.tol]
     head = min(ok, key=lambda k: variants[k]["s"]) if ok else "fp64"
+    variants.update({k: {"failed": v} for k, v in failed.items()})
     dev_s = variants[head]["s"]
     wall = variants[head]["wall_s"]
     iters = variants["fp64"]["iterations"]
@@ -409,7 +423,7 @@ def main():
             "metric": METRIC, "value": dev_s, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_s * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if head in ("fp64", "learned_fp64") else "f32+f64",
+            "dtype": "f64" if head in ("fp64", "learned_fp64") else "f64+bf16",
             "data": "synthetic", "config": cfg,
             "variants": variants,
             "training": train,

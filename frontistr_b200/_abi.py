@@ -13,6 +13,8 @@ SIGNATURES = {
     "hecmw33_gpu_solve_resident_device": [_i, _v, _v, _i, _d, _i, _d, _d, _i],
     "hecmw33_gpu_solve": [_i, _i, _i, _i, _i, _i, _i, _i, _i, _d, _d, _d, _d, _d, _i, _d, _i, _d,
                           _d, _i],
+    "hecmw33_gpu_solve_multi": [_i, _i, _d, _d, _i, _d, _i, _d, _i, _d, _d, _i],
+    "hecmw33_gpu_solve_multi_device": [_i, _i, _v, _v, _i, _d, _i, _d, _i, _d, _d, _i],
     "hecmw33_gpu_matvec": [_i, _d, _d, _i],
     "hecmw33_gpu_precond_apply": [_i, _d, _d, _i, _d, _i],
     "hecmw33_gpu_get_colouring": [_i, _i, _i, _i, _i],

@@ -261,8 +261,10 @@ __device__ __forceinline__ float ld_val<float, __nv_bfloat16>(const __nv_bfloat1
 // (SellLayout: block k of a row sits in slot k/K at lane offset k%K): this lane
 // accumulates blocks sub, sub+K, sub+2K, ... of the row in the working precision
 // R (matrix values, vectors and accumulators alike).  BACKWARD walks them in
-// descending order (the reference's backward-sweep order when K == 1).
-template <class R, class TV, int K, bool BACKWARD>
+// descending order (the reference's backward-sweep order when K == 1).  XL2 reads x
+// through L2 (coherent with writes made earlier in the same launch by other CTAs)
+// instead of the read-only path.
+template <class R, class TV, int K, bool BACKWARD, bool XL2 = false>
 __device__ __forceinline__ void row_gemv(const SellView<TV> &A, int s, int lane, int rowlen,
                                          const R *__restrict__ x, R &y0, R &y1, R &y2) {
   const int sub = lane & (K - 1);
@@ -274,7 +276,9 @@ __device__ __forceinline__ void row_gemv(const SellView<TV> &A, int s, int lane,
     const int sl = slot0 + k;
     const int c = __ldg(&A.col[sl * 32 + lane]);
     const TV *v = A.val + sl * 288 + lane;
-    const R x0 = __ldg(&x[3 * c]), x1 = __ldg(&x[3 * c + 1]), x2 = __ldg(&x[3 * c + 2]);
+    const R x0 = XL2 ? __ldcg(&x[3 * c]) : __ldg(&x[3 * c]);
+    const R x1 = XL2 ? __ldcg(&x[3 * c + 1]) : __ldg(&x[3 * c + 1]);
+    const R x2 = XL2 ? __ldcg(&x[3 * c + 2]) : __ldg(&x[3 * c + 2]);
     const R v0 = ld_val<R>(v), v1 = ld_val<R>(v + 32), v2 = ld_val<R>(v + 64);
     const R v3 = ld_val<R>(v + 96), v4 = ld_val<R>(v + 128), v5 = ld_val<R>(v + 160);
     const R v6 = ld_val<R>(v + 192), v7 = ld_val<R>(v + 224), v8 = ld_val<R>(v + 256);
@@ -372,6 +376,32 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<R> A, const R *
   if (MODE == 2) reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[1], [&](double v) { fin_pq(st, v); });
 }
 
+// The 3x3 forward/backward substitution of lu_solve with the nine entries in registers.
+template <class R>
+__device__ __forceinline__ void lu_solve_reg(const R (&a)[9], R &x1, R &x2, R &x3) {
+  x2 = x2 - a[3] * x1;
+  x3 = x3 - a[6] * x1 - a[7] * x2;
+  x3 = a[8] * x3;
+  x2 = a[4] * (x2 - a[5] * x3);
+  x1 = a[0] * (x1 - a[2] * x3 - a[1] * x2);
+}
+
+// The K lanes of a sweep row share the loads of the row's own data: lane `sub` of
+// the row loads ALU entries sub, sub+K, ... and vector entries sub, sub+K, ... of the
+// row's node BEFORE the row's gather (so their latency overlaps it); the row's
+// leader lane collects them with shuffles afterwards.
+template <int K>
+struct RowShare {
+  static constexpr int NA = (9 + K - 1) / K;  // ALU entries per lane
+  static constexpr int NV = (3 + K - 1) / K;  // vector entries per lane
+};
+
+template <int K, class T, int N>
+__device__ __forceinline__ T row_take(const T (&v)[N], int e, int base) {
+  if (K == 1) return v[e];
+  return __shfl_sync(0xffffffffu, v[e / K], base + e % K);
+}
+
 // Forward sweep over the slices [sbeg, send) of one colour / level, each row spread
 // over K lanes:  z(node) = LU^-1 ( r(node) - sum_lower A z(col) )
 // (hecmw_precond_SSOR_33.F90:309-345)
@@ -381,19 +411,40 @@ __global__ void __launch_bounds__(kThreads) sweep_fwd_kernel(SellView<TV> L, con
                                                              const R *__restrict__ r, R *__restrict__ z,
                                                              int sbeg, int send, const CgState *st) {
   if (st && st->done) return;
+  constexpr int NA = RowShare<K>::NA, NV = RowShare<K>::NV;
   const int lane = threadIdx.x & 31;
-  const int roff = lane / K;
+  const int roff = lane / K, sub = lane & (K - 1), base = lane & ~(K - 1);
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
     const bool active = roff < L.nrows[s];
     const int row = L.row0[s] + roff;
     const int len = active ? L.rowlen[s * 32 + roff] : 0;
+    int node = 0;
+    TA ap[NA];
+    R rp[NV];
+#pragma unroll
+    for (int j = 0; j < NA; j++) ap[j] = TA(0);
+#pragma unroll
+    for (int j = 0; j < NV; j++) rp[j] = R(0);
+    if (active) {
+      node = __ldg(&perm[row]);
+#pragma unroll
+      for (int j = 0; j < NA; j++)
+        if (sub + j * K < 9) ap[j] = __ldg(&alu[(sub + j * K) * npos + row]);
+#pragma unroll
+      for (int j = 0; j < NV; j++)
+        if (sub + j * K < 3) rp[j] = r[3 * node + sub + j * K];
+    }
     R a0 = 0, a1 = 0, a2 = 0;
     row_gemv<R, TV, K, false>(L, s, lane, len, z, a0, a1, a2);
-    if (active && (lane & (K - 1)) == 0) {
-      const int node = perm[row];
-      R x1 = r[3 * node] - a0, x2 = r[3 * node + 1] - a1, x3 = r[3 * node + 2] - a2;
-      lu_solve(alu, npos, row, x1, x2, x3);
+    R av[9], rv[3];
+#pragma unroll
+    for (int e = 0; e < 9; e++) av[e] = R(row_take<K>(ap, e, base));
+#pragma unroll
+    for (int c = 0; c < 3; c++) rv[c] = row_take<K>(rp, c, base);
+    if (active && sub == 0) {
+      R x1 = rv[0] - a0, x2 = rv[1] - a1, x3 = rv[2] - a2;
+      lu_solve_reg(av, x1, x2, x3);
       z[3 * node] = x1;
       z[3 * node + 1] = x2;
       z[3 * node + 2] = x3;
@@ -413,26 +464,51 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, con
                                                              double *partials, int part_base,
                                                              int part_total) {
   if (st && st->done) return;
+  constexpr int NA = RowShare<K>::NA, NV = RowShare<K>::NV;
   const int lane = threadIdx.x & 31;
-  const int roff = lane / K;
+  const int roff = lane / K, sub = lane & (K - 1), base = lane & ~(K - 1);
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double dot = 0.0;
   for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
     const bool active = roff < U.nrows[s];
     const int row = U.row0[s] + roff;
     const int len = active ? U.rowlen[s * 32 + roff] : 0;
+    int node = 0;
+    TA ap[NA];
+    R zp[NV], rp[NV];
+#pragma unroll
+    for (int j = 0; j < NA; j++) ap[j] = TA(0);
+#pragma unroll
+    for (int j = 0; j < NV; j++) zp[j] = rp[j] = R(0);
+    if (active) {
+      node = __ldg(&perm[row]);
+#pragma unroll
+      for (int j = 0; j < NA; j++)
+        if (sub + j * K < 9) ap[j] = __ldg(&alu[(sub + j * K) * npos + row]);
+#pragma unroll
+      for (int j = 0; j < NV; j++)
+        if (sub + j * K < 3) {
+          zp[j] = z[3 * node + sub + j * K];  // this row's own entry: written by the forward sweep
+          if (FUSE_RHO) rp[j] = r[3 * node + sub + j * K];
+        }
+    }
     R x1 = 0, x2 = 0, x3 = 0;
     row_gemv<R, TV, K, true>(U, s, lane, len, z, x1, x2, x3);
-    if (active && (lane & (K - 1)) == 0) {
-      const int node = perm[row];
-      lu_solve(alu, npos, row, x1, x2, x3);
-      const R z0 = z[3 * node] - x1, z1 = z[3 * node + 1] - x2, z2 = z[3 * node + 2] - x3;
+    R av[9], zv[3], rv[3];
+#pragma unroll
+    for (int e = 0; e < 9; e++) av[e] = R(row_take<K>(ap, e, base));
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      zv[c] = row_take<K>(zp, c, base);
+      rv[c] = FUSE_RHO ? row_take<K>(rp, c, base) : R(0);
+    }
+    if (active && sub == 0) {
+      lu_solve_reg(av, x1, x2, x3);
+      const R z0 = zv[0] - x1, z1 = zv[1] - x2, z2 = zv[2] - x3;
       z[3 * node] = z0;
       z[3 * node + 1] = z1;
       z[3 * node + 2] = z2;
-      if (FUSE_RHO)
-        dot += double(r[3 * node]) * double(z0) + double(r[3 * node + 1]) * double(z1) +
-               double(r[3 * node + 2]) * double(z2);
+      if (FUSE_RHO) dot += double(rv[0]) * double(z0) + double(rv[1]) * double(z1) + double(rv[2]) * double(z2);
     }
   }
   if (FUSE_RHO)
@@ -593,7 +669,7 @@ __global__ void __launch_bounds__(kThreads) resid_ctl_kernel(SellView<R> A, cons
 // ---- mixed precision with reliable updates --------------------------------
 // Start: r32 = float(r64) (r64 = b - A x64 computed by the FP64 SpMV), x32 = 0,
 // ru_mark = ||r64|| / ||b||; a start already within the tolerance ends the loop.
-__global__ void __launch_bounds__(kThreads) ru_init_kernel(const double *__restrict__ r64, float *__restrict__ r32,
+static __global__ void __launch_bounds__(kThreads) ru_init_kernel(const double *__restrict__ r64, float *__restrict__ r32,
                                                            float *__restrict__ x32, int n3, CgState *st,
                                                            double *partials, cudaGraphConditionalHandle h,
                                                            int use_cond) {
@@ -618,7 +694,7 @@ __global__ void __launch_bounds__(kThreads) ru_init_kernel(const double *__restr
 }
 
 // Reliable update, part 1 (only when pending): x64 += x32, x32 = 0.
-__global__ void __launch_bounds__(kThreads) ru_update_x_kernel(double *__restrict__ x64, float *__restrict__ x32,
+static __global__ void __launch_bounds__(kThreads) ru_update_x_kernel(double *__restrict__ x64, float *__restrict__ x32,
                                                                int n3, const CgState *st) {
   if (st->done || !st->ru_pending) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
@@ -630,7 +706,7 @@ __global__ void __launch_bounds__(kThreads) ru_update_x_kernel(double *__restric
 // Reliable update, part 2 and the end of the iteration: when pending, the FP64 true
 // residual r64 = b - A x64 replaces the FP32 one (r32 = float(r64)) and decides
 // convergence on ||r64|| / ||b||; then the loop control.
-__global__ void __launch_bounds__(kThreads) ru_resid_kernel(SellView<double> A, const double *__restrict__ x64,
+static __global__ void __launch_bounds__(kThreads) ru_resid_kernel(SellView<double> A, const double *__restrict__ x64,
                                                             double *__restrict__ r64, const double *__restrict__ b64,
                                                             float *__restrict__ r32, CgState *st, double *partials,
                                                             cudaGraphConditionalHandle h, int use_cond) {
@@ -706,13 +782,13 @@ __global__ void __launch_bounds__(kThreads) dot_kernel(const R *__restrict__ a, 
 }
 
 // First kernel of every loop body: fail-safe loop condition and body counter.
-__global__ void iter_begin_kernel(CgState *st, cudaGraphConditionalHandle h, int use_cond) {
+static __global__ void iter_begin_kernel(CgState *st, cudaGraphConditionalHandle h, int use_cond) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   st->guard++;
   set_loop(h, use_cond, 0);
 }
 
-__global__ void cg_init_kernel(CgState *st, const CgParams *prm) {
+static __global__ void cg_init_kernel(CgState *st, const CgParams *prm) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   st->rho = st->rho1 = st->alpha = st->beta = st->pq = st->rr = 0.0;
   st->bnrm2 = 0.0;
@@ -756,11 +832,11 @@ __global__ void add_kernel(const R *__restrict__ a, R *__restrict__ b, int n, co
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = b[i] + a[i];
 }
 // b = float(a) (inner right-hand side from the FP64 residual)
-__global__ void narrow_kernel(const double *__restrict__ a, float *__restrict__ b, int n) {
+static __global__ void narrow_kernel(const double *__restrict__ a, float *__restrict__ b, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = float(a[i]);
 }
 // x += double(d) (FP64 correction of the outer refinement)
-__global__ void widen_add_kernel(const float *__restrict__ d, double *__restrict__ x, int n) {
+static __global__ void widen_add_kernel(const float *__restrict__ d, double *__restrict__ x, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     x[i] = x[i] + double(d[i]);
 }
@@ -771,7 +847,7 @@ __global__ void convert_kernel(const double *__restrict__ a, R *__restrict__ b, 
     b[i] = R(a[i]);
 }
 // BF16 copies of stored values (round to nearest even)
-__global__ void convert_bf16_kernel(const double *__restrict__ a, __nv_bfloat16 *__restrict__ b, size_t n) {
+static __global__ void convert_bf16_kernel(const double *__restrict__ a, __nv_bfloat16 *__restrict__ b, size_t n) {
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
     b[i] = __float2bfloat16_rn(float(a[i]));
 }

@@ -1,0 +1,413 @@
+// h33_multi.cuh -- multi-right-hand-side CG: up to 16 load cases on one matrix.
+//
+// Every right-hand side runs its own hecmw_solve_CG recurrence (its own RHO, ALPHA,
+// BETA, breakdown tests, 50-iteration true-residual refresh and convergence), but
+// the matrix and preconditioner values are streamed once per iteration for all of
+// them: the SpMV becomes an SpMM and the SSOR / ILU(0) sweeps solve 16 vectors at
+// once.  A half-warp covers one block row and lane l of it carries right-hand side
+// l, so each 3x3 block is read once (a broadcast to the 16 lanes) and the vector
+// gathers are 128-byte coalesced.
+//
+// Vector layout ("node-major, RHS-minor"): entry c of node i for right-hand side l
+// is v[i*48 + c*16 + l].  Right-hand sides beyond nrhs are padding lanes that start
+// as converged.
+#pragma once
+
+#include "h33_kernels.cuh"
+
+namespace h33 {
+
+constexpr int kMaxRhs = 16;
+constexpr int kRhsStride = 3 * kMaxRhs;  // doubles per node
+
+// Loop control shared by all right-hand sides.
+struct MultiCtl {
+  int all_done;
+  int guard;
+  int nrhs;
+  unsigned int ticket[8];
+};
+
+// Deterministic per-RHS reduction: this CTA's 16 sums go to partials[cta*16 + l];
+// the last CTA to arrive sums the partials of every CTA in a fixed order and runs
+// fin(l, sum) on threads 0..15, then re-arms the ticket.  v is this thread's
+// partial for RHS (threadIdx.x & 15).
+template <class Fin>
+__device__ __forceinline__ void mr_reduce_finish(double v, double *partials, int part, int total,
+                                                 unsigned int *ticket, Fin fin) {
+  __shared__ double sh[kThreads / 16][kMaxRhs];
+  __shared__ int is_last;
+  const int l = threadIdx.x & 15, hw = threadIdx.x >> 4;
+  sh[hw][l] = v;
+  __syncthreads();
+  if (threadIdx.x < kMaxRhs) {
+    double s = 0.0;
+    for (int k = 0; k < kThreads / 16; k++) s += sh[k][threadIdx.x];
+    partials[size_t(part) * kMaxRhs + threadIdx.x] = s;
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int t = atomicAdd(ticket, 1u);
+    is_last = (t == unsigned(total) - 1u);
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  // 16 threads per RHS sum strided subsets, then thread l combines its 16 subsets
+  double s = 0.0;
+  for (int i = hw; i < total; i += kThreads / 16) s += __ldcg(&partials[size_t(i) * kMaxRhs + l]);
+  __syncthreads();
+  sh[hw][l] = s;
+  __syncthreads();
+  if (threadIdx.x < kMaxRhs) {
+    double t = 0.0;
+    for (int k = 0; k < kThreads / 16; k++) t += sh[k][threadIdx.x];
+    fin(int(threadIdx.x), t);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// Sum of A(row, :) x over the blocks of one row of a sliced layout with K lanes per
+// row (block k at slot slot0 + k/K, lane roff*K + k%K), for this lane's RHS.
+template <int K>
+__device__ __forceinline__ void mr_row(const SellView<double> &A, int s, int roff, int len, int l,
+                                       const double *__restrict__ x, double &y0, double &y1, double &y2) {
+  const int slot0 = A.slot0[s];
+#pragma unroll 2
+  for (int k = 0; k < len; k++) {
+    const int sl = slot0 + k / K;
+    const int lp = roff * K + (k & (K - 1));
+    const int c = __ldg(&A.col[sl * 32 + lp]);
+    const double *v = A.val + sl * 288 + lp;
+    const double *xc = x + size_t(c) * kRhsStride + l;
+    const double x0 = xc[0], x1 = xc[16], x2 = xc[32];
+    const double v0 = __ldg(v), v1 = __ldg(v + 32), v2 = __ldg(v + 64);
+    const double v3 = __ldg(v + 96), v4 = __ldg(v + 128), v5 = __ldg(v + 160);
+    const double v6 = __ldg(v + 192), v7 = __ldg(v + 224), v8 = __ldg(v + 256);
+    y0 = fma(v2, x2, fma(v1, x1, fma(v0, x0, y0)));
+    y1 = fma(v5, x2, fma(v4, x1, fma(v3, x0, y1)));
+    y2 = fma(v8, x2, fma(v7, x1, fma(v6, x0, y2)));
+  }
+}
+
+// Half-warp t of a group of slices [sb, se) with 32/K rows per slice -> (slice, row offset).
+template <int K>
+__device__ __forceinline__ bool mr_locate(const SellView<double> &A, int sb, int se, int t, int &s, int &roff) {
+  constexpr int rps = 32 / K;
+  s = sb + t / rps;
+  roff = t % rps;
+  return s < se && roff < A.nrows[s];
+}
+
+// y = A x (MODE 0); y = b - A x (MODE 1); MODE 2: q = A p with the per-RHS {p}{q}
+// and ALPHA; MODE 3: r = b - A x with the per-RHS DNRM2 for the RHS whose true
+// residual is due, then the per-RHS end-of-iteration control (resid_ctl_kernel's
+// logic for every RHS).
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) mr_spmv_kernel(SellView<double> A, const double *__restrict__ x,
+                                                           double *__restrict__ y, const double *__restrict__ b,
+                                                           CgState *st, MultiCtl *ctl, double *partials) {
+  if (MODE >= 2 && ctl->all_done) return;
+  const int l = threadIdx.x & 15;
+  bool mine = true;  // this lane's RHS takes part
+  if (MODE == 2) mine = !st[l].done;
+  if (MODE == 3) {
+    mine = !st[l].done && ((st[l].iter % kIterRecomputeR) == 0 || st[l].recompute);
+    // no true residual due for any RHS: only the end-of-iteration control runs
+    const int any = __syncthreads_or(mine ? 1 : 0);
+    if (!any) {
+      if (blockIdx.x == 0 && threadIdx.x < kMaxRhs) loop_ctl(&st[threadIdx.x], 0, 0);
+      return;
+    }
+  }
+  const int hw0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  const int nrows_total = A.nslices * 32;
+  double dot = 0.0;
+  for (int t = hw0; t < nrows_total; t += nhw) {
+    const int s = t >> 5, roff = t & 31;
+    if (roff >= A.nrows[s]) continue;
+    const int row = A.row0[s] + roff;
+    const int len = A.rowlen[s * 32 + roff];
+    double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+    mr_row<1>(A, s, roff, len, l, x, y0, y1, y2);
+    const size_t o = size_t(row) * kRhsStride + l;
+    if (MODE == 1 || MODE == 3) {
+      y0 = b[o] - y0;
+      y1 = b[o + 16] - y1;
+      y2 = b[o + 32] - y2;
+    }
+    if ((MODE == 2 || MODE == 3) && !mine) continue;  // the other RHS keep their vectors
+    y[o] = y0;
+    y[o + 16] = y1;
+    y[o + 32] = y2;
+    if (MODE == 2) dot += x[o] * y0 + x[o + 16] * y1 + x[o + 32] * y2;
+    if (MODE == 3) dot += y0 * y0 + y1 * y1 + y2 * y2;
+  }
+  if (MODE == 2)
+    mr_reduce_finish(dot, partials, blockIdx.x, gridDim.x, &ctl->ticket[1], [&](int k, double v) {
+      if (!st[k].done) fin_pq(&st[k], v);
+    });
+  if (MODE == 3)
+    mr_reduce_finish(dot, partials, blockIdx.x, gridDim.x, &ctl->ticket[3], [&](int k, double v) {
+      CgState *s = &st[k];
+      const bool need = !s->done && ((s->iter % kIterRecomputeR) == 0 || s->recompute);
+      if (need) {
+        s->rr = v;
+        s->resid = sqrt(v / s->bnrm2);
+        if (s->resid <= s->tol) {
+          s->done = 1;
+          s->converged = 1;
+        }
+      }
+      loop_ctl(s, 0, 0);  // the loop decision over all RHS is mr_ctl_kernel's
+    });
+}
+
+// Forward sweep over the slices [sb, se) of one colour / level, 16 RHS at once.
+template <int K>
+__global__ void __launch_bounds__(kThreads) mr_sweep_fwd_kernel(SellView<double> L, const int *__restrict__ perm,
+                                                                const double *__restrict__ alu, int npos,
+                                                                const double *__restrict__ r, double *__restrict__ z,
+                                                                int sb, int se, const MultiCtl *ctl) {
+  if (ctl && ctl->all_done) return;
+  const int l = threadIdx.x & 15;
+  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  const int total = (se - sb) * (32 / K);
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; t < total; t += nhw) {
+    int s, roff;
+    if (!mr_locate<K>(L, sb, se, t, s, roff)) continue;
+    const int row = L.row0[s] + roff;
+    const int len = L.rowlen[s * 32 + roff];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    mr_row<K>(L, s, roff, len, l, z, a0, a1, a2);
+    const int node = perm[row];
+    const size_t o = size_t(node) * kRhsStride + l;
+    double x1 = r[o] - a0, x2 = r[o + 16] - a1, x3 = r[o + 32] - a2;
+    lu_solve(alu, npos, row, x1, x2, x3);
+    z[o] = x1;
+    z[o + 16] = x2;
+    z[o + 32] = x3;
+  }
+}
+
+// Backward sweep; FUSE_RHO: per-RHS {r}{z} of the finished rows and, in the last
+// launch's last CTA, the RHO finisher of every RHS.
+template <int K, bool FUSE_RHO>
+__global__ void __launch_bounds__(kThreads) mr_sweep_bwd_kernel(SellView<double> U, const int *__restrict__ perm,
+                                                                const double *__restrict__ alu, int npos,
+                                                                const double *__restrict__ r, double *__restrict__ z,
+                                                                int sb, int se, CgState *st, MultiCtl *ctl,
+                                                                double *partials, int part_base, int part_total) {
+  if (ctl && ctl->all_done) return;
+  const int l = threadIdx.x & 15;
+  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  const int total = (se - sb) * (32 / K);
+  double dot = 0.0;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; t < total; t += nhw) {
+    int s, roff;
+    if (!mr_locate<K>(U, sb, se, t, s, roff)) continue;
+    const int row = U.row0[s] + roff;
+    const int len = U.rowlen[s * 32 + roff];
+    double x1 = 0.0, x2 = 0.0, x3 = 0.0;
+    mr_row<K>(U, s, roff, len, l, z, x1, x2, x3);
+    const int node = perm[row];
+    lu_solve(alu, npos, row, x1, x2, x3);
+    const size_t o = size_t(node) * kRhsStride + l;
+    const double z0 = z[o] - x1, z1 = z[o + 16] - x2, z2 = z[o + 32] - x3;
+    z[o] = z0;
+    z[o + 16] = z1;
+    z[o + 32] = z2;
+    if (FUSE_RHO) dot += r[o] * z0 + r[o + 16] * z1 + r[o + 32] * z2;
+  }
+  if (FUSE_RHO)
+    mr_reduce_finish(dot, partials, part_base + blockIdx.x, part_total, &ctl->ticket[0], [&](int k, double v) {
+      if (!st[k].done) fin_rho(&st[k], v);
+    });
+}
+
+// Block-diagonal preconditioner for 16 RHS (optionally with the fused RHO).
+template <bool FUSE_RHO>
+__global__ void __launch_bounds__(kThreads) mr_diag_kernel(const double *__restrict__ alu, int n,
+                                                           const double *__restrict__ r, double *__restrict__ z,
+                                                           CgState *st, MultiCtl *ctl, double *partials) {
+  if (ctl && ctl->all_done) return;
+  const int l = threadIdx.x & 15;
+  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  double dot = 0.0;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < n; i += nhw) {
+    const size_t o = size_t(i) * kRhsStride + l;
+    double x1 = r[o], x2 = r[o + 16], x3 = r[o + 32];
+    lu_solve(alu, n, i, x1, x2, x3);
+    z[o] = x1;
+    z[o + 16] = x2;
+    z[o + 32] = x3;
+    if (FUSE_RHO) dot += r[o] * x1 + r[o + 16] * x2 + r[o + 32] * x3;
+  }
+  if (FUSE_RHO)
+    mr_reduce_finish(dot, partials, blockIdx.x, gridDim.x, &ctl->ticket[0], [&](int k, double v) {
+      if (!st[k].done) fin_rho(&st[k], v);
+    });
+}
+
+// Per-RHS dot over all nodes: WHICH 0 = BNRM2 at the start, 1 = RHO (unfused
+// preconditioner paths), 2 = plain result into rr_true (final true residual).
+template <int WHICH>
+__global__ void __launch_bounds__(kThreads) mr_dot_kernel(const double *__restrict__ a, const double *__restrict__ b,
+                                                          int n, CgState *st, MultiCtl *ctl, double *partials) {
+  if (WHICH == 1 && ctl->all_done) return;
+  const int l = threadIdx.x & 15;
+  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  double dot = 0.0;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < n; i += nhw) {
+    const size_t o = size_t(i) * kRhsStride + l;
+    dot += a[o] * b[o] + a[o + 16] * b[o + 16] + a[o + 32] * b[o + 32];
+  }
+  mr_reduce_finish(dot, partials, blockIdx.x, gridDim.x, &ctl->ticket[4 + WHICH], [&](int k, double v) {
+    CgState *s = &st[k];
+    if (WHICH == 0) {
+      s->bnrm2 = v;
+      if (k >= ctl->nrhs) {
+        s->done = 1;  // padding lane
+      } else if (v == 0.0) {
+        s->zero_rhs = 1;
+        s->done = 1;
+      }
+      if (s->maxit <= 0) s->done = 1;
+    } else if (WHICH == 1) {
+      if (!s->done) fin_rho(s, v);
+    } else {
+      s->rr_true = v;
+    }
+  });
+}
+
+// {p} = {z} or {z} + BETA {p} for the RHS still iterating.
+__global__ void __launch_bounds__(kThreads) mr_update_p_kernel(const double *__restrict__ z, double *__restrict__ p,
+                                                               int n, const CgState *st, const MultiCtl *ctl) {
+  if (ctl->all_done) return;
+  const int l = threadIdx.x & 15;
+  if (st[l].done) return;  // no barrier below: lanes of finished RHS simply leave
+  const bool first = st[l].iter == 1;
+  const double beta = st[l].beta;
+  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < n; i += nhw) {
+    const size_t o = size_t(i) * kRhsStride + l;
+#pragma unroll
+    for (int c = 0; c < 3; c++) p[o + 16 * c] = first ? z[o + 16 * c] : z[o + 16 * c] + beta * p[o + 16 * c];
+  }
+}
+
+// {x} += ALPHA {p}; {r} -= ALPHA {q} with the per-RHS DNRM2 (not on refresh iterations).
+__global__ void __launch_bounds__(kThreads) mr_update_xr_kernel(double *__restrict__ x, const double *__restrict__ p,
+                                                                double *__restrict__ r, const double *__restrict__ q,
+                                                                int n, CgState *st, MultiCtl *ctl, double *partials) {
+  if (ctl->all_done) return;
+  const int l = threadIdx.x & 15;
+  const bool act = !st[l].done;
+  const double alpha = st[l].alpha;
+  const bool refresh = (st[l].iter % kIterRecomputeR) == 0;
+  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  double dot = 0.0;
+  if (act) {
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < n; i += nhw) {
+      const size_t o = size_t(i) * kRhsStride + l;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        x[o + 16 * c] = alpha * p[o + 16 * c] + x[o + 16 * c];
+        if (!refresh) {
+          const double ri = -alpha * q[o + 16 * c] + r[o + 16 * c];
+          r[o + 16 * c] = ri;
+          dot += ri * ri;
+        }
+      }
+    }
+  }
+  mr_reduce_finish(dot, partials, blockIdx.x, gridDim.x, &ctl->ticket[2], [&](int k, double v) {
+    CgState *s = &st[k];
+    if (!s->done && (s->iter % kIterRecomputeR) != 0) fin_rr(s, v);
+  });
+}
+
+__global__ void mr_init_kernel(CgState *st, MultiCtl *ctl, const CgParams *prm, int nrhs) {
+  const int k = threadIdx.x;
+  if (blockIdx.x != 0) return;
+  if (k < kMaxRhs) {
+    CgState *s = &st[k];
+    s->rho = s->rho1 = s->alpha = s->beta = s->pq = s->rr = 0.0;
+    s->bnrm2 = s->resid = s->rr_true = 0.0;
+    s->tol = prm->tol;
+    s->maxit = prm->maxit;
+    s->iter = 1;
+    s->done = s->error = s->n_indef = s->recompute = s->converged = s->zero_rhs = 0;
+    s->guard = 0;
+    s->inner = 0;
+    s->flexible = s->use_gnn = s->restart = s->fallback = 0;
+    s->resid_mark = 1.0;
+    s->gamma = 1.0f;
+    s->reliable = s->ru_pending = s->ru_count = 0;
+    s->ru_delta = 0.0;
+    s->ru_mark = 1.0;
+    for (int i = 0; i < 8; i++) s->ticket[i] = 0u;
+  }
+  if (k == 0) {
+    ctl->all_done = 0;
+    ctl->guard = 0;
+    ctl->nrhs = nrhs;
+    for (int i = 0; i < 8; i++) ctl->ticket[i] = 0u;
+  }
+}
+
+// Start of a loop body: body counter of every RHS still iterating, fail-safe condition.
+__global__ void mr_iter_begin_kernel(CgState *st, MultiCtl *ctl, cudaGraphConditionalHandle h, int use_cond) {
+  if (blockIdx.x != 0) return;
+  const int k = threadIdx.x;
+  if (k < kMaxRhs && !st[k].done) st[k].guard++;
+  if (k == 0) {
+    ctl->guard++;
+    set_loop(h, use_cond, 0);
+  }
+}
+
+// Loop decision after the control of every RHS: continue while one still iterates
+// (and the body count stays within the fail-safe bound).
+__global__ void mr_ctl_kernel(const CgState *st, MultiCtl *ctl, cudaGraphConditionalHandle h, int use_cond) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int any = 0, maxit = 0;
+  for (int k = 0; k < kMaxRhs; k++) {
+    any |= !st[k].done;
+    maxit = max(maxit, st[k].maxit);
+  }
+  if (ctl->guard > maxit + 1) any = 0;
+  ctl->all_done = !any;
+  set_loop(h, use_cond, any);
+}
+
+// Column-major host layout (n3 x nrhs) <-> node-major RHS-minor layout.
+__global__ void mr_pack_kernel(const double *__restrict__ src, double *__restrict__ dst, int n, int nrhs) {
+  const size_t total = size_t(n) * kRhsStride;
+  for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
+    const int l = int(t % kMaxRhs);
+    const int c = int((t / kMaxRhs) % 3);
+    const size_t i = t / kRhsStride;
+    dst[t] = l < nrhs ? src[size_t(l) * 3 * n + 3 * i + c] : 0.0;
+  }
+}
+__global__ void mr_unpack_kernel(const double *__restrict__ src, double *__restrict__ dst, int n, int nrhs) {
+  const size_t total = size_t(n) * 3 * nrhs;
+  for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
+    const int l = int(t / (3 * size_t(n)));
+    const size_t j = t % (3 * size_t(n));
+    dst[t] = src[(j / 3) * kRhsStride + (j % 3) * kMaxRhs + l];
+  }
+}
+// Zero-RHS lanes leave x = 0 (hecmw_solver.f90:32-37).
+__global__ void mr_zero_x_kernel(double *__restrict__ x, int n, const CgState *st) {
+  const size_t total = size_t(n) * kRhsStride;
+  for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x)
+    if (st[t % kMaxRhs].zero_rhs) x[t] = 0.0;
+}
+
+}  // namespace h33

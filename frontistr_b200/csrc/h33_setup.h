@@ -3,9 +3,16 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 namespace h33 {
+
+// Checks an hecmwST profile for one GPU domain (N == NP, indexX[0..N] consistent with
+// NPL/NPU, itemL ascending ids below the row, itemU ascending ids above it, 1-based).
+// Returns "" or the first problem found.
+std::string check_profile(int N, int NP, int NPL, int NPU, const int *indexL, const int *itemL,
+                          const int *indexU, const int *itemU);
 
 // Borrowed hecmwST_matrix profile (indexX[0..N], itemX 1-based ids).
 struct Profile {

@@ -30,6 +30,7 @@
 #include "h33_common.cuh"
 #include "h33_gnn.cuh"
 #include "h33_kernels.cuh"
+#include "h33_multi.cuh"
 #include "h33_setup.h"
 
 namespace h33 {
@@ -204,6 +205,14 @@ struct Solver {
   double bnrm2 = 0.0;
   // graphs (FP64 drop-in, FP32 inner solve)
   GraphSlot g64, g32;
+  // multi-RHS CG: node-major RHS-minor vectors (48 doubles per node), per-RHS states
+  DevArray<double> mb, mx, mr, mz, mp, mq, mw, mzp, mpart;
+  DevArray<CgState> mst;
+  DevArray<MultiCtl> mctl;
+  CgState *h_mst = nullptr;
+  MultiCtl *h_mctl = nullptr;
+  GraphSlot gm;
+  int occ_mr = 4;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int build_counter = 0;  // monotonic id of preconditioner builds (graph cache key)
   // last-solve record
@@ -217,11 +226,15 @@ struct Solver {
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_spmv, spmv_kernel<double, 2>, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep, sweep_bwd_kernel<double, double, double, 8, true>, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_vec, update_xr_kernel<double>, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mr, mr_sweep_bwd_kernel<8, true>, kThreads, 0));
     occ_spmv = std::max(occ_spmv, 1);
     occ_sweep = std::max(occ_sweep, 1);
     occ_vec = std::max(occ_vec, 1);
+    occ_mr = std::max(occ_mr, 1);
     H33_CUDA(cudaMallocHost(&h_params, sizeof(CgParams)));
     H33_CUDA(cudaMallocHost(&h_state, sizeof(CgState)));
+    H33_CUDA(cudaMallocHost(&h_mst, sizeof(CgState) * kMaxRhs));
+    H33_CUDA(cudaMallocHost(&h_mctl, sizeof(MultiCtl)));
     state.alloc(1);
     params.alloc(1);
     d_err.alloc(1);
@@ -234,6 +247,8 @@ struct Solver {
     if (ev1) cudaEventDestroy(ev1);
     if (h_params) cudaFreeHost(h_params);
     if (h_state) cudaFreeHost(h_state);
+    if (h_mst) cudaFreeHost(h_mst);
+    if (h_mctl) cudaFreeHost(h_mctl);
     if (stream) {
       cudaStreamSynchronize(stream);
       cudaStreamDestroy(stream);
@@ -242,6 +257,7 @@ struct Solver {
   void drop_graph() {
     g64.drop();
     g32.drop();
+    gm.drop();
   }
   int n3() const { return 3 * N; }
   int grid_vec() const { return std::max(1, std::min((n3() + kThreads - 1) / kThreads, nsm * occ_vec)); }
@@ -253,6 +269,8 @@ struct Solver {
     const int need = (nslices + kWarpsPerCta - 1) / kWarpsPerCta;
     return std::max(1, std::min(need, nsm * occ_sweep));
   }
+  // multi-RHS kernels: one half-warp per block row
+  int grid_mr(int rows) const { return std::max(1, std::min((rows + 15) / 16, nsm * occ_mr)); }
   void sync() { H33_CUDA(cudaStreamSynchronize(stream)); }
 };
 
@@ -286,28 +304,8 @@ struct DeviceGuard {
 // Matrix upload
 void validate(int N, int NP, int NPL, int NPU, const int *indexL, const int *itemL,
               const int *indexU, const int *itemU) {
-  if (N <= 0) throw Failure(HECMW33_ERR_BAD_INPUT, "N must be positive");
-  if (NP != N) throw Failure(HECMW33_ERR_BAD_INPUT, "NP != N: one GPU domain has no halo nodes");
-  if (!indexL || !indexU || (NPL > 0 && !itemL) || (NPU > 0 && !itemU))
-    throw Failure(HECMW33_ERR_BAD_INPUT, "null profile array");
-  if (indexL[0] != 0 || indexU[0] != 0 || indexL[N] != NPL || indexU[N] != NPU)
-    throw Failure(HECMW33_ERR_BAD_INPUT, "indexL/indexU inconsistent with NPL/NPU");
-  for (int i = 0; i < N; i++) {
-    if (indexL[i + 1] < indexL[i] || indexU[i + 1] < indexU[i])
-      throw Failure(HECMW33_ERR_BAD_INPUT, "index arrays must be non-decreasing");
-    int prev = 0;
-    for (int j = indexL[i]; j < indexL[i + 1]; j++) {
-      const int c = itemL[j];
-      if (c <= prev || c >= i + 1) throw Failure(HECMW33_ERR_BAD_INPUT, "itemL must be ascending ids < row");
-      prev = c;
-    }
-    prev = i + 1;
-    for (int j = indexU[i]; j < indexU[i + 1]; j++) {
-      const int c = itemU[j];
-      if (c <= prev || c > N) throw Failure(HECMW33_ERR_BAD_INPUT, "itemU must be ascending ids in (row, N]");
-      prev = c;
-    }
-  }
+  const std::string msg = check_profile(N, NP, NPL, NPU, indexL, itemL, indexU, itemU);
+  if (!msg.empty()) throw Failure(HECMW33_ERR_BAD_INPUT, msg);
 }
 
 void set_matrix(Solver &S, int N, int NP, int NPL, int NPU, const int *indexL, const int *itemL,
@@ -1473,6 +1471,285 @@ int solve_mixed_reliable(Solver &S, int *Iarray, double *Rarray, int *iter, doub
   return error;
 }
 
+// ---------------------------------------------------------------------------
+// Multi-RHS CG: up to kMaxRhs load cases per pass over the matrix (h33_multi.cuh).
+
+template <int K, bool FUSE_RHO>
+void launch_mr_sweep_k(Solver &S, const double *rin, double *zout) {
+  Precond &P = S.pc;
+  cudaStream_t s = S.stream;
+  const int *perm_b = P.alu_shared ? P.perm_fwd.p : P.perm_bwd.p;
+  const double *alu_b = P.alu_shared ? P.alu_fwd.p : P.alu_bwd.p;
+  MultiCtl *ctl = S.mctl.p;
+  const SellView<double> lo = P.lo.view(), up = P.up.view();
+  const int gf = int(P.lo.group_slice.size()) - 1;
+  for (int g = 0; g < gf; g++) {
+    const int sb = P.lo.group_slice[g], se = P.lo.group_slice[g + 1];
+    if (se <= sb) continue;
+    mr_sweep_fwd_kernel<K><<<S.grid_mr((se - sb) * (32 / K)), kThreads, 0, s>>>(lo, P.perm_fwd.p, P.alu_fwd.p, S.N,
+                                                                             rin, zout, sb, se, ctl);
+  }
+  const int gb = int(P.up.group_slice.size()) - 1;
+  int total = 0;
+  for (int g = gb - 1; g >= 0; g--) {
+    const int sb = P.up.group_slice[g], se = P.up.group_slice[g + 1];
+    total += S.grid_mr(std::max(se - sb, 1) * (32 / K));
+  }
+  int base = 0;
+  for (int g = gb - 1; g >= 0; g--) {
+    const int sb = P.up.group_slice[g], se = P.up.group_slice[g + 1];
+    const int grid = S.grid_mr(std::max(se - sb, 1) * (32 / K));
+    mr_sweep_bwd_kernel<K, FUSE_RHO><<<grid, kThreads, 0, s>>>(up, perm_b, alu_b, S.N, rin, zout, sb, se,
+                                                                S.mst.p, ctl, S.mpart.p, base, total);
+    base += grid;
+  }
+}
+
+template <bool FUSE_RHO>
+void launch_mr_sweep(Solver &S, const double *rin, double *zout) {
+  Precond &P = S.pc;
+  if (P.kind == 3) {
+    mr_diag_kernel<FUSE_RHO><<<S.grid_mr(S.N), kThreads, 0, S.stream>>>(P.alu_fwd.p, S.N, rin, zout, S.mst.p,
+                                                                         S.mctl.p, S.mpart.p);
+    return;
+  }
+  switch (P.lo.lanes) {
+    case 1: return launch_mr_sweep_k<1, FUSE_RHO>(S, rin, zout);
+    case 2: return launch_mr_sweep_k<2, FUSE_RHO>(S, rin, zout);
+    case 4: return launch_mr_sweep_k<4, FUSE_RHO>(S, rin, zout);
+    case 16: return launch_mr_sweep_k<16, FUSE_RHO>(S, rin, zout);
+    case 32: return launch_mr_sweep_k<32, FUSE_RHO>(S, rin, zout);
+    default: return launch_mr_sweep_k<8, FUSE_RHO>(S, rin, zout);
+  }
+}
+
+// Largest number of CTAs one reduction of the multi-RHS loop uses.
+int mr_max_parts(Solver &S) {
+  Precond &P = S.pc;
+  int m = std::max(S.grid_mr(S.A.nslices * 32), S.grid_mr(S.N));
+  if (P.valid && P.kind != 3) {
+    const int K = P.lo.lanes;
+    int total = 0;
+    const int gb = int(P.up.group_slice.size()) - 1;
+    for (int g = 0; g < gb; g++)
+      total += S.grid_mr(std::max(P.up.group_slice[g + 1] - P.up.group_slice[g], 1) * (32 / K));
+    m = std::max(m, total);
+  }
+  return m;
+}
+
+// hecmw_precond_apply for 16 RHS (iterPREmax passes; RHO fused when iterPREmax == 1).
+void launch_mr_precond(Solver &S, int iterpremax) {
+  cudaStream_t s = S.stream;
+  const int n48 = S.N * kRhsStride;
+  const int gv = std::max(1, std::min((n48 + kThreads - 1) / kThreads, S.nsm * S.occ_vec));
+  if (iterpremax <= 0) {
+    copy_kernel<double><<<gv, kThreads, 0, s>>>(S.mr.p, S.mz.p, n48, nullptr);
+    mr_dot_kernel<1><<<S.grid_mr(S.N), kThreads, 0, s>>>(S.mr.p, S.mz.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
+    return;
+  }
+  if (iterpremax == 1) {
+    launch_mr_sweep<true>(S, S.mr.p, S.mz.p);
+    return;
+  }
+  const double *in = S.mr.p;
+  for (int it = 1; it <= iterpremax; it++) {
+    launch_mr_sweep<false>(S, in, S.mzp.p);
+    if (it == 1) copy_kernel<double><<<gv, kThreads, 0, s>>>(S.mzp.p, S.mz.p, n48, nullptr);
+    else add_kernel<double><<<gv, kThreads, 0, s>>>(S.mzp.p, S.mz.p, n48, nullptr);
+    if (it == iterpremax) break;
+    mr_spmv_kernel<1><<<S.grid_mr(S.A.nslices * 32), kThreads, 0, s>>>(S.A.view(), S.mz.p, S.mw.p, S.mr.p, S.mst.p,
+                                                                       S.mctl.p, S.mpart.p);
+    in = S.mw.p;
+  }
+  mr_dot_kernel<1><<<S.grid_mr(S.N), kThreads, 0, s>>>(S.mr.p, S.mz.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
+}
+
+void launch_mr_prologue(Solver &S, int nrhs, cudaGraphConditionalHandle h, int use_cond) {
+  cudaStream_t s = S.stream;
+  const int gs = S.grid_mr(S.A.nslices * 32);
+  mr_init_kernel<<<1, 32, 0, s>>>(S.mst.p, S.mctl.p, S.params.p, nrhs);
+  mr_spmv_kernel<1><<<gs, kThreads, 0, s>>>(S.A.view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p, S.mpart.p);
+  mr_dot_kernel<0><<<S.grid_mr(S.N), kThreads, 0, s>>>(S.mb.p, S.mb.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
+  mr_ctl_kernel<<<1, 32, 0, s>>>(S.mst.p, S.mctl.p, h, use_cond);
+}
+
+void launch_mr_iteration(Solver &S, int iterpremax, cudaGraphConditionalHandle h, int use_cond) {
+  cudaStream_t s = S.stream;
+  const int gs = S.grid_mr(S.A.nslices * 32), gn = S.grid_mr(S.N);
+  mr_iter_begin_kernel<<<1, 32, 0, s>>>(S.mst.p, S.mctl.p, h, use_cond);
+  launch_mr_precond(S, iterpremax);
+  mr_update_p_kernel<<<gn, kThreads, 0, s>>>(S.mz.p, S.mp.p, S.N, S.mst.p, S.mctl.p);
+  mr_spmv_kernel<2><<<gs, kThreads, 0, s>>>(S.A.view(), S.mp.p, S.mq.p, nullptr, S.mst.p, S.mctl.p, S.mpart.p);
+  mr_update_xr_kernel<<<gn, kThreads, 0, s>>>(S.mx.p, S.mp.p, S.mr.p, S.mq.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
+  mr_spmv_kernel<3><<<gs, kThreads, 0, s>>>(S.A.view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p, S.mpart.p);
+  mr_ctl_kernel<<<1, 32, 0, s>>>(S.mst.p, S.mctl.p, h, use_cond);
+}
+
+// Graph of the whole multi-RHS loop (prologue + WHILE node), as build_graph.
+void build_graph_multi(Solver &S, int iterpremax, int nrhs) {
+  GraphSlot &G = S.gm;
+  const int key[5] = {S.generation, S.pc.generation, S.pc.kind, iterpremax, nrhs};
+  if (G.exec && std::equal(key, key + 5, G.key)) return;
+  G.drop();
+  cudaGraph_t g = nullptr;
+  H33_CUDA(cudaGraphCreate(&g, 0));
+  G.graph = g;
+  cudaGraphConditionalHandle h;
+  H33_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+  H33_CUDA(cudaStreamBeginCaptureToGraph(S.stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  launch_mr_prologue(S, nrhs, h, 1);
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  H33_CUDA(cudaStreamGetCaptureInfo(S.stream, &cs, nullptr, nullptr, &deps, &ndeps));
+  std::vector<cudaGraphNode_t> dep(deps, deps + ndeps);
+  cudaGraph_t g2 = nullptr;
+  H33_CUDA(cudaStreamEndCapture(S.stream, &g2));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  H33_CUDA(cudaGraphAddNode(&cnode, g, dep.data(), dep.size(), &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  H33_CUDA(cudaStreamBeginCaptureToGraph(S.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  launch_mr_iteration(S, iterpremax, h, 1);
+  cudaGraph_t b2 = nullptr;
+  H33_CUDA(cudaStreamEndCapture(S.stream, &b2));
+  H33_CUDA(cudaGraphInstantiate(&G.exec, g, 0));
+  std::copy(key, key + 5, G.key);
+  size_t nbody = 0, nall = 0;
+  H33_CUDA(cudaGraphGetNodes(body, nullptr, &nbody));
+  H33_CUDA(cudaGraphGetNodes(g, nullptr, &nall));
+  G.kernels_per_iter = int(nbody);
+  G.prologue_kernels = int(nall) - 1;
+}
+
+void ensure_multi_buffers(Solver &S) {
+  const size_t n48 = size_t(S.N) * kRhsStride;
+  for (auto *v : {&S.mb, &S.mx, &S.mr, &S.mz, &S.mp, &S.mq, &S.mw, &S.mzp}) v->alloc(n48);
+  S.mst.alloc(kMaxRhs);
+  S.mctl.alloc(1);
+  S.mpart.alloc(size_t(mr_max_parts(S)) * kMaxRhs + 1024);
+}
+
+// Solves nrhs <= kMaxRhs systems A X(:, k) = B(:, k); dB and dX are device arrays in
+// the column-major hecmwST layout (3N x nrhs).  Per-RHS results in iter/resid/error/
+// true_resid; returns the device time in ms and counts the kernels launched.
+float run_multi_chunk(Solver &S, int nrhs, const double *dB, double *dX, int iterpremax, double tol, int maxit,
+                      int *iter, double *resid, int *error, double *true_resid, int *kernels) {
+  cudaStream_t s = S.stream;
+  const int n = S.N;
+  const size_t n48 = size_t(n) * kRhsStride;
+  const int gp = std::max(1, std::min(int((n48 + kThreads - 1) / kThreads), S.nsm * S.occ_vec));
+  mr_pack_kernel<<<gp, kThreads, 0, s>>>(dB, S.mb.p, n, nrhs);
+  mr_pack_kernel<<<gp, kThreads, 0, s>>>(dX, S.mx.p, n, nrhs);
+  S.h_params->tol = tol;
+  S.h_params->maxit = maxit;
+  S.h_params->iterpremax = iterpremax;
+  S.h_params->inner = 0;
+  S.h_params->flexible = 0;
+  S.h_params->use_gnn = 0;
+  S.h_params->reliable = 0;
+  S.h_params->ru_delta = 0.0;
+  H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, s));
+  H33_CUDA(cudaEventRecord(S.ev0, s));
+  if (graph_mode()) {
+    build_graph_multi(S, iterpremax, nrhs);
+    H33_CUDA(cudaGraphLaunch(S.gm.exec, s));
+  } else {
+    launch_mr_prologue(S, nrhs, 0, 0);
+    for (int it = 0; it <= maxit + kStreamChunk; it += kStreamChunk) {
+      for (int k = 0; k < kStreamChunk; k++) launch_mr_iteration(S, iterpremax, 0, 0);
+      H33_CUDA(cudaGetLastError());
+      H33_CUDA(cudaMemcpyAsync(S.h_mctl, S.mctl.p, sizeof(MultiCtl), cudaMemcpyDeviceToHost, s));
+      S.sync();
+      if (S.h_mctl->all_done) break;
+    }
+  }
+  H33_CUDA(cudaEventRecord(S.ev1, s));
+  // final true residuals (hecmw_rel_resid_L2_33 per RHS) and the zero-RHS lanes
+  mr_spmv_kernel<1><<<S.grid_mr(S.A.nslices * 32), kThreads, 0, s>>>(S.A.view(), S.mx.p, S.mw.p, S.mb.p, S.mst.p,
+                                                                     S.mctl.p, S.mpart.p);
+  mr_dot_kernel<2><<<S.grid_mr(n), kThreads, 0, s>>>(S.mw.p, S.mw.p, n, S.mst.p, S.mctl.p, S.mpart.p);
+  mr_zero_x_kernel<<<gp, kThreads, 0, s>>>(S.mx.p, n, S.mst.p);
+  mr_unpack_kernel<<<gp, kThreads, 0, s>>>(S.mx.p, dX, n, nrhs);
+  H33_CUDA(cudaGetLastError());
+  H33_CUDA(cudaMemcpyAsync(S.h_mst, S.mst.p, sizeof(CgState) * kMaxRhs, cudaMemcpyDeviceToHost, s));
+  H33_CUDA(cudaMemcpyAsync(S.h_mctl, S.mctl.p, sizeof(MultiCtl), cudaMemcpyDeviceToHost, s));
+  S.sync();
+  float ms = 0.0f;
+  H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+  if (!S.h_mctl->all_done) throw Failure(HECMW33_ERR_TIMEOUT, "multi-RHS loop ended without a decision");
+  for (int k = 0; k < nrhs; k++) {
+    const CgState &st = S.h_mst[k];
+    iter[k] = st.zero_rhs ? 0 : st.iter;
+    resid[k] = st.zero_rhs ? 0.0 : st.resid;
+    error[k] = st.zero_rhs ? HECMW33_ERR_ZERO_RHS : st.error;
+    true_resid[k] = st.bnrm2 > 0.0 ? std::sqrt(st.rr_true / st.bnrm2) : 0.0;
+  }
+  if (kernels) {
+    const int body = S.h_mctl->guard;
+    *kernels += (graph_mode() ? S.gm.prologue_kernels + body * S.gm.kernels_per_iter : 0) + 6;
+  }
+  return ms;
+}
+
+// hecmw_solve for nrhs load cases on the resident matrix: the checks and the
+// preconditioner setup of hecmw_solve_iterative once, then the RHS in chunks of
+// kMaxRhs.  Returns the first non-zero per-RHS code other than 2002 (or 0).
+int solve_multi(Solver &S, int nrhs, const double *dB, double *dX, int *Iarray, double *Rarray, int *iter,
+                double *resid, int *error, double *true_resid, double *times) {
+  if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_set_matrix first");
+  if (nrhs < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "nrhs must be positive");
+  const double t0 = wall();
+  if (times) times[0] = times[1] = times[2] = 0.0;
+  const int METHOD = Iarray[1], PRECOND = Iarray[2], iterPREmax = Iarray[4], MAXIT = Iarray[0];
+  const double TOL = Rarray[0];
+  double sigma = Rarray[1];
+  if (sigma < 0.0) sigma = 1.0;
+  if (S.zero_diag && PRECOND < 10 && iterPREmax > 0) return HECMW33_ERR_ZERO_DIAG;
+  if (METHOD != 1)
+    throw Failure(HECMW33_ERR_INCONS_PC, "METHOD " + std::to_string(METHOD) + ": the GPU drop-in implements CG (1)");
+  recycle_precond_setting(Iarray);
+  if (iterPREmax > 0) precond_setup(S, PRECOND, Iarray[33], sigma, Iarray);
+  ensure_multi_buffers(S);
+  const double t1 = wall();
+  Range rs("hecmw33_solve_multi");
+  float ms = 0.0f;
+  int kernels = 0, rc = 0, conv = 1, div = 0;
+  const size_t n3 = size_t(S.n3());
+  for (int k0 = 0; k0 < nrhs; k0 += kMaxRhs) {
+    const int m = std::min(kMaxRhs, nrhs - k0);
+    ms += run_multi_chunk(S, m, dB + n3 * k0, dX + n3 * k0, iterPREmax, TOL, MAXIT, iter + k0, resid + k0,
+                          error + k0, true_resid + k0, &kernels);
+    for (int k = k0; k < k0 + m; k++) {
+      if (!rc && error[k] != 0 && error[k] != HECMW33_ERR_ZERO_RHS) rc = error[k];
+      if (!(error[k] == HECMW33_ERR_ZERO_RHS || true_resid[k] < TOL)) conv = 0;
+      if (error[k] == HECMW33_ERR_DIVERGE_PC || error[k] == HECMW33_ERR_DIVERGE_MAT ||
+          error[k] == HECMW33_ERR_DIVERGE_NAN)
+        div = 1;
+    }
+  }
+  Iarray[80] = conv;
+  Iarray[81] = div;
+  S.last_iter = *std::max_element(iter, iter + nrhs);
+  S.last_outer = (nrhs + kMaxRhs - 1) / kMaxRhs;
+  S.last_kernels = kernels;
+  S.last_solve_s = ms * 1e-3;
+  S.last_setup_s = t1 - t0;
+  S.last_true_resid = *std::max_element(true_resid, true_resid + nrhs);
+  S.last_learned = 0;
+  S.last_fallback = 0;
+  if (times) {
+    times[0] = t1 - t0;
+    times[1] = ms * 1e-3;
+  }
+  return rc;
+}
+
 int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
   switch (Iarray[41]) {
     case 1: return solve_fp64(S, Iarray, Rarray, iter, resid, times, 1);
@@ -1610,6 +1887,43 @@ HECMW33_API void hecmw33_gpu_solve(const int *handle, const int *N, const int *N
   H33_CUDA(cudaMemcpyAsync(X, S.x.p, bytes, cudaMemcpyDeviceToHost, S.stream));
   S.sync();
   if (times) times[0] += tm;
+  if (ierr) *ierr = rc;
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_solve_multi(const int *handle, const int *nrhs, const double *B, double *X,
+                                         int *Iarray, double *Rarray, int *iter, double *resid, int *error,
+                                         double *true_resid, double *times, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_set_matrix first");
+  if (!nrhs || *nrhs < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "nrhs must be positive");
+  const size_t total = size_t(S.n3()) * size_t(*nrhs);
+  DevArray<double> dB, dX;
+  dB.upload(B, total, S.stream);
+  dX.upload(X, total, S.stream);
+  std::vector<double> tr(static_cast<size_t>(*nrhs));
+  const int rc = solve_multi(S, *nrhs, dB.p, dX.p, Iarray, Rarray, iter, resid, error, tr.data(), times);
+  H33_CUDA(cudaMemcpyAsync(X, dX.p, sizeof(double) * total, cudaMemcpyDeviceToHost, S.stream));
+  S.sync();
+  if (true_resid) std::copy(tr.begin(), tr.end(), true_resid);
+  if (ierr) *ierr = rc;
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_solve_multi_device(const int *handle, const int *nrhs, const double *dB, double *dX,
+                                                int *Iarray, double *Rarray, int *iter, double *resid, int *error,
+                                                double *true_resid, double *times, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  if (!nrhs || *nrhs < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "nrhs must be positive");
+  std::vector<double> tr(static_cast<size_t>(*nrhs));
+  const int rc = solve_multi(S, *nrhs, dB, dX, Iarray, Rarray, iter, resid, error, tr.data(), times);
+  if (true_resid) std::copy(tr.begin(), tr.end(), true_resid);
   if (ierr) *ierr = rc;
   H33_ENTRY_END
 }

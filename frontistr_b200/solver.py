@@ -153,6 +153,43 @@ class GpuSolver:
         self._check(err.value)
         return self._record(err.value, it, res, times)
 
+    def solve_multi(self, B, X, Iarray, Rarray):
+        """Several load cases on the resident matrix (hecmw33_gpu_solve_multi).
+
+        B, X: host arrays of shape (nrhs, 3N) (row k = load case k, i.e. the
+        column-major 3N x nrhs layout of the C call); X is updated in place.
+        Returns per-case iter, resid, error and true_resid arrays and the times."""
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        assert X.flags.c_contiguous and X.dtype == np.float64 and X.shape == B.shape
+        nrhs = B.shape[0]
+        it = np.zeros(nrhs, np.int32)
+        res = np.zeros(nrhs)
+        errs = np.zeros(nrhs, np.int32)
+        tres = np.zeros(nrhs)
+        times = np.zeros(3)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_solve_multi(ctypes.byref(self.handle), _i(nrhs), _dp(B), _dp(X), _ip(Iarray),
+                                         _dp(Rarray), _ip(it), _dp(res), _ip(errs), _dp(tres), _dp(times),
+                                         ctypes.byref(err))
+        self._check(err.value)
+        return dict(error=int(err.value), iter=it, resid=res, errors=errs, true_resid=tres,
+                    t_setup=float(times[0]), t_solve=float(times[1]))
+
+    def solve_multi_device(self, nrhs, dB_ptr, dX_ptr, Iarray, Rarray):
+        """As solve_multi with B and X in device memory (3N x nrhs column-major)."""
+        it = np.zeros(nrhs, np.int32)
+        res = np.zeros(nrhs)
+        errs = np.zeros(nrhs, np.int32)
+        tres = np.zeros(nrhs)
+        times = np.zeros(3)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_solve_multi_device(ctypes.byref(self.handle), _i(nrhs), ctypes.c_void_p(dB_ptr),
+                                                ctypes.c_void_p(dX_ptr), _ip(Iarray), _dp(Rarray), _ip(it),
+                                                _dp(res), _ip(errs), _dp(tres), _dp(times), ctypes.byref(err))
+        self._check(err.value)
+        return dict(error=int(err.value), iter=it, resid=res, errors=errs, true_resid=tres,
+                    t_setup=float(times[0]), t_solve=float(times[1]))
+
     def last_solve_info(self):
         info = np.zeros(16, np.int32)
         dinfo = np.zeros(16)

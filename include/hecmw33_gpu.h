@@ -119,6 +119,31 @@ HECMW33_API void hecmw33_gpu_solve(const int *handle, const int *N, const int *N
                                    const double *B, double *X, int *Iarray, double *Rarray,
                                    int *iter, double *resid, double *times, int *ierr);
 
+/* Several load cases on the resident matrix: hecmw_solve once per column of B
+ * (hecmw_solver.f90:9-88 per right-hand side), with the checks, the recycle policy and
+ * the preconditioner setup done once.  Every right-hand side runs its own CG
+ * recurrence (hecmw_solver_CG.f90:19-289: own RHO/ALPHA/BETA, breakdown codes, 50-
+ * iteration true-residual refresh, convergence and ITER), while the matrix and
+ * preconditioner values are read once per iteration for up to 16 of them (SpMM and
+ * 16-vector sweeps); more than 16 are taken 16 at a time.
+ * B, X: host arrays of 3*NP x nrhs, column-major (column k = load case k; X: initial
+ * guesses in, solutions out).  iter[k], resid[k], error[k]: ITER, RESID and the
+ * hecmw_solve_CG code of case k (2002 for a zero column, whose solution is 0);
+ * true_resid[k] (may be NULL): ||b - A x|| / ||b|| after the solve.
+ * Iarray(81) = 1 when every case reached Rarray(1); Iarray(82) = 1 when one diverged.
+ * ierr: the first non-zero code of a case other than 2002, or 0. */
+HECMW33_API void hecmw33_gpu_solve_multi(const int *handle, const int *nrhs, const double *B,
+                                         double *X, int *Iarray, double *Rarray, int *iter,
+                                         double *resid, int *error, double *true_resid,
+                                         double *times, int *ierr);
+
+/* As hecmw33_gpu_solve_multi, with B and X in device memory (3*NP x nrhs doubles). */
+HECMW33_API void hecmw33_gpu_solve_multi_device(const int *handle, const int *nrhs,
+                                                const double *dB, double *dX, int *Iarray,
+                                                double *Rarray, int *iter, double *resid,
+                                                int *error, double *true_resid, double *times,
+                                                int *ierr);
+
 /* y = A x on the resident matrix (hecmw_matvec_33), host vectors of 3*NP. */
 HECMW33_API void hecmw33_gpu_matvec(const int *handle, const double *X, double *Y, int *ierr);
 

@@ -1,0 +1,106 @@
+"""Multi-RHS solve (hecmw33_gpu_solve_multi): every load case against the oracle's
+own hecmw_solve of that load case, with the drop-in's parity bars (iterations
+within +-2, solution within 1e-8 relative, true residual at or below the
+tolerance), the per-case codes (2002 for a zero column, 3001 at MAXIT) and more
+cases than one pass holds (16)."""
+import numpy as np
+import pytest
+
+from frontistr_b200.mesh import box_system
+from frontistr_b200.solver import GpuSolver
+from oracle_ctypes import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def load_cases(m, k, seed):
+    """The cantilever load and k-1 random unit-norm tractions on the loaded face."""
+    rng = np.random.default_rng(seed)
+    top = np.unique(np.nonzero(m.B)[0] // 3)
+    out = [m.B.copy()]
+    for _ in range(k - 1):
+        t = rng.standard_normal(3)
+        t /= np.linalg.norm(t)
+        b = np.zeros_like(m.B)
+        for node in top:
+            b[3 * node:3 * node + 3] = t
+        out.append(b)
+    return np.array(out)
+
+
+def flags(m, precond, maxit=20000, tol=1e-8):
+    ia, ra = m.Iarray.copy(), m.Rarray.copy()
+    ia[0] = maxit
+    ia[2] = precond
+    ra[0] = tol
+    return ia, ra
+
+
+@pytest.mark.parametrize("precond", [1, 3, 10])
+def test_multi_matches_oracle_per_case(precond):
+    m = box_system(16, 16, 64)
+    B = load_cases(m, 6, seed=5)
+    B[3] = 0.0  # a zero load case
+    ia, ra = flags(m, precond)
+    X = np.zeros_like(B)
+    with GpuSolver() as s:
+        s.set_matrix(m)
+        rec = s.solve_multi(B, X, ia, ra)
+    orc = Oracle(m)
+    for k in range(B.shape[0]):
+        if k == 3:
+            assert rec["errors"][k] == 2002 and np.all(X[k] == 0.0)
+            continue
+        ref = Oracle(m.copy()).solve(B=B[k], Iarray=flags(m, precond)[0])
+        assert rec["errors"][k] == 0, (k, rec["errors"])
+        assert abs(int(rec["iter"][k]) - ref["iter"]) <= 2, (k, rec["iter"][k], ref["iter"])
+        err = np.linalg.norm(X[k] - ref["X"]) / np.linalg.norm(ref["X"])
+        assert err <= 1e-8, (k, err)
+        tr = orc.rel_resid(X[k], B[k])
+        assert tr <= 1e-8
+        assert abs(rec["true_resid"][k] - tr) <= 1e-4 * tr  # cancellation in b - A x near 1e-8
+    assert rec["error"] == 0
+    assert ia[80] == 1 and ia[81] == 0
+
+
+def test_multi_equals_single_solves_and_chunks():
+    """20 load cases (two passes: 16 + 4) against single-RHS GPU solves."""
+    m = box_system(8, 8, 24, jitter=0.1, sigma_E=0.3, seed=3)
+    B = load_cases(m, 20, seed=9)
+    ia, ra = flags(m, 1)
+    X = np.zeros_like(B)
+    with GpuSolver() as s:
+        s.set_matrix(m)
+        rec = s.solve_multi(B, X, ia.copy(), ra.copy())
+        for k in (0, 7, 15, 16, 19):
+            g = m.copy()
+            g.B = B[k].copy()
+            g.X = np.zeros_like(g.B)
+            g.set_iter(20000)
+            info = s.solve(g)
+            assert info["error"] == 0
+            assert abs(int(rec["iter"][k]) - info["iter"]) <= 2
+            assert np.linalg.norm(X[k] - g.X) <= 1e-8 * np.linalg.norm(g.X)
+    assert rec["error"] == 0
+
+
+def test_multi_maxit_and_initial_guess():
+    m = box_system(6, 6, 12)
+    B = load_cases(m, 3, seed=1)
+    with GpuSolver() as s:
+        s.set_matrix(m)
+        ia, ra = flags(m, 1, maxit=4)
+        X = np.zeros_like(B)
+        rec = s.solve_multi(B, X, ia, ra)
+        assert list(rec["errors"]) == [3001, 3001, 3001]
+        assert list(rec["iter"]) == [5, 5, 5]  # a completed DO loop leaves ITER = MAXIT+1
+        assert rec["error"] == 3001 and ia[80] == 0
+        # initial guesses are honoured: started from the oracle's solutions, every
+        # case is within the tolerance after the first iteration's check
+        X = np.array([Oracle(m.copy()).solve(B=B[k], Iarray=flags(m, 1)[0])["X"] for k in range(3)])
+        ia, ra = flags(m, 1)
+        rec2 = s.solve_multi(B, X, ia, ra)
+        assert rec2["error"] == 0
+        for k in range(3):
+            assert rec2["iter"][k] <= 3
+            assert Oracle(m).rel_resid(X[k], B[k]) <= 1e-8
