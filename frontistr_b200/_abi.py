@@ -27,6 +27,13 @@ SIGNATURES = {
     "hecmw33_gpu_learn_eval": [_i, ctypes.POINTER(ctypes.c_float), _d, _d, _d, _d, ctypes.POINTER(ctypes.c_float),
                                _i],
     "hecmw33_gpu_rel_resid_noalloc": [_i, _v, _v, _v, _v, _v, _v, _v, _v, _v, _d, _i],
+    "hecmw33_gpu_batch_create": [_i, _i],
+    "hecmw33_gpu_batch_destroy": [_i, _i],
+    "hecmw33_gpu_batch_set_matrix": [_i, _i, _i, _i, _i, _i, _i, _i, _i, _i, _i, _d, _d, _d, _i, _d, _i],
+    "hecmw33_gpu_batch_solve": [_i, _d, _d, _i, _d, _i, _d, _i, _d, _d, _i],
+    "hecmw33_gpu_batch_solve_device": [_i, _v, _v, _i, _d, _i, _d, _i, _d, _d, _i],
+    "hecmw33_gpu_batch_autotune": [_i, _d, _d, _i, _d, _i],
+    "hecmw33_gpu_batch_info": [_i, _i, _d, _i],
     "hecmw33_gpu_last_error": [ctypes.c_char_p, ctypes.c_int],
 }
 

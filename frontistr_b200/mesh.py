@@ -85,3 +85,25 @@ def mesh_system(coords, elements, etype, E, nu, fixed=(), cload=()):
                              _ip(m.indexU), _ip(m.itemU), _dp(m.D), _dp(m.AL), _dp(m.AU), _dp(m.B))
     m.coords = coords
     return m
+
+
+def random_box_batch(nsys, edge_range=(8, 40), E_range=(1.0e3, 1.0e6), nu_range=(0.2, 0.45), seed=0):
+    """nsys independent clamped HEX8 boxes: edge lengths (elements per axis) uniform
+    in edge_range, E log-uniform in E_range, nu uniform in nu_range, and a random
+    unit-norm traction on every node of the loaded face z = nz (seeded)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nsys):
+        nx, ny, nz = (int(v) for v in rng.integers(edge_range[0], edge_range[1] + 1, size=3))
+        E = float(np.exp(rng.uniform(np.log(E_range[0]), np.log(E_range[1]))))
+        nu = float(rng.uniform(nu_range[0], nu_range[1]))
+        m = box_system(nx, ny, nz, E=E, nu=nu)
+        t = rng.standard_normal(3)
+        t /= np.linalg.norm(t)
+        top = np.unique(np.nonzero(m.B)[0] // 3)
+        m.B[:] = 0.0
+        for c in range(3):
+            m.B[3 * top + c] = t[c]
+        m.dims = (nx, ny, nz)
+        out.append(m)
+    return out

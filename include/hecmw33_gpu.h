@@ -244,6 +244,60 @@ HECMW33_API void hecmw33_gpu_rel_resid_noalloc(const int *N, const int *d_indexL
                                                const double *d_AU, const double *d_X,
                                                const double *d_B, double *resid, int *ierr);
 
+/* ---- batched solves ------------------------------------------------------------
+ * Many independent systems solved together, each as hecmw_solve would solve it alone
+ * (hecmw_solver.f90:9-88, hecmw_solve_CG in hecmw_solver_CG.f90:19-289, SSOR_33 in its
+ * own RCM + multicolour order or DIAG_33).  The systems are the diagonal blocks of one
+ * hecmwST matrix: system s owns the nodes sys_ptr[s] .. sys_ptr[s+1]-1 (0-based,
+ * sys_ptr[0] = 0, sys_ptr[nsys] = N) and no block couples two systems.  One solve is
+ * one CUDA-graph launch of a persistent kernel; its launch schedule (lanes per sweep
+ * row, cluster size of the teams that take the largest systems, their share) comes
+ * from hecmw33_gpu_batch_autotune or a JSON-lines cache of earlier tunings
+ * (HECMW33_AUTOTUNE_CACHE, default $HOME/.cache/frontistr_b200_autotune.jsonl).
+ * No single call of the reference takes a batch: the reference solves the systems
+ * one hecmw_solve at a time. */
+HECMW33_API void hecmw33_gpu_batch_create(int *handle, int *ierr);
+HECMW33_API void hecmw33_gpu_batch_destroy(const int *handle, int *ierr);
+
+/* Uploads the block-diagonal matrix and builds the per-system preconditioners
+ * (Iarray(3) PRECOND 1, 2 = SSOR or 3 = DIAG; Iarray(34) ncolor_in; Rarray(2)
+ * sigma_diag).  Structure kept when nsys, sys_ptr, N, NPL, NPU, PRECOND and ncolor_in
+ * are unchanged and Iarray(98) == 0 (values only). */
+HECMW33_API void hecmw33_gpu_batch_set_matrix(const int *handle, const int *nsys, const int *sys_ptr,
+                                              const int *N, const int *NP, const int *NPL,
+                                              const int *NPU, const int *indexL, const int *itemL,
+                                              const int *indexU, const int *itemU, const double *D,
+                                              const double *AL, const double *AU, const int *Iarray,
+                                              const double *Rarray, int *ierr);
+
+/* Solves every system: B, X host arrays of 3*N (system s at 3*sys_ptr[s]); Iarray(1)
+ * MAXIT, Rarray(1) tolerance, Iarray(5) iterPREmax 0 or 1, for every system.
+ * iter[s], resid[s], error[s]: ITER, RESID and the hecmw_solve_CG code of system s
+ * (2002 zero right-hand side, 2001 zero diagonal: not solved); true_resid[s] (may be
+ * NULL): ||b - A x|| / ||b|| of system s.  Iarray(81) = 1 when every system reached
+ * the tolerance, Iarray(82) = 1 when one diverged.  ierr: the first non-zero system
+ * code other than 2002, or 0.  times: set-up, device solve time, 0. */
+HECMW33_API void hecmw33_gpu_batch_solve(const int *handle, const double *B, double *X, int *Iarray,
+                                         double *Rarray, int *iter, double *resid, int *error,
+                                         double *true_resid, double *times, int *ierr);
+
+/* As hecmw33_gpu_batch_solve with B and X in device memory. */
+HECMW33_API void hecmw33_gpu_batch_solve_device(const int *handle, const double *dB, double *dX,
+                                                int *Iarray, double *Rarray, int *iter,
+                                                double *resid, int *error, double *true_resid,
+                                                double *times, int *ierr);
+
+/* Times candidate launch schedules by solving from B/X (X is not modified), keeps the
+ * fastest for this handle and appends it to the cache. */
+HECMW33_API void hecmw33_gpu_batch_autotune(const int *handle, const double *B, const double *X,
+                                            const int *Iarray, const double *Rarray, int *ierr);
+
+/* info[16]: lanes, cluster size, systems taken by teams, by single CTAs, grid (CTAs),
+ * tuned (1/0), nsys, kernels per solve, total and largest iteration count of the last
+ * solve.  dinfo[16]: last device solve seconds, last set-up seconds, team share,
+ * device bytes held. */
+HECMW33_API void hecmw33_gpu_batch_info(const int *handle, int *info, double *dinfo, int *ierr);
+
 /* Copies the message of the last error of the calling thread into buf; returns its length. */
 HECMW33_API int hecmw33_gpu_last_error(char *buf, int len);
 
