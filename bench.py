@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision variant")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner variants")
     ap.add_argument("--train-steps", type=int, default=60)
+    ap.add_argument("--no-multi", action="store_true", help="skip the 16-load-case multi-RHS measurement")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 256-system batched measurement")
+    ap.add_argument("--batch-systems", type=int, default=256)
+    ap.add_argument("--batch-edges", default="8,40", help="element range per box edge of the batch")
     ap.add_argument("--spmv-only", type=int, default=0,
                     help="only build the system and run this many SpMV launches (profiling)")
     ap.add_argument("--profile-solve", action="store_true",
@@ -217,6 +221,107 @@ def run_reference(args, rank, world):
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+def face_load_cases(m, k, seed):
+    """k load cases: random unit-norm tractions on every node of the loaded face."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    top = np.unique(np.nonzero(m.B)[0] // 3)
+    out = np.zeros((k, 3 * m.N))
+    for j in range(k):
+        t = rng.standard_normal(3)
+        t /= np.linalg.norm(t)
+        for c in range(3):
+            out[j, 3 * top + c] = t[c]
+    return out
+
+
+def bench_multi(solver, m, nrhs=16):
+    """16 load cases on the resident matrix: one multi-RHS solve (SpMM + 16-vector
+    sweeps) against the same 16 cases solved one after another (device times)."""
+    import numpy as np
+    B = face_load_cases(m, nrhs, seed=11)
+    ia, ra = m.Iarray.copy(), m.Rarray.copy()
+    ia[96] = ia[97] = 0
+    X = np.zeros_like(B)
+    solver.solve_multi(B, X, ia.copy(), ra.copy())  # warm (buffers, graph)
+    X = np.zeros_like(B)
+    rec = solver.solve_multi(B, X, ia.copy(), ra.copy())
+    t_multi = rec["t_solve"]
+    kernels = solver.last_solve_info()["kernels"]
+    t_seq, it_seq = 0.0, []
+    for k in range(nrhs):
+        x = np.zeros(3 * m.N)
+        r1 = solver.solve_resident(B[k].copy(), x, ia.copy(), ra.copy())
+        t_seq += r1["t_solve"]
+        it_seq.append(int(r1["iter"]))
+    return {"load_cases": nrhs, "s": t_multi, "rhs_per_s": nrhs / t_multi, "sequential_s": t_seq,
+            "sequential_rhs_per_s": nrhs / t_seq, "speedup_vs_sequential": t_seq / t_multi,
+            "iterations": [int(v) for v in rec["iter"]], "sequential_iterations": it_seq,
+            "max_true_resid": float(np.max(rec["true_resid"])),
+            "errors": sorted(set(int(v) for v in rec["errors"])), "gpu_launches": kernels,
+            "workload": "%d random unit-norm tractions on the loaded face of the same matrix, CG+SSOR to 1e-8"
+                        % nrhs}
+
+
+def bench_batched(args):
+    """Independent boxes (edges uniform in [8, 40] elements, E log-uniform in
+    [1e3, 1e6], nu in [0.2, 0.45], random traction on the top face; seeded) solved
+    in one persistent launch with the autotuned schedule, against the same systems
+    solved one after another on one handle (device times, set-up excluded)."""
+    import numpy as np
+    from frontistr_b200.batch import BatchSolver, stack_systems
+    from frontistr_b200.mesh import random_box_batch
+    from frontistr_b200.solver import GpuSolver
+    lo, hi = (int(v) for v in args.batch_edges.split(","))
+    t0 = time.perf_counter()
+    systems = random_box_batch(args.batch_systems, edge_range=(lo, hi), seed=2024)
+    big, sys_ptr = stack_systems(systems)
+    t_asm = time.perf_counter() - t0
+    ia, ra = big.Iarray.copy(), big.Rarray.copy()
+    ia[0] = 20000
+    ra[0] = args.tol
+    out = {"systems": len(systems), "nodes": int(big.N), "dof": 3 * int(big.N), "blocks": int(big.NZ),
+           "dof_range": [3 * min(m.N for m in systems), 3 * max(m.N for m in systems)], "assemble_s": t_asm}
+    with BatchSolver() as bs:
+        t = time.perf_counter()
+        bs.set_matrix(big, sys_ptr, ia, ra)
+        out["setup_s"] = time.perf_counter() - t
+        t = time.perf_counter()
+        bs.autotune(big.B, np.zeros(3 * big.N), ia.copy(), ra.copy())
+        out["autotune_s"] = time.perf_counter() - t
+        X = np.zeros(3 * big.N)
+        bs.solve(big.B, X, ia.copy(), ra.copy())  # warm
+        times = []
+        for _ in range(2):
+            X = np.zeros(3 * big.N)
+            rec = bs.solve(big.B, X, ia.copy(), ra.copy())
+            times.append(rec["t_solve"])
+        info = bs.info()
+    t_b = min(times)
+    out.update({"s": t_b, "systems_per_s": len(systems) / t_b,
+                "schedule": {k: info[k] for k in ("lanes", "cluster", "big", "small", "grid", "big_frac")},
+                "total_iterations": int(np.sum(rec["iter"])), "max_iterations": int(np.max(rec["iter"])),
+                "max_true_resid": float(np.max(rec["true_resid"])),
+                "errors": sorted(set(int(v) for v in rec["errors"])), "gpu_launches": info["kernels_per_solve"]})
+    t_seq = 0.0
+    with GpuSolver() as s:
+        for m in systems:
+            g = m.copy()
+            g.set_iter(20000)
+            g.set_resid(args.tol)
+            s.solve(g)  # set-up (not timed)
+            g.X[:] = 0.0
+            g.Iarray[96] = g.Iarray[97] = 0
+            r1 = s.solve_resident(g.B, g.X, g.Iarray, g.Rarray)
+            t_seq += r1["t_solve"]
+    out.update({"sequential_s": t_seq, "sequential_systems_per_s": len(systems) / t_seq,
+                "speedup_vs_sequential": t_seq / t_b,
+                "workload": "%d HEX8 boxes, edges uniform in [%d, %d] elements, E log-uniform [1e3, 1e6], "
+                            "nu [0.2, 0.45], random unit traction on z = nz; CG+SSOR to %g" %
+                            (len(systems), lo, hi, args.tol)})
+    return out
 
 
 def config_dict(nx, ny, nz, m, args):
@@ -403,6 +508,9 @@ def main():
     if e2e:
         e2e["value"] = float(vals[2])
 
+    multi = None if args.no_multi else bench_multi(solver, m)
+    batched = None if args.no_batched else bench_batched(args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         per_iter, n, cores, t_setup = cpu_oracle_sample(m, args.precond, iters, args.cpu_sample_s)
@@ -440,6 +548,8 @@ def main():
             "e2e": e2e,
             "gpu_launches": variants[head]["kernels"] * args.steps,
             "clocks": clk,
+            "multi_rhs": multi,
+            "batched": batched,
         }
         print(json.dumps(line))
     solver.close()
