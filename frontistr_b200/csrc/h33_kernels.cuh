@@ -376,32 +376,6 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<R> A, const R *
   if (MODE == 2) reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[1], [&](double v) { fin_pq(st, v); });
 }
 
-// The 3x3 forward/backward substitution of lu_solve with the nine entries in registers.
-template <class R>
-__device__ __forceinline__ void lu_solve_reg(const R (&a)[9], R &x1, R &x2, R &x3) {
-  x2 = x2 - a[3] * x1;
-  x3 = x3 - a[6] * x1 - a[7] * x2;
-  x3 = a[8] * x3;
-  x2 = a[4] * (x2 - a[5] * x3);
-  x1 = a[0] * (x1 - a[2] * x3 - a[1] * x2);
-}
-
-// The K lanes of a sweep row share the loads of the row's own data: lane `sub` of
-// the row loads ALU entries sub, sub+K, ... and vector entries sub, sub+K, ... of the
-// row's node BEFORE the row's gather (so their latency overlaps it); the row's
-// leader lane collects them with shuffles afterwards.
-template <int K>
-struct RowShare {
-  static constexpr int NA = (9 + K - 1) / K;  // ALU entries per lane
-  static constexpr int NV = (3 + K - 1) / K;  // vector entries per lane
-};
-
-template <int K, class T, int N>
-__device__ __forceinline__ T row_take(const T (&v)[N], int e, int base) {
-  if (K == 1) return v[e];
-  return __shfl_sync(0xffffffffu, v[e / K], base + e % K);
-}
-
 // Forward sweep over the slices [sbeg, send) of one colour / level, each row spread
 // over K lanes:  z(node) = LU^-1 ( r(node) - sum_lower A z(col) )
 // (hecmw_precond_SSOR_33.F90:309-345)
@@ -411,40 +385,19 @@ __global__ void __launch_bounds__(kThreads) sweep_fwd_kernel(SellView<TV> L, con
                                                              const R *__restrict__ r, R *__restrict__ z,
                                                              int sbeg, int send, const CgState *st) {
   if (st && st->done) return;
-  constexpr int NA = RowShare<K>::NA, NV = RowShare<K>::NV;
   const int lane = threadIdx.x & 31;
-  const int roff = lane / K, sub = lane & (K - 1), base = lane & ~(K - 1);
+  const int roff = lane / K;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
     const bool active = roff < L.nrows[s];
     const int row = L.row0[s] + roff;
     const int len = active ? L.rowlen[s * 32 + roff] : 0;
-    int node = 0;
-    TA ap[NA];
-    R rp[NV];
-#pragma unroll
-    for (int j = 0; j < NA; j++) ap[j] = TA(0);
-#pragma unroll
-    for (int j = 0; j < NV; j++) rp[j] = R(0);
-    if (active) {
-      node = __ldg(&perm[row]);
-#pragma unroll
-      for (int j = 0; j < NA; j++)
-        if (sub + j * K < 9) ap[j] = __ldg(&alu[(sub + j * K) * npos + row]);
-#pragma unroll
-      for (int j = 0; j < NV; j++)
-        if (sub + j * K < 3) rp[j] = r[3 * node + sub + j * K];
-    }
     R a0 = 0, a1 = 0, a2 = 0;
     row_gemv<R, TV, K, false>(L, s, lane, len, z, a0, a1, a2);
-    R av[9], rv[3];
-#pragma unroll
-    for (int e = 0; e < 9; e++) av[e] = R(row_take<K>(ap, e, base));
-#pragma unroll
-    for (int c = 0; c < 3; c++) rv[c] = row_take<K>(rp, c, base);
-    if (active && sub == 0) {
-      R x1 = rv[0] - a0, x2 = rv[1] - a1, x3 = rv[2] - a2;
-      lu_solve_reg(av, x1, x2, x3);
+    if (active && (lane & (K - 1)) == 0) {
+      const int node = perm[row];
+      R x1 = r[3 * node] - a0, x2 = r[3 * node + 1] - a1, x3 = r[3 * node + 2] - a2;
+      lu_solve(alu, npos, row, x1, x2, x3);
       z[3 * node] = x1;
       z[3 * node + 1] = x2;
       z[3 * node + 2] = x3;
@@ -464,51 +417,26 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, con
                                                              double *partials, int part_base,
                                                              int part_total) {
   if (st && st->done) return;
-  constexpr int NA = RowShare<K>::NA, NV = RowShare<K>::NV;
   const int lane = threadIdx.x & 31;
-  const int roff = lane / K, sub = lane & (K - 1), base = lane & ~(K - 1);
+  const int roff = lane / K;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double dot = 0.0;
   for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
     const bool active = roff < U.nrows[s];
     const int row = U.row0[s] + roff;
     const int len = active ? U.rowlen[s * 32 + roff] : 0;
-    int node = 0;
-    TA ap[NA];
-    R zp[NV], rp[NV];
-#pragma unroll
-    for (int j = 0; j < NA; j++) ap[j] = TA(0);
-#pragma unroll
-    for (int j = 0; j < NV; j++) zp[j] = rp[j] = R(0);
-    if (active) {
-      node = __ldg(&perm[row]);
-#pragma unroll
-      for (int j = 0; j < NA; j++)
-        if (sub + j * K < 9) ap[j] = __ldg(&alu[(sub + j * K) * npos + row]);
-#pragma unroll
-      for (int j = 0; j < NV; j++)
-        if (sub + j * K < 3) {
-          zp[j] = z[3 * node + sub + j * K];  // this row's own entry: written by the forward sweep
-          if (FUSE_RHO) rp[j] = r[3 * node + sub + j * K];
-        }
-    }
     R x1 = 0, x2 = 0, x3 = 0;
     row_gemv<R, TV, K, true>(U, s, lane, len, z, x1, x2, x3);
-    R av[9], zv[3], rv[3];
-#pragma unroll
-    for (int e = 0; e < 9; e++) av[e] = R(row_take<K>(ap, e, base));
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      zv[c] = row_take<K>(zp, c, base);
-      rv[c] = FUSE_RHO ? row_take<K>(rp, c, base) : R(0);
-    }
-    if (active && sub == 0) {
-      lu_solve_reg(av, x1, x2, x3);
-      const R z0 = zv[0] - x1, z1 = zv[1] - x2, z2 = zv[2] - x3;
+    if (active && (lane & (K - 1)) == 0) {
+      const int node = perm[row];
+      lu_solve(alu, npos, row, x1, x2, x3);
+      const R z0 = z[3 * node] - x1, z1 = z[3 * node + 1] - x2, z2 = z[3 * node + 2] - x3;
       z[3 * node] = z0;
       z[3 * node + 1] = z1;
       z[3 * node + 2] = z2;
-      if (FUSE_RHO) dot += double(rv[0]) * double(z0) + double(rv[1]) * double(z1) + double(rv[2]) * double(z2);
+      if (FUSE_RHO)
+        dot += double(r[3 * node]) * double(z0) + double(r[3 * node + 1]) * double(z1) +
+               double(r[3 * node + 2]) * double(z2);
     }
   }
   if (FUSE_RHO)
