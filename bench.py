@@ -61,6 +61,10 @@ def parse():
                     help="only build the system and run this many SpMV launches (profiling)")
     ap.add_argument("--profile-solve", action="store_true",
                     help="one solve capped at 5 CG iterations, nothing printed (profiling)")
+    ap.add_argument("--profile-multi", action="store_true",
+                    help="one 16-load-case solve capped at 3 CG iterations, nothing printed (profiling)")
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="one batched solve of --batch-systems boxes, nothing printed (profiling)")
     return ap.parse_args()
 
 
@@ -358,6 +362,26 @@ def main():
         solver.set_matrix(m)
         solver.time_spmv(args.spmv_only)
         torch.cuda.synchronize()
+        return
+    if args.profile_multi:
+        import numpy as np
+        solver.set_matrix(m)
+        B = face_load_cases(m, 16, seed=11)
+        ia, ra = m.Iarray.copy(), m.Rarray.copy()
+        ia[0] = 3
+        solver.solve_multi(B, np.zeros_like(B), ia, ra)
+        return
+    if args.profile_batch:
+        import numpy as np
+        from frontistr_b200.batch import BatchSolver, stack_systems
+        from frontistr_b200.mesh import random_box_batch
+        lo, hi = (int(v) for v in args.batch_edges.split(","))
+        big, sys_ptr = stack_systems(random_box_batch(args.batch_systems, edge_range=(lo, hi), seed=2024))
+        ia, ra = big.Iarray.copy(), big.Rarray.copy()
+        ia[0] = 20000
+        with BatchSolver() as bs:
+            bs.set_matrix(big, sys_ptr, ia, ra)
+            bs.solve(big.B, np.zeros(3 * big.N), ia, ra)
         return
     if args.profile_solve:
         mm = m.copy()
