@@ -70,25 +70,36 @@ __device__ __forceinline__ void mr_reduce_finish(double v, double *partials, int
 }
 
 // Sum of A(row, :) x over the blocks of one row of a sliced layout with K lanes per
-// row (block k at slot slot0 + k/K, lane roff*K + k%K), for this lane's RHS.
+// row (block k at slot slot0 + k/K, lane roff*K + k%K), for this lane's RHS.  The
+// 16 lanes of the half-warp first load 16 of the row's column indices at once (one
+// each) and pass them round by shuffles, so the x gathers of successive blocks do
+// not wait on one another's index loads.  hmask: this half-warp's lanes.
 template <int K>
 __device__ __forceinline__ void mr_row(const SellView<double> &A, int s, int roff, int len, int l,
-                                       const double *__restrict__ x, double &y0, double &y1, double &y2) {
+                                       unsigned hmask, const double *__restrict__ x, double &y0, double &y1,
+                                       double &y2) {
   const int slot0 = A.slot0[s];
-#pragma unroll 2
-  for (int k = 0; k < len; k++) {
-    const int sl = slot0 + k / K;
-    const int lp = roff * K + (k & (K - 1));
-    const int c = __ldg(&A.col[sl * 32 + lp]);
-    const double *v = A.val + sl * 288 + lp;
-    const double *xc = x + size_t(c) * kRhsStride + l;
-    const double x0 = xc[0], x1 = xc[16], x2 = xc[32];
-    const double v0 = __ldg(v), v1 = __ldg(v + 32), v2 = __ldg(v + 64);
-    const double v3 = __ldg(v + 96), v4 = __ldg(v + 128), v5 = __ldg(v + 160);
-    const double v6 = __ldg(v + 192), v7 = __ldg(v + 224), v8 = __ldg(v + 256);
-    y0 = fma(v2, x2, fma(v1, x1, fma(v0, x0, y0)));
-    y1 = fma(v5, x2, fma(v4, x1, fma(v3, x0, y1)));
-    y2 = fma(v8, x2, fma(v7, x1, fma(v6, x0, y2)));
+  for (int k0 = 0; k0 < len; k0 += 16) {
+    const int kn = min(16, len - k0);
+    int myc = 0;
+    if (l < kn) {
+      const int k = k0 + l;
+      myc = __ldg(&A.col[(slot0 + k / K) * 32 + roff * K + (k & (K - 1))]);
+    }
+#pragma unroll 4
+    for (int kk = 0; kk < kn; kk++) {
+      const int k = k0 + kk;
+      const int c = __shfl_sync(hmask, myc, kk, 16);
+      const double *v = A.val + (slot0 + k / K) * 288 + roff * K + (k & (K - 1));
+      const double *xc = x + size_t(c) * kRhsStride + l;
+      const double x0 = xc[0], x1 = xc[16], x2 = xc[32];
+      const double v0 = __ldg(v), v1 = __ldg(v + 32), v2 = __ldg(v + 64);
+      const double v3 = __ldg(v + 96), v4 = __ldg(v + 128), v5 = __ldg(v + 160);
+      const double v6 = __ldg(v + 192), v7 = __ldg(v + 224), v8 = __ldg(v + 256);
+      y0 = fma(v2, x2, fma(v1, x1, fma(v0, x0, y0)));
+      y1 = fma(v5, x2, fma(v4, x1, fma(v3, x0, y1)));
+      y2 = fma(v8, x2, fma(v7, x1, fma(v6, x0, y2)));
+    }
   }
 }
 
@@ -125,6 +136,7 @@ __global__ void __launch_bounds__(kThreads) mr_spmv_kernel(SellView<double> A, c
   const int hw0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
   const int nhw = (gridDim.x * blockDim.x) >> 4;
   const int nrows_total = A.nslices * 32;
+  const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
   double dot = 0.0;
   for (int t = hw0; t < nrows_total; t += nhw) {
     const int s = t >> 5, roff = t & 31;
@@ -132,7 +144,7 @@ __global__ void __launch_bounds__(kThreads) mr_spmv_kernel(SellView<double> A, c
     const int row = A.row0[s] + roff;
     const int len = A.rowlen[s * 32 + roff];
     double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-    mr_row<1>(A, s, roff, len, l, x, y0, y1, y2);
+    mr_row<1>(A, s, roff, len, l, hmask, x, y0, y1, y2);
     const size_t o = size_t(row) * kRhsStride + l;
     if (MODE == 1 || MODE == 3) {
       y0 = b[o] - y0;
@@ -176,13 +188,14 @@ __global__ void __launch_bounds__(kThreads) mr_sweep_fwd_kernel(SellView<double>
   const int l = threadIdx.x & 15;
   const int nhw = (gridDim.x * blockDim.x) >> 4;
   const int total = (se - sb) * (32 / K);
+  const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
   for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; t < total; t += nhw) {
     int s, roff;
     if (!mr_locate<K>(L, sb, se, t, s, roff)) continue;
     const int row = L.row0[s] + roff;
     const int len = L.rowlen[s * 32 + roff];
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    mr_row<K>(L, s, roff, len, l, z, a0, a1, a2);
+    mr_row<K>(L, s, roff, len, l, hmask, z, a0, a1, a2);
     const int node = perm[row];
     const size_t o = size_t(node) * kRhsStride + l;
     double x1 = r[o] - a0, x2 = r[o + 16] - a1, x3 = r[o + 32] - a2;
@@ -205,6 +218,7 @@ __global__ void __launch_bounds__(kThreads) mr_sweep_bwd_kernel(SellView<double>
   const int l = threadIdx.x & 15;
   const int nhw = (gridDim.x * blockDim.x) >> 4;
   const int total = (se - sb) * (32 / K);
+  const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
   double dot = 0.0;
   for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; t < total; t += nhw) {
     int s, roff;
@@ -212,7 +226,7 @@ __global__ void __launch_bounds__(kThreads) mr_sweep_bwd_kernel(SellView<double>
     const int row = U.row0[s] + roff;
     const int len = U.rowlen[s * 32 + roff];
     double x1 = 0.0, x2 = 0.0, x3 = 0.0;
-    mr_row<K>(U, s, roff, len, l, z, x1, x2, x3);
+    mr_row<K>(U, s, roff, len, l, hmask, z, x1, x2, x3);
     const int node = perm[row];
     lu_solve(alu, npos, row, x1, x2, x3);
     const size_t o = size_t(node) * kRhsStride + l;
