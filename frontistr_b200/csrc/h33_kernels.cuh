@@ -378,59 +378,100 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<R> A, const R *
 
 // Forward sweep over the slices [sbeg, send) of one colour / level, each row spread
 // over K lanes:  z(node) = LU^-1 ( r(node) - sum_lower A z(col) )
-// (hecmw_precond_SSOR_33.F90:309-345)
-template <class R, class TV, class TA, int K>
+// (hecmw_precond_SSOR_33.F90:309-345).
+// POS (the multicolour SSOR): the layout's columns are positions in the colour
+// order and the sweep keeps its intermediate vector zpos in that order, so a row's
+// own entries sit at zpos[row] and only the right-hand side needs the permutation;
+// its load (perm -> r) is issued before the row's gather.  Without POS (ILU(0)
+// level schedules) columns are nodes and z is gathered and written in node order.
+template <class R, class TV, class TA, int K, bool POS>
 __global__ void __launch_bounds__(kThreads) sweep_fwd_kernel(SellView<TV> L, const int *__restrict__ perm,
                                                              const TA *__restrict__ alu, int npos,
                                                              const R *__restrict__ r, R *__restrict__ z,
-                                                             int sbeg, int send, const CgState *st) {
+                                                             R *__restrict__ zpos, int sbeg, int send,
+                                                             const CgState *st) {
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
   const int roff = lane / K;
+  const bool leader = (lane & (K - 1)) == 0;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
     const bool active = roff < L.nrows[s];
     const int row = L.row0[s] + roff;
     const int len = active ? L.rowlen[s * 32 + roff] : 0;
+    R r0 = 0, r1 = 0, r2 = 0;
+    int node = 0;
+    if (POS && active && leader) {
+      node = perm[row];
+      r0 = r[3 * node];
+      r1 = r[3 * node + 1];
+      r2 = r[3 * node + 2];
+    }
     R a0 = 0, a1 = 0, a2 = 0;
-    row_gemv<R, TV, K, false>(L, s, lane, len, z, a0, a1, a2);
-    if (active && (lane & (K - 1)) == 0) {
-      const int node = perm[row];
-      R x1 = r[3 * node] - a0, x2 = r[3 * node + 1] - a1, x3 = r[3 * node + 2] - a2;
+    row_gemv<R, TV, K, false>(L, s, lane, len, POS ? zpos : z, a0, a1, a2);
+    if (active && leader) {
+      if (!POS) {
+        node = perm[row];
+        r0 = r[3 * node];
+        r1 = r[3 * node + 1];
+        r2 = r[3 * node + 2];
+      }
+      R x1 = r0 - a0, x2 = r1 - a1, x3 = r2 - a2;
       lu_solve(alu, npos, row, x1, x2, x3);
-      z[3 * node] = x1;
-      z[3 * node + 1] = x2;
-      z[3 * node + 2] = x3;
+      R *out = POS ? zpos + 3 * row : z + 3 * node;
+      out[0] = x1;
+      out[1] = x2;
+      out[2] = x3;
     }
   }
 }
 
 // Backward sweep over [sbeg, send), rows spread over K lanes:
 // z(node) -= LU^-1 ( sum_upper A z(col) )   (hecmw_precond_SSOR_33.F90:353-405).
-// FUSE_RHO accumulates {r}{z} of the finished rows; the last launch's last CTA
-// runs the RHO finisher.
-template <class R, class TV, class TA, int K, bool FUSE_RHO>
+// POS: gathers and updates zpos in colour order and writes the finished rows to z
+// in node order.  FUSE_RHO accumulates {r}{z} of the finished rows; the last
+// launch's last CTA runs the RHO finisher.
+template <class R, class TV, class TA, int K, bool FUSE_RHO, bool POS>
 __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, const int *__restrict__ perm,
                                                              const TA *__restrict__ alu, int npos,
                                                              const R *__restrict__ r, R *__restrict__ z,
-                                                             int sbeg, int send, CgState *st,
+                                                             R *__restrict__ zpos, int sbeg, int send, CgState *st,
                                                              double *partials, int part_base,
                                                              int part_total) {
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
   const int roff = lane / K;
+  const bool leader = (lane & (K - 1)) == 0;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double dot = 0.0;
   for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
     const bool active = roff < U.nrows[s];
     const int row = U.row0[s] + roff;
     const int len = active ? U.rowlen[s * 32 + roff] : 0;
+    int node = 0;
+    R c0 = 0, c1 = 0, c2 = 0;  // this row's current z (written by the forward sweep)
+    if (POS && active && leader) {
+      node = perm[row];
+      c0 = zpos[3 * row];
+      c1 = zpos[3 * row + 1];
+      c2 = zpos[3 * row + 2];
+    }
     R x1 = 0, x2 = 0, x3 = 0;
-    row_gemv<R, TV, K, true>(U, s, lane, len, z, x1, x2, x3);
-    if (active && (lane & (K - 1)) == 0) {
-      const int node = perm[row];
+    row_gemv<R, TV, K, true>(U, s, lane, len, POS ? zpos : z, x1, x2, x3);
+    if (active && leader) {
+      if (!POS) {
+        node = perm[row];
+        c0 = z[3 * node];
+        c1 = z[3 * node + 1];
+        c2 = z[3 * node + 2];
+      }
       lu_solve(alu, npos, row, x1, x2, x3);
-      const R z0 = z[3 * node] - x1, z1 = z[3 * node + 1] - x2, z2 = z[3 * node + 2] - x3;
+      const R z0 = c0 - x1, z1 = c1 - x2, z2 = c2 - x3;
+      if (POS) {
+        zpos[3 * row] = z0;
+        zpos[3 * row + 1] = z1;
+        zpos[3 * row + 2] = z2;
+      }
       z[3 * node] = z0;
       z[3 * node + 1] = z1;
       z[3 * node + 2] = z2;

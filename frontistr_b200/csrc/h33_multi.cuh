@@ -179,11 +179,14 @@ __global__ void __launch_bounds__(kThreads) mr_spmv_kernel(SellView<double> A, c
 }
 
 // Forward sweep over the slices [sb, se) of one colour / level, 16 RHS at once.
-template <int K>
+// POS: columns are colour positions and the intermediate lives in zpos (colour
+// order), as in sweep_fwd_kernel; otherwise node order throughout.
+template <int K, bool POS>
 __global__ void __launch_bounds__(kThreads) mr_sweep_fwd_kernel(SellView<double> L, const int *__restrict__ perm,
                                                                 const double *__restrict__ alu, int npos,
                                                                 const double *__restrict__ r, double *__restrict__ z,
-                                                                int sb, int se, const MultiCtl *ctl) {
+                                                                double *__restrict__ zpos, int sb, int se,
+                                                                const MultiCtl *ctl) {
   if (ctl && ctl->all_done) return;
   const int l = threadIdx.x & 15;
   const int nhw = (gridDim.x * blockDim.x) >> 4;
@@ -194,26 +197,30 @@ __global__ void __launch_bounds__(kThreads) mr_sweep_fwd_kernel(SellView<double>
     if (!mr_locate<K>(L, sb, se, t, s, roff)) continue;
     const int row = L.row0[s] + roff;
     const int len = L.rowlen[s * 32 + roff];
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    mr_row<K>(L, s, roff, len, l, hmask, z, a0, a1, a2);
     const int node = perm[row];
     const size_t o = size_t(node) * kRhsStride + l;
-    double x1 = r[o] - a0, x2 = r[o + 16] - a1, x3 = r[o + 32] - a2;
+    const double r0 = r[o], r1 = r[o + 16], r2 = r[o + 32];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    mr_row<K>(L, s, roff, len, l, hmask, POS ? zpos : z, a0, a1, a2);
+    double x1 = r0 - a0, x2 = r1 - a1, x3 = r2 - a2;
     lu_solve(alu, npos, row, x1, x2, x3);
-    z[o] = x1;
-    z[o + 16] = x2;
-    z[o + 32] = x3;
+    double *out = (POS ? zpos + size_t(row) * kRhsStride + l : z + o);
+    out[0] = x1;
+    out[16] = x2;
+    out[32] = x3;
   }
 }
 
 // Backward sweep; FUSE_RHO: per-RHS {r}{z} of the finished rows and, in the last
-// launch's last CTA, the RHO finisher of every RHS.
-template <int K, bool FUSE_RHO>
+// launch's last CTA, the RHO finisher of every RHS.  POS: updates zpos and writes the
+// finished rows to z in node order.
+template <int K, bool FUSE_RHO, bool POS>
 __global__ void __launch_bounds__(kThreads) mr_sweep_bwd_kernel(SellView<double> U, const int *__restrict__ perm,
                                                                 const double *__restrict__ alu, int npos,
                                                                 const double *__restrict__ r, double *__restrict__ z,
-                                                                int sb, int se, CgState *st, MultiCtl *ctl,
-                                                                double *partials, int part_base, int part_total) {
+                                                                double *__restrict__ zpos, int sb, int se, CgState *st,
+                                                                MultiCtl *ctl, double *partials, int part_base,
+                                                                int part_total) {
   if (ctl && ctl->all_done) return;
   const int l = threadIdx.x & 15;
   const int nhw = (gridDim.x * blockDim.x) >> 4;
@@ -225,12 +232,20 @@ __global__ void __launch_bounds__(kThreads) mr_sweep_bwd_kernel(SellView<double>
     if (!mr_locate<K>(U, sb, se, t, s, roff)) continue;
     const int row = U.row0[s] + roff;
     const int len = U.rowlen[s * 32 + roff];
-    double x1 = 0.0, x2 = 0.0, x3 = 0.0;
-    mr_row<K>(U, s, roff, len, l, hmask, z, x1, x2, x3);
     const int node = perm[row];
-    lu_solve(alu, npos, row, x1, x2, x3);
     const size_t o = size_t(node) * kRhsStride + l;
-    const double z0 = z[o] - x1, z1 = z[o + 16] - x2, z2 = z[o + 32] - x3;
+    const size_t op = POS ? size_t(row) * kRhsStride + l : o;
+    const double *zc = POS ? zpos : z;
+    const double c0 = zc[op], c1 = zc[op + 16], c2 = zc[op + 32];
+    double x1 = 0.0, x2 = 0.0, x3 = 0.0;
+    mr_row<K>(U, s, roff, len, l, hmask, POS ? zpos : z, x1, x2, x3);
+    lu_solve(alu, npos, row, x1, x2, x3);
+    const double z0 = c0 - x1, z1 = c1 - x2, z2 = c2 - x3;
+    if (POS) {
+      zpos[op] = z0;
+      zpos[op + 16] = z1;
+      zpos[op + 32] = z2;
+    }
     z[o] = z0;
     z[o + 16] = z1;
     z[o + 32] = z2;

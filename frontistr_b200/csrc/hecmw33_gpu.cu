@@ -55,13 +55,13 @@ bool graph_mode() {
 constexpr int kStreamChunk = 16;
 
 // Lanes per row of the preconditioner sweep layouts (HECMW33_SWEEP_LANES overrides;
-// 1, 2, 4, 8, 16 or 32).  Several lanes per row shorten each row's dependent load
+// 4, 8 or 16).  Several lanes per row shorten each row's dependent load
 // chain and multiply the warps of a colour, which the sweeps need: a colour holds
 // a tenth of the rows, too few one-lane rows to cover HBM latency.
 int sweep_lanes() {
   const char *e = std::getenv("HECMW33_SWEEP_LANES");
   const int k = e ? std::atoi(e) : 8;
-  return (k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32) ? k : 8;
+  return (k == 4 || k == 8 || k == 16) ? k : 8;
 }
 
 double wall() {
@@ -130,6 +130,7 @@ struct Precond {
   DevArray<double> ilu_raw;           // ILU(0) factor blocks, raw numbering
   DevArray<float> alu32_fwd, alu32_bwd;
   int numeric_version = 0, fp32_version = -1, lowp_version = -1;
+  bool pos_cols = false;  // lo/up columns are colour positions (multicolour SSOR)
 };
 
 // The learned preconditioner: node graph of the matrix, weights, activations and
@@ -200,13 +201,15 @@ struct Solver {
   // flexible CG buffers (SSOR output and previous residual) and the learned preconditioner
   DevArray<double> zs, rold;
   DevArray<float> zsf, roldf;
+  DevArray<double> zpos;  // SSOR sweep intermediate in colour-position order (FP64 / FP32)
+  DevArray<float> zposf;
   Learned L;
   int values_version = 0, a32_version = -1;
   double bnrm2 = 0.0;
   // graphs (FP64 drop-in, FP32 inner solve)
   GraphSlot g64, g32;
   // multi-RHS CG: node-major RHS-minor vectors (48 doubles per node), per-RHS states
-  DevArray<double> mb, mx, mr, mz, mp, mq, mw, mzp, mpart;
+  DevArray<double> mb, mx, mr, mz, mp, mq, mw, mzp, mzpos, mpart;
   DevArray<CgState> mst;
   DevArray<MultiCtl> mctl;
   CgState *h_mst = nullptr;
@@ -224,9 +227,9 @@ struct Solver {
     H33_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     H33_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_spmv, spmv_kernel<double, 2>, kThreads, 0));
-    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep, sweep_bwd_kernel<double, double, double, 8, true>, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep, sweep_bwd_kernel<double, double, double, 8, true, true>, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_vec, update_xr_kernel<double>, kThreads, 0));
-    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mr, mr_sweep_bwd_kernel<8, true>, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mr, mr_sweep_bwd_kernel<8, true, true>, kThreads, 0));
     occ_spmv = std::max(occ_spmv, 1);
     occ_sweep = std::max(occ_sweep, 1);
     occ_vec = std::max(occ_vec, 1);
@@ -374,9 +377,15 @@ void setup_ssor(Solver &S, int ncolor_in, double sigma, bool symbolic) {
     P.ncolor = ordering_mc(prof, perm_rcm, ncolor_in, colorindex, perm, iperm);
     BlockRows lower, upper;
     reordered_rows(prof, perm, iperm, lower, upper);
+    // the device sweeps gather from their colour-ordered intermediate: columns as
+    // positions (the same blocks in the same order; only the index names change)
+    for (auto *br : {&lower, &upper})
+      for (int &c : br->col) c = iperm[c];
     SellLayout lo, up;
     build_sell(lower, colorindex, lo, sweep_lanes());
     build_sell(upper, colorindex, up, sweep_lanes());
+    P.pos_cols = true;
+    S.zpos.alloc(size_t(3) * S.N);
     P.lo.upload(lo, S.stream);
     P.up.upload(up, S.stream);
     P.perm_fwd.upload(perm, S.stream);
@@ -524,6 +533,7 @@ struct Views {
   int lowp;
   SellView<__nv_bfloat16> lo16, up16;
   const float *alu32_f, *alu32_b;
+  R *zpos;  // the sweeps' intermediate in colour-position order (multicolour SSOR)
 };
 
 Views<double> views(Solver &S, double, int lowp = 0) {
@@ -532,7 +542,7 @@ Views<double> views(Solver &S, double, int lowp = 0) {
                        P.alu_shared ? P.alu_fwd.p : P.alu_bwd.p,
                        S.b.p, S.x.p, S.r.p, S.z.p, S.p.p, S.q.p, S.w.p, S.zp.p, S.zs.p, S.rold.p,
                        lowp, P.lo.view16(), P.up.view16(), P.alu32_fwd.p,
-                       P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p};
+                       P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p, S.zpos.p};
 }
 Views<float> views(Solver &S, float, int lowp = 0) {
   Precond &P = S.pc;
@@ -540,14 +550,14 @@ Views<float> views(Solver &S, float, int lowp = 0) {
                       P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p,
                       S.bf.p, S.xf.p, S.rf.p, S.zf.p, S.pf.p, S.qf.p, S.wf.p, S.zpf.p, S.zsf.p, S.roldf.p,
                       lowp, P.lo.view16(), P.up.view16(), P.alu32_fwd.p,
-                      P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p};
+                      P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p, S.zposf.p};
 }
 
 // z = M^-1 r, one pass; FUSE_RHO adds the RHO reduction + finisher.  K = lanes per
 // row of the sweep layouts.
-template <class R, class TV, class TA, bool FUSE_RHO, int K>
+template <class R, class TV, class TA, bool FUSE_RHO, int K, bool POS>
 void launch_sweep_k(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f, const TA *alu_b,
-                    const R *rin, R *zout, CgState *st) {
+                    const R *rin, R *zout, R *zpos, CgState *st) {
   Precond &P = S.pc;
   cudaStream_t s = S.stream;
   const int *perm_b = P.alu_shared ? P.perm_fwd.p : P.perm_bwd.p;
@@ -555,8 +565,8 @@ void launch_sweep_k(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, c
   for (int g = 0; g < gf; g++) {
     const int sb = P.lo.group_slice[g], se = P.lo.group_slice[g + 1];
     if (se <= sb) continue;
-    sweep_fwd_kernel<R, TV, TA, K><<<S.grid_sweep(se - sb), kThreads, 0, s>>>(lo, P.perm_fwd.p, alu_f, S.N, rin,
-                                                                              zout, sb, se, st);
+    sweep_fwd_kernel<R, TV, TA, K, POS><<<S.grid_sweep(se - sb), kThreads, 0, s>>>(lo, P.perm_fwd.p, alu_f, S.N,
+                                                                                   rin, zout, zpos, sb, se, st);
   }
   const int gb = int(P.up.group_slice.size()) - 1;
   int total = 0;
@@ -570,36 +580,43 @@ void launch_sweep_k(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, c
     const int grid = S.grid_sweep(std::max(se - sb, 1));
     // a group without slices still launches (one idle CTA) so that the reduction
     // ticket count stays exact
-    sweep_bwd_kernel<R, TV, TA, K, FUSE_RHO><<<grid, kThreads, 0, s>>>(up, perm_b, alu_b, S.N, rin, zout, sb, se,
-                                                                       st, S.partials.p, base, total);
+    sweep_bwd_kernel<R, TV, TA, K, FUSE_RHO, POS><<<grid, kThreads, 0, s>>>(up, perm_b, alu_b, S.N, rin, zout, zpos,
+                                                                            sb, se, st, S.partials.p, base, total);
     base += grid;
   }
 }
 
+// Lanes per row are 4, 8 or 16 (sweep_lanes()); POS for the multicolour SSOR layout
+// (columns renumbered to colour positions), node order for the ILU(0) levels.
 template <class R, class TV, class TA, bool FUSE_RHO>
 void launch_sweep_t(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f, const TA *alu_b,
-                    const R *rin, R *zout, CgState *st) {
+                    const R *rin, R *zout, R *zpos, CgState *st) {
   Precond &P = S.pc;
   if (P.kind == 3) {
     diag_kernel<R, TA, FUSE_RHO><<<S.grid_vec(), kThreads, 0, S.stream>>>(alu_f, S.N, rin, zout, st, S.partials.p);
     return;
   }
+  if (P.pos_cols) {
+    switch (P.lo.lanes) {
+      case 4: return launch_sweep_k<R, TV, TA, FUSE_RHO, 4, true>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
+      case 16: return launch_sweep_k<R, TV, TA, FUSE_RHO, 16, true>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
+      default: return launch_sweep_k<R, TV, TA, FUSE_RHO, 8, true>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
+    }
+  }
   switch (P.lo.lanes) {
-    case 1: return launch_sweep_k<R, TV, TA, FUSE_RHO, 1>(S, lo, up, alu_f, alu_b, rin, zout, st);
-    case 2: return launch_sweep_k<R, TV, TA, FUSE_RHO, 2>(S, lo, up, alu_f, alu_b, rin, zout, st);
-    case 4: return launch_sweep_k<R, TV, TA, FUSE_RHO, 4>(S, lo, up, alu_f, alu_b, rin, zout, st);
-    case 16: return launch_sweep_k<R, TV, TA, FUSE_RHO, 16>(S, lo, up, alu_f, alu_b, rin, zout, st);
-    case 32: return launch_sweep_k<R, TV, TA, FUSE_RHO, 32>(S, lo, up, alu_f, alu_b, rin, zout, st);
-    default: return launch_sweep_k<R, TV, TA, FUSE_RHO, 8>(S, lo, up, alu_f, alu_b, rin, zout, st);
+    case 4: return launch_sweep_k<R, TV, TA, FUSE_RHO, 4, false>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
+    case 16: return launch_sweep_k<R, TV, TA, FUSE_RHO, 16, false>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
+    default: return launch_sweep_k<R, TV, TA, FUSE_RHO, 8, false>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
   }
 }
 
 template <class R, bool FUSE_RHO>
 void launch_sweep(Solver &S, const Views<R> &V, const R *rin, R *zout, CgState *st) {
   if (V.lowp)
-    launch_sweep_t<R, __nv_bfloat16, float, FUSE_RHO>(S, V.lo16, V.up16, V.alu32_f, V.alu32_b, rin, zout, st);
+    launch_sweep_t<R, __nv_bfloat16, float, FUSE_RHO>(S, V.lo16, V.up16, V.alu32_f, V.alu32_b, rin, zout, V.zpos,
+                                                      st);
   else
-    launch_sweep_t<R, R, R, FUSE_RHO>(S, V.lo, V.up, V.alu_f, V.alu_b, rin, zout, st);
+    launch_sweep_t<R, R, R, FUSE_RHO>(S, V.lo, V.up, V.alu_f, V.alu_b, rin, zout, V.zpos, st);
 }
 
 // hecmw_precond_apply (hecmw_precond.f90:86-172): z = M^-1 r with iterPREmax passes.
@@ -906,7 +923,7 @@ void ensure_fp32(Solver &S) {
     P.fp32_version = P.numeric_version;
   }
   const size_t n3 = size_t(S.n3());
-  for (auto *v : {&S.bf, &S.xf, &S.rf, &S.zf, &S.pf, &S.qf, &S.wf, &S.zpf}) v->alloc(n3);
+  for (auto *v : {&S.bf, &S.xf, &S.rf, &S.zf, &S.pf, &S.qf, &S.wf, &S.zpf, &S.zposf}) v->alloc(n3);
 }
 
 // ---------------------------------------------------------------------------
@@ -1474,7 +1491,7 @@ int solve_mixed_reliable(Solver &S, int *Iarray, double *Rarray, int *iter, doub
 // ---------------------------------------------------------------------------
 // Multi-RHS CG: up to kMaxRhs load cases per pass over the matrix (h33_multi.cuh).
 
-template <int K, bool FUSE_RHO>
+template <int K, bool FUSE_RHO, bool POS>
 void launch_mr_sweep_k(Solver &S, const double *rin, double *zout) {
   Precond &P = S.pc;
   cudaStream_t s = S.stream;
@@ -1486,8 +1503,8 @@ void launch_mr_sweep_k(Solver &S, const double *rin, double *zout) {
   for (int g = 0; g < gf; g++) {
     const int sb = P.lo.group_slice[g], se = P.lo.group_slice[g + 1];
     if (se <= sb) continue;
-    mr_sweep_fwd_kernel<K><<<S.grid_mr((se - sb) * (32 / K)), kThreads, 0, s>>>(lo, P.perm_fwd.p, P.alu_fwd.p, S.N,
-                                                                             rin, zout, sb, se, ctl);
+    mr_sweep_fwd_kernel<K, POS><<<S.grid_mr((se - sb) * (32 / K)), kThreads, 0, s>>>(
+        lo, P.perm_fwd.p, P.alu_fwd.p, S.N, rin, zout, S.mzpos.p, sb, se, ctl);
   }
   const int gb = int(P.up.group_slice.size()) - 1;
   int total = 0;
@@ -1499,8 +1516,8 @@ void launch_mr_sweep_k(Solver &S, const double *rin, double *zout) {
   for (int g = gb - 1; g >= 0; g--) {
     const int sb = P.up.group_slice[g], se = P.up.group_slice[g + 1];
     const int grid = S.grid_mr(std::max(se - sb, 1) * (32 / K));
-    mr_sweep_bwd_kernel<K, FUSE_RHO><<<grid, kThreads, 0, s>>>(up, perm_b, alu_b, S.N, rin, zout, sb, se,
-                                                                S.mst.p, ctl, S.mpart.p, base, total);
+    mr_sweep_bwd_kernel<K, FUSE_RHO, POS><<<grid, kThreads, 0, s>>>(up, perm_b, alu_b, S.N, rin, zout, S.mzpos.p,
+                                                                     sb, se, S.mst.p, ctl, S.mpart.p, base, total);
     base += grid;
   }
 }
@@ -1513,13 +1530,17 @@ void launch_mr_sweep(Solver &S, const double *rin, double *zout) {
                                                                          S.mctl.p, S.mpart.p);
     return;
   }
+  if (P.pos_cols) {
+    switch (P.lo.lanes) {
+      case 4: return launch_mr_sweep_k<4, FUSE_RHO, true>(S, rin, zout);
+      case 16: return launch_mr_sweep_k<16, FUSE_RHO, true>(S, rin, zout);
+      default: return launch_mr_sweep_k<8, FUSE_RHO, true>(S, rin, zout);
+    }
+  }
   switch (P.lo.lanes) {
-    case 1: return launch_mr_sweep_k<1, FUSE_RHO>(S, rin, zout);
-    case 2: return launch_mr_sweep_k<2, FUSE_RHO>(S, rin, zout);
-    case 4: return launch_mr_sweep_k<4, FUSE_RHO>(S, rin, zout);
-    case 16: return launch_mr_sweep_k<16, FUSE_RHO>(S, rin, zout);
-    case 32: return launch_mr_sweep_k<32, FUSE_RHO>(S, rin, zout);
-    default: return launch_mr_sweep_k<8, FUSE_RHO>(S, rin, zout);
+    case 4: return launch_mr_sweep_k<4, FUSE_RHO, false>(S, rin, zout);
+    case 16: return launch_mr_sweep_k<16, FUSE_RHO, false>(S, rin, zout);
+    default: return launch_mr_sweep_k<8, FUSE_RHO, false>(S, rin, zout);
   }
 }
 
@@ -1629,7 +1650,7 @@ void build_graph_multi(Solver &S, int iterpremax, int nrhs) {
 
 void ensure_multi_buffers(Solver &S) {
   const size_t n48 = size_t(S.N) * kRhsStride;
-  for (auto *v : {&S.mb, &S.mx, &S.mr, &S.mz, &S.mp, &S.mq, &S.mw, &S.mzp}) v->alloc(n48);
+  for (auto *v : {&S.mb, &S.mx, &S.mr, &S.mz, &S.mp, &S.mq, &S.mw, &S.mzp, &S.mzpos}) v->alloc(n48);
   S.mst.alloc(kMaxRhs);
   S.mctl.alloc(1);
   S.mpart.alloc(size_t(mr_max_parts(S)) * kMaxRhs + 1024);
