@@ -71,9 +71,10 @@ __device__ __forceinline__ void mr_reduce_finish(double v, double *partials, int
 
 // Sum of A(row, :) x over the blocks of one row of a sliced layout with K lanes per
 // row (block k at slot slot0 + k/K, lane roff*K + k%K), for this lane's RHS.  The
-// 16 lanes of the half-warp first load 16 of the row's column indices at once (one
-// each) and pass them round by shuffles, so the x gathers of successive blocks do
-// not wait on one another's index loads.  hmask: this half-warp's lanes.
+// row is taken 16 blocks at a time: lane j of the half-warp loads block j's column
+// index and its nine entries (all issued at once), then every lane receives them by
+// shuffles, so inside a chunk only the x gathers touch memory.  hmask: this
+// half-warp's lanes.
 template <int K>
 __device__ __forceinline__ void mr_row(const SellView<double> &A, int s, int roff, int len, int l,
                                        unsigned hmask, const double *__restrict__ x, double &y0, double &y1,
@@ -82,23 +83,28 @@ __device__ __forceinline__ void mr_row(const SellView<double> &A, int s, int rof
   for (int k0 = 0; k0 < len; k0 += 16) {
     const int kn = min(16, len - k0);
     int myc = 0;
+    double mv[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) mv[e] = 0.0;
     if (l < kn) {
       const int k = k0 + l;
-      myc = __ldg(&A.col[(slot0 + k / K) * 32 + roff * K + (k & (K - 1))]);
+      const int sl = slot0 + k / K, lp = roff * K + (k & (K - 1));
+      myc = __ldg(&A.col[sl * 32 + lp]);
+      const double *v = A.val + sl * 288 + lp;
+#pragma unroll
+      for (int e = 0; e < 9; e++) mv[e] = __ldg(v + 32 * e);
     }
 #pragma unroll 4
     for (int kk = 0; kk < kn; kk++) {
-      const int k = k0 + kk;
       const int c = __shfl_sync(hmask, myc, kk, 16);
-      const double *v = A.val + (slot0 + k / K) * 288 + roff * K + (k & (K - 1));
       const double *xc = x + size_t(c) * kRhsStride + l;
       const double x0 = xc[0], x1 = xc[16], x2 = xc[32];
-      const double v0 = __ldg(v), v1 = __ldg(v + 32), v2 = __ldg(v + 64);
-      const double v3 = __ldg(v + 96), v4 = __ldg(v + 128), v5 = __ldg(v + 160);
-      const double v6 = __ldg(v + 192), v7 = __ldg(v + 224), v8 = __ldg(v + 256);
-      y0 = fma(v2, x2, fma(v1, x1, fma(v0, x0, y0)));
-      y1 = fma(v5, x2, fma(v4, x1, fma(v3, x0, y1)));
-      y2 = fma(v8, x2, fma(v7, x1, fma(v6, x0, y2)));
+      double v[9];
+#pragma unroll
+      for (int e = 0; e < 9; e++) v[e] = __shfl_sync(hmask, mv[e], kk, 16);
+      y0 = fma(v[2], x2, fma(v[1], x1, fma(v[0], x0, y0)));
+      y1 = fma(v[5], x2, fma(v[4], x1, fma(v[3], x0, y1)));
+      y2 = fma(v[8], x2, fma(v[7], x1, fma(v[6], x0, y2)));
     }
   }
 }
