@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--train-steps", type=int, default=60)
     ap.add_argument("--no-multi", action="store_true", help="skip the 16-load-case multi-RHS measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-system batched measurement")
+    ap.add_argument("--no-config3", action="store_true",
+                    help="skip the mixed-precision measurement on the jittered heterogeneous 80^3 system")
     ap.add_argument("--batch-systems", type=int, default=256)
     ap.add_argument("--batch-edges", default="8,40", help="element range per box edge of the batch")
     ap.add_argument("--spmv-only", type=int, default=0,
@@ -267,6 +269,38 @@ def bench_multi(solver, m, nrhs=16):
             "errors": sorted(set(int(v) for v in rec["errors"])), "gpu_launches": kernels,
             "workload": "%d random unit-norm tractions on the loaded face of the same matrix, CG+SSOR to 1e-8"
                         % nrhs}
+
+
+def bench_config3(tol=1e-10):
+    """Mixed precision on the harder system: 80x80x80 HEX8, interior nodes jittered by
+    +-0.2h, log-normal E (median 210000, sigma 1.0), nu uniform in [0.25, 0.40]
+    (seeded), same supports and load; FP64 CG+SSOR and the three mixed modes to 1e-10,
+    each with its error against the FP64 solution."""
+    import numpy as np
+    from frontistr_b200.mesh import box_system
+    from frontistr_b200.solver import GpuSolver
+    m = box_system(80, 80, 80, jitter=0.2, sigma_E=1.0, nu_range=(0.25, 0.40), seed=3)
+    out = {"workload": "80x80x80 HEX8, jitter 0.2h, log-normal E (sigma 1), nu U[0.25, 0.40], seed 3; "
+                       "CG+SSOR to %g" % tol, "dof": 3 * m.N, "modes": {}}
+    ref = None
+    with GpuSolver() as s:
+        for name, mode in (("fp64", 0), ("bf16_precond", 1), ("fp32_restart", 2), ("fp32_reliable", 3)):
+            recs = []
+            for _ in range(2):  # warm + timed
+                g = m.copy()
+                g.set_iter(40000)
+                g.set_resid(tol)
+                g.Iarray[41] = mode
+                rec = s.solve(g)
+                recs.append(rec)
+            info = s.last_solve_info()
+            if mode == 0:
+                ref = g.X.copy()
+            out["modes"][name] = {"s": recs[-1]["t_solve"], "iterations": int(recs[-1]["iter"]),
+                                  "outer": info["outer"], "error": int(recs[-1]["error"]),
+                                  "true_resid": info["true_resid"],
+                                  "rel_err_vs_fp64": float(np.linalg.norm(g.X - ref) / np.linalg.norm(ref))}
+    return out
 
 
 def bench_batched(args):
@@ -533,6 +567,7 @@ def main():
         e2e["value"] = float(vals[2])
 
     multi = None if args.no_multi else bench_multi(solver, m)
+    config3 = None if args.no_config3 else bench_config3()
     batched = None if args.no_batched else bench_batched(args)
 
     cpu = None
@@ -573,6 +608,7 @@ def main():
             "gpu_launches": variants[head]["kernels"] * args.steps,
             "clocks": clk,
             "multi_rhs": multi,
+            "mixed_config3": config3,
             "batched": batched,
         }
         print(json.dumps(line))
