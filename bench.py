@@ -566,6 +566,10 @@ def main():
     if e2e:
         e2e["value"] = float(vals[2])
 
+    if world > 1:
+        # the 16-load-case, batched and config-3 figures are single-GPU measurements
+        # reported at N = 1; replicas only repeat the headline
+        args.no_multi = args.no_batched = args.no_config3 = True
     multi = None if args.no_multi else bench_multi(solver, m)
     config3 = None if args.no_config3 else bench_config3()
     batched = None if args.no_batched else bench_batched(args)
