@@ -133,6 +133,16 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def max_over_ranks(values, dist, device):
+    """Every rank's timings -> the maximum over ranks (the job is as slow as its
+    slowest replica); identity without a process group."""
+    import torch
+    vals = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    return [float(v) for v in vals]
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -559,12 +569,9 @@ def main():
         e2e = {"value": statistics.mean(e2e_t), "unit": "s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "solver": head}
 
-    vals = torch.tensor([dev_s, wall, e2e["value"] if e2e else 0.0], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    dev_s, wall = float(vals[0]), float(vals[1])
+    dev_s, wall, e2e_v = max_over_ranks([dev_s, wall, e2e["value"] if e2e else 0.0], dist, dev)
     if e2e:
-        e2e["value"] = float(vals[2])
+        e2e["value"] = e2e_v
 
     if world > 1:
         # the 16-load-case, batched and config-3 figures are single-GPU measurements
