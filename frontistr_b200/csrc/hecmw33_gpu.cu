@@ -60,8 +60,8 @@ constexpr int kStreamChunk = 16;
 // a tenth of the rows, too few one-lane rows to cover HBM latency.
 int sweep_lanes() {
   const char *e = std::getenv("HECMW33_SWEEP_LANES");
-  const int k = e ? std::atoi(e) : 8;
-  return (k == 4 || k == 8 || k == 16) ? k : 8;
+  const int k = e ? std::atoi(e) : 4;
+  return (k == 4 || k == 8 || k == 16) ? k : 4;
 }
 
 double wall() {
