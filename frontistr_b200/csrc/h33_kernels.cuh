@@ -295,6 +295,39 @@ __device__ __forceinline__ void row_gemv(const SellView<TV> &A, int s, int lane,
   }
 }
 
+// row_gemv for a uniform layout: every row of the slice owns nslots slots starting
+// at slot0, padded with zero blocks (column 0), so the loop needs no row length.
+// Padding adds exact zeros; the real blocks are summed in row_gemv's order.
+template <class R, class TV, int K, bool BACKWARD>
+__device__ __forceinline__ void row_gemv_u(const SellView<TV> &A, int slot0, int nslots, int lane,
+                                           const R *__restrict__ x, R &y0, R &y1, R &y2) {
+#pragma unroll 4
+  for (int kk = 0; kk < nslots; kk++) {
+    const int sl = slot0 + (BACKWARD ? nslots - 1 - kk : kk);
+    const int c = __ldg(&A.col[sl * 32 + lane]);
+    const TV *v = A.val + sl * 288 + lane;
+    const R x0 = __ldg(&x[3 * c]), x1 = __ldg(&x[3 * c + 1]), x2 = __ldg(&x[3 * c + 2]);
+    const R v0 = ld_val<R>(v), v1 = ld_val<R>(v + 32), v2 = ld_val<R>(v + 64);
+    const R v3 = ld_val<R>(v + 96), v4 = ld_val<R>(v + 128), v5 = ld_val<R>(v + 160);
+    const R v6 = ld_val<R>(v + 192), v7 = ld_val<R>(v + 224), v8 = ld_val<R>(v + 256);
+    y0 = fma(v2, x2, fma(v1, x1, fma(v0, x0, y0)));
+    y1 = fma(v5, x2, fma(v4, x1, fma(v3, x0, y1)));
+    y2 = fma(v8, x2, fma(v7, x1, fma(v6, x0, y2)));
+  }
+#pragma unroll
+  for (int o = K / 2; o > 0; o >>= 1) {
+    y0 += __shfl_xor_sync(0xffffffffu, y0, o);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, o);
+    y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+  }
+}
+
+// Launch parameters of one colour of a uniform layout: rows [row0, row1) in slices of
+// 32/K rows, slice j of the colour starting at slot slot0 + j*len.
+struct GroupShape {
+  int row0, row1, slot0, len;
+};
+
 // ---- kernels ---------------------------------------------------------------
 
 // Scatter raw hecmwST blocks (D|AL|AU, 9 doubles each) into a sliced layout.
@@ -389,16 +422,17 @@ __global__ void __launch_bounds__(kThreads) sweep_fwd_kernel(SellView<TV> L, con
                                                              const TA *__restrict__ alu, int npos,
                                                              const R *__restrict__ r, R *__restrict__ z,
                                                              R *__restrict__ zpos, int sbeg, int send,
-                                                             const CgState *st) {
+                                                             GroupShape gs, const CgState *st) {
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
   const int roff = lane / K;
   const bool leader = (lane & (K - 1)) == 0;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
-    const bool active = roff < L.nrows[s];
-    const int row = L.row0[s] + roff;
-    const int len = active ? L.rowlen[s * 32 + roff] : 0;
+    // POS layouts are uniform: the slice's rows and slots follow from its index
+    const int row = POS ? gs.row0 + (s - sbeg) * (32 / K) + roff : L.row0[s] + roff;
+    const bool active = POS ? row < gs.row1 : roff < L.nrows[s];
+    const int len = (!POS && active) ? L.rowlen[s * 32 + roff] : 0;
     R r0 = 0, r1 = 0, r2 = 0;
     int node = 0;
     if (POS && active && leader) {
@@ -408,7 +442,8 @@ __global__ void __launch_bounds__(kThreads) sweep_fwd_kernel(SellView<TV> L, con
       r2 = r[3 * node + 2];
     }
     R a0 = 0, a1 = 0, a2 = 0;
-    row_gemv<R, TV, K, false>(L, s, lane, len, POS ? zpos : z, a0, a1, a2);
+    if (POS) row_gemv_u<R, TV, K, false>(L, gs.slot0 + (s - sbeg) * gs.len, gs.len, lane, zpos, a0, a1, a2);
+    else row_gemv<R, TV, K, false>(L, s, lane, len, z, a0, a1, a2);
     if (active && leader) {
       if (!POS) {
         node = perm[row];
@@ -435,8 +470,8 @@ template <class R, class TV, class TA, int K, bool FUSE_RHO, bool POS>
 __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, const int *__restrict__ perm,
                                                              const TA *__restrict__ alu, int npos,
                                                              const R *__restrict__ r, R *__restrict__ z,
-                                                             R *__restrict__ zpos, int sbeg, int send, CgState *st,
-                                                             double *partials, int part_base,
+                                                             R *__restrict__ zpos, int sbeg, int send, GroupShape gs,
+                                                             CgState *st, double *partials, int part_base,
                                                              int part_total) {
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
@@ -445,9 +480,9 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, con
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double dot = 0.0;
   for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
-    const bool active = roff < U.nrows[s];
-    const int row = U.row0[s] + roff;
-    const int len = active ? U.rowlen[s * 32 + roff] : 0;
+    const int row = POS ? gs.row0 + (s - sbeg) * (32 / K) + roff : U.row0[s] + roff;
+    const bool active = POS ? row < gs.row1 : roff < U.nrows[s];
+    const int len = (!POS && active) ? U.rowlen[s * 32 + roff] : 0;
     int node = 0;
     R c0 = 0, c1 = 0, c2 = 0;  // this row's current z (written by the forward sweep)
     if (POS && active && leader) {
@@ -457,7 +492,8 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, con
       c2 = zpos[3 * row + 2];
     }
     R x1 = 0, x2 = 0, x3 = 0;
-    row_gemv<R, TV, K, true>(U, s, lane, len, POS ? zpos : z, x1, x2, x3);
+    if (POS) row_gemv_u<R, TV, K, true>(U, gs.slot0 + (s - sbeg) * gs.len, gs.len, lane, zpos, x1, x2, x3);
+    else row_gemv<R, TV, K, true>(U, s, lane, len, z, x1, x2, x3);
     if (active && leader) {
       if (!POS) {
         node = perm[row];

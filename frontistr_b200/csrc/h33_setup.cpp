@@ -279,18 +279,27 @@ void reordered_rows(const Profile &p, const std::vector<int> &perm, const std::v
   }
 }
 
-void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out, int lanes) {
+void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out, int lanes,
+                bool uniform) {
   if (lanes < 1 || lanes > 32 || (32 % lanes) != 0) throw std::runtime_error("lanes per row must divide 32");
   out = SellLayout();
   out.lanes = lanes;
   const int per_slice = 32 / lanes;
   const int ngroups = int(group_rows.size()) - 1;
   out.group_slice.assign(size_t(ngroups) + 1, 0);
+  out.group_slot0.assign(size_t(ngroups), 0);
+  out.group_len.assign(size_t(ngroups), 0);
   for (int g = 0; g < ngroups; g++) {
+    int glen = 0;
+    if (uniform)
+      for (int r = group_rows[g]; r < group_rows[g + 1]; r++)
+        glen = std::max(glen, int((rows.ptr[r + 1] - rows.ptr[r] + lanes - 1) / lanes));
+    out.group_slot0[g] = int(out.nslots);
+    out.group_len[g] = glen;
     for (int r0 = group_rows[g]; r0 < group_rows[g + 1]; r0 += per_slice) {
       const int nr = std::min(per_slice, group_rows[g + 1] - r0);
-      int len = 0;
-      for (int l = 0; l < nr; l++) {
+      int len = glen;
+      for (int l = 0; l < nr && !uniform; l++) {
         const int n = int(rows.ptr[r0 + l + 1] - rows.ptr[r0 + l]);
         len = std::max(len, (n + lanes - 1) / lanes);
       }

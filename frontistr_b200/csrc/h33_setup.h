@@ -63,10 +63,13 @@ struct SellLayout {
   std::vector<int> rowlen;                    // per slice*32 + row offset (blocks in the row)
   std::vector<int> col, src;                  // per slot*32 + lane (pad: col 0, src -1)
   std::vector<int> group_slice;               // group g -> slices [group_slice[g], group_slice[g+1])
+  std::vector<int> group_slot0, group_len;    // uniform layouts: first slot and slots per slice of group g
 };
 // group_rows: row boundaries of the groups (size ngroups+1, rows 0..nrows-1).
+// uniform: every slice of a group gets the group's largest slot count, so that a
+// slice's first slot and rows follow from its index (padding: column 0, no value).
 void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out,
-                int lanes = 1);
+                int lanes = 1, bool uniform = false);
 
 // Block ILU(0) in natural order (FORM_ILU0_33, hecmw_precond_BILU_33.f90:185-362),
 // computed on the host from the hecmwST arrays.  Outputs the factor blocks in the

@@ -76,7 +76,7 @@ struct DevSell {
   DevArray<T> val;
   DevArray<float> val32;  // FP32 copy of val (mixed precision), same layout
   DevArray<__nv_bfloat16> val16;  // BF16 copy of val (low-precision preconditioner), same layout
-  std::vector<int> group_slice;
+  std::vector<int> group_slice, group_rows, group_slot0, group_len;
 
   int lanes = 1;
   void upload(const SellLayout &L, cudaStream_t s) {
@@ -92,6 +92,8 @@ struct DevSell {
     src.upload(L.src, s);
     val.alloc(size_t(nslots) * 288);
     group_slice = L.group_slice;
+    group_slot0 = L.group_slot0;
+    group_len = L.group_len;
   }
   SellView<T> view() const {
     return SellView<T>{nslices, row0.p, nrows.p, slot0.p, len.p, rowlen.p, col.p, val.p};
@@ -382,12 +384,16 @@ void setup_ssor(Solver &S, int ncolor_in, double sigma, bool symbolic) {
     for (auto *br : {&lower, &upper})
       for (int &c : br->col) c = iperm[c];
     SellLayout lo, up;
-    build_sell(lower, colorindex, lo, sweep_lanes());
-    build_sell(upper, colorindex, up, sweep_lanes());
+    build_sell(lower, colorindex, lo, sweep_lanes(), true);
+    build_sell(upper, colorindex, up, sweep_lanes(), true);
     P.pos_cols = true;
+    // padding blocks gather zpos[0]: it must hold finite values from the start
     S.zpos.alloc(size_t(3) * S.N);
+    S.zpos.zero(S.stream);
     P.lo.upload(lo, S.stream);
     P.up.upload(up, S.stream);
+    P.lo.group_rows = colorindex;
+    P.up.group_rows = colorindex;
     P.perm_fwd.upload(perm, S.stream);
     P.colorindex = colorindex;
     P.perm = perm;
@@ -565,8 +571,11 @@ void launch_sweep_k(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, c
   for (int g = 0; g < gf; g++) {
     const int sb = P.lo.group_slice[g], se = P.lo.group_slice[g + 1];
     if (se <= sb) continue;
+    const GroupShape gsh = POS ? GroupShape{P.lo.group_rows[g], P.lo.group_rows[g + 1], P.lo.group_slot0[g],
+                                            P.lo.group_len[g]}
+                               : GroupShape{0, 0, 0, 0};
     sweep_fwd_kernel<R, TV, TA, K, POS><<<S.grid_sweep(se - sb), kThreads, 0, s>>>(lo, P.perm_fwd.p, alu_f, S.N,
-                                                                                   rin, zout, zpos, sb, se, st);
+                                                                                   rin, zout, zpos, sb, se, gsh, st);
   }
   const int gb = int(P.up.group_slice.size()) - 1;
   int total = 0;
@@ -580,8 +589,12 @@ void launch_sweep_k(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, c
     const int grid = S.grid_sweep(std::max(se - sb, 1));
     // a group without slices still launches (one idle CTA) so that the reduction
     // ticket count stays exact
+    const GroupShape gsh = POS ? GroupShape{P.up.group_rows[g], P.up.group_rows[g + 1], P.up.group_slot0[g],
+                                            P.up.group_len[g]}
+                               : GroupShape{0, 0, 0, 0};
     sweep_bwd_kernel<R, TV, TA, K, FUSE_RHO, POS><<<grid, kThreads, 0, s>>>(up, perm_b, alu_b, S.N, rin, zout, zpos,
-                                                                            sb, se, st, S.partials.p, base, total);
+                                                                            sb, se, gsh, st, S.partials.p, base,
+                                                                            total);
     base += grid;
   }
 }
@@ -923,7 +936,11 @@ void ensure_fp32(Solver &S) {
     P.fp32_version = P.numeric_version;
   }
   const size_t n3 = size_t(S.n3());
-  for (auto *v : {&S.bf, &S.xf, &S.rf, &S.zf, &S.pf, &S.qf, &S.wf, &S.zpf, &S.zposf}) v->alloc(n3);
+  for (auto *v : {&S.bf, &S.xf, &S.rf, &S.zf, &S.pf, &S.qf, &S.wf, &S.zpf}) v->alloc(n3);
+  if (S.zposf.n != n3) {
+    S.zposf.alloc(n3);
+    S.zposf.zero(S.stream);  // padding blocks gather zposf[0]
+  }
 }
 
 // ---------------------------------------------------------------------------
