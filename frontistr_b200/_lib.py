@@ -43,6 +43,13 @@ def assemble_lib():
         lib.fistr_mat_ass_bc.restype = None
         lib.fistr_mat_ass_bc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, _i32p, _i32p,
                                          _i32p, _i32p, _f64p, _f64p, _f64p, _f64p]
+        lib.fistr_mat_ass_bc_list.restype = None
+        lib.fistr_mat_ass_bc_list.argtypes = [ctypes.c_int, _i32p, _i32p, _f64p, _i32p, _i32p, _i32p, _i32p,
+                                              _f64p, _f64p, _f64p, _f64p]
+        lib.fistr_box_neohooke.restype = ctypes.c_int
+        lib.fistr_box_neohooke.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_double, _f64p, _i32p, _i32p, _i32p, _i32p,
+                                           _f64p, _f64p, _f64p, _f64p]
         _asm = lib
     return _asm
 

@@ -13,6 +13,10 @@
 //   isotropic D      fistr1/src/lib/physics/ElasticLinear.f90:38-60 (bulk/shear form)
 //   scatter          hecmw1/src/solver/matrix/hecmw_mat_ass.f90:32-135 (row-major blocks)
 //   boundary cond.   hecmw1/src/solver/matrix/hecmw_mat_ass.f90:328-463 (hecmw_mat_ass_bc)
+//   Neo-Hookean      fistr1/src/lib/physics/Hyperelastic.f90:286-381 (compressible
+//                    NEOHOOKE: W = C10 (I1bar - 3) + (J - 1)^2 / D1), total-Lagrangian
+//                    element forces and tangent in the manner of fistr1/src/lib/static_LIB_3d.f90
+//                    (TOTALLAG), with the material tangent derived from W (below)
 //
 // Node ids are 1-based in every array that leaves this file (itemL/itemU), as in
 // hecmwST_matrix; element connectivity passed in is 0-based.
@@ -146,6 +150,130 @@ void stiff_tet4(const double x[4][3], double E, double nu, double *K) {
   double gderiv[4][3];
   const double det = global_deriv<4>(deriv, x, gderiv);
   add_btdb<4>(gderiv, D, det / 6.0, K);
+}
+
+// ---- compressible Neo-Hookean, total Lagrangian --------------------------------
+// Voigt order of symmetric tensors: 11, 22, 33, 12, 23, 31 (as the linear element).
+const int kVi[6] = {0, 1, 2, 0, 1, 2}, kVj[6] = {0, 1, 2, 1, 2, 0};
+
+// Second Piola-Kirchhoff stress S and material tangent D = 2 dS/dC (Voigt, D_vw =
+// C_IJKL) of W = C10 (J^-2/3 I1 - 3) + (J - 1)^2 / D1 at deformation gradient F:
+//   S = 2 C10 J^-2/3 (I - I1/3 C^-1) + p C^-1,            p = 2/D1 (J - 1) J
+//   D = -4C10/3 J^-2/3 (I (x) C^-1 + C^-1 (x) I) + 4C10/9 J^-2/3 I1 C^-1 (x) C^-1
+//       + 4C10/3 J^-2/3 I1 Ic + 2/D1 (2J - 1) J C^-1 (x) C^-1 - 2p Ic,
+//   Ic_IJKL = (C^-1_IK C^-1_JL + C^-1_IL C^-1_JK) / 2.
+// Returns J.
+double neohooke_stress(const double F[3][3], double C10, double D1, double S[6], double D[6][6]) {
+  double C[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double s = 0.0;
+      for (int k = 0; k < 3; k++) s += F[k][i] * F[k][j];
+      C[i][j] = s;
+    }
+  const double J = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) -
+                   F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+                   F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+  const double detC = J * J;
+  double Ci[3][3];
+  Ci[0][0] = (C[1][1] * C[2][2] - C[1][2] * C[2][1]) / detC;
+  Ci[0][1] = (C[0][2] * C[2][1] - C[0][1] * C[2][2]) / detC;
+  Ci[0][2] = (C[0][1] * C[1][2] - C[0][2] * C[1][1]) / detC;
+  Ci[1][0] = Ci[0][1];
+  Ci[1][1] = (C[0][0] * C[2][2] - C[0][2] * C[2][0]) / detC;
+  Ci[1][2] = (C[0][2] * C[1][0] - C[0][0] * C[1][2]) / detC;
+  Ci[2][0] = Ci[0][2];
+  Ci[2][1] = Ci[1][2];
+  Ci[2][2] = (C[0][0] * C[1][1] - C[0][1] * C[1][0]) / detC;
+  const double I1 = C[0][0] + C[1][1] + C[2][2];
+  const double j23 = std::pow(J, -2.0 / 3.0);
+  const double a = 2.0 * C10, p = 2.0 / D1 * (J - 1.0) * J;
+  const double q = 2.0 / D1 * (2.0 * J - 1.0) * J;
+  for (int v = 0; v < 6; v++) {
+    const int I = kVi[v], Jv = kVj[v];
+    const double dIJ = I == Jv ? 1.0 : 0.0;
+    S[v] = a * j23 * (dIJ - I1 / 3.0 * Ci[I][Jv]) + p * Ci[I][Jv];
+    for (int w = 0; w < 6; w++) {
+      const int K = kVi[w], L = kVj[w];
+      const double dKL = K == L ? 1.0 : 0.0;
+      const double Ic = 0.5 * (Ci[I][K] * Ci[Jv][L] + Ci[I][L] * Ci[Jv][K]);
+      D[v][w] = -(2.0 * a / 3.0) * j23 * (dIJ * Ci[K][L] + Ci[I][Jv] * dKL) +
+                (2.0 * a / 9.0) * j23 * I1 * Ci[I][Jv] * Ci[K][L] + (2.0 * a / 3.0) * j23 * I1 * Ic +
+                q * Ci[I][Jv] * Ci[K][L] - 2.0 * p * Ic;
+    }
+  }
+  return J;
+}
+
+// HEX8 element at nodal displacements u (reference coordinates X), 2x2x2 Gauss:
+// internal force fint (24) and tangent K (24x24 row-major, material + geometric).
+// Returns 0, or 1 when J <= 0 at a Gauss point (inverted element).
+int neohooke_hex8(const double X[8][3], const double u[8][3], double C10, double D1, double *K,
+                  double *fint) {
+  static const double sgn[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                   {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+  std::memset(K, 0, sizeof(double) * 576);
+  std::memset(fint, 0, sizeof(double) * 24);
+  const double g = 1.0 / std::sqrt(3.0);
+  const double gp[2] = {-g, g};
+  int bad = 0;
+  for (int lz = 0; lz < 2; lz++)
+    for (int ly = 0; ly < 2; ly++)
+      for (int lx = 0; lx < 2; lx++) {
+        const double xi[3] = {gp[lx], gp[ly], gp[lz]};
+        double deriv[8][3];
+        for (int a = 0; a < 8; a++) {
+          const double f0 = 1.0 + sgn[a][0] * xi[0], f1 = 1.0 + sgn[a][1] * xi[1],
+                       f2 = 1.0 + sgn[a][2] * xi[2];
+          deriv[a][0] = 0.125 * sgn[a][0] * f1 * f2;
+          deriv[a][1] = 0.125 * sgn[a][1] * f0 * f2;
+          deriv[a][2] = 0.125 * sgn[a][2] * f0 * f1;
+        }
+        double N[8][3];  // dN_a / dX_J
+        const double w = global_deriv<8>(deriv, X, N);
+        double F[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+        for (int a = 0; a < 8; a++)
+          for (int i = 0; i < 3; i++)
+            for (int J = 0; J < 3; J++) F[i][J] += u[a][i] * N[a][J];
+        double S[6], D[6][6];
+        if (neohooke_stress(F, C10, D1, S, D) <= 0.0) bad = 1;
+        // B (6 x 24): dE_v / du_ak, engineering shear
+        double B[6][24];
+        for (int a = 0; a < 8; a++)
+          for (int k = 0; k < 3; k++)
+            for (int v = 0; v < 6; v++) {
+              const int I = kVi[v], J = kVj[v];
+              B[v][3 * a + k] = I == J ? F[k][I] * N[a][I] : F[k][I] * N[a][J] + F[k][J] * N[a][I];
+            }
+        for (int c = 0; c < 24; c++) {
+          double f = 0.0;
+          for (int v = 0; v < 6; v++) f += B[v][c] * S[v];
+          fint[c] += w * f;
+        }
+        double DB[6][24];
+        for (int v = 0; v < 6; v++)
+          for (int c = 0; c < 24; c++) {
+            double t = 0.0;
+            for (int x = 0; x < 6; x++) t += D[v][x] * B[x][c];
+            DB[v][c] = t;
+          }
+        for (int r = 0; r < 24; r++)
+          for (int c = 0; c < 24; c++) {
+            double t = 0.0;
+            for (int v = 0; v < 6; v++) t += B[v][r] * DB[v][c];
+            K[r * 24 + c] += w * t;
+          }
+        // geometric part: (N_a,I S_IJ N_b,J) on the diagonal of every 3x3 block
+        const double Sm[3][3] = {{S[0], S[3], S[5]}, {S[3], S[1], S[4]}, {S[5], S[4], S[2]}};
+        for (int a = 0; a < 8; a++)
+          for (int b = 0; b < 8; b++) {
+            double gab = 0.0;
+            for (int I = 0; I < 3; I++)
+              for (int J = 0; J < 3; J++) gab += N[a][I] * Sm[I][J] * N[b][J];
+            for (int k = 0; k < 3; k++) K[(3 * a + k) * 24 + 3 * b + k] += w * gab;
+          }
+      }
+  return bad;
 }
 
 int find_col(const int *item, int is, int ie, int key) {
@@ -326,6 +454,14 @@ void fistr_mat_ass_bc(int inode, int idof, double RHS, const int *indexL, const 
   }
 }
 
+// hecmw_mat_ass_bc for n (node, dof, value) triples in order (node 1-based, dof 1..3).
+void fistr_mat_ass_bc_list(int n, const int *inode, const int *idof, const double *value, const int *indexL,
+                           const int *itemL, const int *indexU, const int *itemU, double *D, double *AL,
+                           double *AU, double *B) {
+  for (int k = 0; k < n; k++)
+    fistr_mat_ass_bc(inode[k], idof[k], value[k], indexL, itemL, indexU, itemU, D, AL, AU, B);
+}
+
 // ---------------------------------------------------------------------------
 // Structured HEX8 boxes: nx*ny*nz unit cubes of edge h, nodes numbered
 // lexicographically (x fastest), elements likewise, hex8n node order.
@@ -341,6 +477,73 @@ int fistr_box_counts(int nx, int ny, int nz, int *n_node, int *NPL, int *NPU) {
   *NPL = int((nz_blocks - nnode) / 2);
   *NPU = *NPL;
   return 0;
+}
+
+// Tangent stiffness and residual of a compressible Neo-Hookean HEX8 box (edge h,
+// nodes as in fistr_box_assemble) at the nodal displacements U (3 per node):
+// D/AL/AU = K(U), R = -f_int(U) (no external load: the Newton sequence drives the
+// block by prescribed displacements).  Returns 0, or the number of elements with
+// J <= 0 at a Gauss point.
+int fistr_box_neohooke(int nx, int ny, int nz, double h, double C10, double D1, const double *U, int *indexL,
+                       int *itemL, int *indexU, int *itemU, double *D, double *AL, double *AU, double *R) {
+  const int nx1 = nx + 1, ny1 = ny + 1, nz1 = nz + 1;
+  const int n_node = nx1 * ny1 * nz1;
+  auto nid = [&](int ix, int iy, int iz) { return ix + nx1 * (iy + ny1 * iz); };
+  indexL[0] = indexU[0] = 0;
+  {
+    int cl = 0, cu = 0;
+    for (int iz = 0; iz < nz1; iz++)
+      for (int iy = 0; iy < ny1; iy++)
+        for (int ix = 0; ix < nx1; ix++) {
+          const int self = nid(ix, iy, iz);
+          for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+              for (int dx = -1; dx <= 1; dx++) {
+                const int jx = ix + dx, jy = iy + dy, jz = iz + dz;
+                if (jx < 0 || jx > nx || jy < 0 || jy > ny || jz < 0 || jz > nz) continue;
+                const int j = nid(jx, jy, jz);
+                if (j < self) itemL[cl++] = j + 1;
+                else if (j > self) itemU[cu++] = j + 1;
+              }
+          indexL[self + 1] = cl;
+          indexU[self + 1] = cu;
+        }
+  }
+  const size_t NPL = size_t(indexL[n_node]), NPU = size_t(indexU[n_node]);
+  std::memset(D, 0, sizeof(double) * 9 * size_t(n_node));
+  std::memset(AL, 0, sizeof(double) * 9 * NPL);
+  std::memset(AU, 0, sizeof(double) * 9 * NPU);
+  std::memset(R, 0, sizeof(double) * 3 * size_t(n_node));
+  Csr m{n_node, indexL, itemL, indexU, itemU, D, AL, AU};
+  int bad = 0;
+  for (int color = 0; color < 8; color++) {
+    const int px = color & 1, py = (color >> 1) & 1, pz = (color >> 2) & 1;
+#pragma omp parallel for collapse(2) schedule(static) reduction(+ : bad)
+    for (int ez = pz; ez < nz; ez += 2)
+      for (int ey = py; ey < ny; ey += 2) {
+        double Kl[576], fl[24];
+        for (int ex = px; ex < nx; ex += 2) {
+          const int nodes[8] = {nid(ex, ey, ez),         nid(ex + 1, ey, ez),
+                                nid(ex + 1, ey + 1, ez), nid(ex, ey + 1, ez),
+                                nid(ex, ey, ez + 1),     nid(ex + 1, ey, ez + 1),
+                                nid(ex + 1, ey + 1, ez + 1), nid(ex, ey + 1, ez + 1)};
+          const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                 {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+          double X[8][3], u[8][3];
+          for (int a = 0; a < 8; a++) {
+            X[a][0] = (ex + off[a][0]) * h;
+            X[a][1] = (ey + off[a][1]) * h;
+            X[a][2] = (ez + off[a][2]) * h;
+            for (int d = 0; d < 3; d++) u[a][d] = U[3 * size_t(nodes[a]) + d];
+          }
+          bad += neohooke_hex8(X, u, C10, D1, Kl, fl);
+          scatter(m, 8, nodes, Kl);
+          for (int a = 0; a < 8; a++)
+            for (int d = 0; d < 3; d++) R[3 * size_t(nodes[a]) + d] -= fl[3 * a + d];
+        }
+      }
+  }
+  return bad;
 }
 
 // params: [0]=h, [1]=E0, [2]=nu0, [3]=load_y, [4]=jitter fraction (0 = none),
