@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--batch-edges", default="8,40", help="element range per box edge of the batch")
     ap.add_argument("--spmv-only", type=int, default=0,
                     help="only build the system and run this many SpMV launches (profiling)")
+    ap.add_argument("--learned-newton", action="store_true",
+                    help="the learned preconditioner in a Neo-Hookean Newton sequence (prints its own JSON line)")
+    ap.add_argument("--newton-mesh", default="64,64,64")
     ap.add_argument("--profile-solve", action="store_true",
                     help="one solve capped at 5 CG iterations, nothing printed (profiling)")
     ap.add_argument("--profile-multi", action="store_true",
@@ -313,6 +316,80 @@ def bench_config3(tol=1e-10):
     return out
 
 
+def bench_learned_newton(args):
+    """The learned preconditioner where the network is meant to live: a Newton
+    sequence.  64x64x64 compressible Neo-Hookean block (C10 = 1.0, D1 = 0.01, h = 1),
+    clamped at z = 0, top face held in x, y and moved down by 10 % of the height over
+    12 equal increments.  Increments 1-4 are solved with plain FP64 CG + SSOR while
+    (r, e) pairs are recorded; the network is trained on them on the GPU; every
+    tangent system of increments 5-12 is solved both ways (plain, and flexible CG
+    with the network), and the learned solution advances the sequence."""
+    import numpy as np
+    from frontistr_b200.newton import NeoHookeBox, newton_sequence
+    from frontistr_b200.solver import GpuSolver
+    nx, ny, nz = (int(v) for v in args.newton_mesh.split(","))
+    box = NeoHookeBox(nx, ny, nz, h=1.0, C10=1.0, D1=0.01)
+    top_uz = -0.1 * nz
+    rows = []
+    train = {}
+    t_asm = [0.0]
+    s = GpuSolver()
+    s.learn_record(1, max_pairs=32)
+
+    first = [True]
+
+    def solve(inc, it, m):
+        m.set_iter(40000)
+        m.set_resid(args.tol)
+        if not first[0]:
+            m.Iarray[97] = 0  # same structure: keep the orderings and layouts
+            m.Iarray[96] = 2  # new tangent values: rebuild the preconditioner numerically
+        first[0] = False
+        if inc == 5 and it == 1 and not train:
+            n = s.learn_record(0)
+            t0 = time.perf_counter()
+            l0, l1 = s.learn_train(steps=args.train_steps, lr=2e-3)
+            train.update(pairs=n, steps=args.train_steps, loss_before=l0, loss_after=l1,
+                         train_s=time.perf_counter() - t0)
+        rec = {"increment": inc, "newton": it}
+        if inc >= 5:
+            g = m.copy()
+            r = s.solve(g)
+            rec["plain"] = {"iter": int(r["iter"]), "s": float(r["t_solve"]), "error": int(r["error"]),
+                            "true_resid": s.last_solve_info()["true_resid"]}
+            g = m.copy()
+            g.Iarray[42] = 1
+            r = s.solve(g)
+            info = s.last_solve_info()
+            rec["learned"] = {"iter": int(r["iter"]), "s": float(r["t_solve"]), "error": int(r["error"]),
+                              "true_resid": info["true_resid"], "fallback_iter": info["fallback"]}
+        else:
+            g = m.copy()
+            r = s.solve(g)
+            rec["plain"] = {"iter": int(r["iter"]), "s": float(r["t_solve"]), "error": int(r["error"]),
+                            "true_resid": s.last_solve_info()["true_resid"]}
+        rows.append(rec)
+        return g.X.copy()
+
+    t0 = time.perf_counter()
+    steps = list(newton_sequence(box, solve, top_uz=top_uz, n_incr=12, max_newton=6, tol=1e-6))
+    wall = time.perf_counter() - t0
+    s.close()
+    late = [r for r in rows if "learned" in r]
+    sum_plain = sum(r["plain"]["s"] for r in late)
+    sum_learned = sum(r["learned"]["s"] for r in late)
+    return {"impl": "ours", "workload": "%dx%dx%d Neo-Hookean HEX8 (C10 1.0, D1 0.01), top z displaced by %g "
+                                        "in 12 increments; CG+SSOR to %g" % (nx, ny, nz, top_uz, args.tol),
+            "dof": 3 * box.N, "newton_systems": len(rows), "training": train,
+            "increments_5_12": {"systems": len(late), "plain_s": sum_plain, "learned_s": sum_learned,
+                                "plain_iterations": sum(r["plain"]["iter"] for r in late),
+                                "learned_iterations": sum(r["learned"]["iter"] for r in late),
+                                "speedup": sum_plain / sum_learned if sum_learned else None,
+                                "max_true_resid_learned": max(r["learned"]["true_resid"] for r in late)},
+            "newton": [{"increment": x["increment"], "newton": x["newton"], "residual": x["residual"]}
+                       for x in steps], "systems": rows, "wall_s": wall}
+
+
 def bench_batched(args):
     """Independent boxes (edges uniform in [8, 40] elements, E log-uniform in
     [1e3, 1e6], nu in [0.2, 0.45], random traction on the top face; seeded) solved
@@ -388,6 +465,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.learned_newton:
+        if rank == 0:
+            print(json.dumps(bench_learned_newton(args)))
+        return
 
     import numpy as np
     import torch
