@@ -13,6 +13,16 @@
 
 namespace h33 {
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start while its predecessor drains; it waits here until the
+// predecessor grid has completed and its writes are visible, then lets its own
+// successor start launching.  Without the launch attribute both are no-ops.  Every
+// kernel of the solver calls this first, before it reads anything.
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" :::);
+}
+
 // Slice height of the sliced block-ELL layout: one warp lane per block row.
 constexpr int kSlice = 32;
 // Threads per CTA for the sliced kernels (8 slices per CTA).

@@ -73,6 +73,7 @@ __device__ __forceinline__ float wload<__nv_bfloat16>(const __nv_bfloat16 *p) {
 // w[l][e] = tanh(u_l . feat_e + c_l) for all layers
 template <class W>
 __global__ void gnn_edge_weights_kernel(GnnGraph g, const W *__restrict__ theta, float *__restrict__ w) {
+  pdl_entry();
   const GnnOffsets o = GnnOffsets::make();
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.nedges; e += gridDim.x * blockDim.x) {
     float f[9];
@@ -90,6 +91,7 @@ __global__ void gnn_edge_weights_kernel(GnnGraph g, const W *__restrict__ theta,
 
 // gamma = sqrt(mean(zs^2)) from zs.zs kept in *zz (double), into *gamma (float)
 __global__ void gnn_gamma_kernel(const double *zz, int n3, float *gamma) {
+  pdl_entry();
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     const double g2 = *zz / double(n3);
     *gamma = g2 > 0.0 ? float(sqrt(g2)) : 1.0f;
@@ -101,6 +103,7 @@ template <class R, class W>
 __global__ void gnn_encode_kernel(GnnGraph g, const W *__restrict__ theta, const R *__restrict__ zs,
                                   const R *__restrict__ r, const float *__restrict__ gamma, float *__restrict__ x_out,
                                   float *__restrict__ h0, const CgState *st) {
+  pdl_entry();
   if (st && (st->done || !st->use_gnn)) return;
   const GnnOffsets o = GnnOffsets::make();
   __shared__ float Win[kGnnWidth * 6];
@@ -132,6 +135,7 @@ __global__ void __launch_bounds__(kThreads) gnn_layer_kernel(GnnGraph g, const W
                                                              const float *__restrict__ h_prev,
                                                              float *__restrict__ m_out, float *__restrict__ h_new,
                                                              const CgState *st) {
+  pdl_entry();
   if (st && (st->done || !st->use_gnn)) return;
   const GnnOffsets o = GnnOffsets::make();
   __shared__ float Ws[kGnnWidth * kGnnWidth], Wm[kGnnWidth * kGnnWidth];
@@ -164,6 +168,7 @@ template <class R, class W>
 __global__ void gnn_decode_kernel(int n, const W *__restrict__ theta, const float *__restrict__ h3,
                                   const R *__restrict__ zs, const float *__restrict__ gamma, R *__restrict__ z,
                                   const CgState *st) {
+  pdl_entry();
   if (st && st->done) return;
   if (st && !st->use_gnn) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x) z[i] = zs[i];
@@ -197,6 +202,7 @@ __global__ void __launch_bounds__(kThreads) gnn_decode_bwd_kernel(int n, const f
                                                                   const float *__restrict__ gamma,
                                                                   float *__restrict__ dh3, float *__restrict__ part,
                                                                   int stride) {
+  pdl_entry();
   const GnnOffsets o = GnnOffsets::make();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -238,6 +244,7 @@ __global__ void __launch_bounds__(kThreads) gnn_layer_bwd_kernel(GnnGraph g, con
                                                                  float *__restrict__ gm_out,
                                                                  float *__restrict__ dh_prev,
                                                                  float *__restrict__ part, int stride) {
+  pdl_entry();
   const GnnOffsets o = GnnOffsets::make();
   __shared__ float Ws[kGnnWidth * kGnnWidth], Wm[kGnnWidth * kGnnWidth];
   for (int k = threadIdx.x; k < kGnnWidth * kGnnWidth; k += blockDim.x) {
@@ -312,6 +319,7 @@ __global__ void __launch_bounds__(kThreads) gnn_layer_bwd_kernel(GnnGraph g, con
 __global__ void __launch_bounds__(kThreads) gnn_layer_bwd_gather_kernel(GnnGraph g, int l, const float *__restrict__ w,
                                                                         const float *__restrict__ gm,
                                                                         float *__restrict__ dh_prev) {
+  pdl_entry();
   const int lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const float *wl = w + size_t(l) * g.nedges;
@@ -326,6 +334,7 @@ __global__ void __launch_bounds__(kThreads) gnn_layer_bwd_gather_kernel(GnnGraph
 __global__ void __launch_bounds__(kThreads) gnn_encode_bwd_kernel(int n, const float *__restrict__ x,
                                                                   const float *__restrict__ dh0,
                                                                   float *__restrict__ part, int stride) {
+  pdl_entry();
   const GnnOffsets o = GnnOffsets::make();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -348,6 +357,7 @@ __global__ void __launch_bounds__(kThreads) gnn_encode_bwd_kernel(int n, const f
 // grad[k] = sum over CTAs of part[cta * stride + k]  (fixed order; thread per k)
 __global__ void gnn_reduce_grads_kernel(const float *__restrict__ part, int nparts, int stride,
                                         float *__restrict__ grad, int nparam) {
+  pdl_entry();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nparam; k += gridDim.x * blockDim.x) {
     float s = 0.0f;
     for (int q = 0; q < nparts; q++) s += part[size_t(q) * stride + k];
@@ -360,6 +370,7 @@ __global__ void gnn_adam_kernel(float *__restrict__ theta, const float *__restri
                                 float *__restrict__ m1, float *__restrict__ m2, int nparam, float lr,
                                 float b1, float b2, float eps, int step, float gscale,
                                 __nv_bfloat16 *__restrict__ theta_bf16) {
+  pdl_entry();
   const float c1 = 1.0f - powf(b1, float(step)), c2 = 1.0f - powf(b2, float(step));
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nparam; k += gridDim.x * blockDim.x) {
     const float gk = grad[k] * gscale;
@@ -374,6 +385,7 @@ __global__ void gnn_adam_kernel(float *__restrict__ theta, const float *__restri
 
 // s_i = (trace(D_i)/3)^(-1/2) from the raw diagonal blocks (first n blocks of raw)
 __global__ void gnn_node_scale_kernel(const double *__restrict__ raw, int n, float *__restrict__ s) {
+  pdl_entry();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double t = (raw[9 * size_t(i)] + raw[9 * size_t(i) + 4] + raw[9 * size_t(i) + 8]) / 3.0;
     s[i] = t > 0.0 ? float(1.0 / sqrt(t)) : 1.0f;
@@ -383,6 +395,7 @@ __global__ void gnn_node_scale_kernel(const double *__restrict__ raw, int n, flo
 // feat_e = s_i A_ij s_j for edge e = (i, j), A_ij the raw block src[e]
 __global__ void gnn_edge_feat_kernel(GnnGraph g, const int *__restrict__ row_of, const int *__restrict__ src,
                                      const double *__restrict__ raw, float *__restrict__ feat) {
+  pdl_entry();
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.nedges; e += gridDim.x * blockDim.x) {
     const double f = double(g.s[row_of[e]]) * double(g.s[g.col[e]]);
     for (int k = 0; k < 9; k++) feat[9 * size_t(e) + k] = float(raw[9 * size_t(src[e]) + k] * f);
@@ -392,26 +405,31 @@ __global__ void gnn_edge_feat_kernel(GnnGraph g, const int *__restrict__ row_of,
 // out = float(a - b)
 __global__ void diff_narrow_kernel(const double *__restrict__ a, const double *__restrict__ b,
                                    float *__restrict__ out, int n) {
+  pdl_entry();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = float(a[i] - b[i]);
 }
 
 // d = z - e
 __global__ void sub_kernel(const float *__restrict__ z, const float *__restrict__ e, float *__restrict__ d, int n) {
+  pdl_entry();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[i] = z[i] - e[i];
 }
 
 // dz = c * q with c = 2 / (e.r)
 __global__ void scale_kernel(const float *__restrict__ q, float c, float *__restrict__ dz, int n) {
+  pdl_entry();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dz[i] = c * q[i];
 }
 
 // acc += g * c
 __global__ void accum_kernel(const float *__restrict__ g, float c, float *__restrict__ acc, int n) {
+  pdl_entry();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[i] += c * g[i];
 }
 
 // state for a network application outside a solve (training, evaluation)
 __global__ void gnn_state_kernel(CgState *st) {
+  pdl_entry();
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     st->done = 0;
     st->use_gnn = 1;

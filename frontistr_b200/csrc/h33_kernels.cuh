@@ -334,6 +334,7 @@ struct GroupShape {
 template <class T>
 __global__ void pack_sell_kernel(T *__restrict__ val, const int *__restrict__ src, int nslots,
                                  const double *__restrict__ raw) {
+  pdl_entry();
   const int total = nslots * 32;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     const int b = src[t];
@@ -350,6 +351,7 @@ __global__ void pack_sell_kernel(T *__restrict__ val, const int *__restrict__ sr
 template <class T>
 __global__ void alu_kernel(const double *__restrict__ blocks, const int *__restrict__ perm, int n,
                            double sigma, int lu_done, T *__restrict__ alu, int *__restrict__ err) {
+  pdl_entry();
   for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += gridDim.x * blockDim.x) {
     const int node = perm ? perm[pos] : pos;
     double a[3][3];
@@ -381,6 +383,7 @@ template <class R, int MODE>
 __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<R> A, const R *__restrict__ x,
                                                         R *__restrict__ y, const R *__restrict__ b,
                                                         CgState *st, double *partials) {
+  pdl_entry();
   if (MODE == 2 && st->done) return;
   const int lane = threadIdx.x & 31;
   const int warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -423,6 +426,7 @@ __global__ void __launch_bounds__(kThreads) sweep_fwd_kernel(SellView<TV> L, con
                                                              const R *__restrict__ r, R *__restrict__ z,
                                                              R *__restrict__ zpos, int sbeg, int send,
                                                              GroupShape gs, const CgState *st) {
+  pdl_entry();
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
   const int roff = lane / K;
@@ -473,6 +477,7 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, con
                                                              R *__restrict__ zpos, int sbeg, int send, GroupShape gs,
                                                              CgState *st, double *partials, int part_base,
                                                              int part_total) {
+  pdl_entry();
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
   const int roff = lane / K;
@@ -527,6 +532,7 @@ template <class R, class TA, bool FUSE_RHO>
 __global__ void __launch_bounds__(kThreads) diag_kernel(const TA *__restrict__ alu, int n,
                                                         const R *__restrict__ r, R *__restrict__ z,
                                                         CgState *st, double *partials) {
+  pdl_entry();
   if (st && st->done) return;
   double dot = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -547,6 +553,7 @@ template <class R>
 __global__ void __launch_bounds__(kThreads) fcg_rho_kernel(const R *__restrict__ z, const R *__restrict__ r,
                                                            const R *__restrict__ r_old, int n3, CgState *st,
                                                            double *partials) {
+  pdl_entry();
   if (st->done) return;
   double a = 0.0, b = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
@@ -564,6 +571,7 @@ __global__ void __launch_bounds__(kThreads) update_xr_flex_kernel(R *__restrict_
                                                                   R *__restrict__ r, R *__restrict__ r_old,
                                                                   const R *__restrict__ q, int n3, CgState *st,
                                                                   double *partials) {
+  pdl_entry();
   if (st->done) return;
   const R alpha = R(st->alpha);
   const bool refresh = !st->inner && (st->iter % kIterRecomputeR) == 0;
@@ -585,6 +593,7 @@ __global__ void __launch_bounds__(kThreads) update_xr_flex_kernel(R *__restrict_
 template <class R>
 __global__ void __launch_bounds__(kThreads) gamma_kernel(const R *__restrict__ zs, int n3, CgState *st,
                                                          double *partials) {
+  pdl_entry();
   if (st->done || !st->use_gnn) return;
   double a = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
@@ -599,6 +608,7 @@ __global__ void __launch_bounds__(kThreads) gamma_kernel(const R *__restrict__ z
 template <class R>
 __global__ void __launch_bounds__(kThreads) update_p_kernel(const R *__restrict__ z, R *__restrict__ p,
                                                             int n3, const CgState *st) {
+  pdl_entry();
   if (st->done) return;
   const bool first = st->iter == 1;
   const R beta = R(st->beta);
@@ -612,6 +622,7 @@ template <class R>
 __global__ void __launch_bounds__(kThreads) update_xr_kernel(R *__restrict__ x, const R *__restrict__ p,
                                                              R *__restrict__ r, const R *__restrict__ q,
                                                              int n3, CgState *st, double *partials) {
+  pdl_entry();
   if (st->done) return;
   const R alpha = R(st->alpha);
   const bool refresh = !st->inner && (st->iter % kIterRecomputeR) == 0;
@@ -635,6 +646,7 @@ __global__ void __launch_bounds__(kThreads) resid_ctl_kernel(SellView<R> A, cons
                                                              R *__restrict__ r, const R *__restrict__ b,
                                                              CgState *st, double *partials,
                                                              cudaGraphConditionalHandle h, int use_cond) {
+  pdl_entry();
   const bool need = !st->done && ((!st->inner && (st->iter % kIterRecomputeR) == 0) || st->recompute);
   if (!need) {
     if (blockIdx.x == 0 && threadIdx.x == 0) loop_ctl(st, h, use_cond);
@@ -678,6 +690,7 @@ static __global__ void __launch_bounds__(kThreads) ru_init_kernel(const double *
                                                            float *__restrict__ x32, int n3, CgState *st,
                                                            double *partials, cudaGraphConditionalHandle h,
                                                            int use_cond) {
+  pdl_entry();
   double dot = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
     const double v = r64[i];
@@ -701,6 +714,7 @@ static __global__ void __launch_bounds__(kThreads) ru_init_kernel(const double *
 // Reliable update, part 1 (only when pending): x64 += x32, x32 = 0.
 static __global__ void __launch_bounds__(kThreads) ru_update_x_kernel(double *__restrict__ x64, float *__restrict__ x32,
                                                                int n3, const CgState *st) {
+  pdl_entry();
   if (st->done || !st->ru_pending) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
     x64[i] = x64[i] + double(x32[i]);
@@ -715,6 +729,7 @@ static __global__ void __launch_bounds__(kThreads) ru_resid_kernel(SellView<doub
                                                             double *__restrict__ r64, const double *__restrict__ b64,
                                                             float *__restrict__ r32, CgState *st, double *partials,
                                                             cudaGraphConditionalHandle h, int use_cond) {
+  pdl_entry();
   const bool need = !st->done && st->ru_pending;
   if (!need) {
     if (blockIdx.x == 0 && threadIdx.x == 0) loop_ctl(st, h, use_cond);
@@ -765,6 +780,7 @@ template <class R, int WHICH>
 __global__ void __launch_bounds__(kThreads) dot_kernel(const R *__restrict__ a, const R *__restrict__ b,
                                                        int n3, CgState *st, double *partials,
                                                        cudaGraphConditionalHandle h, int use_cond) {
+  pdl_entry();
   if (WHICH == 1 && st->done) return;
   double dot = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
@@ -788,12 +804,14 @@ __global__ void __launch_bounds__(kThreads) dot_kernel(const R *__restrict__ a, 
 
 // First kernel of every loop body: fail-safe loop condition and body counter.
 static __global__ void iter_begin_kernel(CgState *st, cudaGraphConditionalHandle h, int use_cond) {
+  pdl_entry();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   st->guard++;
   set_loop(h, use_cond, 0);
 }
 
 static __global__ void cg_init_kernel(CgState *st, const CgParams *prm) {
+  pdl_entry();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   st->rho = st->rho1 = st->alpha = st->beta = st->pq = st->rr = 0.0;
   st->bnrm2 = 0.0;
@@ -828,31 +846,37 @@ static __global__ void cg_init_kernel(CgState *st, const CgParams *prm) {
 // precision conversions of the mixed-precision refinement.
 template <class R>
 __global__ void copy_kernel(const R *__restrict__ a, R *__restrict__ b, int n, const CgState *st) {
+  pdl_entry();
   if (st && st->done) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
 template <class R>
 __global__ void add_kernel(const R *__restrict__ a, R *__restrict__ b, int n, const CgState *st) {
+  pdl_entry();
   if (st && st->done) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = b[i] + a[i];
 }
 // b = float(a) (inner right-hand side from the FP64 residual)
 static __global__ void narrow_kernel(const double *__restrict__ a, float *__restrict__ b, int n) {
+  pdl_entry();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = float(a[i]);
 }
 // x += double(d) (FP64 correction of the outer refinement)
 static __global__ void widen_add_kernel(const float *__restrict__ d, double *__restrict__ x, int n) {
+  pdl_entry();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     x[i] = x[i] + double(d[i]);
 }
 // b = R(a) for value arrays (FP32 copies of the matrix / preconditioner values)
 template <class R>
 __global__ void convert_kernel(const double *__restrict__ a, R *__restrict__ b, size_t n) {
+  pdl_entry();
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
     b[i] = R(a[i]);
 }
 // BF16 copies of stored values (round to nearest even)
 static __global__ void convert_bf16_kernel(const double *__restrict__ a, __nv_bfloat16 *__restrict__ b, size_t n) {
+  pdl_entry();
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
     b[i] = __float2bfloat16_rn(float(a[i]));
 }

@@ -126,6 +126,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kThreads) mr_spmv_kernel(SellView<double> A, const double *__restrict__ x,
                                                            double *__restrict__ y, const double *__restrict__ b,
                                                            CgState *st, MultiCtl *ctl, double *partials) {
+  pdl_entry();
   if (MODE >= 2 && ctl->all_done) return;
   const int l = threadIdx.x & 15;
   bool mine = true;  // this lane's RHS takes part
@@ -193,6 +194,7 @@ __global__ void __launch_bounds__(kThreads) mr_sweep_fwd_kernel(SellView<double>
                                                                 const double *__restrict__ r, double *__restrict__ z,
                                                                 double *__restrict__ zpos, int sb, int se,
                                                                 const MultiCtl *ctl) {
+  pdl_entry();
   if (ctl && ctl->all_done) return;
   const int l = threadIdx.x & 15;
   const int nhw = (gridDim.x * blockDim.x) >> 4;
@@ -227,6 +229,7 @@ __global__ void __launch_bounds__(kThreads) mr_sweep_bwd_kernel(SellView<double>
                                                                 double *__restrict__ zpos, int sb, int se, CgState *st,
                                                                 MultiCtl *ctl, double *partials, int part_base,
                                                                 int part_total) {
+  pdl_entry();
   if (ctl && ctl->all_done) return;
   const int l = threadIdx.x & 15;
   const int nhw = (gridDim.x * blockDim.x) >> 4;
@@ -268,6 +271,7 @@ template <bool FUSE_RHO>
 __global__ void __launch_bounds__(kThreads) mr_diag_kernel(const double *__restrict__ alu, int n,
                                                            const double *__restrict__ r, double *__restrict__ z,
                                                            CgState *st, MultiCtl *ctl, double *partials) {
+  pdl_entry();
   if (ctl && ctl->all_done) return;
   const int l = threadIdx.x & 15;
   const int nhw = (gridDim.x * blockDim.x) >> 4;
@@ -292,6 +296,7 @@ __global__ void __launch_bounds__(kThreads) mr_diag_kernel(const double *__restr
 template <int WHICH>
 __global__ void __launch_bounds__(kThreads) mr_dot_kernel(const double *__restrict__ a, const double *__restrict__ b,
                                                           int n, CgState *st, MultiCtl *ctl, double *partials) {
+  pdl_entry();
   if (WHICH == 1 && ctl->all_done) return;
   const int l = threadIdx.x & 15;
   const int nhw = (gridDim.x * blockDim.x) >> 4;
@@ -322,6 +327,7 @@ __global__ void __launch_bounds__(kThreads) mr_dot_kernel(const double *__restri
 // {p} = {z} or {z} + BETA {p} for the RHS still iterating.
 __global__ void __launch_bounds__(kThreads) mr_update_p_kernel(const double *__restrict__ z, double *__restrict__ p,
                                                                int n, const CgState *st, const MultiCtl *ctl) {
+  pdl_entry();
   if (ctl->all_done) return;
   const int l = threadIdx.x & 15;
   if (st[l].done) return;  // no barrier below: lanes of finished RHS simply leave
@@ -339,6 +345,7 @@ __global__ void __launch_bounds__(kThreads) mr_update_p_kernel(const double *__r
 __global__ void __launch_bounds__(kThreads) mr_update_xr_kernel(double *__restrict__ x, const double *__restrict__ p,
                                                                 double *__restrict__ r, const double *__restrict__ q,
                                                                 int n, CgState *st, MultiCtl *ctl, double *partials) {
+  pdl_entry();
   if (ctl->all_done) return;
   const int l = threadIdx.x & 15;
   const bool act = !st[l].done;
@@ -367,6 +374,7 @@ __global__ void __launch_bounds__(kThreads) mr_update_xr_kernel(double *__restri
 }
 
 __global__ void mr_init_kernel(CgState *st, MultiCtl *ctl, const CgParams *prm, int nrhs) {
+  pdl_entry();
   const int k = threadIdx.x;
   if (blockIdx.x != 0) return;
   if (k < kMaxRhs) {
@@ -397,6 +405,7 @@ __global__ void mr_init_kernel(CgState *st, MultiCtl *ctl, const CgParams *prm, 
 
 // Start of a loop body: body counter of every RHS still iterating, fail-safe condition.
 __global__ void mr_iter_begin_kernel(CgState *st, MultiCtl *ctl, cudaGraphConditionalHandle h, int use_cond) {
+  pdl_entry();
   if (blockIdx.x != 0) return;
   const int k = threadIdx.x;
   if (k < kMaxRhs && !st[k].done) st[k].guard++;
@@ -409,6 +418,7 @@ __global__ void mr_iter_begin_kernel(CgState *st, MultiCtl *ctl, cudaGraphCondit
 // Loop decision after the control of every RHS: continue while one still iterates
 // (and the body count stays within the fail-safe bound).
 __global__ void mr_ctl_kernel(const CgState *st, MultiCtl *ctl, cudaGraphConditionalHandle h, int use_cond) {
+  pdl_entry();
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   int any = 0, maxit = 0;
   for (int k = 0; k < kMaxRhs; k++) {
@@ -422,6 +432,7 @@ __global__ void mr_ctl_kernel(const CgState *st, MultiCtl *ctl, cudaGraphConditi
 
 // Column-major host layout (n3 x nrhs) <-> node-major RHS-minor layout.
 __global__ void mr_pack_kernel(const double *__restrict__ src, double *__restrict__ dst, int n, int nrhs) {
+  pdl_entry();
   const size_t total = size_t(n) * kRhsStride;
   for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
     const int l = int(t % kMaxRhs);
@@ -431,6 +442,7 @@ __global__ void mr_pack_kernel(const double *__restrict__ src, double *__restric
   }
 }
 __global__ void mr_unpack_kernel(const double *__restrict__ src, double *__restrict__ dst, int n, int nrhs) {
+  pdl_entry();
   const size_t total = size_t(n) * 3 * nrhs;
   for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
     const int l = int(t / (3 * size_t(n)));
@@ -440,6 +452,7 @@ __global__ void mr_unpack_kernel(const double *__restrict__ src, double *__restr
 }
 // Zero-RHS lanes leave x = 0 (hecmw_solver.f90:32-37).
 __global__ void mr_zero_x_kernel(double *__restrict__ x, int n, const CgState *st) {
+  pdl_entry();
   const size_t total = size_t(n) * kRhsStride;
   for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x)
     if (st[t % kMaxRhs].zero_rhs) x[t] = 0.0;

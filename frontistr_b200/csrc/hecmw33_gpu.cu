@@ -54,6 +54,30 @@ bool graph_mode() {
 }
 constexpr int kStreamChunk = 16;
 
+// Programmatic dependent launch for every kernel of the solver (HECMW33_PDL=0 turns
+// it off): a kernel may be scheduled while its predecessor drains and waits on the
+// device (pdl_entry) for the predecessor's results, which hides the launch gap
+// between the ~40 dependent kernels of a CG iteration.
+bool pdl_mode() {
+  const char *e = std::getenv("HECMW33_PDL");
+  return !(e && e[0] == '0');
+}
+
+template <typename... KArgs, typename... Args>
+void launch_k(cudaStream_t s, void (*kern)(KArgs...), int grid, int block, Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(grid), 1, 1);
+  cfg.blockDim = dim3(unsigned(block), 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_mode() ? 1 : 0;
+  H33_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
+}
+
 // Lanes per row of the preconditioner sweep layouts (HECMW33_SWEEP_LANES overrides;
 // 4, 8 or 16).  Several lanes per row shorten each row's dependent load
 // chain and multiply the warps of a colour, which the sweeps need: a colour holds
@@ -108,7 +132,7 @@ struct DevSell {
     if (nslots == 0) return;
     const int total = nslots * 32;
     const int grid = std::min((total + kThreads - 1) / kThreads, nsm * 8);
-    pack_sell_kernel<T><<<grid, kThreads, 0, s>>>(val.p, src.p, nslots, raw);
+    launch_k(s, pack_sell_kernel<T>, grid, kThreads, val.p, src.p, nslots, raw);
     H33_CUDA(cudaGetLastError());
   }
   size_t bytes() const {
@@ -366,7 +390,7 @@ void diag_alu(Solver &S, DevArray<double> &alu, const double *blocks, const int 
   alu.alloc(size_t(9) * S.N);
   H33_CUDA(cudaMemsetAsync(S.d_err.p, 0, sizeof(int), S.stream));
   const int grid = std::max(1, std::min((S.N + kThreads - 1) / kThreads, S.nsm * 8));
-  alu_kernel<double><<<grid, kThreads, 0, S.stream>>>(blocks, perm, S.N, sigma, lu_done, alu.p, S.d_err.p);
+  launch_k(S.stream, alu_kernel<double>, grid, kThreads, blocks, perm, S.N, sigma, lu_done, alu.p, S.d_err.p);
   H33_CUDA(cudaGetLastError());
 }
 
@@ -574,7 +598,7 @@ void launch_sweep_k(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, c
     const GroupShape gsh = POS ? GroupShape{P.lo.group_rows[g], P.lo.group_rows[g + 1], P.lo.group_slot0[g],
                                             P.lo.group_len[g]}
                                : GroupShape{0, 0, 0, 0};
-    sweep_fwd_kernel<R, TV, TA, K, POS><<<S.grid_sweep(se - sb), kThreads, 0, s>>>(lo, P.perm_fwd.p, alu_f, S.N,
+    launch_k(s, sweep_fwd_kernel<R, TV, TA, K, POS>, S.grid_sweep(se - sb), kThreads, lo, P.perm_fwd.p, alu_f, S.N,
                                                                                    rin, zout, zpos, sb, se, gsh, st);
   }
   const int gb = int(P.up.group_slice.size()) - 1;
@@ -592,7 +616,7 @@ void launch_sweep_k(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, c
     const GroupShape gsh = POS ? GroupShape{P.up.group_rows[g], P.up.group_rows[g + 1], P.up.group_slot0[g],
                                             P.up.group_len[g]}
                                : GroupShape{0, 0, 0, 0};
-    sweep_bwd_kernel<R, TV, TA, K, FUSE_RHO, POS><<<grid, kThreads, 0, s>>>(up, perm_b, alu_b, S.N, rin, zout, zpos,
+    launch_k(s, sweep_bwd_kernel<R, TV, TA, K, FUSE_RHO, POS>, grid, kThreads, up, perm_b, alu_b, S.N, rin, zout, zpos,
                                                                             sb, se, gsh, st, S.partials.p, base,
                                                                             total);
     base += grid;
@@ -606,7 +630,7 @@ void launch_sweep_t(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, c
                     const R *rin, R *zout, R *zpos, CgState *st) {
   Precond &P = S.pc;
   if (P.kind == 3) {
-    diag_kernel<R, TA, FUSE_RHO><<<S.grid_vec(), kThreads, 0, S.stream>>>(alu_f, S.N, rin, zout, st, S.partials.p);
+    launch_k(S.stream, diag_kernel<R, TA, FUSE_RHO>, S.grid_vec(), kThreads, alu_f, S.N, rin, zout, st, S.partials.p);
     return;
   }
   if (P.pos_cols) {
@@ -640,8 +664,8 @@ void launch_precond(Solver &S, const Views<R> &V, int iterpremax, const R *r, R 
   cudaStream_t s = S.stream;
   const int n3 = S.n3();
   if (iterpremax <= 0) {
-    copy_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(r, z, n3, st);
-    if (st) dot_kernel<R, 1><<<S.grid_vec(), kThreads, 0, s>>>(r, z, n3, st, S.partials.p, 0, 0);
+    launch_k(s, copy_kernel<R>, S.grid_vec(), kThreads, r, z, n3, st);
+    if (st) launch_k(s, dot_kernel<R, 1>, S.grid_vec(), kThreads, r, z, n3, st, S.partials.p, 0, 0);
     return;
   }
   if (iterpremax == 1) {
@@ -652,22 +676,22 @@ void launch_precond(Solver &S, const Views<R> &V, int iterpremax, const R *r, R 
   const R *in = r;
   for (int it = 1; it <= iterpremax; it++) {
     launch_sweep<R, false>(S, V, in, V.zp, st);
-    if (it == 1) copy_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.zp, z, n3, st);
-    else add_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.zp, z, n3, st);
+    if (it == 1) launch_k(s, copy_kernel<R>, S.grid_vec(), kThreads, V.zp, z, n3, st);
+    else launch_k(s, add_kernel<R>, S.grid_vec(), kThreads, V.zp, z, n3, st);
     if (it == iterpremax) break;
-    spmv_kernel<R, 1><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, z, V.w, r, nullptr, nullptr);
+    launch_k(s, spmv_kernel<R, 1>, S.grid_spmv(), kThreads, V.A, z, V.w, r, nullptr, nullptr);
     in = V.w;
   }
-  if (st) dot_kernel<R, 1><<<S.grid_vec(), kThreads, 0, s>>>(r, z, n3, st, S.partials.p, 0, 0);
+  if (st) launch_k(s, dot_kernel<R, 1>, S.grid_vec(), kThreads, r, z, n3, st, S.partials.p, 0, 0);
 }
 
 template <class R>
 void launch_prologue(Solver &S, const Views<R> &V, cudaGraphConditionalHandle h, int use_cond) {
   cudaStream_t s = S.stream;
   CgState *st = S.state.p;
-  cg_init_kernel<<<1, 32, 0, s>>>(st, S.params.p);
-  spmv_kernel<R, 1><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.x, V.r, V.b, nullptr, nullptr);
-  dot_kernel<R, 0><<<S.grid_vec(), kThreads, 0, s>>>(V.b, V.b, S.n3(), st, S.partials.p, h, use_cond);
+  launch_k(s, cg_init_kernel, 1, 32, st, S.params.p);
+  launch_k(s, spmv_kernel<R, 1>, S.grid_spmv(), kThreads, V.A, V.x, V.r, V.b, nullptr, nullptr);
+  launch_k(s, dot_kernel<R, 0>, S.grid_vec(), kThreads, V.b, V.b, S.n3(), st, S.partials.p, h, use_cond);
 }
 
 template <class R>
@@ -675,12 +699,12 @@ void launch_iteration(Solver &S, const Views<R> &V, int iterpremax, cudaGraphCon
   cudaStream_t s = S.stream;
   CgState *st = S.state.p;
   const int n3 = S.n3();
-  iter_begin_kernel<<<1, 32, 0, s>>>(st, h, use_cond);
+  launch_k(s, iter_begin_kernel, 1, 32, st, h, use_cond);
   launch_precond<R>(S, V, iterpremax, V.r, V.z, st);
-  update_p_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.z, V.p, n3, st);
-  spmv_kernel<R, 2><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.p, V.q, nullptr, st, S.partials.p);
-  update_xr_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.x, V.p, V.r, V.q, n3, st, S.partials.p);
-  resid_ctl_kernel<R><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.x, V.r, V.b, st, S.partials.p, h, use_cond);
+  launch_k(s, update_p_kernel<R>, S.grid_vec(), kThreads, V.z, V.p, n3, st);
+  launch_k(s, spmv_kernel<R, 2>, S.grid_spmv(), kThreads, V.A, V.p, V.q, nullptr, st, S.partials.p);
+  launch_k(s, update_xr_kernel<R>, S.grid_vec(), kThreads, V.x, V.p, V.r, V.q, n3, st, S.partials.p);
+  launch_k(s, resid_ctl_kernel<R>, S.grid_spmv(), kThreads, V.A, V.x, V.r, V.b, st, S.partials.p, h, use_cond);
 }
 
 // Network application z = zs + gamma W_out h3 (or z = zs when it is off), R-precision
@@ -692,19 +716,19 @@ void launch_gnn(Solver &S, const R *zs, const R *r, R *z, CgState *st, bool bf16
   const GnnGraph g = L.graph();
   const int gw = std::max(1, std::min((S.N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8));
   const int gt = S.grid_vec();
-  gamma_kernel<R><<<gt, kThreads, 0, s>>>(zs, S.n3(), st, S.partials.p);
+  launch_k(s, gamma_kernel<R>, gt, kThreads, zs, S.n3(), st, S.partials.p);
   if (bf16_weights) {
     const __nv_bfloat16 *th = L.theta_bf16.p;
-    gnn_encode_kernel<R, __nv_bfloat16><<<gt, kThreads, 0, s>>>(g, th, zs, r, &st->gamma, nullptr, L.h[0].p, st);
+    launch_k(s, gnn_encode_kernel<R, __nv_bfloat16>, gt, kThreads, g, th, zs, r, &st->gamma, nullptr, L.h[0].p, st);
     for (int l = 0; l < kGnnLayers; l++)
-      gnn_layer_kernel<__nv_bfloat16><<<gw, kThreads, 0, s>>>(g, th, l, L.w.p, L.h[l].p, nullptr, L.h[l + 1].p, st);
-    gnn_decode_kernel<R, __nv_bfloat16><<<gt, kThreads, 0, s>>>(S.N, th, L.h[3].p, zs, &st->gamma, z, st);
+      launch_k(s, gnn_layer_kernel<__nv_bfloat16>, gw, kThreads, g, th, l, L.w.p, L.h[l].p, nullptr, L.h[l + 1].p, st);
+    launch_k(s, gnn_decode_kernel<R, __nv_bfloat16>, gt, kThreads, S.N, th, L.h[3].p, zs, &st->gamma, z, st);
   } else {
     const float *th = L.theta.p;
-    gnn_encode_kernel<R, float><<<gt, kThreads, 0, s>>>(g, th, zs, r, &st->gamma, nullptr, L.h[0].p, st);
+    launch_k(s, gnn_encode_kernel<R, float>, gt, kThreads, g, th, zs, r, &st->gamma, nullptr, L.h[0].p, st);
     for (int l = 0; l < kGnnLayers; l++)
-      gnn_layer_kernel<float><<<gw, kThreads, 0, s>>>(g, th, l, L.w.p, L.h[l].p, nullptr, L.h[l + 1].p, st);
-    gnn_decode_kernel<R, float><<<gt, kThreads, 0, s>>>(S.N, th, L.h[3].p, zs, &st->gamma, z, st);
+      launch_k(s, gnn_layer_kernel<float>, gw, kThreads, g, th, l, L.w.p, L.h[l].p, nullptr, L.h[l + 1].p, st);
+    launch_k(s, gnn_decode_kernel<R, float>, gt, kThreads, S.N, th, L.h[3].p, zs, &st->gamma, z, st);
   }
 }
 
@@ -716,14 +740,14 @@ void launch_iteration_flex(Solver &S, const Views<R> &V, cudaGraphConditionalHan
   cudaStream_t s = S.stream;
   CgState *st = S.state.p;
   const int n3 = S.n3();
-  iter_begin_kernel<<<1, 32, 0, s>>>(st, h, use_cond);
+  launch_k(s, iter_begin_kernel, 1, 32, st, h, use_cond);
   launch_sweep<R, false>(S, V, V.r, V.zs, st);
   launch_gnn<R>(S, V.zs, V.r, V.z, st, true);
-  fcg_rho_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.z, V.r, V.rold, n3, st, S.partials.p);
-  update_p_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.z, V.p, n3, st);
-  spmv_kernel<R, 2><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.p, V.q, nullptr, st, S.partials.p);
-  update_xr_flex_kernel<R><<<S.grid_vec(), kThreads, 0, s>>>(V.x, V.p, V.r, V.rold, V.q, n3, st, S.partials.p);
-  resid_ctl_kernel<R><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.x, V.r, V.b, st, S.partials.p, h, use_cond);
+  launch_k(s, fcg_rho_kernel<R>, S.grid_vec(), kThreads, V.z, V.r, V.rold, n3, st, S.partials.p);
+  launch_k(s, update_p_kernel<R>, S.grid_vec(), kThreads, V.z, V.p, n3, st);
+  launch_k(s, spmv_kernel<R, 2>, S.grid_spmv(), kThreads, V.A, V.p, V.q, nullptr, st, S.partials.p);
+  launch_k(s, update_xr_flex_kernel<R>, S.grid_vec(), kThreads, V.x, V.p, V.r, V.rold, V.q, n3, st, S.partials.p);
+  launch_k(s, resid_ctl_kernel<R>, S.grid_spmv(), kThreads, V.A, V.x, V.r, V.b, st, S.partials.p, h, use_cond);
 }
 
 // Mixed precision with reliable updates (graph body in FP32, FP64 pieces inside).
@@ -731,10 +755,10 @@ void launch_iteration_flex(Solver &S, const Views<R> &V, cudaGraphConditionalHan
 void launch_prologue_reliable(Solver &S, cudaGraphConditionalHandle h, int use_cond) {
   cudaStream_t s = S.stream;
   CgState *st = S.state.p;
-  cg_init_kernel<<<1, 32, 0, s>>>(st, S.params.p);
-  spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.r.p, S.b.p, nullptr, nullptr);
-  dot_kernel<double, 0><<<S.grid_vec(), kThreads, 0, s>>>(S.b.p, S.b.p, S.n3(), st, S.partials.p, h, use_cond);
-  ru_init_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.r.p, S.rf.p, S.xf.p, S.n3(), st, S.partials.p, h, use_cond);
+  launch_k(s, cg_init_kernel, 1, 32, st, S.params.p);
+  launch_k(s, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, S.A.view(), S.x.p, S.r.p, S.b.p, nullptr, nullptr);
+  launch_k(s, dot_kernel<double, 0>, S.grid_vec(), kThreads, S.b.p, S.b.p, S.n3(), st, S.partials.p, h, use_cond);
+  launch_k(s, ru_init_kernel, S.grid_vec(), kThreads, S.r.p, S.rf.p, S.xf.p, S.n3(), st, S.partials.p, h, use_cond);
 }
 
 // One FP32 CG (or flexible CG with the network) iteration followed by the FP64
@@ -745,22 +769,22 @@ void launch_iteration_reliable(Solver &S, int iterpremax, bool learned, cudaGrap
   CgState *st = S.state.p;
   const int n3 = S.n3();
   const Views<float> V = views(S, 0.0f);
-  iter_begin_kernel<<<1, 32, 0, s>>>(st, h, use_cond);
+  launch_k(s, iter_begin_kernel, 1, 32, st, h, use_cond);
   if (learned) {
     launch_sweep<float, false>(S, V, V.r, V.zs, st);
     launch_gnn<float>(S, V.zs, V.r, V.z, st, true);
-    fcg_rho_kernel<float><<<S.grid_vec(), kThreads, 0, s>>>(V.z, V.r, V.rold, n3, st, S.partials.p);
+    launch_k(s, fcg_rho_kernel<float>, S.grid_vec(), kThreads, V.z, V.r, V.rold, n3, st, S.partials.p);
   } else {
     launch_precond<float>(S, V, iterpremax, V.r, V.z, st);
   }
-  update_p_kernel<float><<<S.grid_vec(), kThreads, 0, s>>>(V.z, V.p, n3, st);
-  spmv_kernel<float, 2><<<S.grid_spmv(), kThreads, 0, s>>>(V.A, V.p, V.q, nullptr, st, S.partials.p);
+  launch_k(s, update_p_kernel<float>, S.grid_vec(), kThreads, V.z, V.p, n3, st);
+  launch_k(s, spmv_kernel<float, 2>, S.grid_spmv(), kThreads, V.A, V.p, V.q, nullptr, st, S.partials.p);
   if (learned)
-    update_xr_flex_kernel<float><<<S.grid_vec(), kThreads, 0, s>>>(V.x, V.p, V.r, V.rold, V.q, n3, st, S.partials.p);
+    launch_k(s, update_xr_flex_kernel<float>, S.grid_vec(), kThreads, V.x, V.p, V.r, V.rold, V.q, n3, st, S.partials.p);
   else
-    update_xr_kernel<float><<<S.grid_vec(), kThreads, 0, s>>>(V.x, V.p, V.r, V.q, n3, st, S.partials.p);
-  ru_update_x_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.x.p, S.xf.p, n3, st);
-  ru_resid_kernel<<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.r.p, S.b.p, S.rf.p, st, S.partials.p, h,
+    launch_k(s, update_xr_kernel<float>, S.grid_vec(), kThreads, V.x, V.p, V.r, V.q, n3, st, S.partials.p);
+  launch_k(s, ru_update_x_kernel, S.grid_vec(), kThreads, S.x.p, S.xf.p, n3, st);
+  launch_k(s, ru_resid_kernel, S.grid_spmv(), kThreads, S.A.view(), S.x.p, S.r.p, S.b.p, S.rf.p, st, S.partials.p, h,
                                                      use_cond);
 }
 
@@ -879,8 +903,8 @@ float run_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels, int
 double rel_resid_device(Solver &S) {
   cudaStream_t s = S.stream;
   CgState *st = S.state.p;
-  spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.w.p, S.b.p, nullptr, nullptr);
-  dot_kernel<double, 2><<<S.grid_vec(), kThreads, 0, s>>>(S.w.p, S.w.p, S.n3(), st, S.partials.p, 0, 0);
+  launch_k(s, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, S.A.view(), S.x.p, S.w.p, S.b.p, nullptr, nullptr);
+  launch_k(s, dot_kernel<double, 2>, S.grid_vec(), kThreads, S.w.p, S.w.p, S.n3(), st, S.partials.p, 0, 0);
   double rr = 0.0;
   H33_CUDA(cudaMemcpyAsync(&rr, &st->rr_true, sizeof(double), cudaMemcpyDeviceToHost, s));
   S.sync();
@@ -891,7 +915,7 @@ double rel_resid_device(Solver &S) {
 
 double dot_device_f(Solver &S, const float *a, const float *b) {
   CgState *st = S.state.p;
-  dot_kernel<float, 2><<<S.grid_vec(), kThreads, 0, S.stream>>>(a, b, S.n3(), st, S.partials.p, 0, 0);
+  launch_k(S.stream, dot_kernel<float, 2>, S.grid_vec(), kThreads, a, b, S.n3(), st, S.partials.p, 0, 0);
   double v = 0.0;
   H33_CUDA(cudaMemcpyAsync(&v, &st->rr_true, sizeof(double), cudaMemcpyDeviceToHost, S.stream));
   S.sync();
@@ -900,7 +924,7 @@ double dot_device_f(Solver &S, const float *a, const float *b) {
 
 double dot_device(Solver &S, const double *a, const double *b) {
   CgState *st = S.state.p;
-  dot_kernel<double, 2><<<S.grid_vec(), kThreads, 0, S.stream>>>(a, b, S.n3(), st, S.partials.p, 0, 0);
+  launch_k(S.stream, dot_kernel<double, 2>, S.grid_vec(), kThreads, a, b, S.n3(), st, S.partials.p, 0, 0);
   double v = 0.0;
   H33_CUDA(cudaMemcpyAsync(&v, &st->rr_true, sizeof(double), cudaMemcpyDeviceToHost, S.stream));
   S.sync();
@@ -913,7 +937,7 @@ void ensure_fp32(Solver &S) {
   auto conv = [&](const double *a, float *b, size_t n) {
     if (n == 0) return;
     const int grid = int(std::min<size_t>((n + kThreads - 1) / kThreads, size_t(S.nsm) * 16));
-    convert_kernel<float><<<grid, kThreads, 0, S.stream>>>(a, b, n);
+    launch_k(S.stream, convert_kernel<float>, grid, kThreads, a, b, n);
     H33_CUDA(cudaGetLastError());
   };
   if (S.a32_version != S.values_version) {
@@ -994,9 +1018,9 @@ void learned_graph(Solver &S) {
   }
   if (L.feat_version != S.values_version) {
     const int grid = std::max(1, std::min((N + kThreads - 1) / kThreads, S.nsm * 8));
-    gnn_node_scale_kernel<<<grid, kThreads, 0, S.stream>>>(S.raw.p, N, L.s.p);
+    launch_k(S.stream, gnn_node_scale_kernel, grid, kThreads, S.raw.p, N, L.s.p);
     const int ge = std::max(1, std::min((L.nedges + kThreads - 1) / kThreads, S.nsm * 16));
-    gnn_edge_feat_kernel<<<ge, kThreads, 0, S.stream>>>(L.graph(), L.row_of.p, L.src.p, S.raw.p, L.feat.p);
+    launch_k(S.stream, gnn_edge_feat_kernel, ge, kThreads, L.graph(), L.row_of.p, L.src.p, S.raw.p, L.feat.p);
     H33_CUDA(cudaGetLastError());
     L.feat_version = S.values_version;
     L.w_version = -1;
@@ -1007,8 +1031,8 @@ void learned_graph(Solver &S) {
 void learned_edge_weights(Solver &S, bool bf16) {
   Learned &L = S.L;
   const int ge = std::max(1, std::min((L.nedges + kThreads - 1) / kThreads, S.nsm * 16));
-  if (bf16) gnn_edge_weights_kernel<__nv_bfloat16><<<ge, kThreads, 0, S.stream>>>(L.graph(), L.theta_bf16.p, L.w.p);
-  else gnn_edge_weights_kernel<float><<<ge, kThreads, 0, S.stream>>>(L.graph(), L.theta.p, L.w.p);
+  if (bf16) launch_k(S.stream, gnn_edge_weights_kernel<__nv_bfloat16>, ge, kThreads, L.graph(), L.theta_bf16.p, L.w.p);
+  else launch_k(S.stream, gnn_edge_weights_kernel<float>, ge, kThreads, L.graph(), L.theta.p, L.w.p);
   H33_CUDA(cudaGetLastError());
   L.w_version = bf16 ? L.weights_version : -1;
 }
@@ -1107,31 +1131,31 @@ void learned_pair_grad(Solver &S, const float *r, const float *e, const float *z
   const int n3 = S.n3();
   const int gw = std::max(1, std::min((S.N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8));
   const int gt = S.grid_vec();
-  gnn_state_kernel<<<1, 32, 0, s>>>(st);
-  gamma_kernel<float><<<gt, kThreads, 0, s>>>(zs, n3, st, S.partials.p);
-  gnn_encode_kernel<float, float><<<gt, kThreads, 0, s>>>(g, L.theta.p, zs, r, &st->gamma, L.x.p, L.h[0].p, st);
+  launch_k(s, gnn_state_kernel, 1, 32, st);
+  launch_k(s, gamma_kernel<float>, gt, kThreads, zs, n3, st, S.partials.p);
+  launch_k(s, gnn_encode_kernel<float, float>, gt, kThreads, g, L.theta.p, zs, r, &st->gamma, L.x.p, L.h[0].p, st);
   for (int l = 0; l < kGnnLayers; l++)
-    gnn_layer_kernel<float><<<gw, kThreads, 0, s>>>(g, L.theta.p, l, L.w.p, L.h[l].p, L.m[l].p, L.h[l + 1].p, st);
-  gnn_decode_kernel<float, float><<<gt, kThreads, 0, s>>>(S.N, L.theta.p, L.h[3].p, zs, &st->gamma, L.t_z.p, st);
+    launch_k(s, gnn_layer_kernel<float>, gw, kThreads, g, L.theta.p, l, L.w.p, L.h[l].p, L.m[l].p, L.h[l + 1].p, st);
+  launch_k(s, gnn_decode_kernel<float, float>, gt, kThreads, S.N, L.theta.p, L.h[3].p, zs, &st->gamma, L.t_z.p, st);
   // d = z - e, q = A d (FP32), loss = d.q / e.r, dz = 2 q / e.r
-  sub_kernel<<<gt, kThreads, 0, s>>>(L.t_z.p, e, L.t_d.p, n3);
-  spmv_kernel<float, 0><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view32(), L.t_d.p, L.t_q.p, nullptr, nullptr, nullptr);
-  dot_kernel<float, 2><<<gt, kThreads, 0, s>>>(L.t_d.p, L.t_q.p, n3, st, S.partials.p, 0, 0);
+  launch_k(s, sub_kernel, gt, kThreads, L.t_z.p, e, L.t_d.p, n3);
+  launch_k(s, spmv_kernel<float, 0>, S.grid_spmv(), kThreads, S.A.view32(), L.t_d.p, L.t_q.p, nullptr, nullptr, nullptr);
+  launch_k(s, dot_kernel<float, 2>, gt, kThreads, L.t_d.p, L.t_q.p, n3, st, S.partials.p, 0, 0);
   H33_CUDA(cudaMemcpyAsync(loss_slot, &st->rr_true, sizeof(double), cudaMemcpyDeviceToDevice, s));
-  scale_kernel<<<gt, kThreads, 0, s>>>(L.t_q.p, float(2.0 / er), L.t_dz.p, n3);
+  launch_k(s, scale_kernel, gt, kThreads, L.t_q.p, float(2.0 / er), L.t_dz.p, n3);
   // backward
   const int np = L.nparts, stride = L.stride;
-  gnn_decode_bwd_kernel<<<np, kThreads, 0, s>>>(S.N, L.theta.p, L.h[3].p, L.t_dz.p, &st->gamma, L.dh.p, L.part.p,
+  launch_k(s, gnn_decode_bwd_kernel, np, kThreads, S.N, L.theta.p, L.h[3].p, L.t_dz.p, &st->gamma, L.dh.p, L.part.p,
                                                 stride);
   for (int l = kGnnLayers - 1; l >= 0; l--) {
-    gnn_layer_bwd_kernel<<<np, kThreads, 0, s>>>(g, L.theta.p, l, L.w.p, L.h[l].p, L.h[l + 1].p, L.m[l].p, L.dh.p,
+    launch_k(s, gnn_layer_bwd_kernel, np, kThreads, g, L.theta.p, l, L.w.p, L.h[l].p, L.h[l + 1].p, L.m[l].p, L.dh.p,
                                                  L.gm.p, L.dhp.p, L.part.p, stride);
-    gnn_layer_bwd_gather_kernel<<<gw, kThreads, 0, s>>>(g, l, L.w.p, L.gm.p, L.dhp.p);
+    launch_k(s, gnn_layer_bwd_gather_kernel, gw, kThreads, g, l, L.w.p, L.gm.p, L.dhp.p);
     std::swap(L.dh, L.dhp);
   }
-  gnn_encode_bwd_kernel<<<np, kThreads, 0, s>>>(S.N, L.x.p, L.dh.p, L.part.p, stride);
-  gnn_reduce_grads_kernel<<<(stride + 255) / 256, 256, 0, s>>>(L.part.p, np, stride, L.grad.p, stride);
-  accum_kernel<<<(stride + 255) / 256, 256, 0, s>>>(L.grad.p, coef, L.gacc.p, stride);
+  launch_k(s, gnn_encode_bwd_kernel, np, kThreads, S.N, L.x.p, L.dh.p, L.part.p, stride);
+  launch_k(s, gnn_reduce_grads_kernel, (stride + 255) / 256, 256, L.part.p, np, stride, L.grad.p, stride);
+  launch_k(s, accum_kernel, (stride + 255) / 256, 256, L.grad.p, coef, L.gacc.p, stride);
   H33_CUDA(cudaGetLastError());
   (void)er;
 }
@@ -1180,10 +1204,10 @@ float record_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels) 
       DevArray<float> pr, pe;
       pr.alloc(n3);
       pe.alloc(n3);
-      spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, S.stream>>>(S.A.view(), x.p, S.w.p, S.b.p, nullptr,
+      launch_k(S.stream, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, S.A.view(), x.p, S.w.p, S.b.p, nullptr,
                                                                         nullptr);
-      narrow_kernel<<<gt, kThreads, 0, S.stream>>>(S.w.p, pr.p, int(n3));
-      diff_narrow_kernel<<<gt, kThreads, 0, S.stream>>>(S.x.p, x.p, pe.p, int(n3));
+      launch_k(S.stream, narrow_kernel, gt, kThreads, S.w.p, pr.p, int(n3));
+      launch_k(S.stream, diff_narrow_kernel, gt, kThreads, S.x.p, x.p, pe.p, int(n3));
       H33_CUDA(cudaGetLastError());
       // e.r of the stored FP32 pair (FP64 accumulation) -- the normaliser of its loss
       const double er = dot_device_f(S, pe.p, pr.p);
@@ -1234,7 +1258,7 @@ void learned_train(Solver &S, int steps, double lr, double *loss) {
                         1.0f / float(np), L.losses.p + k);
     if (update) {
       L.adam_step++;
-      gnn_adam_kernel<<<(nparam + 255) / 256, 256, 0, S.stream>>>(L.theta.p, L.gacc.p, L.m1.p, L.m2.p, nparam,
+      launch_k(S.stream, gnn_adam_kernel, (nparam + 255) / 256, 256, L.theta.p, L.gacc.p, L.m1.p, L.m2.p, nparam,
                                                                   float(lr), 0.9f, 0.999f, 1e-8f, L.adam_step, 1.0f,
                                                                   L.theta_bf16.p);
       H33_CUDA(cudaGetLastError());
@@ -1259,13 +1283,13 @@ void ensure_lowp(Solver &S) {
   auto grid = [&](size_t n) { return int(std::max<size_t>(1, std::min<size_t>((n + kThreads - 1) / kThreads, size_t(S.nsm) * 16))); };
   for (auto *d : {&P.lo, &P.up}) {
     d->val16.alloc(d->val.n);
-    if (d->val.n) convert_bf16_kernel<<<grid(d->val.n), kThreads, 0, S.stream>>>(d->val.p, d->val16.p, d->val.n);
+    if (d->val.n) launch_k(S.stream, convert_bf16_kernel, grid(d->val.n), kThreads, d->val.p, d->val16.p, d->val.n);
   }
   P.alu32_fwd.alloc(P.alu_fwd.n);
-  if (P.alu_fwd.n) convert_kernel<float><<<grid(P.alu_fwd.n), kThreads, 0, S.stream>>>(P.alu_fwd.p, P.alu32_fwd.p, P.alu_fwd.n);
+  if (P.alu_fwd.n) launch_k(S.stream, convert_kernel<float>, grid(P.alu_fwd.n), kThreads, P.alu_fwd.p, P.alu32_fwd.p, P.alu_fwd.n);
   if (!P.alu_shared) {
     P.alu32_bwd.alloc(P.alu_bwd.n);
-    convert_kernel<float><<<grid(P.alu_bwd.n), kThreads, 0, S.stream>>>(P.alu_bwd.p, P.alu32_bwd.p, P.alu_bwd.n);
+    launch_k(S.stream, convert_kernel<float>, grid(P.alu_bwd.n), kThreads, P.alu_bwd.p, P.alu32_bwd.p, P.alu_bwd.n);
   }
   H33_CUDA(cudaGetLastError());
   P.lowp_version = P.numeric_version;
@@ -1393,7 +1417,7 @@ int solve_mixed_restart(Solver &S, int *Iarray, double *Rarray, int *iter, doubl
   H33_CUDA(cudaEventRecord(e0, s));
   int kernels = 1, total_inner = 0, outer = 0, error = 0;
   // r = b - A x in FP64
-  spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.r.p, S.b.p, nullptr, nullptr);
+  launch_k(s, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, S.A.view(), S.x.p, S.r.p, S.b.p, nullptr, nullptr);
   double rr = dot_device(S, S.r.p, S.r.p);
   kernels += 2;
   double res = std::sqrt(rr / S.bnrm2);
@@ -1407,7 +1431,7 @@ int solve_mixed_restart(Solver &S, int *Iarray, double *Rarray, int *iter, doubl
       error = HECMW33_ERR_NOCONV_MAXIT;
       break;
     }
-    narrow_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.r.p, S.bf.p, n3);
+    launch_k(s, narrow_kernel, S.grid_vec(), kThreads, S.r.p, S.bf.p, n3);
     H33_CUDA(cudaMemsetAsync(S.xf.p, 0, sizeof(float) * n3, s));
     run_cg<float>(S, iterPREmax, TOL_IN, MAXIT - total_inner, &kernels, 1);
     const CgState st = *S.h_state;
@@ -1419,8 +1443,8 @@ int solve_mixed_restart(Solver &S, int *Iarray, double *Rarray, int *iter, doubl
       Iarray[81] = 1;
       break;
     }
-    widen_add_kernel<<<S.grid_vec(), kThreads, 0, s>>>(S.xf.p, S.x.p, n3);
-    spmv_kernel<double, 1><<<S.grid_spmv(), kThreads, 0, s>>>(S.A.view(), S.x.p, S.r.p, S.b.p, nullptr, nullptr);
+    launch_k(s, widen_add_kernel, S.grid_vec(), kThreads, S.xf.p, S.x.p, n3);
+    launch_k(s, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, S.A.view(), S.x.p, S.r.p, S.b.p, nullptr, nullptr);
     rr = dot_device(S, S.r.p, S.r.p);
     kernels += 4;
     res = std::sqrt(rr / S.bnrm2);
@@ -1481,7 +1505,7 @@ int solve_mixed_reliable(Solver &S, int *Iarray, double *Rarray, int *iter, doub
   const float ms = run_cg<float>(S, iterPREmax, TOL, MAXIT, &kernels, 0, learned, 1, DELTA);
   const CgState st = *S.h_state;
   // fold a correction not yet carried into x64 (a stop between reliable updates)
-  widen_add_kernel<<<S.grid_vec(), kThreads, 0, S.stream>>>(S.xf.p, S.x.p, S.n3());
+  launch_k(S.stream, widen_add_kernel, S.grid_vec(), kThreads, S.xf.p, S.x.p, S.n3());
   const int error = st.error;
   *iter = st.iter;
   *resid = st.resid;
@@ -1520,7 +1544,7 @@ void launch_mr_sweep_k(Solver &S, const double *rin, double *zout) {
   for (int g = 0; g < gf; g++) {
     const int sb = P.lo.group_slice[g], se = P.lo.group_slice[g + 1];
     if (se <= sb) continue;
-    mr_sweep_fwd_kernel<K, POS><<<S.grid_mr((se - sb) * (32 / K)), kThreads, 0, s>>>(
+    launch_k(s, mr_sweep_fwd_kernel<K, POS>, S.grid_mr((se - sb) * (32 / K)), kThreads, 
         lo, P.perm_fwd.p, P.alu_fwd.p, S.N, rin, zout, S.mzpos.p, sb, se, ctl);
   }
   const int gb = int(P.up.group_slice.size()) - 1;
@@ -1533,7 +1557,7 @@ void launch_mr_sweep_k(Solver &S, const double *rin, double *zout) {
   for (int g = gb - 1; g >= 0; g--) {
     const int sb = P.up.group_slice[g], se = P.up.group_slice[g + 1];
     const int grid = S.grid_mr(std::max(se - sb, 1) * (32 / K));
-    mr_sweep_bwd_kernel<K, FUSE_RHO, POS><<<grid, kThreads, 0, s>>>(up, perm_b, alu_b, S.N, rin, zout, S.mzpos.p,
+    launch_k(s, mr_sweep_bwd_kernel<K, FUSE_RHO, POS>, grid, kThreads, up, perm_b, alu_b, S.N, rin, zout, S.mzpos.p,
                                                                      sb, se, S.mst.p, ctl, S.mpart.p, base, total);
     base += grid;
   }
@@ -1543,7 +1567,7 @@ template <bool FUSE_RHO>
 void launch_mr_sweep(Solver &S, const double *rin, double *zout) {
   Precond &P = S.pc;
   if (P.kind == 3) {
-    mr_diag_kernel<FUSE_RHO><<<S.grid_mr(S.N), kThreads, 0, S.stream>>>(P.alu_fwd.p, S.N, rin, zout, S.mst.p,
+    launch_k(S.stream, mr_diag_kernel<FUSE_RHO>, S.grid_mr(S.N), kThreads, P.alu_fwd.p, S.N, rin, zout, S.mst.p,
                                                                          S.mctl.p, S.mpart.p);
     return;
   }
@@ -1582,8 +1606,8 @@ void launch_mr_precond(Solver &S, int iterpremax) {
   const int n48 = S.N * kRhsStride;
   const int gv = std::max(1, std::min((n48 + kThreads - 1) / kThreads, S.nsm * S.occ_vec));
   if (iterpremax <= 0) {
-    copy_kernel<double><<<gv, kThreads, 0, s>>>(S.mr.p, S.mz.p, n48, nullptr);
-    mr_dot_kernel<1><<<S.grid_mr(S.N), kThreads, 0, s>>>(S.mr.p, S.mz.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
+    launch_k(s, copy_kernel<double>, gv, kThreads, S.mr.p, S.mz.p, n48, nullptr);
+    launch_k(s, mr_dot_kernel<1>, S.grid_mr(S.N), kThreads, S.mr.p, S.mz.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
     return;
   }
   if (iterpremax == 1) {
@@ -1593,35 +1617,35 @@ void launch_mr_precond(Solver &S, int iterpremax) {
   const double *in = S.mr.p;
   for (int it = 1; it <= iterpremax; it++) {
     launch_mr_sweep<false>(S, in, S.mzp.p);
-    if (it == 1) copy_kernel<double><<<gv, kThreads, 0, s>>>(S.mzp.p, S.mz.p, n48, nullptr);
-    else add_kernel<double><<<gv, kThreads, 0, s>>>(S.mzp.p, S.mz.p, n48, nullptr);
+    if (it == 1) launch_k(s, copy_kernel<double>, gv, kThreads, S.mzp.p, S.mz.p, n48, nullptr);
+    else launch_k(s, add_kernel<double>, gv, kThreads, S.mzp.p, S.mz.p, n48, nullptr);
     if (it == iterpremax) break;
-    mr_spmv_kernel<1><<<S.grid_mr(S.A.nslices * 32), kThreads, 0, s>>>(S.A.view(), S.mz.p, S.mw.p, S.mr.p, S.mst.p,
+    launch_k(s, mr_spmv_kernel<1>, S.grid_mr(S.A.nslices * 32), kThreads, S.A.view(), S.mz.p, S.mw.p, S.mr.p, S.mst.p,
                                                                        S.mctl.p, S.mpart.p);
     in = S.mw.p;
   }
-  mr_dot_kernel<1><<<S.grid_mr(S.N), kThreads, 0, s>>>(S.mr.p, S.mz.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
+  launch_k(s, mr_dot_kernel<1>, S.grid_mr(S.N), kThreads, S.mr.p, S.mz.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
 }
 
 void launch_mr_prologue(Solver &S, int nrhs, cudaGraphConditionalHandle h, int use_cond) {
   cudaStream_t s = S.stream;
   const int gs = S.grid_mr(S.A.nslices * 32);
-  mr_init_kernel<<<1, 32, 0, s>>>(S.mst.p, S.mctl.p, S.params.p, nrhs);
-  mr_spmv_kernel<1><<<gs, kThreads, 0, s>>>(S.A.view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p, S.mpart.p);
-  mr_dot_kernel<0><<<S.grid_mr(S.N), kThreads, 0, s>>>(S.mb.p, S.mb.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
-  mr_ctl_kernel<<<1, 32, 0, s>>>(S.mst.p, S.mctl.p, h, use_cond);
+  launch_k(s, mr_init_kernel, 1, 32, S.mst.p, S.mctl.p, S.params.p, nrhs);
+  launch_k(s, mr_spmv_kernel<1>, gs, kThreads, S.A.view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p, S.mpart.p);
+  launch_k(s, mr_dot_kernel<0>, S.grid_mr(S.N), kThreads, S.mb.p, S.mb.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
+  launch_k(s, mr_ctl_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
 }
 
 void launch_mr_iteration(Solver &S, int iterpremax, cudaGraphConditionalHandle h, int use_cond) {
   cudaStream_t s = S.stream;
   const int gs = S.grid_mr(S.A.nslices * 32), gn = S.grid_mr(S.N);
-  mr_iter_begin_kernel<<<1, 32, 0, s>>>(S.mst.p, S.mctl.p, h, use_cond);
+  launch_k(s, mr_iter_begin_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
   launch_mr_precond(S, iterpremax);
-  mr_update_p_kernel<<<gn, kThreads, 0, s>>>(S.mz.p, S.mp.p, S.N, S.mst.p, S.mctl.p);
-  mr_spmv_kernel<2><<<gs, kThreads, 0, s>>>(S.A.view(), S.mp.p, S.mq.p, nullptr, S.mst.p, S.mctl.p, S.mpart.p);
-  mr_update_xr_kernel<<<gn, kThreads, 0, s>>>(S.mx.p, S.mp.p, S.mr.p, S.mq.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
-  mr_spmv_kernel<3><<<gs, kThreads, 0, s>>>(S.A.view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p, S.mpart.p);
-  mr_ctl_kernel<<<1, 32, 0, s>>>(S.mst.p, S.mctl.p, h, use_cond);
+  launch_k(s, mr_update_p_kernel, gn, kThreads, S.mz.p, S.mp.p, S.N, S.mst.p, S.mctl.p);
+  launch_k(s, mr_spmv_kernel<2>, gs, kThreads, S.A.view(), S.mp.p, S.mq.p, nullptr, S.mst.p, S.mctl.p, S.mpart.p);
+  launch_k(s, mr_update_xr_kernel, gn, kThreads, S.mx.p, S.mp.p, S.mr.p, S.mq.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
+  launch_k(s, mr_spmv_kernel<3>, gs, kThreads, S.A.view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p, S.mpart.p);
+  launch_k(s, mr_ctl_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
 }
 
 // Graph of the whole multi-RHS loop (prologue + WHILE node), as build_graph.
@@ -1682,8 +1706,8 @@ float run_multi_chunk(Solver &S, int nrhs, const double *dB, double *dX, int ite
   const int n = S.N;
   const size_t n48 = size_t(n) * kRhsStride;
   const int gp = std::max(1, std::min(int((n48 + kThreads - 1) / kThreads), S.nsm * S.occ_vec));
-  mr_pack_kernel<<<gp, kThreads, 0, s>>>(dB, S.mb.p, n, nrhs);
-  mr_pack_kernel<<<gp, kThreads, 0, s>>>(dX, S.mx.p, n, nrhs);
+  launch_k(s, mr_pack_kernel, gp, kThreads, dB, S.mb.p, n, nrhs);
+  launch_k(s, mr_pack_kernel, gp, kThreads, dX, S.mx.p, n, nrhs);
   S.h_params->tol = tol;
   S.h_params->maxit = maxit;
   S.h_params->iterpremax = iterpremax;
@@ -1709,11 +1733,11 @@ float run_multi_chunk(Solver &S, int nrhs, const double *dB, double *dX, int ite
   }
   H33_CUDA(cudaEventRecord(S.ev1, s));
   // final true residuals (hecmw_rel_resid_L2_33 per RHS) and the zero-RHS lanes
-  mr_spmv_kernel<1><<<S.grid_mr(S.A.nslices * 32), kThreads, 0, s>>>(S.A.view(), S.mx.p, S.mw.p, S.mb.p, S.mst.p,
+  launch_k(s, mr_spmv_kernel<1>, S.grid_mr(S.A.nslices * 32), kThreads, S.A.view(), S.mx.p, S.mw.p, S.mb.p, S.mst.p,
                                                                      S.mctl.p, S.mpart.p);
-  mr_dot_kernel<2><<<S.grid_mr(n), kThreads, 0, s>>>(S.mw.p, S.mw.p, n, S.mst.p, S.mctl.p, S.mpart.p);
-  mr_zero_x_kernel<<<gp, kThreads, 0, s>>>(S.mx.p, n, S.mst.p);
-  mr_unpack_kernel<<<gp, kThreads, 0, s>>>(S.mx.p, dX, n, nrhs);
+  launch_k(s, mr_dot_kernel<2>, S.grid_mr(n), kThreads, S.mw.p, S.mw.p, n, S.mst.p, S.mctl.p, S.mpart.p);
+  launch_k(s, mr_zero_x_kernel, gp, kThreads, S.mx.p, n, S.mst.p);
+  launch_k(s, mr_unpack_kernel, gp, kThreads, S.mx.p, dX, n, nrhs);
   H33_CUDA(cudaGetLastError());
   H33_CUDA(cudaMemcpyAsync(S.h_mst, S.mst.p, sizeof(CgState) * kMaxRhs, cudaMemcpyDeviceToHost, s));
   H33_CUDA(cudaMemcpyAsync(S.h_mctl, S.mctl.p, sizeof(MultiCtl), cudaMemcpyDeviceToHost, s));
@@ -1974,7 +1998,7 @@ HECMW33_API void hecmw33_gpu_matvec(const int *handle, const double *X, double *
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_set_matrix first");
   const size_t bytes = sizeof(double) * S.n3();
   H33_CUDA(cudaMemcpyAsync(S.w.p, X, bytes, cudaMemcpyHostToDevice, S.stream));
-  spmv_kernel<double, 0><<<S.grid_spmv(), kThreads, 0, S.stream>>>(S.A.view(), S.w.p, S.zp.p, nullptr, nullptr,
+  launch_k(S.stream, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, S.A.view(), S.w.p, S.zp.p, nullptr, nullptr,
                                                                     nullptr);
   H33_CUDA(cudaGetLastError());
   H33_CUDA(cudaMemcpyAsync(Y, S.zp.p, bytes, cudaMemcpyDeviceToHost, S.stream));
@@ -2077,10 +2101,10 @@ HECMW33_API void hecmw33_gpu_time_spmv(const int *handle, const int *reps, doubl
   DeviceGuard dg(S.device);
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix");
   const int n = std::max(1, *reps);
-  spmv_kernel<double, 0><<<S.grid_spmv(), kThreads, 0, S.stream>>>(S.A.view(), S.x.p, S.zp.p, nullptr, nullptr, nullptr);
+  launch_k(S.stream, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, S.A.view(), S.x.p, S.zp.p, nullptr, nullptr, nullptr);
   H33_CUDA(cudaEventRecord(S.ev0, S.stream));
   for (int i = 0; i < n; i++)
-    spmv_kernel<double, 0><<<S.grid_spmv(), kThreads, 0, S.stream>>>(S.A.view(), S.x.p, S.zp.p, nullptr, nullptr,
+    launch_k(S.stream, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, S.A.view(), S.x.p, S.zp.p, nullptr, nullptr,
                                                                       nullptr);
   H33_CUDA(cudaGetLastError());
   H33_CUDA(cudaEventRecord(S.ev1, S.stream));
