@@ -412,71 +412,173 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<R> A, const R *
   if (MODE == 2) reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[1], [&](double v) { fin_pq(st, v); });
 }
 
-// Forward sweep over the slices [sbeg, send) of one colour / level, each row spread
+// Node-order sweeps (the ILU(0) level schedules, whose forward and backward orders
+// differ).  Forward sweep over the slices [sbeg, send) of one level, each row spread
 // over K lanes:  z(node) = LU^-1 ( r(node) - sum_lower A z(col) )
-// (hecmw_precond_SSOR_33.F90:309-345).
-// POS (the multicolour SSOR): the layout's columns are positions in the colour
-// order and the sweep keeps its intermediate vector zpos in that order, so a row's
-// own entries sit at zpos[row] and only the right-hand side needs the permutation;
-// its load (perm -> r) is issued before the row's gather.  Without POS (ILU(0)
-// level schedules) columns are nodes and z is gathered and written in node order.
-template <class R, class TV, class TA, int K, bool POS>
+// (hecmw_precond_SSOR_33.F90:309-345)
+template <class R, class TV, class TA, int K>
 __global__ void __launch_bounds__(kThreads) sweep_fwd_kernel(SellView<TV> L, const int *__restrict__ perm,
                                                              const TA *__restrict__ alu, int npos,
                                                              const R *__restrict__ r, R *__restrict__ z,
-                                                             R *__restrict__ zpos, int sbeg, int send,
-                                                             GroupShape gs, const CgState *st) {
+                                                             int sbeg, int send, const CgState *st) {
   pdl_entry();
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
   const int roff = lane / K;
-  const bool leader = (lane & (K - 1)) == 0;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
-    // POS layouts are uniform: the slice's rows and slots follow from its index
-    const int row = POS ? gs.row0 + (s - sbeg) * (32 / K) + roff : L.row0[s] + roff;
-    const bool active = POS ? row < gs.row1 : roff < L.nrows[s];
-    const int len = (!POS && active) ? L.rowlen[s * 32 + roff] : 0;
-    R r0 = 0, r1 = 0, r2 = 0;
-    int node = 0;
-    if (POS && active && leader) {
-      node = perm[row];
-      r0 = r[3 * node];
-      r1 = r[3 * node + 1];
-      r2 = r[3 * node + 2];
-    }
+    const bool active = roff < L.nrows[s];
+    const int row = L.row0[s] + roff;
+    const int len = active ? L.rowlen[s * 32 + roff] : 0;
     R a0 = 0, a1 = 0, a2 = 0;
-    if (POS) row_gemv_u<R, TV, K, false>(L, gs.slot0 + (s - sbeg) * gs.len, gs.len, lane, zpos, a0, a1, a2);
-    else row_gemv<R, TV, K, false>(L, s, lane, len, z, a0, a1, a2);
-    if (active && leader) {
-      if (!POS) {
-        node = perm[row];
-        r0 = r[3 * node];
-        r1 = r[3 * node + 1];
-        r2 = r[3 * node + 2];
-      }
-      R x1 = r0 - a0, x2 = r1 - a1, x3 = r2 - a2;
+    row_gemv<R, TV, K, false>(L, s, lane, len, z, a0, a1, a2);
+    if (active && (lane & (K - 1)) == 0) {
+      const int node = perm[row];
+      R x1 = r[3 * node] - a0, x2 = r[3 * node + 1] - a1, x3 = r[3 * node + 2] - a2;
       lu_solve(alu, npos, row, x1, x2, x3);
-      R *out = POS ? zpos + 3 * row : z + 3 * node;
-      out[0] = x1;
-      out[1] = x2;
-      out[2] = x3;
+      z[3 * node] = x1;
+      z[3 * node + 1] = x2;
+      z[3 * node + 2] = x3;
     }
   }
 }
 
 // Backward sweep over [sbeg, send), rows spread over K lanes:
 // z(node) -= LU^-1 ( sum_upper A z(col) )   (hecmw_precond_SSOR_33.F90:353-405).
-// POS: gathers and updates zpos in colour order and writes the finished rows to z
-// in node order.  FUSE_RHO accumulates {r}{z} of the finished rows; the last
-// launch's last CTA runs the RHO finisher.
-template <class R, class TV, class TA, int K, bool FUSE_RHO, bool POS>
+// FUSE_RHO accumulates {r}{z} of the finished rows; the last launch's last CTA
+// runs the RHO finisher.
+template <class R, class TV, class TA, int K, bool FUSE_RHO>
 __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, const int *__restrict__ perm,
                                                              const TA *__restrict__ alu, int npos,
                                                              const R *__restrict__ r, R *__restrict__ z,
-                                                             R *__restrict__ zpos, int sbeg, int send, GroupShape gs,
-                                                             CgState *st, double *partials, int part_base,
+                                                             int sbeg, int send, CgState *st,
+                                                             double *partials, int part_base,
                                                              int part_total) {
+  pdl_entry();
+  if (st && st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int roff = lane / K;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double dot = 0.0;
+  for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
+    const bool active = roff < U.nrows[s];
+    const int row = U.row0[s] + roff;
+    const int len = active ? U.rowlen[s * 32 + roff] : 0;
+    R x1 = 0, x2 = 0, x3 = 0;
+    row_gemv<R, TV, K, true>(U, s, lane, len, z, x1, x2, x3);
+    if (active && (lane & (K - 1)) == 0) {
+      const int node = perm[row];
+      lu_solve(alu, npos, row, x1, x2, x3);
+      const R z0 = z[3 * node] - x1, z1 = z[3 * node + 1] - x2, z2 = z[3 * node + 2] - x3;
+      z[3 * node] = z0;
+      z[3 * node + 1] = z1;
+      z[3 * node + 2] = z2;
+      if (FUSE_RHO)
+        dot += double(r[3 * node]) * double(z0) + double(r[3 * node + 1]) * double(z1) +
+               double(r[3 * node + 2]) * double(z2);
+    }
+  }
+  if (FUSE_RHO)
+    reduce_finish(dot, partials, part_base + blockIdx.x, part_total, &st->ticket[0],
+                  [&](double v) { fin_rho(st, v); });
+}
+
+// ---- sweeps on the uniform colour layout (multicolour SSOR) ----------------
+// Every slice of a colour has the colour's slot count (GroupShape), so a slice's rows
+// and slots follow from its index; the intermediate zpos is in colour-position order
+// (columns of the layout are positions).  A warp takes SL slices of the colour at
+// once (slices s, s + nwarps, ...) and issues their loads together: a large colour
+// then fits in one round of resident warps.
+
+// Gathers of SL slices with the same slot count; has[j]: slice j exists (warp-uniform).
+template <class R, class TV, int K, bool BACKWARD, int SL>
+__device__ __forceinline__ void slices_gemv_u(const SellView<TV> &A, const int (&slot0)[SL], const bool (&has)[SL],
+                                              int nslots, int lane, const R *__restrict__ x, R (&y)[SL][3]) {
+#pragma unroll 2
+  for (int kk = 0; kk < nslots; kk++) {
+    const int o = BACKWARD ? nslots - 1 - kk : kk;
+#pragma unroll
+    for (int j = 0; j < SL; j++) {
+      if (!has[j]) continue;
+      const int sl = slot0[j] + o;
+      const int c = __ldg(&A.col[sl * 32 + lane]);
+      const TV *v = A.val + sl * 288 + lane;
+      const R x0 = __ldg(&x[3 * c]), x1 = __ldg(&x[3 * c + 1]), x2 = __ldg(&x[3 * c + 2]);
+      const R v0 = ld_val<R>(v), v1 = ld_val<R>(v + 32), v2 = ld_val<R>(v + 64);
+      const R v3 = ld_val<R>(v + 96), v4 = ld_val<R>(v + 128), v5 = ld_val<R>(v + 160);
+      const R v6 = ld_val<R>(v + 192), v7 = ld_val<R>(v + 224), v8 = ld_val<R>(v + 256);
+      y[j][0] = fma(v2, x2, fma(v1, x1, fma(v0, x0, y[j][0])));
+      y[j][1] = fma(v5, x2, fma(v4, x1, fma(v3, x0, y[j][1])));
+      y[j][2] = fma(v8, x2, fma(v7, x1, fma(v6, x0, y[j][2])));
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < SL; j++)
+#pragma unroll
+    for (int o = K / 2; o > 0; o >>= 1) {
+      y[j][0] += __shfl_xor_sync(0xffffffffu, y[j][0], o);
+      y[j][1] += __shfl_xor_sync(0xffffffffu, y[j][1], o);
+      y[j][2] += __shfl_xor_sync(0xffffffffu, y[j][2], o);
+    }
+}
+
+// Forward sweep of one colour: zpos(pos) = LU^-1 ( r(perm(pos)) - sum_lower A zpos(col) )
+// (hecmw_precond_SSOR_33.F90:309-345).
+template <class R, class TV, class TA, int K, int SL>
+__global__ void __launch_bounds__(kThreads) sweep_fwd_uni_kernel(SellView<TV> L, const int *__restrict__ perm,
+                                                                 const TA *__restrict__ alu, int npos,
+                                                                 const R *__restrict__ r, R *__restrict__ zpos,
+                                                                 int sbeg, int send, GroupShape gs,
+                                                                 const CgState *st) {
+  pdl_entry();
+  if (st && st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int roff = lane / K;
+  const bool leader = (lane & (K - 1)) == 0;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int s0 = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s0 < send; s0 += SL * nwarps) {
+    int slot0[SL], row[SL];
+    bool has[SL], act[SL];
+    R rr[SL][3], y[SL][3];
+#pragma unroll
+    for (int j = 0; j < SL; j++) {
+      const int s = s0 + j * nwarps;
+      has[j] = s < send;
+      row[j] = gs.row0 + (s - sbeg) * (32 / K) + roff;
+      act[j] = has[j] && row[j] < gs.row1 && leader;
+      slot0[j] = gs.slot0 + (s - sbeg) * gs.len;
+      rr[j][0] = rr[j][1] = rr[j][2] = R(0);
+      y[j][0] = y[j][1] = y[j][2] = R(0);
+      if (act[j]) {
+        const int node = perm[row[j]];
+        rr[j][0] = r[3 * node];
+        rr[j][1] = r[3 * node + 1];
+        rr[j][2] = r[3 * node + 2];
+      }
+    }
+    slices_gemv_u<R, TV, K, false, SL>(L, slot0, has, gs.len, lane, zpos, y);
+#pragma unroll
+    for (int j = 0; j < SL; j++) {
+      if (!act[j]) continue;
+      R x1 = rr[j][0] - y[j][0], x2 = rr[j][1] - y[j][1], x3 = rr[j][2] - y[j][2];
+      lu_solve(alu, npos, row[j], x1, x2, x3);
+      zpos[3 * row[j]] = x1;
+      zpos[3 * row[j] + 1] = x2;
+      zpos[3 * row[j] + 2] = x3;
+    }
+  }
+}
+
+// Backward sweep of one colour: zpos(pos) -= LU^-1 ( sum_upper A zpos(col) ), the
+// finished rows also written to z in node order; FUSE_RHO accumulates {r}{z} and the
+// last launch's last CTA runs the RHO finisher (hecmw_precond_SSOR_33.F90:353-405).
+template <class R, class TV, class TA, int K, bool FUSE_RHO, int SL>
+__global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U, const int *__restrict__ perm,
+                                                                 const TA *__restrict__ alu, int npos,
+                                                                 const R *__restrict__ r, R *__restrict__ z,
+                                                                 R *__restrict__ zpos, int sbeg, int send,
+                                                                 GroupShape gs, CgState *st, double *partials,
+                                                                 int part_base, int part_total) {
   pdl_entry();
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
@@ -484,35 +586,36 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, con
   const bool leader = (lane & (K - 1)) == 0;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double dot = 0.0;
-  for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
-    const int row = POS ? gs.row0 + (s - sbeg) * (32 / K) + roff : U.row0[s] + roff;
-    const bool active = POS ? row < gs.row1 : roff < U.nrows[s];
-    const int len = (!POS && active) ? U.rowlen[s * 32 + roff] : 0;
-    int node = 0;
-    R c0 = 0, c1 = 0, c2 = 0;  // this row's current z (written by the forward sweep)
-    if (POS && active && leader) {
-      node = perm[row];
-      c0 = zpos[3 * row];
-      c1 = zpos[3 * row + 1];
-      c2 = zpos[3 * row + 2];
+  for (int s0 = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s0 < send; s0 += SL * nwarps) {
+    int slot0[SL], row[SL];
+    bool has[SL], act[SL];
+    R cz[SL][3], y[SL][3];
+#pragma unroll
+    for (int j = 0; j < SL; j++) {
+      const int s = s0 + j * nwarps;
+      has[j] = s < send;
+      row[j] = gs.row0 + (s - sbeg) * (32 / K) + roff;
+      act[j] = has[j] && row[j] < gs.row1 && leader;
+      slot0[j] = gs.slot0 + (s - sbeg) * gs.len;
+      cz[j][0] = cz[j][1] = cz[j][2] = R(0);
+      y[j][0] = y[j][1] = y[j][2] = R(0);
+      if (act[j]) {  // this row's current value (written by the forward sweep)
+        cz[j][0] = zpos[3 * row[j]];
+        cz[j][1] = zpos[3 * row[j] + 1];
+        cz[j][2] = zpos[3 * row[j] + 2];
+      }
     }
-    R x1 = 0, x2 = 0, x3 = 0;
-    if (POS) row_gemv_u<R, TV, K, true>(U, gs.slot0 + (s - sbeg) * gs.len, gs.len, lane, zpos, x1, x2, x3);
-    else row_gemv<R, TV, K, true>(U, s, lane, len, z, x1, x2, x3);
-    if (active && leader) {
-      if (!POS) {
-        node = perm[row];
-        c0 = z[3 * node];
-        c1 = z[3 * node + 1];
-        c2 = z[3 * node + 2];
-      }
-      lu_solve(alu, npos, row, x1, x2, x3);
-      const R z0 = c0 - x1, z1 = c1 - x2, z2 = c2 - x3;
-      if (POS) {
-        zpos[3 * row] = z0;
-        zpos[3 * row + 1] = z1;
-        zpos[3 * row + 2] = z2;
-      }
+    slices_gemv_u<R, TV, K, true, SL>(U, slot0, has, gs.len, lane, zpos, y);
+#pragma unroll
+    for (int j = 0; j < SL; j++) {
+      if (!act[j]) continue;
+      R x1 = y[j][0], x2 = y[j][1], x3 = y[j][2];
+      lu_solve(alu, npos, row[j], x1, x2, x3);
+      const R z0 = cz[j][0] - x1, z1 = cz[j][1] - x2, z2 = cz[j][2] - x3;
+      zpos[3 * row[j]] = z0;
+      zpos[3 * row[j] + 1] = z1;
+      zpos[3 * row[j] + 2] = z2;
+      const int node = perm[row[j]];
       z[3 * node] = z0;
       z[3 * node + 1] = z1;
       z[3 * node + 2] = z2;

@@ -83,6 +83,12 @@ void launch_k(cudaStream_t s, void (*kern)(KArgs...), int grid, int block, Args 
 // 4, 8 or 16).  Several lanes per row shorten each row's dependent load
 // chain and multiply the warps of a colour, which the sweeps need: a colour holds
 // a tenth of the rows, too few one-lane rows to cover HBM latency.
+// Slices a warp of the SSOR sweeps takes at once (HECMW33_SWEEP_SLICES: 1 or 2).
+int sweep_slices() {
+  const char *e = std::getenv("HECMW33_SWEEP_SLICES");
+  return (e && e[0] == '1') ? 1 : 2;
+}
+
 int sweep_lanes() {
   const char *e = std::getenv("HECMW33_SWEEP_LANES");
   const int k = e ? std::atoi(e) : 4;
@@ -205,7 +211,7 @@ struct Solver {
   int device = 0;
   cudaStream_t stream = nullptr;
   int nsm = 148;
-  int occ_spmv = 4, occ_sweep = 4, occ_vec = 8;
+  int occ_spmv = 4, occ_sweep = 4, occ_vec = 8, occ_sweep_uni = 4;
   // matrix
   bool has_matrix = false;
   int N = 0, NPL = 0, NPU = 0;
@@ -254,7 +260,9 @@ struct Solver {
     H33_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     H33_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_spmv, spmv_kernel<double, 2>, kThreads, 0));
-    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep, sweep_bwd_kernel<double, double, double, 8, true, true>, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep, sweep_bwd_kernel<double, double, double, 8, true>, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep_uni, sweep_bwd_uni_kernel<double, double, double, 4, true, 2>, kThreads, 0));
+    occ_sweep_uni = std::max(occ_sweep_uni, 1);
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_vec, update_xr_kernel<double>, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mr, mr_sweep_bwd_kernel<8, true, true>, kThreads, 0));
     occ_spmv = std::max(occ_spmv, 1);
@@ -294,6 +302,10 @@ struct Solver {
   int grid_spmv() const {
     const int need = (A.nslices + kWarpsPerCta - 1) / kWarpsPerCta;
     return std::max(1, std::min(need, nsm * occ_spmv));
+  }
+  int grid_sweep_uni(int nslices, int sl) const {
+    const int need = (nslices + kWarpsPerCta * sl - 1) / (kWarpsPerCta * sl);
+    return std::max(1, std::min(need, nsm * occ_sweep_uni));
   }
   int grid_sweep(int nslices) const {
     const int need = (nslices + kWarpsPerCta - 1) / kWarpsPerCta;
@@ -586,9 +598,10 @@ Views<float> views(Solver &S, float, int lowp = 0) {
 
 // z = M^-1 r, one pass; FUSE_RHO adds the RHO reduction + finisher.  K = lanes per
 // row of the sweep layouts.
-template <class R, class TV, class TA, bool FUSE_RHO, int K, bool POS>
-void launch_sweep_k(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f, const TA *alu_b,
-                    const R *rin, R *zout, R *zpos, CgState *st) {
+// Node-order sweeps: the ILU(0) level schedules.
+template <class R, class TV, class TA, bool FUSE_RHO, int K>
+void launch_sweep_node(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f,
+                       const TA *alu_b, const R *rin, R *zout, CgState *st) {
   Precond &P = S.pc;
   cudaStream_t s = S.stream;
   const int *perm_b = P.alu_shared ? P.perm_fwd.p : P.perm_bwd.p;
@@ -596,55 +609,83 @@ void launch_sweep_k(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, c
   for (int g = 0; g < gf; g++) {
     const int sb = P.lo.group_slice[g], se = P.lo.group_slice[g + 1];
     if (se <= sb) continue;
-    const GroupShape gsh = POS ? GroupShape{P.lo.group_rows[g], P.lo.group_rows[g + 1], P.lo.group_slot0[g],
-                                            P.lo.group_len[g]}
-                               : GroupShape{0, 0, 0, 0};
-    launch_k(s, sweep_fwd_kernel<R, TV, TA, K, POS>, S.grid_sweep(se - sb), kThreads, lo, P.perm_fwd.p, alu_f, S.N,
-                                                                                   rin, zout, zpos, sb, se, gsh, st);
+    launch_k(s, sweep_fwd_kernel<R, TV, TA, K>, S.grid_sweep(se - sb), kThreads, lo, P.perm_fwd.p, alu_f, S.N, rin,
+             zout, sb, se, st);
   }
   const int gb = int(P.up.group_slice.size()) - 1;
   int total = 0;
-  for (int g = gb - 1; g >= 0; g--) {
-    const int sb = P.up.group_slice[g], se = P.up.group_slice[g + 1];
-    total += S.grid_sweep(std::max(se - sb, 1));
-  }
+  for (int g = gb - 1; g >= 0; g--)
+    total += S.grid_sweep(std::max(P.up.group_slice[g + 1] - P.up.group_slice[g], 1));
   int base = 0;
   for (int g = gb - 1; g >= 0; g--) {
     const int sb = P.up.group_slice[g], se = P.up.group_slice[g + 1];
     const int grid = S.grid_sweep(std::max(se - sb, 1));
     // a group without slices still launches (one idle CTA) so that the reduction
     // ticket count stays exact
-    const GroupShape gsh = POS ? GroupShape{P.up.group_rows[g], P.up.group_rows[g + 1], P.up.group_slot0[g],
-                                            P.up.group_len[g]}
-                               : GroupShape{0, 0, 0, 0};
-    launch_k(s, sweep_bwd_kernel<R, TV, TA, K, FUSE_RHO, POS>, grid, kThreads, up, perm_b, alu_b, S.N, rin, zout, zpos,
-                                                                            sb, se, gsh, st, S.partials.p, base,
-                                                                            total);
+    launch_k(s, sweep_bwd_kernel<R, TV, TA, K, FUSE_RHO>, grid, kThreads, up, perm_b, alu_b, S.N, rin, zout, sb, se,
+             st, S.partials.p, base, total);
     base += grid;
   }
 }
 
-// Lanes per row are 4, 8 or 16 (sweep_lanes()); POS for the multicolour SSOR layout
-// (columns renumbered to colour positions), node order for the ILU(0) levels.
+// Uniform colour layout (multicolour SSOR): intermediate in colour-position order,
+// SL slices per warp.
+template <class R, class TV, class TA, bool FUSE_RHO, int K, int SL>
+void launch_sweep_uni(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f, const R *rin,
+                      R *zout, R *zpos, CgState *st) {
+  Precond &P = S.pc;
+  cudaStream_t s = S.stream;
+  const int gf = int(P.lo.group_slice.size()) - 1;
+  for (int g = 0; g < gf; g++) {
+    const int sb = P.lo.group_slice[g], se = P.lo.group_slice[g + 1];
+    if (se <= sb) continue;
+    const GroupShape gsh{P.lo.group_rows[g], P.lo.group_rows[g + 1], P.lo.group_slot0[g], P.lo.group_len[g]};
+    launch_k(s, sweep_fwd_uni_kernel<R, TV, TA, K, SL>, S.grid_sweep_uni(se - sb, SL), kThreads, lo, P.perm_fwd.p,
+             alu_f, S.N, rin, zpos, sb, se, gsh, st);
+  }
+  const int gb = int(P.up.group_slice.size()) - 1;
+  int total = 0;
+  for (int g = gb - 1; g >= 0; g--)
+    total += S.grid_sweep_uni(std::max(P.up.group_slice[g + 1] - P.up.group_slice[g], 1), SL);
+  int base = 0;
+  for (int g = gb - 1; g >= 0; g--) {
+    const int sb = P.up.group_slice[g], se = P.up.group_slice[g + 1];
+    const int grid = S.grid_sweep_uni(std::max(se - sb, 1), SL);
+    const GroupShape gsh{P.up.group_rows[g], P.up.group_rows[g + 1], P.up.group_slot0[g], P.up.group_len[g]};
+    launch_k(s, sweep_bwd_uni_kernel<R, TV, TA, K, FUSE_RHO, SL>, grid, kThreads, up, P.perm_fwd.p, alu_f, S.N, rin,
+             zout, zpos, sb, se, gsh, st, S.partials.p, base, total);
+    base += grid;
+  }
+}
+
+// Lanes per row are 4, 8 or 16 (sweep_lanes()).
 template <class R, class TV, class TA, bool FUSE_RHO>
 void launch_sweep_t(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f, const TA *alu_b,
                     const R *rin, R *zout, R *zpos, CgState *st) {
   Precond &P = S.pc;
   if (P.kind == 3) {
-    launch_k(S.stream, diag_kernel<R, TA, FUSE_RHO>, S.grid_vec(), kThreads, alu_f, S.N, rin, zout, st, S.partials.p);
+    launch_k(S.stream, diag_kernel<R, TA, FUSE_RHO>, S.grid_vec(), kThreads, alu_f, S.N, rin, zout, st,
+             S.partials.p);
     return;
   }
   if (P.pos_cols) {
+    const bool two = sweep_slices() == 2;
     switch (P.lo.lanes) {
-      case 4: return launch_sweep_k<R, TV, TA, FUSE_RHO, 4, true>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
-      case 16: return launch_sweep_k<R, TV, TA, FUSE_RHO, 16, true>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
-      default: return launch_sweep_k<R, TV, TA, FUSE_RHO, 8, true>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
+      case 8:
+        return two ? launch_sweep_uni<R, TV, TA, FUSE_RHO, 8, 2>(S, lo, up, alu_f, rin, zout, zpos, st)
+                   : launch_sweep_uni<R, TV, TA, FUSE_RHO, 8, 1>(S, lo, up, alu_f, rin, zout, zpos, st);
+      case 16:
+        return two ? launch_sweep_uni<R, TV, TA, FUSE_RHO, 16, 2>(S, lo, up, alu_f, rin, zout, zpos, st)
+                   : launch_sweep_uni<R, TV, TA, FUSE_RHO, 16, 1>(S, lo, up, alu_f, rin, zout, zpos, st);
+      default:
+        return two ? launch_sweep_uni<R, TV, TA, FUSE_RHO, 4, 2>(S, lo, up, alu_f, rin, zout, zpos, st)
+                   : launch_sweep_uni<R, TV, TA, FUSE_RHO, 4, 1>(S, lo, up, alu_f, rin, zout, zpos, st);
     }
   }
   switch (P.lo.lanes) {
-    case 4: return launch_sweep_k<R, TV, TA, FUSE_RHO, 4, false>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
-    case 16: return launch_sweep_k<R, TV, TA, FUSE_RHO, 16, false>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
-    default: return launch_sweep_k<R, TV, TA, FUSE_RHO, 8, false>(S, lo, up, alu_f, alu_b, rin, zout, zpos, st);
+    case 8: return launch_sweep_node<R, TV, TA, FUSE_RHO, 8>(S, lo, up, alu_f, alu_b, rin, zout, st);
+    case 16: return launch_sweep_node<R, TV, TA, FUSE_RHO, 16>(S, lo, up, alu_f, alu_b, rin, zout, st);
+    default: return launch_sweep_node<R, TV, TA, FUSE_RHO, 4>(S, lo, up, alu_f, alu_b, rin, zout, st);
   }
 }
 
