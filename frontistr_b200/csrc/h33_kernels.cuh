@@ -494,7 +494,8 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, con
 template <class R, class TV, int K, bool BACKWARD, int SL>
 __device__ __forceinline__ void slices_gemv_u(const SellView<TV> &A, const int (&slot0)[SL], const bool (&has)[SL],
                                               int nslots, int lane, const R *__restrict__ x, R (&y)[SL][3]) {
-#pragma unroll 2
+  // the same number of slots in flight for any SL
+#pragma unroll (4 / SL)
   for (int kk = 0; kk < nslots; kk++) {
     const int o = BACKWARD ? nslots - 1 - kk : kk;
 #pragma unroll
@@ -587,7 +588,7 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U,
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double dot = 0.0;
   for (int s0 = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s0 < send; s0 += SL * nwarps) {
-    int slot0[SL], row[SL];
+    int slot0[SL], row[SL], node[SL];
     bool has[SL], act[SL];
     R cz[SL][3], y[SL][3];
 #pragma unroll
@@ -599,7 +600,9 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U,
       slot0[j] = gs.slot0 + (s - sbeg) * gs.len;
       cz[j][0] = cz[j][1] = cz[j][2] = R(0);
       y[j][0] = y[j][1] = y[j][2] = R(0);
-      if (act[j]) {  // this row's current value (written by the forward sweep)
+      node[j] = 0;
+      if (act[j]) {  // this row's node and current value (written by the forward sweep)
+        node[j] = perm[row[j]];
         cz[j][0] = zpos[3 * row[j]];
         cz[j][1] = zpos[3 * row[j] + 1];
         cz[j][2] = zpos[3 * row[j] + 2];
@@ -615,13 +618,12 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U,
       zpos[3 * row[j]] = z0;
       zpos[3 * row[j] + 1] = z1;
       zpos[3 * row[j] + 2] = z2;
-      const int node = perm[row[j]];
-      z[3 * node] = z0;
-      z[3 * node + 1] = z1;
-      z[3 * node + 2] = z2;
+      z[3 * node[j]] = z0;
+      z[3 * node[j] + 1] = z1;
+      z[3 * node[j] + 2] = z2;
       if (FUSE_RHO)
-        dot += double(r[3 * node]) * double(z0) + double(r[3 * node + 1]) * double(z1) +
-               double(r[3 * node + 2]) * double(z2);
+        dot += double(r[3 * node[j]]) * double(z0) + double(r[3 * node[j] + 1]) * double(z1) +
+               double(r[3 * node[j] + 2]) * double(z2);
     }
   }
   if (FUSE_RHO)

@@ -83,10 +83,14 @@ void launch_k(cudaStream_t s, void (*kern)(KArgs...), int grid, int block, Args 
 // 4, 8 or 16).  Several lanes per row shorten each row's dependent load
 // chain and multiply the warps of a colour, which the sweeps need: a colour holds
 // a tenth of the rows, too few one-lane rows to cover HBM latency.
-// Slices a warp of the SSOR sweeps takes at once (HECMW33_SWEEP_SLICES: 1 or 2).
-int sweep_slices() {
+// Slices a warp of the SSOR sweeps takes at once: 2 for BF16-stored values (their
+// loads are short; two slices keep more of them in flight: 0.686 -> 0.661 s on the
+// 100^3 cube), 1 for FP64 / FP32 values (two slices cost registers and occupancy
+// there).  HECMW33_SWEEP_SLICES=1 or 2 forces one choice.
+int sweep_slices(bool bf16_values) {
   const char *e = std::getenv("HECMW33_SWEEP_SLICES");
-  return (e && e[0] == '1') ? 1 : 2;
+  if (e && (e[0] == '1' || e[0] == '2')) return e[0] - '0';
+  return bf16_values ? 2 : 1;
 }
 
 int sweep_lanes() {
@@ -211,7 +215,7 @@ struct Solver {
   int device = 0;
   cudaStream_t stream = nullptr;
   int nsm = 148;
-  int occ_spmv = 4, occ_sweep = 4, occ_vec = 8, occ_sweep_uni = 4;
+  int occ_spmv = 4, occ_sweep = 4, occ_vec = 8, occ_sweep_uni = 4, occ_sweep_uni2 = 4;
   // matrix
   bool has_matrix = false;
   int N = 0, NPL = 0, NPU = 0;
@@ -261,8 +265,10 @@ struct Solver {
     H33_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_spmv, spmv_kernel<double, 2>, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep, sweep_bwd_kernel<double, double, double, 8, true>, kThreads, 0));
-    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep_uni, sweep_bwd_uni_kernel<double, double, double, 4, true, 2>, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep_uni, sweep_bwd_uni_kernel<double, double, double, 4, true, 1>, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep_uni2, sweep_bwd_uni_kernel<double, __nv_bfloat16, float, 4, true, 2>, kThreads, 0));
     occ_sweep_uni = std::max(occ_sweep_uni, 1);
+    occ_sweep_uni2 = std::max(occ_sweep_uni2, 1);
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_vec, update_xr_kernel<double>, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mr, mr_sweep_bwd_kernel<8, true, true>, kThreads, 0));
     occ_spmv = std::max(occ_spmv, 1);
@@ -305,7 +311,7 @@ struct Solver {
   }
   int grid_sweep_uni(int nslices, int sl) const {
     const int need = (nslices + kWarpsPerCta * sl - 1) / (kWarpsPerCta * sl);
-    return std::max(1, std::min(need, nsm * occ_sweep_uni));
+    return std::max(1, std::min(need, nsm * (sl == 2 ? occ_sweep_uni2 : occ_sweep_uni)));
   }
   int grid_sweep(int nslices) const {
     const int need = (nslices + kWarpsPerCta - 1) / kWarpsPerCta;
@@ -669,7 +675,7 @@ void launch_sweep_t(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, c
     return;
   }
   if (P.pos_cols) {
-    const bool two = sweep_slices() == 2;
+    const bool two = sweep_slices(sizeof(TV) == 2) == 2;
     switch (P.lo.lanes) {
       case 8:
         return two ? launch_sweep_uni<R, TV, TA, FUSE_RHO, 8, 2>(S, lo, up, alu_f, rin, zout, zpos, st)
