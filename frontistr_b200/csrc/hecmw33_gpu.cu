@@ -83,14 +83,14 @@ void launch_k(cudaStream_t s, void (*kern)(KArgs...), int grid, int block, Args 
 // 4, 8 or 16).  Several lanes per row shorten each row's dependent load
 // chain and multiply the warps of a colour, which the sweeps need: a colour holds
 // a tenth of the rows, too few one-lane rows to cover HBM latency.
-// Slices a warp of the SSOR sweeps takes at once: 2 for BF16-stored values (their
-// loads are short; two slices keep more of them in flight: 0.686 -> 0.661 s on the
-// 100^3 cube), 1 for FP64 / FP32 values (two slices cost registers and occupancy
-// there).  HECMW33_SWEEP_SLICES=1 or 2 forces one choice.
+// Slices a warp of the SSOR sweeps takes at once (HECMW33_SWEEP_SLICES=2 selects two).
+// One is the default: on the 100^3 cube two slices measured 0.947 / 0.806 s (FP64) and
+// 0.709 / 0.697 s (BF16-stored preconditioner) against one -- the extra registers cost
+// more occupancy than the longer load batches gain.
 int sweep_slices(bool bf16_values) {
+  (void)bf16_values;
   const char *e = std::getenv("HECMW33_SWEEP_SLICES");
-  if (e && (e[0] == '1' || e[0] == '2')) return e[0] - '0';
-  return bf16_values ? 2 : 1;
+  return (e && e[0] == '2') ? 2 : 1;
 }
 
 int sweep_lanes() {
