@@ -25,6 +25,7 @@ struct MultiCtl {
   int all_done;
   int guard;
   int nrhs;
+  int fault;  // a bounded wait of the tiled SpMM ran out (reported as an error)
   unsigned int ticket[8];
 };
 
@@ -183,6 +184,131 @@ __global__ void __launch_bounds__(kThreads) mr_spmv_kernel(SellView<double> A, c
       }
       loop_ctl(s, 0, 0);  // the loop decision over all RHS is mr_ctl_kernel's
     });
+}
+
+// ---- tiled SpMM: p staged in shared memory by the bulk-copy engine ------------
+// A tile is 16 consecutive block rows (half a slice of the SpMV layout).  The host
+// lists each tile's distinct columns (tile_cols[tile_ptr[t] ..]) and, for every block,
+// the column's place in that list (lidx, same layout as col).  Warp 0 copies the
+// 384-byte rows p[c][0..47] of the tile's columns into shared memory with
+// cp.async.bulk on an mbarrier; the half-warps then read p from shared memory.  Each
+// p row crosses L2 once per tile instead of once per block that uses it.
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Waits for the mbarrier phase `parity`; bounded by two seconds of the global
+// timer (try_wait itself suspends for a bounded time), returns false when it ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
+  const uint32_t a = smem_addr(mbar);
+  uint64_t t0, t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 > 2000000000ull) return false;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) mr_spmm_tiled_kernel(SellView<double> A, const int *__restrict__ tile_ptr,
+                                                                 const int *__restrict__ tile_cols,
+                                                                 const uint16_t *__restrict__ lidx, int ntiles,
+                                                                 const double *__restrict__ x, double *__restrict__ y,
+                                                                 CgState *st, MultiCtl *ctl, double *partials) {
+  pdl_entry();
+  extern __shared__ __align__(128) double xs[];
+  __shared__ __align__(8) uint64_t mbar;
+  if (ctl->all_done) return;
+  const int l = threadIdx.x & 15, hw = threadIdx.x >> 4;
+  const bool mine = !st[l].done;
+  const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  uint32_t parity = 0;
+  double dot = 0.0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int c0 = tile_ptr[t], nc = tile_ptr[t + 1] - c0;
+    if (threadIdx.x < 32) {
+      // the previous tile's reads of xs are complete (barrier below); order them
+      // before the copy engine's writes
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      if (threadIdx.x == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&mbar)),
+                     "r"(uint32_t(nc) * 384u)
+                     : "memory");
+      __syncwarp();
+      for (int i = threadIdx.x; i < nc; i += 32) {
+        const double *src = x + size_t(tile_cols[c0 + i]) * kRhsStride;
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 384, [%2];" ::"r"(
+                smem_addr(xs + size_t(i) * kRhsStride)),
+            "l"(src), "r"(smem_addr(&mbar))
+            : "memory");
+      }
+    }
+    const bool ok = mbar_wait(&mbar, parity);
+    parity ^= 1u;
+    if (!ok) {
+      if (threadIdx.x == 0) atomicExch(&ctl->fault, 1);
+      mbar_wait(&mbar, parity ^ 1u);  // the copies of this tile, once more (bounded)
+    } else {
+      const int s = t >> 1, roff = 16 * (t & 1) + hw;
+      if (roff < A.nrows[s]) {
+        const int row = A.row0[s] + roff;
+        const int len = A.rowlen[s * 32 + roff];
+        const int slot0 = A.slot0[s];
+        double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+        for (int k0 = 0; k0 < len; k0 += 16) {
+          const int kn = min(16, len - k0);
+          int myi = 0;
+          double mv[9];
+#pragma unroll
+          for (int e = 0; e < 9; e++) mv[e] = 0.0;
+          if (l < kn) {
+            const int sl = slot0 + k0 + l;
+            myi = lidx[sl * 32 + roff];
+            const double *v = A.val + sl * 288 + roff;
+#pragma unroll
+            for (int e = 0; e < 9; e++) mv[e] = __ldg(v + 32 * e);
+          }
+#pragma unroll 4
+          for (int kk = 0; kk < kn; kk++) {
+            const int li = __shfl_sync(hmask, myi, kk, 16);
+            const double *xc = xs + li * kRhsStride + l;
+            const double x0 = xc[0], x1 = xc[16], x2 = xc[32];
+            double v[9];
+#pragma unroll
+            for (int e = 0; e < 9; e++) v[e] = __shfl_sync(hmask, mv[e], kk, 16);
+            y0 = fma(v[2], x2, fma(v[1], x1, fma(v[0], x0, y0)));
+            y1 = fma(v[5], x2, fma(v[4], x1, fma(v[3], x0, y1)));
+            y2 = fma(v[8], x2, fma(v[7], x1, fma(v[6], x0, y2)));
+          }
+        }
+        if (mine) {
+          const size_t o = size_t(row) * kRhsStride + l;
+          y[o] = y0;
+          y[o + 16] = y1;
+          y[o + 32] = y2;
+          dot += x[o] * y0 + x[o + 16] * y1 + x[o + 32] * y2;
+        }
+      }
+    }
+    __syncthreads();  // every half-warp is done with xs before the next tile's copies
+  }
+  if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&mbar)) : "memory");
+  mr_reduce_finish(dot, partials, blockIdx.x, gridDim.x, &ctl->ticket[1], [&](int k, double v) {
+    if (!st[k].done) fin_pq(&st[k], v);
+  });
 }
 
 // Forward sweep over the slices [sb, se) of one colour / level, 16 RHS at once.
@@ -399,6 +525,7 @@ __global__ void mr_init_kernel(CgState *st, MultiCtl *ctl, const CgParams *prm, 
     ctl->all_done = 0;
     ctl->guard = 0;
     ctl->nrhs = nrhs;
+    ctl->fault = 0;
     for (int i = 0; i < 8; i++) ctl->ticket[i] = 0u;
   }
 }

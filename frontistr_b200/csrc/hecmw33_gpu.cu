@@ -64,6 +64,28 @@ bool pdl_mode() {
   return e && e[0] == '1';
 }
 
+// The multi-RHS loop's SpMM stages p through shared memory (mr_spmm_tiled_kernel);
+// HECMW33_MR_TILED=0 keeps the untiled SpMM.
+bool mr_tiled_mode() {
+  const char *e = std::getenv("HECMW33_MR_TILED");
+  return !(e && e[0] == '0');
+}
+
+template <typename... KArgs, typename... Args>
+void launch_ks(cudaStream_t s, void (*kern)(KArgs...), int grid, int block, size_t smem, Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(grid), 1, 1);
+  cfg.blockDim = dim3(unsigned(block), 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_mode() ? 1 : 0;
+  H33_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
+}
+
 template <typename... KArgs, typename... Args>
 void launch_k(cudaStream_t s, void (*kern)(KArgs...), int grid, int block, Args &&...args) {
   cudaLaunchConfig_t cfg = {};
@@ -253,6 +275,11 @@ struct Solver {
   MultiCtl *h_mctl = nullptr;
   GraphSlot gm;
   int occ_mr = 4;
+  // tiled SpMM of the multi-RHS loop: per 16-row tile its distinct columns, and each
+  // block's place in that list
+  DevArray<int> mt_ptr, mt_cols;
+  DevArray<uint16_t> mt_lidx;
+  int mt_generation = -1, mt_maxcols = 0, mt_occ = 0, mt_ntiles = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int build_counter = 0;  // monotonic id of preconditioner builds (graph cache key)
   // last-solve record
@@ -1637,6 +1664,7 @@ void launch_mr_sweep(Solver &S, const double *rin, double *zout) {
 int mr_max_parts(Solver &S) {
   Precond &P = S.pc;
   int m = std::max(S.grid_mr(S.A.nslices * 32), S.grid_mr(S.N));
+  if (S.mt_occ > 0) m = std::max(m, std::min(S.mt_ntiles, S.nsm * S.mt_occ));
   if (P.valid && P.kind != 3) {
     const int K = P.lo.lanes;
     int total = 0;
@@ -1690,7 +1718,12 @@ void launch_mr_iteration(Solver &S, int iterpremax, cudaGraphConditionalHandle h
   launch_k(s, mr_iter_begin_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
   launch_mr_precond(S, iterpremax);
   launch_k(s, mr_update_p_kernel, gn, kThreads, S.mz.p, S.mp.p, S.N, S.mst.p, S.mctl.p);
-  launch_k(s, mr_spmv_kernel<2>, gs, kThreads, S.A.view(), S.mp.p, S.mq.p, nullptr, S.mst.p, S.mctl.p, S.mpart.p);
+  if (mr_tiled_mode() && S.mt_occ > 0)
+    launch_ks(s, mr_spmm_tiled_kernel, std::min(S.mt_ntiles, S.nsm * S.mt_occ), kThreads,
+              size_t(S.mt_maxcols) * kRhsStride * sizeof(double), S.A.view(), S.mt_ptr.p, S.mt_cols.p,
+              S.mt_lidx.p, S.mt_ntiles, S.mp.p, S.mq.p, S.mst.p, S.mctl.p, S.mpart.p);
+  else
+    launch_k(s, mr_spmv_kernel<2>, gs, kThreads, S.A.view(), S.mp.p, S.mq.p, nullptr, S.mst.p, S.mctl.p, S.mpart.p);
   launch_k(s, mr_update_xr_kernel, gn, kThreads, S.mx.p, S.mp.p, S.mr.p, S.mq.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
   launch_k(s, mr_spmv_kernel<3>, gs, kThreads, S.A.view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p, S.mpart.p);
   launch_k(s, mr_ctl_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
@@ -1737,7 +1770,56 @@ void build_graph_multi(Solver &S, int iterpremax, int nrhs) {
   G.prologue_kernels = int(nall) - 1;
 }
 
+// Tiles of the SpMV layout for mr_spmm_tiled_kernel (built from the device layout).
+void build_mr_tiles(Solver &S) {
+  const DevSell<double> &A = S.A;
+  const int ns = A.nslices;
+  std::vector<int> row0(static_cast<size_t>(ns)), nrows(static_cast<size_t>(ns)), slot0(static_cast<size_t>(ns));
+  std::vector<int> rowlen(static_cast<size_t>(ns) * 32), col(static_cast<size_t>(A.nslots) * 32);
+  H33_CUDA(cudaMemcpy(nrows.data(), A.nrows.p, sizeof(int) * ns, cudaMemcpyDeviceToHost));
+  H33_CUDA(cudaMemcpy(slot0.data(), A.slot0.p, sizeof(int) * ns, cudaMemcpyDeviceToHost));
+  H33_CUDA(cudaMemcpy(rowlen.data(), A.rowlen.p, sizeof(int) * rowlen.size(), cudaMemcpyDeviceToHost));
+  H33_CUDA(cudaMemcpy(col.data(), A.col.p, sizeof(int) * col.size(), cudaMemcpyDeviceToHost));
+  const int ntiles = 2 * ns;
+  std::vector<int> ptr(static_cast<size_t>(ntiles) + 1, 0), cols;
+  std::vector<uint16_t> lidx(col.size(), 0);
+  std::vector<int> mark(static_cast<size_t>(S.N), -1), local(static_cast<size_t>(S.N), 0);
+  int maxc = 0;
+  cols.reserve(size_t(ntiles) * 192);
+  for (int t = 0; t < ntiles; t++) {
+    const int sl = t >> 1, r0 = 16 * (t & 1), r1 = std::min(r0 + 16, nrows[sl]);
+    int n = 0;
+    for (int r = r0; r < r1; r++)
+      for (int k = 0; k < rowlen[size_t(sl) * 32 + r]; k++) {
+        const size_t at = (size_t(slot0[sl]) + k) * 32 + r;
+        const int c = col[at];
+        if (mark[c] != t) {
+          mark[c] = t;
+          local[c] = n++;
+          cols.push_back(c);
+        }
+        lidx[at] = uint16_t(local[c]);
+      }
+    ptr[t + 1] = ptr[t] + n;
+    maxc = std::max(maxc, n);
+  }
+  S.mt_ptr.upload(ptr, S.stream);
+  S.mt_cols.upload(cols, S.stream);
+  S.mt_lidx.upload(lidx, S.stream);
+  S.mt_maxcols = maxc;
+  S.mt_ntiles = ntiles;
+  const size_t smem = size_t(maxc) * kRhsStride * sizeof(double);
+  S.mt_occ = 0;
+  if (smem <= size_t(200) * 1024) {
+    H33_CUDA(cudaFuncSetAttribute(mr_spmm_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&S.mt_occ, mr_spmm_tiled_kernel, kThreads, smem));
+  }
+  S.sync();
+  S.mt_generation = S.generation;
+}
+
 void ensure_multi_buffers(Solver &S) {
+  if (S.mt_generation != S.generation) build_mr_tiles(S);
   const size_t n48 = size_t(S.N) * kRhsStride;
   for (auto *v : {&S.mb, &S.mx, &S.mr, &S.mz, &S.mp, &S.mq, &S.mw, &S.mzp, &S.mzpos}) v->alloc(n48);
   S.mst.alloc(kMaxRhs);
@@ -1793,6 +1875,7 @@ float run_multi_chunk(Solver &S, int nrhs, const double *dB, double *dX, int ite
   float ms = 0.0f;
   H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
   if (!S.h_mctl->all_done) throw Failure(HECMW33_ERR_TIMEOUT, "multi-RHS loop ended without a decision");
+  if (S.h_mctl->fault) throw Failure(HECMW33_ERR_TIMEOUT, "multi-RHS SpMM: a bulk copy did not complete in time");
   for (int k = 0; k < nrhs; k++) {
     const CgState &st = S.h_mst[k];
     iter[k] = st.zero_rhs ? 0 : st.iter;
