@@ -104,3 +104,22 @@ def test_multi_maxit_and_initial_guess():
         for k in range(3):
             assert rec2["iter"][k] <= 3
             assert Oracle(m).rel_resid(X[k], B[k]) <= 1e-8
+
+
+def test_multi_tiled_spmm_matches(monkeypatch):
+    """The opt-in tiled SpMM (p staged in shared memory by bulk copies) sums the same
+    products in the same order as the untiled one: identical results."""
+    m = box_system(10, 9, 24, jitter=0.1, seed=4)
+    B = load_cases(m, 5, seed=2)
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("HECMW33_MR_TILED", mode)
+        ia, ra = flags(m, 1)
+        X = np.zeros_like(B)
+        with GpuSolver() as s:  # a new handle: the captured graph follows the mode
+            s.set_matrix(m)
+            rec = s.solve_multi(B, X, ia, ra)
+        assert rec["error"] == 0
+        out[mode] = (X, list(rec["iter"]))
+    assert out["0"][1] == out["1"][1]
+    assert np.array_equal(out["0"][0], out["1"][0])
