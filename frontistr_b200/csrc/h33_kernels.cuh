@@ -324,8 +324,15 @@ __device__ __forceinline__ void row_gemv_u(const SellView<TV> &A, int slot0, int
 
 // Launch parameters of one colour of a uniform layout: rows [row0, row1) in slices of
 // 32/K rows, slice j of the colour starting at slot slot0 + j*len.
-struct GroupShape {
-  int row0, row1, slot0, len;
+// One colour of a run-table layout: rows [row0, row1), 32/K rows per slice; run r
+// covers the colour's slices slice[r] .. slice[r+1]-1 (relative to its first slice),
+// starting at slot slot[r] with len[r] slots per slice.
+constexpr int kMaxRuns = 24;
+struct RunShape {
+  int row0, row1, nruns;
+  int slice[kMaxRuns + 1];
+  int slot[kMaxRuns];
+  int len[kMaxRuns];
 };
 
 // ---- kernels ---------------------------------------------------------------
@@ -483,89 +490,79 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, con
                   [&](double v) { fin_rho(st, v); });
 }
 
-// ---- sweeps on the uniform colour layout (multicolour SSOR) ----------------
-// Every slice of a colour has the colour's slot count (GroupShape), so a slice's rows
-// and slots follow from its index; the intermediate zpos is in colour-position order
-// (columns of the layout are positions).  A warp takes SL slices of the colour at
-// once (slices s, s + nwarps, ...) and issues their loads together: a large colour
-// then fits in one round of resident warps.
+// ---- sweeps on the run-table colour layout (multicolour SSOR) --------------
+// The rows of a colour are ordered by slot count, so its slices form a few runs of
+// equal slot count (RunShape, a kernel parameter): a slice's rows, first slot and slot
+// count follow from its index without a load.  The intermediate zpos is in
+// colour-position order (columns of the layout are positions).
 
-// Gathers of SL slices with the same slot count; has[j]: slice j exists (warp-uniform).
-template <class R, class TV, int K, bool BACKWARD, int SL>
-__device__ __forceinline__ void slices_gemv_u(const SellView<TV> &A, const int (&slot0)[SL], const bool (&has)[SL],
-                                              int nslots, int lane, const R *__restrict__ x, R (&y)[SL][3]) {
-  // the same number of slots in flight for any SL
-#pragma unroll (4 / SL)
+// Gather of one slice: this lane's blocks of slots slot0 .. slot0+nslots-1 (in
+// reverse for BACKWARD), then the sum over the row's K lanes.
+template <class R, class TV, int K, bool BACKWARD>
+__device__ __forceinline__ void slice_gemv_u(const SellView<TV> &A, int slot0, int nslots, int lane,
+                                             const R *__restrict__ x, R &y0, R &y1, R &y2) {
+#pragma unroll 4
   for (int kk = 0; kk < nslots; kk++) {
-    const int o = BACKWARD ? nslots - 1 - kk : kk;
-#pragma unroll
-    for (int j = 0; j < SL; j++) {
-      if (!has[j]) continue;
-      const int sl = slot0[j] + o;
-      const int c = __ldg(&A.col[sl * 32 + lane]);
-      const TV *v = A.val + sl * 288 + lane;
-      const R x0 = __ldg(&x[3 * c]), x1 = __ldg(&x[3 * c + 1]), x2 = __ldg(&x[3 * c + 2]);
-      const R v0 = ld_val<R>(v), v1 = ld_val<R>(v + 32), v2 = ld_val<R>(v + 64);
-      const R v3 = ld_val<R>(v + 96), v4 = ld_val<R>(v + 128), v5 = ld_val<R>(v + 160);
-      const R v6 = ld_val<R>(v + 192), v7 = ld_val<R>(v + 224), v8 = ld_val<R>(v + 256);
-      y[j][0] = fma(v2, x2, fma(v1, x1, fma(v0, x0, y[j][0])));
-      y[j][1] = fma(v5, x2, fma(v4, x1, fma(v3, x0, y[j][1])));
-      y[j][2] = fma(v8, x2, fma(v7, x1, fma(v6, x0, y[j][2])));
-    }
+    const int sl = slot0 + (BACKWARD ? nslots - 1 - kk : kk);
+    const int c = __ldg(&A.col[sl * 32 + lane]);
+    const TV *v = A.val + sl * 288 + lane;
+    const R x0 = __ldg(&x[3 * c]), x1 = __ldg(&x[3 * c + 1]), x2 = __ldg(&x[3 * c + 2]);
+    const R v0 = ld_val<R>(v), v1 = ld_val<R>(v + 32), v2 = ld_val<R>(v + 64);
+    const R v3 = ld_val<R>(v + 96), v4 = ld_val<R>(v + 128), v5 = ld_val<R>(v + 160);
+    const R v6 = ld_val<R>(v + 192), v7 = ld_val<R>(v + 224), v8 = ld_val<R>(v + 256);
+    y0 = fma(v2, x2, fma(v1, x1, fma(v0, x0, y0)));
+    y1 = fma(v5, x2, fma(v4, x1, fma(v3, x0, y1)));
+    y2 = fma(v8, x2, fma(v7, x1, fma(v6, x0, y2)));
   }
 #pragma unroll
-  for (int j = 0; j < SL; j++)
-#pragma unroll
-    for (int o = K / 2; o > 0; o >>= 1) {
-      y[j][0] += __shfl_xor_sync(0xffffffffu, y[j][0], o);
-      y[j][1] += __shfl_xor_sync(0xffffffffu, y[j][1], o);
-      y[j][2] += __shfl_xor_sync(0xffffffffu, y[j][2], o);
-    }
+  for (int o = K / 2; o > 0; o >>= 1) {
+    y0 += __shfl_xor_sync(0xffffffffu, y0, o);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, o);
+    y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+  }
+}
+
+// First slot and slot count of slice t (relative to the colour's first slice).
+__device__ __forceinline__ void run_slots(const RunShape &sh, int t, int &slot0, int &nslots) {
+  int r = 0;
+  while (r + 1 < sh.nruns && sh.slice[r + 1] <= t) r++;
+  nslots = sh.len[r];
+  slot0 = sh.slot[r] + (t - sh.slice[r]) * nslots;
 }
 
 // Forward sweep of one colour: zpos(pos) = LU^-1 ( r(perm(pos)) - sum_lower A zpos(col) )
 // (hecmw_precond_SSOR_33.F90:309-345).
-template <class R, class TV, class TA, int K, int SL>
+template <class R, class TV, class TA, int K>
 __global__ void __launch_bounds__(kThreads) sweep_fwd_uni_kernel(SellView<TV> L, const int *__restrict__ perm,
                                                                  const TA *__restrict__ alu, int npos,
                                                                  const R *__restrict__ r, R *__restrict__ zpos,
-                                                                 int sbeg, int send, GroupShape gs,
-                                                                 const CgState *st) {
+                                                                 int nslices, RunShape sh, const CgState *st) {
   pdl_entry();
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
   const int roff = lane / K;
   const bool leader = (lane & (K - 1)) == 0;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int s0 = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s0 < send; s0 += SL * nwarps) {
-    int slot0[SL], row[SL];
-    bool has[SL], act[SL];
-    R rr[SL][3], y[SL][3];
-#pragma unroll
-    for (int j = 0; j < SL; j++) {
-      const int s = s0 + j * nwarps;
-      has[j] = s < send;
-      row[j] = gs.row0 + (s - sbeg) * (32 / K) + roff;
-      act[j] = has[j] && row[j] < gs.row1 && leader;
-      slot0[j] = gs.slot0 + (s - sbeg) * gs.len;
-      rr[j][0] = rr[j][1] = rr[j][2] = R(0);
-      y[j][0] = y[j][1] = y[j][2] = R(0);
-      if (act[j]) {
-        const int node = perm[row[j]];
-        rr[j][0] = r[3 * node];
-        rr[j][1] = r[3 * node + 1];
-        rr[j][2] = r[3 * node + 2];
-      }
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nslices; t += nwarps) {
+    int slot0, nslots;
+    run_slots(sh, t, slot0, nslots);
+    const int row = sh.row0 + t * (32 / K) + roff;
+    const bool act = row < sh.row1 && leader;
+    R r0 = R(0), r1 = R(0), r2 = R(0);
+    if (act) {
+      const int node = perm[row];
+      r0 = r[3 * node];
+      r1 = r[3 * node + 1];
+      r2 = r[3 * node + 2];
     }
-    slices_gemv_u<R, TV, K, false, SL>(L, slot0, has, gs.len, lane, zpos, y);
-#pragma unroll
-    for (int j = 0; j < SL; j++) {
-      if (!act[j]) continue;
-      R x1 = rr[j][0] - y[j][0], x2 = rr[j][1] - y[j][1], x3 = rr[j][2] - y[j][2];
-      lu_solve(alu, npos, row[j], x1, x2, x3);
-      zpos[3 * row[j]] = x1;
-      zpos[3 * row[j] + 1] = x2;
-      zpos[3 * row[j] + 2] = x3;
+    R y0 = R(0), y1 = R(0), y2 = R(0);
+    slice_gemv_u<R, TV, K, false>(L, slot0, nslots, lane, zpos, y0, y1, y2);
+    if (act) {
+      R x1 = r0 - y0, x2 = r1 - y1, x3 = r2 - y2;
+      lu_solve(alu, npos, row, x1, x2, x3);
+      zpos[3 * row] = x1;
+      zpos[3 * row + 1] = x2;
+      zpos[3 * row + 2] = x3;
     }
   }
 }
@@ -573,13 +570,13 @@ __global__ void __launch_bounds__(kThreads) sweep_fwd_uni_kernel(SellView<TV> L,
 // Backward sweep of one colour: zpos(pos) -= LU^-1 ( sum_upper A zpos(col) ), the
 // finished rows also written to z in node order; FUSE_RHO accumulates {r}{z} and the
 // last launch's last CTA runs the RHO finisher (hecmw_precond_SSOR_33.F90:353-405).
-template <class R, class TV, class TA, int K, bool FUSE_RHO, int SL>
+template <class R, class TV, class TA, int K, bool FUSE_RHO>
 __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U, const int *__restrict__ perm,
                                                                  const TA *__restrict__ alu, int npos,
                                                                  const R *__restrict__ r, R *__restrict__ z,
-                                                                 R *__restrict__ zpos, int sbeg, int send,
-                                                                 GroupShape gs, CgState *st, double *partials,
-                                                                 int part_base, int part_total) {
+                                                                 R *__restrict__ zpos, int nslices, RunShape sh,
+                                                                 CgState *st, double *partials, int part_base,
+                                                                 int part_total) {
   pdl_entry();
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
@@ -587,43 +584,33 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U,
   const bool leader = (lane & (K - 1)) == 0;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double dot = 0.0;
-  for (int s0 = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s0 < send; s0 += SL * nwarps) {
-    int slot0[SL], row[SL], node[SL];
-    bool has[SL], act[SL];
-    R cz[SL][3], y[SL][3];
-#pragma unroll
-    for (int j = 0; j < SL; j++) {
-      const int s = s0 + j * nwarps;
-      has[j] = s < send;
-      row[j] = gs.row0 + (s - sbeg) * (32 / K) + roff;
-      act[j] = has[j] && row[j] < gs.row1 && leader;
-      slot0[j] = gs.slot0 + (s - sbeg) * gs.len;
-      cz[j][0] = cz[j][1] = cz[j][2] = R(0);
-      y[j][0] = y[j][1] = y[j][2] = R(0);
-      node[j] = 0;
-      if (act[j]) {  // this row's node and current value (written by the forward sweep)
-        node[j] = perm[row[j]];
-        cz[j][0] = zpos[3 * row[j]];
-        cz[j][1] = zpos[3 * row[j] + 1];
-        cz[j][2] = zpos[3 * row[j] + 2];
-      }
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nslices; t += nwarps) {
+    int slot0, nslots;
+    run_slots(sh, t, slot0, nslots);
+    const int row = sh.row0 + t * (32 / K) + roff;
+    const bool act = row < sh.row1 && leader;
+    int node = 0;
+    R c0 = R(0), c1 = R(0), c2 = R(0);
+    if (act) {  // this row's node and current value (written by the forward sweep)
+      node = perm[row];
+      c0 = zpos[3 * row];
+      c1 = zpos[3 * row + 1];
+      c2 = zpos[3 * row + 2];
     }
-    slices_gemv_u<R, TV, K, true, SL>(U, slot0, has, gs.len, lane, zpos, y);
-#pragma unroll
-    for (int j = 0; j < SL; j++) {
-      if (!act[j]) continue;
-      R x1 = y[j][0], x2 = y[j][1], x3 = y[j][2];
-      lu_solve(alu, npos, row[j], x1, x2, x3);
-      const R z0 = cz[j][0] - x1, z1 = cz[j][1] - x2, z2 = cz[j][2] - x3;
-      zpos[3 * row[j]] = z0;
-      zpos[3 * row[j] + 1] = z1;
-      zpos[3 * row[j] + 2] = z2;
-      z[3 * node[j]] = z0;
-      z[3 * node[j] + 1] = z1;
-      z[3 * node[j] + 2] = z2;
+    R x1 = R(0), x2 = R(0), x3 = R(0);
+    slice_gemv_u<R, TV, K, true>(U, slot0, nslots, lane, zpos, x1, x2, x3);
+    if (act) {
+      lu_solve(alu, npos, row, x1, x2, x3);
+      const R z0 = c0 - x1, z1 = c1 - x2, z2 = c2 - x3;
+      zpos[3 * row] = z0;
+      zpos[3 * row + 1] = z1;
+      zpos[3 * row + 2] = z2;
+      z[3 * node] = z0;
+      z[3 * node + 1] = z1;
+      z[3 * node + 2] = z2;
       if (FUSE_RHO)
-        dot += double(r[3 * node[j]]) * double(z0) + double(r[3 * node[j] + 1]) * double(z1) +
-               double(r[3 * node[j] + 2]) * double(z2);
+        dot += double(r[3 * node]) * double(z0) + double(r[3 * node + 1]) * double(z1) +
+               double(r[3 * node + 2]) * double(z2);
     }
   }
   if (FUSE_RHO)

@@ -280,34 +280,71 @@ void reordered_rows(const Profile &p, const std::vector<int> &perm, const std::v
 }
 
 void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out, int lanes,
-                bool uniform) {
+                int max_runs) {
   if (lanes < 1 || lanes > 32 || (32 % lanes) != 0) throw std::runtime_error("lanes per row must divide 32");
   out = SellLayout();
   out.lanes = lanes;
   const int per_slice = 32 / lanes;
   const int ngroups = int(group_rows.size()) - 1;
   out.group_slice.assign(size_t(ngroups) + 1, 0);
-  out.group_slot0.assign(size_t(ngroups), 0);
-  out.group_len.assign(size_t(ngroups), 0);
+  if (max_runs > 0) out.run_ptr.assign(size_t(ngroups) + 1, 0);
+  std::vector<int> lens;
   for (int g = 0; g < ngroups; g++) {
-    int glen = 0;
-    if (uniform)
-      for (int r = group_rows[g]; r < group_rows[g + 1]; r++)
-        glen = std::max(glen, int((rows.ptr[r + 1] - rows.ptr[r] + lanes - 1) / lanes));
-    out.group_slot0[g] = int(out.nslots);
-    out.group_len[g] = glen;
+    // natural slot count of each slice of the group
+    lens.clear();
     for (int r0 = group_rows[g]; r0 < group_rows[g + 1]; r0 += per_slice) {
       const int nr = std::min(per_slice, group_rows[g + 1] - r0);
-      int len = glen;
-      for (int l = 0; l < nr && !uniform; l++) {
+      int len = 0;
+      for (int l = 0; l < nr; l++) {
         const int n = int(rows.ptr[r0 + l + 1] - rows.ptr[r0 + l]);
         len = std::max(len, (n + lanes - 1) / lanes);
       }
+      lens.push_back(len);
+    }
+    if (max_runs > 0) {
+      // runs of equal slot counts; while there are too many, merge the adjacent pair
+      // whose merge adds the fewest padding slots
+      std::vector<std::pair<int, int>> runs;  // (slices, slot count)
+      for (int len : lens) {
+        if (!runs.empty() && runs.back().second == len) runs.back().first++;
+        else runs.emplace_back(1, len);
+      }
+      while (int(runs.size()) > max_runs) {
+        size_t best = 0;
+        int64_t best_cost = -1;
+        for (size_t i = 0; i + 1 < runs.size(); i++) {
+          const auto &a = runs[i], &b = runs[i + 1];
+          const int64_t cost = a.second < b.second ? int64_t(a.first) * (b.second - a.second)
+                                                   : int64_t(b.first) * (a.second - b.second);
+          if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = i;
+          }
+        }
+        runs[best].first += runs[best + 1].first;
+        runs[best].second = std::max(runs[best].second, runs[best + 1].second);
+        runs.erase(runs.begin() + int64_t(best) + 1);
+      }
+      int at = 0;
+      for (const auto &rn : runs) {
+        out.run_slice.push_back(at);
+        out.run_slot.push_back(0);  // set below, when the run's first slice is laid out
+        out.run_len.push_back(rn.second);
+        for (int k = 0; k < rn.first; k++) lens[size_t(at + k)] = rn.second;
+        at += rn.first;
+      }
+      out.run_ptr[size_t(g) + 1] = int(out.run_slice.size());
+    }
+    size_t k = 0;
+    int run = max_runs > 0 ? out.run_ptr[size_t(g)] : 0;
+    for (int r0 = group_rows[g]; r0 < group_rows[g + 1]; r0 += per_slice, k++) {
+      if (max_runs > 0 && run < out.run_ptr[size_t(g) + 1] && out.run_slice[size_t(run)] == int(k))
+        out.run_slot[size_t(run++)] = int(out.nslots);
       out.row0.push_back(r0);
-      out.nrows.push_back(nr);
+      out.nrows.push_back(std::min(per_slice, group_rows[g + 1] - r0));
       out.slot0.push_back(int(out.nslots));
-      out.len.push_back(len);
-      out.nslots += len;
+      out.len.push_back(lens[k]);
+      out.nslots += lens[k];
       if (out.nslots > (int64_t(1) << 31) / 32 / 9)
         throw std::runtime_error("matrix too large for 32-bit slot offsets");
     }
@@ -330,6 +367,36 @@ void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellL
         out.col[at] = rows.col[b + k];
         out.src[at] = rows.src[b + k];
       }
+    }
+  }
+}
+
+void order_rows_by_length(const BlockRows &lower, const BlockRows &upper, const std::vector<int> &group_rows,
+                          int lanes, std::vector<int> &order) {
+  const int n = int(lower.ptr.size()) - 1;
+  order.resize(size_t(n));
+  for (int i = 0; i < n; i++) order[size_t(i)] = i;
+  auto cls = [lanes](const BlockRows &br, int r) { return int((br.ptr[r + 1] - br.ptr[r] + lanes - 1) / lanes); };
+  for (size_t g = 0; g + 1 < group_rows.size(); g++)
+    std::stable_sort(order.begin() + group_rows[g], order.begin() + group_rows[g + 1], [&](int a, int b) {
+      const int la = cls(lower, a), lb = cls(lower, b);
+      return la != lb ? la < lb : cls(upper, a) < cls(upper, b);
+    });
+}
+
+void permute_rows(const BlockRows &in, const std::vector<int> &order, const std::vector<int> &iorder,
+                  BlockRows &out) {
+  const int n = int(order.size());
+  out.ptr.assign(size_t(n) + 1, 0);
+  for (int i = 0; i < n; i++) out.ptr[size_t(i) + 1] = out.ptr[size_t(i)] + in.ptr[order[i] + 1] - in.ptr[order[i]];
+  out.col.resize(in.col.size());
+  out.src.resize(in.src.size());
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) {
+    int64_t w = out.ptr[size_t(i)];
+    for (int64_t k = in.ptr[order[i]]; k < in.ptr[order[i] + 1]; k++, w++) {
+      out.col[size_t(w)] = iorder[size_t(in.col[size_t(k)])];
+      out.src[size_t(w)] = in.src[size_t(k)];
     }
   }
 }

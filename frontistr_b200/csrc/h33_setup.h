@@ -63,13 +63,31 @@ struct SellLayout {
   std::vector<int> rowlen;                    // per slice*32 + row offset (blocks in the row)
   std::vector<int> col, src;                  // per slot*32 + lane (pad: col 0, src -1)
   std::vector<int> group_slice;               // group g -> slices [group_slice[g], group_slice[g+1])
-  std::vector<int> group_slot0, group_len;    // uniform layouts: first slot and slots per slice of group g
+  // run tables (built when max_runs > 0): the slices of group g form runs
+  // run_ptr[g] .. run_ptr[g+1]-1 of consecutive slices with one slot count; run i
+  // starts at slice group_slice[g] + run_slice[i] and slot run_slot[i] and gives
+  // each of its slices run_len[i] slots
+  std::vector<int> run_ptr, run_slice, run_slot, run_len;
 };
 // group_rows: row boundaries of the groups (size ngroups+1, rows 0..nrows-1).
-// uniform: every slice of a group gets the group's largest slot count, so that a
-// slice's first slot and rows follow from its index (padding: column 0, no value).
+// Each slice gets the largest slot count of its rows.  max_runs > 0: per group, the
+// slices' slot counts are raised where needed (padding: column 0, value 0) so that
+// they form at most max_runs runs, and the run tables are filled: a kernel then
+// finds a slice's first slot and slot count from its index and the group's table.
 void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out,
-                int lanes = 1, bool uniform = false);
+                int lanes = 1, int max_runs = 0);
+
+// Order of the rows inside each group for the sliced layouts of a lower and an upper
+// part with the same rows: sorted by (lower slot count, upper slot count) at `lanes`
+// lanes per row, ties in the incoming order, so that the slices of a group need few
+// distinct slot counts.  order[new] = old row; rows never leave their group.
+void order_rows_by_length(const BlockRows &lower, const BlockRows &upper, const std::vector<int> &group_rows,
+                          int lanes, std::vector<int> &order);
+
+// Rows of `in` taken in the order `order` (order[new] = old row) and columns renamed
+// by iorder (iorder[old] = new); the blocks of each row keep their order.
+void permute_rows(const BlockRows &in, const std::vector<int> &order, const std::vector<int> &iorder,
+                  BlockRows &out);
 
 // Block ILU(0) in natural order (FORM_ILU0_33, hecmw_precond_BILU_33.f90:185-362),
 // computed on the host from the hecmwST arrays.  Outputs the factor blocks in the

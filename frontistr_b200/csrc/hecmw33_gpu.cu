@@ -108,16 +108,6 @@ void launch_k(cudaStream_t s, void (*kern)(KArgs...), int grid, int block, Args 
 // 4, 8 or 16).  Several lanes per row shorten each row's dependent load
 // chain and multiply the warps of a colour, which the sweeps need: a colour holds
 // a tenth of the rows, too few one-lane rows to cover HBM latency.
-// Slices a warp of the SSOR sweeps takes at once (HECMW33_SWEEP_SLICES=2 selects two).
-// One is the default: on the 100^3 cube two slices measured 0.947 / 0.806 s (FP64) and
-// 0.709 / 0.697 s (BF16-stored preconditioner) against one -- the extra registers cost
-// more occupancy than the longer load batches gain.
-int sweep_slices(bool bf16_values) {
-  (void)bf16_values;
-  const char *e = std::getenv("HECMW33_SWEEP_SLICES");
-  return (e && e[0] == '2') ? 2 : 1;
-}
-
 int sweep_lanes() {
   const char *e = std::getenv("HECMW33_SWEEP_LANES");
   const int k = e ? std::atoi(e) : 4;
@@ -136,7 +126,8 @@ struct DevSell {
   DevArray<T> val;
   DevArray<float> val32;  // FP32 copy of val (mixed precision), same layout
   DevArray<__nv_bfloat16> val16;  // BF16 copy of val (low-precision preconditioner), same layout
-  std::vector<int> group_slice, group_rows, group_slot0, group_len;
+  std::vector<int> group_slice, group_rows;
+  std::vector<int> run_ptr, run_slice, run_slot, run_len;  // run tables (multicolour SSOR layouts)
 
   int lanes = 1;
   void upload(const SellLayout &L, cudaStream_t s) {
@@ -152,8 +143,10 @@ struct DevSell {
     src.upload(L.src, s);
     val.alloc(size_t(nslots) * 288);
     group_slice = L.group_slice;
-    group_slot0 = L.group_slot0;
-    group_len = L.group_len;
+    run_ptr = L.run_ptr;
+    run_slice = L.run_slice;
+    run_slot = L.run_slot;
+    run_len = L.run_len;
   }
   SellView<T> view() const {
     return SellView<T>{nslices, row0.p, nrows.p, slot0.p, len.p, rowlen.p, col.p, val.p};
@@ -240,7 +233,7 @@ struct Solver {
   int device = 0;
   cudaStream_t stream = nullptr;
   int nsm = 148;
-  int occ_spmv = 4, occ_sweep = 4, occ_vec = 8, occ_sweep_uni = 4, occ_sweep_uni2 = 4;
+  int occ_spmv = 4, occ_sweep = 4, occ_vec = 8, occ_sweep_uni = 4;
   // matrix
   bool has_matrix = false;
   int N = 0, NPL = 0, NPU = 0;
@@ -295,10 +288,8 @@ struct Solver {
     H33_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_spmv, spmv_kernel<double, 2>, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep, sweep_bwd_kernel<double, double, double, 8, true>, kThreads, 0));
-    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep_uni, sweep_bwd_uni_kernel<double, double, double, 4, true, 1>, kThreads, 0));
-    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep_uni2, sweep_bwd_uni_kernel<double, __nv_bfloat16, float, 4, true, 2>, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sweep_uni, sweep_bwd_uni_kernel<double, double, double, 4, true>, kThreads, 0));
     occ_sweep_uni = std::max(occ_sweep_uni, 1);
-    occ_sweep_uni2 = std::max(occ_sweep_uni2, 1);
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_vec, update_xr_kernel<double>, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mr, mr_sweep_bwd_kernel<8, true, true>, kThreads, 0));
     occ_spmv = std::max(occ_spmv, 1);
@@ -339,9 +330,9 @@ struct Solver {
     const int need = (A.nslices + kWarpsPerCta - 1) / kWarpsPerCta;
     return std::max(1, std::min(need, nsm * occ_spmv));
   }
-  int grid_sweep_uni(int nslices, int sl) const {
-    const int need = (nslices + kWarpsPerCta * sl - 1) / (kWarpsPerCta * sl);
-    return std::max(1, std::min(need, nsm * (sl == 2 ? occ_sweep_uni2 : occ_sweep_uni)));
+  int grid_sweep_uni(int nslices) const {
+    const int need = (nslices + kWarpsPerCta - 1) / kWarpsPerCta;
+    return std::max(1, std::min(need, nsm * occ_sweep_uni));
   }
   int grid_sweep(int nslices) const {
     const int need = (nslices + kWarpsPerCta - 1) / kWarpsPerCta;
@@ -450,15 +441,26 @@ void setup_ssor(Solver &S, int ncolor_in, double sigma, bool symbolic) {
     std::vector<int> perm_rcm, iperm_rcm, perm, iperm, colorindex;
     ordering_rcm(prof, perm_rcm, iperm_rcm);
     P.ncolor = ordering_mc(prof, perm_rcm, ncolor_in, colorindex, perm, iperm);
-    BlockRows lower, upper;
-    reordered_rows(prof, perm, iperm, lower, upper);
+    BlockRows lower_ref, upper_ref, lower, upper;
+    reordered_rows(prof, perm, iperm, lower_ref, upper_ref);
     // the device sweeps gather from their colour-ordered intermediate: columns as
     // positions (the same blocks in the same order; only the index names change)
-    for (auto *br : {&lower, &upper})
+    for (auto *br : {&lower_ref, &upper_ref})
       for (int &c : br->col) c = iperm[c];
+    // inside each colour the device places its rows by slot count (rows of one
+    // colour never read each other, so the sweep's arithmetic per row is unchanged):
+    // the slices of a colour then need few distinct slot counts and little padding
+    const int lanes = sweep_lanes();
+    std::vector<int> order, iorder(size_t(S.N));
+    order_rows_by_length(lower_ref, upper_ref, colorindex, lanes, order);
+    for (int i = 0; i < S.N; i++) iorder[size_t(order[size_t(i)])] = i;
+    permute_rows(lower_ref, order, iorder, lower);
+    permute_rows(upper_ref, order, iorder, upper);
+    std::vector<int> perm_dev(size_t(S.N));
+    for (int i = 0; i < S.N; i++) perm_dev[size_t(i)] = perm[size_t(order[size_t(i)])];
     SellLayout lo, up;
-    build_sell(lower, colorindex, lo, sweep_lanes(), true);
-    build_sell(upper, colorindex, up, sweep_lanes(), true);
+    build_sell(lower, colorindex, lo, lanes, kMaxRuns);
+    build_sell(upper, colorindex, up, lanes, kMaxRuns);
     P.pos_cols = true;
     // padding blocks gather zpos[0]: it must hold finite values from the start
     S.zpos.alloc(size_t(3) * S.N);
@@ -467,9 +469,9 @@ void setup_ssor(Solver &S, int ncolor_in, double sigma, bool symbolic) {
     P.up.upload(up, S.stream);
     P.lo.group_rows = colorindex;
     P.up.group_rows = colorindex;
-    P.perm_fwd.upload(perm, S.stream);
+    P.perm_fwd.upload(perm_dev, S.stream);
     P.colorindex = colorindex;
-    P.perm = perm;
+    P.perm = perm;  // the reference's ordering (reported); the device uses perm_dev
     P.alu_shared = true;
   }
   P.lo.pack(S.raw.p, S.stream, S.nsm);
@@ -664,32 +666,50 @@ void launch_sweep_node(Solver &S, const SellView<TV> &lo, const SellView<TV> &up
   }
 }
 
-// Uniform colour layout (multicolour SSOR): intermediate in colour-position order,
-// SL slices per warp.
-template <class R, class TV, class TA, bool FUSE_RHO, int K, int SL>
+// Run-table colour layout (multicolour SSOR): intermediate in colour-position order.
+RunShape run_shape(const DevSell<double> &D, int g) {
+  RunShape sh{};
+  sh.row0 = D.group_rows[size_t(g)];
+  sh.row1 = D.group_rows[size_t(g) + 1];
+  const int r0 = D.run_ptr[size_t(g)], r1 = D.run_ptr[size_t(g) + 1];
+  sh.nruns = r1 - r0;
+  if (sh.nruns == 0) {  // a colour without rows
+    sh.nruns = 1;
+    return sh;
+  }
+  if (sh.nruns > kMaxRuns) throw Failure(HECMW33_ERR_CUDA, "run table out of range");
+  for (int r = 0; r < sh.nruns; r++) {
+    sh.slice[r] = D.run_slice[size_t(r0 + r)];
+    sh.slot[r] = D.run_slot[size_t(r0 + r)];
+    sh.len[r] = D.run_len[size_t(r0 + r)];
+  }
+  sh.slice[sh.nruns] = D.group_slice[size_t(g) + 1] - D.group_slice[size_t(g)];
+  return sh;
+}
+
+template <class R, class TV, class TA, bool FUSE_RHO, int K>
 void launch_sweep_uni(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f, const R *rin,
                       R *zout, R *zpos, CgState *st) {
   Precond &P = S.pc;
   cudaStream_t s = S.stream;
   const int gf = int(P.lo.group_slice.size()) - 1;
   for (int g = 0; g < gf; g++) {
-    const int sb = P.lo.group_slice[g], se = P.lo.group_slice[g + 1];
-    if (se <= sb) continue;
-    const GroupShape gsh{P.lo.group_rows[g], P.lo.group_rows[g + 1], P.lo.group_slot0[g], P.lo.group_len[g]};
-    launch_k(s, sweep_fwd_uni_kernel<R, TV, TA, K, SL>, S.grid_sweep_uni(se - sb, SL), kThreads, lo, P.perm_fwd.p,
-             alu_f, S.N, rin, zpos, sb, se, gsh, st);
+    const int ns = P.lo.group_slice[g + 1] - P.lo.group_slice[g];
+    if (ns <= 0) continue;
+    launch_k(s, sweep_fwd_uni_kernel<R, TV, TA, K>, S.grid_sweep_uni(ns), kThreads, lo, P.perm_fwd.p, alu_f, S.N,
+             rin, zpos, ns, run_shape(P.lo, g), static_cast<const CgState *>(st));
   }
   const int gb = int(P.up.group_slice.size()) - 1;
   int total = 0;
-  for (int g = gb - 1; g >= 0; g--)
-    total += S.grid_sweep_uni(std::max(P.up.group_slice[g + 1] - P.up.group_slice[g], 1), SL);
+  for (int g = gb - 1; g >= 0; g--) total += S.grid_sweep_uni(std::max(P.up.group_slice[g + 1] - P.up.group_slice[g], 1));
   int base = 0;
   for (int g = gb - 1; g >= 0; g--) {
-    const int sb = P.up.group_slice[g], se = P.up.group_slice[g + 1];
-    const int grid = S.grid_sweep_uni(std::max(se - sb, 1), SL);
-    const GroupShape gsh{P.up.group_rows[g], P.up.group_rows[g + 1], P.up.group_slot0[g], P.up.group_len[g]};
-    launch_k(s, sweep_bwd_uni_kernel<R, TV, TA, K, FUSE_RHO, SL>, grid, kThreads, up, P.perm_fwd.p, alu_f, S.N, rin,
-             zout, zpos, sb, se, gsh, st, S.partials.p, base, total);
+    const int ns = P.up.group_slice[g + 1] - P.up.group_slice[g];
+    const int grid = S.grid_sweep_uni(std::max(ns, 1));
+    // a colour without slices still launches (one idle CTA) so that the reduction
+    // ticket count stays exact
+    launch_k(s, sweep_bwd_uni_kernel<R, TV, TA, K, FUSE_RHO>, grid, kThreads, up, P.perm_fwd.p, alu_f, S.N, rin,
+             zout, zpos, ns, run_shape(P.up, g), st, S.partials.p, base, total);
     base += grid;
   }
 }
@@ -705,17 +725,10 @@ void launch_sweep_t(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, c
     return;
   }
   if (P.pos_cols) {
-    const bool two = sweep_slices(sizeof(TV) == 2) == 2;
     switch (P.lo.lanes) {
-      case 8:
-        return two ? launch_sweep_uni<R, TV, TA, FUSE_RHO, 8, 2>(S, lo, up, alu_f, rin, zout, zpos, st)
-                   : launch_sweep_uni<R, TV, TA, FUSE_RHO, 8, 1>(S, lo, up, alu_f, rin, zout, zpos, st);
-      case 16:
-        return two ? launch_sweep_uni<R, TV, TA, FUSE_RHO, 16, 2>(S, lo, up, alu_f, rin, zout, zpos, st)
-                   : launch_sweep_uni<R, TV, TA, FUSE_RHO, 16, 1>(S, lo, up, alu_f, rin, zout, zpos, st);
-      default:
-        return two ? launch_sweep_uni<R, TV, TA, FUSE_RHO, 4, 2>(S, lo, up, alu_f, rin, zout, zpos, st)
-                   : launch_sweep_uni<R, TV, TA, FUSE_RHO, 4, 1>(S, lo, up, alu_f, rin, zout, zpos, st);
+      case 8: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 8>(S, lo, up, alu_f, rin, zout, zpos, st);
+      case 16: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 16>(S, lo, up, alu_f, rin, zout, zpos, st);
+      default: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 4>(S, lo, up, alu_f, rin, zout, zpos, st);
     }
   }
   switch (P.lo.lanes) {
