@@ -618,6 +618,37 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U,
                   [&](double v) { fin_rho(st, v); });
 }
 
+// ---- symmetric diagonal scaling (SCALING=YES, hecmw_solver_scaling_33.f90) ----
+// s_(3i+a) = 1 / sqrt(|D_i(a,a)|) (:47-51).
+static __global__ void scale_vector_kernel(const double *__restrict__ D, int n, double *__restrict__ s) {
+  pdl_entry();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x) {
+    const int node = i / 3, a = i - 3 * node;
+    s[i] = 1.0 / sqrt(fabs(D[9 * size_t(node) + 4 * a]));
+  }
+}
+
+// out = in with entry (a,b) of each block (row r, column c) multiplied by s_(3r+a)
+// and then s_(3c+b), in that order (:55-110).
+static __global__ void scale_blocks_kernel(const double *__restrict__ in, double *__restrict__ out,
+                                           const int *__restrict__ brow, const int *__restrict__ bcol,
+                                           const double *__restrict__ s, int64_t nblocks) {
+  pdl_entry();
+  const int64_t total = 9 * nblocks;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t k = i / 9;
+    const int e = int(i - 9 * k), a = e / 3, b = e - 3 * a;
+    out[i] = in[i] * s[3 * size_t(brow[k]) + a] * s[3 * size_t(bcol[k]) + b];
+  }
+}
+
+// y = y * s elementwise (B scaled forward :112-116, X scaled back :144-147).
+static __global__ void mul_vec_kernel(double *__restrict__ y, const double *__restrict__ s, int n) {
+  pdl_entry();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = y[i] * s[i];
+}
+
 // Block-diagonal preconditioner z = ALU^-1 r (hecmw_precond_DIAG_33.F90:116-136),
 // optionally with the fused {r}{z} partial.
 template <class R, class TA, bool FUSE_RHO>

@@ -258,6 +258,11 @@ struct Solver {
   DevArray<float> zsf, roldf;
   DevArray<double> zpos;  // SSOR sweep intermediate in colour-position order (FP64 / FP32)
   DevArray<float> zposf;
+  // SCALING=YES: row and column of every raw block, the scaled copy of the raw
+  // values and the unscaled right-hand side while a scaled solve runs
+  DevArray<int> blk_row, blk_col;
+  DevArray<double> raw_scaled, scale, b_unscaled;
+  int blk_generation = -1;
   Learned L;
   int values_version = 0, a32_version = -1;
   double bnrm2 = 0.0;
@@ -1390,6 +1395,78 @@ void ensure_lowp(Solver &S) {
 // Checks and preconditioner setup shared by the FP64 and mixed solves
 // (hecmw_solve + hecmw_solve_iterative up to the CG call).  Returns 0 to go on,
 // or the code to return (2002 with X = 0, 2001).
+// SCALING=YES (Iarray(7), hecmw_solver_scaling_33.f90:20-208): the solve runs on
+// S A S, S b with S = diag(1/sqrt|D_kk|), and X is multiplied by S after each CG
+// (hecmw_solver_CG.f90:102,283).  The device works on a scaled copy of the resident
+// values (the borrowed host arrays are never written); restore() brings back the
+// unscaled values and right-hand side, so the driver's final true residual is that
+// of the unscaled system, as in hecmw_solver_Iterative.f90:153.
+struct ScaleScope {
+  Solver &S;
+  bool on, active = false;
+  ScaleScope(Solver &S_, bool on_) : S(S_), on(on_) {
+    if (!on) return;
+    const int N = S.N;
+    const int64_t nb = int64_t(N) + S.NPL + S.NPU;
+    if (S.blk_generation != S.generation) {
+      std::vector<int> br(static_cast<size_t>(nb)), bc(static_cast<size_t>(nb));
+      for (int i = 0; i < N; i++) {
+        br[size_t(i)] = bc[size_t(i)] = i;
+        for (int j = S.indexL[i]; j < S.indexL[i + 1]; j++) {
+          br[size_t(N) + j] = i;
+          bc[size_t(N) + j] = S.itemL[j] - 1;
+        }
+        for (int j = S.indexU[i]; j < S.indexU[i + 1]; j++) {
+          br[size_t(N) + S.NPL + j] = i;
+          bc[size_t(N) + S.NPL + j] = S.itemU[j] - 1;
+        }
+      }
+      S.blk_row.upload(br, S.stream);
+      S.blk_col.upload(bc, S.stream);
+      S.blk_generation = S.generation;
+    }
+    const int n3 = S.n3();
+    S.scale.alloc(size_t(n3));
+    S.raw_scaled.alloc(S.raw.n);
+    S.b_unscaled.alloc(size_t(n3));
+    const int gv = S.grid_vec();
+    launch_k(S.stream, scale_vector_kernel, gv, kThreads, static_cast<const double *>(S.raw.p), N, S.scale.p);
+    const int gb = std::max(1, std::min(int((9 * nb + kThreads - 1) / kThreads), S.nsm * 8));
+    launch_k(S.stream, scale_blocks_kernel, gb, kThreads, static_cast<const double *>(S.raw.p), S.raw_scaled.p,
+             static_cast<const int *>(S.blk_row.p), static_cast<const int *>(S.blk_col.p),
+             static_cast<const double *>(S.scale.p), nb);
+    H33_CUDA(cudaMemcpyAsync(S.b_unscaled.p, S.b.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, S.stream));
+    launch_k(S.stream, mul_vec_kernel, gv, kThreads, S.b.p, static_cast<const double *>(S.scale.p), n3);
+    std::swap(S.raw, S.raw_scaled);
+    S.A.pack(S.raw.p, S.stream, S.nsm);
+    S.values_version++;
+    active = true;
+  }
+  // X = S X (hecmw_solver_scaling_bk_33, :144-147)
+  void x_back() {
+    if (on) launch_k(S.stream, mul_vec_kernel, S.grid_vec(), kThreads, S.x.p, static_cast<const double *>(S.scale.p),
+                     S.n3());
+  }
+  void restore() {
+    if (!active) return;
+    active = false;
+    std::swap(S.raw, S.raw_scaled);
+    S.A.pack(S.raw.p, S.stream, S.nsm);
+    S.values_version++;
+    H33_CUDA(cudaMemcpyAsync(S.b.p, S.b_unscaled.p, sizeof(double) * S.n3(), cudaMemcpyDeviceToDevice, S.stream));
+  }
+  ~ScaleScope() {
+    if (!active) return;  // an error path: put the unscaled values back, errors ignored
+    std::swap(S.raw, S.raw_scaled);
+    const int total = S.A.nslots * 32;
+    if (total > 0)
+      pack_sell_kernel<double><<<std::min((total + kThreads - 1) / kThreads, S.nsm * 8), kThreads, 0, S.stream>>>(
+          S.A.val.p, S.A.src.p, S.A.nslots, S.raw.p);
+    S.values_version++;
+    cudaMemcpyAsync(S.b.p, S.b_unscaled.p, sizeof(double) * S.n3(), cudaMemcpyDeviceToDevice, S.stream);
+  }
+};
+
 int prepare_solve(Solver &S, int *Iarray, double *Rarray, double *sigma, bool *auto_sigma) {
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_set_matrix first");
   // zero right-hand side (hecmw_solver.f90:32-37)
@@ -1423,8 +1500,12 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   if (times) times[0] = times[1] = times[2] = 0.0;
   double sigma;
   bool auto_sigma;
+  ScaleScope scaling(S, Iarray[6] != 0);
   const int pre = prepare_solve(S, Iarray, Rarray, &sigma, &auto_sigma);
-  if (pre) return pre;
+  if (pre) {
+    scaling.restore();
+    return pre;
+  }
   const int MAXIT = Iarray[0], PRECOND = Iarray[2], iterPREmax = Iarray[4];
   const double TOL = Rarray[0];
   const int learned = Iarray[42] == 1 ? 1 : 0;
@@ -1446,6 +1527,7 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
     error = st.error;
     *iter = st.iter;
     *resid = st.resid;
+    scaling.x_back();  // the end of each hecmw_solve_CG call
     if (error == HECMW33_ERR_DIVERGE_PC || error == HECMW33_ERR_DIVERGE_MAT || error == HECMW33_ERR_DIVERGE_NAN) {
       Iarray[81] = 1;
       // Iterative.f90:133-137; the reference's retry reuses the factorisation
@@ -1456,6 +1538,10 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
       }
     }
     break;
+  }
+  if (scaling.on) {
+    scaling.restore();
+    S.bnrm2 = dot_device(S, S.b.p, S.b.p);
   }
   const double resid2 = rel_resid_device(S);
   if (resid2 < TOL) Iarray[80] = 1;
@@ -1913,6 +1999,7 @@ int solve_multi(Solver &S, int nrhs, const double *dB, double *dX, int *Iarray, 
                 double *resid, int *error, double *true_resid, double *times) {
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_set_matrix first");
   if (nrhs < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "nrhs must be positive");
+  if (Iarray[6] != 0) throw Failure(HECMW33_ERR_BAD_INPUT, "SCALING=YES is not implemented for multi-RHS solves");
   const double t0 = wall();
   if (times) times[0] = times[1] = times[2] = 0.0;
   const int METHOD = Iarray[1], PRECOND = Iarray[2], iterPREmax = Iarray[4], MAXIT = Iarray[0];
@@ -1960,6 +2047,8 @@ int solve_multi(Solver &S, int nrhs, const double *dB, double *dX, int *Iarray, 
 }
 
 int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
+  if (Iarray[6] != 0 && (Iarray[41] == 2 || Iarray[41] == 3))
+    throw Failure(HECMW33_ERR_BAD_INPUT, "SCALING=YES is implemented for the FP64 CG (Iarray(42) = 0 or 1)");
   switch (Iarray[41]) {
     case 1: return solve_fp64(S, Iarray, Rarray, iter, resid, times, 1);
     case 2: return solve_mixed_restart(S, Iarray, Rarray, iter, resid, times);

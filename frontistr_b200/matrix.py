@@ -121,6 +121,7 @@ class HecMatrix:
         self.Iarray[IDX_I_ITERPREMAX - 1] = min(max(int(v), 0), 4)
 
     def set_ncolor_in(self, v): self.Iarray[IDX_I_NCOLOR_IN - 1] = v
+    def set_scaling(self, v): self.Iarray[IDX_I_SCALING - 1] = v
     def set_resid(self, v): self.Rarray[IDX_R_RESID - 1] = v
     def set_sigma_diag(self, v): self.Rarray[IDX_R_SIGMA_DIAG - 1] = v
     def get_flag_converged(self): return int(self.Iarray[IDX_I_FLAG_CONVERGED - 1])

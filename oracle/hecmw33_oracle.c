@@ -876,6 +876,30 @@ static void recycle_precond_setting(int *Iarray) {
   }
 }
 
+/* hecmw_solver_scaling_fw_33 (hecmw_solver_scaling_33.f90:20-117) on copies:
+ * scale(3i+a) = 1/sqrt|D_i(a,a)|; every block entry (a,b) of row i, column j is
+ * multiplied by scale(3i+a) and then scale(3j+b); B(3i+a) by scale(3i+a). */
+static void scaling_fw(const o33_matrix *A, const double *B, double *scale, double *Ds, double *ALs,
+                       double *AUs, double *Bs) {
+  const int N = A->N;
+  for (int i = 0; i < N; i++)
+    for (int a = 0; a < 3; a++) scale[3 * i + a] = 1.0 / sqrt(fabs(A->D[9 * i + 4 * a]));
+  for (int i = 0; i < N; i++) {
+    for (int e = 0; e < 9; e++) Ds[9 * i + e] = A->D[9 * i + e] * scale[3 * i + e / 3] * scale[3 * i + e % 3];
+    for (int k = A->indexL[i]; k < A->indexL[i + 1]; k++) {
+      const int j = A->itemL[k] - 1;
+      for (int e = 0; e < 9; e++)
+        ALs[9 * (size_t)k + e] = A->AL[9 * (size_t)k + e] * scale[3 * i + e / 3] * scale[3 * j + e % 3];
+    }
+    for (int k = A->indexU[i]; k < A->indexU[i + 1]; k++) {
+      const int j = A->itemU[k] - 1;
+      for (int e = 0; e < 9; e++)
+        AUs[9 * (size_t)k + e] = A->AU[9 * (size_t)k + e] * scale[3 * i + e / 3] * scale[3 * j + e % 3];
+    }
+  }
+  for (int i = 0; i < 3 * N; i++) Bs[i] = B[i] * scale[i];
+}
+
 int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, double *Rarray,
               int ssor_coloured, o33_precond **cache, int *iter_out, double *resid_out,
               double *resid_true_out) {
@@ -911,6 +935,29 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
   if (METHOD != 1) return ERR_INCONS_PC;
   recycle_precond_setting(Iarray);
 
+  /* SCALING=YES (Iarray(7)): hecmw_solve_CG works on S A S, S B and multiplies X
+   * by S before it returns (hecmw_solver_CG.f90:102,283); the driver's final
+   * true residual is that of the unscaled system.  The reference scales its own
+   * arrays in place and divides them back after each CG call; the copies here
+   * leave the caller's arrays exactly as they were. */
+  const int SCALING = Iarray[6];
+  o33_matrix As = *A;
+  double *scale = NULL, *Ds = NULL, *ALs = NULL, *AUs = NULL, *Bs = NULL;
+  if (SCALING) {
+    scale = (double *)malloc(sizeof(double) * 3 * (size_t)N);
+    Ds = (double *)malloc(sizeof(double) * 9 * (size_t)N);
+    ALs = (double *)malloc(sizeof(double) * 9 * ((size_t)A->NPL + 1));
+    AUs = (double *)malloc(sizeof(double) * 9 * ((size_t)A->NPU + 1));
+    Bs = (double *)malloc(sizeof(double) * 3 * (size_t)NP);
+    for (size_t i = 0; i < 3 * (size_t)NP; i++) Bs[i] = B[i];
+    scaling_fw(A, B, scale, Ds, ALs, AUs, Bs);
+    As.D = Ds;
+    As.AL = ALs;
+    As.AU = AUs;
+  }
+  const o33_matrix *Aw = SCALING ? &As : A;
+  const double *Bw = SCALING ? Bs : B;
+
   int error = 0, iter = 0;
   double resid = 0.0;
   for (;;) {
@@ -926,9 +973,14 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
           *cache = NULL;
         }
         int perr = 0;
-        P = o33_precond_setup(A, PRECOND, NCOLOR_IN, SIGMA_DIAG, ssor_coloured, &perr);
+        P = o33_precond_setup(Aw, PRECOND, NCOLOR_IN, SIGMA_DIAG, ssor_coloured, &perr);
         if (perr) {
           o33_precond_free(P);
+          free(scale);
+          free(Ds);
+          free(ALs);
+          free(AUs);
+          free(Bs);
           return perr;
         }
         if (cache) *cache = P;
@@ -938,8 +990,10 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
         P = *cache;
       }
     }
-    error = o33_cg(A, P, iterPREmax, MAXIT, TOL, B, X, &iter, &resid, NULL);
+    error = o33_cg(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid, NULL);
     if (!cache) o33_precond_free(P);
+    if (SCALING) /* hecmw_solver_scaling_bk_33: X = S X (:144-147) */
+      for (int i = 0; i < 3 * N; i++) X[i] = X[i] * scale[i];
     if (error == ERR_DIVERGE_PC || error == ERR_DIVERGE_MAT || error == ERR_DIVERGE_NAN) {
       Iarray[81] = 1;
       if (PRECOND >= 10 && PRECOND < 20 && auto_sigma_diag == 1 && SIGMA_DIAG < 2.0) {
@@ -949,6 +1003,11 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
     }
     break;
   }
+  free(scale);
+  free(Ds);
+  free(ALs);
+  free(AUs);
+  free(Bs);
   const double resid2 = o33_rel_resid_L2(A, X, B);
   if (resid2 < TOL) Iarray[80] = 1;
   *iter_out = iter;
