@@ -24,6 +24,10 @@
  *   - Host pointers are borrowed for the duration of the call only.  Device buffers
  *     belong to the handle.  One host thread per handle; every call is synchronous.
  *   - One GPU domain: N == NP is required (no halo; hecmw_update_R is a no-op).
+ *   - Iarray(7) = 1 (SCALING=YES, hecmw_solver_scaling_33.f90:20-208): the CG runs on
+ *     S A S, S b with S = diag(1/sqrt|D_kk|) and X is multiplied by S after it; the
+ *     caller's arrays are not written.  FP64 CG only (Iarray(42) = 0 or 1): 9101 for
+ *     Iarray(42) = 2, 3 and for the multi-RHS solves.
  *   - Options of this library in the SOLVER_OPT block of Iarray/Rarray (41-50,
  *     hecmw_matrix_misc.F90:137-147), unused by the reference's CG:
  *       Iarray(42) = 0  FP64 CG (the drop-in, default)
