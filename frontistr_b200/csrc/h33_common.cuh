@@ -30,7 +30,8 @@ constexpr int kThreads = 256;
 constexpr int kWarpsPerCta = kThreads / 32;
 
 // True-residual refresh period of hecmw_solve_CG (hecmw_solver_CG.f90:67).
-constexpr int kIterRecomputeR = 50;
+constexpr int kIterRecomputeR = 50;       // hecmw_solver_CG.f90 N_ITER_RECOMPUTE_R
+constexpr int kIterRecomputeRBicg = 100;  // hecmw_solver_BiCGSTAB.f90:65
 
 struct Failure : std::runtime_error {
   int code;
@@ -112,6 +113,10 @@ struct CgState {
   // folded into FP64 each time the FP32 residual falls by ru_delta
   int reliable, ru_pending, ru_count;
   double ru_delta, ru_mark;
+  // BiCGSTAB (hecmw_solver_BiCGSTAB.f90): OMEGA and C2 = {r_tld}{v}; the true
+  // residual refresh period (50 for CG, 100 for BiCGSTAB)
+  double omega, c2;
+  int nrecompute;
   unsigned int ticket[8];
 };
 
@@ -125,6 +130,7 @@ struct CgParams {
   int use_gnn;   // 1: learned preconditioner active at the start of the solve
   int reliable;  // 1: FP32 CG with FP64 reliable updates
   double ru_delta;
+  int method;    // hecmw METHOD: 1 CG, 2 BiCGSTAB
 };
 
 }  // namespace h33

@@ -697,7 +697,7 @@ __global__ void __launch_bounds__(kThreads) update_xr_flex_kernel(R *__restrict_
   pdl_entry();
   if (st->done) return;
   const R alpha = R(st->alpha);
-  const bool refresh = !st->inner && (st->iter % kIterRecomputeR) == 0;
+  const bool refresh = !st->inner && (st->iter % st->nrecompute) == 0;
   double dot = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
     x[i] = alpha * p[i] + x[i];
@@ -748,7 +748,7 @@ __global__ void __launch_bounds__(kThreads) update_xr_kernel(R *__restrict__ x, 
   pdl_entry();
   if (st->done) return;
   const R alpha = R(st->alpha);
-  const bool refresh = !st->inner && (st->iter % kIterRecomputeR) == 0;
+  const bool refresh = !st->inner && (st->iter % st->nrecompute) == 0;
   double dot = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
     x[i] = alpha * p[i] + x[i];
@@ -770,7 +770,7 @@ __global__ void __launch_bounds__(kThreads) resid_ctl_kernel(SellView<R> A, cons
                                                              CgState *st, double *partials,
                                                              cudaGraphConditionalHandle h, int use_cond) {
   pdl_entry();
-  const bool need = !st->done && ((!st->inner && (st->iter % kIterRecomputeR) == 0) || st->recompute);
+  const bool need = !st->done && ((!st->inner && (st->iter % st->nrecompute) == 0) || st->recompute);
   if (!need) {
     if (blockIdx.x == 0 && threadIdx.x == 0) loop_ctl(st, h, use_cond);
     return;
@@ -955,6 +955,8 @@ static __global__ void cg_init_kernel(CgState *st, const CgParams *prm) {
   st->use_gnn = prm->use_gnn;
   st->restart = 0;
   st->fallback = 0;
+  st->omega = st->c2 = 0.0;
+  st->nrecompute = prm->method == 2 ? kIterRecomputeRBicg : kIterRecomputeR;
   st->resid_mark = 1.0;
   st->gamma = 1.0f;
   st->reliable = prm->reliable;

@@ -22,11 +22,13 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <type_traits>
 #include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
 
+#include "h33_bicg.cuh"
 #include "h33_common.cuh"
 #include "h33_gnn.cuh"
 #include "h33_kernels.cuh"
@@ -260,6 +262,8 @@ struct Solver {
   DevArray<float> zposf;
   // SCALING=YES: row and column of every raw block, the scaled copy of the raw
   // values and the unscaled right-hand side while a scaled solve runs
+  // BiCGSTAB vectors: r_tld, s, s_tld, t ({p_tld} and {v} use z and q)
+  DevArray<double> b_rt, b_s, b_st, b_t;
   DevArray<int> blk_row, blk_col;
   DevArray<double> raw_scaled, scale, b_unscaled;
   int blk_generation = -1;
@@ -302,6 +306,7 @@ struct Solver {
     occ_vec = std::max(occ_vec, 1);
     occ_mr = std::max(occ_mr, 1);
     H33_CUDA(cudaMallocHost(&h_params, sizeof(CgParams)));
+    std::memset(h_params, 0, sizeof(CgParams));
     H33_CUDA(cudaMallocHost(&h_state, sizeof(CgState)));
     H33_CUDA(cudaMallocHost(&h_mst, sizeof(CgState) * kMaxRhs));
     H33_CUDA(cudaMallocHost(&h_mctl, sizeof(MultiCtl)));
@@ -805,6 +810,81 @@ void launch_iteration(Solver &S, const Views<R> &V, int iterpremax, cudaGraphCon
 
 // Network application z = zs + gamma W_out h3 (or z = zs when it is off), R-precision
 // vectors, BF16 weights, FP32 activations.
+// hecmw_precond_apply without the RHO reduction (BiCGSTAB computes its own dots);
+// st (optional) only lets the kernels skip work once the loop has ended.
+template <class R>
+void launch_precond_plain(Solver &S, const Views<R> &V, int iterpremax, const R *r, R *z, CgState *st) {
+  cudaStream_t s = S.stream;
+  const int n3 = S.n3();
+  if (iterpremax <= 0) {
+    launch_k(s, copy_kernel<R>, S.grid_vec(), kThreads, r, z, n3, st);
+    return;
+  }
+  const R *in = r;
+  for (int it = 1; it <= iterpremax; it++) {
+    launch_sweep<R, false>(S, V, in, it == 1 && iterpremax == 1 ? z : V.zp, st);
+    if (iterpremax == 1) break;
+    if (it == 1) launch_k(s, copy_kernel<R>, S.grid_vec(), kThreads, V.zp, z, n3, st);
+    else launch_k(s, add_kernel<R>, S.grid_vec(), kThreads, V.zp, z, n3, st);
+    if (it == iterpremax) break;
+    launch_k(s, spmv_kernel<R, 1>, S.grid_spmv(), kThreads, V.A, z, V.w, r, nullptr, nullptr);
+    in = V.w;
+  }
+}
+
+// BiCGSTAB prologue (hecmw_solver_BiCGSTAB.f90:125-137): r = b - A x, r_tld = r,
+// BNRM2 = b.b (which also decides whether the loop runs).
+void launch_prologue_bicg(Solver &S, const Views<double> &V, cudaGraphConditionalHandle h, int use_cond) {
+  cudaStream_t s = S.stream;
+  CgState *st = S.state.p;
+  launch_k(s, cg_init_kernel, 1, 32, st, static_cast<const CgParams *>(S.params.p));
+  launch_k(s, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, V.A, V.x, V.r, V.b, nullptr, nullptr);
+  launch_k(s, copy_kernel<double>, S.grid_vec(), kThreads, V.r, S.b_rt.p, S.n3(), static_cast<const CgState *>(nullptr));
+  launch_k(s, dot_kernel<double, 0>, S.grid_vec(), kThreads, V.b, V.b, S.n3(), st, S.partials.p, h, use_cond);
+}
+
+// One BiCGSTAB iteration (:161-271): {p_tld} in z, {v} in q.
+void launch_iteration_bicg(Solver &S, const Views<double> &V, int iterpremax, cudaGraphConditionalHandle h,
+                           int use_cond) {
+  cudaStream_t s = S.stream;
+  CgState *st = S.state.p;
+  const int n3 = S.n3();
+  launch_k(s, iter_begin_kernel, 1, 32, st, h, use_cond);
+  launch_k(s, bicg_rho_kernel<double>, S.grid_vec(), kThreads, V.r, S.b_rt.p, n3, st, S.partials.p);
+  launch_k(s, bicg_p_kernel<double>, S.grid_vec(), kThreads, V.r, V.p, V.q, n3, static_cast<const CgState *>(st));
+  launch_precond_plain<double>(S, V, iterpremax, V.p, V.z, st);
+  launch_k(s, bicg_spmv_kernel<double, 0>, S.grid_spmv(), kThreads, V.A, V.z, V.q, S.b_rt.p, st, S.partials.p);
+  launch_k(s, bicg_s_kernel<double>, S.grid_vec(), kThreads, S.b_s.p, V.r, V.q, n3, static_cast<const CgState *>(st));
+  launch_precond_plain<double>(S, V, iterpremax, S.b_s.p, S.b_st.p, st);
+  launch_k(s, bicg_spmv_kernel<double, 1>, S.grid_spmv(), kThreads, V.A, S.b_st.p, S.b_t.p, S.b_s.p, st,
+           S.partials.p);
+  launch_k(s, bicg_update_kernel<double>, S.grid_vec(), kThreads, V.x, V.z, S.b_st.p, V.r, S.b_s.p, S.b_t.p, n3, st,
+           S.partials.p);
+  launch_k(s, resid_ctl_kernel<double>, S.grid_spmv(), kThreads, V.A, V.x, V.r, V.b, st, S.partials.p, h, use_cond);
+}
+
+// BiCGSTAB runs in FP64 only (the FP32 inner solves of modes 2 and 3 are CG).
+template <class R>
+void launch_prologue_bicg_t(Solver &S, const Views<R> &V, cudaGraphConditionalHandle h, int use_cond) {
+  if constexpr (std::is_same<R, double>::value) launch_prologue_bicg(S, V, h, use_cond);
+  else throw Failure(HECMW33_ERR_BAD_INPUT, "BiCGSTAB runs in FP64 only");
+}
+template <class R>
+void launch_iteration_bicg_t(Solver &S, const Views<R> &V, int iterpremax, cudaGraphConditionalHandle h,
+                             int use_cond) {
+  if constexpr (std::is_same<R, double>::value) launch_iteration_bicg(S, V, iterpremax, h, use_cond);
+  else throw Failure(HECMW33_ERR_BAD_INPUT, "BiCGSTAB runs in FP64 only");
+}
+
+void ensure_bicg(Solver &S) {
+  const size_t n3 = size_t(S.n3());
+  for (auto *v : {&S.b_rt, &S.b_s, &S.b_st, &S.b_t})
+    if (v->n != n3) {
+      v->alloc(n3);
+      v->zero(S.stream);
+    }
+}
+
 template <class R>
 void launch_gnn(Solver &S, const R *zs, const R *r, R *z, CgState *st, bool bf16_weights) {
   Learned &L = S.L;
@@ -909,6 +989,7 @@ void build_graph(Solver &S, int iterpremax, int mode = 0) {
   // prologue
   H33_CUDA(cudaStreamBeginCaptureToGraph(S.stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   if (mode & 2) launch_prologue_reliable(S, h, 1);
+  else if (mode & 8) launch_prologue_bicg_t(S, V, h, 1);
   else launch_prologue<R>(S, V, h, 1);
   cudaStreamCaptureStatus cs;
   const cudaGraphNode_t *deps = nullptr;
@@ -928,6 +1009,7 @@ void build_graph(Solver &S, int iterpremax, int mode = 0) {
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   H33_CUDA(cudaStreamBeginCaptureToGraph(S.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   if (mode & 2) launch_iteration_reliable(S, iterpremax, flexible != 0, h, 1);
+  else if (mode & 8) launch_iteration_bicg_t(S, V, iterpremax, h, 1);
   else if (flexible) launch_iteration_flex<R>(S, V, h, 1);
   else launch_iteration<R>(S, V, iterpremax, h, 1);
   cudaGraph_t b2 = nullptr;
@@ -945,9 +1027,9 @@ void build_graph(Solver &S, int iterpremax, int mode = 0) {
 // state in S.h_state and the device time in ms; counts launched kernels.
 template <class R>
 float run_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels, int inner = 0, int learned = 0,
-             int reliable = 0, double ru_delta = 1e-4, int lowp = 0) {
+             int reliable = 0, double ru_delta = 1e-4, int lowp = 0, int method = 1) {
   const Views<R> V = views(S, R(), lowp);
-  const int mode = (learned ? 1 : 0) | (reliable ? 2 : 0) | (lowp ? 4 : 0);
+  const int mode = (learned ? 1 : 0) | (reliable ? 2 : 0) | (lowp ? 4 : 0) | (method == 2 ? 8 : 0);
   S.h_params->tol = tol;
   S.h_params->maxit = maxit;
   S.h_params->iterpremax = iterpremax;
@@ -956,6 +1038,7 @@ float run_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels, int
   S.h_params->use_gnn = learned;
   S.h_params->reliable = reliable;
   S.h_params->ru_delta = ru_delta;
+  S.h_params->method = method;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, S.stream));
   H33_CUDA(cudaEventRecord(S.ev0, S.stream));
   if (graph_mode()) {
@@ -969,11 +1052,13 @@ float run_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels, int
     if (kernels) *kernels += G.prologue_kernels + executed * G.kernels_per_iter;
   } else {
     if (reliable) launch_prologue_reliable(S, 0, 0);
+    else if (mode & 8) launch_prologue_bicg_t(S, V, 0, 0);
     else launch_prologue<R>(S, V, 0, 0);
     int launched = 0;
     for (int done = 0, it = 0; !done && it <= maxit + kStreamChunk; it += kStreamChunk) {
       for (int k = 0; k < kStreamChunk; k++) {
         if (reliable) launch_iteration_reliable(S, iterpremax, learned != 0, 0, 0);
+        else if (mode & 8) launch_iteration_bicg_t(S, V, iterpremax, 0, 0);
         else if (learned) launch_iteration_flex<R>(S, V, 0, 0);
         else launch_iteration<R>(S, V, iterpremax, 0, 0);
       }
@@ -1271,6 +1356,7 @@ float record_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels) 
   S.h_params->use_gnn = 0;
   S.h_params->reliable = 0;
   S.h_params->ru_delta = 1.0;
+  S.h_params->method = 1;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, S.stream));
   H33_CUDA(cudaEventRecord(S.ev0, S.stream));
   launch_prologue<double>(S, V, 0, 0);
@@ -1483,8 +1569,10 @@ int prepare_solve(Solver &S, int *Iarray, double *Rarray, double *sigma, bool *a
   *auto_sigma = *sigma < 0.0;
   if (*auto_sigma) *sigma = 1.0;
   if (S.zero_diag && PRECOND < 10 && iterPREmax > 0) return HECMW33_ERR_ZERO_DIAG;
-  if (METHOD != 1)
-    throw Failure(HECMW33_ERR_INCONS_PC, "METHOD " + std::to_string(METHOD) + ": the GPU drop-in implements CG (1)");
+  if (METHOD != 1 && METHOD != 2)
+    throw Failure(HECMW33_ERR_INCONS_PC,
+                  "METHOD " + std::to_string(METHOD) + ": the GPU drop-in implements CG (1) and BiCGSTAB (2)");
+  if (METHOD == 2 || Iarray[7] == 2) ensure_bicg(S);
   recycle_precond_setting(Iarray);
   Range rg("hecmw33_precond_setup");
   if (iterPREmax > 0) precond_setup(S, PRECOND, Iarray[33], *sigma, Iarray);
@@ -1506,14 +1594,16 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
     scaling.restore();
     return pre;
   }
-  const int MAXIT = Iarray[0], PRECOND = Iarray[2], iterPREmax = Iarray[4];
+  const int MAXIT = Iarray[0], PRECOND = Iarray[2], iterPREmax = Iarray[4], METHOD2 = Iarray[7];
   const double TOL = Rarray[0];
-  const int learned = Iarray[42] == 1 ? 1 : 0;
+  int method = Iarray[1];
+  int learned = (Iarray[42] == 1 && method == 1) ? 1 : 0;  // the learned network runs in flexible CG
   if (learned) learned_prepare_inference(S);
   if (lowp && iterPREmax > 0) ensure_lowp(S);
   else lowp = 0;
-  const bool record = S.L.recording && !learned;
-  if (graph_mode() && !record) build_graph<double>(S, iterPREmax, learned | (lowp ? 4 : 0));
+  const bool record = S.L.recording && !learned && method == 1;
+  if (graph_mode() && !record)
+    build_graph<double>(S, iterPREmax, learned | (lowp ? 4 : 0) | (method == 2 ? 8 : 0));
   Range rs("hecmw33_solve");
   const double t1 = wall();
   int error = 0, kernels = 1;
@@ -1522,7 +1612,7 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
     Iarray[80] = 0;
     Iarray[81] = 0;
     if (record) ms_total += record_cg(S, iterPREmax, TOL, MAXIT, &kernels);
-    else ms_total += run_cg<double>(S, iterPREmax, TOL, MAXIT, &kernels, 0, learned, 0, 1e-4, lowp);
+    else ms_total += run_cg<double>(S, iterPREmax, TOL, MAXIT, &kernels, 0, learned, 0, 1e-4, lowp, method);
     const CgState &st = *S.h_state;
     error = st.error;
     *iter = st.iter;
@@ -1534,6 +1624,15 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
       // already built (flags 97/98 are cleared), continuing from the current X
       if (PRECOND >= 10 && PRECOND < 20 && auto_sigma && sigma < 2.0) {
         sigma = sigma + 0.1;
+        continue;
+      } else if (method == 1 && METHOD2 > 1) {
+        // Iterative.f90:138-142: a diverged CG hands over to METHOD2 from the current X
+        if (METHOD2 != 2)
+          throw Failure(HECMW33_ERR_INCONS_PC, "METHOD2 " + std::to_string(METHOD2) +
+                                                   ": the GPU drop-in implements BiCGSTAB (2) as the fallback");
+        if (auto_sigma) sigma = 1.0;
+        method = METHOD2;
+        learned = 0;
         continue;
       }
     }
@@ -1948,6 +2047,7 @@ float run_multi_chunk(Solver &S, int nrhs, const double *dB, double *dX, int ite
   S.h_params->use_gnn = 0;
   S.h_params->reliable = 0;
   S.h_params->ru_delta = 0.0;
+  S.h_params->method = 1;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, s));
   H33_CUDA(cudaEventRecord(S.ev0, s));
   if (graph_mode()) {
@@ -2049,6 +2149,8 @@ int solve_multi(Solver &S, int nrhs, const double *dB, double *dX, int *Iarray, 
 int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
   if (Iarray[6] != 0 && (Iarray[41] == 2 || Iarray[41] == 3))
     throw Failure(HECMW33_ERR_BAD_INPUT, "SCALING=YES is implemented for the FP64 CG (Iarray(42) = 0 or 1)");
+  if (Iarray[1] == 2 && (Iarray[41] == 2 || Iarray[41] == 3))
+    throw Failure(HECMW33_ERR_BAD_INPUT, "BiCGSTAB runs in FP64 (Iarray(42) = 0 or 1)");
   switch (Iarray[41]) {
     case 1: return solve_fp64(S, Iarray, Rarray, iter, resid, times, 1);
     case 2: return solve_mixed_restart(S, Iarray, Rarray, iter, resid, times);

@@ -7,6 +7,8 @@
  *   hecmw1/src/solver/main/hecmw_solver.f90:9-88                 (hecmw_solve)
  *   hecmw1/src/solver/iterative/hecmw_solver_Iterative.f90:13-187,255-323
  *   hecmw1/src/solver/iterative/hecmw_solver_CG.f90:19-320        (hecmw_solve_CG)
+ *   hecmw1/src/solver/iterative/hecmw_solver_BiCGSTAB.f90:125-271 (hecmw_solve_BiCGSTAB)
+ *   hecmw1/src/solver/las/hecmw_solver_scaling_33.f90:20-208      (SCALING=YES)
  *   hecmw1/src/solver/las/hecmw_solver_las_33.F90:120-435         (matvec/matresid/rel_resid)
  *   hecmw1/src/solver/communication/hecmw_solver_misc.F90:46-201  (dot/axpy/xpay)
  *   hecmw1/src/solver/precond/hecmw_precond.f90:30-172            (setup/apply dispatch)
@@ -821,6 +823,77 @@ int o33_cg(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit,
   return error;
 }
 
+/* hecmw_solve_BiCGSTAB (hecmw_solver_BiCGSTAB.f90:125-271): no breakdown tests,
+ * true residual recomputed every 100th iteration and on convergence. */
+int o33_bicgstab(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
+                 const double *B, double *X, int *iter_out, double *resid_out) {
+  const int NP = A->NP, NN = 3 * A->N;
+  const size_t len = 3 * (size_t)NP;
+  enum { NREC = 100 };
+  double *R = (double *)calloc(len, sizeof(double)), *RT = (double *)calloc(len, sizeof(double));
+  double *Pv = (double *)calloc(len, sizeof(double)), *PT = (double *)calloc(len, sizeof(double));
+  double *S = (double *)calloc(len, sizeof(double)), *ST = (double *)calloc(len, sizeof(double));
+  double *T = (double *)calloc(len, sizeof(double)), *V = (double *)calloc(len, sizeof(double));
+  double *WK = (double *)calloc(len, sizeof(double));
+  int error = 0, iter;
+  double RHO1 = 0.0, ALPHA = 0.0, BETA = 0.0, OMEGA = 0.0, RESID = 0.0;
+  o33_matresid(A, X, B, R);                        /* :125 */
+  memcpy(RT, R, sizeof(double) * (size_t)NN);     /* :128 */
+  const double BNRM2 = o33_dot(NN, B, B);          /* :131 */
+  if (BNRM2 == 0.0) {
+    maxit = 0;
+    RESID = 0.0;
+    for (size_t i = 0; i < len; i++) X[i] = 0.0;
+  }
+  for (iter = 1; iter <= maxit; iter++) {
+    const double RHO = o33_dot(NN, R, RT);         /* :168 */
+    if (iter > 1) {                                /* :176-181 */
+      BETA = (RHO / RHO1) * (ALPHA / OMEGA);
+      axpy(NN, -OMEGA, V, Pv);
+      xpay(NN, BETA, R, Pv);
+    } else {
+      memcpy(Pv, R, sizeof(double) * (size_t)NN);
+    }
+    o33_precond_apply(P, A, iterpremax, Pv, PT, WK); /* :189 */
+    o33_matvec(A, PT, V);                            /* :196 */
+    const double C2 = o33_dot(NN, RT, V);            /* :200 */
+    ALPHA = RHO / C2;
+    for (int i = 0; i < NN; i++) S[i] = -ALPHA * V[i] + R[i]; /* hecmw_axpyz_R :206 */
+    o33_precond_apply(P, A, iterpremax, S, ST, WK);  /* :213 */
+    o33_matvec(A, ST, T);                            /* :220 */
+    const double C_TS = o33_dot(NN, T, S), C_TT = o33_dot(NN, T, T);
+    OMEGA = C_TS / C_TT;                             /* :234 */
+    axpy(NN, ALPHA, PT, X);                          /* :241-242 */
+    axpy(NN, OMEGA, ST, X);
+    if (iter % NREC == 0) o33_matresid(A, X, B, R);
+    else
+      for (int i = 0; i < NN; i++) R[i] = -OMEGA * T[i] + S[i];
+    double DNRM2 = o33_dot(NN, R, R);
+    RESID = sqrt(DNRM2 / BNRM2);
+    if (RESID <= tol) {
+      if (iter % NREC == 0) break;
+      o33_matresid(A, X, B, R);
+      DNRM2 = o33_dot(NN, R, R);
+      RESID = sqrt(DNRM2 / BNRM2);
+      if (RESID <= tol) break;
+    }
+    if (iter == maxit) error = ERR_NOCONV_MAXIT;
+    RHO1 = RHO;
+  }
+  *iter_out = iter;
+  *resid_out = RESID;
+  free(R);
+  free(RT);
+  free(Pv);
+  free(PT);
+  free(S);
+  free(ST);
+  free(T);
+  free(V);
+  free(WK);
+  return error;
+}
+
 double o33_cg_fixed_iters(const o33_matrix *A, const o33_precond *P, int iterpremax, int n,
                           const double *B, double *X) {
   const int NP = A->NP, NN = 3 * A->N;
@@ -917,7 +990,8 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
     Iarray[81] = 0;
     return ERR_ZERO_RHS;
   }
-  const int METHOD = Iarray[1], PRECOND = Iarray[2], iterPREmax = Iarray[4];
+  int METHOD = Iarray[1];
+  const int PRECOND = Iarray[2], iterPREmax = Iarray[4], METHOD2 = Iarray[7];
   const int MAXIT = Iarray[0], NCOLOR_IN = Iarray[33];
   const double TOL = Rarray[0];
   double SIGMA_DIAG = Rarray[1];
@@ -932,7 +1006,7 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
     for (int j = 0; j < 3; j++)
       if (fabs(A->D[9 * i + 4 * j]) == 0.0) zdiag = ERR_ZERO_DIAG;
   if (zdiag && PRECOND < 10 && iterPREmax > 0) return ERR_ZERO_DIAG;
-  if (METHOD != 1) return ERR_INCONS_PC;
+  if (METHOD != 1 && METHOD != 2) return ERR_INCONS_PC;
   recycle_precond_setting(Iarray);
 
   /* SCALING=YES (Iarray(7)): hecmw_solve_CG works on S A S, S B and multiplies X
@@ -990,7 +1064,8 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
         P = *cache;
       }
     }
-    error = o33_cg(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid, NULL);
+    if (METHOD == 2) error = o33_bicgstab(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid);
+    else error = o33_cg(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid, NULL);
     if (!cache) o33_precond_free(P);
     if (SCALING) /* hecmw_solver_scaling_bk_33: X = S X (:144-147) */
       for (int i = 0; i < 3 * N; i++) X[i] = X[i] * scale[i];
@@ -998,6 +1073,14 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
       Iarray[81] = 1;
       if (PRECOND >= 10 && PRECOND < 20 && auto_sigma_diag == 1 && SIGMA_DIAG < 2.0) {
         SIGMA_DIAG = SIGMA_DIAG + 0.1;
+        continue;
+      } else if (METHOD == 1 && METHOD2 > 1) { /* hecmw_solver_Iterative.f90:138-142 */
+        if (auto_sigma_diag == 1) SIGMA_DIAG = 1.0;
+        if (METHOD2 != 2) {
+          error = ERR_INCONS_PC; /* only BiCGSTAB is restated here */
+          break;
+        }
+        METHOD = METHOD2;
         continue;
       }
     }
