@@ -19,6 +19,7 @@
 module hecmw_solver_gpu33
   use iso_c_binding
   use hecmw_util
+  use hecmw_matrix_dump
   use m_hecmw_solve_error
   implicit none
   private
@@ -70,10 +71,15 @@ contains
       call hecmw33_gpu_create(gpu_handle, ierr)
       if (ierr /= 0) call hecmw_abort(hecmw_comm_get_comm())
     endif
+    ! hecmw_solve_iterative dumps the matrix and right-hand side before the solve
+    ! (hecmw_solver_Iterative.f90:90, DUMPTYPE of !SOLVER) and the solution after it
+    ! (:160); both return at once when no dump is requested
+    call hecmw_mat_dump(hecMAT, hecMESH)
     call hecmw33_gpu_solve(gpu_handle, hecMAT%N, hecMAT%NP, hecMAT%indexL(hecMAT%N), &
       hecMAT%indexU(hecMAT%N), hecMAT%indexL, hecMAT%itemL, hecMAT%indexU, hecMAT%itemU, &
       hecMAT%D, hecMAT%AL, hecMAT%AU, hecMAT%B, hecMAT%X, hecMAT%Iarray, hecMAT%Rarray, &
       iter, resid, times, ierr)
+    call hecmw_mat_dump_solution(hecMAT)
     if (hecmw_mat_get_timelog(hecMAT) >= 1 .and. hecMESH%my_rank == 0) then
       write (*,'(/a)')          '### summary of linear solver (GPU)'
       write (*,'(i10,a, 1pe16.6)')      iter, ' iterations  ', resid

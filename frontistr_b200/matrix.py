@@ -26,6 +26,7 @@ IDX_I_ESTCOND = 14
 IDX_I_ITERLOG = 21
 IDX_I_TIMELOG = 22
 IDX_I_DUMP = 31
+IDX_I_DUMP_EXIT = 32
 IDX_I_USEJAD = 33
 IDX_I_NCOLOR_IN = 34
 IDX_I_MAXRECYCLE_PRECOND = 35

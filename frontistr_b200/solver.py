@@ -265,14 +265,35 @@ class GpuSolver:
 _default = None
 
 
-def hecmw_solve(hecMAT, solver=None):
-    """hecmw_solve(hecMESH, hecMAT) for one GPU domain: updates hecMAT.X and flags."""
-    global _default
+_dumper = None
+
+
+def hecmw_solve(hecMAT, solver=None, dumper=None):
+    """hecmw_solve(hecMESH, hecMAT) for one GPU domain: updates hecMAT.X and flags.
+
+    With Iarray(31) = DUMPTYPE (1 MM, 2 CSR, 3 BSR) the matrix and right-hand side
+    are dumped before the solve and the solution after it, as hecmw_solve_iterative
+    does (hecmw_solver_Iterative.f90:90,160); a zero right-hand side returns before
+    that (hecmw_solver.f90:32-37).  `dumper` (frontistr_b200.dump.Dumper) sets the
+    directory and rank of the files; by default one process-wide Dumper in ".".
+    """
+    global _default, _dumper
     if solver is None:
         if _default is None:
             _default = GpuSolver()
         solver = _default
-    return solver.solve(hecMAT)
+    if dumper is None:
+        from .dump import Dumper
+        if _dumper is None:
+            _dumper = Dumper()
+        dumper = _dumper
+    b = hecMAT.B[:3 * hecMAT.NP]
+    if float(np.dot(b, b)) == 0.0:
+        return solver.solve(hecMAT)
+    dumper.dump(hecMAT)
+    info = solver.solve(hecMAT)
+    dumper.dump_solution(hecMAT)
+    return info
 
 
 def colour_schedule(m, ncolor_in=10):
