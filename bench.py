@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--train-steps", type=int, default=60)
     ap.add_argument("--no-multi", action="store_true", help="skip the 16-load-case multi-RHS measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-system batched measurement")
+    ap.add_argument("--no-assembly", action="store_true", help="skip the HEX8 assembly measurement")
     ap.add_argument("--no-config3", action="store_true",
                     help="skip the mixed-precision measurement on the jittered heterogeneous 80^3 system")
     ap.add_argument("--batch-systems", type=int, default=256)
@@ -314,6 +315,57 @@ def bench_config3(tol=1e-10):
                                   "true_resid": info["true_resid"],
                                   "rel_err_vs_fp64": float(np.linalg.norm(g.X - ref) / np.linalg.norm(ref))}
     return out
+
+
+def bench_assembly(n=64, seed=3):
+    """HEX8 linear-elastic assembly of an n^3 box (interior nodes jittered by +-0.2h,
+    log-normal E, nu in [0.25, 0.40], clamped base, loaded top) on the device
+    (hecmw33_gpu_assemble_hex8: profile and per-block lists on the host once, element
+    blocks and element-order sums on the device, constraints) against the host
+    restatement it is bitwise equal to (fistr_mesh_assemble + fistr_mat_ass_bc, one
+    thread).  Times: the first call (symbolic + numeric), a re-assembly of new values
+    on the same mesh (a Newton iteration), and the host call."""
+    import numpy as np
+    from frontistr_b200.mesh import mesh_system
+    from frontistr_b200.solver import GpuSolver
+    rng = np.random.default_rng(seed)
+    n1 = n + 1
+    g = np.arange(n1, dtype=np.float64)
+    X = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).transpose(2, 1, 0, 3).reshape(-1, 3).copy()
+    inner = np.all((X > 0) & (X < n), axis=1)
+    X[inner] += rng.uniform(-0.2, 0.2, size=(int(inner.sum()), 3))
+    e = np.arange(n)
+    ex, ey, ez = (a.reshape(-1) for a in np.meshgrid(e, e, e, indexing="ij"))
+    order = np.lexsort((ex, ey, ez))
+    ex, ey, ez = ex[order], ey[order], ez[order]
+    nid = lambda x, y, z: x + n1 * (y + n1 * z)
+    el = np.stack([nid(ex, ey, ez), nid(ex + 1, ey, ez), nid(ex + 1, ey + 1, ez), nid(ex, ey + 1, ez),
+                   nid(ex, ey, ez + 1), nid(ex + 1, ey, ez + 1), nid(ex + 1, ey + 1, ez + 1),
+                   nid(ex, ey + 1, ez + 1)], 1).astype(np.int32)
+    E = 2.1e5 * np.exp(rng.standard_normal(len(el)))
+    nu = rng.uniform(0.25, 0.40, len(el))
+    F = np.zeros(3 * len(X))
+    top = np.nonzero(X[:, 2] == n)[0]
+    F[3 * top + 1] = -1.0
+    base = np.nonzero(X[:, 2] == 0)[0]
+    fixed = [(int(b), d, 0.0) for b in base for d in (1, 2, 3)]
+    with GpuSolver() as s:
+        t0 = time.perf_counter()
+        s.assemble_hex8(X, el, E, nu, F=F, fixed=fixed)
+        t1 = time.perf_counter()
+        s.assemble_hex8(X, el, 1.1 * E, nu, F=F, fixed=fixed, symbolic=False)
+        t2 = time.perf_counter()
+        g2 = s.get_matrix()
+    t3 = time.perf_counter()
+    cload = [(int(i) // 3, int(i) % 3 + 1, float(F[i])) for i in np.nonzero(F)[0]]
+    ref = mesh_system(X, el, 361, 1.1 * E, nu, fixed=fixed, cload=cload)
+    t4 = time.perf_counter()
+    same = bool(np.array_equal(g2.D, ref.D) and np.array_equal(g2.AL[:9 * ref.NPL], ref.AL[:9 * ref.NPL])
+                and np.array_equal(g2.AU[:9 * ref.NPU], ref.AU[:9 * ref.NPU]) and np.array_equal(g2.B, ref.B))
+    return {"workload": "%d^3 HEX8 box, jitter 0.2h, log-normal E, nu U[0.25, 0.40], clamped base" % n,
+            "elements": int(len(el)), "nodes": int(len(X)), "gpu_first_call_s": t1 - t0,
+            "gpu_reassembly_s": t2 - t1, "host_s": t4 - t3, "host_kind": "fistr_mesh_assemble, 1 thread",
+            "bitwise_equal_to_host": same, "speedup_reassembly_vs_host": (t4 - t3) / (t2 - t1)}
 
 
 def bench_learned_newton(args):
@@ -629,12 +681,24 @@ def main():
     peak, peak_kind = measured_peaks()
     achieved = info["spmv_bytes"] / (spmv_ms * 1e-3) / 1e9
 
-    # end-to-end through the drop-in call with host buffers
+    # end-to-end through the drop-in call with host buffers: the caller's matrix
+    # values, B and X sit in pinned host memory (page-locked, as a GPU-aware caller
+    # allocates them); the call copies them in, rebuilds the numeric preconditioner,
+    # solves and copies X back
     e2e = None
     if not args.no_e2e:
+        def pinned(a):
+            t_ = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+            out = t_.numpy()
+            out[:] = a
+            return out
+        pin = {k: pinned(getattr(m, k)) for k in ("D", "AL", "AU", "B", "X")}
         e2e_t = []
         for i in range(max(1, min(args.steps, 3)) + 1):
             mm = m.copy()
+            for k, v in pin.items():
+                v[:] = getattr(m, k)
+                setattr(mm, k, v)
             mm.Iarray[97] = 0  # structure unchanged (flag 98)
             mm.Iarray[96] = 2  # numerical preconditioner rebuild forced (flag 97), as a new Newton increment
             mm.Iarray[41] = 1 if head.endswith("mixed") else 0
@@ -648,7 +712,7 @@ def main():
         h2d = 8 * 9 * m.NZ + 2 * 8 * 3 * m.N
         d2h = 8 * 3 * m.N
         e2e = {"value": statistics.mean(e2e_t), "unit": "s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "solver": head}
+               "d2h_bytes_per_step": d2h, "solver": head, "host_buffers": "pinned"}
 
     dev_s, wall, e2e_v = max_over_ranks([dev_s, wall, e2e["value"] if e2e else 0.0], dist, dev)
     if e2e:
@@ -657,9 +721,10 @@ def main():
     if world > 1:
         # the 16-load-case, batched and config-3 figures are single-GPU measurements
         # reported at N = 1; replicas only repeat the headline
-        args.no_multi = args.no_batched = args.no_config3 = True
+        args.no_multi = args.no_batched = args.no_config3 = args.no_assembly = True
     multi = None if args.no_multi else bench_multi(solver, m)
     config3 = None if args.no_config3 else bench_config3()
+    assembly = None if args.no_assembly else bench_assembly()
     batched = None if args.no_batched else bench_batched(args)
 
     cpu = None
@@ -701,6 +766,7 @@ def main():
             "clocks": clk,
             "multi_rhs": multi,
             "mixed_config3": config3,
+            "assembly": assembly,
             "batched": batched,
         }
         print(json.dumps(line))

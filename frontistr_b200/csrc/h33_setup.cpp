@@ -371,6 +371,83 @@ void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellL
   }
 }
 
+void element_profile(int n_node, int n_elem, int nn, const int *conn, std::vector<int> &indexL,
+                     std::vector<int> &itemL, std::vector<int> &indexU, std::vector<int> &itemU) {
+  // node -> elements, then the neighbour sets of each node (independent per node)
+  std::vector<int> eptr(size_t(n_node) + 1, 0), elist(size_t(n_elem) * nn);
+  for (int64_t k = 0; k < int64_t(n_elem) * nn; k++) {
+    const int v = conn[k];
+    if (v < 1 || v > n_node) throw std::runtime_error("element node id out of range");
+    eptr[size_t(v)]++;
+  }
+  for (int i = 0; i < n_node; i++) eptr[size_t(i) + 1] += eptr[size_t(i)];
+  {
+    std::vector<int> at(eptr.begin(), eptr.end() - 1);
+    for (int e = 0; e < n_elem; e++)
+      for (int a = 0; a < nn; a++) elist[size_t(at[size_t(conn[size_t(e) * nn + a] - 1)]++)] = e;
+  }
+  std::vector<std::vector<int>> lo(static_cast<size_t>(n_node)), up(static_cast<size_t>(n_node));
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int i = 0; i < n_node; i++) {
+    auto &l = lo[size_t(i)], &u = up[size_t(i)];
+    for (int k = eptr[size_t(i)]; k < eptr[size_t(i) + 1]; k++) {
+      const int e = elist[size_t(k)];
+      for (int a = 0; a < nn; a++) {
+        const int j = conn[size_t(e) * nn + a];
+        if (j < i + 1) l.push_back(j);
+        else if (j > i + 1) u.push_back(j);
+      }
+    }
+    std::sort(l.begin(), l.end());
+    l.erase(std::unique(l.begin(), l.end()), l.end());
+    std::sort(u.begin(), u.end());
+    u.erase(std::unique(u.begin(), u.end()), u.end());
+  }
+  indexL.assign(size_t(n_node) + 1, 0);
+  indexU.assign(size_t(n_node) + 1, 0);
+  for (int i = 0; i < n_node; i++) {
+    indexL[size_t(i) + 1] = indexL[size_t(i)] + int(lo[size_t(i)].size());
+    indexU[size_t(i) + 1] = indexU[size_t(i)] + int(up[size_t(i)].size());
+  }
+  itemL.resize(size_t(indexL[size_t(n_node)]));
+  itemU.resize(size_t(indexU[size_t(n_node)]));
+  for (int i = 0; i < n_node; i++) {
+    std::copy(lo[size_t(i)].begin(), lo[size_t(i)].end(), itemL.begin() + indexL[size_t(i)]);
+    std::copy(up[size_t(i)].begin(), up[size_t(i)].end(), itemU.begin() + indexU[size_t(i)]);
+  }
+}
+
+void element_contributions(int n_node, int n_elem, int nn, const int *conn, const std::vector<int> &indexL,
+                           const std::vector<int> &itemL, const std::vector<int> &indexU,
+                           const std::vector<int> &itemU, std::vector<int64_t> &ptr, std::vector<int> &code) {
+  if (int64_t(n_elem) * nn * nn >= (int64_t(1) << 31)) throw std::runtime_error("too many elements");
+  const int64_t NPL = indexL[size_t(n_node)], NPU = indexU[size_t(n_node)];
+  const int64_t nb = int64_t(n_node) + NPL + NPU;
+  // raw block id of (row i, column j), both 0-based
+  auto block_of = [&](int i, int j) -> int64_t {
+    if (i == j) return i;
+    if (j < i) {
+      const int *b = itemL.data() + indexL[size_t(i)], *e = itemL.data() + indexL[size_t(i) + 1];
+      return int64_t(n_node) + (std::lower_bound(b, e, j + 1) - itemL.data());
+    }
+    const int *b = itemU.data() + indexU[size_t(i)], *e = itemU.data() + indexU[size_t(i) + 1];
+    return int64_t(n_node) + NPL + (std::lower_bound(b, e, j + 1) - itemU.data());
+  };
+  std::vector<int64_t> blk(size_t(n_elem) * nn * nn);
+#pragma omp parallel for schedule(static)
+  for (int e = 0; e < n_elem; e++)
+    for (int a = 0; a < nn; a++)
+      for (int b = 0; b < nn; b++)
+        blk[(size_t(e) * nn + a) * nn + b] = block_of(conn[size_t(e) * nn + a] - 1, conn[size_t(e) * nn + b] - 1);
+  ptr.assign(size_t(nb) + 1, 0);
+  for (int64_t v : blk) ptr[size_t(v) + 1]++;
+  for (int64_t i = 0; i < nb; i++) ptr[size_t(i) + 1] += ptr[size_t(i)];
+  code.resize(blk.size());
+  std::vector<int64_t> at(ptr.begin(), ptr.end() - 1);
+  // element order inside every block's list (e ascending, then a, b as in the scatter loop)
+  for (size_t k = 0; k < blk.size(); k++) code[size_t(at[size_t(blk[k])]++)] = int(k);
+}
+
 void order_rows_by_length(const BlockRows &lower, const BlockRows &upper, const std::vector<int> &group_rows,
                           int lanes, std::vector<int> &order) {
   const int n = int(lower.ptr.size()) - 1;

@@ -89,6 +89,19 @@ void order_rows_by_length(const BlockRows &lower, const BlockRows &upper, const 
 void permute_rows(const BlockRows &in, const std::vector<int> &order, const std::vector<int> &iorder,
                   BlockRows &out);
 
+// Element mesh profile (hecmw_mat_con, hecmw1/src/solver/matrix/hecmw_mat_con.f90:21-107):
+// per node the sorted, unique lists of lower and upper neighbours over all elements
+// sharing it.  conn: n_elem x nn node ids, 1-based.  Outputs 1-based items.
+void element_profile(int n_node, int n_elem, int nn, const int *conn, std::vector<int> &indexL,
+                     std::vector<int> &itemL, std::vector<int> &indexU, std::vector<int> &itemU);
+
+// For every raw block (D blocks 0..N-1, then AL, then AU) the element contributions
+// in element order, as CSR: ptr (nblocks+1) and code = e*nn*nn + a*nn + b (block (a, b)
+// of element e).  Throws when the code does not fit in 31 bits.
+void element_contributions(int n_node, int n_elem, int nn, const int *conn, const std::vector<int> &indexL,
+                           const std::vector<int> &itemL, const std::vector<int> &indexU,
+                           const std::vector<int> &itemU, std::vector<int64_t> &ptr, std::vector<int> &code);
+
 // Block ILU(0) in natural order (FORM_ILU0_33, hecmw_precond_BILU_33.f90:185-362),
 // computed on the host from the hecmwST arrays.  Outputs the factor blocks in the
 // layout of the input (Dlu0 9N, ALlu0 9NPL, AUlu0 9NPU).  Returns 0 or 9001 on a

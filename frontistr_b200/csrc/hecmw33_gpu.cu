@@ -28,6 +28,7 @@
 #include <string>
 #include <vector>
 
+#include "h33_assemble.cuh"
 #include "h33_bicg.cuh"
 #include "h33_common.cuh"
 #include "h33_gnn.cuh"
@@ -267,6 +268,14 @@ struct Solver {
   DevArray<int> blk_row, blk_col;
   DevArray<double> raw_scaled, scale, b_unscaled;
   int blk_generation = -1;
+  // HEX8 assembly on the device: mesh, per-block element contribution lists, the
+  // element blocks, the profile on the device and the constraint tables
+  struct {
+    int n_node = 0, n_elem = 0, generation = -1;
+    DevArray<double> coords, E, nu, Ke, bc_value;
+    DevArray<int> conn, code, bc_first, bc_last, indexL, itemL, indexU, itemU, flag;
+    DevArray<int64_t> ptr;
+  } asmb;
   Learned L;
   int values_version = 0, a32_version = -1;
   double bnrm2 = 0.0;
@@ -387,6 +396,31 @@ void validate(int N, int NP, int NPL, int NPU, const int *indexL, const int *ite
   if (!msg.empty()) throw Failure(HECMW33_ERR_BAD_INPUT, msg);
 }
 
+// Symbolic part of set_matrix: host copy of the profile, SpMV layout, vectors.
+void set_profile(Solver &S, int N, int NPL, int NPU, const int *indexL, const int *itemL, const int *indexU,
+                 const int *itemU) {
+  S.has_matrix = false;
+  S.N = N;
+  S.NPL = NPL;
+  S.NPU = NPU;
+  S.indexL.assign(indexL, indexL + N + 1);
+  S.itemL.assign(itemL, itemL + NPL);
+  S.indexU.assign(indexU, indexU + N + 1);
+  S.itemU.assign(itemU, itemU + NPU);
+  Profile prof{N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
+  BlockRows rows;
+  unified_rows(prof, rows);
+  SellLayout lay;
+  build_sell(rows, std::vector<int>{0, N}, lay);
+  S.A.upload(lay, S.stream);
+  const size_t n3 = size_t(3) * N;
+  for (auto *v : {&S.b, &S.x, &S.r, &S.z, &S.p, &S.q, &S.w, &S.zp}) v->alloc(n3);
+  S.partials.alloc(size_t(std::max(N / 32 + 64, S.nsm * 16)) + 1024);
+  S.generation++;
+  S.pc.valid = false;
+  S.drop_graph();
+}
+
 void set_matrix(Solver &S, int N, int NP, int NPL, int NPU, const int *indexL, const int *itemL,
                 const int *indexU, const int *itemU, const double *D, const double *AL,
                 const double *AU, const int *Iarray) {
@@ -394,26 +428,7 @@ void set_matrix(Solver &S, int N, int NP, int NPL, int NPU, const int *indexL, c
                         Iarray[97] != 0;
   if (symbolic) {
     validate(N, NP, NPL, NPU, indexL, itemL, indexU, itemU);
-    S.has_matrix = false;
-    S.N = N;
-    S.NPL = NPL;
-    S.NPU = NPU;
-    S.indexL.assign(indexL, indexL + N + 1);
-    S.itemL.assign(itemL, itemL + NPL);
-    S.indexU.assign(indexU, indexU + N + 1);
-    S.itemU.assign(itemU, itemU + NPU);
-    Profile prof{N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
-    BlockRows rows;
-    unified_rows(prof, rows);
-    SellLayout lay;
-    build_sell(rows, std::vector<int>{0, N}, lay);
-    S.A.upload(lay, S.stream);
-    const size_t n3 = size_t(3) * N;
-    for (auto *v : {&S.b, &S.x, &S.r, &S.z, &S.p, &S.q, &S.w, &S.zp}) v->alloc(n3);
-    S.partials.alloc(size_t(std::max(N / 32 + 64, S.nsm * 16)) + 1024);
-    S.generation++;
-    S.pc.valid = false;
-    S.drop_graph();
+    set_profile(S, N, NPL, NPU, indexL, itemL, indexU, itemU);
   }
   const size_t nb = size_t(N) + NPL + NPU;
   S.raw.alloc(9 * nb);
@@ -1481,6 +1496,29 @@ void ensure_lowp(Solver &S) {
 // Checks and preconditioner setup shared by the FP64 and mixed solves
 // (hecmw_solve + hecmw_solve_iterative up to the CG call).  Returns 0 to go on,
 // or the code to return (2002 with X = 0, 2001).
+// Row and column (0-based nodes) of every raw block, for the kernels that need a
+// block's position (scaling, constraints); rebuilt when the profile changes.
+void ensure_block_rc(Solver &S) {
+  if (S.blk_generation == S.generation) return;
+  const int N = S.N;
+  const int64_t nb = int64_t(N) + S.NPL + S.NPU;
+  std::vector<int> br(static_cast<size_t>(nb)), bc(static_cast<size_t>(nb));
+  for (int i = 0; i < N; i++) {
+    br[size_t(i)] = bc[size_t(i)] = i;
+    for (int j = S.indexL[i]; j < S.indexL[i + 1]; j++) {
+      br[size_t(N) + j] = i;
+      bc[size_t(N) + j] = S.itemL[j] - 1;
+    }
+    for (int j = S.indexU[i]; j < S.indexU[i + 1]; j++) {
+      br[size_t(N) + S.NPL + j] = i;
+      bc[size_t(N) + S.NPL + j] = S.itemU[j] - 1;
+    }
+  }
+  S.blk_row.upload(br, S.stream);
+  S.blk_col.upload(bc, S.stream);
+  S.blk_generation = S.generation;
+}
+
 // SCALING=YES (Iarray(7), hecmw_solver_scaling_33.f90:20-208): the solve runs on
 // S A S, S b with S = diag(1/sqrt|D_kk|), and X is multiplied by S after each CG
 // (hecmw_solver_CG.f90:102,283).  The device works on a scaled copy of the resident
@@ -1494,23 +1532,7 @@ struct ScaleScope {
     if (!on) return;
     const int N = S.N;
     const int64_t nb = int64_t(N) + S.NPL + S.NPU;
-    if (S.blk_generation != S.generation) {
-      std::vector<int> br(static_cast<size_t>(nb)), bc(static_cast<size_t>(nb));
-      for (int i = 0; i < N; i++) {
-        br[size_t(i)] = bc[size_t(i)] = i;
-        for (int j = S.indexL[i]; j < S.indexL[i + 1]; j++) {
-          br[size_t(N) + j] = i;
-          bc[size_t(N) + j] = S.itemL[j] - 1;
-        }
-        for (int j = S.indexU[i]; j < S.indexU[i + 1]; j++) {
-          br[size_t(N) + S.NPL + j] = i;
-          bc[size_t(N) + S.NPL + j] = S.itemU[j] - 1;
-        }
-      }
-      S.blk_row.upload(br, S.stream);
-      S.blk_col.upload(bc, S.stream);
-      S.blk_generation = S.generation;
-    }
+    ensure_block_rc(S);
     const int n3 = S.n3();
     S.scale.alloc(size_t(n3));
     S.raw_scaled.alloc(S.raw.n);
@@ -1552,6 +1574,88 @@ struct ScaleScope {
     cudaMemcpyAsync(S.b.p, S.b_unscaled.p, sizeof(double) * S.n3(), cudaMemcpyDeviceToDevice, S.stream);
   }
 };
+
+// HEX8 linear-elastic assembly on the device (the caller side of hecmw_solve):
+// profile (hecmw_mat_con) and per-block contribution lists on the host when
+// `symbolic`, element blocks and their element-order sums on the device, nodal
+// loads F, then the constraints (hecmw_mat_ass_bc) in list order.  Leaves the
+// matrix and the right-hand side resident, as set_matrix and a B upload would.
+void assemble_hex8(Solver &S, int n_node, const double *coords, int n_elem, const int *conn, const double *E,
+                   const double *nu, const double *F, int n_bc, const int *bc_node, const int *bc_dof,
+                   const double *bc_value, bool symbolic) {
+  auto &M = S.asmb;
+  if (n_node < 1 || n_elem < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "empty mesh");
+  if (!symbolic && (M.generation != S.generation || M.n_node != n_node || M.n_elem != n_elem))
+    symbolic = true;
+  if (symbolic) {
+    std::vector<int> iL, tL, iU, tU;
+    try {
+      element_profile(n_node, n_elem, 8, conn, iL, tL, iU, tU);
+    } catch (const std::exception &e) {
+      throw Failure(HECMW33_ERR_BAD_INPUT, e.what());
+    }
+    set_profile(S, n_node, iL[size_t(n_node)], iU[size_t(n_node)], iL.data(), tL.data(), iU.data(), tU.data());
+    std::vector<int64_t> ptr;
+    std::vector<int> code;
+    element_contributions(n_node, n_elem, 8, conn, iL, tL, iU, tU, ptr, code);
+    M.ptr.upload(ptr, S.stream);
+    M.code.upload(code, S.stream);
+    M.conn.upload(conn, size_t(n_elem) * 8, S.stream);
+    M.indexL.upload(iL, S.stream);
+    M.indexU.upload(iU, S.stream);
+    M.itemL.upload(tL.empty() ? std::vector<int>{0} : tL, S.stream);
+    M.itemU.upload(tU.empty() ? std::vector<int>{0} : tU, S.stream);
+    M.Ke.alloc(size_t(n_elem) * 576);
+    M.n_node = n_node;
+    M.n_elem = n_elem;
+    M.generation = S.generation;
+  }
+  ensure_block_rc(S);
+  cudaStream_t s = S.stream;
+  M.coords.upload(coords, size_t(3) * n_node, s);
+  M.E.upload(E, size_t(n_elem), s);
+  M.nu.upload(nu, size_t(n_elem), s);
+  const int64_t nb = int64_t(n_node) + S.NPL + S.NPU;
+  S.raw.alloc(size_t(9 * nb));
+  const int64_t ne64 = int64_t(n_elem) * 64;
+  launch_k(s, hex8_element_kernel, int((ne64 + 255) / 256), 256, static_cast<const double *>(M.coords.p),
+           static_cast<const int *>(M.conn.p), n_elem, static_cast<const double *>(M.E.p),
+           static_cast<const double *>(M.nu.p), M.Ke.p);
+  launch_k(s, hex8_gather_kernel, int((9 * nb + 255) / 256), 256, static_cast<const double *>(M.Ke.p),
+           static_cast<const int64_t *>(M.ptr.p), static_cast<const int *>(M.code.p), nb, S.raw.p);
+  // right-hand side: nodal loads, then the constraints
+  if (F) H33_CUDA(cudaMemcpyAsync(S.b.p, F, sizeof(double) * 3 * n_node, cudaMemcpyHostToDevice, s));
+  else H33_CUDA(cudaMemsetAsync(S.b.p, 0, sizeof(double) * 3 * n_node, s));
+  if (n_bc > 0) {
+    std::vector<int> first(size_t(3) * n_node, -1), last(size_t(3) * n_node, -1);
+    for (int k = 0; k < n_bc; k++) {
+      if (bc_node[k] < 1 || bc_node[k] > n_node || bc_dof[k] < 1 || bc_dof[k] > 3)
+        throw Failure(HECMW33_ERR_BAD_INPUT, "constraint node or dof out of range");
+      const size_t at = size_t(3) * (bc_node[k] - 1) + (bc_dof[k] - 1);
+      if (first[at] < 0) first[at] = k;
+      last[at] = k;
+    }
+    M.bc_first.upload(first, s);
+    M.bc_last.upload(last, s);
+    M.bc_value.upload(bc_value, size_t(n_bc), s);
+    const BcArgs args{n_node, M.indexL.p, M.itemL.p, M.indexU.p, M.itemU.p, M.bc_first.p, M.bc_last.p,
+                      M.bc_value.p};
+    launch_k(s, bc_rhs_kernel, (3 * n_node + 255) / 256, 256, args, static_cast<const double *>(S.raw.p), S.b.p);
+    launch_k(s, bc_matrix_kernel, int((9 * nb + 255) / 256), 256, args, static_cast<const int *>(S.blk_row.p),
+             static_cast<const int *>(S.blk_col.p), nb, S.raw.p);
+  }
+  S.A.pack(S.raw.p, s, S.nsm);
+  S.values_version++;
+  M.flag.alloc(1);
+  H33_CUDA(cudaMemsetAsync(M.flag.p, 0, sizeof(int), s));
+  launch_k(s, zero_diag_kernel, std::max(1, std::min((n_node + kThreads - 1) / kThreads, S.nsm * 8)), kThreads,
+           static_cast<const double *>(S.raw.p), n_node, M.flag.p);
+  int zd = 0;
+  H33_CUDA(cudaMemcpyAsync(&zd, M.flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  S.sync();
+  S.zero_diag = zd != 0;
+  S.has_matrix = true;
+}
 
 int prepare_solve(Solver &S, int *Iarray, double *Rarray, double *sigma, bool *auto_sigma) {
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_set_matrix first");
@@ -2361,6 +2465,63 @@ HECMW33_API void hecmw33_gpu_precond_apply(const int *handle, const double *R, d
   H33_CUDA(cudaGetLastError());
   H33_CUDA(cudaMemcpyAsync(Z, S.z.p, bytes, cudaMemcpyDeviceToHost, S.stream));
   S.sync();
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_assemble_hex8(const int *handle, const int *n_node, const double *coords,
+                                           const int *n_elem, const int *conn, const double *E, const double *nu,
+                                           const double *F, const int *n_bc, const int *bc_node,
+                                           const int *bc_dof, const double *bc_value, const int *symbolic,
+                                           int *NPL, int *NPU, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  const int nbc = n_bc ? *n_bc : 0;
+  assemble_hex8(S, *n_node, coords, *n_elem, conn, E, nu, F, nbc, bc_node, bc_dof, bc_value,
+                !symbolic || *symbolic != 0);
+  if (NPL) *NPL = S.NPL;
+  if (NPU) *NPU = S.NPU;
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_get_matrix(const int *handle, int *indexL, int *itemL, int *indexU, int *itemU,
+                                        double *D, double *AL, double *AU, double *B, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix");
+  const int N = S.N;
+  if (indexL) std::copy(S.indexL.begin(), S.indexL.end(), indexL);
+  if (itemL) std::copy(S.itemL.begin(), S.itemL.end(), itemL);
+  if (indexU) std::copy(S.indexU.begin(), S.indexU.end(), indexU);
+  if (itemU) std::copy(S.itemU.begin(), S.itemU.end(), itemU);
+  if (D) H33_CUDA(cudaMemcpyAsync(D, S.raw.p, sizeof(double) * 9 * N, cudaMemcpyDeviceToHost, S.stream));
+  if (AL && S.NPL)
+    H33_CUDA(cudaMemcpyAsync(AL, S.raw.p + 9 * size_t(N), sizeof(double) * 9 * S.NPL, cudaMemcpyDeviceToHost,
+                             S.stream));
+  if (AU && S.NPU)
+    H33_CUDA(cudaMemcpyAsync(AU, S.raw.p + 9 * (size_t(N) + S.NPL), sizeof(double) * 9 * S.NPU,
+                             cudaMemcpyDeviceToHost, S.stream));
+  if (B) H33_CUDA(cudaMemcpyAsync(B, S.b.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, S.stream));
+  S.sync();
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_solve_assembled(const int *handle, double *X, int *Iarray, double *Rarray,
+                                             int *iter, double *resid, double *times, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_assemble_hex8 first");
+  const size_t bytes = sizeof(double) * S.n3();
+  H33_CUDA(cudaMemcpyAsync(S.x.p, X, bytes, cudaMemcpyHostToDevice, S.stream));
+  const int rc = solve_resident(S, Iarray, Rarray, iter, resid, times);
+  H33_CUDA(cudaMemcpyAsync(X, S.x.p, bytes, cudaMemcpyDeviceToHost, S.stream));
+  S.sync();
+  if (ierr) *ierr = rc;
   H33_ENTRY_END
 }
 

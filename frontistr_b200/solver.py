@@ -103,6 +103,53 @@ class GpuSolver:
         self._check(err.value)
         return z
 
+    # ---- HEX8 assembly on the device -------------------------------------------
+    def assemble_hex8(self, coords, elements, E, nu, F=None, fixed=(), symbolic=True):
+        """Assembles a linear-elastic HEX8 mesh into the resident matrix and right-hand
+        side (hecmw33_gpu_assemble_hex8).  coords (n,3); elements (ne,8) 0-based node
+        indices in hex8n order; E, nu scalars or per element; F (3n) nodal loads;
+        fixed: iterable of (node0, dof1, value) applied in order."""
+        coords = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+        conn = np.ascontiguousarray(np.asarray(elements, dtype=np.int32) + 1)
+        n, ne = coords.shape[0], conn.shape[0]
+        Ee = np.ascontiguousarray(np.broadcast_to(np.asarray(E, dtype=np.float64), (ne,)))
+        nue = np.ascontiguousarray(np.broadcast_to(np.asarray(nu, dtype=np.float64), (ne,)))
+        fixed = list(fixed)
+        bn = np.array([f[0] + 1 for f in fixed] or [0], dtype=np.int32)
+        bd = np.array([f[1] for f in fixed] or [0], dtype=np.int32)
+        bv = np.array([f[2] for f in fixed] or [0.0], dtype=np.float64)
+        Fp = None if F is None else np.ascontiguousarray(F, dtype=np.float64)
+        npl, npu, err = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        self.lib.hecmw33_gpu_assemble_hex8(
+            ctypes.byref(self.handle), _i(n), _dp(coords), _i(ne), _ip(conn), _dp(Ee), _dp(nue),
+            _dp(Fp) if Fp is not None else None, _i(len(fixed)), _ip(bn), _ip(bd), _dp(bv),
+            _i(1 if symbolic else 0), ctypes.byref(npl), ctypes.byref(npu), ctypes.byref(err))
+        self._check(err.value)
+        self.N = n
+        self.NPL, self.NPU = npl.value, npu.value
+        return self.NPL, self.NPU
+
+    def get_matrix(self):
+        """The resident matrix and right-hand side as a HecMatrix."""
+        from .matrix import HecMatrix
+        m = HecMatrix.empty(self.N, self.NPL, self.NPU)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_get_matrix(ctypes.byref(self.handle), _ip(m.indexL), _ip(m.itemL), _ip(m.indexU),
+                                        _ip(m.itemU), _dp(m.D), _dp(m.AL), _dp(m.AU), _dp(m.B),
+                                        ctypes.byref(err))
+        self._check(err.value)
+        return m
+
+    def solve_assembled(self, Iarray, Rarray, X=None):
+        """Solves the resident assembled system; returns (X, record)."""
+        X = np.zeros(3 * self.N) if X is None else np.ascontiguousarray(X, dtype=np.float64).copy()
+        err, it, res = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+        times = np.zeros(3)
+        self.lib.hecmw33_gpu_solve_assembled(ctypes.byref(self.handle), _dp(X), _ip(Iarray), _dp(Rarray),
+                                             ctypes.byref(it), ctypes.byref(res), _dp(times), ctypes.byref(err))
+        self._check(err.value)
+        return X, self._record(err.value, it, res, times)
+
     def colouring(self):
         n = self.N
         nc = ctypes.c_int(0)

@@ -14,8 +14,8 @@
  *   (C-side plugin precedent: hecmw_ML_wrapper_setup/apply/clear,
  *    hecmw1/src/solver/precond/ml/hecmw_ML_wrapper.c:320,546,571)
  *
- * Conventions (all arguments by pointer, Fortran-callable; see the mangled
- * aliases at the end):
+ * Conventions (all arguments by pointer, callable from Fortran through iso_c_binding
+ * with bind(C, name=...), as frontistr_b200/fortran/hecmw_solver_gpu33.f90 does):
  *   - Matrix arrays use the hecmwST_matrix layout: indexL/indexU have NP+1 entries
  *     (index[0] = 0); itemL/itemU hold 1-based node ids sorted ascending per row;
  *     D has 9*NP, AL 9*NPL, AU 9*NPU doubles of row-major 3x3 blocks.
@@ -304,6 +304,37 @@ HECMW33_API void hecmw33_gpu_batch_autotune(const int *handle, const double *B, 
  * solve.  dinfo[16]: last device solve seconds, last set-up seconds, team share,
  * device bytes held. */
 HECMW33_API void hecmw33_gpu_batch_info(const int *handle, int *info, double *dinfo, int *ierr);
+
+/* ---- HEX8 assembly on the device (the caller side of hecmw_solve) -------------
+ * Linear-elastic HEX8 stiffness (fistr1/src/lib/static_LIB_3d.f90:50-208, STF_C3 with
+ * full 2x2x2 Gauss, FORM361=FI; isotropic D of fistr1/src/lib/physics/ElasticLinear.f90)
+ * assembled into the handle's resident matrix in element order
+ * (hecmw1/src/solver/matrix/hecmw_mat_ass.f90:32-135), with the profile of
+ * hecmw_mat_con.f90:21-107, nodal loads F and the constraints of hecmw_mat_ass_bc
+ * (hecmw_mat_ass.f90:328-463) applied in list order.  coords: 3*n_node; conn:
+ * 8*n_elem 1-based node ids in hex8n order; E, nu: per element; F: 3*n_node nodal
+ * loads (NULL = none); bc_node (1-based), bc_dof (1..3), bc_value: n_bc constraints.
+ * symbolic = 0 reuses the profile of the previous call on the same mesh (Newton
+ * iterations).  NPL, NPU (may be NULL) receive the profile sizes.  Afterwards the
+ * matrix and right-hand side are resident: hecmw33_gpu_solve_assembled solves them,
+ * hecmw33_gpu_get_matrix copies them out.  No counterpart in hecmw_solve's interface:
+ * the reference assembles on the host before calling it. */
+HECMW33_API void hecmw33_gpu_assemble_hex8(const int *handle, const int *n_node, const double *coords,
+                                           const int *n_elem, const int *conn, const double *E,
+                                           const double *nu, const double *F, const int *n_bc,
+                                           const int *bc_node, const int *bc_dof, const double *bc_value,
+                                           const int *symbolic, int *NPL, int *NPU, int *ierr);
+
+/* Copies the resident matrix (hecmwST arrays, sizes as hecmw33_gpu_assemble_hex8
+ * reports) and right-hand side to host arrays; any pointer may be NULL. */
+HECMW33_API void hecmw33_gpu_get_matrix(const int *handle, int *indexL, int *itemL, int *indexU,
+                                        int *itemU, double *D, double *AL, double *AU, double *B,
+                                        int *ierr);
+
+/* hecmw33_gpu_solve_resident on the resident right-hand side of the last assembly:
+ * X (host, 3*N) initial guess in, solution out. */
+HECMW33_API void hecmw33_gpu_solve_assembled(const int *handle, double *X, int *Iarray, double *Rarray,
+                                             int *iter, double *resid, double *times, int *ierr);
 
 /* Copies the message of the last error of the calling thread into buf; returns its length. */
 HECMW33_API int hecmw33_gpu_last_error(char *buf, int len);
