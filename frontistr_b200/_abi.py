@@ -35,6 +35,8 @@ SIGNATURES = {
     "hecmw33_gpu_batch_autotune": [_i, _d, _d, _i, _d, _i],
     "hecmw33_gpu_batch_info": [_i, _i, _d, _i],
     "hecmw33_gpu_assemble_hex8": [_i, _i, _d, _i, _i, _d, _d, _d, _i, _i, _i, _d, _i, _i, _i, _i],
+    "hecmw33_gpu_assemble_hex8_neohooke": [_i, _i, _d, _i, _i, _d, _d, _d, _d, _i, _i, _i, _d, _i, _i, _i, _i,
+                                           _i],
     "hecmw33_gpu_get_matrix": [_i, _i, _i, _i, _i, _d, _d, _d, _d, _i],
     "hecmw33_gpu_solve_assembled": [_i, _d, _i, _d, _i, _d, _d, _i],
     "hecmw33_gpu_last_error": [ctypes.c_char_p, ctypes.c_int],

@@ -1,4 +1,5 @@
-// h33_assemble.cuh -- HEX8 linear-elastic assembly on the device.
+// h33_assemble.cuh -- HEX8 assembly on the device: linear elastic and compressible
+// Neo-Hookean (tangent and internal force).
 //
 //   element matrix   fistr1/src/lib/static_LIB_3d.f90:50-208 (STF_C3, INFINITESIMAL,
 //                    FORM361=FI: full 2x2x2 Gauss), hex8n.f90 shape functions,
@@ -230,6 +231,230 @@ static __global__ void __launch_bounds__(256) bc_matrix_kernel(BcArgs A, const i
   const bool row_fixed = A.bc_first[3 * i + r] >= 0, col_fixed = A.bc_first[3 * j + c] >= 0;
   if (!row_fixed && !col_fixed) return;
   raw[t] = (i == j && r == c) ? 1.0 : 0.0;
+}
+
+// ---- compressible Neo-Hookean, total Lagrangian (assemble.cpp neohooke_hex8) ----
+// W = C10 (J^-2/3 I1 - 3) + (J - 1)^2 / D1 (fistr1/src/lib/physics/Hyperelastic.f90:286-381).
+// Operations in the host's order with rounded intrinsics; J^-2/3 is CUDA's pow, so the
+// blocks agree with the host's to rounding rather than bitwise.
+
+// S (Voigt 11 22 33 12 23 31) and D = 2 dS/dC at F; returns J.
+__device__ __forceinline__ double nh_stress(const double F[3][3], double C10, double D1, double S[6],
+                                            double D[6][6]) {
+  const int Vi[6] = {0, 1, 2, 0, 1, 2}, Vj[6] = {0, 1, 2, 1, 2, 0};
+  double C[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < 3; k++) s = add_rn(s, mul_rn(F[k][i], F[k][j]));
+      C[i][j] = s;
+    }
+  double J = mul_rn(F[0][0], sub_rn(mul_rn(F[1][1], F[2][2]), mul_rn(F[1][2], F[2][1])));
+  J = sub_rn(J, mul_rn(F[0][1], sub_rn(mul_rn(F[1][0], F[2][2]), mul_rn(F[1][2], F[2][0]))));
+  J = add_rn(J, mul_rn(F[0][2], sub_rn(mul_rn(F[1][0], F[2][1]), mul_rn(F[1][1], F[2][0]))));
+  const double detC = mul_rn(J, J);
+  double Ci[3][3];
+  Ci[0][0] = sub_rn(mul_rn(C[1][1], C[2][2]), mul_rn(C[1][2], C[2][1])) / detC;
+  Ci[0][1] = sub_rn(mul_rn(C[0][2], C[2][1]), mul_rn(C[0][1], C[2][2])) / detC;
+  Ci[0][2] = sub_rn(mul_rn(C[0][1], C[1][2]), mul_rn(C[0][2], C[1][1])) / detC;
+  Ci[1][0] = Ci[0][1];
+  Ci[1][1] = sub_rn(mul_rn(C[0][0], C[2][2]), mul_rn(C[0][2], C[2][0])) / detC;
+  Ci[1][2] = sub_rn(mul_rn(C[0][2], C[1][0]), mul_rn(C[0][0], C[1][2])) / detC;
+  Ci[2][0] = Ci[0][2];
+  Ci[2][1] = Ci[1][2];
+  Ci[2][2] = sub_rn(mul_rn(C[0][0], C[1][1]), mul_rn(C[0][1], C[1][0])) / detC;
+  const double I1 = add_rn(add_rn(C[0][0], C[1][1]), C[2][2]);
+  const double j23 = pow(J, -2.0 / 3.0);
+  const double a = mul_rn(2.0, C10);
+  const double p = mul_rn(mul_rn(2.0 / D1, sub_rn(J, 1.0)), J);
+  const double q = mul_rn(mul_rn(2.0 / D1, sub_rn(mul_rn(2.0, J), 1.0)), J);
+  const double a23 = mul_rn(2.0, a) / 3.0, a29 = mul_rn(2.0, a) / 9.0;
+#pragma unroll
+  for (int v = 0; v < 6; v++) {
+    const int I = Vi[v], Jv = Vj[v];
+    const double dIJ = I == Jv ? 1.0 : 0.0;
+    const double cij = Ci[I][Jv];
+    S[v] = add_rn(mul_rn(mul_rn(a, j23), sub_rn(dIJ, mul_rn(I1 / 3.0, cij))), mul_rn(p, cij));
+#pragma unroll
+    for (int w = 0; w < 6; w++) {
+      const int K = Vi[w], L = Vj[w];
+      const double dKL = K == L ? 1.0 : 0.0;
+      const double ckl = Ci[K][L];
+      const double Ic = mul_rn(0.5, add_rn(mul_rn(Ci[I][K], Ci[Jv][L]), mul_rn(Ci[I][L], Ci[Jv][K])));
+      const double t1 = mul_rn(mul_rn(-a23, j23), add_rn(mul_rn(dIJ, ckl), mul_rn(cij, dKL)));
+      const double t2 = mul_rn(mul_rn(mul_rn(mul_rn(a29, j23), I1), cij), ckl);
+      const double t3 = mul_rn(mul_rn(mul_rn(a23, j23), I1), Ic);
+      const double t4 = mul_rn(mul_rn(q, cij), ckl);
+      const double t5 = mul_rn(mul_rn(2.0, p), Ic);
+      D[v][w] = sub_rn(add_rn(add_rn(add_rn(t1, t2), t3), t4), t5);
+    }
+  }
+  return J;
+}
+
+// Ke[e][a][b][9] of the tangent (material + geometric) and, from the b = 0 threads,
+// fe[e][a][3] of the internal force, at nodal displacements U; elements with J <= 0
+// at a Gauss point are counted in *inverted.
+static __global__ void __launch_bounds__(128) neohooke_element_kernel(
+    const double *__restrict__ coords, const double *__restrict__ U, const int *__restrict__ conn, int n_elem,
+    double C10, double D1, double *__restrict__ Ke, double *__restrict__ fe, int *inverted) {
+  pdl_entry();
+  const int Vi[6] = {0, 1, 2, 0, 1, 2}, Vj[6] = {0, 1, 2, 1, 2, 0};
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= int64_t(n_elem) * 64) return;
+  const int e = int(t >> 6), a = int(t & 63) >> 3, b = int(t & 7);
+  double X[8][3], u[8][3];
+#pragma unroll
+  for (int n = 0; n < 8; n++) {
+    const int node = conn[8 * size_t(e) + n] - 1;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      X[n][d] = coords[3 * size_t(node) + d];
+      u[n][d] = U[3 * size_t(node) + d];
+    }
+  }
+  const double sgn[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                            {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+  const double g = 1.0 / sqrt(3.0);
+  const double gp[2] = {-g, g};
+  double K[3][3] = {}, fa[3] = {};
+  int bad = 0;
+  for (int lz = 0; lz < 2; lz++)
+    for (int ly = 0; ly < 2; ly++)
+      for (int lx = 0; lx < 2; lx++) {
+        const double xi[3] = {gp[lx], gp[ly], gp[lz]};
+        double N[8][3];
+        double deriv[8][3];
+#pragma unroll
+        for (int n = 0; n < 8; n++) {
+          const double f0 = add_rn(1.0, mul_rn(sgn[n][0], xi[0]));
+          const double f1 = add_rn(1.0, mul_rn(sgn[n][1], xi[1]));
+          const double f2 = add_rn(1.0, mul_rn(sgn[n][2], xi[2]));
+          deriv[n][0] = mul_rn(mul_rn(mul_rn(0.125, sgn[n][0]), f1), f2);
+          deriv[n][1] = mul_rn(mul_rn(mul_rn(0.125, sgn[n][1]), f0), f2);
+          deriv[n][2] = mul_rn(mul_rn(mul_rn(0.125, sgn[n][2]), f0), f1);
+        }
+        double XJ[3][3] = {};
+#pragma unroll
+        for (int n = 0; n < 8; n++)
+#pragma unroll
+          for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) XJ[i][j] = add_rn(XJ[i][j], mul_rn(X[n][i], deriv[n][j]));
+        double w = mul_rn(mul_rn(XJ[0][0], XJ[1][1]), XJ[2][2]);
+        w = add_rn(w, mul_rn(mul_rn(XJ[1][0], XJ[2][1]), XJ[0][2]));
+        w = add_rn(w, mul_rn(mul_rn(XJ[2][0], XJ[0][1]), XJ[1][2]));
+        w = sub_rn(w, mul_rn(mul_rn(XJ[2][0], XJ[1][1]), XJ[0][2]));
+        w = sub_rn(w, mul_rn(mul_rn(XJ[1][0], XJ[0][1]), XJ[2][2]));
+        w = sub_rn(w, mul_rn(mul_rn(XJ[0][0], XJ[2][1]), XJ[1][2]));
+        const double dinv = 1.0 / w;
+        double XJI[3][3];
+        XJI[0][0] = mul_rn(dinv, sub_rn(mul_rn(XJ[1][1], XJ[2][2]), mul_rn(XJ[2][1], XJ[1][2])));
+        XJI[0][1] = mul_rn(dinv, add_rn(mul_rn(-XJ[0][1], XJ[2][2]), mul_rn(XJ[2][1], XJ[0][2])));
+        XJI[0][2] = mul_rn(dinv, sub_rn(mul_rn(XJ[0][1], XJ[1][2]), mul_rn(XJ[1][1], XJ[0][2])));
+        XJI[1][0] = mul_rn(dinv, add_rn(mul_rn(-XJ[1][0], XJ[2][2]), mul_rn(XJ[2][0], XJ[1][2])));
+        XJI[1][1] = mul_rn(dinv, sub_rn(mul_rn(XJ[0][0], XJ[2][2]), mul_rn(XJ[2][0], XJ[0][2])));
+        XJI[1][2] = mul_rn(dinv, add_rn(mul_rn(-XJ[0][0], XJ[1][2]), mul_rn(XJ[1][0], XJ[0][2])));
+        XJI[2][0] = mul_rn(dinv, sub_rn(mul_rn(XJ[1][0], XJ[2][1]), mul_rn(XJ[2][0], XJ[1][1])));
+        XJI[2][1] = mul_rn(dinv, add_rn(mul_rn(-XJ[0][0], XJ[2][1]), mul_rn(XJ[2][0], XJ[0][1])));
+        XJI[2][2] = mul_rn(dinv, sub_rn(mul_rn(XJ[0][0], XJ[1][1]), mul_rn(XJ[1][0], XJ[0][1])));
+#pragma unroll
+        for (int n = 0; n < 8; n++)
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < 3; j++) s = add_rn(s, mul_rn(deriv[n][j], XJI[j][k]));
+            N[n][k] = s;
+          }
+        double F[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+#pragma unroll
+        for (int n = 0; n < 8; n++)
+#pragma unroll
+          for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int J = 0; J < 3; J++) F[i][J] = add_rn(F[i][J], mul_rn(u[n][i], N[n][J]));
+        double S[6], D[6][6];
+        if (nh_stress(F, C10, D1, S, D) <= 0.0) bad = 1;
+        // B columns of nodes a and b: dE_v / du_{a,k}
+        double Ba[6][3], Bb[6][3];
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+#pragma unroll
+          for (int v = 0; v < 6; v++) {
+            const int I = Vi[v], J = Vj[v];
+            Ba[v][k] = I == J ? mul_rn(F[k][I], N[a][I])
+                              : add_rn(mul_rn(F[k][I], N[a][J]), mul_rn(F[k][J], N[a][I]));
+            Bb[v][k] = I == J ? mul_rn(F[k][I], N[b][I])
+                              : add_rn(mul_rn(F[k][I], N[b][J]), mul_rn(F[k][J], N[b][I]));
+          }
+        if (b == 0)
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            double f = 0.0;
+#pragma unroll
+            for (int v = 0; v < 6; v++) f = add_rn(f, mul_rn(Ba[v][k], S[v]));
+            fa[k] = add_rn(fa[k], mul_rn(w, f));
+          }
+        double DB[6][3];
+#pragma unroll
+        for (int v = 0; v < 6; v++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            double s = 0.0;
+#pragma unroll
+            for (int x = 0; x < 6; x++) s = add_rn(s, mul_rn(D[v][x], Bb[x][c]));
+            DB[v][c] = s;
+          }
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            double s = 0.0;
+#pragma unroll
+            for (int v = 0; v < 6; v++) s = add_rn(s, mul_rn(Ba[v][r], DB[v][c]));
+            K[r][c] = add_rn(K[r][c], mul_rn(w, s));
+          }
+        // geometric part on the block diagonal: N_a,I S_IJ N_b,J
+        const double Sm[3][3] = {{S[0], S[3], S[5]}, {S[3], S[1], S[4]}, {S[5], S[4], S[2]}};
+        double gab = 0.0;
+#pragma unroll
+        for (int I = 0; I < 3; I++)
+#pragma unroll
+          for (int J = 0; J < 3; J++) gab = add_rn(gab, mul_rn(mul_rn(N[a][I], Sm[I][J]), N[b][J]));
+#pragma unroll
+        for (int k = 0; k < 3; k++) K[k][k] = add_rn(K[k][k], mul_rn(w, gab));
+      }
+  double *out = Ke + 576 * size_t(e) + 9 * (8 * a + b);
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[3 * r + c] = K[r][c];
+  if (b == 0)
+#pragma unroll
+    for (int k = 0; k < 3; k++) fe[24 * size_t(e) + 3 * a + k] = fa[k];
+  if (a == 0 && b == 0 && bad) atomicAdd(inverted, 1);
+}
+
+// B(node) -= internal forces of the elements around the node, in element order (the
+// D block's contribution list of node i holds exactly those (element, local a)).
+static __global__ void __launch_bounds__(256) node_force_gather_kernel(const double *__restrict__ fe,
+                                                                      const int64_t *__restrict__ ptr,
+                                                                      const int *__restrict__ code, int n_node,
+                                                                      double *__restrict__ B) {
+  pdl_entry();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3 * n_node) return;
+  const int i = t / 3, d = t - 3 * i;
+  double s = B[t];
+  for (int64_t k = ptr[i]; k < ptr[i + 1]; k++) {
+    const int c = code[k];
+    s = sub_rn(s, fe[24 * size_t(c >> 6) + 3 * ((c & 63) >> 3) + d]);
+  }
+  B[t] = s;
 }
 
 // Any zero diagonal entry of D (hecmw_solve_check_zerodiag, hecmw_solver_Iterative.f90:255-282).

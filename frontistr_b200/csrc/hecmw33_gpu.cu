@@ -272,7 +272,7 @@ struct Solver {
   // element blocks, the profile on the device and the constraint tables
   struct {
     int n_node = 0, n_elem = 0, generation = -1;
-    DevArray<double> coords, E, nu, Ke, bc_value;
+    DevArray<double> coords, E, nu, Ke, bc_value, U, fe;
     DevArray<int> conn, code, bc_first, bc_last, indexL, itemL, indexU, itemU, flag;
     DevArray<int64_t> ptr;
   } asmb;
@@ -1575,14 +1575,23 @@ struct ScaleScope {
   }
 };
 
-// HEX8 linear-elastic assembly on the device (the caller side of hecmw_solve):
-// profile (hecmw_mat_con) and per-block contribution lists on the host when
-// `symbolic`, element blocks and their element-order sums on the device, nodal
-// loads F, then the constraints (hecmw_mat_ass_bc) in list order.  Leaves the
-// matrix and the right-hand side resident, as set_matrix and a B upload would.
-void assemble_hex8(Solver &S, int n_node, const double *coords, int n_elem, const int *conn, const double *E,
-                   const double *nu, const double *F, int n_bc, const int *bc_node, const int *bc_dof,
-                   const double *bc_value, bool symbolic) {
+// HEX8 assembly on the device (the caller side of hecmw_solve): profile
+// (hecmw_mat_con) and per-block contribution lists on the host when `symbolic`,
+// element blocks and their element-order sums on the device, nodal loads F, then
+// the constraints (hecmw_mat_ass_bc) in list order.  Leaves the matrix and the
+// right-hand side resident, as set_matrix and a B upload would.
+// Material: linear elastic (E, nu per element) or, when U is given, compressible
+// Neo-Hookean (C10, D1) at nodal displacements U: tangent K(U) and right-hand side
+// F - f_int(U); *inverted receives the number of elements with J <= 0.
+struct HexMaterial {
+  const double *E = nullptr, *nu = nullptr;  // linear elastic
+  const double *U = nullptr;                 // Neo-Hookean
+  double C10 = 0.0, D1 = 0.0;
+};
+
+void assemble_hex8(Solver &S, int n_node, const double *coords, int n_elem, const int *conn,
+                   const HexMaterial &mat, const double *F, int n_bc, const int *bc_node, const int *bc_dof,
+                   const double *bc_value, bool symbolic, int *inverted = nullptr) {
   auto &M = S.asmb;
   if (n_node < 1 || n_elem < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "empty mesh");
   if (!symbolic && (M.generation != S.generation || M.n_node != n_node || M.n_elem != n_elem))
@@ -1613,19 +1622,33 @@ void assemble_hex8(Solver &S, int n_node, const double *coords, int n_elem, cons
   ensure_block_rc(S);
   cudaStream_t s = S.stream;
   M.coords.upload(coords, size_t(3) * n_node, s);
-  M.E.upload(E, size_t(n_elem), s);
-  M.nu.upload(nu, size_t(n_elem), s);
   const int64_t nb = int64_t(n_node) + S.NPL + S.NPU;
   S.raw.alloc(size_t(9 * nb));
   const int64_t ne64 = int64_t(n_elem) * 64;
-  launch_k(s, hex8_element_kernel, int((ne64 + 255) / 256), 256, static_cast<const double *>(M.coords.p),
-           static_cast<const int *>(M.conn.p), n_elem, static_cast<const double *>(M.E.p),
-           static_cast<const double *>(M.nu.p), M.Ke.p);
+  const bool nh = mat.U != nullptr;
+  M.flag.alloc(2);
+  H33_CUDA(cudaMemsetAsync(M.flag.p, 0, 2 * sizeof(int), s));
+  if (nh) {
+    M.U.upload(mat.U, size_t(3) * n_node, s);
+    M.fe.alloc(size_t(n_elem) * 24);
+    launch_k(s, neohooke_element_kernel, int((ne64 + 127) / 128), 128, static_cast<const double *>(M.coords.p),
+             static_cast<const double *>(M.U.p), static_cast<const int *>(M.conn.p), n_elem, mat.C10, mat.D1,
+             M.Ke.p, M.fe.p, M.flag.p + 1);
+  } else {
+    M.E.upload(mat.E, size_t(n_elem), s);
+    M.nu.upload(mat.nu, size_t(n_elem), s);
+    launch_k(s, hex8_element_kernel, int((ne64 + 255) / 256), 256, static_cast<const double *>(M.coords.p),
+             static_cast<const int *>(M.conn.p), n_elem, static_cast<const double *>(M.E.p),
+             static_cast<const double *>(M.nu.p), M.Ke.p);
+  }
   launch_k(s, hex8_gather_kernel, int((9 * nb + 255) / 256), 256, static_cast<const double *>(M.Ke.p),
            static_cast<const int64_t *>(M.ptr.p), static_cast<const int *>(M.code.p), nb, S.raw.p);
-  // right-hand side: nodal loads, then the constraints
+  // right-hand side: nodal loads (minus the internal forces), then the constraints
   if (F) H33_CUDA(cudaMemcpyAsync(S.b.p, F, sizeof(double) * 3 * n_node, cudaMemcpyHostToDevice, s));
   else H33_CUDA(cudaMemsetAsync(S.b.p, 0, sizeof(double) * 3 * n_node, s));
+  if (nh)
+    launch_k(s, node_force_gather_kernel, (3 * n_node + 255) / 256, 256, static_cast<const double *>(M.fe.p),
+             static_cast<const int64_t *>(M.ptr.p), static_cast<const int *>(M.code.p), n_node, S.b.p);
   if (n_bc > 0) {
     std::vector<int> first(size_t(3) * n_node, -1), last(size_t(3) * n_node, -1);
     for (int k = 0; k < n_bc; k++) {
@@ -1646,14 +1669,13 @@ void assemble_hex8(Solver &S, int n_node, const double *coords, int n_elem, cons
   }
   S.A.pack(S.raw.p, s, S.nsm);
   S.values_version++;
-  M.flag.alloc(1);
-  H33_CUDA(cudaMemsetAsync(M.flag.p, 0, sizeof(int), s));
   launch_k(s, zero_diag_kernel, std::max(1, std::min((n_node + kThreads - 1) / kThreads, S.nsm * 8)), kThreads,
            static_cast<const double *>(S.raw.p), n_node, M.flag.p);
-  int zd = 0;
-  H33_CUDA(cudaMemcpyAsync(&zd, M.flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  int fl[2] = {0, 0};
+  H33_CUDA(cudaMemcpyAsync(fl, M.flag.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
   S.sync();
-  S.zero_diag = zd != 0;
+  S.zero_diag = fl[0] != 0;
+  if (inverted) *inverted = fl[1];
   S.has_matrix = true;
 }
 
@@ -2478,10 +2500,38 @@ HECMW33_API void hecmw33_gpu_assemble_hex8(const int *handle, const int *n_node,
   Solver &S = get(handle);
   DeviceGuard dg(S.device);
   const int nbc = n_bc ? *n_bc : 0;
-  assemble_hex8(S, *n_node, coords, *n_elem, conn, E, nu, F, nbc, bc_node, bc_dof, bc_value,
+  HexMaterial mat;
+  mat.E = E;
+  mat.nu = nu;
+  assemble_hex8(S, *n_node, coords, *n_elem, conn, mat, F, nbc, bc_node, bc_dof, bc_value,
                 !symbolic || *symbolic != 0);
   if (NPL) *NPL = S.NPL;
   if (NPU) *NPU = S.NPU;
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_assemble_hex8_neohooke(const int *handle, const int *n_node, const double *coords,
+                                                    const int *n_elem, const int *conn, const double *C10,
+                                                    const double *D1, const double *U, const double *F,
+                                                    const int *n_bc, const int *bc_node, const int *bc_dof,
+                                                    const double *bc_value, const int *symbolic, int *NPL,
+                                                    int *NPU, int *n_inverted, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  if (!U) throw Failure(HECMW33_ERR_BAD_INPUT, "nodal displacements U are required");
+  const int nbc = n_bc ? *n_bc : 0;
+  HexMaterial mat;
+  mat.U = U;
+  mat.C10 = *C10;
+  mat.D1 = *D1;
+  int inv = 0;
+  assemble_hex8(S, *n_node, coords, *n_elem, conn, mat, F, nbc, bc_node, bc_dof, bc_value,
+                !symbolic || *symbolic != 0, &inv);
+  if (NPL) *NPL = S.NPL;
+  if (NPU) *NPU = S.NPU;
+  if (n_inverted) *n_inverted = inv;
   H33_ENTRY_END
 }
 

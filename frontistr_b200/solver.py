@@ -129,6 +129,30 @@ class GpuSolver:
         self.NPL, self.NPU = npl.value, npu.value
         return self.NPL, self.NPU
 
+    def assemble_hex8_neohooke(self, coords, elements, C10, D1, U, F=None, fixed=(), symbolic=True):
+        """Neo-Hookean tangent K(U) and right-hand side F - f_int(U), then the
+        constraints (hecmw33_gpu_assemble_hex8_neohooke); returns (NPL, NPU, inverted)."""
+        coords = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+        conn = np.ascontiguousarray(np.asarray(elements, dtype=np.int32) + 1)
+        n, ne = coords.shape[0], conn.shape[0]
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        fixed = list(fixed)
+        bn = np.array([f[0] + 1 for f in fixed] or [0], dtype=np.int32)
+        bd = np.array([f[1] for f in fixed] or [0], dtype=np.int32)
+        bv = np.array([f[2] for f in fixed] or [0.0], dtype=np.float64)
+        Fp = None if F is None else np.ascontiguousarray(F, dtype=np.float64)
+        npl, npu, inv, err = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        c10, d1 = ctypes.c_double(C10), ctypes.c_double(D1)
+        self.lib.hecmw33_gpu_assemble_hex8_neohooke(
+            ctypes.byref(self.handle), _i(n), _dp(coords), _i(ne), _ip(conn), ctypes.byref(c10),
+            ctypes.byref(d1), _dp(U), _dp(Fp) if Fp is not None else None, _i(len(fixed)), _ip(bn), _ip(bd),
+            _dp(bv), _i(1 if symbolic else 0), ctypes.byref(npl), ctypes.byref(npu), ctypes.byref(inv),
+            ctypes.byref(err))
+        self._check(err.value)
+        self.N = n
+        self.NPL, self.NPU = npl.value, npu.value
+        return self.NPL, self.NPU, inv.value
+
     def get_matrix(self):
         """The resident matrix and right-hand side as a HecMatrix."""
         from .matrix import HecMatrix

@@ -325,6 +325,20 @@ HECMW33_API void hecmw33_gpu_assemble_hex8(const int *handle, const int *n_node,
                                            const int *bc_node, const int *bc_dof, const double *bc_value,
                                            const int *symbolic, int *NPL, int *NPU, int *ierr);
 
+/* As hecmw33_gpu_assemble_hex8 for a compressible Neo-Hookean material
+ * (fistr1/src/lib/physics/Hyperelastic.f90:286-381, W = C10 (I1bar - 3) + (J - 1)^2 / D1),
+ * total Lagrangian: the tangent K(U) (material + geometric) at nodal displacements U
+ * (3*n_node) and the right-hand side F - f_int(U), then the constraints.  Blocks agree
+ * with the host restatement to rounding (J^-2/3 comes from CUDA's pow).  n_inverted
+ * (may be NULL) receives the number of elements with J <= 0 at a Gauss point. */
+HECMW33_API void hecmw33_gpu_assemble_hex8_neohooke(const int *handle, const int *n_node,
+                                                    const double *coords, const int *n_elem,
+                                                    const int *conn, const double *C10, const double *D1,
+                                                    const double *U, const double *F, const int *n_bc,
+                                                    const int *bc_node, const int *bc_dof,
+                                                    const double *bc_value, const int *symbolic, int *NPL,
+                                                    int *NPU, int *n_inverted, int *ierr);
+
 /* Copies the resident matrix (hecmwST arrays, sizes as hecmw33_gpu_assemble_hex8
  * reports) and right-hand side to host arrays; any pointer may be NULL. */
 HECMW33_API void hecmw33_gpu_get_matrix(const int *handle, int *indexL, int *itemL, int *indexU,

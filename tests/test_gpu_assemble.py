@@ -93,3 +93,45 @@ def test_reassembly_reuses_profile():
     ref = host_system(X, el, 2.0 * E, nu, F, fixed)
     assert np.array_equal(g.D, ref.D) and np.array_equal(g.AL[:9 * g.NPL], ref.AL[:9 * ref.NPL])
     assert np.array_equal(g.B, ref.B)
+
+
+def box_grid(nx, ny, nz, h):
+    X, el, nid = box_mesh(nx, ny, nz, jitter=0.0)
+    return X * h, el, nid
+
+
+@pytest.mark.parametrize("amp", [0.0, 0.02])
+def test_neohooke_assembly_matches_host(amp):
+    """Tangent and residual of the compressible Neo-Hookean block at a displacement
+    field U against the host (fistr_box_neohooke + hecmw_mat_ass_bc), to rounding."""
+    from frontistr_b200.newton import NeoHookeBox
+    nx, ny, nz, h = 5, 4, 6, 0.5
+    box = NeoHookeBox(nx, ny, nz, h=h, C10=1.0, D1=0.01)
+    rng = np.random.default_rng(7)
+    X, el, nid = box_grid(nx, ny, nz, h)
+    U = amp * h * rng.standard_normal(3 * box.N)
+    ref = box.tangent(U)
+    nodes, dofs, vals = box.constraints(-0.05 * h)
+    box.apply_bc(ref, nodes, dofs, vals)
+    fixed = list(zip((nodes - 1).tolist(), dofs.tolist(), vals.tolist()))
+    with GpuSolver() as s:
+        npl, npu, inv = s.assemble_hex8_neohooke(X, el, 1.0, 0.01, U, fixed=fixed)
+        g = s.get_matrix()
+    assert inv == 0 and (npl, npu) == (ref.NPL, ref.NPU)
+    assert np.array_equal(g.itemL[:npl], ref.itemL[:npl]) and np.array_equal(g.itemU[:npu], ref.itemU[:npu])
+    scale = max(np.abs(ref.D).max(), np.abs(ref.AL[:9 * npl]).max())
+    for a, n in (("D", 9 * g.N), ("AL", 9 * npl), ("AU", 9 * npu)):
+        assert np.abs(getattr(g, a)[:n] - getattr(ref, a)[:n]).max() <= 1e-13 * scale, a
+    bscale = max(np.abs(ref.B).max(), 1e-300)
+    assert np.abs(g.B - ref.B).max() <= 1e-12 * bscale
+
+
+def test_neohooke_inverted_elements_are_counted():
+    nx, ny, nz, h = 2, 2, 2, 1.0
+    X, el, nid = box_grid(nx, ny, nz, h)
+    U = np.zeros(3 * len(X))
+    c = nid(1, 1, 1)
+    U[3 * c:3 * c + 3] = [2.5, 2.5, 2.5]  # the centre node pushed through its neighbours
+    with GpuSolver() as s:
+        _, _, inv = s.assemble_hex8_neohooke(X, el, 1.0, 0.01, U)
+    assert inv == 4  # as the host counts them (fistr_box_neohooke)
