@@ -362,10 +362,30 @@ def bench_assembly(n=64, seed=3):
     t4 = time.perf_counter()
     same = bool(np.array_equal(g2.D, ref.D) and np.array_equal(g2.AL[:9 * ref.NPL], ref.AL[:9 * ref.NPL])
                 and np.array_equal(g2.AU[:9 * ref.NPU], ref.AU[:9 * ref.NPU]) and np.array_equal(g2.B, ref.B))
-    return {"workload": "%d^3 HEX8 box, jitter 0.2h, log-normal E, nu U[0.25, 0.40], clamped base" % n,
-            "elements": int(len(el)), "nodes": int(len(X)), "gpu_first_call_s": t1 - t0,
-            "gpu_reassembly_s": t2 - t1, "host_s": t4 - t3, "host_kind": "fistr_mesh_assemble, 1 thread",
-            "bitwise_equal_to_host": same, "speedup_reassembly_vs_host": (t4 - t3) / (t2 - t1)}
+    out = {"workload": "%d^3 HEX8 box, jitter 0.2h, log-normal E, nu U[0.25, 0.40], clamped base" % n,
+           "elements": int(len(el)), "nodes": int(len(X)), "gpu_first_call_s": t1 - t0,
+           "gpu_reassembly_s": t2 - t1, "host_s": t4 - t3, "host_kind": "fistr_mesh_assemble, 1 thread",
+           "bitwise_equal_to_host": same, "speedup_reassembly_vs_host": (t4 - t3) / (t2 - t1)}
+    # Neo-Hookean tangent + residual of the Newton workload's block (64^3, h = 1) at a
+    # displacement field, against the host's OpenMP assembly (fistr_box_neohooke)
+    from frontistr_b200.newton import NeoHookeBox
+    box = NeoHookeBox(n, n, n, h=1.0, C10=1.0, D1=0.01)
+    Xg = X.copy()
+    Xg[:] = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).transpose(2, 1, 0, 3).reshape(-1, 3)
+    U = np.zeros(3 * box.N)
+    U[2::3] = -0.02 * Xg[:, 2]
+    with GpuSolver() as s:
+        s.assemble_hex8_neohooke(Xg, el, 1.0, 0.01, U)
+        t5 = time.perf_counter()
+        s.assemble_hex8_neohooke(Xg, el, 1.0, 0.01, U, symbolic=False)
+        t6 = time.perf_counter()
+    t7 = time.perf_counter()
+    box.tangent(U)
+    t8 = time.perf_counter()
+    out["neohooke"] = {"gpu_reassembly_s": t6 - t5, "host_s": t8 - t7,
+                       "host_kind": "fistr_box_neohooke, OpenMP over %d threads" % (os.cpu_count() or 1),
+                       "speedup_vs_host": (t8 - t7) / (t6 - t5)}
+    return out
 
 
 def bench_learned_newton(args):
