@@ -10,7 +10,7 @@ public dataset).  One step = one solve to relative residual 1e-8 with CG + SSOR
 
   value        seconds per solve with B, X and the matrix resident in HBM
                (device events around the one-graph CG solve), max over ranks
-  e2e          seconds per solve through the drop-in C-ABI call with host buffers
+  e2e          seconds per solve through the drop-in C-ABI call with host buffers (pinned)
                (hecmw33_gpu_solve: matrix values + B + X uploaded, numeric
                preconditioner rebuild, solve, X downloaded), wall clock
   roofline     the plain FP64 SpMV (spmv_kernel) against measured HBM bandwidth
