@@ -31,6 +31,7 @@
 #include "h33_assemble.cuh"
 #include "h33_bicg.cuh"
 #include "h33_common.cuh"
+#include "h33_gmres.cuh"
 #include "h33_gnn.cuh"
 #include "h33_kernels.cuh"
 #include "h33_multi.cuh"
@@ -265,6 +266,10 @@ struct Solver {
   // values and the unscaled right-hand side while a scaled solve runs
   // BiCGSTAB vectors: r_tld, s, s_tld, t ({p_tld} and {v} use z and q)
   DevArray<double> b_rt, b_s, b_st, b_t;
+  // GMRES(m): Krylov basis (m+1 vectors), w, zq, av; the small system (H, s, y, ss,
+  // scalars) and the breakdown flag
+  DevArray<double> g_V, g_w, g_zq, g_av, g_small;
+  DevArray<int> g_flag;
   DevArray<int> blk_row, blk_col;
   DevArray<double> raw_scaled, scale, b_unscaled;
   int blk_generation = -1;
@@ -1695,14 +1700,138 @@ int prepare_solve(Solver &S, int *Iarray, double *Rarray, double *sigma, bool *a
   *auto_sigma = *sigma < 0.0;
   if (*auto_sigma) *sigma = 1.0;
   if (S.zero_diag && PRECOND < 10 && iterPREmax > 0) return HECMW33_ERR_ZERO_DIAG;
-  if (METHOD != 1 && METHOD != 2)
-    throw Failure(HECMW33_ERR_INCONS_PC,
-                  "METHOD " + std::to_string(METHOD) + ": the GPU drop-in implements CG (1) and BiCGSTAB (2)");
+  if (METHOD < 1 || METHOD > 3)
+    throw Failure(HECMW33_ERR_INCONS_PC, "METHOD " + std::to_string(METHOD) +
+                                             ": the GPU drop-in implements CG (1), BiCGSTAB (2) and GMRES (3)");
   if (METHOD == 2 || Iarray[7] == 2) ensure_bicg(S);
   recycle_precond_setting(Iarray);
   Range rg("hecmw33_precond_setup");
   if (iterPREmax > 0) precond_setup(S, PRECOND, Iarray[33], *sigma, Iarray);
   return 0;
+}
+
+// hecmw_solve_GMRES (hecmw_solver_GMRES.f90:123-411) on the resident B and X in FP64:
+// right-preconditioned GMRES(NREST) with modified Gram-Schmidt and Givens rotations.
+// Returns the device-side seconds; sets *error (0 or 3001), *iter and *resid.
+float run_gmres(Solver &S, int iterpremax, double tol, int maxit, int nrest, int lowp, int *kernels, int *error,
+                int *iter, double *resid) {
+  cudaStream_t s = S.stream;
+  const int n3 = S.n3();
+  int m = nrest;
+  if (m >= n3 - 1) m = n3 - 2;  // :93
+  if (m < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "GMRES needs NREST >= 1");
+  const int ld = m + 7, CS = m + 1, SN = m + 2;
+  S.g_V.alloc(size_t(m + 1) * n3);
+  for (auto *v : {&S.g_w, &S.g_zq, &S.g_av}) v->alloc(size_t(n3));
+  const size_t nsmall = size_t(ld) * ld + 3 * size_t(ld + 2) + 3;
+  S.g_small.alloc(nsmall);
+  S.g_flag.alloc(1);
+  H33_CUDA(cudaMemsetAsync(S.g_small.p, 0, sizeof(double) * nsmall, s));
+  double *base = S.g_small.p;
+  GmresDev g{base, base + size_t(ld) * ld, base + size_t(ld) * ld + (ld + 2), base + nsmall - 3,
+             base + nsmall - 2, base + nsmall - 1, S.g_flag.p, ld};
+  double *ss = base + size_t(ld) * ld + 2 * size_t(ld + 2);
+  const Views<double> V = views(S, 0.0, lowp);
+  CgState *st = S.state.p;
+  S.h_params->tol = tol;
+  S.h_params->maxit = maxit;
+  S.h_params->iterpremax = iterpremax;
+  S.h_params->inner = S.h_params->flexible = S.h_params->use_gnn = S.h_params->reliable = 0;
+  S.h_params->ru_delta = 0.0;
+  S.h_params->method = 3;
+  H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, s));
+  H33_CUDA(cudaEventRecord(S.ev0, s));
+  launch_k(s, cg_init_kernel, 1, 32, st, static_cast<const CgParams *>(S.params.p));
+  int launched = 1;
+  auto vec = [&](int k) { return S.g_V.p + size_t(k) * n3; };
+  auto precond = [&](const double *in, double *out) { launch_precond_plain<double>(S, V, iterpremax, in, out, nullptr); };
+  auto finish = [&](int irow) {  // [H]{y} = {s}; {av} = V y; {zq} = M^-1 {av}; {x} += {zq}
+    launch_k(s, gmres_trisolve_kernel, 1, 32, g, irow, ss);
+    launch_k(s, gmres_combine_kernel, S.grid_vec(), kThreads, static_cast<const double *>(S.g_V.p), size_t(n3),
+             irow, g, n3, S.g_av.p);
+    precond(S.g_av.p, S.g_zq.p);
+    launch_k(s, gmres_update_x_kernel, S.grid_vec(), kThreads, static_cast<const double *>(S.g_zq.p), S.x.p, n3);
+    launched += 4;
+  };
+  // {r} = {b} - [A]{x0}, BNRM2
+  launch_k(s, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, V.A, V.x, V.r, V.b, nullptr, nullptr);
+  const double bnrm2 = dot_device(S, S.b.p, S.b.p);
+  *error = 0;
+  *iter = 0;
+  *resid = 0.0;
+  int I = 0;
+  bool exit_outer = false;
+  while (!exit_outer) {
+    I = 0;
+    const double dnrm2 = dot_device(S, S.r.p, S.r.p);
+    if (dnrm2 == 0.0) break;  // converged
+    const double rnorm = std::sqrt(dnrm2);
+    launch_k(s, gmres_start_kernel, S.grid_vec(), kThreads, static_cast<const double *>(S.r.p), vec(0), n3,
+             1.0 / rnorm);
+    H33_CUDA(cudaMemsetAsync(g.s, 0, sizeof(double) * (ld + 2), s));
+    H33_CUDA(cudaMemcpyAsync(g.s + 1, &rnorm, sizeof(double), cudaMemcpyHostToDevice, s));
+    H33_CUDA(cudaMemsetAsync(S.g_flag.p, 0, sizeof(int), s));
+    launched++;
+    bool broke = false;
+    for (I = 1; I <= m; I++) {
+      (*iter)++;
+      precond(vec(I - 1), S.g_zq.p);
+      launch_k(s, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, V.A, static_cast<const double *>(S.g_zq.p),
+               S.g_w.p, static_cast<const double *>(nullptr), static_cast<CgState *>(nullptr),
+               static_cast<double *>(nullptr));
+      for (int K = 1; K <= I; K++) {
+        launch_k(s, gmres_dot_kernel, S.grid_vec(), kThreads, static_cast<const double *>(S.g_w.p),
+                 static_cast<const double *>(vec(K - 1)), n3, g, K, I, st, S.partials.p);
+        launch_k(s, gmres_orth_kernel, S.grid_vec(), kThreads, S.g_w.p, static_cast<const double *>(vec(K - 1)),
+                 n3, g, K, I);
+      }
+      launch_k(s, gmres_norm_kernel, S.grid_vec(), kThreads, static_cast<const double *>(S.g_w.p), n3, g, I, st,
+               S.partials.p);
+      launch_k(s, gmres_scale_kernel, S.grid_vec(), kThreads, static_cast<const double *>(S.g_w.p), vec(I), n3, g);
+      launch_k(s, gmres_givens_kernel, 1, 32, g, I, CS, SN, bnrm2);
+      launched += 5 + 2 * I;
+      int brk = 0;
+      double rs = 0.0;
+      H33_CUDA(cudaMemcpyAsync(&brk, S.g_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      H33_CUDA(cudaMemcpyAsync(&rs, g.resid, sizeof(double), cudaMemcpyDeviceToHost, s));
+      S.sync();
+      if (brk) {  // {w} = 0: the reference leaves the inner loop (:231)
+        broke = true;
+        break;
+      }
+      *resid = rs;
+      if (rs <= tol) {
+        finish(I);
+        exit_outer = true;
+        break;
+      }
+      if (*iter > maxit) {
+        *error = HECMW33_ERR_NOCONV_MAXIT;
+        exit_outer = true;
+        break;
+      }
+    }
+    if (exit_outer) break;
+    (void)broke;
+    // current solution and the true residual of the restart (:331-377)
+    finish(m);
+    launch_k(s, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, V.A, V.x, V.r, V.b, nullptr, nullptr);
+    const double d2 = dot_device(S, S.r.p, S.r.p);
+    *resid = std::sqrt(d2 / bnrm2);
+    launched += 2;
+    if (*resid <= tol) break;
+    if (*iter > maxit) {
+      *error = HECMW33_ERR_NOCONV_MAXIT;
+      break;
+    }
+  }
+  if (*error == HECMW33_ERR_NOCONV_MAXIT) finish(I);  // :382-411
+  H33_CUDA(cudaEventRecord(S.ev1, s));
+  S.sync();
+  float ms = 0.0f;
+  H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+  if (kernels) *kernels += launched;
+  return ms;
 }
 
 // The hecmw_solve / hecmw_solve_iterative sequence on resident B (S.b) and X (S.x),
@@ -1728,7 +1857,7 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   if (lowp && iterPREmax > 0) ensure_lowp(S);
   else lowp = 0;
   const bool record = S.L.recording && !learned && method == 1;
-  if (graph_mode() && !record)
+  if (graph_mode() && !record && method != 3)
     build_graph<double>(S, iterPREmax, learned | (lowp ? 4 : 0) | (method == 2 ? 8 : 0));
   Range rs("hecmw33_solve");
   const double t1 = wall();
@@ -1737,12 +1866,16 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   for (;;) {
     Iarray[80] = 0;
     Iarray[81] = 0;
-    if (record) ms_total += record_cg(S, iterPREmax, TOL, MAXIT, &kernels);
-    else ms_total += run_cg<double>(S, iterPREmax, TOL, MAXIT, &kernels, 0, learned, 0, 1e-4, lowp, method);
-    const CgState &st = *S.h_state;
-    error = st.error;
-    *iter = st.iter;
-    *resid = st.resid;
+    if (method == 3) {
+      ms_total += run_gmres(S, iterPREmax, TOL, MAXIT, Iarray[5], lowp, &kernels, &error, iter, resid);
+    } else {
+      if (record) ms_total += record_cg(S, iterPREmax, TOL, MAXIT, &kernels);
+      else ms_total += run_cg<double>(S, iterPREmax, TOL, MAXIT, &kernels, 0, learned, 0, 1e-4, lowp, method);
+      const CgState &st = *S.h_state;
+      error = st.error;
+      *iter = st.iter;
+      *resid = st.resid;
+    }
     scaling.x_back();  // the end of each hecmw_solve_CG call
     if (error == HECMW33_ERR_DIVERGE_PC || error == HECMW33_ERR_DIVERGE_MAT || error == HECMW33_ERR_DIVERGE_NAN) {
       Iarray[81] = 1;
@@ -1753,9 +1886,9 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
         continue;
       } else if (method == 1 && METHOD2 > 1) {
         // Iterative.f90:138-142: a diverged CG hands over to METHOD2 from the current X
-        if (METHOD2 != 2)
+        if (METHOD2 != 2 && METHOD2 != 3)
           throw Failure(HECMW33_ERR_INCONS_PC, "METHOD2 " + std::to_string(METHOD2) +
-                                                   ": the GPU drop-in implements BiCGSTAB (2) as the fallback");
+                                                   ": the GPU drop-in implements BiCGSTAB (2) and GMRES (3)");
         if (auto_sigma) sigma = 1.0;
         method = METHOD2;
         learned = 0;
@@ -2275,8 +2408,8 @@ int solve_multi(Solver &S, int nrhs, const double *dB, double *dX, int *Iarray, 
 int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
   if (Iarray[6] != 0 && (Iarray[41] == 2 || Iarray[41] == 3))
     throw Failure(HECMW33_ERR_BAD_INPUT, "SCALING=YES is implemented for the FP64 CG (Iarray(42) = 0 or 1)");
-  if (Iarray[1] == 2 && (Iarray[41] == 2 || Iarray[41] == 3))
-    throw Failure(HECMW33_ERR_BAD_INPUT, "BiCGSTAB runs in FP64 (Iarray(42) = 0 or 1)");
+  if (Iarray[1] >= 2 && (Iarray[41] == 2 || Iarray[41] == 3))
+    throw Failure(HECMW33_ERR_BAD_INPUT, "BiCGSTAB and GMRES run in FP64 (Iarray(42) = 0 or 1)");
   switch (Iarray[41]) {
     case 1: return solve_fp64(S, Iarray, Rarray, iter, resid, times, 1);
     case 2: return solve_mixed_restart(S, Iarray, Rarray, iter, resid, times);

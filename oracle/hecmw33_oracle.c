@@ -8,6 +8,7 @@
  *   hecmw1/src/solver/iterative/hecmw_solver_Iterative.f90:13-187,255-323
  *   hecmw1/src/solver/iterative/hecmw_solver_CG.f90:19-320        (hecmw_solve_CG)
  *   hecmw1/src/solver/iterative/hecmw_solver_BiCGSTAB.f90:125-271 (hecmw_solve_BiCGSTAB)
+ *   hecmw1/src/solver/iterative/hecmw_solver_GMRES.f90:93-411     (hecmw_solve_GMRES)
  *   hecmw1/src/solver/las/hecmw_solver_scaling_33.f90:20-208      (SCALING=YES)
  *   hecmw1/src/solver/las/hecmw_solver_las_33.F90:120-435         (matvec/matresid/rel_resid)
  *   hecmw1/src/solver/communication/hecmw_solver_misc.F90:46-201  (dot/axpy/xpay)
@@ -894,6 +895,134 @@ int o33_bicgstab(const o33_matrix *A, const o33_precond *P, int iterpremax, int 
   return error;
 }
 
+/* hecmw_solve_GMRES (hecmw_solver_GMRES.f90:93-411): right-preconditioned
+ * GMRES(NREST), modified Gram-Schmidt, Givens rotations stored in H(:,CS/SN). */
+int o33_gmres(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol, int nrest,
+              const double *B, double *X, int *iter_out, double *resid_out) {
+  const int NP = A->NP, NN = 3 * A->N;
+  const size_t len = 3 * (size_t)NP;
+  int NREST = nrest;
+  if (NREST >= 3 * NP - 1) NREST = 3 * NP - 2;
+  const int NRK = NREST + 7, CS = NREST + 1, SN = CS + 1;
+  double *H = (double *)calloc((size_t)NRK * NRK, sizeof(double));
+#define HH(k, i) H[(size_t)((i)-1) * NRK + ((k)-1)]
+  double *SS = (double *)calloc((size_t)NRK + 1, sizeof(double));
+  double *Sv = (double *)calloc((size_t)NRK + 2, sizeof(double)); /* WW(:,S), 1-based */
+  double *Yv = (double *)calloc((size_t)NRK + 2, sizeof(double)); /* WW(:,Y) leading entries */
+  double *R = (double *)calloc(len, sizeof(double)), *W = (double *)calloc(len, sizeof(double));
+  double *ZQ = (double *)calloc(len, sizeof(double)), *ZP = (double *)calloc(len, sizeof(double));
+  double *AV = (double *)calloc(len, sizeof(double));
+  double *V = (double *)calloc(len * (size_t)(NREST + 1), sizeof(double));
+  int error = 0, ITER = 0, I = 0;
+  double RESID = 0.0;
+  o33_matresid(A, X, B, R);
+  const double BNRM2 = o33_dot(NN, B, B);
+  /* [H]{y} = {s}, {x} += M^-1 (V y) */
+#define GMRES_FINISH(IROW_)                                                         \
+  do {                                                                              \
+    const int IROW = (IROW_);                                                       \
+    for (int ik = 1; ik <= IROW; ik++) SS[ik] = Sv[ik];                              \
+    Yv[IROW] = SS[IROW] / HH(IROW, IROW);                                           \
+    for (int kk = IROW - 1; kk >= 1; kk--) {                                        \
+      for (int jj = IROW; jj >= kk + 1; jj--) SS[kk] = SS[kk] - HH(kk, jj) * Yv[jj]; \
+      Yv[kk] = SS[kk] / HH(kk, kk);                                                 \
+    }                                                                               \
+    for (int i_ = 0; i_ < NN; i_++) AV[i_] = 0.0;                                   \
+    for (int jj = 1; jj <= IROW; jj++) axpy(NN, Yv[jj], V + len * (size_t)(jj - 1), AV); \
+    o33_precond_apply(P, A, iterpremax, AV, ZQ, ZP);                                \
+    axpy(NN, 1.0, ZQ, X);                                                           \
+  } while (0)
+  for (;;) { /* OUTER */
+    I = 0;
+    const double DNRM2 = o33_dot(NN, R, R);
+    if (DNRM2 == 0.0) break;
+    const double RNORM = sqrt(DNRM2);
+    const double coef = 1.0 / RNORM;
+    for (int i = 0; i < NN; i++) V[i] = coef * R[i]; /* hecmw_axpby_R(coef, 0) */
+    for (int k = 0; k < NRK + 2; k++) Sv[k] = 0.0;
+    Sv[1] = RNORM;
+    int exit_outer = 0;
+    for (I = 1; I <= NREST; I++) {
+      ITER++;
+      o33_precond_apply(P, A, iterpremax, V + len * (size_t)(I - 1), ZQ, ZP);
+      o33_matvec(A, ZQ, W);
+      for (int K = 1; K <= I; K++) {
+        const double val = o33_dot(NN, W, V + len * (size_t)(K - 1));
+        axpy(NN, -val, V + len * (size_t)(K - 1), W);
+        HH(K, I) = val;
+      }
+      const double val = o33_dot(NN, W, W);
+      if (val == 0.0) break;
+      HH(I + 1, I) = sqrt(val);
+      const double c2 = 1.0 / HH(I + 1, I);
+      for (int i = 0; i < NN; i++) V[len * (size_t)I + i] = c2 * W[i];
+      for (int k = 1; k <= I - 1; k++) {
+        const double VCS = HH(k, CS), VSN = HH(k, SN);
+        const double DTEMP = VCS * HH(k, I) + VSN * HH(k + 1, I);
+        HH(k + 1, I) = VCS * HH(k + 1, I) - VSN * HH(k, I);
+        HH(k, I) = DTEMP;
+      }
+      const double AA = HH(I, I), BB = HH(I + 1, I);
+      double R0 = BB;
+      if (fabs(AA) > fabs(BB)) R0 = AA;
+      const double scale = fabs(AA) + fabs(BB);
+      if (scale != 0.0) {
+        double RR = scale * sqrt((AA / scale) * (AA / scale) + (BB / scale) * (BB / scale));
+        RR = copysign(1.0, R0) * RR;
+        HH(I, CS) = AA / RR;
+        HH(I, SN) = BB / RR;
+      } else {
+        HH(I, CS) = 1.0;
+        HH(I, SN) = 0.0;
+      }
+      const double VCS = HH(I, CS), VSN = HH(I, SN);
+      double DTEMP = VCS * HH(I, I) + VSN * HH(I + 1, I);
+      HH(I + 1, I) = VCS * HH(I + 1, I) - VSN * HH(I, I);
+      HH(I, I) = DTEMP;
+      DTEMP = VCS * Sv[I] + VSN * Sv[I + 1];
+      Sv[I + 1] = VCS * Sv[I + 1] - VSN * Sv[I];
+      Sv[I] = DTEMP;
+      RESID = fabs(Sv[I + 1]) / sqrt(BNRM2);
+      if (RESID <= tol) {
+        GMRES_FINISH(I);
+        exit_outer = 1;
+        break;
+      }
+      if (ITER > maxit) {
+        error = ERR_NOCONV_MAXIT;
+        exit_outer = 1;
+        break;
+      }
+    }
+    if (exit_outer) break;
+    GMRES_FINISH(NREST);
+    o33_matresid(A, X, B, R);
+    const double D2 = o33_dot(NN, R, R);
+    RESID = sqrt(D2 / BNRM2);
+    if (RESID <= tol) break;
+    if (ITER > maxit) {
+      error = ERR_NOCONV_MAXIT;
+      break;
+    }
+  }
+  if (error == ERR_NOCONV_MAXIT) GMRES_FINISH(I);
+#undef GMRES_FINISH
+#undef HH
+  *iter_out = ITER;
+  *resid_out = RESID;
+  free(H);
+  free(SS);
+  free(Sv);
+  free(Yv);
+  free(R);
+  free(W);
+  free(ZQ);
+  free(ZP);
+  free(AV);
+  free(V);
+  return error;
+}
+
 double o33_cg_fixed_iters(const o33_matrix *A, const o33_precond *P, int iterpremax, int n,
                           const double *B, double *X) {
   const int NP = A->NP, NN = 3 * A->N;
@@ -1006,7 +1135,7 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
     for (int j = 0; j < 3; j++)
       if (fabs(A->D[9 * i + 4 * j]) == 0.0) zdiag = ERR_ZERO_DIAG;
   if (zdiag && PRECOND < 10 && iterPREmax > 0) return ERR_ZERO_DIAG;
-  if (METHOD != 1 && METHOD != 2) return ERR_INCONS_PC;
+  if (METHOD < 1 || METHOD > 3) return ERR_INCONS_PC;
   recycle_precond_setting(Iarray);
 
   /* SCALING=YES (Iarray(7)): hecmw_solve_CG works on S A S, S B and multiplies X
@@ -1065,6 +1194,7 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
       }
     }
     if (METHOD == 2) error = o33_bicgstab(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid);
+    else if (METHOD == 3) error = o33_gmres(Aw, P, iterPREmax, MAXIT, TOL, Iarray[5], Bw, X, &iter, &resid);
     else error = o33_cg(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid, NULL);
     if (!cache) o33_precond_free(P);
     if (SCALING) /* hecmw_solver_scaling_bk_33: X = S X (:144-147) */
@@ -1076,8 +1206,8 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
         continue;
       } else if (METHOD == 1 && METHOD2 > 1) { /* hecmw_solver_Iterative.f90:138-142 */
         if (auto_sigma_diag == 1) SIGMA_DIAG = 1.0;
-        if (METHOD2 != 2) {
-          error = ERR_INCONS_PC; /* only BiCGSTAB is restated here */
+        if (METHOD2 != 2 && METHOD2 != 3) {
+          error = ERR_INCONS_PC; /* only BiCGSTAB and GMRES are restated here */
           break;
         }
         METHOD = METHOD2;
