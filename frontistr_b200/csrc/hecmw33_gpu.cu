@@ -31,6 +31,7 @@
 #include "h33_assemble.cuh"
 #include "h33_bicg.cuh"
 #include "h33_common.cuh"
+#include "h33_cr.cuh"
 #include "h33_gmres.cuh"
 #include "h33_gnn.cuh"
 #include "h33_kernels.cuh"
@@ -1700,10 +1701,11 @@ int prepare_solve(Solver &S, int *Iarray, double *Rarray, double *sigma, bool *a
   *auto_sigma = *sigma < 0.0;
   if (*auto_sigma) *sigma = 1.0;
   if (S.zero_diag && PRECOND < 10 && iterPREmax > 0) return HECMW33_ERR_ZERO_DIAG;
-  if (METHOD < 1 || METHOD > 3)
-    throw Failure(HECMW33_ERR_INCONS_PC, "METHOD " + std::to_string(METHOD) +
-                                             ": the GPU drop-in implements CG (1), BiCGSTAB (2) and GMRES (3)");
-  if (METHOD == 2 || Iarray[7] == 2) ensure_bicg(S);
+  if (METHOD < 1 || (METHOD > 3 && METHOD != 7))
+    throw Failure(HECMW33_ERR_INCONS_PC,
+                  "METHOD " + std::to_string(METHOD) + ": the GPU drop-in implements CG (1), BiCGSTAB (2), GMRES (3) "
+                                                       "and CR (7)");
+  if (METHOD == 2 || Iarray[7] == 2 || METHOD == 7 || Iarray[7] == 7) ensure_bicg(S);
   recycle_precond_setting(Iarray);
   Range rg("hecmw33_precond_setup");
   if (iterPREmax > 0) precond_setup(S, PRECOND, Iarray[33], *sigma, Iarray);
@@ -1834,6 +1836,116 @@ float run_gmres(Solver &S, int iterpremax, double tol, int maxit, int nrest, int
   return ms;
 }
 
+// hecmw_solve_CR (hecmw_solver_CR.f90:108-296) on the resident B and X in FP64:
+// preconditioned conjugate residual with the recursive residual {rt} and explicit
+// true-residual checks (every 100th iteration, at RESID_REC <= TOL and at MAXIT).
+// Vectors: x, rt = S.r, z = S.z, p = S.p, ap = S.q, map / az / wk in the BiCGSTAB
+// buffers.  Returns the device-side seconds; sets *error, *iter, *resid.
+float run_cr(Solver &S, int iterpremax, double tol, int maxit, int lowp, int *kernels, int *error, int *iter,
+             double *resid) {
+  cudaStream_t s = S.stream;
+  const int n3 = S.n3();
+  constexpr int kCheckTrue = 100;  // N_ITER_CHECK_TRUE_R
+  ensure_bicg(S);
+  double *x = S.x.p, *rt = S.r.p, *z = S.z.p, *p = S.p.p, *ap = S.q.p;
+  double *map = S.b_s.p, *az = S.b_t.p, *wk = S.b_st.p;
+  const Views<double> V = views(S, 0.0, lowp);
+  int launched = 0;
+  auto spmv = [&](const double *in, double *out) {
+    launch_k(s, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, V.A, in, out, static_cast<const double *>(nullptr),
+             static_cast<CgState *>(nullptr), static_cast<double *>(nullptr));
+    launched++;
+  };
+  auto resid_into = [&](double *out) {  // out = b - A x
+    launch_k(s, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, V.A, static_cast<const double *>(x), out,
+             static_cast<const double *>(S.b.p), static_cast<CgState *>(nullptr), static_cast<double *>(nullptr));
+    launched++;
+  };
+  auto precond = [&](const double *in, double *out) { launch_precond_plain<double>(S, V, iterpremax, in, out, nullptr); };
+  H33_CUDA(cudaEventRecord(S.ev0, s));
+  *error = 0;
+  *iter = 0;
+  *resid = 0.0;
+  resid_into(rt);
+  const double bnrm2 = dot_device(S, S.b.p, S.b.p);
+  double rTAr_old = 0.0;
+  int MAXIT = maxit;
+  {
+    const double dnrm2 = dot_device(S, rt, rt);
+    *resid = std::sqrt(dnrm2 / bnrm2);
+    if (*resid <= tol) {
+      MAXIT = 0;
+    } else {
+      precond(rt, z);
+      H33_CUDA(cudaMemcpyAsync(p, z, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+      spmv(z, az);
+      H33_CUDA(cudaMemcpyAsync(ap, az, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+      rTAr_old = dot_device(S, z, az);
+      if (rTAr_old != rTAr_old) {
+        *error = HECMW33_ERR_DIVERGE_NAN;
+        MAXIT = 0;
+      } else if (rTAr_old <= 0.0) {
+        *error = HECMW33_ERR_DIVERGE_MAT;
+        MAXIT = 0;
+      }
+    }
+  }
+  int it = 1;
+  for (it = 1; it <= MAXIT; it++) {
+    precond(ap, map);
+    const double apTap = dot_device(S, ap, map);
+    if (apTap != apTap) {
+      *error = HECMW33_ERR_DIVERGE_NAN;
+      break;
+    } else if (apTap <= 0.0) {
+      *error = HECMW33_ERR_DIVERGE_PC;
+      break;
+    }
+    const double alpha = rTAr_old / apTap;
+    launch_k(s, cr_update_kernel, S.grid_vec(), kThreads, x, static_cast<const double *>(p), rt,
+             static_cast<const double *>(ap), z, static_cast<const double *>(map), n3, alpha);
+    launched++;
+    const double dnrm2 = dot_device(S, rt, rt);
+    const double resid_rec = std::sqrt(dnrm2 / bnrm2);
+    bool true_checked = false;
+    double resid_true = 0.0;
+    if (resid_rec <= tol || it % kCheckTrue == 0 || it == MAXIT) {
+      resid_into(wk);
+      resid_true = std::sqrt(dot_device(S, wk, wk) / bnrm2);
+      true_checked = true;
+    }
+    *resid = true_checked ? resid_true : resid_rec;
+    if (true_checked) {
+      if (resid_true <= tol) break;
+      if (it == MAXIT) {
+        *error = HECMW33_ERR_NOCONV_MAXIT;
+        break;
+      }
+    }
+    spmv(z, az);
+    const double rTAr = dot_device(S, z, az);
+    if (rTAr != rTAr) {
+      *error = HECMW33_ERR_DIVERGE_NAN;
+      break;
+    } else if (rTAr <= 0.0) {
+      *error = HECMW33_ERR_DIVERGE_MAT;
+      break;
+    }
+    const double beta = rTAr / rTAr_old;
+    rTAr_old = rTAr;
+    launch_k(s, cr_direction_kernel, S.grid_vec(), kThreads, p, static_cast<const double *>(z), ap,
+             static_cast<const double *>(az), n3, beta);
+    launched++;
+  }
+  *iter = MAXIT == 0 ? 0 : it;  // (:296; a completed DO loop would leave MAXIT+1)
+  H33_CUDA(cudaEventRecord(S.ev1, s));
+  S.sync();
+  float ms = 0.0f;
+  H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+  if (kernels) *kernels += launched;
+  return ms;
+}
+
 // The hecmw_solve / hecmw_solve_iterative sequence on resident B (S.b) and X (S.x),
 // FP64 throughout (the drop-in).
 int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times, int lowp = 0) {
@@ -1857,7 +1969,7 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   if (lowp && iterPREmax > 0) ensure_lowp(S);
   else lowp = 0;
   const bool record = S.L.recording && !learned && method == 1;
-  if (graph_mode() && !record && method != 3)
+  if (graph_mode() && !record && method != 3 && method != 7)
     build_graph<double>(S, iterPREmax, learned | (lowp ? 4 : 0) | (method == 2 ? 8 : 0));
   Range rs("hecmw33_solve");
   const double t1 = wall();
@@ -1868,6 +1980,8 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
     Iarray[81] = 0;
     if (method == 3) {
       ms_total += run_gmres(S, iterPREmax, TOL, MAXIT, Iarray[5], lowp, &kernels, &error, iter, resid);
+    } else if (method == 7) {
+      ms_total += run_cr(S, iterPREmax, TOL, MAXIT, lowp, &kernels, &error, iter, resid);
     } else {
       if (record) ms_total += record_cg(S, iterPREmax, TOL, MAXIT, &kernels);
       else ms_total += run_cg<double>(S, iterPREmax, TOL, MAXIT, &kernels, 0, learned, 0, 1e-4, lowp, method);
@@ -1886,9 +2000,9 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
         continue;
       } else if (method == 1 && METHOD2 > 1) {
         // Iterative.f90:138-142: a diverged CG hands over to METHOD2 from the current X
-        if (METHOD2 != 2 && METHOD2 != 3)
+        if (METHOD2 != 2 && METHOD2 != 3 && METHOD2 != 7)
           throw Failure(HECMW33_ERR_INCONS_PC, "METHOD2 " + std::to_string(METHOD2) +
-                                                   ": the GPU drop-in implements BiCGSTAB (2) and GMRES (3)");
+                                                   ": the GPU drop-in implements BiCGSTAB (2), GMRES (3) and CR (7)");
         if (auto_sigma) sigma = 1.0;
         method = METHOD2;
         learned = 0;

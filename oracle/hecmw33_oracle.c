@@ -9,6 +9,7 @@
  *   hecmw1/src/solver/iterative/hecmw_solver_CG.f90:19-320        (hecmw_solve_CG)
  *   hecmw1/src/solver/iterative/hecmw_solver_BiCGSTAB.f90:125-271 (hecmw_solve_BiCGSTAB)
  *   hecmw1/src/solver/iterative/hecmw_solver_GMRES.f90:93-411     (hecmw_solve_GMRES)
+ *   hecmw1/src/solver/iterative/hecmw_solver_CR.f90:108-296       (hecmw_solve_CR)
  *   hecmw1/src/solver/las/hecmw_solver_scaling_33.f90:20-208      (SCALING=YES)
  *   hecmw1/src/solver/las/hecmw_solver_las_33.F90:120-435         (matvec/matresid/rel_resid)
  *   hecmw1/src/solver/communication/hecmw_solver_misc.F90:46-201  (dot/axpy/xpay)
@@ -1023,6 +1024,103 @@ int o33_gmres(const o33_matrix *A, const o33_precond *P, int iterpremax, int max
   return error;
 }
 
+/* hecmw_solve_CR (hecmw_solver_CR.f90:108-296): preconditioned conjugate residual,
+ * recursive residual rt, true residual checked every 100th iteration, at
+ * RESID_REC <= TOL and at MAXIT. */
+int o33_cr(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol, const double *B,
+           double *X, int *iter_out, double *resid_out) {
+  const int NP = A->NP, NN = 3 * A->N;
+  const size_t len = 3 * (size_t)NP;
+  enum { NCHECK = 100 };
+  double *Z = (double *)calloc(len, sizeof(double)), *Pv = (double *)calloc(len, sizeof(double));
+  double *AP = (double *)calloc(len, sizeof(double)), *AZ = (double *)calloc(len, sizeof(double));
+  double *MAP = (double *)calloc(len, sizeof(double)), *RT = (double *)calloc(len, sizeof(double));
+  double *WK = (double *)calloc(len, sizeof(double));
+  int error = 0, iter = 0;
+  double RESID = 0.0, rTAr_old = 0.0;
+  o33_matresid(A, X, B, RT);
+  const double BNRM2 = o33_dot(NN, B, B);
+  if (BNRM2 == 0.0) {
+    maxit = 0;
+    for (size_t i = 0; i < len; i++) X[i] = 0.0;
+  } else {
+    const double DNRM2 = o33_dot(NN, RT, RT);
+    RESID = sqrt(DNRM2 / BNRM2);
+    if (RESID <= tol) {
+      maxit = 0;
+    } else {
+      o33_precond_apply(P, A, iterpremax, RT, Z, WK);
+      memcpy(Pv, Z, sizeof(double) * (size_t)NN);
+      o33_matvec(A, Z, AZ);
+      memcpy(AP, AZ, sizeof(double) * (size_t)NN);
+      rTAr_old = o33_dot(NN, Z, AZ);
+      if (rTAr_old != rTAr_old) {
+        error = ERR_DIVERGE_NAN;
+        maxit = 0;
+      } else if (rTAr_old <= 0.0) {
+        error = ERR_DIVERGE_MAT;
+        maxit = 0;
+      }
+    }
+  }
+  for (iter = 1; iter <= maxit; iter++) {
+    o33_precond_apply(P, A, iterpremax, AP, MAP, WK);
+    const double ApTAp = o33_dot(NN, AP, MAP);
+    if (ApTAp != ApTAp) {
+      error = ERR_DIVERGE_NAN;
+      break;
+    } else if (ApTAp <= 0.0) {
+      error = ERR_DIVERGE_PC;
+      break;
+    }
+    const double ALPHA = rTAr_old / ApTAp;
+    axpy(NN, ALPHA, Pv, X);
+    axpy(NN, -ALPHA, AP, RT);
+    axpy(NN, -ALPHA, MAP, Z);
+    const double DNRM2 = o33_dot(NN, RT, RT);
+    const double RESID_REC = sqrt(DNRM2 / BNRM2);
+    int true_checked = 0;
+    double RESID_TRUE = 0.0;
+    if (RESID_REC <= tol || iter % NCHECK == 0 || iter == maxit) {
+      o33_matresid(A, X, B, WK);
+      RESID_TRUE = sqrt(o33_dot(NN, WK, WK) / BNRM2);
+      true_checked = 1;
+    }
+    RESID = true_checked ? RESID_TRUE : RESID_REC;
+    if (true_checked) {
+      if (RESID_TRUE <= tol) break;
+      if (iter == maxit) {
+        error = ERR_NOCONV_MAXIT;
+        break;
+      }
+    }
+    o33_matvec(A, Z, AZ);
+    const double rTAr = o33_dot(NN, Z, AZ);
+    if (rTAr != rTAr) {
+      error = ERR_DIVERGE_NAN;
+      break;
+    } else if (rTAr <= 0.0) {
+      error = ERR_DIVERGE_MAT;
+      break;
+    }
+    const double BETA = rTAr / rTAr_old;
+    rTAr_old = rTAr;
+    xpay(NN, BETA, Z, Pv);
+    xpay(NN, BETA, AZ, AP);
+  }
+  if (maxit == 0) iter = 0;
+  *iter_out = iter;
+  *resid_out = RESID;
+  free(Z);
+  free(Pv);
+  free(AP);
+  free(AZ);
+  free(MAP);
+  free(RT);
+  free(WK);
+  return error;
+}
+
 double o33_cg_fixed_iters(const o33_matrix *A, const o33_precond *P, int iterpremax, int n,
                           const double *B, double *X) {
   const int NP = A->NP, NN = 3 * A->N;
@@ -1135,7 +1233,7 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
     for (int j = 0; j < 3; j++)
       if (fabs(A->D[9 * i + 4 * j]) == 0.0) zdiag = ERR_ZERO_DIAG;
   if (zdiag && PRECOND < 10 && iterPREmax > 0) return ERR_ZERO_DIAG;
-  if (METHOD < 1 || METHOD > 3) return ERR_INCONS_PC;
+  if (METHOD < 1 || (METHOD > 3 && METHOD != 7)) return ERR_INCONS_PC;
   recycle_precond_setting(Iarray);
 
   /* SCALING=YES (Iarray(7)): hecmw_solve_CG works on S A S, S B and multiplies X
@@ -1195,6 +1293,7 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
     }
     if (METHOD == 2) error = o33_bicgstab(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid);
     else if (METHOD == 3) error = o33_gmres(Aw, P, iterPREmax, MAXIT, TOL, Iarray[5], Bw, X, &iter, &resid);
+    else if (METHOD == 7) error = o33_cr(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid);
     else error = o33_cg(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid, NULL);
     if (!cache) o33_precond_free(P);
     if (SCALING) /* hecmw_solver_scaling_bk_33: X = S X (:144-147) */
@@ -1206,8 +1305,8 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
         continue;
       } else if (METHOD == 1 && METHOD2 > 1) { /* hecmw_solver_Iterative.f90:138-142 */
         if (auto_sigma_diag == 1) SIGMA_DIAG = 1.0;
-        if (METHOD2 != 2 && METHOD2 != 3) {
-          error = ERR_INCONS_PC; /* only BiCGSTAB and GMRES are restated here */
+        if (METHOD2 != 2 && METHOD2 != 3 && METHOD2 != 7) {
+          error = ERR_INCONS_PC; /* BiCGSTAB, GMRES and CR are restated here */
           break;
         }
         METHOD = METHOD2;
