@@ -37,6 +37,7 @@
 #include "h33_kernels.cuh"
 #include "h33_multi.cuh"
 #include "h33_setup.h"
+#include "h33_vecops.cuh"
 
 namespace h33 {
 
@@ -270,6 +271,7 @@ struct Solver {
   // GMRES(m): Krylov basis (m+1 vectors), w, zq, av; the small system (H, s, y, ss,
   // scalars) and the breakdown flag
   DevArray<double> g_V, g_w, g_zq, g_av, g_small;
+  DevArray<double> gp_W;  // GPBiCG: its twelve work vectors
   DevArray<int> g_flag;
   DevArray<int> blk_row, blk_col;
   DevArray<double> raw_scaled, scale, b_unscaled;
@@ -1701,10 +1703,10 @@ int prepare_solve(Solver &S, int *Iarray, double *Rarray, double *sigma, bool *a
   *auto_sigma = *sigma < 0.0;
   if (*auto_sigma) *sigma = 1.0;
   if (S.zero_diag && PRECOND < 10 && iterPREmax > 0) return HECMW33_ERR_ZERO_DIAG;
-  if (METHOD < 1 || (METHOD > 3 && METHOD != 7))
-    throw Failure(HECMW33_ERR_INCONS_PC,
-                  "METHOD " + std::to_string(METHOD) + ": the GPU drop-in implements CG (1), BiCGSTAB (2), GMRES (3) "
-                                                       "and CR (7)");
+  if (METHOD < 1 || METHOD == 5 || METHOD == 6 || METHOD > 7)
+    throw Failure(HECMW33_ERR_INCONS_PC, "METHOD " + std::to_string(METHOD) +
+                                             ": the GPU drop-in implements CG (1), BiCGSTAB (2), GMRES (3), "
+                                             "GPBiCG (4) and CR (7)");
   if (METHOD == 2 || Iarray[7] == 2 || METHOD == 7 || Iarray[7] == 7) ensure_bicg(S);
   recycle_precond_setting(Iarray);
   Range rg("hecmw33_precond_setup");
@@ -1946,6 +1948,140 @@ float run_cr(Solver &S, int iterpremax, double tol, int maxit, int lowp, int *ke
   return ms;
 }
 
+// hecmw_solve_GPBiCG (hecmw_solver_GPBiCG.f90:117-322, pol_coef_vanilla2 :458-506) on
+// the resident B and X in FP64, the vector operations in the reference's order.
+float run_gpbicg(Solver &S, int iterpremax, double tol, int maxit, int lowp, int *kernels, int *error, int *iter,
+                 double *resid) {
+  cudaStream_t s = S.stream;
+  const int n3 = S.n3();
+  constexpr int kRecompute = 20;  // N_ITER_RECOMPUTE_R
+  constexpr double kOmega = 0.707106781;
+  S.gp_W.alloc(size_t(12) * n3);
+  H33_CUDA(cudaMemsetAsync(S.gp_W.p, 0, sizeof(double) * 12 * size_t(n3), s));  // WW = 0
+  auto col = [&](int k) { return S.gp_W.p + size_t(k) * n3; };
+  double *R = S.r.p, *RT = col(0), *T = col(1), *TT = col(2), *T0 = col(3), *P = col(4), *PT = col(5);
+  double *U = col(6), *W1 = col(7), *Y = col(8), *Z = col(9), *WK = col(10), *W2 = col(11), *X = S.x.p;
+  const Views<double> V = views(S, 0.0, lowp);
+  int launched = 0;
+  const int gv = S.grid_vec();
+  auto axpy = [&](double a, const double *x, double *y) {
+    launch_k(s, vec_axpy_kernel, gv, kThreads, y, a, x, n3);
+    launched++;
+  };
+  auto xpay = [&](double a, const double *x, double *y) {
+    launch_k(s, vec_xpay_kernel, gv, kThreads, y, a, x, n3);
+    launched++;
+  };
+  auto axpyz = [&](double a, const double *x, const double *y, double *z) {
+    launch_k(s, vec_axpyz_kernel, gv, kThreads, z, a, x, y, n3);
+    launched++;
+  };
+  auto axpby = [&](double a, double b, const double *x, double *y) {
+    launch_k(s, vec_axpby_kernel, gv, kThreads, y, a, b, x, n3);
+    launched++;
+  };
+  auto copy = [&](const double *x, double *y) {
+    H33_CUDA(cudaMemcpyAsync(y, x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+  };
+  auto matvec = [&](const double *in, double *out) {
+    launch_k(s, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, V.A, in, out, static_cast<const double *>(nullptr),
+             static_cast<CgState *>(nullptr), static_cast<double *>(nullptr));
+    launched++;
+  };
+  auto matresid = [&](double *out) {
+    launch_k(s, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, V.A, static_cast<const double *>(X), out,
+             static_cast<const double *>(S.b.p), static_cast<CgState *>(nullptr), static_cast<double *>(nullptr));
+    launched++;
+  };
+  auto precond = [&](const double *in, double *out) { launch_precond_plain<double>(S, V, iterpremax, in, out, nullptr); };
+  auto dot = [&](const double *a, const double *b) { return dot_device(S, a, b); };
+  H33_CUDA(cudaEventRecord(S.ev0, s));
+  matresid(R);
+  copy(R, RT);
+  const double bnrm2 = dot(S.b.p, S.b.p);
+  double RHO = dot(RT, R), BETA = 0.0, ALPHA = 0.0, QSI = 0.0, ETA = 0.0;
+  *error = 0;
+  *resid = 0.0;
+  int it;
+  for (it = 1; it <= maxit; it++) {
+    copy(R, WK);  // {r} = M^-1 {r} (:169-170)
+    precond(WK, R);
+    if (it > 1) {  // {p} = {r} + BETA ({p} - {u}) (:179-184)
+      axpy(-1.0, U, P);
+      xpay(BETA, R, P);
+    } else {
+      copy(R, P);
+    }
+    matvec(P, PT);  // (:195)
+    const double RHO1 = dot(RT, PT);
+    ALPHA = RHO / RHO1;
+    axpyz(-1.0, W1, PT, Y);  // (:210-213)
+    xpay(ALPHA, T, Y);
+    axpy(-1.0, WK, Y);
+    axpyz(-ALPHA, PT, WK, T);
+    precond(T, TT);  // (:226-229)
+    precond(T0, W2);
+    copy(W2, T0);
+    precond(PT, W2);
+    matvec(TT, WK);  // (:235-236)
+    copy(WK, TT);
+    {  // pol_coef_vanilla2 (:458-506)
+      const double c1 = dot(T, T), c2 = dot(TT, TT), c3 = dot(T, TT);
+      double gamma1 = 0.0, gamma2 = 0.0;
+      if (it > 1) {
+        const double c4 = dot(Y, Y), c5 = dot(Y, TT), c6 = dot(Y, T);
+        gamma1 = c6 / c4;
+        gamma2 = c5 / c4;
+      }
+      const double c = c3 / std::sqrt(c1 * c2);
+      if (std::fabs(c) > kOmega) QSI = c * std::sqrt(c1 / c2);
+      else if (c >= 0.0) QSI = kOmega * std::sqrt(c1 / c2);
+      else QSI = -kOmega * std::sqrt(c1 / c2);
+      ETA = gamma1 - QSI * gamma2;
+    }
+    if (it > 1) {  // {u}, {z} (:260-273)
+      xpay(BETA, T0, U);
+      axpy(-1.0, R, U);
+      axpby(QSI, ETA, W2, U);
+      axpby(-ALPHA, ETA, U, Z);
+      axpy(QSI, R, Z);
+    } else {
+      axpyz(-1.0, R, T0, U);
+      axpby(QSI, ETA, W2, U);
+      axpby(-ALPHA, ETA, U, Z);
+      axpy(QSI, R, Z);
+    }
+    axpy(ALPHA, P, X);  // (:279-281)
+    axpy(1.0, Z, X);
+    copy(T, T0);
+    if (it % kRecompute == 0) {  // (:284-290)
+      matresid(R);
+    } else {
+      axpyz(-ETA, Y, T, R);
+      axpy(-QSI, TT, R);
+    }
+    const double DNRM2 = dot(R, R), COEF1 = dot(R, RT);
+    BETA = ALPHA * COEF1 / (QSI * RHO);
+    axpyz(BETA, PT, TT, W1);
+    *resid = std::sqrt(DNRM2 / bnrm2);
+    RHO = COEF1;
+    if (*resid <= tol) {  // (:311-319)
+      if (it % kRecompute == 0) break;
+      matresid(R);
+      *resid = std::sqrt(dot(R, R) / bnrm2);
+      if (*resid <= tol) break;
+    }
+    if (it == maxit) *error = HECMW33_ERR_NOCONV_MAXIT;
+  }
+  *iter = it;  // a completed DO loop leaves MAXIT+1
+  H33_CUDA(cudaEventRecord(S.ev1, s));
+  S.sync();
+  float ms = 0.0f;
+  H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+  if (kernels) *kernels += launched;
+  return ms;
+}
+
 // The hecmw_solve / hecmw_solve_iterative sequence on resident B (S.b) and X (S.x),
 // FP64 throughout (the drop-in).
 int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times, int lowp = 0) {
@@ -1969,7 +2105,7 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   if (lowp && iterPREmax > 0) ensure_lowp(S);
   else lowp = 0;
   const bool record = S.L.recording && !learned && method == 1;
-  if (graph_mode() && !record && method != 3 && method != 7)
+  if (graph_mode() && !record && (method == 1 || method == 2))
     build_graph<double>(S, iterPREmax, learned | (lowp ? 4 : 0) | (method == 2 ? 8 : 0));
   Range rs("hecmw33_solve");
   const double t1 = wall();
@@ -1982,6 +2118,8 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
       ms_total += run_gmres(S, iterPREmax, TOL, MAXIT, Iarray[5], lowp, &kernels, &error, iter, resid);
     } else if (method == 7) {
       ms_total += run_cr(S, iterPREmax, TOL, MAXIT, lowp, &kernels, &error, iter, resid);
+    } else if (method == 4) {
+      ms_total += run_gpbicg(S, iterPREmax, TOL, MAXIT, lowp, &kernels, &error, iter, resid);
     } else {
       if (record) ms_total += record_cg(S, iterPREmax, TOL, MAXIT, &kernels);
       else ms_total += run_cg<double>(S, iterPREmax, TOL, MAXIT, &kernels, 0, learned, 0, 1e-4, lowp, method);
@@ -2000,9 +2138,10 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
         continue;
       } else if (method == 1 && METHOD2 > 1) {
         // Iterative.f90:138-142: a diverged CG hands over to METHOD2 from the current X
-        if (METHOD2 != 2 && METHOD2 != 3 && METHOD2 != 7)
-          throw Failure(HECMW33_ERR_INCONS_PC, "METHOD2 " + std::to_string(METHOD2) +
-                                                   ": the GPU drop-in implements BiCGSTAB (2), GMRES (3) and CR (7)");
+        if (METHOD2 == 5 || METHOD2 == 6 || METHOD2 > 7)
+          throw Failure(HECMW33_ERR_INCONS_PC,
+                        "METHOD2 " + std::to_string(METHOD2) +
+                            ": the GPU drop-in implements BiCGSTAB (2), GMRES (3), GPBiCG (4) and CR (7)");
         if (auto_sigma) sigma = 1.0;
         method = METHOD2;
         learned = 0;

@@ -2,7 +2,8 @@
  * hecmw33_gpu.h -- C ABI of the B200 (sm_100a) 3x3-block CG solver, a drop-in for
  * FrontISTR's hecmw_solve on a hecmwST_matrix with NDOF = 3 and METHOD = 1 (CG),
  * 2 (BiCGSTAB, hecmw1/src/solver/iterative/hecmw_solver_BiCGSTAB.f90:16), 3 (GMRES,
- * hecmw1/src/solver/iterative/hecmw_solver_GMRES.f90) or 7 (CR,
+ * hecmw1/src/solver/iterative/hecmw_solver_GMRES.f90), 4 (GPBiCG,
+ * hecmw1/src/solver/iterative/hecmw_solver_GPBiCG.f90) or 7 (CR,
  * hecmw1/src/solver/iterative/hecmw_solver_CR.f90).
  *
  * Reference interfaces replaced (paths inside the FrontISTR tree):
@@ -103,7 +104,8 @@ HECMW33_API void hecmw33_gpu_set_matrix(const int *handle, const int *N, const i
  * zero-RHS check, zero-diagonal check, preconditioner recycle policy
  * (hecmw_matrix_misc.F90:858-877), preconditioner setup (PRECOND 1,2 = SSOR with the
  * reference's RCM + multicolour ordering, 3 = DIAG, 10 = block ILU(0)), CG (or
- * BiCGSTAB, GMRES(Iarray(6)), CR) to Rarray(1), the METHOD2 = 2, 3 or 7 fallback of a diverged CG
+ * BiCGSTAB, GMRES(Iarray(6)), GPBiCG, CR) to Rarray(1), the METHOD2 = 2, 3, 4 or 7 fallback of a
+ * diverged CG
  * (hecmw_solver_Iterative.f90:138-142), true relative residual, converged/diverged
  * flags Iarray(81)/(82).
  * B, X: host arrays of 3*NP (X: initial guess in, solution out).

@@ -10,6 +10,7 @@
  *   hecmw1/src/solver/iterative/hecmw_solver_BiCGSTAB.f90:125-271 (hecmw_solve_BiCGSTAB)
  *   hecmw1/src/solver/iterative/hecmw_solver_GMRES.f90:93-411     (hecmw_solve_GMRES)
  *   hecmw1/src/solver/iterative/hecmw_solver_CR.f90:108-296       (hecmw_solve_CR)
+ *   hecmw1/src/solver/iterative/hecmw_solver_GPBiCG.f90:117-506   (hecmw_solve_GPBiCG)
  *   hecmw1/src/solver/las/hecmw_solver_scaling_33.f90:20-208      (SCALING=YES)
  *   hecmw1/src/solver/las/hecmw_solver_las_33.F90:120-435         (matvec/matresid/rel_resid)
  *   hecmw1/src/solver/communication/hecmw_solver_misc.F90:46-201  (dot/axpy/xpay)
@@ -1121,6 +1122,116 @@ int o33_cr(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit,
   return error;
 }
 
+/* hecmw_axpyz_R: z = a x + y; hecmw_axpby_R: y = a x (b == 0) or a x + b y
+ * (hecmw_solver_misc.F90:208-291) */
+static void axpyz(int n, double a, const double *x, const double *y, double *z) {
+  for (int i = 0; i < n; i++) z[i] = a * x[i] + y[i];
+}
+static void axpby(int n, double a, double b, const double *x, double *y) {
+  if (b == 0.0)
+    for (int i = 0; i < n; i++) y[i] = a * x[i];
+  else
+    for (int i = 0; i < n; i++) y[i] = a * x[i] + b * y[i];
+}
+
+/* hecmw_solve_GPBiCG (hecmw_solver_GPBiCG.f90:117-322) with pol_coef_vanilla2
+ * (:458-506): true residual recomputed every 20th iteration and on convergence. */
+int o33_gpbicg(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol, const double *B,
+               double *X, int *iter_out, double *resid_out) {
+  const int NP = A->NP, NN = 3 * A->N;
+  const size_t len = 3 * (size_t)NP;
+  enum { NREC = 20 };
+  const double OMEGA = 0.707106781;
+  double *W = (double *)calloc(len * 14, sizeof(double));
+  double *R = W, *RT = W + len, *T = W + 2 * len, *TT = W + 3 * len, *T0 = W + 4 * len, *Pv = W + 5 * len;
+  double *PT = W + 6 * len, *U = W + 7 * len, *W1 = W + 8 * len, *Y = W + 9 * len, *Z = W + 10 * len;
+  double *WK = W + 11 * len, *W2 = W + 12 * len, *ZQ = W + 13 * len;
+  int error = 0, iter;
+  double RESID = 0.0, BETA = 0.0, ALPHA = 0.0, QSI = 0.0, ETA = 0.0;
+  o33_matresid(A, X, B, R);
+  memcpy(RT, R, sizeof(double) * (size_t)NN);
+  const double BNRM2 = o33_dot(NN, B, B);
+  if (BNRM2 == 0.0) {
+    maxit = 0;
+    for (size_t i = 0; i < len; i++) X[i] = 0.0;
+  }
+  double RHO = o33_dot(NN, RT, R);
+  for (iter = 1; iter <= maxit; iter++) {
+    memcpy(WK, R, sizeof(double) * (size_t)NN);
+    o33_precond_apply(P, A, iterpremax, WK, R, ZQ);
+    if (iter > 1) {
+      axpy(NN, -1.0, U, Pv);
+      xpay(NN, BETA, R, Pv);
+    } else {
+      memcpy(Pv, R, sizeof(double) * (size_t)NN);
+    }
+    o33_matvec(A, Pv, PT);
+    const double RHO1 = o33_dot(NN, RT, PT);
+    ALPHA = RHO / RHO1;
+    axpyz(NN, -1.0, W1, PT, Y);
+    xpay(NN, ALPHA, T, Y);
+    axpy(NN, -1.0, WK, Y);
+    axpyz(NN, -ALPHA, PT, WK, T);
+    o33_precond_apply(P, A, iterpremax, T, TT, ZQ);
+    o33_precond_apply(P, A, iterpremax, T0, W2, ZQ);
+    memcpy(T0, W2, sizeof(double) * (size_t)NN);
+    o33_precond_apply(P, A, iterpremax, PT, W2, ZQ);
+    o33_matvec(A, TT, WK);
+    memcpy(TT, WK, sizeof(double) * (size_t)NN);
+    {
+      const double c1 = o33_dot(NN, T, T), c2 = o33_dot(NN, TT, TT), c3 = o33_dot(NN, T, TT);
+      double gamma1 = 0.0, gamma2 = 0.0;
+      if (iter > 1) {
+        const double c4 = o33_dot(NN, Y, Y), c5 = o33_dot(NN, Y, TT), c6 = o33_dot(NN, Y, T);
+        gamma1 = c6 / c4;
+        gamma2 = c5 / c4;
+      }
+      const double c = c3 / sqrt(c1 * c2);
+      if (fabs(c) > OMEGA) QSI = c * sqrt(c1 / c2);
+      else if (c >= 0.0) QSI = OMEGA * sqrt(c1 / c2);
+      else QSI = -OMEGA * sqrt(c1 / c2);
+      ETA = gamma1 - QSI * gamma2;
+    }
+    if (iter > 1) {
+      xpay(NN, BETA, T0, U);
+      axpy(NN, -1.0, R, U);
+      axpby(NN, QSI, ETA, W2, U);
+      axpby(NN, -ALPHA, ETA, U, Z);
+      axpy(NN, QSI, R, Z);
+    } else {
+      axpyz(NN, -1.0, R, T0, U);
+      axpby(NN, QSI, ETA, W2, U);
+      axpby(NN, -ALPHA, ETA, U, Z);
+      axpy(NN, QSI, R, Z);
+    }
+    axpy(NN, ALPHA, Pv, X);
+    axpy(NN, 1.0, Z, X);
+    memcpy(T0, T, sizeof(double) * (size_t)NN);
+    if (iter % NREC == 0) {
+      o33_matresid(A, X, B, R);
+    } else {
+      axpyz(NN, -ETA, Y, T, R);
+      axpy(NN, -QSI, TT, R);
+    }
+    const double DNRM2 = o33_dot(NN, R, R), COEF1 = o33_dot(NN, R, RT);
+    BETA = ALPHA * COEF1 / (QSI * RHO);
+    axpyz(NN, BETA, PT, TT, W1);
+    RESID = sqrt(DNRM2 / BNRM2);
+    RHO = COEF1;
+    if (RESID <= tol) {
+      if (iter % NREC == 0) break;
+      o33_matresid(A, X, B, R);
+      RESID = sqrt(o33_dot(NN, R, R) / BNRM2);
+      if (RESID <= tol) break;
+    }
+    if (iter == maxit) error = ERR_NOCONV_MAXIT;
+  }
+  *iter_out = iter;
+  *resid_out = RESID;
+  free(W);
+  return error;
+}
+
 double o33_cg_fixed_iters(const o33_matrix *A, const o33_precond *P, int iterpremax, int n,
                           const double *B, double *X) {
   const int NP = A->NP, NN = 3 * A->N;
@@ -1233,7 +1344,7 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
     for (int j = 0; j < 3; j++)
       if (fabs(A->D[9 * i + 4 * j]) == 0.0) zdiag = ERR_ZERO_DIAG;
   if (zdiag && PRECOND < 10 && iterPREmax > 0) return ERR_ZERO_DIAG;
-  if (METHOD < 1 || (METHOD > 3 && METHOD != 7)) return ERR_INCONS_PC;
+  if (METHOD < 1 || METHOD == 5 || METHOD == 6 || METHOD > 7) return ERR_INCONS_PC;
   recycle_precond_setting(Iarray);
 
   /* SCALING=YES (Iarray(7)): hecmw_solve_CG works on S A S, S B and multiplies X
@@ -1294,6 +1405,7 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
     if (METHOD == 2) error = o33_bicgstab(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid);
     else if (METHOD == 3) error = o33_gmres(Aw, P, iterPREmax, MAXIT, TOL, Iarray[5], Bw, X, &iter, &resid);
     else if (METHOD == 7) error = o33_cr(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid);
+    else if (METHOD == 4) error = o33_gpbicg(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid);
     else error = o33_cg(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid, NULL);
     if (!cache) o33_precond_free(P);
     if (SCALING) /* hecmw_solver_scaling_bk_33: X = S X (:144-147) */
@@ -1305,8 +1417,8 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
         continue;
       } else if (METHOD == 1 && METHOD2 > 1) { /* hecmw_solver_Iterative.f90:138-142 */
         if (auto_sigma_diag == 1) SIGMA_DIAG = 1.0;
-        if (METHOD2 != 2 && METHOD2 != 3 && METHOD2 != 7) {
-          error = ERR_INCONS_PC; /* BiCGSTAB, GMRES and CR are restated here */
+        if (METHOD2 == 5 || METHOD2 == 6 || METHOD2 > 7) {
+          error = ERR_INCONS_PC; /* BiCGSTAB, GMRES, GPBiCG and CR are restated here */
           break;
         }
         METHOD = METHOD2;

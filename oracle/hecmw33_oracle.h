@@ -68,8 +68,8 @@ int o33_precond_ncolor(const o33_precond *P);
 void o33_precond_ordering(const o33_precond *P, int *colorindex, int *perm, int *iperm);
 
 /* ---- hecmw_solve (hecmw1/src/solver/main/hecmw_solver.f90:9-88) restricted to
- * METHOD=1 (CG), 2 (BiCGSTAB), 3 (GMRES) or 7 (CR), the last three also as the METHOD2
- * fallback of a diverged CG,
+ * METHOD=1 (CG), 2 (BiCGSTAB), 3 (GMRES), 4 (GPBiCG) or 7 (CR), the last four also as
+ * the METHOD2 fallback of a diverged CG,
  * PRECOND in {1,2,3,10}.  X holds x0 on entry and the solution on
  * return.  Iarray flags 81/82/96/97/98 are updated as the reference does.
  * Returns the solver error code (0, 2001, 2002, 3001..3004, 1001).  The
@@ -96,6 +96,10 @@ int o33_gmres(const o33_matrix *A, const o33_precond *P, int iterpremax, int max
 /* Conjugate residual iterations only (hecmw_solve_CR), given a ready preconditioner. */
 int o33_cr(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
            const double *B, double *X, int *iter_out, double *resid_out);
+
+/* GPBiCG iterations only (hecmw_solve_GPBiCG), given a ready preconditioner. */
+int o33_gpbicg(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
+               const double *B, double *X, int *iter_out, double *resid_out);
 
 /* run exactly n CG iterations (no convergence exit) and return elapsed seconds;
  * used for the bounded CPU-baseline sample. */
