@@ -272,6 +272,7 @@ struct Solver {
   // scalars) and the breakdown flag
   DevArray<double> g_V, g_w, g_zq, g_av, g_small;
   DevArray<double> gp_W;  // GPBiCG: its twelve work vectors
+  DevArray<double> gr_W;  // GMRESR / GMRESREN: u, c, uin, cin (xi, eta), BFGS pairs, vecR, tmp
   DevArray<int> g_flag;
   DevArray<int> blk_row, blk_col;
   DevArray<double> raw_scaled, scale, b_unscaled;
@@ -1703,10 +1704,8 @@ int prepare_solve(Solver &S, int *Iarray, double *Rarray, double *sigma, bool *a
   *auto_sigma = *sigma < 0.0;
   if (*auto_sigma) *sigma = 1.0;
   if (S.zero_diag && PRECOND < 10 && iterPREmax > 0) return HECMW33_ERR_ZERO_DIAG;
-  if (METHOD < 1 || METHOD == 5 || METHOD == 6 || METHOD > 7)
-    throw Failure(HECMW33_ERR_INCONS_PC, "METHOD " + std::to_string(METHOD) +
-                                             ": the GPU drop-in implements CG (1), BiCGSTAB (2), GMRES (3), "
-                                             "GPBiCG (4) and CR (7)");
+  if (METHOD < 1 || METHOD > 7)
+    throw Failure(HECMW33_ERR_INCONS_PC, "METHOD " + std::to_string(METHOD) + ": undefined (1-7)");
   if (METHOD == 2 || Iarray[7] == 2 || METHOD == 7 || Iarray[7] == 7) ensure_bicg(S);
   recycle_precond_setting(Iarray);
   Range rg("hecmw33_precond_setup");
@@ -2082,6 +2081,158 @@ float run_gpbicg(Solver &S, int iterpremax, double tol, int maxit, int lowp, int
   return ms;
 }
 
+// hecmw_solve_GMRESR (hecmw_solver_GMRESR.f90:158-232, with the NBFGS = Iarray(60)
+// quasi-Newton correction of the preconditioned direction) and hecmw_solve_GMRESREN
+// (hecmw_solver_GMRESREN.f90:136-207) on the resident B and X in FP64: truncated
+// GCR-type methods restarted after NREST steps, whose direction is the
+// preconditioned residual (GMRESR) or is built from the renormalised xi/eta pair
+// (GMRESREN).  GMRESREN's second orthogonalisation takes the coefficient left by the
+// previous step (the reference computes, then ignores, {c}{cin}); that is kept.
+float run_gmresr(Solver &S, int iterpremax, double tol, int maxit, int nrest, int nbfgs, bool ren, int lowp,
+                 int *kernels, int *error, int *iter, double *resid) {
+  cudaStream_t s = S.stream;
+  const int n3 = S.n3();
+  if (nrest < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "GMRESR needs NREST >= 1");
+  if (ren) nbfgs = 0;
+  if (nbfgs < 0) nbfgs = 0;
+  const int ncol = 4 * nrest + (ren ? 2 * nrest : 0) + 2 * nbfgs + 2;
+  S.gr_W.alloc(size_t(ncol) * n3);
+  H33_CUDA(cudaMemsetAsync(S.gr_W.p, 0, sizeof(double) * ncol * size_t(n3), s));
+  auto col = [&](int k) { return S.gr_W.p + size_t(k) * n3; };
+  // 1-based columns as in the reference
+  auto u = [&](int i) { return col(i - 1); };
+  auto c = [&](int i) { return col(nrest + i - 1); };
+  auto uin = [&](int i) { return col(2 * nrest + i - 1); };
+  auto cin = [&](int i) { return col(3 * nrest + i - 1); };
+  auto xi = [&](int i) { return col(4 * nrest + i - 1); };
+  auto eta = [&](int i) { return col(5 * nrest + i - 1); };
+  const int bf0 = 4 * nrest + (ren ? 2 * nrest : 0);
+  auto sB = [&](int i) { return col(bf0 + i - 1); };
+  auto yB = [&](int i) { return col(bf0 + nbfgs + i - 1); };
+  double *vecR = col(ncol - 2), *tmp = col(ncol - 1), *X = S.x.p;
+  const Views<double> V = views(S, 0.0, lowp);
+  int launched = 0;
+  const int gv = S.grid_vec();
+  auto axpy = [&](double a, const double *x, double *y) {
+    launch_k(s, vec_axpy_kernel, gv, kThreads, y, a, x, n3);
+    launched++;
+  };
+  auto xpay = [&](double a, const double *x, double *y) {
+    launch_k(s, vec_xpay_kernel, gv, kThreads, y, a, x, n3);
+    launched++;
+  };
+  auto axpyz = [&](double a, const double *x, const double *y, double *z) {
+    launch_k(s, vec_axpyz_kernel, gv, kThreads, z, a, x, y, n3);
+    launched++;
+  };
+  auto scal = [&](double a, const double *x, double *y) {  // hecmw_axpby_R(a, 0)
+    launch_k(s, vec_axpby_kernel, gv, kThreads, y, a, 0.0, x, n3);
+    launched++;
+  };
+  auto matvec = [&](const double *in, double *out) {
+    launch_k(s, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, V.A, in, out, static_cast<const double *>(nullptr),
+             static_cast<CgState *>(nullptr), static_cast<double *>(nullptr));
+    launched++;
+  };
+  auto precond = [&](const double *in, double *out) { launch_precond_plain<double>(S, V, iterpremax, in, out, nullptr); };
+  auto dot = [&](const double *a, const double *b) { return dot_device(S, a, b); };
+  H33_CUDA(cudaEventRecord(S.ev0, s));
+  const double bnrm2 = dot(S.b.p, S.b.p);
+  std::vector<int> idx(size_t(std::max(nbfgs, 1)));
+  for (int k = 0; k < nbfgs; k++) idx[size_t(k)] = k + 1;
+  std::vector<double> rho(size_t(std::max(nbfgs, 1))), alpha(size_t(std::max(nbfgs, 1)));
+  int ib = 0, it = 0;
+  double coef = 0.0;
+  *error = 0;
+  *resid = 0.0;
+  bool done = false;
+  while (!done) {  // OUTER
+    launch_k(s, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, V.A, static_cast<const double *>(X), vecR,
+             static_cast<const double *>(S.b.p), static_cast<CgState *>(nullptr), static_cast<double *>(nullptr));
+    launched++;
+    for (int I = 1; I <= nrest; I++) {
+      it++;
+      if (ren) {
+        precond(vecR, eta(1));
+        matvec(eta(1), xi(1));
+        xpay(-1.0, vecR, xi(1));
+        for (int o = 1; o <= I - 1; o++) {
+          const double a = dot(c(o), xi(o));
+          axpyz(-a, c(o), xi(o), xi(o + 1));
+          axpyz(a, u(o), eta(o), eta(o + 1));
+        }
+        precond(xi(I), uin(1));
+      } else if (ib == 0) {
+        precond(vecR, uin(1));
+      } else {
+        H33_CUDA(cudaMemcpyAsync(tmp, vecR, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+        for (int k = 1; k <= ib; k++) {
+          const int q = idx[size_t(k - 1)];
+          rho[size_t(k - 1)] = 1.0 / dot(sB(q), yB(q));
+          alpha[size_t(k - 1)] = rho[size_t(k - 1)] * dot(sB(q), tmp);
+          axpy(-alpha[size_t(k - 1)], yB(q), tmp);
+        }
+        precond(tmp, uin(1));
+        for (int k = ib; k >= 1; k--) {
+          const int q = idx[size_t(k - 1)];
+          const double coef2 = rho[size_t(k - 1)] * dot(yB(q), uin(1));
+          axpy(alpha[size_t(k - 1)] - coef2, sB(q), uin(1));
+        }
+      }
+      matvec(uin(1), cin(1));
+      for (int o = 1; o <= I - 1; o++) {
+        if (!ren) coef = dot(c(o), cin(o));
+        axpyz(-coef, c(o), cin(o), cin(o + 1));
+        axpyz(-coef, u(o), uin(o), uin(o + 1));
+      }
+      coef = 1.0 / std::sqrt(dot(cin(I), cin(I)));
+      scal(coef, cin(I), c(I));
+      scal(coef, uin(I), u(I));
+      if (ren) {
+        coef = dot(c(I), xi(I));
+        axpy(coef, u(I), X);
+        axpy(1.0, eta(I), X);
+        axpyz(-coef, c(I), xi(I), vecR);
+      } else {
+        coef = dot(c(I), vecR);
+        axpy(coef, u(I), X);
+        axpy(-coef, c(I), vecR);
+        if (nbfgs > 0) {
+          ib++;
+          if (ib == nbfgs + 1) {
+            const int t = idx[0];
+            for (int k = 0; k < nbfgs - 1; k++) idx[size_t(k)] = idx[size_t(k) + 1];
+            idx[size_t(nbfgs - 1)] = t;
+            ib--;
+          }
+          scal(coef, c(I), yB(idx[size_t(ib - 1)]));
+          scal(coef, u(I), sB(idx[size_t(ib - 1)]));
+        }
+      }
+      *resid = std::sqrt(dot(vecR, vecR) / bnrm2);
+      if (*resid <= tol) {
+        done = true;
+        break;
+      }
+      if (it > maxit) {
+        *error = HECMW33_ERR_NOCONV_MAXIT;
+        done = true;
+        break;
+      }
+    }
+  }
+  *iter = it;
+  // hecmw_precond_clear at the end of the solve: the next solve builds the
+  // preconditioner again
+  S.pc.valid = false;
+  H33_CUDA(cudaEventRecord(S.ev1, s));
+  S.sync();
+  float ms = 0.0f;
+  H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+  if (kernels) *kernels += launched;
+  return ms;
+}
+
 // The hecmw_solve / hecmw_solve_iterative sequence on resident B (S.b) and X (S.x),
 // FP64 throughout (the drop-in).
 int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times, int lowp = 0) {
@@ -2120,6 +2271,9 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
       ms_total += run_cr(S, iterPREmax, TOL, MAXIT, lowp, &kernels, &error, iter, resid);
     } else if (method == 4) {
       ms_total += run_gpbicg(S, iterPREmax, TOL, MAXIT, lowp, &kernels, &error, iter, resid);
+    } else if (method == 5 || method == 6) {
+      ms_total += run_gmresr(S, iterPREmax, TOL, MAXIT, Iarray[5], Iarray[59], method == 6, lowp, &kernels, &error,
+                             iter, resid);
     } else {
       if (record) ms_total += record_cg(S, iterPREmax, TOL, MAXIT, &kernels);
       else ms_total += run_cg<double>(S, iterPREmax, TOL, MAXIT, &kernels, 0, learned, 0, 1e-4, lowp, method);
@@ -2138,10 +2292,8 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
         continue;
       } else if (method == 1 && METHOD2 > 1) {
         // Iterative.f90:138-142: a diverged CG hands over to METHOD2 from the current X
-        if (METHOD2 == 5 || METHOD2 == 6 || METHOD2 > 7)
-          throw Failure(HECMW33_ERR_INCONS_PC,
-                        "METHOD2 " + std::to_string(METHOD2) +
-                            ": the GPU drop-in implements BiCGSTAB (2), GMRES (3), GPBiCG (4) and CR (7)");
+        if (METHOD2 > 7)
+          throw Failure(HECMW33_ERR_INCONS_PC, "METHOD2 " + std::to_string(METHOD2) + ": undefined (2-7)");
         if (auto_sigma) sigma = 1.0;
         method = METHOD2;
         learned = 0;

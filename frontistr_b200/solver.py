@@ -1,7 +1,7 @@
 """Host-side mirror of FrontISTR's solver interface on top of the CUDA C ABI.
 
 ``hecmw_solve(hecMAT)`` follows hecmw_solve (hecmw1/src/solver/main/hecmw_solver.f90:9-88)
-for METHOD=1: it updates hecMAT.X and the converged / diverged flags in
+for METHOD=1-7 (CG, BiCGSTAB, GMRES, GPBiCG, GMRESR, GMRESREN, CR): it updates hecMAT.X and the converged / diverged flags in
 hecMAT.Iarray(81)/(82), consumes the preconditioner flags 97/98 and returns the
 iteration record.  Error behaviour follows hecmw_solve_error
 (hecmw1/src/solver/init/hecmw_solve_error.f90:20-93): 1001 and 2001 abort the

@@ -3,7 +3,9 @@
  * FrontISTR's hecmw_solve on a hecmwST_matrix with NDOF = 3 and METHOD = 1 (CG),
  * 2 (BiCGSTAB, hecmw1/src/solver/iterative/hecmw_solver_BiCGSTAB.f90:16), 3 (GMRES,
  * hecmw1/src/solver/iterative/hecmw_solver_GMRES.f90), 4 (GPBiCG,
- * hecmw1/src/solver/iterative/hecmw_solver_GPBiCG.f90) or 7 (CR,
+ * hecmw1/src/solver/iterative/hecmw_solver_GPBiCG.f90), 5 (GMRESR with NBFGS = Iarray(60)
+ * quasi-Newton pairs, hecmw1/src/solver/iterative/hecmw_solver_GMRESR.f90), 6 (GMRESREN,
+ * hecmw1/src/solver/iterative/hecmw_solver_GMRESREN.f90) or 7 (CR,
  * hecmw1/src/solver/iterative/hecmw_solver_CR.f90).
  *
  * Reference interfaces replaced (paths inside the FrontISTR tree):
@@ -100,12 +102,13 @@ HECMW33_API void hecmw33_gpu_set_matrix(const int *handle, const int *N, const i
                                         const double *D, const double *AL, const double *AU,
                                         const int *Iarray, int *ierr);
 
-/* hecmw_solve (hecmw_solver.f90:9-88) for METHOD=1 or 2 on the resident matrix:
+/* hecmw_solve (hecmw_solver.f90:9-88) for METHOD = 1-7 on the resident matrix:
  * zero-RHS check, zero-diagonal check, preconditioner recycle policy
  * (hecmw_matrix_misc.F90:858-877), preconditioner setup (PRECOND 1,2 = SSOR with the
  * reference's RCM + multicolour ordering, 3 = DIAG, 10 = block ILU(0)), CG (or
- * BiCGSTAB, GMRES(Iarray(6)), GPBiCG, CR) to Rarray(1), the METHOD2 = 2, 3, 4 or 7 fallback of a
- * diverged CG
+ * BiCGSTAB, GMRES(Iarray(6)), GPBiCG, GMRESR, GMRESREN, CR) to Rarray(1), the METHOD2 = 2-7
+ * fallback of a diverged CG (GMRESR and GMRESREN clear the preconditioner when they return,
+ * as hecmw_precond_clear does, so the next solve sets it up again)
  * (hecmw_solver_Iterative.f90:138-142), true relative residual, converged/diverged
  * flags Iarray(81)/(82).
  * B, X: host arrays of 3*NP (X: initial guess in, solution out).

@@ -47,7 +47,10 @@ enum {
   ERR_DIVERGE_NAN = 3004,
   /* not a reference code: FORM_ILU0_33/ILU1a33 stop the program on a zero pivot
    * (hecmw_precond_BILU_33.f90:1510-1513); the oracle returns this instead. */
-  ERR_ILU_ZERO_PIVOT = 9001
+  ERR_ILU_ZERO_PIVOT = 9001,
+  /* not a reference code: GMRESR / GMRESREN with NREST < 1 never leave their outer
+   * loop in the reference (hecmw_solver_GMRESR.f90:158-160) */
+  ERR_BAD_INPUT = 9101
 };
 
 static double now_s(void) {
@@ -1232,6 +1235,118 @@ int o33_gpbicg(const o33_matrix *A, const o33_precond *P, int iterpremax, int ma
   return error;
 }
 
+/* hecmw_solve_GMRESR (hecmw_solver_GMRESR.f90:158-232) and, with ren != 0,
+ * hecmw_solve_GMRESREN (hecmw_solver_GMRESREN.f90:136-207).  GMRESR preconditions
+ * the residual, corrected by the last NBFGS quasi-Newton pairs (sBFGS, yBFGS), and
+ * orthogonalises A M^-1 r against the c vectors of the cycle; GMRESREN builds its
+ * direction from the xi/eta pair.  GMRESREN's second orthogonalisation uses the
+ * coefficient left by the previous step (the dot it computes there is unused), as
+ * the reference does.  BNRM2 = 0 is handled by the caller. */
+int o33_gmresr(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol, int nrest,
+               int nbfgs, int ren, const double *B, double *X, int *iter_out, double *resid_out) {
+  const int NP = A->NP, NN = 3 * A->N;
+  const size_t len = 3 * (size_t)NP;
+  if (nrest < 1) return ERR_BAD_INPUT;
+  if (ren || nbfgs < 0) nbfgs = 0;
+  const int ncol = 4 * nrest + (ren ? 2 * nrest : 0) + 2 * nbfgs + 3;
+  double *W = (double *)calloc(len * (size_t)ncol, sizeof(double));
+  double *u = W, *c = W + len * nrest, *uin = W + 2 * len * nrest, *cin = W + 3 * len * nrest;
+  double *xi = W + 4 * len * nrest, *eta = W + 5 * len * nrest; /* GMRESREN only */
+  double *sB = W + len * (size_t)(4 * nrest + (ren ? 2 * nrest : 0)), *yB = sB + len * (size_t)nbfgs;
+  double *vecR = yB + len * (size_t)nbfgs, *tmp = vecR + len, *ZP = tmp + len;
+#define COL(v, i) ((v) + len * (size_t)((i)-1))
+  int *idx = (int *)malloc(sizeof(int) * (size_t)(nbfgs + 1));
+  double *rho = (double *)malloc(sizeof(double) * (size_t)(nbfgs + 1));
+  double *alpha = (double *)malloc(sizeof(double) * (size_t)(nbfgs + 1));
+  for (int k = 0; k < nbfgs; k++) idx[k] = k + 1;
+  const double BNRM2 = o33_dot(NN, B, B);
+  int error = 0, iter = 0, ib = 0;
+  double RESID = 0.0, coef = 0.0;
+  for (;;) { /* OUTER */
+    int done = 0;
+    o33_matresid(A, X, B, vecR);
+    for (int I = 1; I <= nrest; I++) {
+      iter++;
+      if (ren) {
+        o33_precond_apply(P, A, iterpremax, vecR, COL(eta, 1), ZP);
+        o33_matvec(A, COL(eta, 1), COL(xi, 1));
+        xpay(NN, -1.0, vecR, COL(xi, 1));
+        for (int o = 1; o <= I - 1; o++) {
+          const double a = o33_dot(NN, COL(c, o), COL(xi, o));
+          axpyz(NN, -a, COL(c, o), COL(xi, o), COL(xi, o + 1));
+          axpyz(NN, a, COL(u, o), COL(eta, o), COL(eta, o + 1));
+        }
+        o33_precond_apply(P, A, iterpremax, COL(xi, I), COL(uin, 1), ZP);
+      } else if (ib == 0) {
+        o33_precond_apply(P, A, iterpremax, vecR, COL(uin, 1), ZP);
+      } else {
+        memcpy(tmp, vecR, sizeof(double) * (size_t)NN);
+        for (int k = 1; k <= ib; k++) {
+          const int q = idx[k - 1];
+          rho[k - 1] = 1.0 / o33_dot(NN, COL(sB, q), COL(yB, q));
+          alpha[k - 1] = rho[k - 1] * o33_dot(NN, COL(sB, q), tmp);
+          axpy(NN, -alpha[k - 1], COL(yB, q), tmp);
+        }
+        o33_precond_apply(P, A, iterpremax, tmp, COL(uin, 1), ZP);
+        for (int k = ib; k >= 1; k--) {
+          const int q = idx[k - 1];
+          const double coef2 = rho[k - 1] * o33_dot(NN, COL(yB, q), COL(uin, 1));
+          axpy(NN, alpha[k - 1] - coef2, COL(sB, q), COL(uin, 1));
+        }
+      }
+      o33_matvec(A, COL(uin, 1), COL(cin, 1));
+      for (int o = 1; o <= I - 1; o++) {
+        if (!ren) coef = o33_dot(NN, COL(c, o), COL(cin, o));
+        axpyz(NN, -coef, COL(c, o), COL(cin, o), COL(cin, o + 1));
+        axpyz(NN, -coef, COL(u, o), COL(uin, o), COL(uin, o + 1));
+      }
+      coef = 1.0 / sqrt(o33_dot(NN, COL(cin, I), COL(cin, I)));
+      axpby(NN, coef, 0.0, COL(cin, I), COL(c, I));
+      axpby(NN, coef, 0.0, COL(uin, I), COL(u, I));
+      if (ren) {
+        coef = o33_dot(NN, COL(c, I), COL(xi, I));
+        axpy(NN, coef, COL(u, I), X);
+        axpy(NN, 1.0, COL(eta, I), X);
+        axpyz(NN, -coef, COL(c, I), COL(xi, I), vecR);
+      } else {
+        coef = o33_dot(NN, COL(c, I), vecR);
+        axpy(NN, coef, COL(u, I), X);
+        axpy(NN, -coef, COL(c, I), vecR);
+        if (nbfgs > 0) {
+          ib++;
+          if (ib == nbfgs + 1) {
+            const int t = idx[0];
+            for (int k = 0; k < nbfgs - 1; k++) idx[k] = idx[k + 1];
+            idx[nbfgs - 1] = t;
+            ib--;
+          }
+          axpby(NN, coef, 0.0, COL(c, I), COL(yB, idx[ib - 1]));
+          axpby(NN, coef, 0.0, COL(u, I), COL(sB, idx[ib - 1]));
+        }
+      }
+      RESID = sqrt(o33_dot(NN, vecR, vecR) / BNRM2);
+      if (RESID <= tol) {
+        done = 1;
+        break;
+      }
+      if (iter > maxit) {
+        error = ERR_NOCONV_MAXIT;
+        done = 1;
+        break;
+      }
+    }
+    if (done) break;
+  }
+#undef COL
+  *iter_out = iter;
+  *resid_out = RESID;
+  free(W);
+  free(idx);
+  free(rho);
+  free(alpha);
+  return error;
+}
+
 double o33_cg_fixed_iters(const o33_matrix *A, const o33_precond *P, int iterpremax, int n,
                           const double *B, double *X) {
   const int NP = A->NP, NN = 3 * A->N;
@@ -1344,7 +1459,7 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
     for (int j = 0; j < 3; j++)
       if (fabs(A->D[9 * i + 4 * j]) == 0.0) zdiag = ERR_ZERO_DIAG;
   if (zdiag && PRECOND < 10 && iterPREmax > 0) return ERR_ZERO_DIAG;
-  if (METHOD < 1 || METHOD == 5 || METHOD == 6 || METHOD > 7) return ERR_INCONS_PC;
+  if (METHOD < 1 || METHOD > 7) return ERR_INCONS_PC;
   recycle_precond_setting(Iarray);
 
   /* SCALING=YES (Iarray(7)): hecmw_solve_CG works on S A S, S B and multiplies X
@@ -1406,8 +1521,14 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
     else if (METHOD == 3) error = o33_gmres(Aw, P, iterPREmax, MAXIT, TOL, Iarray[5], Bw, X, &iter, &resid);
     else if (METHOD == 7) error = o33_cr(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid);
     else if (METHOD == 4) error = o33_gpbicg(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid);
+    else if (METHOD == 5 || METHOD == 6)
+      error = o33_gmresr(Aw, P, iterPREmax, MAXIT, TOL, Iarray[5], Iarray[59], METHOD == 6, Bw, X, &iter, &resid);
     else error = o33_cg(Aw, P, iterPREmax, MAXIT, TOL, Bw, X, &iter, &resid, NULL);
     if (!cache) o33_precond_free(P);
+    else if (METHOD == 5 || METHOD == 6) { /* hecmw_precond_clear at the end of GMRESR / GMRESREN */
+      o33_precond_free(*cache);
+      *cache = NULL;
+    }
     if (SCALING) /* hecmw_solver_scaling_bk_33: X = S X (:144-147) */
       for (int i = 0; i < 3 * N; i++) X[i] = X[i] * scale[i];
     if (error == ERR_DIVERGE_PC || error == ERR_DIVERGE_MAT || error == ERR_DIVERGE_NAN) {
@@ -1417,8 +1538,8 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
         continue;
       } else if (METHOD == 1 && METHOD2 > 1) { /* hecmw_solver_Iterative.f90:138-142 */
         if (auto_sigma_diag == 1) SIGMA_DIAG = 1.0;
-        if (METHOD2 == 5 || METHOD2 == 6 || METHOD2 > 7) {
-          error = ERR_INCONS_PC; /* BiCGSTAB, GMRES, GPBiCG and CR are restated here */
+        if (METHOD2 > 7) {
+          error = ERR_INCONS_PC;
           break;
         }
         METHOD = METHOD2;

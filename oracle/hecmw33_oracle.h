@@ -101,6 +101,11 @@ int o33_cr(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit,
 int o33_gpbicg(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
                const double *B, double *X, int *iter_out, double *resid_out);
 
+/* GMRESR (ren = 0; nbfgs quasi-Newton pairs) or GMRESREN (ren = 1) iterations only
+ * (hecmw_solve_GMRESR / hecmw_solve_GMRESREN), given a ready preconditioner. */
+int o33_gmresr(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol, int nrest,
+               int nbfgs, int ren, const double *B, double *X, int *iter_out, double *resid_out);
+
 /* run exactly n CG iterations (no convergence exit) and return elapsed seconds;
  * used for the bounded CPU-baseline sample. */
 double o33_cg_fixed_iters(const o33_matrix *A, const o33_precond *P, int iterpremax,

@@ -189,9 +189,9 @@ def test_maxit(solver):
 
 
 def test_unsupported_method_is_fatal(solver):
-    """METHOD 3 (GMRES) is not built here: 1001, as the reference's undefined METHOD."""
+    """METHOD 8 is undefined (1-7 are): 1001, as the reference's hecmw_solve_iterative."""
     m = SYSTEMS["box_3x4x5"].copy()
-    m.set_method(3)
+    m.set_method(8)
     with pytest.raises(HecmwSolverError) as e:
         solver.solve(m)
     assert e.value.code == 1001
