@@ -4,11 +4,16 @@ import ctypes
 _i = ctypes.POINTER(ctypes.c_int)
 _d = ctypes.POINTER(ctypes.c_double)
 _v = ctypes.c_void_p
+# hecmw33_exchange_fn / hecmw33_allreduce_fn
+EXCHANGE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double))
+ALLREDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_void_p, ctypes.c_double)
 
 SIGNATURES = {
     "hecmw33_gpu_create": [_i, _i],
     "hecmw33_gpu_destroy": [_i, _i],
     "hecmw33_gpu_set_matrix": [_i, _i, _i, _i, _i, _i, _i, _i, _i, _d, _d, _d, _i, _i],
+    "hecmw33_gpu_set_domain": [_i, _i, _i, _i, _i, _i, _i, EXCHANGE_FN, ALLREDUCE_FN, _v, _i],
     "hecmw33_gpu_solve_resident": [_i, _d, _d, _i, _d, _i, _d, _d, _i],
     "hecmw33_gpu_solve_resident_device": [_i, _v, _v, _i, _d, _i, _d, _d, _i],
     "hecmw33_gpu_solve": [_i, _i, _i, _i, _i, _i, _i, _i, _i, _d, _d, _d, _d, _d, _i, _d, _i, _d,

@@ -19,11 +19,11 @@ namespace h33 {
 std::string check_profile(int N, int NP, int NPL, int NPU, const int *indexL, const int *itemL,
                           const int *indexU, const int *itemU) {
   if (N <= 0) return "N must be positive";
-  if (NP != N) return "NP != N: one GPU domain has no halo nodes";
+  if (NP < N) return "NP < N";
   if (!indexL || !indexU || (NPL > 0 && !itemL) || (NPU > 0 && !itemU)) return "null profile array";
-  if (indexL[0] != 0 || indexU[0] != 0 || indexL[N] != NPL || indexU[N] != NPU)
+  if (indexL[0] != 0 || indexU[0] != 0 || indexL[NP] != NPL || indexU[NP] != NPU)
     return "indexL/indexU inconsistent with NPL/NPU";
-  for (int i = 0; i < N; i++) {
+  for (int i = 0; i < NP; i++) {
     if (indexL[i + 1] < indexL[i] || indexU[i + 1] < indexU[i]) return "index arrays must be non-decreasing";
     int prev = 0;
     for (int j = indexL[i]; j < indexL[i + 1]; j++) {
@@ -34,7 +34,7 @@ std::string check_profile(int N, int NP, int NPL, int NPU, const int *indexL, co
     prev = i + 1;
     for (int j = indexU[i]; j < indexU[i + 1]; j++) {
       const int c = itemU[j];
-      if (c <= prev || c > N) return "itemU must be ascending ids in (row, N]";
+      if (c <= prev || c > NP) return "itemU must be ascending ids in (row, NP]";
       prev = c;
     }
   }

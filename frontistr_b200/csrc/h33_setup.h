@@ -8,8 +8,9 @@
 
 namespace h33 {
 
-// Checks an hecmwST profile for one GPU domain (N == NP, indexX[0..N] consistent with
-// NPL/NPU, itemL ascending ids below the row, itemU ascending ids above it, 1-based).
+// Checks an hecmwST profile of one domain (NP >= N rows, indexX[0..NP] consistent
+// with NPL/NPU, itemL ascending ids below the row, itemU ascending ids above it up to
+// NP, 1-based).
 // Returns "" or the first problem found.
 std::string check_profile(int N, int NP, int NPL, int NPU, const int *indexL, const int *itemL,
                           const int *indexU, const int *itemU);

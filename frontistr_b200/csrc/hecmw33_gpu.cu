@@ -32,6 +32,7 @@
 #include "h33_bicg.cuh"
 #include "h33_common.cuh"
 #include "h33_cr.cuh"
+#include "h33_domain.cuh"
 #include "h33_gmres.cuh"
 #include "h33_gnn.cuh"
 #include "h33_kernels.cuh"
@@ -235,6 +236,51 @@ struct GraphSlot {
   }
 };
 
+// One domain of a decomposed mesh (N internal of NP local nodes): the blocks of
+// internal rows at external columns, the communication table and the caller's
+// exchange / allreduce, the external values of X and of the CG direction, and the
+// host staging of the exchanged values.
+struct DomainState {
+  bool on = false;
+  int NP = 0, n_ext = 0, NPL = 0, NPU = 0;
+  // A_IE: interface rows (internal row, its blocks at external positions)
+  int n_irows = 0;
+  std::vector<int> au_src;  // per A_II upper block: its index in the caller's AU
+  std::vector<int> ie_src;  // per A_IE block: its index in the caller's AU
+  DevArray<int> irow, iptr, icol;
+  DevArray<double> ival;
+  // communication
+  bool has_table = false;
+  int n_exp = 0, n_imp = 0;
+  DevArray<int> exp_idx, imp_idx;
+  DevArray<double> send_d, recv_d, xe_x, xe_p;
+  double *send_h = nullptr, *recv_h = nullptr;
+  hecmw33_exchange_fn exchange = nullptr;
+  hecmw33_allreduce_fn allreduce = nullptr;
+  void *ctx = nullptr;
+  void free_host() {
+    if (send_h) cudaFreeHost(send_h);
+    if (recv_h) cudaFreeHost(recv_h);
+    send_h = recv_h = nullptr;
+  }
+  void clear_table() {
+    has_table = false;
+    n_exp = n_imp = 0;
+    exchange = nullptr;
+    allreduce = nullptr;
+    ctx = nullptr;
+    free_host();
+  }
+  void reset() {
+    clear_table();
+    on = false;
+    NP = n_ext = NPL = NPU = n_irows = 0;
+    au_src.clear();
+    ie_src.clear();
+  }
+  ~DomainState() { free_host(); }
+};
+
 struct Solver {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -273,6 +319,7 @@ struct Solver {
   DevArray<double> g_V, g_w, g_zq, g_av, g_small;
   DevArray<double> gp_W;  // GPBiCG: its twelve work vectors
   DevArray<double> gr_W;  // GMRESR / GMRESREN: u, c, uin, cin (xi, eta), BFGS pairs, vecR, tmp
+  DomainState dom;
   DevArray<int> g_flag;
   DevArray<int> blk_row, blk_col;
   DevArray<double> raw_scaled, scale, b_unscaled;
@@ -430,15 +477,101 @@ void set_profile(Solver &S, int N, int NPL, int NPU, const int *indexL, const in
   S.drop_graph();
 }
 
+void set_matrix_square(Solver &S, int N, int NPL, int NPU, const int *indexL, const int *itemL,
+                       const int *indexU, const int *itemU, const double *D, const double *AL, const double *AU,
+                       const int *Iarray);
+
+// A domain of a decomposed mesh (N < NP): the internal block A_II (rows and columns
+// 1..N) goes to the usual layouts, the internal rows' blocks at external columns to
+// the interface list; rows N+1..NP are not read by the solve.
+void set_matrix_domain(Solver &S, int N, int NP, int NPL, int NPU, const int *indexL, const int *itemL,
+                       const int *indexU, const int *itemU, const double *D, const double *AL, const double *AU,
+                       const int *Iarray) {
+  validate(N, NP, NPL, NPU, indexL, itemL, indexU, itemU);
+  DomainState &d = S.dom;
+  const bool same_nodes = d.on && d.NP == NP && S.has_matrix && S.N == N;  // the table stays valid
+  const bool symbolic = !d.on || d.NP != NP || d.NPL != NPL || d.NPU != NPU || !S.has_matrix || N != S.N ||
+                        Iarray == nullptr || Iarray[97] != 0;
+  std::vector<int> indexU2(size_t(N) + 1, 0), itemU2;
+  if (symbolic) {
+    d.au_src.clear();
+    d.ie_src.clear();
+    std::vector<int> irow, iptr{0}, icol;
+    for (int i = 0; i < N; i++) {
+      bool iface = false;
+      for (int j = indexU[i]; j < indexU[i + 1]; j++) {
+        const int c = itemU[j];
+        if (c <= N) {
+          itemU2.push_back(c);
+          d.au_src.push_back(j);
+        } else {
+          icol.push_back(c - N - 1);
+          d.ie_src.push_back(j);
+          iface = true;
+        }
+      }
+      indexU2[size_t(i) + 1] = int(itemU2.size());
+      if (iface) {
+        irow.push_back(i);
+        iptr.push_back(int(icol.size()));
+      }
+    }
+    d.n_irows = int(irow.size());
+    d.irow.upload(irow, S.stream);
+    d.iptr.upload(iptr, S.stream);
+    d.icol.upload(icol, S.stream);
+  } else {
+    for (int i = 0, k = 0; i < N; i++) {
+      for (int j = indexU[i]; j < indexU[i + 1]; j++)
+        if (itemU[j] <= N) itemU2.push_back(itemU[j]), k++;
+      indexU2[size_t(i) + 1] = k;
+    }
+  }
+  const int NPU2 = int(d.au_src.size());
+  std::vector<double> AU2(9 * size_t(std::max(NPU2, 1))), IE(9 * std::max<size_t>(d.ie_src.size(), 1));
+  for (int k = 0; k < NPU2; k++) std::memcpy(&AU2[9 * size_t(k)], AU + 9 * size_t(d.au_src[size_t(k)]), 9 * sizeof(double));
+  for (size_t k = 0; k < d.ie_src.size(); k++) std::memcpy(&IE[9 * k], AU + 9 * size_t(d.ie_src[k]), 9 * sizeof(double));
+  d.ival.upload(IE.data(), 9 * d.ie_src.size(), S.stream);
+  int *flags = nullptr;
+  std::vector<int> ia;
+  if (Iarray) {
+    ia.assign(Iarray, Iarray + 100);
+    if (symbolic) ia[97] = 1;  // the compact profile is new
+    flags = ia.data();
+  }
+  set_matrix_square(S, N, indexL[N], NPU2, indexL, itemL, indexU2.data(), itemU2.data(), D, AL, AU2.data(), flags);
+  d.on = true;
+  d.NP = NP;
+  d.NPL = NPL;
+  d.NPU = NPU;
+  d.n_ext = NP - N;
+  d.xe_x.alloc(3 * size_t(std::max(d.n_ext, 1)));
+  d.xe_p.alloc(3 * size_t(std::max(d.n_ext, 1)));
+  if (!same_nodes) d.clear_table();
+  S.sync();
+}
+
 void set_matrix(Solver &S, int N, int NP, int NPL, int NPU, const int *indexL, const int *itemL,
                 const int *indexU, const int *itemU, const double *D, const double *AL,
                 const double *AU, const int *Iarray) {
+  if (NP != N) {
+    set_matrix_domain(S, N, NP, NPL, NPU, indexL, itemL, indexU, itemU, D, AL, AU, Iarray);
+    return;
+  }
+  if (S.dom.on) {
+    S.dom.reset();
+    S.has_matrix = false;  // a new profile
+  }
+  validate(N, NP, NPL, NPU, indexL, itemL, indexU, itemU);
+  set_matrix_square(S, N, NPL, NPU, indexL, itemL, indexU, itemU, D, AL, AU, Iarray);
+}
+
+void set_matrix_square(Solver &S, int N, int NPL, int NPU, const int *indexL, const int *itemL,
+                       const int *indexU, const int *itemU, const double *D, const double *AL, const double *AU,
+                       const int *Iarray) {
   const bool symbolic = !S.has_matrix || N != S.N || NPL != S.NPL || NPU != S.NPU || Iarray == nullptr ||
                         Iarray[97] != 0;
-  if (symbolic) {
-    validate(N, NP, NPL, NPU, indexL, itemL, indexU, itemU);
-    set_profile(S, N, NPL, NPU, indexL, itemL, indexU, itemU);
-  }
+  if (symbolic) set_profile(S, N, NPL, NPU, indexL, itemL, indexU, itemU);
   const size_t nb = size_t(N) + NPL + NPU;
   S.raw.alloc(9 * nb);
   H33_CUDA(cudaMemcpyAsync(S.raw.p, D, sizeof(double) * 9 * N, cudaMemcpyHostToDevice, S.stream));
@@ -1603,6 +1736,10 @@ void assemble_hex8(Solver &S, int n_node, const double *coords, int n_elem, cons
                    const double *bc_value, bool symbolic, int *inverted = nullptr) {
   auto &M = S.asmb;
   if (n_node < 1 || n_elem < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "empty mesh");
+  if (S.dom.on) {  // the assembled mesh is one whole domain
+    S.dom.reset();
+    symbolic = true;
+  }
   if (!symbolic && (M.generation != S.generation || M.n_node != n_node || M.n_elem != n_elem))
     symbolic = true;
   if (symbolic) {
@@ -2810,7 +2947,224 @@ int solve_multi(Solver &S, int nrhs, const double *dB, double *dX, int *Iarray, 
   return rc;
 }
 
+// ---------------------------------------------------------------------------
+// A domain of a decomposed mesh: hecmw_update_R and hecmw_allreduce_R1 through the
+// caller's functions, CG (hecmw_solver_CG.f90:77-288) with the halo update before
+// every product and allreduced inner products.
+
+// hecmw_allreduce_R1 (hecmw_sum); a domain without a table sums over itself.
+double domain_allreduce(Solver &S, double v) {
+  const DomainState &d = S.dom;
+  return (d.has_table && d.allreduce) ? d.allreduce(d.ctx, v) : v;
+}
+
+// hecmw_update_R of the vector whose internal part is v (3N, device): its external
+// values land in xe (3 n_ext, device).  No neighbours: nothing changes
+// (hecmw_comm_f.F90:850).
+void halo_update(Solver &S, const double *v, double *xe) {
+  DomainState &d = S.dom;
+  if (!d.has_table || (d.n_exp == 0 && d.n_imp == 0)) return;
+  cudaStream_t s = S.stream;
+  const int gv = S.grid_vec();
+  if (d.n_exp) {
+    launch_k(s, halo_pack_kernel, gv, kThreads, v, static_cast<const int *>(d.exp_idx.p), d.n_exp, d.send_d.p);
+    H33_CUDA(cudaMemcpyAsync(d.send_h, d.send_d.p, sizeof(double) * 3 * d.n_exp, cudaMemcpyDeviceToHost, s));
+  }
+  S.sync();
+  d.exchange(d.ctx, d.send_h, d.recv_h);
+  if (d.n_imp) {
+    H33_CUDA(cudaMemcpyAsync(d.recv_d.p, d.recv_h, sizeof(double) * 3 * d.n_imp, cudaMemcpyHostToDevice, s));
+    launch_k(s, halo_unpack_kernel, gv, kThreads, static_cast<const double *>(d.recv_d.p),
+             static_cast<const int *>(d.imp_idx.p), d.n_imp, xe);
+  }
+}
+
+// y = A v over the internal rows: halo update of v into xe, the A_II product, then
+// the interface blocks (the reference's matvec order: external columns last).
+void domain_matvec(Solver &S, const double *v, double *xe, double *y, int *launched) {
+  halo_update(S, v, xe);
+  launch_k(S.stream, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, S.A.view(), v, y,
+           static_cast<const double *>(nullptr), static_cast<CgState *>(nullptr), static_cast<double *>(nullptr));
+  (*launched)++;
+  const DomainState &d = S.dom;
+  if (d.n_irows) {
+    launch_k(S.stream, interface_spmv_kernel, std::max(1, std::min((d.n_irows + kThreads - 1) / kThreads, S.nsm * 8)),
+             kThreads, static_cast<const int *>(d.irow.p), static_cast<const int *>(d.iptr.p),
+             static_cast<const int *>(d.icol.p), static_cast<const double *>(d.ival.p), d.n_irows,
+             static_cast<const double *>(xe), y);
+    (*launched)++;
+  }
+}
+
+// r = b - A x (hecmw_matresid_33, hecmw_solver_las_33.F90:367-399)
+void domain_matresid(Solver &S, const double *x, double *xe, const double *b, double *r, int *launched) {
+  domain_matvec(S, x, xe, r, launched);
+  launch_k(S.stream, vec_xpay_kernel, S.grid_vec(), kThreads, r, -1.0, b, S.n3());
+  (*launched)++;
+}
+
+double domain_dot(Solver &S, const double *a, const double *b) { return domain_allreduce(S, dot_device(S, a, b)); }
+
+// hecmw_solve_CG on one domain, host-driven (every inner product is a global sum).
+float run_cg_domain(Solver &S, int iterpremax, double tol, int maxit, int *error, int *iter, double *resid,
+                    int *kernels) {
+  cudaStream_t s = S.stream;
+  DomainState &d = S.dom;
+  const int n3 = S.n3(), gv = S.grid_vec();
+  const Views<double> V = views(S, 0.0, 0);
+  double *X = S.x.p, *R = S.r.p, *Z = S.z.p, *P = S.p.p, *Q = S.q.p;
+  const double *B = S.b.p;
+  int launched = 0;
+  H33_CUDA(cudaEventRecord(S.ev0, s));
+  d.xe_p.zero(s);  // the direction's external entries start at zero (WW is allocated zeroed)
+  domain_matresid(S, X, d.xe_x.p, B, R, &launched);
+  const double BNRM2 = domain_dot(S, B, B);
+  *error = 0;
+  *resid = 0.0;
+  if (BNRM2 == 0.0) {
+    maxit = 0;
+    H33_CUDA(cudaMemsetAsync(X, 0, sizeof(double) * n3, s));
+    d.xe_x.zero(s);
+  }
+  int n_indef = 0, it;
+  double RHO1 = 0.0;
+  for (it = 1; it <= maxit; it++) {
+    launch_precond_plain<double>(S, V, iterpremax, R, Z, nullptr);
+    launched += 2 * std::max(1, int(S.pc.lo.group_slice.size()));
+    const double RHO = domain_dot(S, R, Z);
+    if (RHO == 0.0) break;
+    else if (it > 1 && RHO * RHO1 <= 0) {
+      if (++n_indef >= 3) {
+        *error = HECMW33_ERR_DIVERGE_PC;
+        break;
+      }
+    } else if (RHO != RHO) {
+      *error = HECMW33_ERR_DIVERGE_NAN;
+      break;
+    }
+    if (it == 1) {
+      H33_CUDA(cudaMemcpyAsync(P, Z, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    } else {
+      launch_k(s, vec_xpay_kernel, gv, kThreads, P, RHO / RHO1, static_cast<const double *>(Z), n3);
+      launched++;
+    }
+    domain_matvec(S, P, d.xe_p.p, Q, &launched);
+    const double C1 = domain_dot(S, P, Q);
+    if (C1 <= 0) {
+      *error = HECMW33_ERR_DIVERGE_MAT;
+      break;
+    } else if (C1 != C1) {
+      *error = HECMW33_ERR_DIVERGE_NAN;
+      break;
+    }
+    const double ALPHA = RHO / C1;
+    launch_k(s, vec_axpy_kernel, gv, kThreads, X, ALPHA, static_cast<const double *>(P), n3);
+    launched++;
+    if (it % kIterRecomputeR == 0) {
+      domain_matresid(S, X, d.xe_x.p, B, R, &launched);
+    } else {
+      launch_k(s, vec_axpy_kernel, gv, kThreads, R, -ALPHA, static_cast<const double *>(Q), n3);
+      launched++;
+    }
+    double DNRM2 = domain_dot(S, R, R);
+    *resid = std::sqrt(DNRM2 / BNRM2);
+    if (*resid <= tol) {
+      if (it % kIterRecomputeR == 0) break;
+      domain_matresid(S, X, d.xe_x.p, B, R, &launched);
+      DNRM2 = domain_dot(S, R, R);
+      *resid = std::sqrt(DNRM2 / BNRM2);
+      if (*resid <= tol) break;
+    }
+    if (it == maxit) *error = HECMW33_ERR_NOCONV_MAXIT;
+    RHO1 = RHO;
+  }
+  halo_update(S, X, d.xe_x.p);  // hecmw_solver_CG.f90:288
+  *iter = it;
+  H33_CUDA(cudaEventRecord(S.ev1, s));
+  S.sync();
+  float ms = 0.0f;
+  H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+  if (kernels) *kernels += launched;
+  return ms;
+}
+
+// hecmw_solve -> hecmw_solve_iterative (METHOD = 1) on one domain: allreduced zero-RHS
+// and zero-diagonal checks (hecmw_solver_Iterative.f90:255-323), the recycle policy
+// and the local preconditioner, CG, the sigma_diag retry of a diverged ILU, and the
+// allreduced true residual.
+int solve_domain(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
+  const double t0 = wall();
+  *iter = 0;
+  *resid = 0.0;
+  if (times) times[0] = times[1] = times[2] = 0.0;
+  if (Iarray[1] != 1) throw Failure(HECMW33_ERR_BAD_INPUT, "a decomposed domain runs CG (METHOD = 1)");
+  if (Iarray[41] != 0 || Iarray[42] != 0)
+    throw Failure(HECMW33_ERR_BAD_INPUT, "a decomposed domain runs the FP64 CG (Iarray(42) = Iarray(43) = 0)");
+  if (Iarray[6] != 0) throw Failure(HECMW33_ERR_BAD_INPUT, "a decomposed domain runs with SCALING=NO");
+  if (Iarray[4] > 1) throw Failure(HECMW33_ERR_BAD_INPUT, "a decomposed domain runs with iterPREmax <= 1");
+  DomainState &d = S.dom;
+  const double bb = domain_allreduce(S, dot_device(S, S.b.p, S.b.p));
+  S.bnrm2 = bb;
+  if (bb == 0.0) {
+    H33_CUDA(cudaMemsetAsync(S.x.p, 0, sizeof(double) * S.n3(), S.stream));
+    d.xe_x.zero(S.stream);
+    S.sync();
+    Iarray[80] = 1;
+    Iarray[81] = 0;
+    return HECMW33_ERR_ZERO_RHS;
+  }
+  const int MAXIT = Iarray[0], PRECOND = Iarray[2], iterPREmax = Iarray[4];
+  const double TOL = Rarray[0];
+  double sigma = Rarray[1];
+  const bool auto_sigma = sigma < 0.0;
+  if (auto_sigma) sigma = 1.0;
+  if (domain_allreduce(S, S.zero_diag ? 1.0 : 0.0) > 0.0 && PRECOND < 10 && iterPREmax > 0)
+    return HECMW33_ERR_ZERO_DIAG;
+  recycle_precond_setting(Iarray);
+  const double t1 = wall();
+  int error = 0, kernels = 0;
+  float ms_total = 0.0f;
+  if (iterPREmax > 0) precond_setup(S, PRECOND, Iarray[33], sigma, Iarray);
+  Range rs("hecmw33_solve_domain");
+  for (;;) {
+    Iarray[80] = 0;
+    Iarray[81] = 0;
+    ms_total += run_cg_domain(S, iterPREmax, TOL, MAXIT, &error, iter, resid, &kernels);
+    if (error == HECMW33_ERR_DIVERGE_PC || error == HECMW33_ERR_DIVERGE_MAT || error == HECMW33_ERR_DIVERGE_NAN) {
+      Iarray[81] = 1;
+      // Iterative.f90:133-137: the retry's setup finds flags 97/98 cleared and keeps
+      // the factorisation; CG continues from the current X
+      if (PRECOND >= 10 && PRECOND < 20 && auto_sigma && sigma < 2.0) {
+        sigma = sigma + 0.1;
+        continue;
+      }
+    }
+    break;
+  }
+  // hecmw_rel_resid_L2_33 with the halo update inside matresid
+  int launched = 0;
+  domain_matresid(S, S.x.p, d.xe_x.p, S.b.p, S.w.p, &launched);
+  double bn = domain_dot(S, S.b.p, S.b.p);
+  if (bn == 0.0) bn = 1.0;
+  const double resid2 = std::sqrt(domain_dot(S, S.w.p, S.w.p) / bn);
+  if (resid2 < TOL) Iarray[80] = 1;
+  S.last_learned = 0;
+  S.last_fallback = 0;
+  S.last_iter = *iter;
+  S.last_outer = 1;
+  S.last_kernels = kernels + launched;
+  S.last_solve_s = ms_total * 1e-3;
+  S.last_setup_s = t1 - t0;
+  S.last_true_resid = resid2;
+  if (times) {
+    times[0] = t1 - t0;
+    times[1] = ms_total * 1e-3;
+  }
+  return error;
+}
+
 int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
+  if (S.dom.on) return solve_domain(S, Iarray, Rarray, iter, resid, times);
   if (Iarray[6] != 0 && (Iarray[41] == 2 || Iarray[41] == 3))
     throw Failure(HECMW33_ERR_BAD_INPUT, "SCALING=YES is implemented for the FP64 CG (Iarray(42) = 0 or 1)");
   if (Iarray[1] >= 2 && (Iarray[41] == 2 || Iarray[41] == 3))
@@ -2832,6 +3186,24 @@ namespace {
 void fail(int *ierr, int code, const char *msg) {
   g_last_error = msg;
   if (ierr) *ierr = code;
+}
+
+// The external part of X (entries 3N..3NP-1) of a decomposed domain, to or from the
+// handle's copy (in: before the solve; out: after it, or `out` for device-to-device).
+void halo_x(Solver &S, double *Xe, cudaMemcpyKind kind, bool out = false) {
+  DomainState &d = S.dom;
+  if (!d.on || d.n_ext == 0) return;
+  const size_t bytes = sizeof(double) * 3 * size_t(d.n_ext);
+  const bool to_dev = kind == cudaMemcpyHostToDevice || (kind == cudaMemcpyDeviceToDevice && !out);
+  if (to_dev) H33_CUDA(cudaMemcpyAsync(d.xe_x.p, Xe, bytes, kind, S.stream));
+  else H33_CUDA(cudaMemcpyAsync(Xe, d.xe_x.p, bytes, kind, S.stream));
+}
+void halo_x(Solver &S, const double *Xe, cudaMemcpyKind kind) {
+  halo_x(S, const_cast<double *>(Xe), kind, false);
+}
+
+void no_domain(const Solver &S, const char *what) {
+  if (S.dom.on) throw Failure(HECMW33_ERR_BAD_INPUT, std::string(what) + " is for a whole (one-domain) mesh");
 }
 
 }  // namespace
@@ -2896,6 +3268,58 @@ HECMW33_API void hecmw33_gpu_set_matrix(const int *handle, const int *N, const i
   H33_ENTRY_END
 }
 
+HECMW33_API void hecmw33_gpu_set_domain(const int *handle, const int *n_neighbor_pe, const int *neighbor_pe,
+                                        const int *import_index, const int *import_item,
+                                        const int *export_index, const int *export_item,
+                                        hecmw33_exchange_fn exchange, hecmw33_allreduce_fn allreduce,
+                                        void *ctx, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  if (!S.has_matrix || !S.dom.on)
+    throw Failure(HECMW33_ERR_NO_MATRIX, "set_domain: first a domain matrix (N < NP) by hecmw33_gpu_set_matrix");
+  DomainState &d = S.dom;
+  const int nn = n_neighbor_pe ? *n_neighbor_pe : 0;
+  if (nn < 0) throw Failure(HECMW33_ERR_BAD_INPUT, "n_neighbor_pe < 0");
+  if (nn > 0 && (!neighbor_pe || !import_index || !export_index || !exchange || !allreduce))
+    throw Failure(HECMW33_ERR_BAD_INPUT, "set_domain: null table or function");
+  const int n_imp = nn ? import_index[nn] : 0, n_exp = nn ? export_index[nn] : 0;
+  if (nn && (import_index[0] != 0 || export_index[0] != 0 || n_imp < 0 || n_exp < 0 ||
+             (n_imp && !import_item) || (n_exp && !export_item)))
+    throw Failure(HECMW33_ERR_BAD_INPUT, "set_domain: inconsistent import/export index");
+  for (int k = 0; k < nn; k++)
+    if (import_index[k + 1] < import_index[k] || export_index[k + 1] < export_index[k])
+      throw Failure(HECMW33_ERR_BAD_INPUT, "set_domain: index arrays must be non-decreasing");
+  const int N = S.N;
+  std::vector<int> imp(static_cast<size_t>(n_imp)), expt(static_cast<size_t>(n_exp));
+  for (int k = 0; k < n_imp; k++) {
+    const int it = import_item[k];
+    if (it <= N || it > d.NP) throw Failure(HECMW33_ERR_BAD_INPUT, "set_domain: import_item outside N+1..NP");
+    imp[size_t(k)] = it - N - 1;
+  }
+  for (int k = 0; k < n_exp; k++) {
+    const int it = export_item[k];
+    if (it < 1 || it > N) throw Failure(HECMW33_ERR_BAD_INPUT, "set_domain: export_item outside 1..N");
+    expt[size_t(k)] = it - 1;
+  }
+  d.clear_table();
+  d.n_imp = n_imp;
+  d.n_exp = n_exp;
+  d.imp_idx.upload(imp, S.stream);
+  d.exp_idx.upload(expt, S.stream);
+  d.send_d.alloc(3 * size_t(std::max(n_exp, 1)));
+  d.recv_d.alloc(3 * size_t(std::max(n_imp, 1)));
+  H33_CUDA(cudaMallocHost(&d.send_h, sizeof(double) * 3 * size_t(std::max(n_exp, 1))));
+  H33_CUDA(cudaMallocHost(&d.recv_h, sizeof(double) * 3 * size_t(std::max(n_imp, 1))));
+  d.exchange = exchange;
+  d.allreduce = allreduce;
+  d.ctx = ctx;
+  d.has_table = nn > 0;
+  S.sync();
+  H33_ENTRY_END
+}
+
 HECMW33_API void hecmw33_gpu_solve_resident(const int *handle, const double *B, double *X, int *Iarray,
                                             double *Rarray, int *iter, double *resid, double *times,
                                             int *ierr) {
@@ -2907,8 +3331,10 @@ HECMW33_API void hecmw33_gpu_solve_resident(const int *handle, const double *B, 
   const size_t bytes = sizeof(double) * S.n3();
   H33_CUDA(cudaMemcpyAsync(S.b.p, B, bytes, cudaMemcpyHostToDevice, S.stream));
   H33_CUDA(cudaMemcpyAsync(S.x.p, X, bytes, cudaMemcpyHostToDevice, S.stream));
+  halo_x(S, X + S.n3(), cudaMemcpyHostToDevice);
   const int rc = solve_resident(S, Iarray, Rarray, iter, resid, times);
   H33_CUDA(cudaMemcpyAsync(X, S.x.p, bytes, cudaMemcpyDeviceToHost, S.stream));
+  halo_x(S, X + S.n3(), cudaMemcpyDeviceToHost);
   S.sync();
   if (ierr) *ierr = rc;
   H33_ENTRY_END
@@ -2925,8 +3351,10 @@ HECMW33_API void hecmw33_gpu_solve_resident_device(const int *handle, const doub
   const size_t bytes = sizeof(double) * S.n3();
   H33_CUDA(cudaMemcpyAsync(S.b.p, dB, bytes, cudaMemcpyDeviceToDevice, S.stream));
   H33_CUDA(cudaMemcpyAsync(S.x.p, dX, bytes, cudaMemcpyDeviceToDevice, S.stream));
+  halo_x(S, dX + S.n3(), cudaMemcpyDeviceToDevice);
   const int rc = solve_resident(S, Iarray, Rarray, iter, resid, times);
   H33_CUDA(cudaMemcpyAsync(dX, S.x.p, bytes, cudaMemcpyDeviceToDevice, S.stream));
+  halo_x(S, dX + S.n3(), cudaMemcpyDeviceToDevice, true);
   S.sync();
   if (ierr) *ierr = rc;
   H33_ENTRY_END
@@ -2947,8 +3375,10 @@ HECMW33_API void hecmw33_gpu_solve(const int *handle, const int *N, const int *N
   const size_t bytes = sizeof(double) * S.n3();
   H33_CUDA(cudaMemcpyAsync(S.b.p, B, bytes, cudaMemcpyHostToDevice, S.stream));
   H33_CUDA(cudaMemcpyAsync(S.x.p, X, bytes, cudaMemcpyHostToDevice, S.stream));
+  halo_x(S, X + S.n3(), cudaMemcpyHostToDevice);
   const int rc = solve_resident(S, Iarray, Rarray, iter, resid, times);
   H33_CUDA(cudaMemcpyAsync(X, S.x.p, bytes, cudaMemcpyDeviceToHost, S.stream));
+  halo_x(S, X + S.n3(), cudaMemcpyDeviceToHost);
   S.sync();
   if (times) times[0] += tm;
   if (ierr) *ierr = rc;
@@ -2962,6 +3392,7 @@ HECMW33_API void hecmw33_gpu_solve_multi(const int *handle, const int *nrhs, con
   H33_ENTRY_BEGIN
   Solver &S = get(handle);
   DeviceGuard dg(S.device);
+  no_domain(S, "hecmw33_gpu_solve_multi");
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_set_matrix first");
   if (!nrhs || *nrhs < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "nrhs must be positive");
   const size_t total = size_t(S.n3()) * size_t(*nrhs);
@@ -2984,6 +3415,7 @@ HECMW33_API void hecmw33_gpu_solve_multi_device(const int *handle, const int *nr
   H33_ENTRY_BEGIN
   Solver &S = get(handle);
   DeviceGuard dg(S.device);
+  no_domain(S, "hecmw33_gpu_solve_multi_device");
   if (!nrhs || *nrhs < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "nrhs must be positive");
   std::vector<double> tr(static_cast<size_t>(*nrhs));
   const int rc = solve_multi(S, *nrhs, dB, dX, Iarray, Rarray, iter, resid, error, tr.data(), times);
@@ -2997,6 +3429,7 @@ HECMW33_API void hecmw33_gpu_matvec(const int *handle, const double *X, double *
   H33_ENTRY_BEGIN
   Solver &S = get(handle);
   DeviceGuard dg(S.device);
+  no_domain(S, "hecmw33_gpu_matvec");
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_set_matrix first");
   const size_t bytes = sizeof(double) * S.n3();
   H33_CUDA(cudaMemcpyAsync(S.w.p, X, bytes, cudaMemcpyHostToDevice, S.stream));
@@ -3014,6 +3447,7 @@ HECMW33_API void hecmw33_gpu_precond_apply(const int *handle, const double *R, d
   H33_ENTRY_BEGIN
   Solver &S = get(handle);
   DeviceGuard dg(S.device);
+  no_domain(S, "hecmw33_gpu_precond_apply");
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_set_matrix first");
   const int iterPREmax = Iarray[4];
   double sigma = Rarray[1];

@@ -86,6 +86,58 @@ class GpuSolver:
         self._check(err.value)
         self.N = m.N
 
+    def set_domain(self, comm, endpoint):
+        """The communication table (domain.CommTable) of the resident domain matrix
+        (N < NP) and its exchanges: endpoint.exchange(send) -> recv and
+        endpoint.allreduce(v) (domain.LocalExchange / TorchExchange), called by the C
+        solver at every hecmw_update_R / hecmw_allreduce_R1 (hecmw33_gpu_set_domain).
+        An exception inside them turns the exchanged values into NaN, so that the CG
+        stops at its next check; solve() then raises it."""
+        from ._abi import ALLREDUCE_FN, EXCHANGE_FN
+        n_send = 3 * int(comm.export_index[-1]) if comm.n_neighbor_pe else 0
+        n_recv = 3 * int(comm.import_index[-1]) if comm.n_neighbor_pe else 0
+        self._cb_error = None
+
+        def exchange(_ctx, sp, rp):
+            try:
+                if self._cb_error is not None:
+                    raise self._cb_error
+                send = np.ctypeslib.as_array(sp, shape=(n_send,)).copy() if n_send else np.zeros(0)
+                recv = np.asarray(endpoint.exchange(send), dtype=np.float64)
+                if n_recv:
+                    np.ctypeslib.as_array(rp, shape=(n_recv,))[:] = recv
+            except BaseException as e:  # noqa: BLE001 -- surfaced by solve()
+                self._cb_error = self._cb_error or e
+                if n_recv:
+                    np.ctypeslib.as_array(rp, shape=(n_recv,))[:] = np.nan
+
+        def allreduce(_ctx, v):
+            try:
+                if self._cb_error is not None:
+                    raise self._cb_error
+                return float(endpoint.allreduce(v))
+            except BaseException as e:  # noqa: BLE001
+                self._cb_error = self._cb_error or e
+                return float("nan")
+
+        self._domain_cbs = (EXCHANGE_FN(exchange), ALLREDUCE_FN(allreduce))
+        self._domain_arrays = (comm.neighbor_pe, comm.import_index, comm.import_item, comm.export_index,
+                               comm.export_item)
+        err = ctypes.c_int(0)
+        empty = np.zeros(1, np.int32)
+        self.lib.hecmw33_gpu_set_domain(
+            ctypes.byref(self.handle), _i(comm.n_neighbor_pe), _ip(comm.neighbor_pe), _ip(comm.import_index),
+            _ip(comm.import_item if comm.import_item.size else empty),
+            _ip(comm.export_index), _ip(comm.export_item if comm.export_item.size else empty),
+            self._domain_cbs[0], self._domain_cbs[1], None, ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+
+    def _raise_cb_error(self):
+        e = getattr(self, "_cb_error", None)
+        if e is not None:
+            self._cb_error = None
+            raise e
+
     def matvec(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.empty_like(x)
@@ -200,6 +252,7 @@ class GpuSolver:
             _dp(m.B), _dp(m.X), _ip(m.Iarray), _dp(m.Rarray), ctypes.byref(it), ctypes.byref(res),
             _dp(times), ctypes.byref(err))
         self.N = m.N
+        self._raise_cb_error()
         self._check(err.value)
         return self._record(err.value, it, res, times)
 
@@ -210,6 +263,7 @@ class GpuSolver:
         self.lib.hecmw33_gpu_solve_resident(ctypes.byref(self.handle), _dp(B), _dp(X), _ip(Iarray),
                                             _dp(Rarray), ctypes.byref(it), ctypes.byref(res), _dp(times),
                                             ctypes.byref(err))
+        self._raise_cb_error()
         self._check(err.value)
         return self._record(err.value, it, res, times)
 

@@ -29,7 +29,10 @@
  *     hecmw1/src/solver/matrix/hecmw_matrix_misc.F90:107-150.
  *   - Host pointers are borrowed for the duration of the call only.  Device buffers
  *     belong to the handle.  One host thread per handle; every call is synchronous.
- *   - One GPU domain: N == NP is required (no halo; hecmw_update_R is a no-op).
+ *   - One domain per handle.  N < NP is a domain of a decomposed mesh (internal nodes
+ *     1..N, external nodes N+1..NP): hecmw33_gpu_set_domain gives its communication
+ *     table and the caller's exchange / allreduce; such a domain runs CG (METHOD = 1)
+ *     in FP64 with iterPREmax <= 1 and SCALING=NO (9101 otherwise).
  *   - Iarray(7) = 1 (SCALING=YES, hecmw_solver_scaling_33.f90:20-208): the CG runs on
  *     S A S, S b with S = diag(1/sqrt|D_kk|) and X is multiplied by S after it; the
  *     caller's arrays are not written.  FP64 CG only (Iarray(42) = 0 or 1): 9101 for
@@ -79,10 +82,22 @@ extern "C" {
 /* codes of this library (no counterpart in the reference) */
 #define HECMW33_ERR_ILU_ZERO_PIVOT 9001 /* the reference stops the program here */
 #define HECMW33_ERR_CUDA 9100           /* CUDA runtime error; see hecmw33_gpu_last_error */
-#define HECMW33_ERR_BAD_INPUT 9101      /* inconsistent sizes, indices out of range, NP != N */
+#define HECMW33_ERR_BAD_INPUT 9101      /* inconsistent sizes, indices out of range, unsupported options */
 #define HECMW33_ERR_BAD_HANDLE 9102
 #define HECMW33_ERR_TIMEOUT 9103        /* a bounded device-side wait gave up */
 #define HECMW33_ERR_NO_MATRIX 9104      /* solve/matvec before set_matrix */
+
+/* The two communications of a decomposed domain, supplied by the caller (MPI through
+ * hecmw_solve_send_recv / hecmw_allreduce_R1 in FrontISTR; torch.distributed in the
+ * Python mirror).  Every domain calls them at the same points of the solve.
+ *   exchange: hecmw_update_R (hecmw1/src/solver/communication/hecmw_comm_f.F90:838-863)
+ *     -- send[] holds 3 values per export item (in export_item order, i.e. grouped by
+ *     neighbour as export_index says); the function sends each neighbour its part and
+ *     fills recv[] with 3 values per import item (import_item order).
+ *   allreduce: hecmw_allreduce_R1 with hecmw_sum (:494-528) -- the sum of value over
+ *     the domains (every domain must get the same bits). */
+typedef void (*hecmw33_exchange_fn)(void *ctx, const double *send, double *recv);
+typedef double (*hecmw33_allreduce_fn)(void *ctx, double value);
 
 /* Create a solver handle bound to the current CUDA device (its own stream).
  * Counterpart of the integer id table of hecmw1/src/solver/matrix/hecmw_mat_id.f90:21-72. */
@@ -101,6 +116,20 @@ HECMW33_API void hecmw33_gpu_set_matrix(const int *handle, const int *N, const i
                                         const int *itemL, const int *indexU, const int *itemU,
                                         const double *D, const double *AL, const double *AU,
                                         const int *Iarray, int *ierr);
+
+/* The communication table of the handle's domain (hecmwST_local_mesh:
+ * n_neighbor_pe, neighbor_pe, import_index(0:n), import_item, export_index(0:n),
+ * export_item; items are 1-based local node ids, imports in N+1..NP, exports in 1..N)
+ * and the caller's exchange / allreduce (ctx is passed back to them).  Call after
+ * hecmw33_gpu_set_matrix with N < NP; a domain without this call has no neighbours
+ * (hecmw_update_R returns at once, hecmw_solver_SR's n_neighbor_pe == 0) and sums
+ * over itself.  Replaces the hecMESH argument of hecmw_solve
+ * (hecmw1/src/solver/main/hecmw_solver.f90:9) for the communication it carries. */
+HECMW33_API void hecmw33_gpu_set_domain(const int *handle, const int *n_neighbor_pe, const int *neighbor_pe,
+                                        const int *import_index, const int *import_item,
+                                        const int *export_index, const int *export_item,
+                                        hecmw33_exchange_fn exchange, hecmw33_allreduce_fn allreduce,
+                                        void *ctx, int *ierr);
 
 /* hecmw_solve (hecmw_solver.f90:9-88) for METHOD = 1-7 on the resident matrix:
  * zero-RHS check, zero-diagonal check, preconditioner recycle policy

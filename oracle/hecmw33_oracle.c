@@ -49,7 +49,8 @@ enum {
    * (hecmw_precond_BILU_33.f90:1510-1513); the oracle returns this instead. */
   ERR_ILU_ZERO_PIVOT = 9001,
   /* not a reference code: GMRESR / GMRESREN with NREST < 1 never leave their outer
-   * loop in the reference (hecmw_solver_GMRESR.f90:158-160) */
+   * loop in the reference (hecmw_solver_GMRESR.f90:158-160); o33_solve_dd restates
+   * METHOD = 1 without SCALING only */
   ERR_BAD_INPUT = 9101
 };
 
@@ -1344,6 +1345,193 @@ int o33_gmresr(const o33_matrix *A, const o33_precond *P, int iterpremax, int ma
   free(idx);
   free(rho);
   free(alpha);
+  return error;
+}
+
+static void recycle_precond_setting(int *Iarray);
+
+/* ------------------------------------------------------------------------ */
+/* Domain decomposition: the CG path of one domain with hecmw_update_R and
+ * hecmw_allreduce_R1 where the reference calls them. */
+static double dd_dot(const o33_comm *c, int n, const double *x, const double *y) {
+  return c->allreduce(c->ctx, o33_dot(n, x, y)); /* hecmw_InnerProduct_R: hecmw_solver_misc.F90:46-76 */
+}
+static void dd_matvec(const o33_matrix *A, const o33_comm *c, double *X, double *Y) {
+  c->update(c->ctx, X); /* hecmw_solver_las_33.F90:231 */
+  o33_matvec(A, X, Y);
+}
+static void dd_matresid(const o33_matrix *A, const o33_comm *c, double *X, const double *B, double *R) {
+  dd_matvec(A, c, X, R);
+  const int n = 3 * A->N;
+  for (int i = 0; i < n; i++) R[i] = B[i] - R[i];
+}
+static void dd_precond_apply(const o33_precond *P, const o33_matrix *A, const o33_comm *c, int iterpremax,
+                             const double *R, double *Z, double *ZP) {
+  const int NN = 3 * A->N, NPN = 3 * A->NP;
+  if (iterpremax <= 0 || P == NULL) {
+    for (int i = 0; i < NN; i++) Z[i] = R[i];
+    return;
+  }
+  for (int i = 0; i < NN; i++) ZP[i] = R[i];
+  for (int i = NN; i < NPN; i++) ZP[i] = 0.0;
+  for (int i = 0; i < NPN; i++) Z[i] = 0.0;
+  for (int it = 1; it <= iterpremax; it++) {
+    o33_precond_sweep(P, ZP);
+    for (int i = 0; i < NN; i++) Z[i] = Z[i] + ZP[i];
+    if (it == iterpremax) break;
+    dd_matresid(A, c, Z, R, ZP); /* hecmw_precond.f90:166 */
+  }
+}
+
+int o33_cg_dd(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
+              const double *B, double *X, int *iter_out, double *resid_out, const o33_comm *comm) {
+  const int NP = A->NP, NN = 3 * A->N;
+  const size_t len = 3 * (size_t)NP;
+  double *R = (double *)calloc(len, sizeof(double));
+  double *Z = (double *)calloc(len, sizeof(double)); /* Z and Q share storage */
+  double *Pv = (double *)calloc(len, sizeof(double));
+  double *WK = (double *)calloc(len, sizeof(double));
+  int error = 0, n_indef_precond = 0, iter;
+  double RHO1 = 0.0, BETA = 0.0, RESID = 0.0;
+
+  dd_matresid(A, comm, X, B, R);
+  const double BNRM2 = dd_dot(comm, NN, B, B);
+  if (BNRM2 == 0.0) {
+    maxit = 0;
+    RESID = 0.0;
+    for (size_t i = 0; i < len; i++) X[i] = 0.0;
+  }
+  for (iter = 1; iter <= maxit; iter++) {
+    dd_precond_apply(P, A, comm, iterpremax, R, Z, WK);
+    const double RHO = dd_dot(comm, NN, R, Z);
+    if (RHO == 0.0) break;
+    else if (iter > 1 && RHO * RHO1 <= 0) {
+      n_indef_precond++;
+      if (n_indef_precond >= 3) {
+        error = ERR_DIVERGE_PC;
+        break;
+      }
+    } else if (RHO != RHO) {
+      error = ERR_DIVERGE_NAN;
+      break;
+    }
+    if (iter == 1) memcpy(Pv, Z, sizeof(double) * (size_t)NN);
+    else {
+      BETA = RHO / RHO1;
+      xpay(NN, BETA, Z, Pv);
+    }
+    dd_matvec(A, comm, Pv, Z);
+    const double C1 = dd_dot(comm, NN, Pv, Z);
+    if (C1 <= 0) {
+      error = ERR_DIVERGE_MAT;
+      break;
+    } else if (C1 != C1) {
+      error = ERR_DIVERGE_NAN;
+      break;
+    }
+    const double ALPHA = RHO / C1;
+    axpy(NN, ALPHA, Pv, X);
+    if (iter % N_ITER_RECOMPUTE_R == 0) dd_matresid(A, comm, X, B, R);
+    else axpy(NN, -ALPHA, Z, R);
+    double DNRM2 = dd_dot(comm, NN, R, R);
+    RESID = sqrt(DNRM2 / BNRM2);
+    if (RESID <= tol) {
+      if (iter % N_ITER_RECOMPUTE_R == 0) break;
+      dd_matresid(A, comm, X, B, R);
+      DNRM2 = dd_dot(comm, NN, R, R);
+      RESID = sqrt(DNRM2 / BNRM2);
+      if (RESID <= tol) break;
+    }
+    if (iter == maxit) error = ERR_NOCONV_MAXIT;
+    RHO1 = RHO;
+  }
+  comm->update(comm->ctx, X); /* hecmw_solver_CG.f90:288 */
+  *iter_out = iter;
+  *resid_out = RESID;
+  free(R);
+  free(Z);
+  free(Pv);
+  free(WK);
+  return error;
+}
+
+int o33_solve_dd(const o33_matrix *A, const double *B, double *X, int *Iarray, double *Rarray,
+                 const o33_comm *comm, int *iter_out, double *resid_out, double *resid_true_out) {
+  const int N = A->N, NP = A->NP;
+  *iter_out = 0;
+  *resid_out = 0.0;
+  *resid_true_out = 0.0;
+  if (Iarray[1] != 1 || Iarray[6] != 0) return ERR_BAD_INPUT;
+  /* hecmw_solve_check_zerorhs (hecmw_solver_Iterative.f90:284-323) */
+  double rhs = 0.0;
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < 3; j++) rhs = rhs + B[3 * i + j] * B[3 * i + j];
+  rhs = comm->allreduce(comm->ctx, rhs);
+  if (rhs == 0.0) {
+    for (size_t i = 0; i < 3 * (size_t)NP; i++) X[i] = 0.0;
+    Iarray[80] = 1;
+    Iarray[81] = 0;
+    return ERR_ZERO_RHS;
+  }
+  const int PRECOND = Iarray[2], iterPREmax = Iarray[4], MAXIT = Iarray[0], NCOLOR_IN = Iarray[33];
+  const double TOL = Rarray[0];
+  double SIGMA_DIAG = Rarray[1];
+  int auto_sigma_diag = 0;
+  if (SIGMA_DIAG < 0.0) {
+    auto_sigma_diag = 1;
+    SIGMA_DIAG = 1.0;
+  }
+  /* hecmw_solve_check_zerodiag (:255-282), the error allreduced with hecmw_max */
+  double zdiag = 0.0;
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < 3; j++)
+      if (fabs(A->D[9 * i + 4 * j]) == 0.0) zdiag = 1.0;
+  if (comm->allreduce(comm->ctx, zdiag) > 0.0 && PRECOND < 10 && iterPREmax > 0) return ERR_ZERO_DIAG;
+  recycle_precond_setting(Iarray);
+  int error = 0, iter = 0;
+  double resid = 0.0;
+  o33_precond *P = NULL;
+  if (iterPREmax > 0) {
+    int perr = 0;
+    P = o33_precond_setup(A, PRECOND, NCOLOR_IN, SIGMA_DIAG, 1, &perr);
+    if (perr) {
+      o33_precond_free(P);
+      return perr;
+    }
+    Iarray[97] = 0;
+    Iarray[96] = 0;
+  }
+  for (;;) {
+    Iarray[80] = 0;
+    Iarray[81] = 0;
+    error = o33_cg_dd(A, P, iterPREmax, MAXIT, TOL, B, X, &iter, &resid, comm);
+    if (error == ERR_DIVERGE_PC || error == ERR_DIVERGE_MAT || error == ERR_DIVERGE_NAN) {
+      Iarray[81] = 1;
+      /* hecmw_solver_Iterative.f90:133-137; the setup inside the next CG finds flags
+       * 97/98 cleared and keeps the factorisation */
+      if (PRECOND >= 10 && PRECOND < 20 && auto_sigma_diag == 1 && SIGMA_DIAG < 2.0) {
+        SIGMA_DIAG = SIGMA_DIAG + 0.1;
+        continue;
+      }
+    }
+    break;
+  }
+  o33_precond_free(P);
+  /* hecmw_rel_resid_L2_33 (hecmw_solver_las_33.F90:406-435) with the halo update of
+   * X inside matresid and the inner products allreduced */
+  {
+    const int n = 3 * N;
+    double *r = (double *)calloc(3 * (size_t)NP, sizeof(double));
+    double bnorm2 = dd_dot(comm, n, B, B);
+    if (bnorm2 == 0.0) bnorm2 = 1.0;
+    dd_matresid(A, comm, X, B, r);
+    const double rnorm2 = dd_dot(comm, n, r, r);
+    free(r);
+    *resid_true_out = sqrt(rnorm2 / bnorm2);
+  }
+  if (*resid_true_out < TOL) Iarray[80] = 1;
+  *iter_out = iter;
+  *resid_out = resid;
   return error;
 }
 

@@ -106,6 +106,32 @@ int o33_gpbicg(const o33_matrix *A, const o33_precond *P, int iterpremax, int ma
 int o33_gmresr(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol, int nrest,
                int nbfgs, int ren, const double *B, double *X, int *iter_out, double *resid_out);
 
+/* ---- domain decomposition (hecmw1/src/solver/communication) ----
+ * One domain of an overlapping node-based decomposition: rows 0..N-1 are its
+ * internal nodes, N..NP-1 the external (halo) nodes owned by neighbours.
+ * update: hecmw_update_R (hecmw_comm_f.F90:838-863) -- fills the external entries
+ *   3N..3NP-1 of a 3NP vector from their owners, in place;
+ * allreduce: hecmw_allreduce_R1 with hecmw_sum (:494-528) -- the sum of v over the
+ *   domains.  Both are called by every domain at the same points. */
+typedef struct {
+  void *ctx;
+  void (*update)(void *ctx, double *x);
+  double (*allreduce)(void *ctx, double v);
+} o33_comm;
+
+/* hecmw_solve_CG on one domain: matvec / matresid after hecmw_update_R of their
+ * input, inner products over the internal entries and allreduced, the final update
+ * of X (hecmw_solver_CG.f90:77-288, hecmw_solver_las_33.F90:231). */
+int o33_cg_dd(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
+              const double *B, double *X, int *iter_out, double *resid_out, const o33_comm *comm);
+
+/* hecmw_solve -> hecmw_solve_iterative for METHOD = 1 on one domain: allreduced
+ * zero-RHS and zero-diagonal checks, a new local preconditioner (kind as o33_solve;
+ * only internal rows, as the reference's), CG, the sigma_diag retry of a diverged
+ * ILU, the allreduced true residual and the flags.  Other METHODs: 9101. */
+int o33_solve_dd(const o33_matrix *A, const double *B, double *X, int *Iarray, double *Rarray,
+                 const o33_comm *comm, int *iter_out, double *resid_out, double *resid_true_out);
+
 /* run exactly n CG iterations (no convergence exit) and return elapsed seconds;
  * used for the bounded CPU-baseline sample. */
 double o33_cg_fixed_iters(const o33_matrix *A, const o33_precond *P, int iterpremax,

@@ -23,6 +23,14 @@ class O33Matrix(ctypes.Structure):
                 ("itemU", _i32p), ("D", _f64p), ("AL", _f64p), ("AU", _f64p)]
 
 
+UPDATE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, _f64p)
+ALLREDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_void_p, ctypes.c_double)
+
+
+class O33Comm(ctypes.Structure):
+    _fields_ = [("ctx", ctypes.c_void_p), ("update", UPDATE_FN), ("allreduce", ALLREDUCE_FN)]
+
+
 _lib = None
 
 
@@ -66,6 +74,9 @@ def lib():
                                          ctypes.c_int, _f64p, _f64p]
         L.o33_cg_fixed_iters.restype = ctypes.c_double
         L.o33_max_threads.restype = ctypes.c_int
+        L.o33_solve_dd.argtypes = [ctypes.POINTER(O33Matrix), _f64p, _f64p, _i32p, _f64p,
+                                   ctypes.POINTER(O33Comm), _i32p, _f64p, _f64p]
+        L.o33_solve_dd.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -175,3 +186,59 @@ class OraclePrecond:
         if hist:
             out["hist"] = h[:it.value]
         return out
+
+
+def solve_dd(domain, endpoint, Iarray=None, Rarray=None):
+    """o33_solve_dd on one domain; `endpoint` supplies exchange(send) -> recv and
+    allreduce(v) (frontistr_b200.domain).  Every domain of the decomposition must
+    call this at the same time (threads or processes)."""
+    m, c = domain.matrix, domain.comm
+    L = lib()
+    mat = O33Matrix(m.N, m.NP, m.NPL, m.NPU, _ip(m.indexL), _ip(m.itemL), _ip(m.indexU),
+                    _ip(m.itemU), _dp(m.D), _dp(m.AL), _dp(m.AU))
+    n3p = 3 * m.NP
+
+    def update(_ctx, xp):
+        x = np.ctypeslib.as_array(xp, shape=(n3p,))
+        c.unpack(x, endpoint.exchange(c.pack(x)))
+
+    def allreduce(_ctx, v):
+        return endpoint.allreduce(v)
+
+    cb_u, cb_a = UPDATE_FN(update), ALLREDUCE_FN(allreduce)
+    comm = O33Comm(None, cb_u, cb_a)
+    B = np.ascontiguousarray(m.B, dtype=np.float64)
+    X = np.zeros(n3p)
+    Ia = (m.Iarray if Iarray is None else Iarray).astype(np.int32).copy()
+    Ra = (m.Rarray if Rarray is None else Rarray).astype(np.float64).copy()
+    it = ctypes.c_int(0)
+    res = ctypes.c_double(0)
+    rtrue = ctypes.c_double(0)
+    err = L.o33_solve_dd(ctypes.byref(mat), _dp(B), _dp(X), _ip(Ia), _dp(Ra), ctypes.byref(comm),
+                         ctypes.byref(it), ctypes.byref(res), ctypes.byref(rtrue))
+    return dict(X=X, error=err, iter=it.value, resid=res.value, resid_true=rtrue.value, Iarray=Ia)
+
+
+def solve_dd_threads(domains, Iarray=None, Rarray=None):
+    """o33_solve_dd on every domain, one thread each, exchanging in process."""
+    import threading
+    from frontistr_b200.domain import LocalExchange
+    ex = LocalExchange(domains)
+    out = [None] * len(domains)
+    errs = []
+
+    def run(k):
+        try:
+            out[k] = solve_dd(domains[k], ex.endpoint(k), Iarray, Rarray)
+        except BaseException as e:  # surfaced below
+            errs.append(e)
+            ex.barrier.abort()
+
+    ts = [threading.Thread(target=run, args=(k,)) for k in range(len(domains))]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    if errs:
+        raise errs[0]
+    return out
