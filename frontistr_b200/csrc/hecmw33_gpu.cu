@@ -253,7 +253,7 @@ struct DomainState {
   bool has_table = false;
   int n_exp = 0, n_imp = 0;
   DevArray<int> exp_idx, imp_idx;
-  DevArray<double> send_d, recv_d, xe_x, xe_p;
+  DevArray<double> send_d, recv_d, xe_x, xe_p, xe_z;
   double *send_h = nullptr, *recv_h = nullptr;
   hecmw33_exchange_fn exchange = nullptr;
   hecmw33_allreduce_fn allreduce = nullptr;
@@ -547,6 +547,7 @@ void set_matrix_domain(Solver &S, int N, int NP, int NPL, int NPU, const int *in
   d.n_ext = NP - N;
   d.xe_x.alloc(3 * size_t(std::max(d.n_ext, 1)));
   d.xe_p.alloc(3 * size_t(std::max(d.n_ext, 1)));
+  d.xe_z.alloc(3 * size_t(std::max(d.n_ext, 1)));
   if (!same_nodes) d.clear_table();
   S.sync();
 }
@@ -3005,6 +3006,34 @@ void domain_matresid(Solver &S, const double *x, double *xe, const double *b, do
 
 double domain_dot(Solver &S, const double *a, const double *b) { return domain_allreduce(S, dot_device(S, a, b)); }
 
+// hecmw_precond_apply on a domain (hecmw_precond.f90:86-172): with iterPREmax > 1 the
+// outer passes form ZP = R - A Z, whose product updates the halo of Z first (Z,
+// external entries included, starts at zero).
+void domain_precond_apply(Solver &S, const Views<double> &V, int iterpremax, const double *r, double *z,
+                          int *launched) {
+  if (iterpremax <= 1) {
+    launch_precond_plain<double>(S, V, iterpremax, r, z, nullptr);
+    *launched += 2 * std::max(1, int(S.pc.lo.group_slice.size()));
+    return;
+  }
+  cudaStream_t s = S.stream;
+  DomainState &d = S.dom;
+  d.xe_z.zero(s);
+  const double *in = r;
+  for (int it = 1; it <= iterpremax; it++) {
+    launch_sweep<double, false>(S, V, in, V.zp, nullptr);
+    *launched += 2 * std::max(1, int(S.pc.lo.group_slice.size()));
+    if (it == 1) launch_k(s, copy_kernel<double>, S.grid_vec(), kThreads, static_cast<const double *>(V.zp), z, S.n3(),
+                          static_cast<const CgState *>(nullptr));
+    else launch_k(s, add_kernel<double>, S.grid_vec(), kThreads, static_cast<const double *>(V.zp), z, S.n3(),
+                  static_cast<const CgState *>(nullptr));
+    (*launched)++;
+    if (it == iterpremax) break;
+    domain_matresid(S, z, d.xe_z.p, r, V.w, launched);
+    in = V.w;
+  }
+}
+
 // hecmw_solve_CG on one domain, host-driven (every inner product is a global sum).
 float run_cg_domain(Solver &S, int iterpremax, double tol, int maxit, int *error, int *iter, double *resid,
                     int *kernels) {
@@ -3029,8 +3058,7 @@ float run_cg_domain(Solver &S, int iterpremax, double tol, int maxit, int *error
   int n_indef = 0, it;
   double RHO1 = 0.0;
   for (it = 1; it <= maxit; it++) {
-    launch_precond_plain<double>(S, V, iterpremax, R, Z, nullptr);
-    launched += 2 * std::max(1, int(S.pc.lo.group_slice.size()));
+    domain_precond_apply(S, V, iterpremax, R, Z, &launched);
     const double RHO = domain_dot(S, R, Z);
     if (RHO == 0.0) break;
     else if (it > 1 && RHO * RHO1 <= 0) {
@@ -3101,7 +3129,6 @@ int solve_domain(Solver &S, int *Iarray, double *Rarray, int *iter, double *resi
   if (Iarray[41] != 0 || Iarray[42] != 0)
     throw Failure(HECMW33_ERR_BAD_INPUT, "a decomposed domain runs the FP64 CG (Iarray(42) = Iarray(43) = 0)");
   if (Iarray[6] != 0) throw Failure(HECMW33_ERR_BAD_INPUT, "a decomposed domain runs with SCALING=NO");
-  if (Iarray[4] > 1) throw Failure(HECMW33_ERR_BAD_INPUT, "a decomposed domain runs with iterPREmax <= 1");
   DomainState &d = S.dom;
   const double bb = domain_allreduce(S, dot_device(S, S.b.p, S.b.p));
   S.bnrm2 = bb;
@@ -3188,18 +3215,17 @@ void fail(int *ierr, int code, const char *msg) {
   if (ierr) *ierr = code;
 }
 
-// The external part of X (entries 3N..3NP-1) of a decomposed domain, to or from the
-// handle's copy (in: before the solve; out: after it, or `out` for device-to-device).
-void halo_x(Solver &S, double *Xe, cudaMemcpyKind kind, bool out = false) {
-  DomainState &d = S.dom;
-  if (!d.on || d.n_ext == 0) return;
-  const size_t bytes = sizeof(double) * 3 * size_t(d.n_ext);
-  const bool to_dev = kind == cudaMemcpyHostToDevice || (kind == cudaMemcpyDeviceToDevice && !out);
-  if (to_dev) H33_CUDA(cudaMemcpyAsync(d.xe_x.p, Xe, bytes, kind, S.stream));
-  else H33_CUDA(cudaMemcpyAsync(Xe, d.xe_x.p, bytes, kind, S.stream));
+// The external part of X (entries 3N..3NP-1) of a decomposed domain: into the
+// handle's copy before the solve, back to the caller after it.
+void halo_x_in(Solver &S, const double *Xe, cudaMemcpyKind kind) {
+  const DomainState &d = S.dom;
+  if (d.on && d.n_ext)
+    H33_CUDA(cudaMemcpyAsync(d.xe_x.p, Xe, sizeof(double) * 3 * size_t(d.n_ext), kind, S.stream));
 }
-void halo_x(Solver &S, const double *Xe, cudaMemcpyKind kind) {
-  halo_x(S, const_cast<double *>(Xe), kind, false);
+void halo_x_out(Solver &S, double *Xe, cudaMemcpyKind kind) {
+  const DomainState &d = S.dom;
+  if (d.on && d.n_ext)
+    H33_CUDA(cudaMemcpyAsync(Xe, d.xe_x.p, sizeof(double) * 3 * size_t(d.n_ext), kind, S.stream));
 }
 
 void no_domain(const Solver &S, const char *what) {
@@ -3331,10 +3357,10 @@ HECMW33_API void hecmw33_gpu_solve_resident(const int *handle, const double *B, 
   const size_t bytes = sizeof(double) * S.n3();
   H33_CUDA(cudaMemcpyAsync(S.b.p, B, bytes, cudaMemcpyHostToDevice, S.stream));
   H33_CUDA(cudaMemcpyAsync(S.x.p, X, bytes, cudaMemcpyHostToDevice, S.stream));
-  halo_x(S, X + S.n3(), cudaMemcpyHostToDevice);
+  halo_x_in(S, X + S.n3(), cudaMemcpyHostToDevice);
   const int rc = solve_resident(S, Iarray, Rarray, iter, resid, times);
   H33_CUDA(cudaMemcpyAsync(X, S.x.p, bytes, cudaMemcpyDeviceToHost, S.stream));
-  halo_x(S, X + S.n3(), cudaMemcpyDeviceToHost);
+  halo_x_out(S, X + S.n3(), cudaMemcpyDeviceToHost);
   S.sync();
   if (ierr) *ierr = rc;
   H33_ENTRY_END
@@ -3351,10 +3377,10 @@ HECMW33_API void hecmw33_gpu_solve_resident_device(const int *handle, const doub
   const size_t bytes = sizeof(double) * S.n3();
   H33_CUDA(cudaMemcpyAsync(S.b.p, dB, bytes, cudaMemcpyDeviceToDevice, S.stream));
   H33_CUDA(cudaMemcpyAsync(S.x.p, dX, bytes, cudaMemcpyDeviceToDevice, S.stream));
-  halo_x(S, dX + S.n3(), cudaMemcpyDeviceToDevice);
+  halo_x_in(S, dX + S.n3(), cudaMemcpyDeviceToDevice);
   const int rc = solve_resident(S, Iarray, Rarray, iter, resid, times);
   H33_CUDA(cudaMemcpyAsync(dX, S.x.p, bytes, cudaMemcpyDeviceToDevice, S.stream));
-  halo_x(S, dX + S.n3(), cudaMemcpyDeviceToDevice, true);
+  halo_x_out(S, dX + S.n3(), cudaMemcpyDeviceToDevice);
   S.sync();
   if (ierr) *ierr = rc;
   H33_ENTRY_END
@@ -3375,10 +3401,10 @@ HECMW33_API void hecmw33_gpu_solve(const int *handle, const int *N, const int *N
   const size_t bytes = sizeof(double) * S.n3();
   H33_CUDA(cudaMemcpyAsync(S.b.p, B, bytes, cudaMemcpyHostToDevice, S.stream));
   H33_CUDA(cudaMemcpyAsync(S.x.p, X, bytes, cudaMemcpyHostToDevice, S.stream));
-  halo_x(S, X + S.n3(), cudaMemcpyHostToDevice);
+  halo_x_in(S, X + S.n3(), cudaMemcpyHostToDevice);
   const int rc = solve_resident(S, Iarray, Rarray, iter, resid, times);
   H33_CUDA(cudaMemcpyAsync(X, S.x.p, bytes, cudaMemcpyDeviceToHost, S.stream));
-  halo_x(S, X + S.n3(), cudaMemcpyDeviceToHost);
+  halo_x_out(S, X + S.n3(), cudaMemcpyDeviceToHost);
   S.sync();
   if (times) times[0] += tm;
   if (ierr) *ierr = rc;

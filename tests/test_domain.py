@@ -14,7 +14,8 @@ neighbour's import list); one domain reproduces the one-domain oracle bit for bi
 GpuSolver handle driven by its own thread on the one GPU (the domains exchange
 through the host, no kernel waits on another) against the oracle: the same iteration
 count within 2, solution within 1e-8 relative, the global true residual below the
-tolerance; and the options a domain does not run are refused (9101).
+tolerance, also with two outer preconditioner passes; and the options a domain does
+not run are refused (9101).
 """
 import os
 import socket
@@ -38,10 +39,11 @@ def _system(seed=3):
     return m
 
 
-def _domains(m, nd, precond):
+def _domains(m, nd, precond, iterpremax=1):
     doms = partition(m, nd)
     for d in doms:
         d.matrix.set_precond(precond)
+        d.matrix.set_iterpremax(iterpremax)
     return doms
 
 
@@ -106,6 +108,20 @@ def test_oracle_domains_converge_to_the_mesh_solution(nd, precond):
     # the halo of X is the owners' values (the final hecmw_update_R)
     for d, o in zip(doms, out):
         np.testing.assert_array_equal(o["X"].reshape(-1, 3)[d.N:], X.reshape(-1, 3)[d.global_ids[d.N:]])
+
+
+@pytest.mark.parametrize("precond", [1, 10])
+def test_oracle_domains_outer_preconditioner_passes(precond):
+    """iterPREmax = 2: the second pass forms R - A Z, whose product updates the halo
+    of Z (hecmw_precond.f90:166)."""
+    m = _system()
+    doms = _domains(m, 3, precond, iterpremax=2)
+    out = solve_dd_threads(doms)
+    assert all(o["error"] == 0 for o in out)
+    X = gather_solution(doms, [o["X"] for o in out], m.N)
+    assert Oracle(m).rel_resid(X, m.B) <= 1.0e-8
+    one = solve_dd_threads(_domains(m, 3, precond, iterpremax=1))
+    assert out[0]["iter"] < one[0]["iter"]
 
 
 def _free_port():
@@ -179,11 +195,11 @@ def _gpu_domains(doms, method_override=None):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("nd", [2, 3])
-@pytest.mark.parametrize("precond", [1, 3, 10])
-def test_gpu_domains_match_oracle(nd, precond):
+@pytest.mark.parametrize("nd,precond,iterpremax", [(2, 1, 1), (2, 3, 1), (2, 10, 1), (3, 1, 1), (3, 3, 1),
+                                                   (3, 10, 1), (3, 1, 2), (2, 10, 2)])
+def test_gpu_domains_match_oracle(nd, precond, iterpremax):
     m = _system(seed=7)
-    doms = _domains(m, nd, precond)
+    doms = _domains(m, nd, precond, iterpremax)
     ref = solve_dd_threads(doms)
     out = _gpu_domains(doms)
     Xg = gather_solution(doms, [o[1].X for o in out], m.N)
@@ -202,7 +218,10 @@ def test_gpu_domains_match_oracle(nd, precond):
 def test_gpu_domain_refuses_other_options():
     from frontistr_b200.solver import HecmwSolverError
     m = _system()
-    for change in (lambda a: a.set_method(2), lambda a: a.set_iterpremax(2), lambda a: a.set_scaling(1)):
+    def mode1(a):
+        a.Iarray[41] = 1
+
+    for change in (lambda a: a.set_method(2), lambda a: a.set_scaling(1), mode1):
         doms = _domains(m, 2, 1)
         with pytest.raises(HecmwSolverError) as e:
             _gpu_domains(doms, change)
