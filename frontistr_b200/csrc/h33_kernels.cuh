@@ -522,6 +522,19 @@ __device__ __forceinline__ void slice_gemv_u(const SellView<TV> &A, int slot0, i
   }
 }
 
+// L2 prefetch of slots [slot0, slot0 + nslots) of a layout (values and columns), by
+// one lane (cp.async.bulk.prefetch.L2: nothing returns to the SM, nothing waits).
+template <class TV>
+__device__ __forceinline__ void l2_prefetch_slots(const SellView<TV> &A, int slot0, int nslots) {
+  if (nslots <= 0) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.val + size_t(slot0) * 288),
+               "r"(unsigned(nslots) * 288u * unsigned(sizeof(TV)))
+               : "memory");
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.col + size_t(slot0) * 32),
+               "r"(unsigned(nslots) * 128u)
+               : "memory");
+}
+
 // First slot and slot count of slice t (relative to the colour's first slice).
 __device__ __forceinline__ void run_slots(const RunShape &sh, int t, int &slot0, int &nslots) {
   int r = 0;
@@ -530,14 +543,40 @@ __device__ __forceinline__ void run_slots(const RunShape &sh, int t, int &slot0,
   slot0 = sh.slot[r] + (t - sh.slice[r]) * nslots;
 }
 
+// Start of a colour launch.  pre & 1: the launch was made with programmatic stream
+// serialisation -- let the next colour launch as soon as all CTAs of this one run,
+// and wait for the previous colour only after the static work; pre & 2: that static
+// work brings this warp's slices (values, columns) and their diagonal LU entries
+// into L2.  Nothing before the wait reads what an earlier launch wrote.
+template <class TV, class TA, int K>
+__device__ __forceinline__ void colour_prologue(const SellView<TV> &A, const TA *alu, int npos, int nslices,
+                                                const RunShape &sh, int pre) {
+  if (pre & 1) asm volatile("griddepcontrol.launch_dependents;" :::);
+  if (pre & 2) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nslices; t += nwarps) {
+      int slot0, nslots;
+      run_slots(sh, t, slot0, nslots);
+      if (lane == 0) l2_prefetch_slots(A, slot0, nslots);
+      const int row = sh.row0 + t * (32 / K);
+      if (lane >= 1 && lane <= 9 && row < sh.row1)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(alu + size_t(lane - 1) * npos + row));
+    }
+  }
+  if (pre & 1) asm volatile("griddepcontrol.wait;" ::: "memory");
+  else pdl_entry();
+}
+
 // Forward sweep of one colour: zpos(pos) = LU^-1 ( r(perm(pos)) - sum_lower A zpos(col) )
 // (hecmw_precond_SSOR_33.F90:309-345).
 template <class R, class TV, class TA, int K>
 __global__ void __launch_bounds__(kThreads) sweep_fwd_uni_kernel(SellView<TV> L, const int *__restrict__ perm,
                                                                  const TA *__restrict__ alu, int npos,
                                                                  const R *__restrict__ r, R *__restrict__ zpos,
-                                                                 int nslices, RunShape sh, const CgState *st) {
-  pdl_entry();
+                                                                 int nslices, RunShape sh, const CgState *st,
+                                                                 int pre) {
+  colour_prologue<TV, TA, K>(L, alu, npos, nslices, sh, pre);
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
   const int roff = lane / K;
@@ -576,8 +615,8 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U,
                                                                  const R *__restrict__ r, R *__restrict__ z,
                                                                  R *__restrict__ zpos, int nslices, RunShape sh,
                                                                  CgState *st, double *partials, int part_base,
-                                                                 int part_total) {
-  pdl_entry();
+                                                                 int part_total, int pre) {
+  colour_prologue<TV, TA, K>(U, alu, npos, nslices, sh, pre);
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
   const int roff = lane / K;

@@ -71,6 +71,18 @@ bool pdl_mode() {
   return e && e[0] == '1';
 }
 
+// colour_prologue's mode for the SSOR colour launches of values stored as TV: every
+// launch is programmatic (the next colour starts its static work while this one
+// drains); BF16-stored sweeps also bring their slots into L2 before the wait.
+// Measured on the 100^3 cube (FP64 / mode-1 solve): 0.741 / 0.622 s without either,
+// 0.736 / 0.622 s programmatic only, 0.781 / 0.604 s with the prefetch for both
+// (FP64 slot ranges are 4x larger and crowd the vectors out of L2), 0.772 / 0.625 s
+// prefetch only.
+template <class TV>
+constexpr int sweep_pre() {
+  return 1 | (sizeof(TV) <= 2 ? 2 : 0);
+}
+
 // HECMW33_MR_TILED=1: the multi-RHS loop's SpMM stages p through shared memory
 // (mr_spmm_tiled_kernel).  Opt-in: on the 100^3 cube with 16 load cases it measured
 // 4.06 s against 3.77 s untiled -- a CTA waits for its tile's copies before it
@@ -93,6 +105,22 @@ void launch_ks(cudaStream_t s, void (*kern)(KArgs...), int grid, int block, size
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = pdl_mode() ? 1 : 0;
+  H33_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
+}
+
+// As launch_k, with programmatic stream serialisation on or off explicitly.
+template <typename... KArgs, typename... Args>
+void launch_kp(cudaStream_t s, bool pdl, void (*kern)(KArgs...), int grid, int block, Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(grid), 1, 1);
+  cfg.blockDim = dim3(unsigned(block), 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
   H33_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
 }
 
@@ -864,8 +892,9 @@ void launch_sweep_uni(Solver &S, const SellView<TV> &lo, const SellView<TV> &up,
   for (int g = 0; g < gf; g++) {
     const int ns = P.lo.group_slice[g + 1] - P.lo.group_slice[g];
     if (ns <= 0) continue;
-    launch_k(s, sweep_fwd_uni_kernel<R, TV, TA, K>, S.grid_sweep_uni(ns), kThreads, lo, P.perm_fwd.p, alu_f, S.N,
-             rin, zpos, ns, run_shape(P.lo, g), static_cast<const CgState *>(st));
+    constexpr int pre = sweep_pre<TV>();
+    launch_kp(s, true, sweep_fwd_uni_kernel<R, TV, TA, K>, S.grid_sweep_uni(ns), kThreads, lo,
+              P.perm_fwd.p, alu_f, S.N, rin, zpos, ns, run_shape(P.lo, g), static_cast<const CgState *>(st), pre);
   }
   const int gb = int(P.up.group_slice.size()) - 1;
   int total = 0;
@@ -876,8 +905,9 @@ void launch_sweep_uni(Solver &S, const SellView<TV> &lo, const SellView<TV> &up,
     const int grid = S.grid_sweep_uni(std::max(ns, 1));
     // a colour without slices still launches (one idle CTA) so that the reduction
     // ticket count stays exact
-    launch_k(s, sweep_bwd_uni_kernel<R, TV, TA, K, FUSE_RHO>, grid, kThreads, up, P.perm_fwd.p, alu_f, S.N, rin,
-             zout, zpos, ns, run_shape(P.up, g), st, S.partials.p, base, total);
+    constexpr int pre = sweep_pre<TV>();
+    launch_kp(s, true, sweep_bwd_uni_kernel<R, TV, TA, K, FUSE_RHO>, grid, kThreads, up,
+              P.perm_fwd.p, alu_f, S.N, rin, zout, zpos, ns, run_shape(P.up, g), st, S.partials.p, base, total, pre);
     base += grid;
   }
 }
