@@ -525,14 +525,17 @@ __device__ __forceinline__ void slice_gemv_u(const SellView<TV> &A, int slot0, i
 // L2 prefetch of slots [slot0, slot0 + nslots) of a layout (values and columns), by
 // one lane (cp.async.bulk.prefetch.L2: nothing returns to the SM, nothing waits).
 template <class TV>
-__device__ __forceinline__ void l2_prefetch_slots(const SellView<TV> &A, int slot0, int nslots) {
+__device__ __forceinline__ void l2_prefetch_slots(const SellView<TV> &A, int slot0, int nslots, bool vals = true,
+                                                  bool cols = true) {
   if (nslots <= 0) return;
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.val + size_t(slot0) * 288),
-               "r"(unsigned(nslots) * 288u * unsigned(sizeof(TV)))
-               : "memory");
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.col + size_t(slot0) * 32),
-               "r"(unsigned(nslots) * 128u)
-               : "memory");
+  if (vals)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.val + size_t(slot0) * 288),
+                 "r"(unsigned(nslots) * 288u * unsigned(sizeof(TV)))
+                 : "memory");
+  if (cols)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.col + size_t(slot0) * 32),
+                 "r"(unsigned(nslots) * 128u)
+                 : "memory");
 }
 
 // First slot and slot count of slice t (relative to the colour's first slice).
@@ -545,22 +548,23 @@ __device__ __forceinline__ void run_slots(const RunShape &sh, int t, int &slot0,
 
 // Start of a colour launch.  pre & 1: the launch was made with programmatic stream
 // serialisation -- let the next colour launch as soon as all CTAs of this one run,
-// and wait for the previous colour only after the static work; pre & 2: that static
-// work brings this warp's slices (values, columns) and their diagonal LU entries
-// into L2.  Nothing before the wait reads what an earlier launch wrote.
+// and wait for the previous colour only after the static work; that static work
+// brings into L2 this warp's slices' values (pre & 2), columns (pre & 4) and
+// diagonal LU entries (pre & 8).  Nothing before the wait reads what an earlier
+// launch wrote.
 template <class TV, class TA, int K>
 __device__ __forceinline__ void colour_prologue(const SellView<TV> &A, const TA *alu, int npos, int nslices,
                                                 const RunShape &sh, int pre) {
   if (pre & 1) asm volatile("griddepcontrol.launch_dependents;" :::);
-  if (pre & 2) {
+  if (pre & 14) {
     const int lane = threadIdx.x & 31;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nslices; t += nwarps) {
       int slot0, nslots;
       run_slots(sh, t, slot0, nslots);
-      if (lane == 0) l2_prefetch_slots(A, slot0, nslots);
+      if (lane == 0) l2_prefetch_slots(A, slot0, nslots, (pre & 2) != 0, (pre & 4) != 0);
       const int row = sh.row0 + t * (32 / K);
-      if (lane >= 1 && lane <= 9 && row < sh.row1)
+      if ((pre & 8) && lane >= 1 && lane <= 9 && row < sh.row1)
         asm volatile("prefetch.global.L2 [%0];" ::"l"(alu + size_t(lane - 1) * npos + row));
     }
   }

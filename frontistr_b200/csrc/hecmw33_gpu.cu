@@ -73,14 +73,17 @@ bool pdl_mode() {
 
 // colour_prologue's mode for the SSOR colour launches of values stored as TV: every
 // launch is programmatic (the next colour starts its static work while this one
-// drains); BF16-stored sweeps also bring their slots into L2 before the wait.
-// Measured on the 100^3 cube (FP64 / mode-1 solve): 0.741 / 0.622 s without either,
-// 0.736 / 0.622 s programmatic only, 0.781 / 0.604 s with the prefetch for both
-// (FP64 slot ranges are 4x larger and crowd the vectors out of L2), 0.772 / 0.625 s
-// prefetch only.
+// drains), and that work brings into L2 the columns -- the head of each slot's
+// chain of dependent loads -- with the values where they are BF16, with the
+// diagonal LU entries where the values are wider.
+// Measured on the 100^3 cube (FP64 / mode-1 solve, s): none 0.741 / 0.622;
+// programmatic only 0.736 / 0.622; + values, columns and LU 0.781 / 0.604; FP64 with
+// columns 0.719, LU 0.731, columns and LU 0.715; BF16 with values 0.612, columns
+// 0.607, columns and LU 0.607, values and columns 0.600.  Prefetching the FP64
+// values crowds the vectors out of L2 (their slot ranges are 4x the BF16 ones).
 template <class TV>
 constexpr int sweep_pre() {
-  return 1 | (sizeof(TV) <= 2 ? 2 : 0);
+  return sizeof(TV) <= 2 ? (1 | 2 | 4) : (1 | 4 | 8);
 }
 
 // HECMW33_MR_TILED=1: the multi-RHS loop's SpMM stages p through shared memory
