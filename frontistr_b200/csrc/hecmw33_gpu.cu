@@ -3572,6 +3572,7 @@ HECMW33_API void hecmw33_gpu_get_matrix(const int *handle, int *indexL, int *ite
   H33_ENTRY_BEGIN
   Solver &S = get(handle);
   DeviceGuard dg(S.device);
+  no_domain(S, "hecmw33_gpu_get_matrix");
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix");
   const int N = S.N;
   if (indexL) std::copy(S.indexL.begin(), S.indexL.end(), indexL);

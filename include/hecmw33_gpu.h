@@ -32,7 +32,9 @@
  *   - One domain per handle.  N < NP is a domain of a decomposed mesh (internal nodes
  *     1..N, external nodes N+1..NP): hecmw33_gpu_set_domain gives its communication
  *     table and the caller's exchange / allreduce; such a domain runs CG (METHOD = 1)
- *     in FP64 with SCALING=NO (9101 otherwise).
+ *     in FP64 with SCALING=NO (9101 otherwise).  The whole-mesh entries (multi-RHS
+ *     solves, matvec, precond_apply, get_matrix) refuse a domain handle (9101); an
+ *     assembly on the device makes the handle one whole mesh again.
  *   - Iarray(7) = 1 (SCALING=YES, hecmw_solver_scaling_33.f90:20-208): the CG runs on
  *     S A S, S b with S = diag(1/sqrt|D_kk|) and X is multiplied by S after it; the
  *     caller's arrays are not written.  FP64 CG only (Iarray(42) = 0 or 1): 9101 for
