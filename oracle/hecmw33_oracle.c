@@ -72,6 +72,11 @@ int o33_max_threads(void) {
 /* hecmw_matvec_33_inner, CPU branch: hecmw_solver_las_33.F90:279-311.
  * Row i: D block first, then L blocks in ascending order, then U blocks. */
 void o33_matvec(const o33_matrix *A, const double *X, double *Y) {
+  if (A->usejad) { /* hecmw_solver_las_33.F90:155-158, while hecmw_solve_CG holds the
+                     * JAD copy (hecmw_solver_CG.f90:112-113,295-296) */
+    o33_matvec_jad(A, X, Y);
+    return;
+  }
   const int N = A->N;
   const int *indexL = A->indexL, *indexU = A->indexU;
   const int *itemL = A->itemL, *itemU = A->itemU;
@@ -106,6 +111,41 @@ void o33_matvec(const o33_matrix *A, const double *X, double *Y) {
     Y[3 * i] = YV1;
     Y[3 * i + 1] = YV2;
     Y[3 * i + 2] = YV3;
+  }
+}
+
+/* hecmw_JAD_MATVEC_33 (hecmw_jadm_33.f90:57-84) with REPACK and MATJAD (:86-211):
+ * Y = D X row by row, then W accumulated over the jagged diagonals and added.  The
+ * n-th jagged diagonal holds the n-th off-diagonal block of every row long enough,
+ * rows' L blocks first and then their U blocks, each in index order (REPACK); MATJAD
+ * runs over the diagonals in turn, so every row's W sums its off-diagonal blocks in
+ * that order, from zero.  The storage order across rows changes no row's sum, so the
+ * rows are formed here one at a time. */
+void o33_matvec_jad(const o33_matrix *A, const double *X, double *Y) {
+  const int N = A->N;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < N; i++) {
+    const double X1 = X[3 * i], X2 = X[3 * i + 1], X3 = X[3 * i + 2];
+    const double *d = A->D + 9 * (size_t)i;
+    const double Y1 = d[0] * X1 + d[1] * X2 + d[2] * X3;
+    const double Y2 = d[3] * X1 + d[4] * X2 + d[5] * X3;
+    const double Y3 = d[6] * X1 + d[7] * X2 + d[8] * X3;
+    double W1 = 0.0, W2 = 0.0, W3 = 0.0;
+    for (int part = 0; part < 2; part++) {
+      const int *index = part ? A->indexU : A->indexL, *item = part ? A->itemU : A->itemL;
+      const double *V = part ? A->AU : A->AL;
+      for (int j = index[i]; j < index[i + 1]; j++) {
+        const int in = item[j] - 1;
+        const double x1 = X[3 * in], x2 = X[3 * in + 1], x3 = X[3 * in + 2];
+        const double *a = V + 9 * (size_t)j;
+        W1 = W1 + a[0] * x1 + a[1] * x2 + a[2] * x3;
+        W2 = W2 + a[3] * x1 + a[4] * x2 + a[5] * x3;
+        W3 = W3 + a[6] * x1 + a[7] * x2 + a[8] * x3;
+      }
+    }
+    Y[3 * i] = Y1 + W1;
+    Y[3 * i + 1] = Y2 + W2;
+    Y[3 * i + 2] = Y3 + W3;
   }
 }
 
@@ -1670,7 +1710,10 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
     As.AL = ALs;
     As.AU = AUs;
   }
-  const o33_matrix *Aw = SCALING ? &As : A;
+  As.usejad = Iarray[32] != 0; /* IDX_I_USEJAD: the solver's products; the final true
+                                 * residual below uses the plain matvec, as the
+                                 * reference's after hecmw_JAD_FINALIZE */
+  const o33_matrix *Aw = &As;
   const double *Bw = SCALING ? Bs : B;
 
   int error = 0, iter = 0;

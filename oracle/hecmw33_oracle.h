@@ -31,10 +31,16 @@ typedef struct {
   int N, NP, NPL, NPU;
   const int *indexL, *itemL, *indexU, *itemU;
   const double *D, *AL, *AU;
+  /* USEJAD (Iarray(33)): products in the jagged-diagonal order of
+   * hecmw1/src/solver/las/hecmw_jadm_33.f90 (o33_solve sets it from Iarray) */
+  int usejad;
 } o33_matrix;
 
 /* ---- kernels of hecmw1/src/solver/las/hecmw_solver_las_33.F90 ---- */
 void o33_matvec(const o33_matrix *A, const double *x, double *y);
+/* hecmw_JAD_MATVEC_33: y_i = D_i x_i plus the row's off-diagonal blocks summed from
+ * zero (L then U, in index order) */
+void o33_matvec_jad(const o33_matrix *A, const double *x, double *y);
 void o33_matresid(const o33_matrix *A, const double *x, const double *b, double *r);
 double o33_rel_resid_L2(const o33_matrix *A, const double *x, const double *b);
 

@@ -20,7 +20,7 @@ _f64p = ctypes.POINTER(ctypes.c_double)
 class O33Matrix(ctypes.Structure):
     _fields_ = [("N", ctypes.c_int), ("NP", ctypes.c_int), ("NPL", ctypes.c_int),
                 ("NPU", ctypes.c_int), ("indexL", _i32p), ("itemL", _i32p), ("indexU", _i32p),
-                ("itemU", _i32p), ("D", _f64p), ("AL", _f64p), ("AU", _f64p)]
+                ("itemU", _i32p), ("D", _f64p), ("AL", _f64p), ("AU", _f64p), ("usejad", ctypes.c_int)]
 
 
 UPDATE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, _f64p)
@@ -46,6 +46,7 @@ def lib():
         L = ctypes.CDLL(ORACLE_SO)
         L.o33_matvec.argtypes = [ctypes.POINTER(O33Matrix), _f64p, _f64p]
         L.o33_matresid.argtypes = [ctypes.POINTER(O33Matrix), _f64p, _f64p, _f64p]
+        L.o33_matvec_jad.argtypes = [ctypes.POINTER(O33Matrix), _f64p, _f64p]
         L.o33_rel_resid_L2.argtypes = [ctypes.POINTER(O33Matrix), _f64p, _f64p]
         L.o33_rel_resid_L2.restype = ctypes.c_double
         L.o33_dot.argtypes = [ctypes.c_int, _f64p, _f64p]
@@ -102,6 +103,12 @@ class Oracle:
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.zeros(3 * self.m.NP)
         self.L.o33_matvec(ctypes.byref(self.mat), _dp(x), _dp(y))
+        return y
+
+    def matvec_jad(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(3 * self.m.NP)
+        self.L.o33_matvec_jad(ctypes.byref(self.mat), _dp(x), _dp(y))
         return y
 
     def rel_resid(self, x, b):
