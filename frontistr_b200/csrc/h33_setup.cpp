@@ -560,6 +560,150 @@ int factor_bilu0(const Profile &p, const double *D, const double *AL, const doub
   return 0;
 }
 
+void bilu_fill(const Profile &p, int level, FilledProfile &f) {
+  const int N = p.N;
+  // per row: fill columns (0-based) with their level, collected as the reference
+  // scans (the order of collection is undone by the sort)
+  std::vector<std::vector<std::pair<int, int>>> fill(static_cast<size_t>(N));
+  std::vector<int> mark(static_cast<size_t>(N), 0);
+  std::vector<int> touched;
+  auto reset = [&]() {
+    for (int c : touched) mark[size_t(c)] = 0;
+    touched.clear();
+  };
+  auto set = [&](int c) {
+    if (!mark[size_t(c)]) touched.push_back(c);
+    mark[size_t(c)] = 1;
+  };
+  // level 1
+  for (int i = 1; i < N; i++) {
+    set(i);
+    for (int k = p.indexL[i]; k < p.indexL[i + 1]; k++) set(p.itemL[k] - 1);
+    for (int k = p.indexU[i]; k < p.indexU[i + 1]; k++)
+      if (p.itemU[k] <= N) set(p.itemU[k] - 1);
+    for (int kk = p.indexL[i]; kk < p.indexL[i + 1]; kk++) {
+      const int k = p.itemL[kk] - 1;
+      for (int j = p.indexU[k]; j < p.indexU[k + 1]; j++) {
+        const int c = p.itemU[j] - 1;
+        if (c >= N || mark[size_t(c)]) continue;
+        fill[size_t(i)].push_back({c, 1});
+        set(c);
+      }
+    }
+    reset();
+  }
+  // level 2: original L x level-1 U, then level-1 L x original U
+  if (level >= 2) {
+    std::vector<std::vector<std::pair<int, int>>> fill2(static_cast<size_t>(N));
+    for (int i = 1; i < N; i++) {
+      set(i);
+      for (int k = p.indexL[i]; k < p.indexL[i + 1]; k++) set(p.itemL[k] - 1);
+      for (int k = p.indexU[i]; k < p.indexU[i + 1]; k++)
+        if (p.itemU[k] <= N) set(p.itemU[k] - 1);
+      for (const auto &e : fill[size_t(i)]) set(e.first);
+      for (int kk = p.indexL[i]; kk < p.indexL[i + 1]; kk++) {
+        const int k = p.itemL[kk] - 1;
+        for (const auto &e : fill[size_t(k)]) {
+          const int c = e.first;
+          if (c <= k || mark[size_t(c)]) continue;  // level-1 U entries of row k
+          fill2[size_t(i)].push_back({c, 2});
+          set(c);
+        }
+      }
+      for (const auto &fe : fill[size_t(i)]) {
+        const int k = fe.first;
+        if (k >= i) continue;  // level-1 L entries of row i
+        for (int j = p.indexU[k]; j < p.indexU[k + 1]; j++) {
+          const int c = p.itemU[j] - 1;
+          if (c >= N || mark[size_t(c)]) continue;
+          fill2[size_t(i)].push_back({c, 2});
+          set(c);
+        }
+      }
+      reset();
+    }
+    for (int i = 0; i < N; i++)
+      fill[size_t(i)].insert(fill[size_t(i)].end(), fill2[size_t(i)].begin(), fill2[size_t(i)].end());
+  }
+  f = FilledProfile();
+  f.N = N;
+  f.indexL.assign(size_t(N) + 1, 0);
+  f.indexU.assign(size_t(N) + 1, 0);
+  struct E {
+    int col, lev, src;
+  };
+  std::vector<E> lo, up;
+  for (int i = 0; i < N; i++) {
+    lo.clear();
+    up.clear();
+    for (int k = p.indexL[i]; k < p.indexL[i + 1]; k++) lo.push_back({p.itemL[k] - 1, 0, k});
+    for (int k = p.indexU[i]; k < p.indexU[i + 1]; k++)
+      if (p.itemU[k] <= N) up.push_back({p.itemU[k] - 1, 0, k});
+    for (const auto &e : fill[size_t(i)]) (e.first < i ? lo : up).push_back({e.first, e.second, -1});
+    auto by_col = [](const E &a, const E &b) { return a.col < b.col; };
+    std::sort(lo.begin(), lo.end(), by_col);  // distinct columns: any sort gives the reference's order
+    std::sort(up.begin(), up.end(), by_col);
+    for (const auto &e : lo) {
+      f.itemL.push_back(e.col + 1);
+      f.levL.push_back(e.lev);
+      f.srcL.push_back(e.src);
+    }
+    for (const auto &e : up) {
+      f.itemU.push_back(e.col + 1);
+      f.levU.push_back(e.lev);
+      f.srcU.push_back(e.src);
+    }
+    f.indexL[size_t(i) + 1] = int(f.itemL.size());
+    f.indexU[size_t(i) + 1] = int(f.itemU.size());
+  }
+}
+
+int factor_bilu_fill(const FilledProfile &f, int level, const double *D, const double *AL, const double *AU,
+                     double sigma_diag, std::vector<double> &Dlu, std::vector<double> &ALlu,
+                     std::vector<double> &AUlu) {
+  const int N = f.N;
+  const size_t nL = f.itemL.size(), nU = f.itemU.size();
+  Dlu.assign(D, D + 9 * size_t(N));
+  ALlu.assign(9 * nL, 0.0);
+  AUlu.assign(9 * nU, 0.0);
+  for (size_t k = 0; k < nL; k++)
+    if (f.srcL[k] >= 0) std::memcpy(&ALlu[9 * k], AL + 9 * size_t(f.srcL[k]), 9 * sizeof(double));
+  for (size_t k = 0; k < nU; k++)
+    if (f.srcU[k] >= 0) std::memcpy(&AUlu[9 * k], AU + 9 * size_t(f.srcU[k]), 9 * sizeof(double));
+  for (int i = 0; i < N; i++) {
+    Dlu[9 * size_t(i)] *= sigma_diag;
+    Dlu[9 * size_t(i) + 4] *= sigma_diag;
+    Dlu[9 * size_t(i) + 8] *= sigma_diag;
+  }
+  if (N > 0 && lu33_inplace(Dlu.data())) return 9001;
+  std::vector<int> posL(static_cast<size_t>(N), 0), posU(static_cast<size_t>(N), 0);
+  double RHS[9];
+  for (int i = 1; i < N; i++) {
+    for (int k = f.indexL[i]; k < f.indexL[i + 1]; k++) posL[size_t(f.itemL[k] - 1)] = k + 1;
+    for (int k = f.indexU[i]; k < f.indexU[i + 1]; k++) posU[size_t(f.itemU[k] - 1)] = k + 1;
+    for (int kk = f.indexL[i]; kk < f.indexL[i + 1]; kk++) {
+      const int lik = f.levL[size_t(kk)];
+      if (lik >= level) continue;
+      const int k = f.itemL[kk] - 1;
+      double Aik[9];
+      std::memcpy(Aik, &ALlu[9 * size_t(kk)], sizeof(Aik));
+      const double *Dk = &Dlu[9 * size_t(k)];
+      for (int jj = f.indexU[k]; jj < f.indexU[k + 1]; jj++) {
+        if (lik + f.levU[size_t(jj)] >= level) continue;
+        const int j = f.itemU[jj] - 1;
+        aik_dinv_akj(RHS, Dk, Aik, &AUlu[9 * size_t(jj)]);
+        double *dst = j == i ? &Dlu[9 * size_t(i)]
+                             : (j < i ? &ALlu[9 * size_t(posL[size_t(j)] - 1)] : &AUlu[9 * size_t(posU[size_t(j)] - 1)]);
+        for (int e = 0; e < 9; e++) dst[e] = dst[e] - RHS[e];
+      }
+    }
+    if (lu33_inplace(&Dlu[9 * size_t(i)])) return 9001;
+    for (int k = f.indexL[i]; k < f.indexL[i + 1]; k++) posL[size_t(f.itemL[k] - 1)] = 0;
+    for (int k = f.indexU[i]; k < f.indexU[i + 1]; k++) posU[size_t(f.itemU[k] - 1)] = 0;
+  }
+  return 0;
+}
+
 void level_schedule(const Profile &p, bool lower, std::vector<int> &order,
                     std::vector<int> &level_ptr) {
   const int N = p.N;

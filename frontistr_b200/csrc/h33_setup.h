@@ -111,6 +111,29 @@ int factor_bilu0(const Profile &p, const double *D, const double *AL, const doub
                  double sigma_diag, std::vector<double> &Dlu0, std::vector<double> &ALlu0,
                  std::vector<double> &AUlu0);
 
+// Fill pattern of the reference's block ILU(1) / ILU(2) (FORM_ILU1_33 / FORM_ILU2_33,
+// hecmw_precond_BILU_33.f90:371-739, 748-1337) on the internal rows of p: level-1
+// fill = original L(i) x original U(k), not yet in row i; level 2 (ILU(2) only) =
+// original L(i) x level-1 U(k) and level-1 L(i) x original U(k).  Each row's lists
+// sorted ascending (fill_in_S33_SORT), with the level of every entry and the index
+// of its original block (-1 for fill).
+struct FilledProfile {
+  int N = 0;
+  std::vector<int> indexL, itemL, indexU, itemU;  // items 1-based, as hecmwST
+  std::vector<int> levL, levU, srcL, srcU;
+  Profile view() const { return Profile{N, indexL.data(), itemL.data(), indexU.data(), itemU.data()}; }
+};
+void bilu_fill(const Profile &p, int level, FilledProfile &f);
+
+// Numeric block ILU(1) / ILU(2) on a filled pattern: D with sigma_diag on its diagonal,
+// original values at original positions and zero at fill; row i eliminates with
+// every L(i,k) and U(k,j) whose levels sum below `level`, the diagonal included, and
+// ends with the reciprocal-pivot LU of its diagonal block.  Returns 0 or 9001 on a
+// zero pivot.
+int factor_bilu_fill(const FilledProfile &f, int level, const double *D, const double *AL, const double *AU,
+                     double sigma_diag, std::vector<double> &Dlu, std::vector<double> &ALlu,
+                     std::vector<double> &AUlu);
+
 // Level schedule of the natural-order lower (or upper) triangular solve:
 // level[i] = 1 + max level over dependencies.  Rows sorted by group -> order,
 // group boundaries in level_ptr.  Lower: group = level (walked first to last).

@@ -209,7 +209,9 @@ struct DevSell {
 };
 
 struct Precond {
-  int kind = 0;  // 1 SSOR, 3 DIAG, 10 ILU(0)
+  int kind = 0;  // 1 SSOR, 3 DIAG, 10 block ILU(p)
+  int ilu_level = 0;   // p of the block ILU (PRECOND 10, 11, 12)
+  FilledProfile fill;  // its factor pattern when p > 0
   bool valid = false;
   int ncolor_in = 0;
   int generation = 0;
@@ -220,7 +222,7 @@ struct Precond {
   bool alu_shared = true;
   int ncolor = 0;
   std::vector<int> colorindex, perm;  // SSOR: host copies (0-based)
-  DevArray<double> ilu_raw;           // ILU(0) factor blocks, raw numbering
+  DevArray<double> ilu_raw;           // block ILU factor blocks: D | L | U in factor-pattern order
   DevArray<float> alu32_fwd, alu32_bwd;
   int numeric_version = 0, fp32_version = -1, lowp_version = -1;
   bool pos_cols = false;  // lo/up columns are colour positions (multicolour SSOR)
@@ -678,22 +680,28 @@ void setup_ssor(Solver &S, int ncolor_in, double sigma, bool symbolic) {
   diag_alu(S, P.alu_fwd, S.raw.p, P.perm_fwd.p, sigma, 0);
 }
 
-void setup_bilu0(Solver &S, double sigma, bool symbolic) {
+// Block ILU(p) (hecmw_precond_BILU_33.f90): p = 0 on the matrix's own pattern
+// (FORM_ILU0_33), p = 1, 2 on the fill pattern of FORM_ILU1_33 / FORM_ILU2_33.  The
+// factorisation runs on the host from the resident values; the forward and backward
+// solves run on the device in level schedules of the factor pattern.
+void setup_bilu(Solver &S, int level, double sigma, bool symbolic) {
   Precond &P = S.pc;
-  Profile prof{S.N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
+  const Profile prof0{S.N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
   if (symbolic) {
+    if (level > 0) bilu_fill(prof0, level, P.fill);
+    const Profile prof = level > 0 ? P.fill.view() : prof0;
     std::vector<int> ord_f, lev_f, ord_b, lev_b;
     level_schedule(prof, true, ord_f, lev_f);
     level_schedule(prof, false, ord_b, lev_b);
     BlockRows lower, upper;
-    const int N = S.N, NPL = S.NPL;
+    const int N = S.N, NPL = prof.NPL();
     lower.ptr.assign(size_t(N) + 1, 0);
     upper.ptr.assign(size_t(N) + 1, 0);
     for (int pos = 0; pos < N; pos++) {
       const int i = ord_f[pos];
-      lower.ptr[pos + 1] = lower.ptr[pos] + (S.indexL[i + 1] - S.indexL[i]);
+      lower.ptr[pos + 1] = lower.ptr[pos] + (prof.indexL[i + 1] - prof.indexL[i]);
       const int k = ord_b[pos];
-      upper.ptr[pos + 1] = upper.ptr[pos] + (S.indexU[k + 1] - S.indexU[k]);
+      upper.ptr[pos + 1] = upper.ptr[pos] + (prof.indexU[k + 1] - prof.indexU[k]);
     }
     lower.col.resize(size_t(lower.ptr[N]));
     lower.src.resize(size_t(lower.ptr[N]));
@@ -702,14 +710,14 @@ void setup_bilu0(Solver &S, double sigma, bool symbolic) {
     for (int pos = 0; pos < N; pos++) {
       const int i = ord_f[pos];
       int64_t w = lower.ptr[pos];
-      for (int j = S.indexL[i]; j < S.indexL[i + 1]; j++) {
-        lower.col[w] = S.itemL[j] - 1;
+      for (int j = prof.indexL[i]; j < prof.indexL[i + 1]; j++) {
+        lower.col[w] = prof.itemL[j] - 1;
         lower.src[w++] = N + j;
       }
       const int k = ord_b[pos];
       w = upper.ptr[pos];
-      for (int j = S.indexU[k]; j < S.indexU[k + 1]; j++) {
-        upper.col[w] = S.itemU[j] - 1;
+      for (int j = prof.indexU[k]; j < prof.indexU[k + 1]; j++) {
+        upper.col[w] = prof.itemU[j] - 1;
         upper.src[w++] = N + NPL + j;
       }
     }
@@ -722,20 +730,24 @@ void setup_bilu0(Solver &S, double sigma, bool symbolic) {
     P.perm_bwd.upload(ord_b, S.stream);
     P.alu_shared = false;
     P.ncolor = 0;
+    P.ilu_level = level;
   }
   // numeric factorisation on the host, from the resident values
   const size_t nb = size_t(S.N) + S.NPL + S.NPU;
   std::vector<double> host(9 * nb);
   H33_CUDA(cudaMemcpyAsync(host.data(), S.raw.p, sizeof(double) * host.size(), cudaMemcpyDeviceToHost, S.stream));
   S.sync();
+  const double *D = host.data(), *AL = host.data() + 9 * size_t(S.N), *AU = host.data() + 9 * (size_t(S.N) + S.NPL);
   std::vector<double> Dlu, ALlu, AUlu;
-  const int rc = factor_bilu0(prof, host.data(), host.data() + 9 * size_t(S.N),
-                              host.data() + 9 * (size_t(S.N) + S.NPL), sigma, Dlu, ALlu, AUlu);
-  if (rc) throw Failure(HECMW33_ERR_ILU_ZERO_PIVOT, "block ILU(0): zero pivot (the reference stops here)");
-  std::copy(Dlu.begin(), Dlu.end(), host.begin());
-  std::copy(ALlu.begin(), ALlu.end(), host.begin() + 9 * size_t(S.N));
-  std::copy(AUlu.begin(), AUlu.end(), host.begin() + 9 * (size_t(S.N) + S.NPL));
-  P.ilu_raw.upload(host.data(), host.size(), S.stream);
+  const int rc = level > 0 ? factor_bilu_fill(P.fill, level, D, AL, AU, sigma, Dlu, ALlu, AUlu)
+                           : factor_bilu0(prof0, D, AL, AU, sigma, Dlu, ALlu, AUlu);
+  if (rc) throw Failure(HECMW33_ERR_ILU_ZERO_PIVOT, "block ILU: zero pivot (the reference stops here)");
+  std::vector<double> fac;
+  fac.reserve(Dlu.size() + ALlu.size() + AUlu.size());
+  fac.insert(fac.end(), Dlu.begin(), Dlu.end());
+  fac.insert(fac.end(), ALlu.begin(), ALlu.end());
+  fac.insert(fac.end(), AUlu.begin(), AUlu.end());
+  P.ilu_raw.upload(fac.data(), fac.size(), S.stream);
   P.lo.pack(P.ilu_raw.p, S.stream, S.nsm);
   P.up.pack(P.ilu_raw.p, S.stream, S.nsm);
   diag_alu(S, P.alu_fwd, P.ilu_raw.p, P.perm_fwd.p, 1.0, 1);
@@ -766,15 +778,17 @@ void recycle_precond_setting(int *Iarray) {
 // hecmw_precond_setup (hecmw_precond.f90:30-58) with the reuse test of each
 // preconditioner's setup (e.g. hecmw_precond_SSOR_33.F90:74-82).
 void precond_setup(Solver &S, int precond, int ncolor_in, double sigma, int *Iarray) {
-  const int kind = precond == 2 ? 1 : precond;
+  const int kind = precond == 2 ? 1 : (precond >= 10 && precond <= 12 ? 10 : precond);
+  const int level = kind == 10 ? precond - 10 : 0;
   if (kind != 1 && kind != 3 && kind != 10)
     throw Failure(HECMW33_ERR_INCONS_PC, "PRECOND " + std::to_string(precond) +
-                                             " is not available in the GPU drop-in (1, 2, 3, 10 are)");
+                                             " is not available in the GPU drop-in (1, 2, 3, 10, 11, 12 are)");
   Precond &P = S.pc;
-  const bool reuse = P.valid && P.kind == kind && Iarray[97] == 0 && Iarray[96] == 0 &&
-                     (kind != 1 || P.ncolor_in == ncolor_in);
+  const bool same = P.valid && P.kind == kind && (kind != 1 || P.ncolor_in == ncolor_in) &&
+                    (kind != 10 || P.ilu_level == level);
+  const bool reuse = same && Iarray[97] == 0 && Iarray[96] == 0;
   if (reuse) return;
-  const bool symbolic = !P.valid || P.kind != kind || (kind == 1 && P.ncolor_in != ncolor_in);
+  const bool symbolic = !same;
   if (symbolic) {
     P = Precond();
   }
@@ -782,7 +796,7 @@ void precond_setup(Solver &S, int precond, int ncolor_in, double sigma, int *Iar
   P.ncolor_in = ncolor_in;
   if (kind == 1) setup_ssor(S, ncolor_in, sigma, symbolic);
   else if (kind == 3) diag_alu(S, P.alu_fwd, S.raw.p, nullptr, sigma, 0);
-  else setup_bilu0(S, sigma, symbolic);
+  else setup_bilu(S, level, sigma, symbolic);
   int err = 0;
   H33_CUDA(cudaMemcpyAsync(&err, S.d_err.p, sizeof(int), cudaMemcpyDeviceToHost, S.stream));
   S.sync();

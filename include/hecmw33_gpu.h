@@ -136,7 +136,8 @@ HECMW33_API void hecmw33_gpu_set_domain(const int *handle, const int *n_neighbor
 /* hecmw_solve (hecmw_solver.f90:9-88) for METHOD = 1-7 on the resident matrix:
  * zero-RHS check, zero-diagonal check, preconditioner recycle policy
  * (hecmw_matrix_misc.F90:858-877), preconditioner setup (PRECOND 1,2 = SSOR with the
- * reference's RCM + multicolour ordering, 3 = DIAG, 10 = block ILU(0)), CG (or
+ * reference's RCM + multicolour ordering, 3 = DIAG, 10 / 11 / 12 = block ILU(0) / ILU(1) /
+ * ILU(2)), CG (or
  * BiCGSTAB, GMRES(Iarray(6)), GPBiCG, GMRESR, GMRESREN, CR) to Rarray(1), the METHOD2 = 2-7
  * fallback of a diverged CG (GMRESR and GMRESREN clear the preconditioner when they return,
  * as hecmw_precond_clear does, so the next solve sets it up again)

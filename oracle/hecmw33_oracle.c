@@ -428,7 +428,7 @@ static inline void lu33_solve(const double *alu, double *X1, double *X2, double 
 
 /* ------------------------------------------------------------------------ */
 struct o33_precond {
-  int kind; /* 1 SSOR, 3 DIAG, 10 BILU0 */
+  int kind; /* 1 SSOR, 3 DIAG, 10 / 11 / 12 block ILU(0) / ILU(1) / ILU(2) */
   int N, NP;
   /* SSOR: reordered profile (items renumbered to old 1-based ids) */
   int ncolor;
@@ -680,6 +680,203 @@ static o33_precond *bilu0_setup(const o33_matrix *A, double sigma_diag, int *ier
   return P;
 }
 
+/* FORM_ILU1_33 / FORM_ILU2_33 (hecmw_precond_BILU_33.f90:371-739, 748-1337), 1-based
+ * as the reference.  Fill of row i: pass 1 (level 1) adds the columns of original
+ * U(k) for every original L(i,k) that row i does not hold yet; ILU(2)'s pass 2
+ * (level 2) adds those of level-1 U(k) for original L(i,k), then of original U(k) for
+ * level-1 L(i,k).  Each row's lists are sorted by column (fill_in_S33_SORT; the
+ * columns are distinct, so the order is the sort's).  The elimination of row i runs
+ * over its L entries in column order and, for each, over U(k) in column order,
+ * subtracting Aik Dk^-1 Akj from D(i), L(i,j) or U(i,j) when the two levels sum below
+ * the ILU level (ILU(1): original entries only; ILU(2): level sums 0 and 1). */
+typedef struct {
+  int col, lev, src;
+} fill_entry;
+static int cmp_fill(const void *a, const void *b) {
+  const int x = ((const fill_entry *)a)->col, y = ((const fill_entry *)b)->col;
+  return (x > y) - (x < y);
+}
+static o33_precond *bilu_fill_setup(const o33_matrix *A, int level, double sigma_diag, int *ierr) {
+  const int NP = A->NP;
+  const int *INL = A->indexL, *IAL = A->itemL, *INU = A->indexU, *IAU = A->itemU;
+  int *IW1 = (int *)calloc((size_t)NP + 1, sizeof(int));
+  /* fill of each row: CSR over rows, columns 1-based, with levels */
+  int *fptr = (int *)calloc((size_t)NP + 2, sizeof(int));
+  size_t cap = 16 * (size_t)NP + 16, nf = 0;
+  fill_entry *fl = (fill_entry *)malloc(sizeof(fill_entry) * cap);
+  for (int pass = 1; pass <= level; pass++) {
+    /* pass 2 reads the level-1 lists of pass 1, which it appends to */
+    const size_t nf1 = nf;
+    int *f1ptr = NULL;
+    if (pass == 2) {
+      f1ptr = (int *)malloc(sizeof(int) * ((size_t)NP + 2));
+      memcpy(f1ptr, fptr, sizeof(int) * ((size_t)NP + 2));
+    }
+    fill_entry *add = (fill_entry *)malloc(sizeof(fill_entry) * cap);
+    size_t nadd = 0, cap_add = cap;
+    int *addptr = (int *)calloc((size_t)NP + 2, sizeof(int));
+    for (int i = 2; i <= NP; i++) {
+      addptr[i] = (int)nadd;
+      IW1[i] = 1;
+      for (int L = INL[i - 1]; L < INL[i]; L++) IW1[IAL[L]] = 1;
+      for (int L = INU[i - 1]; L < INU[i]; L++) IW1[IAU[L]] = 1;
+      if (pass == 2)
+        for (int q = f1ptr[i]; q < f1ptr[i + 1]; q++) IW1[fl[q].col] = 1;
+#define FILL_ADD(jj)                                                             \
+  do {                                                                           \
+    if (IW1[jj] == 0) {                                                          \
+      if (nadd == cap_add) {                                                     \
+        cap_add *= 2;                                                            \
+        add = (fill_entry *)realloc(add, sizeof(fill_entry) * cap_add);          \
+      }                                                                          \
+      add[nadd].col = (jj);                                                      \
+      add[nadd].lev = pass;                                                      \
+      add[nadd].src = -1;                                                        \
+      nadd++;                                                                    \
+      IW1[jj] = 1;                                                               \
+    }                                                                            \
+  } while (0)
+      for (int k = INL[i - 1]; k < INL[i]; k++) {
+        const int kk = IAL[k];
+        if (pass == 1) {
+          for (int j = INU[kk - 1]; j < INU[kk]; j++) FILL_ADD(IAU[j]);
+        } else {
+          for (int q = f1ptr[kk]; q < f1ptr[kk + 1]; q++)
+            if (fl[q].col > kk) FILL_ADD(fl[q].col);
+        }
+      }
+      if (pass == 2)
+        for (int q = f1ptr[i]; q < f1ptr[i + 1]; q++) {
+          const int kk = fl[q].col;
+          if (kk >= i) continue;
+          for (int j = INU[kk - 1]; j < INU[kk]; j++) FILL_ADD(IAU[j]);
+        }
+#undef FILL_ADD
+      /* clear the markers */
+      IW1[i] = 0;
+      for (int L = INL[i - 1]; L < INL[i]; L++) IW1[IAL[L]] = 0;
+      for (int L = INU[i - 1]; L < INU[i]; L++) IW1[IAU[L]] = 0;
+      if (pass == 2)
+        for (int q = f1ptr[i]; q < f1ptr[i + 1]; q++) IW1[fl[q].col] = 0;
+      for (size_t q = (size_t)addptr[i]; q < nadd; q++) IW1[add[q].col] = 0;
+    }
+    addptr[NP + 1] = (int)nadd;
+    addptr[1] = 0;
+    /* merge: row i's fill = its earlier fill then this pass's additions */
+    fill_entry *merged = (fill_entry *)malloc(sizeof(fill_entry) * (nf1 + nadd + 1));
+    int *mptr = (int *)calloc((size_t)NP + 2, sizeof(int));
+    size_t m = 0;
+    for (int i = 1; i <= NP; i++) {
+      mptr[i] = (int)m;
+      for (int q = fptr[i]; q < fptr[i + 1]; q++) merged[m++] = fl[q];
+      if (i >= 2)
+        for (int q = addptr[i]; q < (i < NP ? addptr[i + 1] : (int)nadd); q++) merged[m++] = add[q];
+    }
+    mptr[NP + 1] = (int)m;
+    free(fl);
+    fl = merged;
+    nf = m;
+    cap = m + 1;
+    memcpy(fptr, mptr, sizeof(int) * ((size_t)NP + 2));
+    free(mptr);
+    free(add);
+    free(addptr);
+    free(f1ptr);
+  }
+  /* the filled rows, sorted by column */
+  int *inL = (int *)calloc((size_t)NP + 1, sizeof(int)), *inU = (int *)calloc((size_t)NP + 1, sizeof(int));
+  size_t nL = (size_t)INL[NP], nU = (size_t)INU[NP];
+  for (int i = 1; i <= NP; i++)
+    for (int q = fptr[i]; q < fptr[i + 1]; q++) {
+      if (fl[q].col < i) nL++;
+      else nU++;
+    }
+  int *iaL = (int *)malloc(sizeof(int) * (nL + 1)), *iaU = (int *)malloc(sizeof(int) * (nU + 1));
+  int *lvL = (int *)malloc(sizeof(int) * (nL + 1)), *lvU = (int *)malloc(sizeof(int) * (nU + 1));
+  double *ALf = (double *)calloc(9 * (nL + 1), sizeof(double)), *AUf = (double *)calloc(9 * (nU + 1), sizeof(double));
+  fill_entry *row = (fill_entry *)malloc(sizeof(fill_entry) * ((size_t)NP + 1));
+  size_t wl = 0, wu = 0;
+  for (int i = 1; i <= NP; i++) {
+    int n = 0;
+    for (int L = INL[i - 1]; L < INL[i]; L++) row[n++] = (fill_entry){IAL[L], 0, L};
+    for (int q = fptr[i]; q < fptr[i + 1]; q++)
+      if (fl[q].col < i) row[n++] = fl[q];
+    qsort(row, (size_t)n, sizeof(fill_entry), cmp_fill);
+    for (int q = 0; q < n; q++, wl++) {
+      iaL[wl] = row[q].col;
+      lvL[wl] = row[q].lev;
+      if (row[q].src >= 0) memcpy(ALf + 9 * wl, A->AL + 9 * (size_t)row[q].src, 9 * sizeof(double));
+    }
+    inL[i] = (int)wl;
+    n = 0;
+    for (int L = INU[i - 1]; L < INU[i]; L++) row[n++] = (fill_entry){IAU[L], 0, L};
+    for (int q = fptr[i]; q < fptr[i + 1]; q++)
+      if (fl[q].col > i) row[n++] = fl[q];
+    qsort(row, (size_t)n, sizeof(fill_entry), cmp_fill);
+    for (int q = 0; q < n; q++, wu++) {
+      iaU[wu] = row[q].col;
+      lvU[wu] = row[q].lev;
+      if (row[q].src >= 0) memcpy(AUf + 9 * wu, A->AU + 9 * (size_t)row[q].src, 9 * sizeof(double));
+    }
+    inU[i] = (int)wu;
+  }
+  free(row);
+  free(fl);
+  free(fptr);
+  o33_precond *P = (o33_precond *)calloc(1, sizeof(o33_precond));
+  P->kind = 10 + level;
+  P->N = A->N;
+  P->NP = NP;
+  P->own_inL = inL;
+  P->own_inU = inU;
+  P->own_iaL = iaL;
+  P->own_iaU = iaU;
+  P->inL = inL;
+  P->inU = inU;
+  P->iaL = iaL;
+  P->iaU = iaU;
+  P->ALlu0 = ALf;
+  P->AUlu0 = AUf;
+  P->Dlu0 = (double *)malloc(sizeof(double) * 9 * (size_t)NP);
+  memcpy(P->Dlu0, A->D, sizeof(double) * 9 * (size_t)NP);
+  *ierr = 0;
+  for (int i = 0; i < NP; i++) {
+    P->Dlu0[9 * i + 0] = P->Dlu0[9 * i + 0] * sigma_diag;
+    P->Dlu0[9 * i + 4] = P->Dlu0[9 * i + 4] * sigma_diag;
+    P->Dlu0[9 * i + 8] = P->Dlu0[9 * i + 8] * sigma_diag;
+  }
+  if (lu33(P->Dlu0, 1.0)) *ierr = ERR_ILU_ZERO_PIVOT;
+  int *IW2 = (int *)calloc((size_t)NP + 1, sizeof(int));
+  double RHS[9];
+  for (int i = 2; i <= NP && !*ierr; i++) {
+    for (int k = inL[i - 1]; k < inL[i]; k++) IW1[iaL[k]] = k + 1;
+    for (int k = inU[i - 1]; k < inU[i]; k++) IW2[iaU[k]] = k + 1;
+    for (int kk = inL[i - 1]; kk < inL[i]; kk++) {
+      if (lvL[kk] >= level) continue;
+      const int k = iaL[kk];
+      const double *DkINV = P->Dlu0 + 9 * (size_t)(k - 1);
+      double Aik[9];
+      memcpy(Aik, ALf + 9 * (size_t)kk, sizeof(Aik));
+      for (int jj = inU[k - 1]; jj < inU[k]; jj++) {
+        if (lvL[kk] + lvU[jj] >= level) continue;
+        const int j = iaU[jj];
+        ilu1b33(RHS, DkINV, Aik, AUf + 9 * (size_t)jj);
+        double *dst = j == i ? P->Dlu0 + 9 * (size_t)(i - 1)
+                             : (j < i ? ALf + 9 * (size_t)(IW1[j] - 1) : AUf + 9 * (size_t)(IW2[j] - 1));
+        for (int e = 0; e < 9; e++) dst[e] = dst[e] - RHS[e];
+      }
+    }
+    if (lu33(P->Dlu0 + 9 * (size_t)(i - 1), 1.0)) *ierr = ERR_ILU_ZERO_PIVOT;
+    for (int k = inL[i - 1]; k < inL[i]; k++) IW1[iaL[k]] = 0;
+    for (int k = inU[i - 1]; k < inU[i]; k++) IW2[iaU[k]] = 0;
+  }
+  free(IW1);
+  free(IW2);
+  free(lvL);
+  free(lvU);
+  return P;
+}
+
 /* hecmw_precond_BILU_33_apply: hecmw_precond_BILU_33.f90:90-157 (serial) */
 static void bilu0_apply(const o33_precond *P, double *WW) {
   const int N = P->N;
@@ -728,6 +925,9 @@ o33_precond *o33_precond_setup(const o33_matrix *A, int kind, int ncolor_in, dou
       o33_precond *P = bilu0_setup(A, sigma_diag, ierr);
       return P;
     }
+    case 11:
+    case 12:
+      return bilu_fill_setup(A, kind - 10, sigma_diag, ierr);
     default:
       *ierr = ERR_INCONS_PC;
       return NULL;
@@ -760,12 +960,27 @@ void o33_precond_sweep(const o33_precond *P, double *zp) {
   switch (P->kind) {
     case 1: ssor_apply(P, zp); break;
     case 3: diag_apply(P, zp); break;
-    case 10: bilu0_apply(P, zp); break;
+    case 10:
+    case 11:
+    case 12: bilu0_apply(P, zp); break;
     default: break;
   }
 }
 
 int o33_precond_ncolor(const o33_precond *P) { return P->kind == 1 ? P->ncolor : 0; }
+
+int o33_precond_bilu_pattern(const o33_precond *P, int *inL, int *iaL, int *inU, int *iaU) {
+  if (P->kind < 10 || P->kind > 12) return -1;
+  const int NP = P->NP;
+  const int nL = P->inL[NP], nU = P->inU[NP];
+  if (inL) {
+    memcpy(inL, P->inL, sizeof(int) * ((size_t)NP + 1));
+    memcpy(inU, P->inU, sizeof(int) * ((size_t)NP + 1));
+    memcpy(iaL, P->iaL, sizeof(int) * (size_t)nL);
+    memcpy(iaU, P->iaU, sizeof(int) * (size_t)nU);
+  }
+  return nL + nU;
+}
 
 void o33_precond_ordering(const o33_precond *P, int *colorindex, int *perm, int *iperm) {
   if (P->kind != 1) return;

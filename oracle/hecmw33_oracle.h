@@ -71,6 +71,9 @@ void o33_precond_apply(const o33_precond *P, const o33_matrix *A, int iterpremax
                        const double *r, double *z, double *zp);
 /* SSOR ordering queries */
 int o33_precond_ncolor(const o33_precond *P);
+/* block ILU(p) factor pattern (indexL/U of NP+1, 1-based items); with NULL arrays,
+ * only the total block count.  -1 for other preconditioners. */
+int o33_precond_bilu_pattern(const o33_precond *P, int *inL, int *iaL, int *inU, int *iaU);
 void o33_precond_ordering(const o33_precond *P, int *colorindex, int *perm, int *iperm);
 
 /* ---- hecmw_solve (hecmw1/src/solver/main/hecmw_solver.f90:9-88) restricted to

@@ -65,6 +65,8 @@ def lib():
         L.o33_precond_ncolor.argtypes = [ctypes.c_void_p]
         L.o33_precond_ncolor.restype = ctypes.c_int
         L.o33_precond_ordering.argtypes = [ctypes.c_void_p, _i32p, _i32p, _i32p]
+        L.o33_precond_bilu_pattern.argtypes = [ctypes.c_void_p, _i32p, _i32p, _i32p, _i32p]
+        L.o33_precond_bilu_pattern.restype = ctypes.c_int
         L.o33_solve.argtypes = [ctypes.POINTER(O33Matrix), _f64p, _f64p, _i32p, _f64p, ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_void_p), _i32p, _f64p, _f64p]
         L.o33_solve.restype = ctypes.c_int
@@ -167,6 +169,18 @@ class OraclePrecond:
         self.orc.L.o33_precond_apply(self.h, ctypes.byref(self.orc.mat), iterpremax, _dp(r), _dp(z),
                                      _dp(zp))
         return z
+
+    def bilu_pattern(self):
+        """(indexL, itemL, indexU, itemU) of a block ILU(p) factor."""
+        m = self.orc.m
+        self.orc.L.o33_precond_bilu_pattern(self.h, None, None, None, None)
+        inL = np.zeros(m.NP + 1, np.int32)
+        inU = np.zeros(m.NP + 1, np.int32)
+        tot = self.orc.L.o33_precond_bilu_pattern(self.h, None, None, None, None)
+        iaL = np.zeros(tot + 1, np.int32)
+        iaU = np.zeros(tot + 1, np.int32)
+        self.orc.L.o33_precond_bilu_pattern(self.h, _ip(inL), _ip(iaL), _ip(inU), _ip(iaU))
+        return inL, iaL[:inL[-1]], inU, iaU[:inU[-1]]
 
     def ordering(self):
         n = self.orc.m.N
