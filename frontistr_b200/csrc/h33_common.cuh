@@ -117,6 +117,10 @@ struct CgState {
   // residual refresh period (50 for CG, 100 for BiCGSTAB)
   double omega, c2;
   int nrecompute;
+  // ESTCOND (Iarray(14)): ALPHA and BETA of every iteration, for the Lanczos
+  // condition estimate of hecmw_solver_CG.f90:256-264 (null when off)
+  double *lanczos;
+  int lanczos_cap, lanczos_n;
   unsigned int ticket[8];
 };
 
@@ -131,6 +135,8 @@ struct CgParams {
   int reliable;  // 1: FP32 CG with FP64 reliable updates
   double ru_delta;
   int method;    // hecmw METHOD: 1 CG, 2 BiCGSTAB
+  double *lanczos;  // ESTCOND: 2 x maxit doubles (ALPHA, BETA per iteration) or null
+  int lanczos_cap;
 };
 
 }  // namespace h33

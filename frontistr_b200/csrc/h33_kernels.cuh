@@ -134,6 +134,11 @@ __device__ __forceinline__ void fin_pq(CgState *st, double c1) {
     st->done = 1;
   } else {
     st->alpha = st->rho / c1;
+    if (st->lanczos && st->iter <= st->lanczos_cap) {
+      st->lanczos[2 * (st->iter - 1)] = st->alpha;
+      st->lanczos[2 * (st->iter - 1) + 1] = st->beta;
+      st->lanczos_n = st->iter;
+    }
   }
 }
 
@@ -1007,6 +1012,9 @@ static __global__ void cg_init_kernel(CgState *st, const CgParams *prm) {
   st->ru_count = 0;
   st->ru_delta = prm->ru_delta;
   st->ru_mark = 1.0;
+  st->lanczos = prm->lanczos;
+  st->lanczos_cap = prm->lanczos_cap;
+  st->lanczos_n = 0;
   for (int i = 0; i < 8; i++) st->ticket[i] = 0u;
 }
 

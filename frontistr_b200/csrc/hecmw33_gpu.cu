@@ -18,7 +18,9 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstdlib>
+#include <limits>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -353,6 +355,11 @@ struct Solver {
   DevArray<double> gp_W;  // GPBiCG: its twelve work vectors
   DevArray<double> gr_W;  // GMRESR / GMRESREN: u, c, uin, cin (xi, eta), BFGS pairs, vecR, tmp
   DomainState dom;
+  // ESTCOND: ALPHA / BETA history of the CG (2 per iteration) and the last estimate
+  bool lanczos_on = false;
+  DevArray<double> lanczos_buf;
+  int last_lanczos_n = 0;
+  double last_emin = 0.0, last_emax = 0.0;
   DevArray<int> g_flag;
   DevArray<int> blk_row, blk_col;
   DevArray<double> raw_scaled, scale, b_unscaled;
@@ -1244,6 +1251,10 @@ float run_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels, int
   S.h_params->reliable = reliable;
   S.h_params->ru_delta = ru_delta;
   S.h_params->method = method;
+  // ESTCOND: the plain FP64-recurrence CG records ALPHA and BETA
+  const bool lanczos = S.lanczos_on && !learned && !reliable && !inner && method == 1;
+  S.h_params->lanczos = lanczos ? S.lanczos_buf.p : nullptr;
+  S.h_params->lanczos_cap = lanczos ? int(S.lanczos_buf.n / 2) : 0;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, S.stream));
   H33_CUDA(cudaEventRecord(S.ev0, S.stream));
   if (graph_mode()) {
@@ -1562,6 +1573,8 @@ float record_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels) 
   S.h_params->reliable = 0;
   S.h_params->ru_delta = 1.0;
   S.h_params->method = 1;
+  S.h_params->lanczos = nullptr;
+  S.h_params->lanczos_cap = 0;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, S.stream));
   H33_CUDA(cudaEventRecord(S.ev0, S.stream));
   launch_prologue<double>(S, V, 0, 0);
@@ -1898,6 +1911,69 @@ int prepare_solve(Solver &S, int *Iarray, double *Rarray, double *sigma, bool *a
   return 0;
 }
 
+// Sturm count of the symmetric tridiagonal matrix (d, e): how many of its eigenvalues
+// lie below x.
+int sturm_count(const std::vector<double> &d, const std::vector<double> &e, int n, double x) {
+  int c = 0;
+  double q = 1.0;
+  for (int i = 0; i < n; i++) {
+    q = d[size_t(i)] - x - (i ? e[size_t(i) - 1] * e[size_t(i) - 1] / q : 0.0);
+    if (q == 0.0) q = -std::numeric_limits<double>::min();
+    if (q < 0.0) c++;
+  }
+  return c;
+}
+
+// The k-th smallest eigenvalue (0-based) of the leading n x n tridiagonal by bisection
+// inside the Gershgorin interval, to the resolution of double precision.
+double tridiag_eigen(const std::vector<double> &d, const std::vector<double> &e, int n, int k) {
+  double lo = d[0], hi = d[0];
+  for (int i = 0; i < n; i++) {
+    const double r = (i ? std::fabs(e[size_t(i) - 1]) : 0.0) + (i + 1 < n ? std::fabs(e[size_t(i)]) : 0.0);
+    lo = std::min(lo, d[size_t(i)] - r);
+    hi = std::max(hi, d[size_t(i)] + r);
+  }
+  for (int it = 0; it < 200; it++) {
+    const double mid = 0.5 * (lo + hi);
+    if (mid <= lo || mid >= hi) break;
+    if (sturm_count(d, e, n, mid) > k) hi = mid;
+    else lo = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// hecmw_estimate_condition_CG (hecmw_estimate_condition.F90:14-99) for the ALPHA /
+// BETA history of a CG solve: the Lanczos tridiagonal of hecmw_solver_CG.f90:256-263
+// (D(1) = 1/ALPHA(1), D(k) = 1/ALPHA(k) + BETA(k)/ALPHA(k-1), E(k-1) =
+// sqrt(BETA(k))/ALPHA(k-1)), its extreme eigenvalues every ESTCOND iterations and at
+// the end of a solve without error, printed as the reference prints them.  The
+// eigenvalues come from bisection on the Sturm count (the reference calls LAPACK's
+// dstegr).
+void condition_report(Solver &S, const std::vector<double> &ab, int n, int estcond, int error) {
+  std::vector<double> d(size_t(std::max(n, 1))), e(size_t(std::max(n, 1)));
+  auto estimate = [&](int m) {
+    if (m <= 1) return;
+    const double emin = tridiag_eigen(d, e, m, 0), emax = tridiag_eigen(d, e, m, m - 1);
+    std::printf("emin=%13.6E, emax=%13.6E, emax/emin=%13.6E\n", emin, emax, emax / emin);
+    S.last_emin = emin;
+    S.last_emax = emax;
+  };
+  for (int k = 1; k <= n; k++) {
+    const double alpha = ab[2 * size_t(k - 1)], beta = ab[2 * size_t(k - 1) + 1];
+    if (k == 1) {
+      d[0] = 1.0 / alpha;
+    } else {
+      const double alpha1 = ab[2 * size_t(k - 2)];
+      d[size_t(k) - 1] = 1.0 / alpha + beta / alpha1;
+      e[size_t(k) - 2] = std::sqrt(beta) / alpha1;
+    }
+    if (k % estcond == 0) estimate(k);
+  }
+  if (error == 0) estimate(n);
+  std::fflush(stdout);
+  S.last_lanczos_n = n;
+}
+
 // hecmw_solve_GMRES (hecmw_solver_GMRES.f90:123-411) on the resident B and X in FP64:
 // right-preconditioned GMRES(NREST) with modified Gram-Schmidt and Givens rotations.
 // Returns the device-side seconds; sets *error (0 or 3001), *iter and *resid.
@@ -1927,6 +2003,8 @@ float run_gmres(Solver &S, int iterpremax, double tol, int maxit, int nrest, int
   S.h_params->inner = S.h_params->flexible = S.h_params->use_gnn = S.h_params->reliable = 0;
   S.h_params->ru_delta = 0.0;
   S.h_params->method = 3;
+  S.h_params->lanczos = nullptr;
+  S.h_params->lanczos_cap = 0;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, s));
   H33_CUDA(cudaEventRecord(S.ev0, s));
   launch_k(s, cg_init_kernel, 1, 32, st, static_cast<const CgParams *>(S.params.p));
@@ -2438,6 +2516,11 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   int method = Iarray[1];
   int learned = (Iarray[42] == 1 && method == 1) ? 1 : 0;  // the learned network runs in flexible CG
   if (learned) learned_prepare_inference(S);
+  const int ESTCOND = Iarray[13];  // hecmw_mat_get_estcond
+  S.lanczos_on = ESTCOND > 0 && method == 1 && !learned;
+  S.last_lanczos_n = 0;
+  S.last_emin = S.last_emax = 0.0;
+  if (S.lanczos_on) S.lanczos_buf.alloc(2 * size_t(std::max(MAXIT, 1)));
   if (lowp && iterPREmax > 0) ensure_lowp(S);
   else lowp = 0;
   const bool record = S.L.recording && !learned && method == 1;
@@ -2466,6 +2549,13 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
       error = st.error;
       *iter = st.iter;
       *resid = st.resid;
+      if (S.lanczos_on && method == 1 && !record) {
+        const int n = std::min(st.lanczos_n, int(S.lanczos_buf.n / 2));
+        std::vector<double> ab(2 * size_t(std::max(n, 1)));
+        if (n > 0)
+          H33_CUDA(cudaMemcpy(ab.data(), S.lanczos_buf.p, sizeof(double) * 2 * size_t(n), cudaMemcpyDeviceToHost));
+        condition_report(S, ab, n, ESTCOND, error);
+      }
     }
     scaling.x_back();  // the end of each hecmw_solve_CG call
     if (error == HECMW33_ERR_DIVERGE_PC || error == HECMW33_ERR_DIVERGE_MAT || error == HECMW33_ERR_DIVERGE_NAN) {
@@ -2493,6 +2583,7 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   }
   const double resid2 = rel_resid_device(S);
   if (resid2 < TOL) Iarray[80] = 1;
+  S.lanczos_on = false;
   S.last_learned = learned;
   S.last_fallback = S.h_state->fallback;
   S.last_iter = *iter;
@@ -2897,6 +2988,8 @@ float run_multi_chunk(Solver &S, int nrhs, const double *dB, double *dX, int ite
   S.h_params->reliable = 0;
   S.h_params->ru_delta = 0.0;
   S.h_params->method = 1;
+  S.h_params->lanczos = nullptr;
+  S.h_params->lanczos_cap = 0;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, s));
   H33_CUDA(cudaEventRecord(S.ev0, s));
   if (graph_mode()) {
@@ -3646,6 +3739,16 @@ HECMW33_API void hecmw33_gpu_colour_schedule(const int *N, const int *indexL, co
   *ncolor = ordering_mc(prof, perm_rcm, *ncolor_in, ci, pm, ipm);
   for (int c = 0; c <= *ncolor; c++) colorindex[c] = ci[c];
   for (int i = 0; i < n; i++) perm[i] = pm[i] + 1;
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_condition_estimate(const int *handle, int *n, double *emin, double *emax, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  *n = S.last_lanczos_n;
+  *emin = S.last_emin;
+  *emax = S.last_emax;
   H33_ENTRY_END
 }
 

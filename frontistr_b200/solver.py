@@ -132,6 +132,15 @@ class GpuSolver:
             self._domain_cbs[0], self._domain_cbs[1], None, ctypes.byref(err))
         self._check(err.value, fatal_only=False)
 
+    def condition_estimate(self):
+        """(n, emin, emax) of the last solve's Lanczos estimate (ESTCOND, Iarray(14));
+        n = 0 when it was off."""
+        n, lo, hi, err = ctypes.c_int(0), ctypes.c_double(0), ctypes.c_double(0), ctypes.c_int(0)
+        self.lib.hecmw33_gpu_condition_estimate(ctypes.byref(self.handle), ctypes.byref(n), ctypes.byref(lo),
+                                                ctypes.byref(hi), ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+        return n.value, lo.value, hi.value
+
     def _raise_cb_error(self):
         e = getattr(self, "_cb_error", None)
         if e is not None:

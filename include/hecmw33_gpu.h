@@ -133,6 +133,14 @@ HECMW33_API void hecmw33_gpu_set_domain(const int *handle, const int *n_neighbor
                                         hecmw33_exchange_fn exchange, hecmw33_allreduce_fn allreduce,
                                         void *ctx, int *ierr);
 
+/* Iarray(14) = ESTCOND > 0 (hecmw_solver_CG.f90:256-264, 299-301): the CG records ALPHA
+ * and BETA; every ESTCOND iterations and at the end of a solve without error the
+ * extreme eigenvalues of the Lanczos tridiagonal are printed on stdout as
+ * "emin=..., emax=..., emax/emin=..." (hecmw_estimate_condition.F90:14-99).  This call
+ * returns the last solve's number of recorded iterations (0 when off) and its last
+ * estimate. */
+HECMW33_API void hecmw33_gpu_condition_estimate(const int *handle, int *n, double *emin, double *emax, int *ierr);
+
 /* hecmw_solve (hecmw_solver.f90:9-88) for METHOD = 1-7 on the resident matrix:
  * zero-RHS check, zero-diagonal check, preconditioner recycle policy
  * (hecmw_matrix_misc.F90:858-877), preconditioner setup (PRECOND 1,2 = SSOR with the

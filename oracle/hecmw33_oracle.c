@@ -1012,8 +1012,23 @@ void o33_precond_apply(const o33_precond *P, const o33_matrix *A, int iterpremax
 /* hecmw_solve_CG: hecmw_solver_CG.f90:77-279 (scaling off, no JAD, no ESTCOND) */
 enum { N_ITER_RECOMPUTE_R = 50 };
 
+static int cg_impl(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
+                   const double *B, double *X, int *iter_out, double *resid_out, double *resid_hist,
+                   double *ab_hist);
+
 int o33_cg(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
            const double *B, double *X, int *iter_out, double *resid_out, double *resid_hist) {
+  return cg_impl(A, P, iterpremax, maxit, tol, B, X, iter_out, resid_out, resid_hist, NULL);
+}
+
+int o33_cg_lanczos(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
+                   const double *B, double *X, int *iter_out, double *resid_out, double *ab_hist) {
+  return cg_impl(A, P, iterpremax, maxit, tol, B, X, iter_out, resid_out, NULL, ab_hist);
+}
+
+static int cg_impl(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
+                   const double *B, double *X, int *iter_out, double *resid_out, double *resid_hist,
+                   double *ab_hist) {
   const int NP = A->NP, NN = 3 * A->N;
   const size_t len = 3 * (size_t)NP;
   double *R = (double *)calloc(len, sizeof(double));
@@ -1065,6 +1080,10 @@ int o33_cg(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit,
     double DNRM2 = o33_dot(NN, R, R);
     RESID = sqrt(DNRM2 / BNRM2);
     if (resid_hist) resid_hist[iter - 1] = RESID;
+    if (ab_hist) { /* the ALPHA and BETA that ESTCOND's Lanczos matrix is built from */
+      ab_hist[2 * (iter - 1)] = ALPHA;
+      ab_hist[2 * (iter - 1) + 1] = iter == 1 ? 0.0 : BETA;
+    }
     if (RESID <= tol) {
       if (iter % N_ITER_RECOMPUTE_R == 0) break;
       o33_matresid(A, X, B, R);

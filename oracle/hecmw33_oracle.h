@@ -102,6 +102,12 @@ int o33_bicgstab(const o33_matrix *A, const o33_precond *P, int iterpremax, int 
 int o33_gmres(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
               int nrest, const double *B, double *X, int *iter_out, double *resid_out);
 
+/* o33_cg that also returns ALPHA and BETA of every iteration (ab[2k], ab[2k+1]; BETA
+ * of the first iteration 0): the data of ESTCOND's Lanczos estimate
+ * (hecmw_solver_CG.f90:256-264). */
+int o33_cg_lanczos(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
+                   const double *B, double *X, int *iter_out, double *resid_out, double *ab);
+
 /* Conjugate residual iterations only (hecmw_solve_CR), given a ready preconditioner. */
 int o33_cr(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
            const double *B, double *X, int *iter_out, double *resid_out);

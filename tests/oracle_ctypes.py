@@ -73,6 +73,9 @@ def lib():
         L.o33_cg.argtypes = [ctypes.POINTER(O33Matrix), ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                              ctypes.c_double, _f64p, _f64p, _i32p, _f64p, _f64p]
         L.o33_cg.restype = ctypes.c_int
+        L.o33_cg_lanczos.argtypes = [ctypes.POINTER(O33Matrix), ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_double, _f64p, _f64p, _i32p, _f64p, _f64p]
+        L.o33_cg_lanczos.restype = ctypes.c_int
         L.o33_cg_fixed_iters.argtypes = [ctypes.POINTER(O33Matrix), ctypes.c_void_p, ctypes.c_int,
                                          ctypes.c_int, _f64p, _f64p]
         L.o33_cg_fixed_iters.restype = ctypes.c_double
@@ -190,6 +193,20 @@ class OraclePrecond:
         iperm = np.zeros(n, np.int32)
         self.orc.L.o33_precond_ordering(self.h, _ip(ci), _ip(perm), _ip(iperm))
         return ci, perm, iperm
+
+    def cg_lanczos(self, B, maxit=20000, tol=1e-8, iterpremax=1):
+        """CG that also returns ALPHA and BETA per iteration (ESTCOND's data)."""
+        orc = self.orc
+        m = orc.m
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        X = np.zeros(3 * m.NP)
+        it = ctypes.c_int(0)
+        res = ctypes.c_double(0)
+        ab = np.zeros(2 * maxit)
+        err = orc.L.o33_cg_lanczos(ctypes.byref(orc.mat), self.h, iterpremax, maxit, tol, _dp(B), _dp(X),
+                                   ctypes.byref(it), ctypes.byref(res), _dp(ab))
+        n = min(it.value, maxit)
+        return dict(X=X, error=err, iter=it.value, alpha=ab[0:2 * n:2].copy(), beta=ab[1:2 * n:2].copy())
 
     def cg(self, B, maxit=20000, tol=1e-8, iterpremax=1, X=None, hist=False, on=None):
         """CG with this preconditioner; `on` (an Oracle) selects another matrix."""

@@ -1,0 +1,76 @@
+"""ESTCOND (Iarray(14)): the Lanczos condition estimate of hecmw_solve_CG
+(hecmw_solver_CG.f90:256-264, 299-301; hecmw_estimate_condition.F90:14-99).  The CG's
+ALPHA / BETA give the tridiagonal D(k) = 1/ALPHA(k) + BETA(k)/ALPHA(k-1),
+E(k-1) = sqrt(BETA(k))/ALPHA(k-1); its extreme eigenvalues estimate those of M^-1 A.
+
+CPU: on a small box the oracle's Lanczos extremes approach the extreme eigenvalues of
+M^-1 A from a dense eigen-decomposition.  GPU: the device records ALPHA / BETA in the
+graph-captured CG; its estimate (bisection on the Sturm count) matches numpy's
+eigenvalues of the oracle's tridiagonal, the "emin=..., emax=..., emax/emin=..." lines
+are printed every ESTCOND iterations and at the end, and nothing is recorded when
+ESTCOND is 0.
+"""
+import re
+
+import numpy as np
+import pytest
+
+from frontistr_b200.matrix import IDX_I_ESTCOND
+from frontistr_b200.mesh import box_system
+from oracle_ctypes import Oracle
+
+
+def _lanczos_extremes(alpha, beta):
+    n = len(alpha)
+    d = np.empty(n)
+    e = np.empty(max(n - 1, 0))
+    d[0] = 1.0 / alpha[0]
+    for k in range(1, n):
+        d[k] = 1.0 / alpha[k] + beta[k] / alpha[k - 1]
+        e[k - 1] = np.sqrt(beta[k]) / alpha[k - 1]
+    T = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+    w = np.linalg.eigvalsh(T)
+    return w[0], w[-1]
+
+
+def test_oracle_lanczos_estimates_the_spectrum():
+    m = box_system(4, 3, 5, jitter=0.2, sigma_E=1.0, nu_range=(0.25, 0.40), seed=2)
+    o = Oracle(m)
+    pc = o.precond(1)
+    r = pc.cg_lanczos(m.B, tol=1e-12)
+    assert r["error"] == 0
+    lo, hi = _lanczos_extremes(r["alpha"], r["beta"])
+    n = 3 * m.N
+    A = np.column_stack([o.matvec(np.eye(n)[:, j]) for j in range(n)])
+    MA = np.column_stack([pc.apply(A[:, j]) for j in range(n)])
+    w = np.sort(np.linalg.eigvals(MA).real)
+    # (the largest eigenvalue, 1, belongs to the constrained rows, which the right-hand
+    # side does not excite: Lanczos approaches it from below)
+    assert abs(hi - w[-1]) <= 1e-3 * w[-1]
+    assert abs(lo - w[0]) <= 1e-3 * w[0]
+
+
+@pytest.mark.gpu
+def test_gpu_estcond(capfd):
+    from frontistr_b200.solver import GpuSolver
+    m = box_system(9, 8, 10, jitter=0.2, sigma_E=1.0, nu_range=(0.25, 0.40), seed=11)
+    m.set_iter(20000)
+    ref = Oracle(m).precond(1).cg_lanczos(m.B)
+    lo, hi = _lanczos_extremes(ref["alpha"], ref["beta"])
+    with GpuSolver() as s:
+        g = m.copy()
+        info0 = s.solve(g)
+        assert s.condition_estimate()[0] == 0
+        g = m.copy()
+        g.Iarray[IDX_I_ESTCOND - 1] = 20
+        capfd.readouterr()
+        info = s.solve(g)
+        n, emin, emax = s.condition_estimate()
+    out = capfd.readouterr().out
+    assert info["error"] == 0 and info["iter"] == info0["iter"]
+    assert abs(n - ref["iter"]) <= 2 and n == info["iter"]
+    assert abs(emin - lo) <= 1e-6 * lo and abs(emax - hi) <= 1e-6 * hi
+    lines = [l for l in out.splitlines() if l.startswith("emin=")]
+    assert len(lines) == n // 20 + 1
+    last = re.match(r"emin= ?([-+0-9.E]+), emax= ?([-+0-9.E]+), emax/emin= ?([-+0-9.E]+)", lines[-1])
+    assert last and abs(float(last.group(1)) - emin) <= 1e-6 * emin
