@@ -13,6 +13,7 @@ SIGNATURES = {
     "hecmw33_gpu_create": [_i, _i],
     "hecmw33_gpu_destroy": [_i, _i],
     "hecmw33_gpu_set_matrix": [_i, _i, _i, _i, _i, _i, _i, _i, _i, _d, _d, _d, _i, _i],
+    "hecmw33_gpu_set_mpc": [_i, _i, _i, _i, _i, _d, _d, _i],
     "hecmw33_gpu_set_domain": [_i, _i, _i, _i, _i, _i, _i, EXCHANGE_FN, ALLREDUCE_FN, _v, _i],
     "hecmw33_gpu_solve_resident": [_i, _d, _d, _i, _d, _i, _d, _d, _i],
     "hecmw33_gpu_solve_resident_device": [_i, _v, _v, _i, _d, _i, _d, _d, _i],

@@ -67,4 +67,38 @@ static __global__ void __launch_bounds__(kThreads) halo_unpack_kernel(const doub
   }
 }
 
+// MPC-CG (MPC_METHOD = 2, hecmw_solver_Iterative.f90:79-84): every product is
+// T^T A T x (hecmw_TtmatTvec_33, hecmw_solver_las_33.F90:572-586).  An MPC is a slave
+// DOF (its first term) and masters with coefficients: T x sets the slave to
+// -sum val_j x(master_j) (hecmw_Tvec_33, :442-497); T^T y zeroes the slave and adds
+// -val_j y(slave) to every master (hecmw_Ttvec_33, :504-565, an atomic scatter as the
+// reference's).  DOF indices are 0-based (3 (node-1) + dof-1); y starts as a copy of x.
+static __global__ void __launch_bounds__(kThreads) mpc_tvec_kernel(const int *__restrict__ slave,
+                                                                  const int *__restrict__ ptr,
+                                                                  const int *__restrict__ idx,
+                                                                  const double *__restrict__ val, int n_mpc,
+                                                                  const double *__restrict__ x,
+                                                                  double *__restrict__ y) {
+  pdl_entry();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_mpc; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int j = ptr[i]; j < ptr[i + 1]; j++) s = s - val[j] * x[idx[j]];
+    y[slave[i]] = s;
+  }
+}
+
+static __global__ void __launch_bounds__(kThreads) mpc_ttvec_kernel(const int *__restrict__ slave,
+                                                                   const int *__restrict__ ptr,
+                                                                   const int *__restrict__ idx,
+                                                                   const double *__restrict__ val, int n_mpc,
+                                                                   const double *__restrict__ x,
+                                                                   double *__restrict__ y) {
+  pdl_entry();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_mpc; i += gridDim.x * blockDim.x) {
+    const double xs = x[slave[i]];
+    y[slave[i]] = 0.0;
+    for (int j = ptr[i]; j < ptr[i + 1]; j++) atomicAdd(&y[idx[j]], -val[j] * xs);
+  }
+}
+
 }  // namespace h33

@@ -355,6 +355,16 @@ struct Solver {
   DevArray<double> gp_W;  // GPBiCG: its twelve work vectors
   DevArray<double> gr_W;  // GMRESR / GMRESREN: u, c, uin, cin (xi, eta), BFGS pairs, vecR, tmp
   DomainState dom;
+  // MPCs of the mesh (hecmwST_local_mesh%mpc): slave DOF, master DOFs and
+  // coefficients of every MPC whose DOFs are all 1-3, the sum of mpc_const^2; active
+  // during a solve with MPC_METHOD = 2
+  struct {
+    int n = 0;
+    bool active = false;
+    double const2 = 0.0;
+    DevArray<int> slave, ptr, idx;
+    DevArray<double> val, t, w;
+  } mpc;
   // ESTCOND: ALPHA / BETA history of the CG (2 per iteration) and the last estimate
   bool lanczos_on = false;
   DevArray<double> lanczos_buf;
@@ -496,6 +506,7 @@ void validate(int N, int NP, int NPL, int NPU, const int *indexL, const int *ite
 void set_profile(Solver &S, int N, int NPL, int NPU, const int *indexL, const int *itemL, const int *indexU,
                  const int *itemU) {
   S.has_matrix = false;
+  if (N != S.N) S.mpc.n = 0;  // the MPC DOF indices belong to the old mesh
   S.N = N;
   S.NPL = NPL;
   S.NPU = NPU;
@@ -1888,9 +1899,10 @@ void assemble_hex8(Solver &S, int n_node, const double *coords, int n_elem, cons
 
 int prepare_solve(Solver &S, int *Iarray, double *Rarray, double *sigma, bool *auto_sigma) {
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix: call hecmw33_gpu_set_matrix first");
-  // zero right-hand side (hecmw_solver.f90:32-37)
+  // zero right-hand side (hecmw_solver.f90:32-37; hecmw_solver_Iterative.f90:284-323,
+  // with the MPC constants)
   S.bnrm2 = dot_device(S, S.b.p, S.b.p);
-  if (S.bnrm2 == 0.0) {
+  if (S.bnrm2 + (S.mpc.n > 0 ? S.mpc.const2 : 0.0) == 0.0) {
     H33_CUDA(cudaMemsetAsync(S.x.p, 0, sizeof(double) * S.n3(), S.stream));
     S.sync();
     Iarray[80] = 1;
@@ -3123,6 +3135,23 @@ void halo_update(Solver &S, const double *v, double *xe) {
 // y = A v over the internal rows: halo update of v into xe, the A_II product, then
 // the interface blocks (the reference's matvec order: external columns last).
 void domain_matvec(Solver &S, const double *v, double *xe, double *y, int *launched) {
+  if (S.mpc.active) {  // y = T^T A T v (hecmw_TtmatTvec_33)
+    cudaStream_t s = S.stream;
+    const int n3 = S.n3(), gm = std::max(1, std::min((S.mpc.n + kThreads - 1) / kThreads, S.nsm * 4));
+    H33_CUDA(cudaMemcpyAsync(S.mpc.t.p, v, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    launch_k(s, mpc_tvec_kernel, gm, kThreads, static_cast<const int *>(S.mpc.slave.p),
+             static_cast<const int *>(S.mpc.ptr.p), static_cast<const int *>(S.mpc.idx.p),
+             static_cast<const double *>(S.mpc.val.p), S.mpc.n, v, S.mpc.t.p);
+    launch_k(s, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, S.A.view(), static_cast<const double *>(S.mpc.t.p),
+             S.mpc.w.p, static_cast<const double *>(nullptr), static_cast<CgState *>(nullptr),
+             static_cast<double *>(nullptr));
+    H33_CUDA(cudaMemcpyAsync(y, S.mpc.w.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    launch_k(s, mpc_ttvec_kernel, gm, kThreads, static_cast<const int *>(S.mpc.slave.p),
+             static_cast<const int *>(S.mpc.ptr.p), static_cast<const int *>(S.mpc.idx.p),
+             static_cast<const double *>(S.mpc.val.p), S.mpc.n, static_cast<const double *>(S.mpc.w.p), y);
+    *launched += 3;
+    return;
+  }
   halo_update(S, v, xe);
   launch_k(S.stream, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, S.A.view(), v, y,
            static_cast<const double *>(nullptr), static_cast<CgState *>(nullptr), static_cast<double *>(nullptr));
@@ -3260,17 +3289,32 @@ float run_cg_domain(Solver &S, int iterpremax, double tol, int maxit, int *error
 // and zero-diagonal checks (hecmw_solver_Iterative.f90:255-323), the recycle policy
 // and the local preconditioner, CG, the sigma_diag retry of a diverged ILU, and the
 // allreduced true residual.
+struct MpcScope {  // the MPC operator for the duration of a solve
+  Solver &S;
+  MpcScope(Solver &s, bool on) : S(s) { S.mpc.active = on; }
+  ~MpcScope() { S.mpc.active = false; }
+};
+
 int solve_domain(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
   const double t0 = wall();
   *iter = 0;
   *resid = 0.0;
   if (times) times[0] = times[1] = times[2] = 0.0;
-  if (Iarray[1] != 1) throw Failure(HECMW33_ERR_BAD_INPUT, "a decomposed domain runs CG (METHOD = 1)");
+  const bool mpc = S.mpc.n > 0 && Iarray[12] == 2;
+  const char *what = S.dom.on ? "a decomposed domain" : "MPC-CG (MPC_METHOD = 2)";
+  if (mpc && S.dom.on) throw Failure(HECMW33_ERR_BAD_INPUT, "MPC-CG runs on a whole (one-domain) mesh");
+  if (Iarray[1] != 1) throw Failure(HECMW33_ERR_BAD_INPUT, std::string(what) + " runs CG (METHOD = 1)");
   if (Iarray[41] != 0 || Iarray[42] != 0)
-    throw Failure(HECMW33_ERR_BAD_INPUT, "a decomposed domain runs the FP64 CG (Iarray(42) = Iarray(43) = 0)");
-  if (Iarray[6] != 0) throw Failure(HECMW33_ERR_BAD_INPUT, "a decomposed domain runs with SCALING=NO");
+    throw Failure(HECMW33_ERR_BAD_INPUT, std::string(what) + " runs the FP64 CG (Iarray(42) = Iarray(43) = 0)");
+  if (Iarray[6] != 0) throw Failure(HECMW33_ERR_BAD_INPUT, std::string(what) + " runs with SCALING=NO");
+  if (mpc) {
+    S.mpc.t.alloc(size_t(S.n3()));
+    S.mpc.w.alloc(size_t(S.n3()));
+  }
+  MpcScope mpc_scope(S, mpc);
   DomainState &d = S.dom;
-  const double bb = domain_allreduce(S, dot_device(S, S.b.p, S.b.p));
+  // hecmw_solve_check_zerorhs adds the MPC constants (hecmw_solver_Iterative.f90:305-309)
+  const double bb = domain_allreduce(S, dot_device(S, S.b.p, S.b.p) + (S.mpc.n > 0 ? S.mpc.const2 : 0.0));
   S.bnrm2 = bb;
   if (bb == 0.0) {
     H33_CUDA(cudaMemsetAsync(S.x.p, 0, sizeof(double) * S.n3(), S.stream));
@@ -3331,7 +3375,7 @@ int solve_domain(Solver &S, int *Iarray, double *Rarray, int *iter, double *resi
 }
 
 int solve_resident(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid, double *times) {
-  if (S.dom.on) return solve_domain(S, Iarray, Rarray, iter, resid, times);
+  if (S.dom.on || (S.mpc.n > 0 && Iarray[12] == 2)) return solve_domain(S, Iarray, Rarray, iter, resid, times);
   if (Iarray[6] != 0 && (Iarray[41] == 2 || Iarray[41] == 3))
     throw Failure(HECMW33_ERR_BAD_INPUT, "SCALING=YES is implemented for the FP64 CG (Iarray(42) = 0 or 1)");
   if (Iarray[1] >= 2 && (Iarray[41] == 2 || Iarray[41] == 3))
@@ -3482,6 +3526,53 @@ HECMW33_API void hecmw33_gpu_set_domain(const int *handle, const int *n_neighbor
   d.allreduce = allreduce;
   d.ctx = ctx;
   d.has_table = nn > 0;
+  S.sync();
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_set_mpc(const int *handle, const int *n_mpc, const int *mpc_index, const int *mpc_item,
+                                     const int *mpc_dof, const double *mpc_val, const double *mpc_const,
+                                     int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "set_mpc: set the matrix first");
+  const int n = n_mpc ? *n_mpc : 0;
+  if (n < 0) throw Failure(HECMW33_ERR_BAD_INPUT, "n_mpc < 0");
+  std::vector<int> slave, ptr{0}, idx;
+  std::vector<double> val;
+  double c2 = 0.0;
+  if (n > 0) {
+    if (!mpc_index || !mpc_item || !mpc_dof || !mpc_val) throw Failure(HECMW33_ERR_BAD_INPUT, "set_mpc: null array");
+    if (mpc_index[0] != 0) throw Failure(HECMW33_ERR_BAD_INPUT, "set_mpc: mpc_index(0) must be 0");
+    const int nn = S.N;
+    for (int i = 0; i < n; i++) {
+      const int j0 = mpc_index[i], j1 = mpc_index[i + 1];
+      if (j1 <= j0) throw Failure(HECMW33_ERR_BAD_INPUT, "set_mpc: an MPC without terms");
+      bool skip = false;  // an MPC with a DOF above 3 is left out (hecmw_solver_las_33.F90:479-481)
+      for (int j = j0; j < j1; j++) {
+        if (mpc_item[j] < 1 || mpc_item[j] > nn || mpc_dof[j] < 1)
+          throw Failure(HECMW33_ERR_BAD_INPUT, "set_mpc: MPC term outside the mesh");
+        if (mpc_dof[j] > 3) skip = true;
+      }
+      if (skip) continue;
+      slave.push_back(3 * (mpc_item[j0] - 1) + mpc_dof[j0] - 1);
+      for (int j = j0 + 1; j < j1; j++) {
+        idx.push_back(3 * (mpc_item[j] - 1) + mpc_dof[j] - 1);
+        val.push_back(mpc_val[j]);
+      }
+      ptr.push_back(int(idx.size()));
+    }
+    if (mpc_const)
+      for (int i = 0; i < n; i++) c2 = c2 + mpc_const[i] * mpc_const[i];
+  }
+  S.mpc.n = int(slave.size());
+  S.mpc.const2 = c2;
+  S.mpc.slave.upload(slave, S.stream);
+  S.mpc.ptr.upload(ptr, S.stream);
+  S.mpc.idx.upload(idx, S.stream);
+  S.mpc.val.upload(val, S.stream);
   S.sync();
   H33_ENTRY_END
 }

@@ -22,6 +22,7 @@ IDX_I_ITERPREMAX = 5
 IDX_I_NREST = 6
 IDX_I_SCALING = 7
 IDX_I_METHOD2 = 8
+IDX_I_MPC_METHOD = 13
 IDX_I_ESTCOND = 14
 IDX_I_ITERLOG = 21
 IDX_I_TIMELOG = 22
@@ -94,6 +95,7 @@ class HecMatrix:
         self.X = np.zeros(3 * self.NP) if X is None else np.ascontiguousarray(X, dtype=np.float64)
         self.Iarray, self.Rarray = default_iarray_rarray()
         self.coords = None
+        self.mpc = None  # (mpc_index, mpc_item, mpc_dof, mpc_val, mpc_const) of the mesh, if any
 
     @classmethod
     def empty(cls, n, npl, npu):
@@ -134,6 +136,7 @@ class HecMatrix:
                       self.B.copy(), self.X.copy())
         m.Iarray, m.Rarray = self.Iarray.copy(), self.Rarray.copy()
         m.coords = self.coords
+        m.mpc = getattr(self, "mpc", None)
         return m
 
     def to_scipy(self):

@@ -86,6 +86,21 @@ class GpuSolver:
         self._check(err.value)
         self.N = m.N
 
+    def set_mpc(self, index, item, dof, val, const=None):
+        """The mesh's MPCs (hecmwST_local_mesh%mpc: mpc_index(0:n), 1-based mpc_item,
+        mpc_dof, mpc_val, mpc_const; the first term of an MPC is its slave) for the
+        resident matrix: a solve with MPC_METHOD = Iarray(13) = 2 runs MPC-CG, whose
+        products are T^T A T x (hecmw33_gpu_set_mpc)."""
+        ix = np.ascontiguousarray(index, dtype=np.int32)
+        it = np.ascontiguousarray(item, dtype=np.int32)
+        df = np.ascontiguousarray(dof, dtype=np.int32)
+        vl = np.ascontiguousarray(val, dtype=np.float64)
+        cs = np.zeros(len(ix) - 1) if const is None else np.ascontiguousarray(const, dtype=np.float64)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_set_mpc(ctypes.byref(self.handle), _i(len(ix) - 1), _ip(ix), _ip(it), _ip(df),
+                                     _dp(vl), _dp(cs), ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+
     def set_domain(self, comm, endpoint):
         """The communication table (domain.CommTable) of the resident domain matrix
         (N < NP) and its exchanges: endpoint.exchange(send) -> recv and

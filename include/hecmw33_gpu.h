@@ -119,6 +119,19 @@ HECMW33_API void hecmw33_gpu_set_matrix(const int *handle, const int *N, const i
                                         const double *D, const double *AL, const double *AU,
                                         const int *Iarray, int *ierr);
 
+/* The MPCs of the mesh (hecmwST_local_mesh%mpc, hecmw1/src/common/hecmw_util_f.F90:98-103):
+ * mpc_index(0:n_mpc), then per term the 1-based node mpc_item, its DOF mpc_dof and the
+ * coefficient mpc_val (the first term of an MPC is its slave); mpc_const(n_mpc) (may
+ * be NULL) enters the zero-RHS check.  MPCs with a DOF above 3 are left out, as
+ * hecmw_Tvec_33 does.  With MPC_METHOD = Iarray(13) = 2 the solve is MPC-CG
+ * (hecmw_solver_Iterative.f90:79-84): CG (METHOD = 1, FP64, SCALING=NO) whose products
+ * are T^T A T x (hecmw_TtmatTvec_33, hecmw_solver_las_33.F90:572-586), the true
+ * residual included.  Kept across value updates; a matrix of another N drops them;
+ * n_mpc = 0 clears them.  One whole (one-domain) mesh. */
+HECMW33_API void hecmw33_gpu_set_mpc(const int *handle, const int *n_mpc, const int *mpc_index, const int *mpc_item,
+                                     const int *mpc_dof, const double *mpc_val, const double *mpc_const,
+                                     int *ierr);
+
 /* The communication table of the handle's domain (hecmwST_local_mesh:
  * n_neighbor_pe, neighbor_pe, import_index(0:n), import_item, export_index(0:n),
  * export_item; items are 1-based local node ids, imports in N+1..NP, exports in 1..N)

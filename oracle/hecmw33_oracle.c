@@ -71,7 +71,46 @@ int o33_max_threads(void) {
 /* ------------------------------------------------------------------------ */
 /* hecmw_matvec_33_inner, CPU branch: hecmw_solver_las_33.F90:279-311.
  * Row i: D block first, then L blocks in ascending order, then U blocks. */
+static void matvec_plain(const o33_matrix *A, const double *X, double *Y);
+
+/* hecmw_Tvec_33 / hecmw_Ttvec_33 (hecmw_solver_las_33.F90:442-565): Y = X over the
+ * internal DOFs, then for every MPC whose DOFs are all 1-3 (first term the slave):
+ * Tvec sets Y(slave) = -sum val_j X(master_j); Ttvec zeroes Y(slave) and subtracts
+ * val_j X(slave) from each Y(master_j), MPC by MPC in order. */
+static void mpc_t(const o33_matrix *A, const double *X, double *Y, int transpose) {
+  const int n = 3 * A->N;
+  for (int i = 0; i < n; i++) Y[i] = X[i];
+  for (int i = 0; i < A->n_mpc; i++) {
+    int skip = 0;
+    for (int j = A->mpc_index[i]; j < A->mpc_index[i + 1]; j++)
+      if (A->mpc_dof[j] > 3) skip = 1;
+    if (skip) continue;
+    const int k = A->mpc_index[i];
+    const int kk = 3 * (A->mpc_item[k] - 1) + A->mpc_dof[k] - 1;
+    Y[kk] = 0.0;
+    for (int j = k + 1; j < A->mpc_index[i + 1]; j++) {
+      const int jj = 3 * (A->mpc_item[j] - 1) + A->mpc_dof[j] - 1;
+      if (transpose) Y[jj] = Y[jj] - A->mpc_val[j] * X[kk];
+      else Y[kk] = Y[kk] - A->mpc_val[j] * X[jj];
+    }
+  }
+}
+
 void o33_matvec(const o33_matrix *A, const double *X, double *Y) {
+  if (A->mpc_matvec && A->n_mpc > 0) { /* hecmw_matvec_33: hecmw_solver_las_33.F90:50-53 */
+    const size_t n = 3 * (size_t)A->NP;
+    double *T = (double *)calloc(n, sizeof(double)), *W = (double *)calloc(n, sizeof(double));
+    mpc_t(A, X, T, 0);
+    matvec_plain(A, T, W);
+    mpc_t(A, W, Y, 1);
+    free(T);
+    free(W);
+    return;
+  }
+  matvec_plain(A, X, Y);
+}
+
+static void matvec_plain(const o33_matrix *A, const double *X, double *Y) {
   if (A->usejad) { /* hecmw_solver_las_33.F90:155-158, while hecmw_solve_CG holds the
                      * JAD copy (hecmw_solver_CG.f90:112-113,295-296) */
     o33_matvec_jad(A, X, Y);
@@ -1899,6 +1938,8 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
   double rhs = 0.0;
   for (int i = 0; i < N; i++)
     for (int j = 0; j < 3; j++) rhs = rhs + B[3 * i + j] * B[3 * i + j];
+  if (A->n_mpc > 0 && A->mpc_const) /* :305-309 */
+    for (int i = 0; i < A->n_mpc; i++) rhs = rhs + A->mpc_const[i] * A->mpc_const[i];
   if (rhs == 0.0) {
     for (size_t i = 0; i < 3 * (size_t)NP; i++) X[i] = 0.0;
     Iarray[80] = 1;
@@ -1947,6 +1988,7 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
   As.usejad = Iarray[32] != 0; /* IDX_I_USEJAD: the solver's products; the final true
                                  * residual below uses the plain matvec, as the
                                  * reference's after hecmw_JAD_FINALIZE */
+  As.mpc_matvec = A->n_mpc > 0 && Iarray[12] == 2; /* IDX_I_MPC_METHOD: MPC-CG (:79-84) */
   const o33_matrix *Aw = &As;
   const double *Bw = SCALING ? Bs : B;
 
@@ -2018,7 +2060,10 @@ int o33_solve(const o33_matrix *A, const double *B, double *X, int *Iarray, doub
   free(ALs);
   free(AUs);
   free(Bs);
-  const double resid2 = o33_rel_resid_L2(A, X, B);
+  /* the true residual (:153) runs before the MPC flag is cleared (:163-166) */
+  o33_matrix Ar = *A;
+  Ar.mpc_matvec = A->n_mpc > 0 && Iarray[12] == 2;
+  const double resid2 = o33_rel_resid_L2(&Ar, X, B);
   if (resid2 < TOL) Iarray[80] = 1;
   *iter_out = iter;
   *resid_out = resid;

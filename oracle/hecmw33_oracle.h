@@ -34,6 +34,13 @@ typedef struct {
   /* USEJAD (Iarray(33)): products in the jagged-diagonal order of
    * hecmw1/src/solver/las/hecmw_jadm_33.f90 (o33_solve sets it from Iarray) */
   int usejad;
+  /* the mesh's MPCs (hecmwST_local_mesh%mpc: mpc_index(0:n_mpc), 1-based items, DOFs,
+   * coefficients, constants); mpc_matvec: products are T^T A T x
+   * (hecmw_TtmatTvec_33; o33_solve sets it for MPC_METHOD = Iarray(13) = 2) */
+  int n_mpc;
+  const int *mpc_index, *mpc_item, *mpc_dof;
+  const double *mpc_val, *mpc_const;
+  int mpc_matvec;
 } o33_matrix;
 
 /* ---- kernels of hecmw1/src/solver/las/hecmw_solver_las_33.F90 ---- */

@@ -20,7 +20,9 @@ _f64p = ctypes.POINTER(ctypes.c_double)
 class O33Matrix(ctypes.Structure):
     _fields_ = [("N", ctypes.c_int), ("NP", ctypes.c_int), ("NPL", ctypes.c_int),
                 ("NPU", ctypes.c_int), ("indexL", _i32p), ("itemL", _i32p), ("indexU", _i32p),
-                ("itemU", _i32p), ("D", _f64p), ("AL", _f64p), ("AU", _f64p), ("usejad", ctypes.c_int)]
+                ("itemU", _i32p), ("D", _f64p), ("AL", _f64p), ("AU", _f64p), ("usejad", ctypes.c_int),
+                ("n_mpc", ctypes.c_int), ("mpc_index", _i32p), ("mpc_item", _i32p), ("mpc_dof", _i32p),
+                ("mpc_val", _f64p), ("mpc_const", _f64p), ("mpc_matvec", ctypes.c_int)]
 
 
 UPDATE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, _f64p)
@@ -102,6 +104,14 @@ class Oracle:
         self.m = m
         self.mat = O33Matrix(m.N, m.NP, m.NPL, m.NPU, _ip(m.indexL), _ip(m.itemL), _ip(m.indexU),
                              _ip(m.itemU), _dp(m.D), _dp(m.AL), _dp(m.AU))
+        mpc = getattr(m, "mpc", None)  # (index, item, dof, val, const) of the mesh's MPCs
+        if mpc is not None:
+            self._mpc = tuple(np.ascontiguousarray(a, dtype=t) for a, t in
+                              zip(mpc, (np.int32, np.int32, np.int32, np.float64, np.float64)))
+            ix, it, dof, val, const = self._mpc
+            self.mat.n_mpc = len(ix) - 1
+            self.mat.mpc_index, self.mat.mpc_item, self.mat.mpc_dof = _ip(ix), _ip(it), _ip(dof)
+            self.mat.mpc_val, self.mat.mpc_const = _dp(val), _dp(const)
         self.L = lib()
 
     def matvec(self, x):
