@@ -81,6 +81,15 @@ module hecmw_solver_gpu33
       integer(c_int), intent(out) :: ierr
     end subroutine hecmw33_gpu_set_domain
 
+    subroutine hecmw33_gpu_set_mpc(handle, n_mpc, mpc_index, mpc_item, mpc_dof, mpc_val, mpc_const, ierr) &
+        bind(C, name="hecmw33_gpu_set_mpc")
+      import :: c_int, c_double
+      integer(c_int), intent(in) :: handle, n_mpc
+      integer(c_int), intent(in) :: mpc_index(*), mpc_item(*), mpc_dof(*)
+      real(c_double), intent(in) :: mpc_val(*), mpc_const(*)
+      integer(c_int), intent(out) :: ierr
+    end subroutine hecmw33_gpu_set_mpc
+
     subroutine hecmw33_gpu_solve_resident(handle, B, X, Iarray, Rarray, iter, resid, times, ierr) &
         bind(C, name="hecmw33_gpu_solve_resident")
       import :: c_int, c_double
@@ -115,7 +124,16 @@ contains
     ! (hecmw_solver_Iterative.f90:90, DUMPTYPE of !SOLVER) and the solution after it
     ! (:160); both return at once when no dump is requested
     call hecmw_mat_dump(hecMAT, hecMESH)
-    if (hecMAT%N == hecMAT%NP) then
+    if (hecMAT%N == hecMAT%NP .and. hecMESH%mpc%n_mpc > 0) then
+      ! the mesh's MPCs: MPC-CG when MPC_METHOD = 2 (hecmw_solver_Iterative.f90:79-84)
+      call hecmw33_gpu_set_matrix(gpu_handle, hecMAT%N, hecMAT%NP, hecMAT%indexL(hecMAT%NP), &
+        hecMAT%indexU(hecMAT%NP), hecMAT%indexL, hecMAT%itemL, hecMAT%indexU, hecMAT%itemU, &
+        hecMAT%D, hecMAT%AL, hecMAT%AU, hecMAT%Iarray, ierr)
+      if (ierr == 0) call hecmw33_gpu_set_mpc(gpu_handle, hecMESH%mpc%n_mpc, hecMESH%mpc%mpc_index, &
+        hecMESH%mpc%mpc_item, hecMESH%mpc%mpc_dof, hecMESH%mpc%mpc_val, hecMESH%mpc%mpc_const, ierr)
+      if (ierr == 0) call hecmw33_gpu_solve_resident(gpu_handle, hecMAT%B, hecMAT%X, hecMAT%Iarray, &
+        hecMAT%Rarray, iter, resid, times, ierr)
+    else if (hecMAT%N == hecMAT%NP) then
       call hecmw33_gpu_solve(gpu_handle, hecMAT%N, hecMAT%NP, hecMAT%indexL(hecMAT%NP), &
         hecMAT%indexU(hecMAT%NP), hecMAT%indexL, hecMAT%itemL, hecMAT%indexU, hecMAT%itemU, &
         hecMAT%D, hecMAT%AL, hecMAT%AU, hecMAT%B, hecMAT%X, hecMAT%Iarray, hecMAT%Rarray, &
