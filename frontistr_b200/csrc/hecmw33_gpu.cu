@@ -359,7 +359,8 @@ struct Solver {
   // coefficients of every MPC whose DOFs are all 1-3, the sum of mpc_const^2; active
   // during a solve with MPC_METHOD = 2
   struct {
-    int n = 0;
+    int n = 0;      // MPCs the T operator applies
+    int n_raw = 0;  // hecMESH%mpc%n_mpc as given (the zero-RHS check's condition)
     bool active = false;
     double const2 = 0.0;
     DevArray<int> slave, ptr, idx;
@@ -506,7 +507,7 @@ void validate(int N, int NP, int NPL, int NPU, const int *indexL, const int *ite
 void set_profile(Solver &S, int N, int NPL, int NPU, const int *indexL, const int *itemL, const int *indexU,
                  const int *itemU) {
   S.has_matrix = false;
-  if (N != S.N) S.mpc.n = 0;  // the MPC DOF indices belong to the old mesh
+  if (N != S.N) S.mpc.n = S.mpc.n_raw = 0;  // the MPC DOF indices belong to the old mesh
   S.N = N;
   S.NPL = NPL;
   S.NPU = NPU;
@@ -1902,7 +1903,7 @@ int prepare_solve(Solver &S, int *Iarray, double *Rarray, double *sigma, bool *a
   // zero right-hand side (hecmw_solver.f90:32-37; hecmw_solver_Iterative.f90:284-323,
   // with the MPC constants)
   S.bnrm2 = dot_device(S, S.b.p, S.b.p);
-  if (S.bnrm2 + (S.mpc.n > 0 ? S.mpc.const2 : 0.0) == 0.0) {
+  if (S.bnrm2 + (S.mpc.n_raw > 0 ? S.mpc.const2 : 0.0) == 0.0) {
     H33_CUDA(cudaMemsetAsync(S.x.p, 0, sizeof(double) * S.n3(), S.stream));
     S.sync();
     Iarray[80] = 1;
@@ -3314,7 +3315,7 @@ int solve_domain(Solver &S, int *Iarray, double *Rarray, int *iter, double *resi
   MpcScope mpc_scope(S, mpc);
   DomainState &d = S.dom;
   // hecmw_solve_check_zerorhs adds the MPC constants (hecmw_solver_Iterative.f90:305-309)
-  const double bb = domain_allreduce(S, dot_device(S, S.b.p, S.b.p) + (S.mpc.n > 0 ? S.mpc.const2 : 0.0));
+  const double bb = domain_allreduce(S, dot_device(S, S.b.p, S.b.p) + (S.mpc.n_raw > 0 ? S.mpc.const2 : 0.0));
   S.bnrm2 = bb;
   if (bb == 0.0) {
     H33_CUDA(cudaMemsetAsync(S.x.p, 0, sizeof(double) * S.n3(), S.stream));
@@ -3568,6 +3569,7 @@ HECMW33_API void hecmw33_gpu_set_mpc(const int *handle, const int *n_mpc, const 
       for (int i = 0; i < n; i++) c2 = c2 + mpc_const[i] * mpc_const[i];
   }
   S.mpc.n = int(slave.size());
+  S.mpc.n_raw = n;
   S.mpc.const2 = c2;
   S.mpc.slave.upload(slave, S.stream);
   S.mpc.ptr.upload(ptr, S.stream);
