@@ -9,6 +9,8 @@ CPU: the oracle's MPC-CG converges, and T x equals a dense solve of the reduced 
 (the non-slave DOFs of T^T A T) and satisfies every MPC.  GPU: the device MPC-CG
 matches the oracle (iterations within 2, T x within 1e-8 relative, its true residual
 below the tolerance); registered MPCs with another MPC_METHOD leave the solve as it is.
+Both: the MPC constants enter the zero-RHS check (a zero B with nonzero constants is
+solved, X = 0, without the 2002 warning).
 """
 import numpy as np
 import pytest
@@ -16,7 +18,6 @@ import pytest
 from frontistr_b200.matrix import IDX_I_MPC_METHOD
 from frontistr_b200.mesh import box_system
 from oracle_ctypes import Oracle
-from test_bicgstab import _flags
 
 NX, NY, NZ = 6, 5, 8
 
@@ -139,3 +140,34 @@ def test_gpu_mpc_other_method_is_the_plain_solve():
         info = s.solve_resident(g.B, g.X, g.Iarray, g.Rarray)
     assert info["error"] == 0 and abs(info["iter"] - ref["iter"]) <= 2
     assert np.linalg.norm(g.X - ref["X"]) <= 1e-8 * np.linalg.norm(ref["X"])
+
+
+def _zero_rhs_case(const):
+    m, mpc = _system()
+    m.B[:] = 0.0
+    mpc = mpc[:4] + (np.full(len(mpc[0]) - 1, const),)
+    m.mpc = mpc
+    return m, mpc
+
+
+def test_oracle_mpc_constants_in_the_zero_rhs_check():
+    """hecmw_solve_check_zerorhs adds sum mpc_const^2 (hecmw_solver_Iterative.f90:305-309)."""
+    m, _ = _zero_rhs_case(0.0)
+    assert Oracle(m).solve()["error"] == 2002
+    m, _ = _zero_rhs_case(0.5)
+    r = Oracle(m).solve()
+    assert r["error"] == 0 and not np.any(r["X"])
+
+
+@pytest.mark.gpu
+def test_gpu_mpc_constants_in_the_zero_rhs_check():
+    from frontistr_b200.solver import GpuSolver
+    for const, code in ((0.0, 2002), (0.5, 0)):
+        m, mpc = _zero_rhs_case(const)
+        ref = Oracle(m).solve()
+        with GpuSolver() as s:
+            s.set_matrix(m)
+            s.set_mpc(*mpc)
+            info = s.solve_resident(m.B, m.X, m.Iarray, m.Rarray)
+        assert info["error"] == ref["error"] == code
+        assert not np.any(m.X)
