@@ -14,7 +14,8 @@ neighbour's import list); one domain reproduces the one-domain oracle bit for bi
 GpuSolver handle driven by its own thread on the one GPU (the domains exchange
 through the host, no kernel waits on another) against the oracle: the same iteration
 count within 2, solution within 1e-8 relative, the global true residual below the
-tolerance, also with two outer preconditioner passes; and the options a domain does
+tolerance, also with two outer preconditioner passes; the same as two processes with
+a handle each, exchanging over torch.distributed (gloo); and the options a domain does
 not run are refused (9101).
 """
 import os
@@ -226,3 +227,48 @@ def test_gpu_domain_refuses_other_options():
         with pytest.raises(HecmwSolverError) as e:
             _gpu_domains(doms, change)
         assert e.value.code == 9101
+
+
+def _gpu_rank(rank, world, port, out):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    from datetime import timedelta
+    from frontistr_b200.domain import TorchExchange
+    from frontistr_b200.solver import GpuSolver
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        dom = _domains(_system(seed=7), world, 1)[rank]
+        m = dom.matrix.copy()
+        with GpuSolver() as s:
+            s.set_matrix(m)
+            s.set_domain(dom.comm, TorchExchange(dom.comm))
+            info = s.solve_resident(m.B, m.X, m.Iarray, m.Rarray)
+        out[rank] = (info["error"], info["iter"], m.X.tolist())
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_gpu_domains_as_processes_over_gloo():
+    """One process and handle per domain, the exchanges over torch.distributed (gloo,
+    host buffers), as ranks of a distributed run; here both ranks share the one GPU
+    (their kernels never wait on each other)."""
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as man:
+        out = man.dict()
+        mp.start_processes(_gpu_rank, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+        res = dict(out)
+    m = _system(seed=7)
+    doms = _domains(m, 2, 1)
+    ref = solve_dd_threads(doms)
+    X = gather_solution(doms, [np.array(res[k][2]) for k in range(2)], m.N)
+    Xo = gather_solution(doms, [r["X"] for r in ref], m.N)
+    for k in range(2):
+        assert res[k][0] == ref[k]["error"] == 0 and abs(res[k][1] - ref[k]["iter"]) <= 2
+    assert _rel(X, Xo) <= 1e-8
+    assert Oracle(m).rel_resid(X, m.B) <= 1.0e-8
