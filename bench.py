@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-multi", action="store_true", help="skip the 16-load-case multi-RHS measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-system batched measurement")
     ap.add_argument("--no-assembly", action="store_true", help="skip the HEX8 assembly measurement")
+    ap.add_argument("--no-domains", action="store_true", help="skip the decomposed-mesh measurement")
     ap.add_argument("--no-config3", action="store_true",
                     help="skip the mixed-precision measurement on the jittered heterogeneous 80^3 system")
     ap.add_argument("--batch-systems", type=int, default=256)
@@ -315,6 +316,63 @@ def bench_config3(tol=1e-10):
                                   "true_resid": info["true_resid"],
                                   "rel_err_vs_fp64": float(np.linalg.norm(g.X - ref) / np.linalg.norm(ref))}
     return out
+
+
+def bench_domains(m, solver, ndom=2):
+    """The cube as `ndom` domains of a decomposed mesh (slabs of node ids,
+    domain.partition): each a GpuSolver handle driven by its own thread on this GPU,
+    exchanging halos and sums through the host (LocalExchange), FP64 CG + SSOR of every
+    domain's internal block to 1e-8.  Wall time of the concurrent solves; iterations
+    against the one-domain solve's (the local SSOR changes them, as in the reference);
+    the true residual of the gathered solution on the whole matrix."""
+    import threading
+    import numpy as np
+    from frontistr_b200.domain import LocalExchange, gather_solution, partition
+    from frontistr_b200.matrix import default_iarray_rarray
+    from frontistr_b200.solver import GpuSolver
+    t0 = time.perf_counter()
+    doms = partition(m, ndom)
+    t_part = time.perf_counter() - t0
+    ex = LocalExchange(doms, timeout=600.0)
+    mats, solvers = [], []
+    for k, d in enumerate(doms):
+        lm = d.matrix.copy()
+        lm.Iarray, lm.Rarray = default_iarray_rarray()
+        lm.set_iter(20000)
+        lm.set_resid(1e-8)
+        s = GpuSolver()
+        s.set_matrix(lm)
+        s.set_domain(d.comm, ex.endpoint(k))
+        mats.append(lm)
+        solvers.append(s)
+    out, errs = [None] * ndom, []
+
+    def run(k):
+        try:
+            out[k] = solvers[k].solve_resident(mats[k].B, mats[k].X, mats[k].Iarray, mats[k].Rarray)
+        except BaseException as e:  # noqa: BLE001 -- re-raised below
+            errs.append(e)
+            ex.barrier.abort()
+
+    threads = [threading.Thread(target=run, args=(k,)) for k in range(ndom)]
+    t0 = time.perf_counter()
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    wall = time.perf_counter() - t0
+    for s in solvers:
+        s.close()
+    if errs:
+        raise errs[0]
+    X = gather_solution(doms, [lm.X for lm in mats], m.N)
+    r = m.B[:3 * m.N] - solver.matvec(X)[:3 * m.N]
+    return {"workload": "the same cube as %d slab domains (N internal of NP nodes each), one GPU handle and "
+                        "host thread per domain on this GPU, halo exchange and sums through the host" % ndom,
+            "domains": ndom, "nodes": [[d.N, d.NP] for d in doms], "partition_s": t_part, "wall_s": wall,
+            "errors": [o["error"] for o in out], "iterations": [o["iter"] for o in out],
+            "device_solve_s": [o["t_solve"] for o in out],
+            "true_resid": float(np.linalg.norm(r) / np.linalg.norm(m.B[:3 * m.N]))}
 
 
 def bench_assembly(n=64, seed=3):
@@ -741,11 +799,12 @@ def main():
     if world > 1:
         # the 16-load-case, batched and config-3 figures are single-GPU measurements
         # reported at N = 1; replicas only repeat the headline
-        args.no_multi = args.no_batched = args.no_config3 = args.no_assembly = True
+        args.no_multi = args.no_batched = args.no_config3 = args.no_assembly = args.no_domains = True
     multi = None if args.no_multi else bench_multi(solver, m)
     config3 = None if args.no_config3 else bench_config3()
     assembly = None if args.no_assembly else bench_assembly()
     batched = None if args.no_batched else bench_batched(args)
+    domains = None if args.no_domains else bench_domains(m, solver)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -788,6 +847,7 @@ def main():
             "mixed_config3": config3,
             "assembly": assembly,
             "batched": batched,
+            "domains": domains,
         }
         print(json.dumps(line))
     solver.close()

@@ -72,19 +72,29 @@ class Domain:
         return self.matrix.NP
 
 
-def _global_rows(m):
-    """Per global row: (columns, 9-value blocks) in ascending column order, 0-based."""
-    D = m.D.reshape(-1, 9)
-    AL = m.AL.reshape(-1, 9)
-    AU = m.AU.reshape(-1, 9)
-    rows = []
-    for i in range(m.N):
-        lo, hi = m.indexL[i], m.indexL[i + 1]
-        ulo, uhi = m.indexU[i], m.indexU[i + 1]
-        cols = np.concatenate([m.itemL[lo:hi] - 1, [i], m.itemU[ulo:uhi] - 1]).astype(np.int64)
-        vals = np.concatenate([AL[lo:hi], D[i:i + 1], AU[ulo:uhi]])
-        rows.append((cols, vals))
-    return rows
+def _global_csr(m):
+    """The whole block matrix as CSR over nodes, each row in ascending column order
+    (L, D, U): row pointer, 0-based columns, 9-value blocks."""
+    n = m.N
+    nl = np.diff(m.indexL[:n + 1]).astype(np.int64)
+    nu = np.diff(m.indexU[:n + 1]).astype(np.int64)
+    cnt = nl + 1 + nu
+    ptr = np.zeros(n + 1, np.int64)
+    np.cumsum(cnt, out=ptr[1:])
+    rows = np.repeat(np.arange(n, dtype=np.int64), cnt)
+    pos_in_row = np.arange(ptr[-1], dtype=np.int64) - ptr[rows]
+    cols = np.empty(ptr[-1], np.int64)
+    vals = np.empty((ptr[-1], 9))
+    lsel = pos_in_row < nl[rows]
+    dsel = pos_in_row == nl[rows]
+    usel = pos_in_row > nl[rows]
+    cols[lsel] = m.itemL[:m.indexL[n]].astype(np.int64) - 1
+    vals[lsel] = m.AL.reshape(-1, 9)[:m.indexL[n]]
+    cols[dsel] = np.arange(n)
+    vals[dsel] = m.D.reshape(-1, 9)[:n]
+    cols[usel] = m.itemU[:m.indexU[n]].astype(np.int64) - 1
+    vals[usel] = m.AU.reshape(-1, 9)[:m.indexU[n]]
+    return ptr, cols, vals
 
 
 def slab_owner(n, ndom):
@@ -109,67 +119,63 @@ def partition(m, ndom, owner=None):
     if m.NP != n:
         raise ValueError("partition: the input is one domain (N == NP)")
     owner = slab_owner(n, ndom) if owner is None else np.asarray(owner, dtype=np.int32)
-    rows = _global_rows(m)
-    members = [np.flatnonzero(owner == d) for d in range(ndom)]
-    local_of = []  # per domain: dict global id -> local id (0-based)
+    ptr, cols, vals = _global_csr(m)
+    row_of = np.repeat(np.arange(n, dtype=np.int64), np.diff(ptr))
+    members = [np.flatnonzero(owner == d).astype(np.int64) for d in range(ndom)]
     externals = []
     for d in range(ndom):
-        internal = members[d]
-        ext = set()
-        for g in internal:
-            for c in rows[g][0]:
-                if owner[c] != d:
-                    ext.add(int(c))
-        ext = sorted(ext, key=lambda g: (int(owner[g]), g))
-        externals.append(np.array(ext, dtype=np.int64))
-        gids = np.concatenate([internal, externals[d]]).astype(np.int64)
-        local_of.append({int(g): k for k, g in enumerate(gids)})
+        mine = owner[row_of] == d
+        ext = np.unique(cols[mine & (owner[cols] != d)])
+        ext = ext[np.lexsort((ext, owner[ext]))]  # by owner, then global id
+        externals.append(ext)
     domains = []
     for d in range(ndom):
         internal, ext = members[d], externals[d]
-        gids = np.concatenate([internal, ext]).astype(np.int64)
-        loc = local_of[d]
-        NP, N = gids.size, internal.size
-        indexL, indexU, itemL, itemU, AL, AU = [0], [0], [], [], [], []
+        gids = np.concatenate([internal, ext])
+        N, NP = internal.size, gids.size
+        loc = np.full(n, -1, np.int64)
+        loc[gids] = np.arange(NP)
+        # the local rows: the global rows of the local nodes, columns kept where local
+        starts, ends = ptr[gids], ptr[gids + 1]
+        lens = ends - starts
+        sel = np.repeat(starts, lens) + (np.arange(lens.sum()) - np.repeat(np.cumsum(lens) - lens, lens))
+        lrow = np.repeat(np.arange(NP, dtype=np.int64), lens)
+        lcol = loc[cols[sel]]
+        keep = lcol >= 0
+        lrow, lcol, sel = lrow[keep], lcol[keep], sel[keep]
+        order = np.lexsort((lcol, lrow))
+        lrow, lcol, sel = lrow[order], lcol[order], sel[order]
+        isL, isD, isU = lcol < lrow, lcol == lrow, lcol > lrow
         D = np.zeros((NP, 9))
-        for k, g in enumerate(gids):
-            cols, vals = rows[int(g)]
-            lcols = np.array([loc.get(int(c), -1) for c in cols], dtype=np.int64)
-            keep = lcols >= 0
-            lcols, lvals = lcols[keep], vals[keep]
-            order = np.argsort(lcols, kind="stable")
-            for lc, v in zip(lcols[order], lvals[order]):
-                if lc < k:
-                    itemL.append(lc + 1)
-                    AL.append(v)
-                elif lc == k:
-                    D[k] = v
-                else:
-                    itemU.append(lc + 1)
-                    AU.append(v)
-            indexL.append(len(itemL))
-            indexU.append(len(itemU))
-        for items_, vals_ in ((itemL, AL), (itemU, AU)):
-            if not items_:
-                items_.append(0)
-                vals_.append(np.zeros(9))
+        D[lrow[isD]] = vals[sel[isD]]
+        indexL = np.zeros(NP + 1, np.int32)
+        indexU = np.zeros(NP + 1, np.int32)
+        np.cumsum(np.bincount(lrow[isL], minlength=NP), out=indexL[1:])
+        np.cumsum(np.bincount(lrow[isU], minlength=NP), out=indexU[1:])
+        itemL = (lcol[isL] + 1).astype(np.int32)
+        itemU = (lcol[isU] + 1).astype(np.int32)
+        AL = vals[sel[isL]]
+        AU = vals[sel[isU]]
+        if itemL.size == 0:  # keep the arrays non-empty (as HecMatrix.empty does)
+            itemL, AL = np.zeros(1, np.int32), np.zeros((1, 9))
+        if itemU.size == 0:
+            itemU, AU = np.zeros(1, np.int32), np.zeros((1, 9))
         B = np.zeros(3 * NP)
         B.reshape(-1, 3)[:] = m.B.reshape(-1, 3)[gids]
-        lm = HecMatrix(N, NP, np.array(indexL, np.int32), np.array(itemL, np.int32),
-                       np.array(indexU, np.int32), np.array(itemU, np.int32), D.reshape(-1),
-                       np.array(AL, np.float64).reshape(-1), np.array(AU, np.float64).reshape(-1), B=B)
+        lm = HecMatrix(N, NP, indexL, itemL, indexU, itemU, D.reshape(-1), AL.reshape(-1), AU.reshape(-1), B=B)
         lm.Iarray, lm.Rarray = m.Iarray.copy(), m.Rarray.copy()
         # communication table: import = my external nodes by owner; export = my internal
         # nodes that a neighbour holds as external, in that neighbour's import order
-        nbrs = sorted(set(int(owner[g]) for g in ext) |
+        nbrs = sorted(set(int(q) for q in np.unique(owner[ext])) |
                       set(q for q in range(ndom) if q != d and np.any(owner[externals[q]] == d)))
         imp_index, imp_item, exp_index, exp_item = [0], [], [0], []
         for q in nbrs:
-            imp = [g for g in ext if owner[g] == q]
-            imp_item += [loc[int(g)] + 1 for g in imp]
+            imp = ext[owner[ext] == q]
+            imp_item.extend((loc[imp] + 1).tolist())
             imp_index.append(len(imp_item))
-            exp = [g for g in externals[q] if owner[g] == d]  # q's import order from d
-            exp_item += [loc[int(g)] + 1 for g in exp]
+            exq = externals[q]
+            exp = exq[owner[exq] == d]  # q's import order from d
+            exp_item.extend((loc[exp] + 1).tolist())
             exp_index.append(len(exp_item))
         comm = CommTable(d, nbrs, imp_index, imp_item, exp_index, exp_item)
         domains.append(Domain(lm, comm, gids))

@@ -125,6 +125,67 @@ def test_oracle_domains_outer_preconditioner_passes(precond):
     assert out[0]["iter"] < one[0]["iter"]
 
 
+def _partition_loops(m, ndom):
+    """The partition rule row by row (a slow restatement of domain.partition)."""
+    from frontistr_b200.domain import slab_owner
+    n = m.N
+    owner = slab_owner(n, ndom)
+    D0, AL0, AU0 = m.D.reshape(-1, 9), m.AL.reshape(-1, 9), m.AU.reshape(-1, 9)
+    rows = []
+    for i in range(n):
+        lo, hi, ulo, uhi = m.indexL[i], m.indexL[i + 1], m.indexU[i], m.indexU[i + 1]
+        rows.append((np.concatenate([m.itemL[lo:hi] - 1, [i], m.itemU[ulo:uhi] - 1]).astype(np.int64),
+                     np.concatenate([AL0[lo:hi], D0[i:i + 1], AU0[ulo:uhi]])))
+    members = [np.flatnonzero(owner == d) for d in range(ndom)]
+    externals = []
+    for d in range(ndom):
+        ext = sorted({int(c) for g in members[d] for c in rows[g][0] if owner[c] != d},
+                     key=lambda g: (int(owner[g]), g))
+        externals.append(np.array(ext, dtype=np.int64))
+    out = []
+    for d in range(ndom):
+        gids = np.concatenate([members[d], externals[d]]).astype(np.int64)
+        loc = {int(g): k for k, g in enumerate(gids)}
+        L, U, Dm = [], [], np.zeros((gids.size, 9))
+        for k, g in enumerate(gids):
+            c, v = rows[int(g)]
+            lc = np.array([loc.get(int(x), -1) for x in c])
+            keep = lc >= 0
+            for col, val in sorted(zip(lc[keep], v[keep]), key=lambda t: t[0]):
+                if col < k:
+                    L.append((k, col, val))
+                elif col == k:
+                    Dm[k] = val
+                else:
+                    U.append((k, col, val))
+        nb = sorted({int(owner[g]) for g in externals[d]} |
+                    {q for q in range(ndom) if q != d and np.any(owner[externals[q]] == d)})
+        imp = [[loc[int(g)] + 1 for g in externals[d] if owner[g] == q] for q in nb]
+        exp = [[loc[int(g)] + 1 for g in externals[q] if owner[g] == d] for q in nb]
+        out.append((gids, members[d].size, L, U, Dm, nb, imp, exp))
+    return out
+
+
+@pytest.mark.parametrize("nd", [2, 3, 4])
+def test_partition_matches_the_row_by_row_rule(nd):
+    m = _system(seed=5)
+    fast = partition(m, nd)
+    for dom, (gids, N, L, U, Dm, nb, imp, exp) in zip(fast, _partition_loops(m, nd)):
+        lm, c = dom.matrix, dom.comm
+        np.testing.assert_array_equal(dom.global_ids, gids)
+        assert lm.N == N and lm.NP == gids.size
+        np.testing.assert_array_equal(lm.D.reshape(-1, 9), Dm)
+        for part, ind, item, A in ((L, lm.indexL, lm.itemL, lm.AL), (U, lm.indexU, lm.itemU, lm.AU)):
+            assert ind[-1] == len(part)
+            for j, (row, col, val) in enumerate(part):
+                assert ind[row] <= j < ind[row + 1] and item[j] == col + 1
+                np.testing.assert_array_equal(A.reshape(-1, 9)[j], val)
+        assert list(c.neighbor_pe) == nb
+        for k in range(len(nb)):
+            assert list(c.import_item[c.import_index[k]:c.import_index[k + 1]]) == imp[k]
+            assert list(c.export_item[c.export_index[k]:c.export_index[k + 1]]) == exp[k]
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
