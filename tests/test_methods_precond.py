@@ -8,7 +8,10 @@ solution within 1e-6 relative (restarted and bi-orthogonal methods carry roundin
 differences through the iterations), a true residual below the tolerance (or within
 10 % of the oracle's where that ends at the tolerance).  GMRESREN's second
 orthogonalisation reuses the previous step's coefficient (as the reference's does),
-which makes its iteration count sensitive to rounding: 15 % there.
+which makes its iteration count sensitive to rounding: 15 % there.  Every method also
+with SCALING=YES (against the oracle's scaled solve) and with the BF16-stored SSOR
+factors of Iarray(42) = 1 (against the FP64 oracle: iterations within 25 %, the
+solution within 1e-6, the true residual at the tolerance).
 """
 import numpy as np
 import pytest
@@ -51,3 +54,37 @@ def test_gpu_matches_oracle(method, precond):
     assert abs(info["iter"] - ref["iter"]) <= max(2, bar), (info["iter"], ref["iter"])
     assert np.linalg.norm(g.X - ref["X"]) <= 1e-6 * np.linalg.norm(ref["X"])
     assert Oracle(m).rel_resid(g.X, m.B) <= max(1e-8, 1.1 * ref["resid_true"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", METHODS)
+def test_gpu_scaling_matches_oracle(method):
+    """SCALING=YES (Iarray(7)) with every method: the solve on S A S, S b."""
+    from frontistr_b200.solver import GpuSolver
+    m, g = _case(method, 1)
+    g.Iarray[6] = 1
+    ref = Oracle(m).solve(Iarray=g.Iarray, Rarray=g.Rarray)
+    with GpuSolver() as s:
+        info = s.solve(g)
+    assert info["error"] == ref["error"] == 0
+    bar = ref["iter"] * 3 // 20 if method == 6 else ref["iter"] // 20
+    assert abs(info["iter"] - ref["iter"]) <= max(2, bar), (info["iter"], ref["iter"])
+    assert np.linalg.norm(g.X - ref["X"]) <= 1e-6 * np.linalg.norm(ref["X"])
+    assert Oracle(m).rel_resid(g.X, m.B) <= max(1e-8, 1.1 * ref["resid_true"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", METHODS)
+def test_gpu_bf16_preconditioner_every_method(method):
+    """Iarray(42) = 1 (BF16-stored SSOR factors, FP64 iterations) with every method:
+    the FP64 oracle's solution to the tolerance's accuracy."""
+    from frontistr_b200.solver import GpuSolver
+    m, g = _case(method, 1)
+    ref = Oracle(m).solve(Iarray=g.Iarray, Rarray=g.Rarray)
+    g.Iarray[41] = 1
+    with GpuSolver() as s:
+        info = s.solve(g)
+    assert info["error"] == 0
+    assert abs(info["iter"] - ref["iter"]) <= max(3, ref["iter"] // 4), (info["iter"], ref["iter"])
+    assert np.linalg.norm(g.X - ref["X"]) <= 1e-6 * np.linalg.norm(ref["X"])
+    assert Oracle(m).rel_resid(g.X, m.B) <= 1.05e-8
