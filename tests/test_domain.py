@@ -91,7 +91,7 @@ def test_oracle_one_domain_is_the_serial_solve():
 
 
 @pytest.mark.parametrize("nd", [2, 3, 4])
-@pytest.mark.parametrize("precond", [1, 3, 10])
+@pytest.mark.parametrize("precond", [1, 3, 10, 11, 12])
 def test_oracle_domains_converge_to_the_mesh_solution(nd, precond):
     m = _system()
     g = m.copy()
@@ -258,7 +258,7 @@ def _gpu_domains(doms, method_override=None):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("nd,precond,iterpremax", [(2, 1, 1), (2, 3, 1), (2, 10, 1), (3, 1, 1), (3, 3, 1),
-                                                   (3, 10, 1), (3, 1, 2), (2, 10, 2)])
+                                                   (3, 10, 1), (3, 1, 2), (2, 10, 2), (3, 11, 1), (2, 12, 1)])
 def test_gpu_domains_match_oracle(nd, precond, iterpremax):
     m = _system(seed=7)
     doms = _domains(m, nd, precond, iterpremax)
