@@ -78,7 +78,8 @@ def default_iarray_rarray():
 
 
 class HecMatrix:
-    """hecmwST_matrix for NDOF = 3 at one domain (N == NP)."""
+    """hecmwST_matrix for NDOF = 3: N internal of NP nodes (N == NP for a whole mesh;
+    N < NP for a domain of a decomposed mesh, frontistr_b200.domain)."""
 
     NDOF = 3
 

@@ -418,7 +418,10 @@ _dumper = None
 
 
 def hecmw_solve(hecMAT, solver=None, dumper=None):
-    """hecmw_solve(hecMESH, hecMAT) for one GPU domain: updates hecMAT.X and flags.
+    """hecmw_solve(hecMESH, hecMAT) for a whole mesh (N == NP): updates hecMAT.X and
+    flags.  hecMAT.mpc (the mesh's MPC table, HecMatrix.mpc) goes to the solver
+    (GpuSolver.set_mpc), so that MPC_METHOD = Iarray(13) = 2 runs MPC-CG.  A domain of a
+    decomposed mesh is solved through GpuSolver.set_domain.
 
     With Iarray(31) = DUMPTYPE (1 MM, 2 CSR, 3 BSR) the matrix and right-hand side
     are dumped before the solve and the solution after it, as hecmw_solve_iterative
@@ -436,11 +439,21 @@ def hecmw_solve(hecMAT, solver=None, dumper=None):
         if _dumper is None:
             _dumper = Dumper()
         dumper = _dumper
+    mpc = getattr(hecMAT, "mpc", None)
+
+    def run():
+        if mpc is None:
+            return solver.solve(hecMAT)
+        solver.set_matrix(hecMAT, hecMAT.Iarray)
+        solver.set_mpc(*mpc)
+        return solver.solve_resident(hecMAT.B, hecMAT.X, hecMAT.Iarray, hecMAT.Rarray)
+
     b = hecMAT.B[:3 * hecMAT.NP]
-    if float(np.dot(b, b)) == 0.0:
-        return solver.solve(hecMAT)
+    consts = 0.0 if mpc is None else float(np.dot(mpc[4], mpc[4]))
+    if float(np.dot(b, b)) + consts == 0.0:
+        return run()
     dumper.dump(hecMAT)
-    info = solver.solve(hecMAT)
+    info = run()
     dumper.dump_solution(hecMAT)
     return info
 

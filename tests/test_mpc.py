@@ -171,3 +171,17 @@ def test_gpu_mpc_constants_in_the_zero_rhs_check():
             info = s.solve_resident(m.B, m.X, m.Iarray, m.Rarray)
         assert info["error"] == ref["error"] == code
         assert not np.any(m.X)
+
+
+@pytest.mark.gpu
+def test_gpu_hecmw_solve_passes_the_mpc_table():
+    """The Python hecmw_solve hands hecMAT.mpc to the solver, as the shim does hecMESH%mpc."""
+    from frontistr_b200.solver import GpuSolver, hecmw_solve
+    m, mpc = _system()
+    ref = Oracle(m).solve()
+    g = m.copy()
+    with GpuSolver() as s:
+        info = hecmw_solve(g, solver=s)
+    assert info["error"] == ref["error"] == 0
+    assert abs(info["iter"] - ref["iter"]) <= 2
+    assert np.linalg.norm(_t(g.X, mpc) - _t(ref["X"], mpc)) <= 1e-8 * np.linalg.norm(_t(ref["X"], mpc))
