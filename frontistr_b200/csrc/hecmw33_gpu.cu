@@ -1987,11 +1987,70 @@ void condition_report(Solver &S, const std::vector<double> &ab, int n, int estco
   S.last_lanczos_n = n;
 }
 
+// Singular values of the n x n column-major matrix a (overwritten) by one-sided Jacobi
+// rotations (Hestenes): columns are orthogonalised pairwise until every pair is
+// orthogonal to rounding; the singular values are then the column norms.
+std::vector<double> jacobi_singular_values(std::vector<double> a, int n) {
+  for (int sweep = 0; sweep < 60; sweep++) {
+    bool rotated = false;
+    for (int p = 0; p < n - 1; p++)
+      for (int q = p + 1; q < n; q++) {
+        double alpha = 0.0, beta = 0.0, gamma = 0.0;
+        for (int i = 0; i < n; i++) {
+          const double x = a[size_t(p) * n + i], y = a[size_t(q) * n + i];
+          alpha += x * x;
+          beta += y * y;
+          gamma += x * y;
+        }
+        if (gamma == 0.0 || std::fabs(gamma) <= 1e-15 * std::sqrt(alpha * beta)) continue;
+        rotated = true;
+        const double zeta = (beta - alpha) / (2.0 * gamma);
+        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / std::sqrt(1.0 + t * t), sn = c * t;
+        for (int i = 0; i < n; i++) {
+          const double x = a[size_t(p) * n + i], y = a[size_t(q) * n + i];
+          a[size_t(p) * n + i] = c * x - sn * y;
+          a[size_t(q) * n + i] = sn * x + c * y;
+        }
+      }
+    if (!rotated) break;
+  }
+  std::vector<double> sv(size_t(std::max(n, 0)));
+  for (int j = 0; j < n; j++) {
+    double s2 = 0.0;
+    for (int i = 0; i < n; i++) s2 += a[size_t(j) * n + i] * a[size_t(j) * n + i];
+    sv[size_t(j)] = std::sqrt(s2);
+  }
+  return sv;
+}
+
+// hecmw_estimate_condition_GMRES (hecmw_estimate_condition.F90:102-170) on the
+// device's Hessenberg (column-major, leading dimension ld, 1-based (k, j) at
+// H[(j-1) ld + k-1]) after step I: the I x I block whose entries below the first
+// subdiagonal are zero, its extreme singular values printed as the reference
+// prints them (the reference calls LAPACK's dgesdd).
+void gmres_condition(Solver &S, const double *dH, int ld, int I) {
+  if (I <= 0) return;
+  std::vector<double> H(size_t(ld) * ld);
+  H33_CUDA(cudaMemcpy(H.data(), dH, sizeof(double) * H.size(), cudaMemcpyDeviceToHost));
+  const int n = std::min(I, ld);
+  std::vector<double> a(size_t(n) * n, 0.0);
+  for (int j = 1; j <= n; j++)
+    for (int k = 1; k <= std::min(j + 1, n); k++) a[size_t(j - 1) * n + (k - 1)] = H[size_t(j - 1) * ld + (k - 1)];
+  const std::vector<double> sv = jacobi_singular_values(a, n);
+  const double emin = *std::min_element(sv.begin(), sv.end()), emax = *std::max_element(sv.begin(), sv.end());
+  std::printf("emin=%13.6E, emax=%13.6E, emax/emin=%13.6E\n", emin, emax, emax / emin);
+  std::fflush(stdout);
+  S.last_emin = emin;
+  S.last_emax = emax;
+  S.last_lanczos_n = n;
+}
+
 // hecmw_solve_GMRES (hecmw_solver_GMRES.f90:123-411) on the resident B and X in FP64:
 // right-preconditioned GMRES(NREST) with modified Gram-Schmidt and Givens rotations.
 // Returns the device-side seconds; sets *error (0 or 3001), *iter and *resid.
 float run_gmres(Solver &S, int iterpremax, double tol, int maxit, int nrest, int lowp, int *kernels, int *error,
-                int *iter, double *resid) {
+                int *iter, double *resid, int estcond = 0) {
   cudaStream_t s = S.stream;
   const int n3 = S.n3();
   int m = nrest;
@@ -2079,6 +2138,7 @@ float run_gmres(Solver &S, int iterpremax, double tol, int maxit, int nrest, int
         break;
       }
       *resid = rs;
+      if (estcond > 0 && *iter % estcond == 0) gmres_condition(S, g.H, ld, I);  // :290-291
       if (rs <= tol) {
         finish(I);
         exit_outer = true;
@@ -2105,6 +2165,7 @@ float run_gmres(Solver &S, int iterpremax, double tol, int maxit, int nrest, int
     }
   }
   if (*error == HECMW33_ERR_NOCONV_MAXIT) finish(I);  // :382-411
+  if (estcond > 0) gmres_condition(S, g.H, ld, I);     // :416-417
   H33_CUDA(cudaEventRecord(S.ev1, s));
   S.sync();
   float ms = 0.0f;
@@ -2547,7 +2608,7 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
     Iarray[80] = 0;
     Iarray[81] = 0;
     if (method == 3) {
-      ms_total += run_gmres(S, iterPREmax, TOL, MAXIT, Iarray[5], lowp, &kernels, &error, iter, resid);
+      ms_total += run_gmres(S, iterPREmax, TOL, MAXIT, Iarray[5], lowp, &kernels, &error, iter, resid, ESTCOND);
     } else if (method == 7) {
       ms_total += run_cr(S, iterPREmax, TOL, MAXIT, lowp, &kernels, &error, iter, resid);
     } else if (method == 4) {

@@ -149,9 +149,10 @@ HECMW33_API void hecmw33_gpu_set_domain(const int *handle, const int *n_neighbor
 /* Iarray(14) = ESTCOND > 0 (hecmw_solver_CG.f90:256-264, 299-301): the CG records ALPHA
  * and BETA; every ESTCOND iterations and at the end of a solve without error the
  * extreme eigenvalues of the Lanczos tridiagonal are printed on stdout as
- * "emin=..., emax=..., emax/emin=..." (hecmw_estimate_condition.F90:14-99).  This call
- * returns the last solve's number of recorded iterations (0 when off) and its last
- * estimate. */
+ * "emin=..., emax=..., emax/emin=..." (hecmw_estimate_condition.F90:14-99).  GMRES
+ * prints the extreme singular values of its rotated Hessenberg block the same way
+ * (hecmw_solver_GMRES.f90:290-291, 416-417).  This call returns the size of the last
+ * estimate's matrix (0 when off) and that estimate. */
 HECMW33_API void hecmw33_gpu_condition_estimate(const int *handle, int *n, double *emin, double *emax, int *ierr);
 
 /* hecmw_solve (hecmw_solver.f90:9-88) for METHOD = 1-7 on the resident matrix:

@@ -1216,8 +1216,21 @@ int o33_bicgstab(const o33_matrix *A, const o33_precond *P, int iterpremax, int 
 
 /* hecmw_solve_GMRES (hecmw_solver_GMRES.f90:93-411): right-preconditioned
  * GMRES(NREST), modified Gram-Schmidt, Givens rotations stored in H(:,CS/SN). */
+static int gmres_impl(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol, int nrest,
+                      const double *B, double *X, int *iter_out, double *resid_out, double *H_out, int *I_out);
+
 int o33_gmres(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol, int nrest,
               const double *B, double *X, int *iter_out, double *resid_out) {
+  return gmres_impl(A, P, iterpremax, maxit, tol, nrest, B, X, iter_out, resid_out, NULL, NULL);
+}
+
+int o33_gmres_hess(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol, int nrest,
+                   const double *B, double *X, int *iter_out, double *resid_out, double *H_out, int *I_out) {
+  return gmres_impl(A, P, iterpremax, maxit, tol, nrest, B, X, iter_out, resid_out, H_out, I_out);
+}
+
+static int gmres_impl(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol, int nrest,
+                      const double *B, double *X, int *iter_out, double *resid_out, double *H_out, int *I_out) {
   const int NP = A->NP, NN = 3 * A->N;
   const size_t len = 3 * (size_t)NP;
   int NREST = nrest;
@@ -1329,6 +1342,10 @@ int o33_gmres(const o33_matrix *A, const o33_precond *P, int iterpremax, int max
 #undef HH
   *iter_out = ITER;
   *resid_out = RESID;
+  if (H_out) { /* the Hessenberg as the end of the solve leaves it (NRK x NRK, column-major) */
+    memcpy(H_out, H, sizeof(double) * (size_t)NRK * NRK);
+    *I_out = I;
+  }
   free(H);
   free(SS);
   free(Sv);

@@ -115,6 +115,12 @@ int o33_gmres(const o33_matrix *A, const o33_precond *P, int iterpremax, int max
 int o33_cg_lanczos(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
                    const double *B, double *X, int *iter_out, double *resid_out, double *ab);
 
+/* o33_gmres that also returns the Hessenberg as the solve leaves it (NREST+7 squared
+ * doubles, column-major, the rotated leading block) and the last step index I: the
+ * data of ESTCOND's estimate (hecmw_solver_GMRES.f90:290-291, 416-417). */
+int o33_gmres_hess(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol, int nrest,
+                   const double *B, double *X, int *iter_out, double *resid_out, double *H_out, int *I_out);
+
 /* Conjugate residual iterations only (hecmw_solve_CR), given a ready preconditioner. */
 int o33_cr(const o33_matrix *A, const o33_precond *P, int iterpremax, int maxit, double tol,
            const double *B, double *X, int *iter_out, double *resid_out);

@@ -78,6 +78,9 @@ def lib():
         L.o33_cg_lanczos.argtypes = [ctypes.POINTER(O33Matrix), ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_double, _f64p, _f64p, _i32p, _f64p, _f64p]
         L.o33_cg_lanczos.restype = ctypes.c_int
+        L.o33_gmres_hess.argtypes = [ctypes.POINTER(O33Matrix), ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_double, ctypes.c_int, _f64p, _f64p, _i32p, _f64p, _f64p, _i32p]
+        L.o33_gmres_hess.restype = ctypes.c_int
         L.o33_cg_fixed_iters.argtypes = [ctypes.POINTER(O33Matrix), ctypes.c_void_p, ctypes.c_int,
                                          ctypes.c_int, _f64p, _f64p]
         L.o33_cg_fixed_iters.restype = ctypes.c_double
@@ -217,6 +220,20 @@ class OraclePrecond:
                                    ctypes.byref(it), ctypes.byref(res), _dp(ab))
         n = min(it.value, maxit)
         return dict(X=X, error=err, iter=it.value, alpha=ab[0:2 * n:2].copy(), beta=ab[1:2 * n:2].copy())
+
+    def gmres_hess(self, B, nrest, maxit=20000, tol=1e-8, iterpremax=1):
+        """GMRES(nrest) with this preconditioner; also the final Hessenberg (column-major,
+        leading dimension nrest + 7) and the last step index I."""
+        orc = self.orc
+        m = orc.m
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        X = np.zeros(3 * m.NP)
+        it, res, I = ctypes.c_int(0), ctypes.c_double(0), ctypes.c_int(0)
+        ld = nrest + 7
+        H = np.zeros(ld * ld)
+        err = orc.L.o33_gmres_hess(ctypes.byref(orc.mat), self.h, iterpremax, maxit, tol, nrest, _dp(B), _dp(X),
+                                   ctypes.byref(it), ctypes.byref(res), _dp(H), ctypes.byref(I))
+        return dict(X=X, error=err, iter=it.value, I=I.value, H=H.reshape(ld, ld).T.copy(), ld=ld)
 
     def cg(self, B, maxit=20000, tol=1e-8, iterpremax=1, X=None, hist=False, on=None):
         """CG with this preconditioner; `on` (an Oracle) selects another matrix."""

@@ -74,3 +74,31 @@ def test_gpu_estcond(capfd):
     assert len(lines) == n // 20 + 1
     last = re.match(r"emin= ?([-+0-9.E]+), emax= ?([-+0-9.E]+), emax/emin= ?([-+0-9.E]+)", lines[-1])
     assert last and abs(float(last.group(1)) - emin) <= 1e-6 * emin
+
+
+@pytest.mark.gpu
+def test_gpu_estcond_gmres(capfd):
+    """GMRES (hecmw_solver_GMRES.f90:290-291, 416-417): the extreme singular values of the
+    rotated Hessenberg's leading I x I block, every ESTCOND iterations and at the end."""
+    from frontistr_b200.solver import GpuSolver
+    m = box_system(9, 8, 10, jitter=0.2, sigma_E=1.0, nu_range=(0.25, 0.40), seed=11)
+    m.set_iter(20000)
+    m.set_method(3)
+    m.Iarray[5] = 40  # NREST
+    ref = Oracle(m).precond(1).gmres_hess(m.B, 40)
+    n = ref["I"]
+    H = ref["H"][:n, :n].copy()
+    H[np.tril_indices(n, -2)] = 0.0
+    sv = np.linalg.svd(H, compute_uv=False)
+    g = m.copy()
+    g.Iarray[IDX_I_ESTCOND - 1] = 7
+    with GpuSolver() as s:
+        capfd.readouterr()
+        info = s.solve(g)
+        k, emin, emax = s.condition_estimate()
+    out = capfd.readouterr().out
+    assert info["error"] == 0 and info["iter"] == ref["iter"]
+    assert k == n
+    assert abs(emin - sv.min()) <= 1e-6 * sv.min() and abs(emax - sv.max()) <= 1e-6 * sv.max()
+    lines = [l for l in out.splitlines() if l.startswith("emin=")]
+    assert len(lines) == info["iter"] // 7 + 1
