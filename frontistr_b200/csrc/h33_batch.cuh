@@ -226,8 +226,10 @@ __device__ void team_solve(const BatchArgs &a, int id, Team &t, CgState &st, dou
     st.guard = 0;
     st.inner = st.flexible = st.use_gnn = st.restart = st.fallback = 0;
     st.reliable = 0;
-    st.lanczos = nullptr;  // no condition estimate in a batch
+    st.lanczos = nullptr;  // no condition estimate or residual history in a batch
     st.lanczos_cap = st.lanczos_n = 0;
+    st.rhist = nullptr;
+    st.rhist_cap = st.rhist_n = 0;
   }
   __syncthreads();
   // prologue: r = b - A x and BNRM2 in one pass

@@ -121,6 +121,10 @@ struct CgState {
   // condition estimate of hecmw_solver_CG.f90:256-264 (null when off)
   double *lanczos;
   int lanczos_cap, lanczos_n;
+  // ITERLOG (Iarray(21) = 1): RESID of every iteration as hecmw_solve_CG prints it
+  // (hecmw_solver_CG.f90:251-253; null when off)
+  double *rhist;
+  int rhist_cap, rhist_n;
   unsigned int ticket[8];
 };
 
@@ -137,6 +141,8 @@ struct CgParams {
   int method;    // hecmw METHOD: 1 CG, 2 BiCGSTAB
   double *lanczos;  // ESTCOND: 2 x maxit doubles (ALPHA, BETA per iteration) or null
   int lanczos_cap;
+  double *rhist;    // ITERLOG: maxit doubles (RESID per iteration) or null
+  int rhist_cap;
 };
 
 }  // namespace h33

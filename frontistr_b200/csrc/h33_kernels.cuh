@@ -143,9 +143,18 @@ __device__ __forceinline__ void fin_pq(CgState *st, double c1) {
 }
 
 // DNRM2 after r -= alpha q (:248-250): a residual at or below TOL asks for a recompute
+// ITERLOG: this iteration's RESID into the history
+__device__ __forceinline__ void record_resid(CgState *st) {
+  if (st->rhist && st->iter >= 1 && st->iter <= st->rhist_cap) {
+    st->rhist[st->iter - 1] = st->resid;
+    st->rhist_n = st->iter;
+  }
+}
+
 __device__ __forceinline__ void fin_rr(CgState *st, double rr) {
   st->rr = rr;
   st->resid = sqrt(rr / st->bnrm2);
+  record_resid(st);
   if (st->reliable) {
     // FP32 recursive residual: ask for an FP64 reliable update when it has fallen
     // by ru_delta since the last one, or reached the tolerance
@@ -846,6 +855,7 @@ __global__ void __launch_bounds__(kThreads) resid_ctl_kernel(SellView<R> A, cons
   reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[3], [&](double v) {
     st->rr = v;
     st->resid = sqrt(v / st->bnrm2);
+    if (!st->inner && (st->iter % st->nrecompute) == 0) record_resid(st);  // the iteration's RESID
     if (st->resid <= st->tol) {
       st->done = 1;
       st->converged = 1;
@@ -1015,6 +1025,9 @@ static __global__ void cg_init_kernel(CgState *st, const CgParams *prm) {
   st->lanczos = prm->lanczos;
   st->lanczos_cap = prm->lanczos_cap;
   st->lanczos_n = 0;
+  st->rhist = prm->rhist;
+  st->rhist_cap = prm->rhist_cap;
+  st->rhist_n = 0;
   for (int i = 0; i < 8; i++) st->ticket[i] = 0u;
 }
 

@@ -519,8 +519,10 @@ __global__ void mr_init_kernel(CgState *st, MultiCtl *ctl, const CgParams *prm, 
     s->reliable = s->ru_pending = s->ru_count = 0;
     s->ru_delta = 0.0;
     s->ru_mark = 1.0;
-    s->lanczos = nullptr;  // no condition estimate for several load cases
+    s->lanczos = nullptr;  // no condition estimate or residual history for several load cases
     s->lanczos_cap = s->lanczos_n = 0;
+    s->rhist = nullptr;
+    s->rhist_cap = s->rhist_n = 0;
     for (int i = 0; i < 8; i++) s->ticket[i] = 0u;
   }
   if (k == 0) {

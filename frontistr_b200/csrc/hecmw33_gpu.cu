@@ -369,6 +369,8 @@ struct Solver {
   // ESTCOND: ALPHA / BETA history of the CG (2 per iteration) and the last estimate
   bool lanczos_on = false;
   DevArray<double> lanczos_buf;
+  bool rhist_on = false;  // ITERLOG: RESID history of the CG
+  DevArray<double> rhist_buf;
   int last_lanczos_n = 0;
   double last_emin = 0.0, last_emax = 0.0;
   DevArray<int> g_flag;
@@ -1267,6 +1269,10 @@ float run_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels, int
   const bool lanczos = S.lanczos_on && !learned && !reliable && !inner && method == 1;
   S.h_params->lanczos = lanczos ? S.lanczos_buf.p : nullptr;
   S.h_params->lanczos_cap = lanczos ? int(S.lanczos_buf.n / 2) : 0;
+  // ITERLOG: the same plain CG records RESID per iteration
+  const bool rhist = S.rhist_on && !learned && !reliable && !inner && method == 1;
+  S.h_params->rhist = rhist ? S.rhist_buf.p : nullptr;
+  S.h_params->rhist_cap = rhist ? int(S.rhist_buf.n) : 0;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, S.stream));
   H33_CUDA(cudaEventRecord(S.ev0, S.stream));
   if (graph_mode()) {
@@ -1587,6 +1593,8 @@ float record_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels) 
   S.h_params->method = 1;
   S.h_params->lanczos = nullptr;
   S.h_params->lanczos_cap = 0;
+  S.h_params->rhist = nullptr;
+  S.h_params->rhist_cap = 0;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, S.stream));
   H33_CUDA(cudaEventRecord(S.ev0, S.stream));
   launch_prologue<double>(S, V, 0, 0);
@@ -2077,6 +2085,8 @@ float run_gmres(Solver &S, int iterpremax, double tol, int maxit, int nrest, int
   S.h_params->method = 3;
   S.h_params->lanczos = nullptr;
   S.h_params->lanczos_cap = 0;
+  S.h_params->rhist = nullptr;
+  S.h_params->rhist_cap = 0;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, s));
   H33_CUDA(cudaEventRecord(S.ev0, s));
   launch_k(s, cg_init_kernel, 1, 32, st, static_cast<const CgParams *>(S.params.p));
@@ -2595,6 +2605,8 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   S.last_lanczos_n = 0;
   S.last_emin = S.last_emax = 0.0;
   if (S.lanczos_on) S.lanczos_buf.alloc(2 * size_t(std::max(MAXIT, 1)));
+  S.rhist_on = Iarray[20] == 1 && method == 1 && !learned;  // hecmw_mat_get_iterlog
+  if (S.rhist_on) S.rhist_buf.alloc(size_t(std::max(MAXIT, 1)));
   if (lowp && iterPREmax > 0) ensure_lowp(S);
   else lowp = 0;
   const bool record = S.L.recording && !learned && method == 1;
@@ -2623,6 +2635,13 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
       error = st.error;
       *iter = st.iter;
       *resid = st.resid;
+      if (S.rhist_on && method == 1 && !record) {  // the ITERATION HISTORY lines (:251-253)
+        const int n = std::min(st.rhist_n, int(S.rhist_buf.n));
+        std::vector<double> h(size_t(std::max(n, 1)));
+        if (n > 0) H33_CUDA(cudaMemcpy(h.data(), S.rhist_buf.p, sizeof(double) * size_t(n), cudaMemcpyDeviceToHost));
+        for (int k = 1; k <= n; k++) std::printf("%7d%16.6E\n", k, h[size_t(k) - 1]);
+        std::fflush(stdout);
+      }
       if (S.lanczos_on && method == 1 && !record) {
         const int n = std::min(st.lanczos_n, int(S.lanczos_buf.n / 2));
         std::vector<double> ab(2 * size_t(std::max(n, 1)));
@@ -2658,6 +2677,7 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   const double resid2 = rel_resid_device(S);
   if (resid2 < TOL) Iarray[80] = 1;
   S.lanczos_on = false;
+  S.rhist_on = false;
   S.last_learned = learned;
   S.last_fallback = S.h_state->fallback;
   S.last_iter = *iter;
@@ -3064,6 +3084,8 @@ float run_multi_chunk(Solver &S, int nrhs, const double *dB, double *dX, int ite
   S.h_params->method = 1;
   S.h_params->lanczos = nullptr;
   S.h_params->lanczos_cap = 0;
+  S.h_params->rhist = nullptr;
+  S.h_params->rhist_cap = 0;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, s));
   H33_CUDA(cudaEventRecord(S.ev0, s));
   if (graph_mode()) {

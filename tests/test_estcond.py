@@ -102,3 +102,29 @@ def test_gpu_estcond_gmres(capfd):
     assert abs(emin - sv.min()) <= 1e-6 * sv.min() and abs(emax - sv.max()) <= 1e-6 * sv.max()
     lines = [l for l in out.splitlines() if l.startswith("emin=")]
     assert len(lines) == info["iter"] // 7 + 1
+
+
+@pytest.mark.gpu
+def test_gpu_iterlog(capfd):
+    """ITERLOG (Iarray(21) = 1): the CG's ITERATION HISTORY lines, ITER and RESID in the
+    reference's '(i7, 1pe16.6)' (hecmw_solver_CG.f90:251-253): one per iteration, the
+    recursive residual (every 50th iteration the recomputed one), as the oracle's."""
+    from frontistr_b200.solver import GpuSolver
+    m = box_system(9, 8, 10, jitter=0.2, sigma_E=1.0, nu_range=(0.25, 0.40), seed=11)
+    m.set_iter(20000)
+    ref = Oracle(m).precond(1).cg(m.B, hist=True)
+    with GpuSolver() as s:
+        capfd.readouterr()
+        info0 = s.solve(m.copy())
+        quiet = capfd.readouterr().out
+        g = m.copy()
+        g.Iarray[20] = 1
+        info = s.solve(g)
+        out = capfd.readouterr().out
+    assert not re.search(r"^ *\d+ +[-+0-9.]+E[-+]\d+$", quiet, re.M)
+    lines = [l for l in out.splitlines() if re.match(r"^ *\d+ +[-+0-9.]+E[-+]\d+$", l)]
+    assert info["iter"] == info0["iter"] and len(lines) == info["iter"]
+    for k, l in enumerate(lines[:20]):
+        it, res = l.split()
+        assert int(it) == k + 1 and len(l) == 23
+        assert abs(float(res) - ref["hist"][k]) <= 1e-5 * ref["hist"][k]
