@@ -369,8 +369,9 @@ struct Solver {
   // ESTCOND: ALPHA / BETA history of the CG (2 per iteration) and the last estimate
   bool lanczos_on = false;
   DevArray<double> lanczos_buf;
-  bool rhist_on = false;  // ITERLOG: RESID history of the CG
+  bool rhist_on = false;  // ITERLOG: RESID history of the CG / BiCGSTAB graph loops
   DevArray<double> rhist_buf;
+  bool iterlog = false;   // ITERLOG (Iarray(21) = 1) for the host-driven methods
   int last_lanczos_n = 0;
   double last_emin = 0.0, last_emax = 0.0;
   DevArray<int> g_flag;
@@ -1270,7 +1271,7 @@ float run_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels, int
   S.h_params->lanczos = lanczos ? S.lanczos_buf.p : nullptr;
   S.h_params->lanczos_cap = lanczos ? int(S.lanczos_buf.n / 2) : 0;
   // ITERLOG: the same plain CG records RESID per iteration
-  const bool rhist = S.rhist_on && !learned && !reliable && !inner && method == 1;
+  const bool rhist = S.rhist_on && !learned && !reliable && !inner && (method == 1 || method == 2);
   S.h_params->rhist = rhist ? S.rhist_buf.p : nullptr;
   S.h_params->rhist_cap = rhist ? int(S.rhist_buf.n) : 0;
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, S.stream));
@@ -2148,6 +2149,7 @@ float run_gmres(Solver &S, int iterpremax, double tol, int maxit, int nrest, int
         break;
       }
       *resid = rs;
+      if (S.iterlog) std::printf("%8d%8d%16.6E\n", *iter, I + 1, rs);  // :286-287
       if (estcond > 0 && *iter % estcond == 0) gmres_condition(S, g.H, ld, I);  // :290-291
       if (rs <= tol) {
         finish(I);
@@ -2263,6 +2265,7 @@ float run_cr(Solver &S, int iterpremax, double tol, int maxit, int lowp, int *ke
       true_checked = true;
     }
     *resid = true_checked ? resid_true : resid_rec;
+    if (S.iterlog) std::printf("%7d%16.6E\n", it, *resid);  // hecmw_solver_CR.f90:249
     if (true_checked) {
       if (resid_true <= tol) break;
       if (it == MAXIT) {
@@ -2410,6 +2413,7 @@ float run_gpbicg(Solver &S, int iterpremax, double tol, int maxit, int lowp, int
     BETA = ALPHA * COEF1 / (QSI * RHO);
     axpyz(BETA, PT, TT, W1);
     *resid = std::sqrt(DNRM2 / bnrm2);
+    if (S.iterlog) std::printf("%5d%16.6E\n", it, *resid);  // hecmw_solver_GPBiCG.f90:306-308
     RHO = COEF1;
     if (*resid <= tol) {  // (:311-319)
       if (it % kRecompute == 0) break;
@@ -2557,6 +2561,7 @@ float run_gmresr(Solver &S, int iterpremax, double tol, int maxit, int nrest, in
         }
       }
       *resid = std::sqrt(dot(vecR, vecR) / bnrm2);
+      if (S.iterlog) std::printf("%7d%16.6E\n", it, *resid);  // GMRESR.f90:227, GMRESREN.f90:199
       if (*resid <= tol) {
         done = true;
         break;
@@ -2605,7 +2610,8 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   S.last_lanczos_n = 0;
   S.last_emin = S.last_emax = 0.0;
   if (S.lanczos_on) S.lanczos_buf.alloc(2 * size_t(std::max(MAXIT, 1)));
-  S.rhist_on = Iarray[20] == 1 && method == 1 && !learned;  // hecmw_mat_get_iterlog
+  S.rhist_on = Iarray[20] == 1 && (method == 1 || method == 2) && !learned;  // hecmw_mat_get_iterlog
+  S.iterlog = Iarray[20] == 1;
   if (S.rhist_on) S.rhist_buf.alloc(size_t(std::max(MAXIT, 1)));
   if (lowp && iterPREmax > 0) ensure_lowp(S);
   else lowp = 0;
@@ -2635,7 +2641,8 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
       error = st.error;
       *iter = st.iter;
       *resid = st.resid;
-      if (S.rhist_on && method == 1 && !record) {  // the ITERATION HISTORY lines (:251-253)
+      if (S.rhist_on && (method == 1 || method == 2) && !record) {  // ITERATION HISTORY (CG.f90:251-253,
+                                                                      // BiCGSTAB.f90:254-256)
         const int n = std::min(st.rhist_n, int(S.rhist_buf.n));
         std::vector<double> h(size_t(std::max(n, 1)));
         if (n > 0) H33_CUDA(cudaMemcpy(h.data(), S.rhist_buf.p, sizeof(double) * size_t(n), cudaMemcpyDeviceToHost));
@@ -2676,8 +2683,10 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   }
   const double resid2 = rel_resid_device(S);
   if (resid2 < TOL) Iarray[80] = 1;
+  if (S.iterlog) std::fflush(stdout);
   S.lanczos_on = false;
   S.rhist_on = false;
+  S.iterlog = false;
   S.last_learned = learned;
   S.last_fallback = S.h_state->fallback;
   S.last_iter = *iter;

@@ -146,9 +146,10 @@ HECMW33_API void hecmw33_gpu_set_domain(const int *handle, const int *n_neighbor
                                         hecmw33_exchange_fn exchange, hecmw33_allreduce_fn allreduce,
                                         void *ctx, int *ierr);
 
-/* Iarray(21) = ITERLOG = 1 (hecmw_solver_CG.f90:251-253): the CG records RESID of every
- * iteration and prints the reference's "ITER RESID" lines ('(i7, 1pe16.6)') on stdout
- * when the solve returns.
+/* Iarray(21) = ITERLOG = 1 (hecmw_solver_CG.f90:251-253): the CG and BiCGSTAB record RESID
+ * of every iteration and print the reference's "ITER RESID" lines ('(i7, 1pe16.6)') on
+ * stdout when the solve returns; GMRES, GPBiCG, CR, GMRESR and GMRESREN print each
+ * iteration's line in their reference's format as they go.
  * Iarray(14) = ESTCOND > 0 (hecmw_solver_CG.f90:256-264, 299-301): the CG records ALPHA
  * and BETA; every ESTCOND iterations and at the end of a solve without error the
  * extreme eigenvalues of the Lanczos tridiagonal are printed on stdout as

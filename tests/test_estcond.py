@@ -128,3 +128,25 @@ def test_gpu_iterlog(capfd):
         it, res = l.split()
         assert int(it) == k + 1 and len(l) == 23
         assert abs(float(res) - ref["hist"][k]) <= 1e-5 * ref["hist"][k]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method,width", [(2, 23), (3, 32), (4, 21), (5, 23), (6, 23), (7, 23)])
+def test_gpu_iterlog_other_methods(capfd, method, width):
+    """ITERLOG with the other methods: one history line per iteration in each
+    reference's format -- BiCGSTAB, CR, GMRESR, GMRESREN '(i7, 1pe16.6)', GMRES
+    '(2i8, 1pe16.6)' (iter, step, RESID), GPBiCG '(i5, 1pe16.6)'."""
+    from frontistr_b200.solver import GpuSolver
+    m = box_system(7, 6, 8, jitter=0.2, sigma_E=1.0, nu_range=(0.25, 0.40), seed=13)
+    m.set_iter(20000)
+    m.set_method(method)
+    m.Iarray[5] = 30
+    m.Iarray[20] = 1
+    with GpuSolver() as s:
+        capfd.readouterr()
+        info = s.solve(m)
+        out = capfd.readouterr().out
+    lines = [l for l in out.splitlines() if re.match(r"^ *\d+( +\d+)? +[-+0-9.]+E[-+]\d+$", l)]
+    assert info["error"] == 0 and len(lines) == info["iter"]
+    assert all(len(l) == width for l in lines)
+    assert [int(l.split()[0]) for l in lines] == list(range(1, info["iter"] + 1))
