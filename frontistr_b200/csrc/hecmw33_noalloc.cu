@@ -14,16 +14,27 @@
 // Limits and sharing rules:
 //   * at most kMaxRows block rows (one CTA of 256 rows per partial sum pair);
 //     larger N is rejected with HECMW33_ERR_BAD_INPUT before anything runs;
+//   * one whole-mesh matrix only (N == NP, no external nodes): every itemL / itemU
+//     must lie in 1..N, since X and B hold 3N doubles.  A domain of a decomposed mesh
+//     (items up to NP > N) needs a halo exchange and a sum over ranks that this call
+//     does not make.  The kernel checks every item before it reads X; an item outside
+//     1..N is skipped and the call returns HECMW33_ERR_BAD_INPUT with no residual;
+//   * null pointers (resid, ierr or any device array) are rejected before any launch;
+//   * the memset, the kernel and the copy of the result run on the legacy default
+//     stream (stream 0), which does not order against non-blocking streams: a caller
+//     whose arrays come from such a stream synchronises it before the call;
 //   * all calls share the scratch array and it keeps the last call's contents, so
 //     the arrival counter is cleared at the start of every call; calls that overlap
 //     on the GPU (from several host threads, or on several devices' streams sharing
 //     one context) race on it and must be serialised by the caller;
 //   * the first call on a device looks up the array's device address there
-//     (cudaGetSymbolAddress with that device current); make that first call before
-//     any stream capture.
+//     (cudaGetSymbolAddress with that device current) and keeps it for the life of
+//     the process; make that first call before any stream capture.  cudaDeviceReset
+//     between calls is not supported: the module may load again at another address.
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstring>
 #include <mutex>
 #include <string>
 
@@ -39,7 +50,11 @@ constexpr int kRowsPerCta = 256;
 constexpr int kMaxParts = 8192;                     // CTAs, i.e. partial-sum pairs
 constexpr int kMaxRows = kMaxParts * kRowsPerCta;  // 2,097,152 block rows
 // layout: [0, kMaxParts) r.r partials, [kMaxParts, 2 kMaxParts) b.b partials,
-// [2 kMaxParts] result, [2 kMaxParts + 1] arrival counter (as unsigned int)
+// [2 kMaxParts] result, [2 kMaxParts + 1] arrival counter (as unsigned int),
+// [2 kMaxParts + 2] count of items outside 1..N (as unsigned int)
+constexpr int kResult = 2 * kMaxParts;
+constexpr int kCounter = kResult + 1;
+constexpr int kBadItems = kResult + 2;
 constexpr int kScratchDoubles = 2 * kMaxParts + 8;
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
@@ -70,6 +85,8 @@ __device__ double block_sum(double v, double *sh) {
 // One thread per block row: r_i = b_i - (D_i x_i + sum_L A x + sum_U A x), with the
 // hecmwST arrays as given (1-based items); per-CTA partials of r.r and b.b in the
 // scratch array; the last CTA sums them in a fixed order and stores the result.
+// An item outside 1..N is counted in the scratch array and its block skipped, so X
+// is never read outside its 3N entries.
 __global__ void __launch_bounds__(kRowsPerCta) rel_resid_kernel(
     int N, const int *__restrict__ indexL, const int *__restrict__ itemL, const int *__restrict__ indexU,
     const int *__restrict__ itemU, const double *__restrict__ D, const double *__restrict__ AL,
@@ -91,6 +108,10 @@ __global__ void __launch_bounds__(kRowsPerCta) rel_resid_kernel(
       const double *A = pass ? AU : AL;
       for (int j = index[i]; j < index[i + 1]; j++) {
         const int c = item[j] - 1;
+        if (c < 0 || c >= N) {
+          atomicAdd(reinterpret_cast<unsigned int *>(scratch + kBadItems), 1u);
+          continue;
+        }
         const double *a = A + 9 * size_t(j);
         const double c0 = X[3 * c], c1 = X[3 * c + 1], c2 = X[3 * c + 2];
         y0 += a[0] * c0 + a[1] * c1 + a[2] * c2;
@@ -105,7 +126,7 @@ __global__ void __launch_bounds__(kRowsPerCta) rel_resid_kernel(
   }
   rr = block_sum(rr, sh);
   bb = block_sum(bb, sh);
-  unsigned int *counter = reinterpret_cast<unsigned int *>(scratch + 2 * kMaxParts + 1);
+  unsigned int *counter = reinterpret_cast<unsigned int *>(scratch + kCounter);
   if (threadIdx.x == 0) {
     scratch[blockIdx.x] = rr;
     scratch[kMaxParts + blockIdx.x] = bb;
@@ -124,7 +145,7 @@ __global__ void __launch_bounds__(kRowsPerCta) rel_resid_kernel(
   sbb = block_sum(sbb, sh);
   if (threadIdx.x == 0) {
     if (sbb == 0.0) sbb = 1.0;  // hecmw_rel_resid_L2_33: b.b = 0 counts as 1
-    scratch[2 * kMaxParts] = sqrt(srr / sbb);
+    scratch[kResult] = sqrt(srr / sbb);
     *counter = 0u;
   }
 }
@@ -154,30 +175,48 @@ HECMW33_API void hecmw33_gpu_rel_resid_noalloc(const int *N, const int *d_indexL
                                                const int *d_indexU, const int *d_itemU, const double *d_D,
                                                const double *d_AL, const double *d_AU, const double *d_X,
                                                const double *d_B, double *resid, int *ierr) {
-  if (ierr) *ierr = 0;
+  if (!ierr) return;
+  *ierr = 0;
+  if (!resid || !d_indexL || !d_itemL || !d_indexU || !d_itemU || !d_D || !d_AL || !d_AU || !d_X || !d_B) {
+    h33::set_last_error("hecmw33_gpu_rel_resid_noalloc: a null pointer among resid and the device arrays");
+    *ierr = HECMW33_ERR_BAD_INPUT;
+    return;
+  }
   const int n = N ? *N : -1;
   if (n <= 0 || n > kMaxRows) {
     h33::set_last_error("hecmw33_gpu_rel_resid_noalloc: N = " + std::to_string(n) + " outside 1.." +
                         std::to_string(kMaxRows) + " (the size of its static scratch array)");
-    if (ierr) *ierr = HECMW33_ERR_BAD_INPUT;
+    *ierr = HECMW33_ERR_BAD_INPUT;
     return;
   }
   double *scratch = nullptr;
   cudaError_t e = scratch_on_current_device(&scratch);
   const int grid = (n + kRowsPerCta - 1) / kRowsPerCta;
-  if (e == cudaSuccess)
-    e = cudaMemsetAsync(scratch + 2 * kMaxParts + 1, 0, sizeof(double), 0);  // arrival counter
+  if (e == cudaSuccess)  // arrival counter and bad-item count
+    e = cudaMemsetAsync(scratch + kCounter, 0, 2 * sizeof(double), 0);
   if (e == cudaSuccess) {
     rel_resid_kernel<<<grid, kRowsPerCta, 0, 0>>>(n, d_indexL, d_itemL, d_indexU, d_itemU, d_D, d_AL, d_AU,
                                                   d_X, d_B, scratch);
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess)
-    e = cudaMemcpy(resid, scratch + 2 * kMaxParts, sizeof(double), cudaMemcpyDeviceToHost);
+  double tail[3] = {0.0, 0.0, 0.0};  // result, arrival counter, bad-item count
+  if (e == cudaSuccess) e = cudaMemcpy(tail, scratch + kResult, sizeof(tail), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) {
     h33::set_last_error(std::string("hecmw33_gpu_rel_resid_noalloc: ") + cudaGetErrorString(e));
-    if (ierr) *ierr = HECMW33_ERR_CUDA;
+    *ierr = HECMW33_ERR_CUDA;
+    return;
   }
+  unsigned int bad = 0;
+  static_assert(sizeof(unsigned int) <= sizeof(double), "bad-item count fits its slot");
+  std::memcpy(&bad, &tail[2], sizeof(bad));
+  if (bad != 0) {
+    h33::set_last_error("hecmw33_gpu_rel_resid_noalloc: " + std::to_string(bad) +
+                        " itemL/itemU entries outside 1..N (a matrix with external nodes, NP > N, is not "
+                        "accepted)");
+    *ierr = HECMW33_ERR_BAD_INPUT;
+    return;
+  }
+  *resid = tail[0];
 }
 
 }  // extern "C"

@@ -149,7 +149,9 @@ HECMW33_API void hecmw33_gpu_set_domain(const int *handle, const int *n_neighbor
 /* Iarray(21) = ITERLOG = 1 (hecmw_solver_CG.f90:251-253): the CG and BiCGSTAB record RESID
  * of every iteration and print the reference's "ITER RESID" lines ('(i7, 1pe16.6)') on
  * stdout when the solve returns; GMRES, GPBiCG, CR, GMRESR and GMRESREN print each
- * iteration's line in their reference's format as they go.
+ * iteration's line in their reference's format as they go.  Solves in precision modes 2
+ * and 3 (Iarray(42)) and with the learned preconditioner (Iarray(43)) have no reference
+ * counterpart and print no history lines.
  * Iarray(14) = ESTCOND > 0 (hecmw_solver_CG.f90:256-264, 299-301): the CG records ALPHA
  * and BETA; every ESTCOND iterations and at the end of a solve without error the
  * extreme eigenvalues of the Lanczos tridiagonal are printed on stdout as
@@ -306,10 +308,19 @@ HECMW33_API void hecmw33_gpu_time_spmv(const int *handle, const int *reps, doubl
  * 1-based items, row-major 3x3 blocks, vectors of 3N doubles).  No handle, no
  * device or pinned allocation: the scratch space is a static 131 kB array in the
  * library, held by every GPU that loads it.  N is limited to 2,097,152 block rows
- * (larger N: HECMW33_ERR_BAD_INPUT, nothing runs).  *resid is a host double; the
- * call returns when it is written.  Calls share the scratch array: calls that
- * overlap on the GPU race and must be serialised.  The first call on a device looks
- * up the array's address there; make it before any stream capture. */
+ * (larger N: HECMW33_ERR_BAD_INPUT, nothing runs).
+ * Whole-mesh matrices only (N == NP): every itemL / itemU entry must lie in 1..N.  A
+ * domain of a decomposed mesh (external nodes N+1..NP) is rejected: the kernel checks
+ * every item before it reads X, skips one outside 1..N, and the call then returns
+ * HECMW33_ERR_BAD_INPUT without a residual.  Null pointers are rejected with
+ * HECMW33_ERR_BAD_INPUT before anything runs.
+ * *resid is a host double; the call returns when it is written.  The work is ordered
+ * on the legacy default stream (stream 0): arrays produced on a non-blocking stream
+ * must be complete (that stream synchronised) before the call.  Calls share the
+ * scratch array: calls that overlap on the GPU race and must be serialised.  The
+ * first call on a device looks up the array's address there and keeps it for the
+ * process; make it before any stream capture, and do not cudaDeviceReset between
+ * calls. */
 HECMW33_API void hecmw33_gpu_rel_resid_noalloc(const int *N, const int *d_indexL, const int *d_itemL,
                                                const int *d_indexU, const int *d_itemU,
                                                const double *d_D, const double *d_AL,

@@ -1,20 +1,24 @@
-"""Extract the reference's CG golden vectors into a small JSON fixture.
+"""Extract the reference's CG and CR golden vectors into a small JSON fixture.
 
-Reads FrontISTR's own end-to-end solver test (tests/solver/CG/{SSOR,ILU0,DIAG}
-.msh/.cnt/.res.0.1 in the FrontISTR tree): a 99-node TET4 (type 341)
-cantilever solved by CG with SSOR (PRECOND=1), ILU(0) (PRECOND=10) and DIAG
-(PRECOND=3) to a relative residual of 1e-8.  The fixture keeps the mesh in
-the reference's internal node order (the order of the result file), the
-boundary conditions, and the DISPLACEMENT field that fistr1 wrote.
+Reads FrontISTR's own end-to-end solver tests (tests/solver/CG/{SSOR,ILU0,DIAG,
+ILU1,ILU2} and tests/solver/CR/{SSOR,ILU0,DIAG,ILU1,ILU2} .msh/.cnt/.res.0.1 in
+the FrontISTR tree): one 99-node TET4 (type 341) cantilever, the same mesh in
+every file, solved by CG (METHOD=CG) and by CR (METHOD=CR) with SSOR
+(PRECOND=1), ILU(0) (10), DIAG (3), block ILU(1) (11) and block ILU(2) (12) to a
+relative residual of 1e-8.  The fixture keeps the mesh in the reference's
+internal node order (the order of the result file), the boundary conditions,
+and the DISPLACEMENT field that fistr1 wrote for every (method, PRECOND):
+"displacement" holds the CG results by PRECOND, "displacement_by_method" holds
+{"CG": {PRECOND: field}, "CR": {PRECOND: field}}.
 
-Run once in a container that has the reference tree:
+Run once in a container that has the reference tree (the path is required):
     python tests/golden/make_golden.py /path/to/FrontISTR
 The output, tests/golden/tet4_cantilever_cg.json, is committed; nothing at
 test time reads the reference tree.
 """
+import argparse
 import json
 import os
-import sys
 
 
 def parse_msh(path):
@@ -135,12 +139,23 @@ def main(ref_root):
         "tol": 1.0e-8,
         "displacement": {},
     }
-    for name, precond in (("SSOR", 1), ("ILU0", 10), ("DIAG", 3)):
-        _, _, solver = parse_cnt(os.path.join(base, name + ".cnt"))
-        assert int(solver["PRECOND"]) == precond
-        o2, disp, _ = parse_res(os.path.join(base, name + ".res.0.1"))
-        assert o2 == order
-        out["displacement"][str(precond)] = disp
+    mesh_text = open(os.path.join(base, "SSOR.msh")).read()
+    out["displacement_by_method"] = {}
+    out["source"] = ("FrontISTR tests/solver/CG and tests/solver/CR (SSOR, ILU0, DIAG, ILU1, ILU2): "
+                     ".msh, .cnt, .res.0.1")
+    for method in ("CG", "CR"):
+        mdir = os.path.join(ref_root, "tests", "solver", method)
+        by_pc = out["displacement_by_method"].setdefault(method, {})
+        for name, precond in (("SSOR", 1), ("ILU0", 10), ("DIAG", 3), ("ILU1", 11), ("ILU2", 12)):
+            assert open(os.path.join(mdir, name + ".msh")).read() == mesh_text  # one mesh throughout
+            bc2, ld2, solver = parse_cnt(os.path.join(mdir, name + ".cnt"))
+            assert (bc2, ld2) == (bcs, loads)
+            assert solver["METHOD"] == method and int(solver["PRECOND"]) == precond
+            o2, disp, _ = parse_res(os.path.join(mdir, name + ".res.0.1"))
+            assert o2 == order
+            by_pc[str(precond)] = disp
+            if method == "CG" and precond in (1, 10, 3):
+                out["displacement"][str(precond)] = disp
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tet4_cantilever_cg.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=0)
@@ -148,4 +163,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("reference_root", help="root of a FrontISTR source tree (the directory holding tests/)")
+    main(ap.parse_args().reference_root)

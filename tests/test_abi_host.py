@@ -13,7 +13,7 @@ from frontistr_b200 import _abi
 from frontistr_b200._lib import gpu_lib
 from frontistr_b200.matrix import HecMatrix
 from frontistr_b200.mesh import box_system
-from frontistr_b200.solver import HecmwSolverError, colour_schedule
+from frontistr_b200.solver import HecmwSolverError, colour_schedule, last_error
 from oracle_ctypes import Oracle
 from test_oracle_golden import golden_system
 
@@ -97,3 +97,23 @@ def test_single_node_and_disconnected_profiles():
     ci, perm = colour_schedule(m2)
     ci_o, perm_o = oracle_schedule(m2, 10)
     assert np.array_equal(ci, ci_o) and np.array_equal(perm, perm_o)
+
+
+def test_rel_resid_noalloc_rejects_null_pointers():
+    """The allocation-free residual call checks its pointers on the host before any
+    CUDA call: a null device array (or a null resid) returns 9101 with a message."""
+    lib = gpu_lib()
+    buf = (ctypes.c_double * 16)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    res, err = ctypes.c_double(-1.0), ctypes.c_int(0)
+    n = ctypes.c_int(4)
+    for hole in range(10):
+        args = [p] * 9
+        if hole < 9:
+            args[hole] = None
+        rp = None if hole == 9 else ctypes.byref(res)
+        err.value = 0
+        lib.hecmw33_gpu_rel_resid_noalloc(ctypes.byref(n), *args, rp, ctypes.byref(err))
+        assert err.value == 9101, hole
+        assert "null pointer" in last_error()
+    assert res.value == -1.0

@@ -124,10 +124,20 @@ def test_gpu_iterlog(capfd):
     assert not re.search(r"^ *\d+ +[-+0-9.]+E[-+]\d+$", quiet, re.M)
     lines = [l for l in out.splitlines() if re.match(r"^ *\d+ +[-+0-9.]+E[-+]\d+$", l)]
     assert info["iter"] == info0["iter"] and len(lines) == info["iter"]
-    for k, l in enumerate(lines[:20]):
+    assert abs(info["iter"] - ref["iter"]) <= 2
+    # every line, the recomputed true residuals of iterations 50, 100, ... and the
+    # last (recompute-on-convergence) among them; the device and the oracle sum in
+    # different orders, so late values agree to a looser bound than early ones
+    n = min(len(lines), ref["iter"])
+    for k, l in enumerate(lines[:n]):
         it, res = l.split()
         assert int(it) == k + 1 and len(l) == 23
-        assert abs(float(res) - ref["hist"][k]) <= 1e-5 * ref["hist"][k]
+        bound = 1e-5 if k < 20 else 1e-3
+        assert abs(float(res) - ref["hist"][k]) <= bound * ref["hist"][k], (k + 1, res, ref["hist"][k])
+    for k in (48, 49, 50):
+        if k < n:
+            assert abs(float(lines[k].split()[1]) - ref["hist"][k]) <= 1e-4 * ref["hist"][k], k + 1
+    assert float(lines[-1].split()[1]) <= 1e-8 and ref["hist"][ref["iter"] - 1] <= 1e-8
 
 
 @pytest.mark.gpu

@@ -128,6 +128,44 @@ def test_cg_golden_displacement(solver):
         assert np.abs(mm.X.reshape(-1, 3) - ref).max() <= 1e-9 * np.abs(ref).max()
 
 
+def test_golden_displacement_ilu_fill_and_cr(solver):
+    """The reference's other solver goldens on the GPU: tests/solver/CG/{ILU1,ILU2} to
+    1e-9, and tests/solver/CR/{SSOR,ILU0,DIAG,ILU1,ILU2}: the converged CR solution to
+    the difference of the goldens' stopping rule (1e-7), and for the natural-order
+    preconditioners the CR iterate at the goldens' stopping iteration (the first with
+    ||z||/||b|| <= 1e-8) to the oracle's bound (test_oracle_golden.py explains both)."""
+    from test_oracle_golden import CR_ITERATE_BOUND, cr_stop_iterations
+    g, m = golden_system()
+    for precond in (11, 12):
+        mm = m.copy()
+        mm.set_precond(precond)
+        mm.set_iter(10000)
+        info = solver.solve(mm)
+        assert info["error"] == 0
+        ref = np.array(g["displacement_by_method"]["CG"][str(precond)])
+        assert np.abs(mm.X.reshape(-1, 3) - ref).max() <= 1e-9 * np.abs(ref).max(), precond
+    for precond in (1, 10, 3, 11, 12):
+        ref = np.array(g["displacement_by_method"]["CR"][str(precond)])
+        scale = np.abs(ref).max()
+        mm = m.copy()
+        mm.set_method(7)
+        mm.set_precond(precond)
+        mm.set_iter(10000)
+        info = solver.solve(mm)
+        assert info["error"] == 0 and info["resid"] <= 1e-8
+        assert np.abs(mm.X.reshape(-1, 3) - ref).max() <= 1e-7 * scale, precond
+        if precond == 1:
+            continue  # the goldens' SSOR ran in natural order; the device's is multicoloured
+        _, k_z = cr_stop_iterations(m, precond, g["tol"])
+        mm = m.copy()
+        mm.set_method(7)
+        mm.set_precond(precond)
+        mm.set_iter(k_z)
+        info = solver.solve(mm)
+        assert info["error"] == 3001 and info["iter"] == k_z
+        assert np.abs(mm.X.reshape(-1, 3) - ref).max() <= CR_ITERATE_BOUND[precond] * scale, precond
+
+
 def test_cg_deterministic(solver):
     m = SYSTEMS["box_16x16x64"]
     a, b = m.copy(), m.copy()

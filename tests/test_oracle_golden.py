@@ -1,9 +1,10 @@
 """Pins the CPU oracle (and the host assembler) to the reference's own golden vectors.
 
 Fixture: tests/golden/tet4_cantilever_cg.json, extracted by make_golden.py from
-FrontISTR's tests/solver/CG: a 99-node TET4 cantilever (E=4000, nu=0.3, 9 nodes
-clamped, -1.0 z-load on node 3121) solved with CG + SSOR / ILU(0) / DIAG to a
-relative residual of 1e-8.  fistr1's DISPLACEMENT field is the known answer.
+FrontISTR's tests/solver/CG and tests/solver/CR: a 99-node TET4 cantilever
+(E=4000, nu=0.3, 9 nodes clamped, -1.0 z-load on node 3121) solved with CG and
+with CR, each with SSOR / ILU(0) / DIAG / ILU(1) / ILU(2), to a relative residual
+of 1e-8.  fistr1's DISPLACEMENT field is the known answer.
 
 The reference's own comparison (tests/compare_res.pl:7-33) pins field L2 norms
 to 1e-4 relative; a CG solve to 1e-8 on this small, well-conditioned system
@@ -46,6 +47,95 @@ def test_oracle_matches_reference_displacement(precond, coloured):
     # field L2 norm as compare_res.pl measures it
     assert abs(np.linalg.norm(u) - np.linalg.norm(ref)) <= 1e-8 * np.linalg.norm(ref)
     assert out["resid_true"] < g["tol"]
+
+
+@pytest.mark.parametrize("precond", [11, 12])
+def test_oracle_matches_reference_displacement_ilu_fill(precond):
+    """fistr1's results of tests/solver/CG/{ILU1,ILU2} (CG with block ILU(1) / ILU(2),
+    hecmw_precond_BILU_33.f90:371-1337) against the oracle's, on the same mesh."""
+    g, m = golden_system()
+    m.set_precond(precond)
+    m.set_iter(10000)
+    m.set_resid(g["tol"])
+    out = Oracle(m).solve(coloured=1)
+    assert out["error"] == 0 and out["Iarray"][80] == 1
+    ref = np.array(g["displacement_by_method"]["CG"][str(precond)])
+    assert np.abs(out["X"].reshape(-1, 3) - ref).max() <= 1e-9 * np.abs(ref).max()
+    assert out["resid_true"] < g["tol"]
+
+
+def cr_stop_iterations(m, precond, tol, coloured=0):
+    """The first iteration at which the preconditioned CR's recursive residual
+    ||b - A x||/||b|| (the test of hecmw_solver_CR.f90:216-253) and the norm of its
+    preconditioned residual ||z||/||b|| fall to tol: the CR recurrences of
+    hecmw_solver_CR.f90:128-296 replayed with the oracle's matvec and preconditioner."""
+    orc = Oracle(m)
+    P = orc.precond(precond, coloured=coloured)
+    B = m.B.copy()
+    bn = B @ B
+    X = np.zeros_like(B)
+    rt = B - orc.matvec(X)
+    z = P.apply(rt)
+    p, az = z.copy(), orc.matvec(z)
+    ap = az.copy()
+    rtar_old = z @ az
+    k_rec = k_z = None
+    for it in range(1, 2000):
+        map_ = P.apply(ap)
+        alpha = rtar_old / (ap @ map_)
+        X += alpha * p
+        rt -= alpha * ap
+        z -= alpha * map_
+        if k_rec is None and np.sqrt(rt @ rt / bn) <= tol:
+            k_rec = it
+        if k_z is None and np.sqrt(z @ z / bn) <= tol:
+            k_z = it
+        if k_rec and k_z:
+            return k_rec, k_z
+        az = orc.matvec(z)
+        rtar = z @ az
+        beta, rtar_old = rtar / rtar_old, rtar
+        p = z + beta * p
+        ap = az + beta * ap
+    raise AssertionError("CR replay did not converge")
+
+
+# fistr1's CR goldens against the oracle's CR at the iteration where ||z||/||b|| first
+# reaches the tolerance; DIAG needs 187 iterations, over which the recurrences' rounding
+# (the reference's compiler may fuse multiply-adds, the oracle does not) grows to 1.4e-8
+CR_ITERATE_BOUND = {1: 1e-9, 10: 1e-9, 11: 1e-9, 12: 1e-9, 3: 5e-8}
+
+
+@pytest.mark.parametrize("precond", [1, 10, 3, 11, 12])
+def test_oracle_matches_reference_displacement_cr(precond):
+    """fistr1's results of tests/solver/CR/{SSOR,ILU0,DIAG,ILU1,ILU2} (METHOD=CR,
+    hecmw_solver_CR.f90:108-296) against the oracle's CR.
+
+    The committed .res files were written by a CR whose convergence test was the norm of
+    the preconditioned residual z: the oracle's CR iterate at the first iteration with
+    ||z||/||b|| <= 1e-8 reproduces them to rounding (k = 80 for SSOR, 79 ILU(0), 47
+    ILU(1), 34 ILU(2)), while the CR of the current source tests ||b - A x||/||b|| and
+    stops 3-10 iterations later.  So the iterates are pinned at that iteration, and the
+    converged solution (the current rule) to the difference the later stop makes.  fistr1
+    ran these on one thread, so SSOR runs in natural order (NColor = 1,
+    hecmw_precond_SSOR_33.F90:93-128), as the oracle's coloured=0 schedule."""
+    g, m = golden_system()
+    m.set_method(7)
+    m.set_precond(precond)
+    m.set_resid(g["tol"])
+    m.set_iter(10000)
+    ref = np.array(g["displacement_by_method"]["CR"][str(precond)])
+    scale = np.abs(ref).max()
+    out = Oracle(m).solve(coloured=0)
+    assert out["error"] == 0 and out["Iarray"][80] == 1 and out["resid_true"] < g["tol"]
+    k_rec, k_z = cr_stop_iterations(m, precond, g["tol"])
+    assert out["iter"] == k_rec  # the replay stops where the oracle does
+    assert k_z < k_rec
+    assert np.abs(out["X"].reshape(-1, 3) - ref).max() <= 1e-7 * scale
+    m.set_iter(k_z)
+    early = Oracle(m).solve(coloured=0)
+    assert early["error"] == 3001 and early["iter"] == k_z
+    assert np.abs(early["X"].reshape(-1, 3) - ref).max() <= CR_ITERATE_BOUND[precond] * scale
 
 
 def test_oracle_matvec_matches_scipy():

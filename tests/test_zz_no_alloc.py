@@ -81,3 +81,26 @@ def test_rel_resid_noalloc_rejects_sizes_beyond_its_scratch():
     got, err = _noalloc(lib, 2_097_153, d, tiny, tiny)
     assert err == 9101
     assert "2097152" in last_error()
+
+
+def test_rel_resid_noalloc_rejects_a_decomposed_domain():
+    """A domain of a decomposed mesh (external nodes N+1..NP in its items) is not a
+    whole-mesh matrix: the kernel skips every item outside 1..N before reading X
+    (which holds 3N doubles here) and the call returns 9101 without a residual."""
+    torch = pytest.importorskip("torch")
+    from frontistr_b200.domain import partition
+    lib = gpu_lib()
+    m = box_system(6, 5, 8, seed=2)
+    dom = partition(m, 2)[0].matrix
+    assert dom.NP > dom.N
+    d = {k: _dev(torch, getattr(dom, k)) for k in ("indexL", "itemL", "indexU", "itemU", "D", "AL", "AU")}
+    x_dev = _dev(torch, np.ones(3 * dom.N))
+    b_dev = _dev(torch, dom.B[:3 * dom.N])
+    torch.cuda.synchronize()
+    got, err = _noalloc(lib, dom.N, d, x_dev, b_dev)
+    assert err == 9101 and got == -1.0
+    assert "outside 1..N" in last_error()
+    # the whole mesh still gives a residual afterwards
+    d = {k: _dev(torch, getattr(m, k)) for k in ("indexL", "itemL", "indexU", "itemU", "D", "AL", "AU")}
+    got, err = _noalloc(lib, m.N, d, _dev(torch, np.zeros(3 * m.N)), _dev(torch, m.B))
+    assert err == 0 and abs(got - 1.0) <= 1e-15
