@@ -13,15 +13,19 @@ public dataset).  One step = one solve to relative residual 1e-8 with CG + SSOR
   e2e          seconds per solve through the drop-in C-ABI call with host buffers (pinned)
                (hecmw33_gpu_solve: matrix values + B + X uploaded, numeric
                preconditioner rebuild, solve, X downloaded), wall clock
-  roofline     the plain FP64 SpMV (spmv_kernel) against measured HBM bandwidth
+  roofline     the dominant kernel of the headline solve, one SSOR application (the
+               forward + backward colour sweeps), against measured HBM bandwidth;
+               roofline_spmv the plain FP64 SpMV (spmv_kernel)
   cpu_baseline the CPU oracle (C restatement of the reference's CG + SSOR,
-               OpenMP over all host cores) on a bounded sample of iterations,
-               extrapolated to this run's iteration count
+               OpenMP over all host cores) solving the same system to the same
+               tolerance, measured (setup reported separately)
+  parity       the GPU solves against that oracle solve: iterations, solution,
+               colour schedule
 
 The path does not shard (one GPU domain): with --gpus N, N independent replicas
 run, one per GPU (torch.distributed only for the barrier and the max).
-`--impl reference` times the CPU oracle alone (the reference's own CPU path is
-Fortran and cannot be built on this image).
+`--impl reference` times the CPU oracle alone, full solves to tolerance (the
+reference's own CPU path is Fortran and cannot be built on this image).
 """
 import argparse
 import json
@@ -47,7 +51,6 @@ def parse():
     ap.add_argument("--mesh", default="100,100,100", help="nx,ny,nz HEX8 elements")
     ap.add_argument("--precond", type=int, default=1)
     ap.add_argument("--tol", type=float, default=1e-8)
-    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision variant")
@@ -59,6 +62,7 @@ def parse():
     ap.add_argument("--no-domains", action="store_true", help="skip the decomposed-mesh measurement")
     ap.add_argument("--no-config3", action="store_true",
                     help="skip the mixed-precision measurement on the jittered heterogeneous 80^3 system")
+    ap.add_argument("--no-ilu0", action="store_true", help="skip the CG + ILU(0) measurement")
     ap.add_argument("--batch-systems", type=int, default=256)
     ap.add_argument("--batch-edges", default="8,40", help="element range per box edge of the batch")
     ap.add_argument("--spmv-only", type=int, default=0,
@@ -156,13 +160,13 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def spmv_traffic_from_profile(tag):
-    """Per-launch DRAM bytes of the SpMV from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "spmv_kernel_%s.txt" % tag)
+def traffic_from_profile(name, key="dram_bytes_per_launch_full"):
+    """Per-launch (or per-application) DRAM bytes from a committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_launch_full:"):
+        if line.startswith(key + ":"):
             return float(line.split(":")[1])
     return None
 
@@ -180,65 +184,98 @@ def solver_flags(m, precond, tol, maxit=20000):
     return m
 
 
-def cpu_oracle_sample(m, precond, iters_full, budget_s, steps=1):
-    """Times the CPU oracle (test infrastructure) on a bounded sample of iterations."""
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import numpy as np
     import oracle_ctypes
     oracle_ctypes.build()
-    L = oracle_ctypes.lib()
-    orc = oracle_ctypes.Oracle(m)
-    t0 = time.time()
+    return oracle_ctypes
+
+
+def oracle_full_solve(m, precond, tol, maxit=40000, reps=1, colouring=False):
+    """The CPU oracle (test infrastructure; the C restatement of hecmw_solve_CG with
+    the reference's SSOR / ILU(0) and serial dots, OpenMP over all host cores) solving
+    the same system to the same tolerance: preconditioner setup timed on its own, then
+    `reps` complete CG solves from X0 = 0, each timed; the last one's solution, its
+    iteration count and its true residual ||b - Ax|| / ||b||."""
+    oc = _oracle()
+    orc = oc.Oracle(m)
+    t0 = time.perf_counter()
     pc = orc.precond(precond, 10, 1.0, 1)
-    t_setup = time.time() - t0
-    X = np.zeros(3 * m.NP)
-    import ctypes
-    # calibrate with 3 iterations, then size the sample to the time budget
-    t3 = L.o33_cg_fixed_iters(ctypes.byref(orc.mat), pc.h, 1, 3, oracle_ctypes._dp(m.B), oracle_ctypes._dp(X))
-    n = int(max(5, min(iters_full, budget_s / max(t3 / 3.0, 1e-6))))
-    per_iter = []
-    for _ in range(steps):
-        X[:] = 0.0
-        t = L.o33_cg_fixed_iters(ctypes.byref(orc.mat), pc.h, 1, n, oracle_ctypes._dp(m.B), oracle_ctypes._dp(X))
-        per_iter.append(t / n)
-    cores = L.o33_max_threads()
-    return per_iter, n, cores, t_setup
+    t_setup = time.perf_counter() - t0
+    times, out = [], None
+    for _ in range(reps):
+        t = time.perf_counter()
+        out = pc.cg(m.B, maxit=maxit, tol=tol)
+        times.append(time.perf_counter() - t)
+    res = {"X": out["X"], "iter": int(out["iter"]), "error": int(out["error"]), "solve_s": times,
+           "setup_s": t_setup, "cores": int(oc.lib().o33_max_threads()),
+           "true_resid": float(orc.rel_resid(out["X"], m.B))}
+    if colouring and precond == 1:
+        ci, perm, _ = pc.ordering()
+        res["colouring"] = (ci, perm)
+    return res
 
 
-def iterations_for(nx, ny, nz, precond):
-    """Iteration count of the oracle's full solve for the reference arm (no GPU there)."""
-    p = os.path.join(ROOT, "tests", "golden", "oracle_iterations.json")
-    if os.path.exists(p):
-        d = json.load(open(p))
-        key = "%d,%d,%d/%d" % (nx, ny, nz, precond)
-        if key in d:
-            return int(d[key]), "oracle full solve (tests/golden/oracle_iterations.json)"
-    return None, None
+def cpu_baseline_from(ref, what, tol):
+    """The cpu_baseline object of a measured oracle solve."""
+    return {"value": statistics.median(ref["solve_s"]), "unit": "s", "cores": ref["cores"], "kind": "port",
+            "iterations": ref["iter"], "true_resid": ref["true_resid"], "setup_s": ref["setup_s"],
+            "runs": len(ref["solve_s"]),
+            "sample": "measured to tolerance: %d complete %s solve(s) of the C oracle to rel. residual %g "
+                      "(median), %d iterations, true residual %.3g; OpenMP over %d host threads, serial dots "
+                      "as the reference; preconditioner setup %.2f s reported separately"
+                      % (len(ref["solve_s"]), what, tol, ref["iter"], ref["true_resid"], ref["cores"],
+                         ref["setup_s"])}
+
+
+def parity_block(ref, gpu_iters, sols, colouring=None):
+    """GPU results against the oracle's solve of the same system: iteration difference,
+    ||X - X_oracle|| / ||X_oracle|| per variant, colour schedule identity."""
+    import numpy as np
+    xo = ref["X"]
+    nx = float(np.linalg.norm(xo))
+    out = {"oracle_iterations": ref["iter"], "gpu_iterations": gpu_iters,
+           "iter_diff": abs(int(gpu_iters) - ref["iter"]),
+           "x_rel_err_vs_oracle": {k: float(np.linalg.norm(v[:len(xo)] - xo) / nx) for k, v in sols.items()},
+           "oracle_true_resid": ref["true_resid"], "bars": {"iterations": 2, "x_rel": 1e-8}}
+    if colouring is not None and "colouring" in ref:
+        ci, perm = colouring
+        ci_o, perm_o = ref["colouring"]
+        out["colour_schedule_equal"] = bool(np.array_equal(ci, ci_o) and np.array_equal(perm, perm_o))
+        out["ncolors"] = int(len(ci) - 1)
+    first = next(iter(sols))
+    out["ok"] = bool(out["iter_diff"] <= 2 and out["x_rel_err_vs_oracle"][first] <= 1e-8 and
+                     out.get("colour_schedule_equal", True))
+    return out
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the CPU oracle (the reference's CG + SSOR restated in C; the
+    Fortran original cannot be built here) on the bench's system, each step one complete
+    solve to tolerance.  A solve takes tens of seconds on the host, so at most three
+    timed solves run (after `warmup` untimed solves capped at 20 iterations), and the
+    value is their median."""
     if rank != 0:
         return
     nx, ny, nz = (int(v) for v in args.mesh.split(","))
     m = solver_flags(build_system(nx, ny, nz), args.precond, args.tol)
-    iters, src = iterations_for(nx, ny, nz, args.precond)
-    if iters is None:
-        print(json.dumps({"impl": "reference", "unavailable": "no recorded oracle iteration count for this mesh"}))
-        return
-    budget = max(5.0, min(args.cpu_sample_s, 150.0 / max(1, args.steps + args.warmup)))
-    per_iter, n, cores, t_setup = cpu_oracle_sample(m, args.precond, iters, budget,
-                                                    steps=args.steps + args.warmup)
-    timed = per_iter[args.warmup:] or per_iter
-    value = statistics.mean(timed) * iters
+    reps = max(1, min(args.steps, 3))
+    oc = _oracle()
+    orc = oc.Oracle(m)
+    warm = orc.precond(args.precond, 10, 1.0, 1)
+    for _ in range(args.warmup):
+        warm.cg(m.B, maxit=20, tol=args.tol)  # warm-up: threads and pages, not timed
+    del warm
+    ref = oracle_full_solve(m, args.precond, args.tol, reps=reps)
+    value = statistics.median(ref["solve_s"])
+    what = {1: "CG+SSOR", 3: "CG+DIAG", 10: "CG+ILU(0)"}.get(args.precond, "CG")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(timed) * n * 1e3,
+        "steps": reps, "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": config_dict(nx, ny, nz, m, args),
-        "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port",
-                         "sample": "%d CG+SSOR iterations per step of the C oracle (OpenMP, serial dots as the "
-                                   "reference), per-iteration time x %d iterations (%s); setup %.2f s not included"
-                                   % (n, iters, src, t_setup)},
+        "iterations": ref["iter"], "true_resid": ref["true_resid"], "error": ref["error"],
+        "cpu_baseline": cpu_baseline_from(ref, what, args.tol),
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -298,6 +335,8 @@ def bench_config3(tol=1e-10):
     out = {"workload": "80x80x80 HEX8, jitter 0.2h, log-normal E (sigma 1), nu U[0.25, 0.40], seed 3; "
                        "CG+SSOR to %g" % tol, "dof": 3 * m.N, "modes": {}}
     ref = None
+    sols = {}
+    colouring = None
     with GpuSolver() as s:
         for name, mode in (("fp64", 0), ("bf16_precond", 1), ("fp32_restart", 2), ("fp32_reliable", 3)):
             recs = []
@@ -311,10 +350,16 @@ def bench_config3(tol=1e-10):
             info = s.last_solve_info()
             if mode == 0:
                 ref = g.X.copy()
+                colouring = s.colouring()
+            sols[name] = g.X.copy()
             out["modes"][name] = {"s": recs[-1]["t_solve"], "iterations": int(recs[-1]["iter"]),
                                   "outer": info["outer"], "error": int(recs[-1]["error"]),
                                   "true_resid": info["true_resid"],
                                   "rel_err_vs_fp64": float(np.linalg.norm(g.X - ref) / np.linalg.norm(ref))}
+    # for the oracle comparison made after the GPU work (bench main)
+    m.set_iter(40000)
+    m.set_resid(tol)
+    out.update(_sols=sols, _system=m, _colouring=colouring)
     return out
 
 
@@ -579,6 +624,57 @@ def bench_batched(args):
     return out
 
 
+def roofline_sweeps(sweeps, head, peak, peak_kind, tag):
+    """The roofline object for one SSOR application (forward + backward colour
+    sweeps), in the storage of the headline variant."""
+    key = "bf16" if (head.endswith("mixed") and "bf16" in sweeps) else "fp64"
+    sw = sweeps[key]
+    return {"bound": "hbm",
+            "kernel": "sweep_fwd_uni_kernel + sweep_bwd_uni_kernel: one SSOR application, all colours, %s"
+                      % ("BF16-stored values, FP32 diagonal LU" if key == "bf16" else "FP64"),
+            "achieved": sw["achieved"], "peak": peak, "unit": "GB/s", "frac": sw["frac"], "peak_kind": peak_kind,
+            "traffic": traffic_from_profile("ssor_sweeps_%s.txt" % tag, "dram_bytes_per_apply_%s" % key),
+            "algorithmic_bytes": sw["algorithmic_bytes"], "ms_per_apply": sw["ms_per_apply"]}
+
+
+def bench_ilu0(m, args, peak):
+    """CG + block ILU(0) (PRECOND = 10: natural order, hecmw_precond_BILU_33.f90:90-362)
+    on the same system, on its own handle: FP64 and BF16-stored factors, device time of
+    the solve, one preconditioner application timed live, the level count."""
+    import numpy as np
+    from frontistr_b200.solver import GpuSolver
+    out = {"workload": "same system, CG + block ILU(0) (PRECOND=10, natural order, level-scheduled sweeps) "
+                       "to %g" % args.tol}
+    sols = {}
+    with GpuSolver() as s:
+        g = m.copy()
+        g.set_precond(10)
+        rec = s.solve(g)
+        if rec["error"] != 0:
+            return {"failed": rec}
+        out["setup_s_first_call"] = rec["t_setup"]
+        ia, ra = g.Iarray.copy(), g.Rarray.copy()
+        for name, mode in (("fp64", 0), ("bf16_factors", 1)):
+            recs = []
+            for _ in range(3):  # warm + 2 timed
+                X = np.zeros(3 * m.N)
+                iam = ia.copy()
+                iam[41] = mode
+                recs.append(s.solve_resident(m.B, X, iam, ra.copy()))
+            info = s.last_solve_info()
+            sols[name] = X
+            out[name] = {"s": statistics.mean(r["t_solve"] for r in recs[1:]), "iterations": int(recs[-1]["iter"]),
+                         "error": int(recs[-1]["error"]), "true_resid": info["true_resid"],
+                         "levels_fwd_plus_bwd": info["sweep_groups"], "kernels": info["kernels"]}
+        for key, lp in (("fp64", 0), ("bf16_factors", 1)):
+            ms, nbytes = s.time_precond(5, lp)
+            out[key]["precond_apply"] = {"ms_per_apply": ms, "algorithmic_bytes": nbytes,
+                                         "achieved": nbytes / (ms * 1e-3) / 1e9,
+                                         "frac": nbytes / (ms * 1e-3) / 1e9 / peak}
+    out["_sols"] = sols
+    return out
+
+
 def config_dict(nx, ny, nz, m, args):
     return {"workload": "HEX8 cantilever %dx%dx%d elements (%d nodes, %d DOF, %d blocks), CG+%s to %g"
                         % (nx, ny, nz, m.N, 3 * m.N, m.NZ, {1: "SSOR", 3: "DIAG", 10: "ILU(0)"}.get(args.precond),
@@ -758,6 +854,17 @@ def main():
     spmv_ms = solver.time_spmv(20)
     peak, peak_kind = measured_peaks()
     achieved = info["spmv_bytes"] / (spmv_ms * 1e-3) / 1e9
+    gpu_colouring = solver.colouring() if args.precond == 1 else None
+
+    # the dominant kernels of an iteration: one preconditioner application (SSOR: the
+    # forward + backward colour sweeps), FP64 and BF16-stored, timed live the same way
+    sweeps = {}
+    for key, lp in (("fp64", 0), ("bf16", 1)):
+        if lp and args.no_mixed:
+            continue
+        ms, nbytes = solver.time_precond(20, lp)
+        sweeps[key] = {"ms_per_apply": ms, "algorithmic_bytes": nbytes, "achieved": nbytes / (ms * 1e-3) / 1e9,
+                       "frac": nbytes / (ms * 1e-3) / 1e9 / peak}
 
     # end-to-end through the drop-in call with host buffers: the caller's matrix
     # values, B and X sit in pinned host memory (page-locked, as a GPU-aware caller
@@ -806,13 +913,29 @@ def main():
     batched = None if args.no_batched else bench_batched(args)
     domains = None if args.no_domains else bench_domains(m, solver)
 
-    cpu = None
+    ilu0 = None if (args.no_ilu0 or world > 1) else bench_ilu0(m, args, peak)
+
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        per_iter, n, cores, t_setup = cpu_oracle_sample(m, args.precond, iters, args.cpu_sample_s)
-        cpu = {"value": per_iter[0] * iters, "unit": "s", "cores": cores, "kind": "port",
-               "sample": "%d CG+SSOR iterations of the C oracle (OpenMP over %d threads, serial dots as the "
-                         "reference), per-iteration time x %d GPU FP64 iterations; oracle setup %.2f s not "
-                         "included" % (n, cores, iters, t_setup)}
+        ref = oracle_full_solve(m, args.precond, args.tol, colouring=True)
+        what = {1: "CG+SSOR", 3: "CG+DIAG", 10: "CG+ILU(0)"}.get(args.precond, "CG")
+        cpu = cpu_baseline_from(ref, what, args.tol)
+        parity = parity_block(ref, variants["fp64"]["iterations"], sols, gpu_colouring)
+        if ilu0 is not None:
+            ref0 = oracle_full_solve(m, 10, args.tol)
+            ilu0["cpu_baseline"] = cpu_baseline_from(ref0, "CG+ILU(0)", args.tol)
+            ilu0["parity"] = parity_block(ref0, ilu0["fp64"]["iterations"], ilu0.pop("_sols"))
+        if config3 is not None:
+            sols3 = config3.pop("_sols")
+            m3 = config3.pop("_system")
+            ref3 = oracle_full_solve(m3, 1, 1e-10, colouring=True)
+            config3["cpu_baseline"] = cpu_baseline_from(ref3, "CG+SSOR", 1e-10)
+            config3["parity"] = parity_block(ref3, config3["modes"]["fp64"]["iterations"], sols3,
+                                             config3.pop("_colouring"))
+    for d in (ilu0, config3):
+        if d is not None:
+            for k in ("_sols", "_system", "_colouring"):
+                d.pop(k, None)
 
     if rank == 0:
         tag = "%dcube" % nx if nx == ny == nz else "%dx%dx%d" % (nx, ny, nz)
@@ -835,11 +958,16 @@ def main():
             "fp64_ms_per_iteration": iter_s * 1e3,
             "fp64_iteration_GBps": info["iter_bytes"] / iter_s / 1e9,
             "setup_s_first_call": info0["t_setup"],
-            "roofline": {"bound": "hbm", "kernel": "spmv_kernel (plain FP64 SpMV, y = A x)",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": spmv_traffic_from_profile(tag),
-                         "algorithmic_bytes": info["spmv_bytes"], "ms_per_launch": spmv_ms},
+            "roofline": roofline_sweeps(sweeps, head, peak, peak_kind, tag),
+            "roofline_spmv": {"bound": "hbm", "kernel": "spmv_kernel (plain FP64 SpMV, y = A x)",
+                              "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                              "peak_kind": peak_kind,
+                              "traffic": traffic_from_profile("spmv_kernel_%s.txt" % tag),
+                              "algorithmic_bytes": info["spmv_bytes"], "ms_per_launch": spmv_ms},
+            "precond_apply": sweeps,
             "cpu_baseline": cpu,
+            "parity": parity,
+            "ilu0": ilu0,
             "e2e": e2e,
             "gpu_launches": variants[head]["kernels"] * args.steps,
             "clocks": clk,

@@ -28,6 +28,7 @@ SIGNATURES = {
     "hecmw33_gpu_last_solve_info": [_i, _i, _d, _i],
     "hecmw33_gpu_condition_estimate": [_i, _i, _d, _d, _i],
     "hecmw33_gpu_time_spmv": [_i, _i, _d, _i],
+    "hecmw33_gpu_time_precond": [_i, _i, _i, _d, _d, _i],
     "hecmw33_gpu_learn_record": [_i, _i, _i, _i, _i],
     "hecmw33_gpu_learn_train": [_i, _i, _d, _d, _i],
     "hecmw33_gpu_learn_weights": [_i, _i, ctypes.POINTER(ctypes.c_float), _i, _i],

@@ -3998,6 +3998,40 @@ HECMW33_API void hecmw33_gpu_time_spmv(const int *handle, const int *reps, doubl
   H33_ENTRY_END
 }
 
+HECMW33_API void hecmw33_gpu_time_precond(const int *handle, const int *reps, const int *lowp,
+                                          double *ms_per_apply, double *bytes_per_apply, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  Solver &S = get(handle);
+  DeviceGuard dg(S.device);
+  if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix");
+  Precond &P = S.pc;
+  if (!P.valid) throw Failure(HECMW33_ERR_BAD_INPUT, "no preconditioner: solve once first");
+  const int lp = (lowp && *lowp && P.kind != 3) ? 1 : 0;
+  if (lp) ensure_lowp(S);
+  const Views<double> V = views(S, 0.0, lp);
+  const int n = std::max(1, *reps);
+  // z = M^-1 r on the resident r (the last solve's residual), one pass (iterPREmax = 1)
+  launch_sweep<double, false>(S, V, S.r.p, S.w.p, nullptr);
+  H33_CUDA(cudaEventRecord(S.ev0, S.stream));
+  for (int i = 0; i < n; i++) launch_sweep<double, false>(S, V, S.r.p, S.w.p, nullptr);
+  H33_CUDA(cudaGetLastError());
+  H33_CUDA(cudaEventRecord(S.ev1, S.stream));
+  S.sync();
+  float ms = 0.0f;
+  H33_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+  *ms_per_apply = double(ms) / n;
+  // algorithmic bytes of one forward + backward application: every off-diagonal block
+  // once (values + column index), the diagonal LU read by both sweeps, the row
+  // pointers of both triangles, and r read / z written and read back per sweep
+  const double nb = double(S.NPL) + double(S.NPU), nn = double(S.N);
+  const double vb = lp ? 18.0 : 72.0, ab = lp ? 36.0 : 72.0;
+  if (bytes_per_apply)
+    *bytes_per_apply = P.kind == 3 ? nn * (ab + 48.0)
+                                   : nb * (vb + 4.0) + 2.0 * ab * nn + 2.0 * 4.0 * 2.0 * (nn + 1.0) + 2.0 * 2.0 * 24.0 * nn;
+  H33_ENTRY_END
+}
+
 HECMW33_API void hecmw33_gpu_learn_record(const int *handle, const int *enable, const int *max_pairs,
                                           int *npairs, int *ierr) {
   if (ierr) *ierr = 0;

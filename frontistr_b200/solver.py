@@ -410,6 +410,16 @@ class GpuSolver:
         self._check(err.value, fatal_only=False)
         return ms.value
 
+    def time_precond(self, reps=20, lowp=0):
+        """(ms per application, algorithmic bytes per application) of the resident
+        preconditioner, one pass z = M^-1 r, timed with device events."""
+        ms, nbytes = ctypes.c_double(0), ctypes.c_double(0)
+        err = ctypes.c_int(0)
+        self.lib.hecmw33_gpu_time_precond(ctypes.byref(self.handle), _i(reps), _i(lowp), ctypes.byref(ms),
+                                          ctypes.byref(nbytes), ctypes.byref(err))
+        self._check(err.value, fatal_only=False)
+        return ms.value, nbytes.value
+
 
 _default = None
 

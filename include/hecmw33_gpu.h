@@ -300,6 +300,19 @@ HECMW33_API void hecmw33_gpu_last_solve_info(const int *handle, int *info, doubl
 HECMW33_API void hecmw33_gpu_time_spmv(const int *handle, const int *reps, double *ms_per_launch,
                                        int *ierr);
 
+/* Times `reps` back-to-back applications of the resident preconditioner, one pass
+ * z = M^-1 r (hecmw_precond_apply with iterPREmax = 1, hecmw_precond.f90:86-172; for
+ * SSOR the forward and backward colour sweeps of hecmw_precond_SSOR_33.F90:302-405, for
+ * ILU(p) the level-scheduled sweeps of hecmw_precond_BILU_33.f90), on the last solve's
+ * residual, with device events on the handle's stream.  *lowp = 1 times the
+ * BF16-stored factors of precision mode 1.  *ms_per_apply receives the average;
+ * *bytes_per_apply (may be NULL) the algorithmic bytes of one application:
+ * 76 B per off-diagonal block (22 B with *lowp), the diagonal LU read by both sweeps
+ * (72 B per node each, 36 B with *lowp), both triangles' row pointers and 96 B of
+ * vector traffic per node.  Needs a solve (or a preconditioner setup) first. */
+HECMW33_API void hecmw33_gpu_time_precond(const int *handle, const int *reps, const int *lowp,
+                                          double *ms_per_apply, double *bytes_per_apply, int *ierr);
+
 /* No counterpart in the reference.  For callers that cannot allocate GPU memory
  * (their device memory is owned in full by another allocator, or allocation is
  * forbidden between their solves): the relative residual ||b - A x|| / ||b|| of

@@ -49,8 +49,7 @@ def test_reference_arm_under_torchrun_world2():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
-           "--impl", "reference", "--gpus", "2", "--mesh", "16,16,64", "--steps", "1", "--warmup", "1",
-           "--cpu-sample-s", "1"]
+           "--impl", "reference", "--gpus", "2", "--mesh", "16,16,64", "--steps", "1", "--warmup", "1"]
     env = dict(os.environ, OMP_NUM_THREADS="2")
     p = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT, env=env)
     assert p.returncode == 0, p.stderr[-2000:]
@@ -59,3 +58,8 @@ def test_reference_arm_under_torchrun_world2():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["unit"] == "s"
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "port"
+    # one complete solve to tolerance, not an extrapolated sample
+    assert d["cpu_baseline"]["sample"].startswith("measured to tolerance")
+    assert d["true_resid"] <= 1e-8 and d["error"] == 0
+    golden = json.load(open(os.path.join(ROOT, "tests", "golden", "oracle_iterations.json")))
+    assert d["iterations"] == golden["16,16,64/1"]
