@@ -11,6 +11,7 @@
 // hecmw_solve_CG decisions (hecmw_solver_CG.f90:164-279).
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
 #include "h33_common.cuh"
@@ -433,6 +434,44 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<R> A, const R *
   if (MODE == 2) reduce_finish(dot, partials, blockIdx.x, gridDim.x, &st->ticket[1], [&](double v) { fin_pq(st, v); });
 }
 
+// Start of a node-order level launch.  pre & 1: the launch was made with programmatic
+// stream serialisation -- let the next level launch as soon as all CTAs of this one
+// run, and wait for the previous level only after the static work; that work brings
+// into L2 this warp's slices' values (pre & 2) and columns (pre & 4) and its rows'
+// diagonal LU entries (pre & 8).  Nothing before the wait reads what an earlier
+// launch wrote.
+template <class TV, class TA, int K>
+__device__ __forceinline__ void level_prologue(const SellView<TV> &A, const TA *alu, int npos, int sbeg, int send,
+                                               int pre) {
+  if (pre & 1) asm volatile("griddepcontrol.launch_dependents;" :::);
+  if (pre & 14) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int s = sbeg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < send; s += nwarps) {
+      const int nslots = A.len[s];
+      if (lane == 0 && nslots > 0 && (pre & 6)) {
+        const int slot0 = A.slot0[s];
+        if (pre & 2)
+          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.val + size_t(slot0) * 288),
+                       "r"(unsigned(nslots) * 288u * unsigned(sizeof(TV)))
+                       : "memory");
+        if (pre & 4)
+          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.col + size_t(slot0) * 32),
+                       "r"(unsigned(nslots) * 128u)
+                       : "memory");
+      }
+      const int roff = lane / K;
+      if ((pre & 8) && (lane & (K - 1)) == 0 && roff < A.nrows[s]) {
+        const int row = A.row0[s] + roff;
+#pragma unroll
+        for (int e = 0; e < 9; e++) asm volatile("prefetch.global.L2 [%0];" ::"l"(alu + size_t(e) * npos + row));
+      }
+    }
+  }
+  if (pre & 1) asm volatile("griddepcontrol.wait;" ::: "memory");
+  else pdl_entry();
+}
+
 // Node-order sweeps (the ILU(0) level schedules, whose forward and backward orders
 // differ).  Forward sweep over the slices [sbeg, send) of one level, each row spread
 // over K lanes:  z(node) = LU^-1 ( r(node) - sum_lower A z(col) )
@@ -441,8 +480,8 @@ template <class R, class TV, class TA, int K>
 __global__ void __launch_bounds__(kThreads) sweep_fwd_kernel(SellView<TV> L, const int *__restrict__ perm,
                                                              const TA *__restrict__ alu, int npos,
                                                              const R *__restrict__ r, R *__restrict__ z,
-                                                             int sbeg, int send, const CgState *st) {
-  pdl_entry();
+                                                             int sbeg, int send, const CgState *st, int pre) {
+  level_prologue<TV, TA, K>(L, alu, npos, sbeg, send, pre);
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
   const int roff = lane / K;
@@ -474,8 +513,8 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, con
                                                              const R *__restrict__ r, R *__restrict__ z,
                                                              int sbeg, int send, CgState *st,
                                                              double *partials, int part_base,
-                                                             int part_total) {
-  pdl_entry();
+                                                             int part_total, int pre) {
+  level_prologue<TV, TA, K>(U, alu, npos, sbeg, send, pre);
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
   const int roff = lane / K;
@@ -512,7 +551,9 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_kernel(SellView<TV> U, con
 
 // Gather of one slice: this lane's blocks of slots slot0 .. slot0+nslots-1 (in
 // reverse for BACKWARD), then the sum over the row's K lanes.
-template <class R, class TV, int K, bool BACKWARD>
+// XL2: x was written during this launch (by other CTAs): read it through L2, never
+// the read-only path.
+template <class R, class TV, int K, bool BACKWARD, bool XL2 = false>
 __device__ __forceinline__ void slice_gemv_u(const SellView<TV> &A, int slot0, int nslots, int lane,
                                              const R *__restrict__ x, R &y0, R &y1, R &y2) {
 #pragma unroll 4
@@ -520,7 +561,9 @@ __device__ __forceinline__ void slice_gemv_u(const SellView<TV> &A, int slot0, i
     const int sl = slot0 + (BACKWARD ? nslots - 1 - kk : kk);
     const int c = __ldg(&A.col[sl * 32 + lane]);
     const TV *v = A.val + sl * 288 + lane;
-    const R x0 = __ldg(&x[3 * c]), x1 = __ldg(&x[3 * c + 1]), x2 = __ldg(&x[3 * c + 2]);
+    const R x0 = XL2 ? __ldcg(&x[3 * c]) : __ldg(&x[3 * c]);
+    const R x1 = XL2 ? __ldcg(&x[3 * c + 1]) : __ldg(&x[3 * c + 1]);
+    const R x2 = XL2 ? __ldcg(&x[3 * c + 2]) : __ldg(&x[3 * c + 2]);
     const R v0 = ld_val<R>(v), v1 = ld_val<R>(v + 32), v2 = ld_val<R>(v + 64);
     const R v3 = ld_val<R>(v + 96), v4 = ld_val<R>(v + 128), v5 = ld_val<R>(v + 160);
     const R v6 = ld_val<R>(v + 192), v7 = ld_val<R>(v + 224), v8 = ld_val<R>(v + 256);
@@ -553,7 +596,8 @@ __device__ __forceinline__ void l2_prefetch_slots(const SellView<TV> &A, int slo
 }
 
 // First slot and slot count of slice t (relative to the colour's first slice).
-__device__ __forceinline__ void run_slots(const RunShape &sh, int t, int &slot0, int &nslots) {
+template <class Shape>
+__device__ __forceinline__ void run_slots(const Shape &sh, int t, int &slot0, int &nslots) {
   int r = 0;
   while (r + 1 < sh.nruns && sh.slice[r + 1] <= t) r++;
   nslots = sh.len[r];

@@ -32,6 +32,7 @@
 
 #include "h33_assemble.cuh"
 #include "h33_bicg.cuh"
+#include "h33_coarse.cuh"
 #include "h33_common.cuh"
 #include "h33_cr.cuh"
 #include "h33_domain.cuh"
@@ -86,6 +87,20 @@ bool pdl_mode() {
 template <class TV>
 constexpr int sweep_pre() {
   return sizeof(TV) <= 2 ? (1 | 2 | 4) : (1 | 4 | 8);
+}
+
+// level_prologue's mode for the node-order level launches of the block ILU sweeps:
+// programmatic launches whose static work, before the wait for the previous level,
+// brings into L2 the level's values, columns and diagonal LU entries (a level of the
+// natural-order schedule is a few MB, far from crowding the vectors out of L2).
+// HECMW33_LEVEL_PRE overrides it (0 = plain launches).
+template <class TV>
+int level_pre() {
+  static const int v = [] {
+    const char *e = std::getenv("HECMW33_LEVEL_PRE");
+    return e ? std::atoi(e) : (1 | 2 | 4 | 8);
+  }();
+  return v;
 }
 
 // HECMW33_MR_TILED=1: the multi-RHS loop's SpMM stages p through shared memory
@@ -254,6 +269,29 @@ struct Learned {
   std::vector<double> per;
   DevArray<double> losses;
   GnnGraph graph() const { return GnnGraph{n, nedges, ptr.p, col.p, rev.p, feat.p, s.p}; }
+  // the coarse space the network shapes (h33_coarse.cuh): aggregation and patterns
+  // (per matrix structure), prolongator, A P, dense coarse inverse (per matrix values
+  // and weights), application and training vectors
+  // coarse smoothing weights: 0 the network's omega, 1 omega = 0 (unsmoothed
+  // aggregation), 2 omega = 1/2 everywhere (the untrained network's output)
+  int coarse_mode = 0;
+  struct Coarse {
+    int built_for = -1, mask_version = -1, t0_version = -1;
+    int op_precond = -1, op_weights = -1, op_mode = -1;  // what the coarse inverse was built from
+    bool ok = false;                                    // coarse inverse usable
+    int n = 0, nagg = 0, nc = 0;
+    DevArray<int> agg, pptr, pagg, rptr, rnode, rpos, qptr, qagg, cptr, cagg, uptr, ucol, usrc;
+    DevArray<float> mask, x, out, omega, dout;
+    DevArray<double> t0, p, q, ac, gjc, gjd, bc, y, v, t0y, apy, dots;
+    DevArray<int> err;
+    float *one = nullptr;  // device 1.0f (the decode scale of the backward pass)
+    DevArray<float> one_buf;
+    CoarseView view() {
+      return CoarseView{n,      nagg,   nc,     agg.p,  pptr.p, pagg.p, rptr.p, rnode.p, rpos.p,
+                        qptr.p, qagg.p, cptr.p, cagg.p, uptr.p, ucol.p, usrc.p, mask.p,  t0.p,
+                        p.p,    q.p,    ac.p};
+    }
+  } C;
 };
 
 // One instantiated CG graph and the key of the device buffers it captured.
@@ -878,12 +916,13 @@ void launch_sweep_node(Solver &S, const SellView<TV> &lo, const SellView<TV> &up
   Precond &P = S.pc;
   cudaStream_t s = S.stream;
   const int *perm_b = P.alu_shared ? P.perm_fwd.p : P.perm_bwd.p;
+  const int pre = level_pre<TV>();
   const int gf = int(P.lo.group_slice.size()) - 1;
   for (int g = 0; g < gf; g++) {
     const int sb = P.lo.group_slice[g], se = P.lo.group_slice[g + 1];
     if (se <= sb) continue;
-    launch_k(s, sweep_fwd_kernel<R, TV, TA, K>, S.grid_sweep(se - sb), kThreads, lo, P.perm_fwd.p, alu_f, S.N, rin,
-             zout, sb, se, st);
+    launch_kp(s, (pre & 1) != 0, sweep_fwd_kernel<R, TV, TA, K>, S.grid_sweep(se - sb), kThreads, lo, P.perm_fwd.p,
+              alu_f, S.N, rin, zout, sb, se, static_cast<const CgState *>(st), pre);
   }
   const int gb = int(P.up.group_slice.size()) - 1;
   int total = 0;
@@ -895,8 +934,8 @@ void launch_sweep_node(Solver &S, const SellView<TV> &lo, const SellView<TV> &up
     const int grid = S.grid_sweep(std::max(se - sb, 1));
     // a group without slices still launches (one idle CTA) so that the reduction
     // ticket count stays exact
-    launch_k(s, sweep_bwd_kernel<R, TV, TA, K, FUSE_RHO>, grid, kThreads, up, perm_b, alu_b, S.N, rin, zout, sb, se,
-             st, S.partials.p, base, total);
+    launch_kp(s, (pre & 1) != 0, sweep_bwd_kernel<R, TV, TA, K, FUSE_RHO>, grid, kThreads, up, perm_b, alu_b, S.N,
+              rin, zout, sb, se, st, S.partials.p, base, total, pre);
     base += grid;
   }
 }
@@ -1112,32 +1151,15 @@ void ensure_bicg(Solver &S) {
     }
 }
 
+// z = zs + P Ac^-1 P^T r: the learned two-level preconditioner's coarse correction
+// (defined with the coarse space below).
 template <class R>
-void launch_gnn(Solver &S, const R *zs, const R *r, R *z, CgState *st, bool bf16_weights) {
-  Learned &L = S.L;
-  cudaStream_t s = S.stream;
-  const GnnGraph g = L.graph();
-  const int gw = std::max(1, std::min((S.N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8));
-  const int gt = S.grid_vec();
-  launch_k(s, gamma_kernel<R>, gt, kThreads, zs, S.n3(), st, S.partials.p);
-  if (bf16_weights) {
-    const __nv_bfloat16 *th = L.theta_bf16.p;
-    launch_k(s, gnn_encode_kernel<R, __nv_bfloat16>, gt, kThreads, g, th, zs, r, &st->gamma, nullptr, L.h[0].p, st);
-    for (int l = 0; l < kGnnLayers; l++)
-      launch_k(s, gnn_layer_kernel<__nv_bfloat16>, gw, kThreads, g, th, l, L.w.p, L.h[l].p, nullptr, L.h[l + 1].p, st);
-    launch_k(s, gnn_decode_kernel<R, __nv_bfloat16>, gt, kThreads, S.N, th, L.h[3].p, zs, &st->gamma, z, st);
-  } else {
-    const float *th = L.theta.p;
-    launch_k(s, gnn_encode_kernel<R, float>, gt, kThreads, g, th, zs, r, &st->gamma, nullptr, L.h[0].p, st);
-    for (int l = 0; l < kGnnLayers; l++)
-      launch_k(s, gnn_layer_kernel<float>, gw, kThreads, g, th, l, L.w.p, L.h[l].p, nullptr, L.h[l + 1].p, st);
-    launch_k(s, gnn_decode_kernel<R, float>, gt, kThreads, S.N, th, L.h[3].p, zs, &st->gamma, z, st);
-  }
-}
+void launch_coarse(Solver &S, const R *zs, const R *r, R *z, CgState *st);
 
-// One flexible-CG iteration with the learned preconditioner after SSOR
-// (iterPREmax = 1).  The network may be switched off on the device (fallback);
-// its kernels then only copy the SSOR output.
+// One flexible-CG iteration with the learned two-level preconditioner: SSOR, then the
+// coarse correction of the space the network shapes (iterPREmax = 1).  The correction
+// may be switched off on the device (fallback); its kernels then only copy the SSOR
+// output.
 template <class R>
 void launch_iteration_flex(Solver &S, const Views<R> &V, cudaGraphConditionalHandle h, int use_cond) {
   cudaStream_t s = S.stream;
@@ -1145,7 +1167,7 @@ void launch_iteration_flex(Solver &S, const Views<R> &V, cudaGraphConditionalHan
   const int n3 = S.n3();
   launch_k(s, iter_begin_kernel, 1, 32, st, h, use_cond);
   launch_sweep<R, false>(S, V, V.r, V.zs, st);
-  launch_gnn<R>(S, V.zs, V.r, V.z, st, true);
+  launch_coarse<R>(S, V.zs, V.r, V.z, st);
   launch_k(s, fcg_rho_kernel<R>, S.grid_vec(), kThreads, V.z, V.r, V.rold, n3, st, S.partials.p);
   launch_k(s, update_p_kernel<R>, S.grid_vec(), kThreads, V.z, V.p, n3, st);
   launch_k(s, spmv_kernel<R, 2>, S.grid_spmv(), kThreads, V.A, V.p, V.q, nullptr, st, S.partials.p);
@@ -1175,7 +1197,7 @@ void launch_iteration_reliable(Solver &S, int iterpremax, bool learned, cudaGrap
   launch_k(s, iter_begin_kernel, 1, 32, st, h, use_cond);
   if (learned) {
     launch_sweep<float, false>(S, V, V.r, V.zs, st);
-    launch_gnn<float>(S, V.zs, V.r, V.z, st, true);
+    launch_coarse<float>(S, V.zs, V.r, V.z, st);
     launch_k(s, fcg_rho_kernel<float>, S.grid_vec(), kThreads, V.z, V.r, V.rold, n3, st, S.partials.p);
   } else {
     launch_precond<float>(S, V, iterpremax, V.r, V.z, st);
@@ -1453,6 +1475,170 @@ void learned_edge_weights(Solver &S, bool bf16) {
   L.w_version = bf16 ? L.weights_version : -1;
 }
 
+// ---- the coarse space of the learned two-level preconditioner -----------------
+// HECMW33_COARSE_AGG: the largest number of aggregates (default 2000: 9x9x9-node
+// aggregates on a 101^3-node mesh, a 4,239-DOF coarse matrix).
+int coarse_max_aggregates() {
+  static const int v = [] {
+    const char *e = std::getenv("HECMW33_COARSE_AGG");
+    return e ? std::max(1, std::atoi(e)) : 2000;
+  }();
+  return v;
+}
+
+// Aggregates, patterns and buffers (once per matrix structure).
+void coarse_structure(Solver &S) {
+  auto &C = S.L.C;
+  if (C.built_for == S.generation) return;
+  Profile prof{S.N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
+  Aggregation ag;
+  aggregate_nodes(prof, coarse_max_aggregates(), ag);
+  BlockRows u;
+  unified_rows(prof, u);
+  if (u.ptr.back() > int64_t(std::numeric_limits<int>::max()))
+    throw Failure(HECMW33_ERR_BAD_INPUT, "coarse space: too many blocks for 32-bit row pointers");
+  std::vector<int> uptr(u.ptr.size());
+  for (size_t k = 0; k < u.ptr.size(); k++) uptr[k] = int(u.ptr[k]);
+  C.n = S.N;
+  C.nagg = ag.n_agg;
+  C.nc = 3 * ag.n_agg;
+  C.agg.upload(ag.agg, S.stream);
+  C.pptr.upload(ag.pptr, S.stream);
+  C.pagg.upload(ag.pagg, S.stream);
+  C.rptr.upload(ag.rptr, S.stream);
+  C.rnode.upload(ag.rnode, S.stream);
+  C.rpos.upload(ag.rpos, S.stream);
+  C.qptr.upload(ag.qptr, S.stream);
+  C.qagg.upload(ag.qagg, S.stream);
+  C.cptr.upload(ag.cptr, S.stream);
+  C.cagg.upload(ag.cagg, S.stream);
+  C.uptr.upload(uptr, S.stream);
+  C.ucol.upload(u.col, S.stream);
+  C.usrc.upload(u.src, S.stream);
+  const size_t n3 = size_t(S.n3()), nnzp = ag.pagg.size(), nnzq = ag.qagg.size(), nc = size_t(C.nc);
+  C.mask.alloc(n3);
+  C.x.alloc(size_t(S.N) * 6);
+  C.out.alloc(n3);
+  C.omega.alloc(n3);
+  C.dout.alloc(n3);
+  C.t0.alloc(9 * nnzp);
+  C.p.alloc(9 * nnzp);
+  C.q.alloc(9 * nnzq);
+  C.ac.alloc(nc * nc);
+  C.gjc.alloc(nc * kGjBlock);
+  C.gjd.alloc(size_t(kGjBlock) * kGjBlock);
+  C.bc.alloc(nc);
+  C.y.alloc(nc);
+  C.v.alloc(n3);
+  C.t0y.alloc(n3);
+  C.apy.alloc(n3);
+  C.dots.alloc(64);
+  C.err.alloc(1);
+  if (!C.one) {
+    const float one = 1.0f;
+    C.one_buf.upload(&one, 1, S.stream);
+    C.one = C.one_buf.p;
+  }
+  C.built_for = S.generation;
+  C.mask_version = C.t0_version = -1;
+  C.op_precond = C.op_weights = C.op_mode = -1;
+  C.ok = false;
+  S.sync();
+}
+
+// DOF mask, the network's static input and T0 (per matrix values).
+void coarse_values(Solver &S) {
+  auto &C = S.L.C;
+  if (C.t0_version == S.values_version) return;
+  const int gt = std::max(1, std::min((S.N + kThreads - 1) / kThreads, S.nsm * 8));
+  launch_k(S.stream, coarse_mask_kernel, gt, kThreads, C.view(), static_cast<const double *>(S.raw.p));
+  launch_k(S.stream, coarse_features_kernel, gt, kThreads, C.view(), C.x.p);
+  launch_k(S.stream, coarse_t0_kernel, gt, kThreads, C.view(), static_cast<const double *>(S.raw.p));
+  H33_CUDA(cudaGetLastError());
+  C.t0_version = S.values_version;
+}
+
+// omega = sigmoid(W_out h3) of the network on the static features: BF16 weights
+// (inference) or FP32 master weights with the activations kept (training).
+void coarse_omega(Solver &S, bool bf16, bool keep) {
+  Learned &L = S.L;
+  auto &C = L.C;
+  cudaStream_t s = S.stream;
+  const GnnGraph g = L.graph();
+  const int gw = std::max(1, std::min((S.N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8));
+  const int gt = std::max(1, std::min((S.N + kThreads - 1) / kThreads, S.nsm * 8));
+  learned_edge_weights(S, bf16);
+  if (bf16) {
+    const __nv_bfloat16 *th = L.theta_bf16.p;
+    launch_k(s, gnn_encode_static_kernel<__nv_bfloat16>, gt, kThreads, S.N, th, static_cast<const float *>(C.x.p),
+             L.h[0].p);
+    for (int l = 0; l < kGnnLayers; l++)
+      launch_k(s, gnn_layer_kernel<__nv_bfloat16>, gw, kThreads, g, th, l, static_cast<const float *>(L.w.p),
+               static_cast<const float *>(L.h[l].p), static_cast<float *>(nullptr), L.h[l + 1].p,
+               static_cast<const CgState *>(nullptr));
+    launch_k(s, gnn_omega_kernel<__nv_bfloat16>, gt, kThreads, S.N, th, static_cast<const float *>(L.h[3].p), C.out.p,
+             C.omega.p);
+  } else {
+    const float *th = L.theta.p;
+    launch_k(s, gnn_encode_static_kernel<float>, gt, kThreads, S.N, th, static_cast<const float *>(C.x.p), L.h[0].p);
+    for (int l = 0; l < kGnnLayers; l++)
+      launch_k(s, gnn_layer_kernel<float>, gw, kThreads, g, th, l, static_cast<const float *>(L.w.p),
+               static_cast<const float *>(L.h[l].p), keep ? L.m[l].p : static_cast<float *>(nullptr), L.h[l + 1].p,
+               static_cast<const CgState *>(nullptr));
+    launch_k(s, gnn_omega_kernel<float>, gt, kThreads, S.N, th, static_cast<const float *>(L.h[3].p), C.out.p,
+             C.omega.p);
+  }
+  H33_CUDA(cudaGetLastError());
+}
+
+// P from omega (nullptr: omega = 0, the unsmoothed aggregation), A P, Ac = P^T A P
+// and its inverse in place (blocked Gauss-Jordan).  Returns false when a pivot of Ac
+// was not positive (the coarse correction is then not applied).
+bool coarse_operator(Solver &S, const float *omega) {
+  auto &C = S.L.C;
+  cudaStream_t s = S.stream;
+  const CoarseView cv = C.view();
+  const int gt = std::max(1, std::min((S.N + kThreads - 1) / kThreads, S.nsm * 8));
+  const int gw = std::max(1, std::min((S.N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 16));
+  launch_k(s, coarse_p_kernel, gt, kThreads, cv, omega);
+  launch_k(s, coarse_ap_kernel, gw, kThreads, cv, static_cast<const double *>(S.raw.p));
+  C.ac.zero(s);
+  C.err.zero(s);
+  launch_k(s, coarse_ac_kernel, std::max(1, S.nsm * 8), kThreads, cv);
+  const int n = C.nc;
+  const int tiles = (n + 63) / 64;
+  for (int k0 = 0; k0 < n; k0 += kGjBlock) {
+    const int nb = std::min(kGjBlock, n - k0);
+    gj_diag_kernel<<<1, 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p, C.err.p);
+    gj_save_col_kernel<<<std::max(1, std::min((n * nb + 255) / 256, S.nsm * 8)), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjc.p);
+    gj_row_kernel<<<std::max(1, (n + 255) / 256), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p);
+    gj_update_kernel<<<dim3(unsigned(tiles), unsigned(tiles)), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjc.p);
+    gj_col_kernel<<<std::max(1, (n + 255) / 256), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjc.p, C.gjd.p);
+  }
+  H33_CUDA(cudaGetLastError());
+  int err = 0;
+  H33_CUDA(cudaMemcpyAsync(&err, C.err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  S.sync();
+  C.ok = err == 0;
+  return C.ok;
+}
+
+// z = zs + P Ac^-1 P^T r (or z = zs when the correction is off), in the solve's stream.
+template <class R>
+void launch_coarse(Solver &S, const R *zs, const R *r, R *z, CgState *st) {
+  auto &C = S.L.C;
+  cudaStream_t s = S.stream;
+  const CoarseView cv = C.view();
+  const int gt = std::max(1, std::min((S.N + kThreads - 1) / kThreads, S.nsm * 8));
+  launch_k(s, coarse_restrict_kernel<R>, std::max(1, std::min((C.nagg + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8)),
+           kThreads, cv, r, C.bc.p, static_cast<const CgState *>(st));
+  launch_k(s, coarse_gemv_kernel, std::max(1, std::min((C.nc + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8)),
+           kThreads, C.nc, static_cast<const double *>(C.ac.p), static_cast<const double *>(C.bc.p), C.y.p,
+           static_cast<const CgState *>(st));
+  launch_k(s, coarse_prolong_kernel<R>, gt, kThreads, cv, static_cast<const double *>(C.y.p), zs, z,
+           static_cast<double *>(nullptr), static_cast<double *>(nullptr), static_cast<const CgState *>(st));
+}
+
 void learned_set_weights(Solver &S, const float *theta_host, bool reset_adam) {
   Learned &L = S.L;
   const int n = GnnOffsets::make().total;
@@ -1474,8 +1660,7 @@ void learned_set_weights(Solver &S, const float *theta_host, bool reset_adam) {
   S.sync();
 }
 
-// Deterministic initial weights (scaled Gaussian; the output layer starts small so
-// that the untrained network is close to plain SSOR).
+// Deterministic initial weights (scaled Gaussian; the output layer starts at zero).
 void learned_init_weights(Solver &S, uint64_t seed) {
   const GnnOffsets o = GnnOffsets::make();
   std::vector<float> th(size_t(o.total), 0.0f);
@@ -1500,18 +1685,40 @@ void learned_init_weights(Solver &S, uint64_t seed) {
       th[size_t(o.Wm[l] + k)] = float(normal() / std::sqrt(double(kGnnWidth)) / 8.0);
     }
   }
-  for (int k = 0; k < 3 * kGnnWidth; k++) th[size_t(o.W_out + k)] = float(0.01 * normal());
+  // W_out = 0: the untrained network gives omega = 1/2 everywhere
+  for (int k = 0; k < 3 * kGnnWidth; k++) th[size_t(o.W_out + k)] = 0.0f;
   learned_set_weights(S, th.data(), true);
 }
 
-// Ready for inference inside a solve: graph, features, BF16 edge weights.
+// Ready for inference inside a solve: the coarse space of the current matrix values,
+// preconditioner and weights (the network's omega with BF16 weights, or the fixed
+// omega of coarse_mode 1 / 2), its inverse, and the flexible-CG buffers.
 void learned_prepare_inference(Solver &S) {
   Learned &L = S.L;
-  if (!L.have_weights) throw Failure(HECMW33_ERR_INCONS_PC, "learned preconditioner requested but not trained");
+  auto &C = L.C;
+  if (L.coarse_mode == 0 && !L.have_weights)
+    throw Failure(HECMW33_ERR_INCONS_PC, "learned preconditioner requested but not trained");
   if (!(S.pc.valid && S.pc.kind == 1))
     throw Failure(HECMW33_ERR_INCONS_PC, "the learned preconditioner works after SSOR (PRECOND 1 or 2)");
   learned_graph(S);
-  if (L.w_version != L.weights_version) learned_edge_weights(S, true);
+  coarse_structure(S);
+  coarse_values(S);
+  const int wv = L.coarse_mode == 0 ? L.weights_version : -1;
+  if (C.op_precond != S.pc.numeric_version || C.op_weights != wv || C.op_mode != L.coarse_mode) {
+    const float *omega = nullptr;
+    if (L.coarse_mode == 0) {
+      coarse_omega(S, true, false);
+      omega = C.omega.p;
+    } else if (L.coarse_mode == 2) {
+      std::vector<float> half(size_t(S.n3()), 0.5f);
+      C.omega.upload(half, S.stream);
+      omega = C.omega.p;
+    }
+    coarse_operator(S, omega);
+    C.op_precond = S.pc.numeric_version;
+    C.op_weights = wv;
+    C.op_mode = L.coarse_mode;
+  }
   const size_t n3 = size_t(S.n3());
   S.zs.alloc(n3);
   S.rold.alloc(n3);
@@ -1535,45 +1742,73 @@ void learned_train_buffers(Solver &S) {
   L.part.alloc(size_t(L.nparts) * L.stride);
 }
 
-// Forward (FP32 weights, activations kept) + energy loss + backward for one pair
-// (r, e) with zs = SSOR(r) precomputed; adds coef * grad into gacc.  Returns the
-// loss value through the device (read by the caller after a sync).
-void learned_pair_grad(Solver &S, const float *r, const float *e, const float *zs, double er, float coef,
-                       double *loss_slot) {
+// One pass of the training loss over pairs (r_k, e_k, e_k.r_k) with the FP32 master
+// weights: the network's omega (activations kept for the backward pass), the coarse
+// operator, then per pair  y = Ac^-1 P^T r,  loss_k = (e.r - (P^T r).y) / e.r  (the
+// energy of e outside the coarse space, relative to its energy) and its gradient in
+// out (coarse_grad_kernel).  With backward, the network's backward pass turns the mean
+// gradient into L.gacc.  Returns the mean loss.
+double learned_coarse_pass(Solver &S, const std::vector<const float *> &pr, const std::vector<double> &per,
+                           bool backward) {
   Learned &L = S.L;
+  auto &C = L.C;
   cudaStream_t s = S.stream;
-  CgState *st = S.state.p;
-  const GnnGraph g = L.graph();
+  const int np = int(pr.size());
   const int n3 = S.n3();
-  const int gw = std::max(1, std::min((S.N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8));
-  const int gt = S.grid_vec();
-  launch_k(s, gnn_state_kernel, 1, 32, st);
-  launch_k(s, gamma_kernel<float>, gt, kThreads, zs, n3, st, S.partials.p);
-  launch_k(s, gnn_encode_kernel<float, float>, gt, kThreads, g, L.theta.p, zs, r, &st->gamma, L.x.p, L.h[0].p, st);
-  for (int l = 0; l < kGnnLayers; l++)
-    launch_k(s, gnn_layer_kernel<float>, gw, kThreads, g, L.theta.p, l, L.w.p, L.h[l].p, L.m[l].p, L.h[l + 1].p, st);
-  launch_k(s, gnn_decode_kernel<float, float>, gt, kThreads, S.N, L.theta.p, L.h[3].p, zs, &st->gamma, L.t_z.p, st);
-  // d = z - e, q = A d (FP32), loss = d.q / e.r, dz = 2 q / e.r
-  launch_k(s, sub_kernel, gt, kThreads, L.t_z.p, e, L.t_d.p, n3);
-  launch_k(s, spmv_kernel<float, 0>, S.grid_spmv(), kThreads, S.A.view32(), L.t_d.p, L.t_q.p, nullptr, nullptr, nullptr);
-  launch_k(s, dot_kernel<float, 2>, gt, kThreads, L.t_d.p, L.t_q.p, n3, st, S.partials.p, 0, 0);
-  H33_CUDA(cudaMemcpyAsync(loss_slot, &st->rr_true, sizeof(double), cudaMemcpyDeviceToDevice, s));
-  launch_k(s, scale_kernel, gt, kThreads, L.t_q.p, float(2.0 / er), L.t_dz.p, n3);
-  // backward
-  const int np = L.nparts, stride = L.stride;
-  launch_k(s, gnn_decode_bwd_kernel, np, kThreads, S.N, L.theta.p, L.h[3].p, L.t_dz.p, &st->gamma, L.dh.p, L.part.p,
-                                                stride);
-  for (int l = kGnnLayers - 1; l >= 0; l--) {
-    launch_k(s, gnn_layer_bwd_kernel, np, kThreads, g, L.theta.p, l, L.w.p, L.h[l].p, L.h[l + 1].p, L.m[l].p, L.dh.p,
-                                                 L.gm.p, L.dhp.p, L.part.p, stride);
-    launch_k(s, gnn_layer_bwd_gather_kernel, gw, kThreads, g, l, L.w.p, L.gm.p, L.dhp.p);
-    std::swap(L.dh, L.dhp);
+  coarse_omega(S, false, backward);
+  if (!coarse_operator(S, C.omega.p))
+    throw Failure(HECMW33_ERR_INCONS_PC, "learned preconditioner: the coarse matrix is not positive definite");
+  const CoarseView cv = C.view();
+  const int gt = std::max(1, std::min((S.N + kThreads - 1) / kThreads, S.nsm * 8));
+  const int gr = std::max(1, std::min((C.nagg + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8));
+  const int gg = std::max(1, std::min((C.nc + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8));
+  C.dout.zero(s);
+  L.losses.alloc(size_t(std::max(np, 1)));
+  for (int k = 0; k < np; k++) {
+    launch_k(s, coarse_restrict_kernel<float>, gr, kThreads, cv, pr[size_t(k)], C.bc.p,
+             static_cast<const CgState *>(nullptr));
+    launch_k(s, coarse_gemv_kernel, gg, kThreads, C.nc, static_cast<const double *>(C.ac.p),
+             static_cast<const double *>(C.bc.p), C.y.p, static_cast<const CgState *>(nullptr));
+    launch_k(s, coarse_prolong_kernel<float>, gt, kThreads, cv, static_cast<const double *>(C.y.p),
+             static_cast<const float *>(nullptr), static_cast<float *>(nullptr), C.v.p, C.t0y.p,
+             static_cast<const CgState *>(nullptr));
+    launch_k(s, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, S.A.view(), static_cast<const double *>(C.v.p),
+             C.apy.p, static_cast<const double *>(nullptr), static_cast<CgState *>(nullptr),
+             static_cast<double *>(nullptr));
+    launch_k(s, coarse_grad_kernel<float>, S.grid_vec(), kThreads, n3, pr[size_t(k)],
+             static_cast<const double *>(C.apy.p), static_cast<const double *>(C.t0y.p),
+             static_cast<const float *>(C.omega.p), 1.0 / (per[size_t(k)] * np), C.dout.p);
+    coarse_dot_kernel<<<1, 256, 0, s>>>(C.nc, C.bc.p, C.y.p, L.losses.p + k);
   }
-  launch_k(s, gnn_encode_bwd_kernel, np, kThreads, S.N, L.x.p, L.dh.p, L.part.p, stride);
-  launch_k(s, gnn_reduce_grads_kernel, (stride + 255) / 256, 256, L.part.p, np, stride, L.grad.p, stride);
-  launch_k(s, accum_kernel, (stride + 255) / 256, 256, L.grad.p, coef, L.gacc.p, stride);
   H33_CUDA(cudaGetLastError());
-  (void)er;
+  if (backward) {
+    const GnnGraph g = L.graph();
+    const int gw = std::max(1, std::min((S.N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8));
+    const int npart = L.nparts, stride = L.stride;
+    launch_k(s, gnn_decode_bwd_kernel, npart, kThreads, S.N, static_cast<const float *>(L.theta.p),
+             static_cast<const float *>(L.h[3].p), static_cast<const float *>(C.dout.p),
+             static_cast<const float *>(C.one), L.dh.p, L.part.p, stride);
+    for (int l = kGnnLayers - 1; l >= 0; l--) {
+      launch_k(s, gnn_layer_bwd_kernel, npart, kThreads, g, static_cast<const float *>(L.theta.p), l,
+               static_cast<const float *>(L.w.p), static_cast<const float *>(L.h[l].p),
+               static_cast<const float *>(L.h[l + 1].p), static_cast<const float *>(L.m[l].p),
+               static_cast<const float *>(L.dh.p), L.gm.p, L.dhp.p, L.part.p, stride);
+      launch_k(s, gnn_layer_bwd_gather_kernel, gw, kThreads, g, l, static_cast<const float *>(L.w.p),
+               static_cast<const float *>(L.gm.p), L.dhp.p);
+      std::swap(L.dh, L.dhp);
+    }
+    launch_k(s, gnn_encode_bwd_kernel, npart, kThreads, S.N, static_cast<const float *>(C.x.p),
+             static_cast<const float *>(L.dh.p), L.part.p, stride);
+    launch_k(s, gnn_reduce_grads_kernel, (stride + 255) / 256, 256, static_cast<const float *>(L.part.p), npart,
+             stride, L.gacc.p, stride);
+    H33_CUDA(cudaGetLastError());
+  }
+  std::vector<double> by(size_t(std::max(np, 1)));
+  H33_CUDA(cudaMemcpyAsync(by.data(), L.losses.p, sizeof(double) * size_t(np), cudaMemcpyDeviceToHost, s));
+  S.sync();
+  double m = 0.0;
+  for (int k = 0; k < np; k++) m += (per[size_t(k)] - by[size_t(k)]) / per[size_t(k)];
+  return np ? m / np : 0.0;
 }
 
 // FP64 CG in stream mode, one iteration per host step, keeping x at iterations
@@ -1649,50 +1884,32 @@ float record_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels) 
   return ms;
 }
 
-// Trains the network on the recorded pairs: Adam on the mean energy-norm loss.
-// loss[0] = mean loss before the first step, loss[1] = after the last.
+// Trains the network on the recorded pairs: Adam on the mean loss of
+// learned_coarse_pass.  loss[0] = mean loss before the first step, loss[1] = after
+// the last.
 void learned_train(Solver &S, int steps, double lr, double *loss) {
   Learned &L = S.L;
   const int np = int(L.pr.size());
   if (np == 0) throw Failure(HECMW33_ERR_BAD_INPUT, "no recorded pairs: enable recording and solve first");
   if (!(S.pc.valid && S.pc.kind == 1))
     throw Failure(HECMW33_ERR_INCONS_PC, "training needs the SSOR preconditioner of the matrix");
-  ensure_fp32(S);
   learned_graph(S);
   learned_train_buffers(S);
+  coarse_structure(S);
+  coarse_values(S);
   if (!L.have_weights) learned_init_weights(S, 12345);
-  const Views<float> V = views(S, 0.0f);
-  const size_t n3 = size_t(S.n3());
-  for (int k = 0; k < np; k++)
-    if (L.pzs[size_t(k)].n != n3) {
-      L.pzs[size_t(k)].alloc(n3);
-      launch_sweep<float, false>(S, V, L.pr[size_t(k)].p, L.pzs[size_t(k)].p, nullptr);
-    }
-  L.losses.alloc(size_t(np));
-  std::vector<double> lh(static_cast<size_t>(np));
+  std::vector<const float *> pr;
+  for (int k = 0; k < np; k++) pr.push_back(L.pr[size_t(k)].p);
   const int nparam = GnnOffsets::make().total;
-  auto eval_pass = [&](bool update) {
-    learned_edge_weights(S, false);
-    L.gacc.zero(S.stream);
-    for (int k = 0; k < np; k++)
-      learned_pair_grad(S, L.pr[size_t(k)].p, L.pe[size_t(k)].p, L.pzs[size_t(k)].p, L.per[size_t(k)],
-                        1.0f / float(np), L.losses.p + k);
-    if (update) {
-      L.adam_step++;
-      launch_k(S.stream, gnn_adam_kernel, (nparam + 255) / 256, 256, L.theta.p, L.gacc.p, L.m1.p, L.m2.p, nparam,
-                                                                  float(lr), 0.9f, 0.999f, 1e-8f, L.adam_step, 1.0f,
-                                                                  L.theta_bf16.p);
-      H33_CUDA(cudaGetLastError());
-    }
-    H33_CUDA(cudaMemcpyAsync(lh.data(), L.losses.p, sizeof(double) * size_t(np), cudaMemcpyDeviceToHost, S.stream));
-    S.sync();
-    double m = 0.0;
-    for (int k = 0; k < np; k++) m += lh[size_t(k)] / L.per[size_t(k)];
-    return m / np;
-  };
-  loss[0] = eval_pass(false);
-  for (int it = 0; it < steps; it++) eval_pass(true);
-  loss[1] = eval_pass(false);
+  loss[0] = learned_coarse_pass(S, pr, L.per, false);
+  for (int it = 0; it < steps; it++) {
+    learned_coarse_pass(S, pr, L.per, true);
+    L.adam_step++;
+    launch_k(S.stream, gnn_adam_kernel, (nparam + 255) / 256, 256, L.theta.p, static_cast<const float *>(L.gacc.p),
+             L.m1.p, L.m2.p, nparam, float(lr), 0.9f, 0.999f, 1e-8f, L.adam_step, 1.0f, L.theta_bf16.p);
+    H33_CUDA(cudaGetLastError());
+  }
+  loss[1] = learned_coarse_pass(S, pr, L.per, false);
   L.weights_version++;
 }
 
@@ -2603,7 +2820,8 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   const int MAXIT = Iarray[0], PRECOND = Iarray[2], iterPREmax = Iarray[4], METHOD2 = Iarray[7];
   const double TOL = Rarray[0];
   int method = Iarray[1];
-  int learned = (Iarray[42] == 1 && method == 1) ? 1 : 0;  // the learned network runs in flexible CG
+  int learned = (Iarray[42] == 1 && method == 1) ? 1 : 0;  // the learned two-level preconditioner
+  S.L.coarse_mode = (Iarray[43] >= 0 && Iarray[43] <= 2) ? Iarray[43] : 0;
   if (learned) learned_prepare_inference(S);
   const int ESTCOND = Iarray[13];  // hecmw_mat_get_estcond
   S.lanczos_on = ESTCOND > 0 && method == 1 && !learned;
@@ -2813,6 +3031,7 @@ int solve_mixed_reliable(Solver &S, int *Iarray, double *Rarray, int *iter, doub
   const double TOL = Rarray[0];
   const double DELTA = Rarray[41] > 0.0 ? Rarray[41] : 0.1;
   const int learned = Iarray[42] == 1 ? 1 : 0;
+  S.L.coarse_mode = (Iarray[43] >= 0 && Iarray[43] <= 2) ? Iarray[43] : 0;
   ensure_fp32(S);
   if (learned) learned_prepare_inference(S);
   if (graph_mode()) build_graph<float>(S, iterPREmax, 2 | learned);
@@ -4094,35 +4313,29 @@ HECMW33_API void hecmw33_gpu_learn_eval(const int *handle, const float *theta, c
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix");
   if (!(S.pc.valid && S.pc.kind == 1)) throw Failure(HECMW33_ERR_INCONS_PC, "build the SSOR preconditioner first");
   const int total = GnnOffsets::make().total;
-  ensure_fp32(S);
   learned_graph(S);
   learned_train_buffers(S);
+  coarse_structure(S);
+  coarse_values(S);
   learned_set_weights(S, theta, false);
   const size_t n3 = size_t(S.n3());
-  std::vector<float> rf(n3), ef(n3), zf(n3);
+  std::vector<float> rf(n3), ef(n3), wf(n3);
   for (size_t i = 0; i < n3; i++) {
     rf[i] = float(R[i]);
     ef[i] = float(E[i]);
   }
-  DevArray<float> dr, de, dzs;
+  DevArray<float> dr, de;
   dr.upload(rf, S.stream);
   de.upload(ef, S.stream);
-  dzs.alloc(n3);
-  const Views<float> V = views(S, 0.0f);
-  launch_sweep<float, false>(S, V, dr.p, dzs.p, nullptr);
   const double er = dot_device_f(S, de.p, dr.p);
-  learned_edge_weights(S, false);
-  S.L.gacc.zero(S.stream);
-  S.L.losses.alloc(1);
-  learned_pair_grad(S, dr.p, de.p, dzs.p, er, 1.0f, S.L.losses.p);
-  double dq = 0.0;
-  H33_CUDA(cudaMemcpyAsync(&dq, S.L.losses.p, sizeof(double), cudaMemcpyDeviceToHost, S.stream));
-  H33_CUDA(cudaMemcpyAsync(zf.data(), S.L.t_z.p, sizeof(float) * n3, cudaMemcpyDeviceToHost, S.stream));
+  if (!(er > 0.0)) throw Failure(HECMW33_ERR_BAD_INPUT, "learn_eval: e.r must be positive (r = A e)");
+  const double l = learned_coarse_pass(S, {dr.p}, {er}, true);
+  H33_CUDA(cudaMemcpyAsync(wf.data(), S.L.C.omega.p, sizeof(float) * n3, cudaMemcpyDeviceToHost, S.stream));
   if (grad)
     H33_CUDA(cudaMemcpyAsync(grad, S.L.gacc.p, sizeof(float) * size_t(total), cudaMemcpyDeviceToHost, S.stream));
   S.sync();
-  for (size_t i = 0; i < n3; i++) Z[i] = zf[i];
-  if (loss) *loss = dq / er;
+  for (size_t i = 0; i < n3; i++) Z[i] = wf[i];
+  if (loss) *loss = l;
   S.L.weights_version++;
   H33_ENTRY_END
 }
