@@ -1,0 +1,456 @@
+// h33_coarse.cuh -- the coarse space of the learned two-level preconditioner.
+//
+// No counterpart in the reference solver.  After SSOR, the flexible CG adds a coarse
+// correction:  z = SSOR(r) + P Ac^-1 P^T r,  Ac = P^T A P,  on aggregates of the node
+// graph (h33_setup.cpp aggregate_nodes).  The prolongator is a smoothed aggregation
+//   P = (I - Omega D^-1 A) P0,
+// P0 the piecewise-constant translations of each aggregate (zero on DOFs whose row of
+// A has no off-diagonal entry: the constrained ones), D the diagonal blocks, and
+// Omega = diag(omega) per DOF from the network (h33_gnn.cuh): omega = sigmoid(out).
+// Row i of P has one 3x3 block per aggregate of i's closed neighbourhood:
+//   P(i,b) = [b == agg(i)] M_i - diag(omega_i) T0(i,b),
+//   T0(i,b) = D_i^-1 sum_{j in N[i], agg(j) = b} A_ij M_j      (M = DOF mask)
+// The coarse matrix is dense (3 x aggregates square, a few thousand) and inverted
+// once per matrix; an application is then one gather (P^T r), one dense GEMV and one
+// scatter (P y).  Every sum runs in a fixed order (warp shuffles in lane order, no
+// atomics), so a coarse operator and its application are deterministic.
+#pragma once
+
+#include "h33_common.cuh"
+
+namespace h33 {
+
+struct CoarseView {
+  int n, nagg, nc;                 // fine nodes, aggregates, coarse DOFs (3 nagg)
+  const int *agg;                  // n
+  const int *pptr, *pagg;          // P pattern (n + 1, nnzp)
+  const int *rptr, *rnode, *rpos;  // restriction gather (nagg + 1, nnzp, nnzp)
+  const int *qptr, *qagg;          // A P pattern (n + 1, nnzq)
+  const int *cptr, *cagg;          // Ac pattern (nagg + 1, nnzc)
+  const int *uptr, *ucol, *usrc;   // unified rows of A (L, D, U; raw block ids)
+  float *mask;                     // 3n: 1 where the DOF's row couples, else 0
+  double *t0, *p;                  // 9 nnzp each
+  double *q;                       // 9 nnzq: A P
+  double *ac;                      // nc x nc, row-major: Ac, then Ac^-1
+};
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// mask[3i+d] = 1 when row 3i+d of A has a nonzero off-diagonal entry (thread per node).
+__global__ void coarse_mask_kernel(CoarseView c, const double *__restrict__ raw) {
+  pdl_entry();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
+    bool cpl[3] = {false, false, false};
+    for (int k = c.uptr[i]; k < c.uptr[i + 1]; k++) {
+      const double *a = raw + 9 * size_t(c.usrc[k]);
+      const bool diag = c.ucol[k] == i;
+      for (int d = 0; d < 3; d++)
+        for (int e = 0; e < 3; e++)
+          if (!(diag && d == e) && a[3 * d + e] != 0.0) cpl[d] = true;
+    }
+    for (int d = 0; d < 3; d++) c.mask[3 * i + d] = cpl[d] ? 1.0f : 0.0f;
+  }
+}
+
+// The network's static input per node: [1, (aggregates of the closed neighbourhood
+// - 1) / 7, share of the neighbours outside the node's aggregate, DOF mask (3)].
+__global__ void coarse_features_kernel(CoarseView c, float *__restrict__ x) {
+  pdl_entry();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
+    int nb = 0, out = 0;
+    for (int k = c.uptr[i]; k < c.uptr[i + 1]; k++) {
+      const int j = c.ucol[k];
+      if (j == i) continue;
+      nb++;
+      out += c.agg[j] != c.agg[i];
+    }
+    float *xi = x + 6 * size_t(i);
+    xi[0] = 1.0f;
+    xi[1] = float(c.pptr[i + 1] - c.pptr[i] - 1) / 7.0f;
+    xi[2] = nb ? float(out) / float(nb) : 0.0f;
+    for (int d = 0; d < 3; d++) xi[3 + d] = c.mask[3 * i + d];
+  }
+}
+
+// sum of a[k] b[k], k < n (one CTA; lane-order partial sums, fixed tree)
+__global__ void coarse_dot_kernel(int n, const double *__restrict__ a, const double *__restrict__ b,
+                                  double *__restrict__ out) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) s += a[k] * b[k];
+  s = warp_sum_d(s);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    s = warp_sum_d(s);
+    if (threadIdx.x == 0) *out = s;
+  }
+}
+
+// T0(i,b) = D_i^-1 sum_{j in N[i], agg(j) = b} A_ij M_j   (thread per node; the node's
+// entries are its own, so no two threads write one entry).  A singular D_i (no such
+// block in an assembled stiffness) leaves the node's T0 at zero.
+__global__ void coarse_t0_kernel(CoarseView c, const double *__restrict__ raw) {
+  pdl_entry();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
+    const int q0 = c.pptr[i], q1 = c.pptr[i + 1];
+    for (int q = q0; q < q1; q++)
+      for (int e = 0; e < 9; e++) c.t0[9 * size_t(q) + e] = 0.0;
+    for (int k = c.uptr[i]; k < c.uptr[i + 1]; k++) {
+      const int j = c.ucol[k];
+      const int b = c.agg[j];
+      int q = q0;
+      while (q < q1 && c.pagg[q] != b) q++;
+      if (q == q1) continue;  // not in the pattern (cannot happen for a closed neighbourhood)
+      const double *a = raw + 9 * size_t(c.usrc[k]);
+      double *t = c.t0 + 9 * size_t(q);
+      for (int d = 0; d < 3; d++)
+        for (int e = 0; e < 3; e++) t[3 * d + e] += a[3 * d + e] * double(c.mask[3 * j + e]);
+    }
+    const double *D = raw + 9 * size_t(i);
+    const double c00 = D[4] * D[8] - D[5] * D[7], c01 = D[5] * D[6] - D[3] * D[8], c02 = D[3] * D[7] - D[4] * D[6];
+    const double det = D[0] * c00 + D[1] * c01 + D[2] * c02;
+    double inv[9];
+    if (det != 0.0) {
+      const double id = 1.0 / det;
+      inv[0] = c00 * id;
+      inv[1] = (D[2] * D[7] - D[1] * D[8]) * id;
+      inv[2] = (D[1] * D[5] - D[2] * D[4]) * id;
+      inv[3] = c01 * id;
+      inv[4] = (D[0] * D[8] - D[2] * D[6]) * id;
+      inv[5] = (D[2] * D[3] - D[0] * D[5]) * id;
+      inv[6] = c02 * id;
+      inv[7] = (D[1] * D[6] - D[0] * D[7]) * id;
+      inv[8] = (D[0] * D[4] - D[1] * D[3]) * id;
+    } else {
+      for (int e = 0; e < 9; e++) inv[e] = 0.0;
+    }
+    for (int q = q0; q < q1; q++) {
+      double *t = c.t0 + 9 * size_t(q);
+      double o[9];
+      for (int d = 0; d < 3; d++)
+        for (int e = 0; e < 3; e++) o[3 * d + e] = inv[3 * d] * t[e] + inv[3 * d + 1] * t[3 + e] + inv[3 * d + 2] * t[6 + e];
+      for (int e = 0; e < 9; e++) t[e] = o[e];
+    }
+  }
+}
+
+// P(i,b) = [b == agg(i)] M_i - diag(omega_i) T0(i,b)   (thread per node)
+__global__ void coarse_p_kernel(CoarseView c, const float *__restrict__ omega) {
+  pdl_entry();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
+    const int ai = c.agg[i];
+    const double w0 = omega ? double(omega[3 * i]) : 0.0, w1 = omega ? double(omega[3 * i + 1]) : 0.0,
+                 w2 = omega ? double(omega[3 * i + 2]) : 0.0;
+    const double w[3] = {w0, w1, w2};
+    for (int q = c.pptr[i]; q < c.pptr[i + 1]; q++) {
+      const double *t = c.t0 + 9 * size_t(q);
+      double *p = c.p + 9 * size_t(q);
+      for (int d = 0; d < 3; d++)
+        for (int e = 0; e < 3; e++)
+          p[3 * d + e] = (c.pagg[q] == ai && d == e ? double(c.mask[3 * i + d]) : 0.0) - w[d] * t[3 * d + e];
+    }
+  }
+}
+
+// Q(i,b) = sum_{j in N[i]} A_ij P(j,b) for b in row i's two-ring pattern (warp per
+// node; lane k takes block k of the row, then a lane-order warp sum per entry).
+__global__ void __launch_bounds__(kThreads) coarse_ap_kernel(CoarseView c, const double *__restrict__ raw) {
+  pdl_entry();
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < c.n; i += nwarps) {
+    const int k0 = c.uptr[i], k1 = c.uptr[i + 1];
+    for (int qq = c.qptr[i]; qq < c.qptr[i + 1]; qq++) {
+      const int b = c.qagg[qq];
+      double acc[9];
+      for (int e = 0; e < 9; e++) acc[e] = 0.0;
+      for (int k = k0 + lane; k < k1; k += 32) {
+        const int j = c.ucol[k];
+        int q = c.pptr[j];
+        const int qe = c.pptr[j + 1];
+        while (q < qe && c.pagg[q] != b) q++;
+        if (q == qe) continue;
+        const double *a = raw + 9 * size_t(c.usrc[k]);
+        const double *p = c.p + 9 * size_t(q);
+        for (int d = 0; d < 3; d++)
+          for (int e = 0; e < 3; e++) acc[3 * d + e] += a[3 * d] * p[e] + a[3 * d + 1] * p[3 + e] + a[3 * d + 2] * p[6 + e];
+      }
+      for (int e = 0; e < 9; e++) {
+        const double v = warp_sum_d(acc[e]);
+        if (lane == 0) c.q[9 * size_t(qq) + e] = v;
+      }
+    }
+  }
+}
+
+// Ac(a,b) = sum_{i in restriction of a} P(i,a)^T Q(i,b)   (warp per aggregate a and
+// coarse block b of its pattern; lanes over the restriction's nodes in ascending
+// order, then a lane-order warp sum).  Ac is dense, zero outside the pattern.
+__global__ void __launch_bounds__(kThreads) coarse_ac_kernel(CoarseView c) {
+  pdl_entry();
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int nblk = c.cptr[c.nagg];
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nblk; w += nwarps) {
+    int a = 0;
+    {  // row of pattern entry w (binary search in cptr)
+      int lo = 0, hi = c.nagg;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (c.cptr[mid] <= w) lo = mid;
+        else hi = mid;
+      }
+      a = lo;
+    }
+    const int b = c.cagg[w];
+    double acc[9];
+    for (int e = 0; e < 9; e++) acc[e] = 0.0;
+    for (int t = c.rptr[a] + lane; t < c.rptr[a + 1]; t += 32) {
+      const int i = c.rnode[t];
+      int qq = c.qptr[i];
+      const int qe = c.qptr[i + 1];
+      while (qq < qe && c.qagg[qq] != b) qq++;
+      if (qq == qe) continue;
+      const double *p = c.p + 9 * size_t(c.rpos[t]);
+      const double *qv = c.q + 9 * size_t(qq);
+      for (int d = 0; d < 3; d++)
+        for (int e = 0; e < 3; e++) acc[3 * d + e] += p[d] * qv[e] + p[3 + d] * qv[3 + e] + p[6 + d] * qv[6 + e];
+    }
+    for (int d = 0; d < 3; d++)
+      for (int e = 0; e < 3; e++) {
+        const double v = warp_sum_d(acc[3 * d + e]);
+        if (lane == 0) c.ac[size_t(3 * a + d) * c.nc + 3 * b + e] = v;
+      }
+  }
+}
+
+// ---- in-place inversion of the SPD coarse matrix: blocked Gauss-Jordan ----------
+// For each block K of kGjBlock pivots (no pivoting: Ac is SPD):
+//   Dinv = M_KK^-1;  C = M_:K (saved);  M_Kj = Dinv M_Kj (j not in K);
+//   M_ij -= C_iK M_Kj (i, j not in K);  M_iK = -C_iK Dinv (i not in K);  M_KK = Dinv.
+// After the last block M holds Ac^-1.
+constexpr int kGjBlock = 32;
+
+// Dinv = M_KK^-1 by unblocked Gauss-Jordan in shared memory (one CTA).  A pivot that
+// is not positive sets *err (the coarse operator is then not used).
+__global__ void gj_diag_kernel(double *__restrict__ M, int n, int k0, int nb, double *__restrict__ dinv,
+                               int *err) {
+  __shared__ double s[kGjBlock][kGjBlock + 1];
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) s[t / nb][t % nb] = M[size_t(k0 + t / nb) * n + k0 + t % nb];
+  __syncthreads();
+  for (int k = 0; k < nb; k++) {
+    const double piv = s[k][k];
+    __syncthreads();
+    if (!(piv > 0.0)) {
+      if (threadIdx.x == 0) atomicOr(err, 1);
+      return;  // uniform: every thread read the same pivot
+    }
+    const double d = 1.0 / piv;
+    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+      const int i = t / nb, j = t % nb;
+      if (i != k && j != k) s[i][j] -= s[i][k] * s[k][j] * d;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+      if (t != k) {
+        s[k][t] *= d;
+        s[t][k] *= -d;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s[k][k] = d;
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) dinv[t] = s[t / nb][t % nb];
+}
+
+// C(i, t) = M(i, k0 + t) for all rows i (n x nb, row-major with stride kGjBlock).
+__global__ void gj_save_col_kernel(const double *__restrict__ M, int n, int k0, int nb, double *__restrict__ C) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n * nb; x += gridDim.x * blockDim.x) {
+    const int i = x / nb, t = x % nb;
+    C[size_t(i) * kGjBlock + t] = M[size_t(i) * n + k0 + t];
+  }
+}
+
+// M(K, j) = Dinv M(K, j) for columns j outside K (thread per column).
+__global__ void gj_row_kernel(double *__restrict__ M, int n, int k0, int nb, const double *__restrict__ dinv) {
+  __shared__ double D[kGjBlock * kGjBlock];
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) D[t] = dinv[t];
+  __syncthreads();
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    if (j >= k0 && j < k0 + nb) continue;
+    double v[kGjBlock];
+    for (int t = 0; t < nb; t++) v[t] = M[size_t(k0 + t) * n + j];
+    for (int s = 0; s < nb; s++) {
+      double a = 0.0;
+      for (int t = 0; t < nb; t++) a += D[s * nb + t] * v[t];
+      M[size_t(k0 + s) * n + j] = a;
+    }
+  }
+}
+
+// M(i, j) -= C(i, :) M(K, j) for i, j outside K: 64 x 64 tiles, the tile's panels in
+// shared memory, 4 x 4 outputs per thread (256 threads).
+__global__ void __launch_bounds__(256) gj_update_kernel(double *__restrict__ M, int n, int k0, int nb,
+                                                        const double *__restrict__ C) {
+  __shared__ double Cs[64][kGjBlock + 1];
+  __shared__ double Rs[kGjBlock][64 + 1];
+  const int i0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+  for (int t = threadIdx.x; t < 64 * kGjBlock; t += blockDim.x) {
+    const int r = t / kGjBlock, k = t % kGjBlock;
+    const int i = i0 + r;
+    Cs[r][k] = (i < n && k < nb) ? C[size_t(i) * kGjBlock + k] : 0.0;
+  }
+  for (int t = threadIdx.x; t < kGjBlock * 64; t += blockDim.x) {
+    const int k = t / 64, cc = t % 64;
+    const int j = j0 + cc;
+    Rs[k][cc] = (j < n && k < nb) ? M[size_t(k0 + k) * n + j] : 0.0;
+  }
+  __syncthreads();
+  const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
+  double acc[4][4] = {};
+  for (int k = 0; k < nb; k++) {
+    double a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      a[u] = Cs[tr + 16 * u][k];
+      b[u] = Rs[k][tc + 16 * u];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int v = 0; v < 4; v++) acc[u][v] += a[u] * b[v];
+  }
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int i = i0 + tr + 16 * u;
+    if (i >= n || (i >= k0 && i < k0 + nb)) continue;
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const int j = j0 + tc + 16 * v;
+      if (j >= n || (j >= k0 && j < k0 + nb)) continue;
+      M[size_t(i) * n + j] -= acc[u][v];
+    }
+  }
+}
+
+// M(i, K) = -C(i, :) Dinv for rows i outside K, M(K, K) = Dinv (thread per row).
+__global__ void gj_col_kernel(double *__restrict__ M, int n, int k0, int nb, const double *__restrict__ C,
+                              const double *__restrict__ dinv) {
+  __shared__ double D[kGjBlock * kGjBlock];
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) D[t] = dinv[t];
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (i >= k0 && i < k0 + nb) {
+      for (int s = 0; s < nb; s++) M[size_t(i) * n + k0 + s] = D[(i - k0) * nb + s];
+      continue;
+    }
+    for (int s = 0; s < nb; s++) {
+      double a = 0.0;
+      for (int t = 0; t < nb; t++) a += C[size_t(i) * kGjBlock + t] * D[t * nb + s];
+      M[size_t(i) * n + k0 + s] = -a;
+    }
+  }
+}
+
+// ---- application ------------------------------------------------------------
+// bc = P^T r   (warp per aggregate; lanes over its restriction entries in order)
+template <class R>
+__global__ void __launch_bounds__(kThreads) coarse_restrict_kernel(CoarseView c, const R *__restrict__ r,
+                                                                   double *__restrict__ bc, const CgState *st) {
+  pdl_entry();
+  if (st && (st->done || !st->use_gnn)) return;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < c.nagg; a += nwarps) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int t = c.rptr[a] + lane; t < c.rptr[a + 1]; t += 32) {
+      const int i = c.rnode[t];
+      const double *p = c.p + 9 * size_t(c.rpos[t]);
+      const double r0 = double(r[3 * i]), r1 = double(r[3 * i + 1]), r2 = double(r[3 * i + 2]);
+      s0 += p[0] * r0 + p[3] * r1 + p[6] * r2;
+      s1 += p[1] * r0 + p[4] * r1 + p[7] * r2;
+      s2 += p[2] * r0 + p[5] * r1 + p[8] * r2;
+    }
+    s0 = warp_sum_d(s0);
+    s1 = warp_sum_d(s1);
+    s2 = warp_sum_d(s2);
+    if (lane == 0) {
+      bc[3 * a] = s0;
+      bc[3 * a + 1] = s1;
+      bc[3 * a + 2] = s2;
+    }
+  }
+}
+
+// y = Ainv bc   (warp per coarse row, FP64)
+__global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(int nc, const double *__restrict__ ainv,
+                                                               const double *__restrict__ bc, double *__restrict__ y,
+                                                               const CgState *st) {
+  pdl_entry();
+  if (st && (st->done || !st->use_gnn)) return;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nc; row += nwarps) {
+    const double *a = ainv + size_t(row) * nc;
+    double s = 0.0;
+    for (int k = lane; k < nc; k += 32) s += __ldcs(a + k) * bc[k];
+    s = warp_sum_d(s);
+    if (lane == 0) y[row] = s;
+  }
+}
+
+// z = zs + P y (thread per node); z = zs once the correction is off.  With t0y given,
+// also t0y = T0 y and v = P y (training).
+template <class R>
+__global__ void coarse_prolong_kernel(CoarseView c, const double *__restrict__ y, const R *__restrict__ zs,
+                                      R *__restrict__ z, double *__restrict__ v, double *__restrict__ t0y,
+                                      const CgState *st) {
+  pdl_entry();
+  if (st && st->done) return;
+  const bool on = !st || st->use_gnn;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
+    double a[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
+    if (on)
+      for (int q = c.pptr[i]; q < c.pptr[i + 1]; q++) {
+        const double *p = c.p + 9 * size_t(q);
+        const int b = c.pagg[q];
+        const double y0 = y[3 * b], y1 = y[3 * b + 1], y2 = y[3 * b + 2];
+        for (int d = 0; d < 3; d++) a[d] += p[3 * d] * y0 + p[3 * d + 1] * y1 + p[3 * d + 2] * y2;
+        if (t0y) {
+          const double *tq = c.t0 + 9 * size_t(q);
+          for (int d = 0; d < 3; d++) t[d] += tq[3 * d] * y0 + tq[3 * d + 1] * y1 + tq[3 * d + 2] * y2;
+        }
+      }
+    for (int d = 0; d < 3; d++) {
+      if (z) z[3 * i + d] = R(double(zs[3 * i + d]) + a[d]);
+      if (v) v[3 * i + d] = a[d];
+      if (t0y) t0y[3 * i + d] = t[d];
+    }
+  }
+}
+
+// ---- training -----------------------------------------------------------------
+// Loss of one recorded pair (r = A e): the energy of e outside the coarse space,
+//   L = (e^T r - bc^T y) / (e^T r),   y = Ac^-1 P^T r,
+// whose gradient in P is -2 (r - A P y) y^T / (e^T r), so in omega (dP/domega = -T0):
+//   dL/domega_(i,d) = 2 g_(i,d) (T0 y)_(i,d) / (e^T r),   g = r - A P y.
+// Accumulated into dout through omega = sigmoid(out): domega * omega (1 - omega).
+template <class RT>
+__global__ void coarse_grad_kernel(int n3, const RT *__restrict__ r, const double *__restrict__ apy,
+                                   const double *__restrict__ t0y, const float *__restrict__ omega, double coef,
+                                   float *__restrict__ dout) {
+  pdl_entry();
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += gridDim.x * blockDim.x) {
+    const double g = double(r[k]) - apy[k];
+    const double w = double(omega[k]);
+    dout[k] += float(2.0 * coef * g * t0y[k] * w * (1.0 - w));
+  }
+}
+
+}  // namespace h33

@@ -191,6 +191,55 @@ __global__ void gnn_decode_kernel(int n, const W *__restrict__ theta, const floa
   }
 }
 
+// ---- the network as the coarse-space generator (learned two-level) ----------
+// Input: six static features per node (h33_coarse.cuh coarse_features_kernel);
+// output: omega = sigmoid(W_out h3) per DOF, the smoothing weights of the prolongator.
+
+// h0_i = W_in x_i   (thread per node; x precomputed, n x 6)
+template <class W>
+__global__ void gnn_encode_static_kernel(int n, const W *__restrict__ theta, const float *__restrict__ x,
+                                         float *__restrict__ h0) {
+  pdl_entry();
+  const GnnOffsets o = GnnOffsets::make();
+  __shared__ float Win[kGnnWidth * 6];
+  for (int k = threadIdx.x; k < kGnnWidth * 6; k += blockDim.x) Win[k] = wload(theta + o.W_in + k);
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float xi[6];
+    for (int d = 0; d < 6; d++) xi[d] = x[6 * size_t(i) + d];
+    for (int c = 0; c < kGnnWidth; c++) {
+      float a = 0.0f;
+#pragma unroll
+      for (int d = 0; d < 6; d++) a += Win[6 * c + d] * xi[d];
+      h0[size_t(i) * kGnnWidth + c] = a;
+    }
+  }
+}
+
+// out_i = W_out h3_i, omega_i = 1 / (1 + exp(-out_i))   (thread per node, 3 each)
+template <class W>
+__global__ void gnn_omega_kernel(int n, const W *__restrict__ theta, const float *__restrict__ h3,
+                                 float *__restrict__ out, float *__restrict__ omega) {
+  pdl_entry();
+  const GnnOffsets o = GnnOffsets::make();
+  __shared__ float Wo[3 * kGnnWidth];
+  for (int k = threadIdx.x; k < 3 * kGnnWidth; k += blockDim.x) Wo[k] = wload(theta + o.W_out + k);
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float a[3] = {0.0f, 0.0f, 0.0f};
+    for (int c = 0; c < kGnnWidth; c++) {
+      const float h = h3[size_t(i) * kGnnWidth + c];
+      a[0] += Wo[c] * h;
+      a[1] += Wo[kGnnWidth + c] * h;
+      a[2] += Wo[2 * kGnnWidth + c] * h;
+    }
+    for (int d = 0; d < 3; d++) {
+      if (out) out[3 * i + d] = a[d];
+      omega[3 * i + d] = 1.0f / (1.0f + expf(-a[d]));
+    }
+  }
+}
+
 // ---- backward (training, FP32) ----------------------------------------------
 // Per-CTA partial gradients are written to partials[blockIdx.x * stride + k] and
 // summed by gnn_reduce_grads_kernel in a fixed order.

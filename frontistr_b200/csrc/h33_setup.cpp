@@ -744,4 +744,142 @@ void level_schedule(const Profile &p, bool lower, std::vector<int> &order,
   }
 }
 
+namespace {
+
+// Symmetric adjacency (no self loops) of a graph given by CSR rows with possibly
+// repeated entries: sorted and unique per row.
+void sym_unique(int n, std::vector<std::vector<int>> &adj) {
+  for (int i = 0; i < n; i++) {
+    auto &a = adj[size_t(i)];
+    std::sort(a.begin(), a.end());
+    a.erase(std::unique(a.begin(), a.end()), a.end());
+  }
+}
+
+// One greedy distance-1 aggregation pass over a graph (adjacency lists, no self).
+int aggregate_pass(int n, const std::vector<std::vector<int>> &adj, std::vector<int> &agg) {
+  agg.assign(size_t(n), -1);
+  int na = 0;
+  for (int i = 0; i < n; i++) {
+    if (agg[size_t(i)] >= 0) continue;
+    bool free_nbhd = true;
+    for (int j : adj[size_t(i)])
+      if (agg[size_t(j)] >= 0) {
+        free_nbhd = false;
+        break;
+      }
+    if (!free_nbhd) continue;
+    agg[size_t(i)] = na;
+    for (int j : adj[size_t(i)]) agg[size_t(j)] = na;
+    na++;
+  }
+  std::vector<int> root_agg(agg);  // the aggregates the roots formed
+  for (int i = 0; i < n; i++) {
+    if (agg[size_t(i)] >= 0) continue;
+    for (int j : adj[size_t(i)])
+      if (root_agg[size_t(j)] >= 0) {
+        agg[size_t(i)] = root_agg[size_t(j)];
+        break;
+      }
+    if (agg[size_t(i)] < 0) agg[size_t(i)] = na++;  // unreachable for a connected graph; kept safe
+  }
+  return na;
+}
+
+}  // namespace
+
+void aggregate_nodes(const Profile &p, int max_aggregates, Aggregation &out) {
+  const int N = p.N;
+  std::vector<std::vector<int>> adj(static_cast<size_t>(N));
+  for (int i = 0; i < N; i++) {
+    for (int j = p.indexL[i]; j < p.indexL[i + 1]; j++) {
+      const int c = p.itemL[j] - 1;
+      if (c >= 0 && c < N && c != i) {
+        adj[size_t(i)].push_back(c);
+        adj[size_t(c)].push_back(i);
+      }
+    }
+    for (int j = p.indexU[i]; j < p.indexU[i + 1]; j++) {
+      const int c = p.itemU[j] - 1;
+      if (c >= 0 && c < N && c != i) {
+        adj[size_t(i)].push_back(c);
+        adj[size_t(c)].push_back(i);
+      }
+    }
+  }
+  sym_unique(N, adj);
+  std::vector<int> agg(static_cast<size_t>(N));
+  for (int i = 0; i < N; i++) agg[size_t(i)] = i;
+  int n = N;
+  std::vector<std::vector<int>> g = adj;
+  while (n > max_aggregates) {
+    std::vector<int> a;
+    const int na = aggregate_pass(n, g, a);
+    if (2 * na > n) break;  // no longer coarsening
+    for (int i = 0; i < N; i++) agg[size_t(i)] = a[size_t(agg[size_t(i)])];
+    std::vector<std::vector<int>> h(static_cast<size_t>(na));
+    for (int u = 0; u < n; u++)
+      for (int v : g[size_t(u)])
+        if (a[size_t(u)] != a[size_t(v)]) h[size_t(a[size_t(u)])].push_back(a[size_t(v)]);
+    sym_unique(na, h);
+    g.swap(h);
+    n = na;
+  }
+  out.n_agg = n;
+  out.agg = agg;
+  // prolongator pattern: aggregates of each closed neighbourhood
+  out.pptr.assign(size_t(N) + 1, 0);
+  out.pagg.clear();
+  std::vector<int> tmp;
+  for (int i = 0; i < N; i++) {
+    tmp.clear();
+    tmp.push_back(agg[size_t(i)]);
+    for (int j : adj[size_t(i)]) tmp.push_back(agg[size_t(j)]);
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    out.pagg.insert(out.pagg.end(), tmp.begin(), tmp.end());
+    out.pptr[size_t(i) + 1] = int(out.pagg.size());
+  }
+  // two-ring pattern (rows of A P)
+  out.qptr.assign(size_t(N) + 1, 0);
+  out.qagg.clear();
+  for (int i = 0; i < N; i++) {
+    tmp.clear();
+    for (int q = out.pptr[size_t(i)]; q < out.pptr[size_t(i) + 1]; q++) tmp.push_back(out.pagg[size_t(q)]);
+    for (int j : adj[size_t(i)])
+      for (int q = out.pptr[size_t(j)]; q < out.pptr[size_t(j) + 1]; q++) tmp.push_back(out.pagg[size_t(q)]);
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    out.qagg.insert(out.qagg.end(), tmp.begin(), tmp.end());
+    out.qptr[size_t(i) + 1] = int(out.qagg.size());
+  }
+  // restriction gather: per aggregate its (node, entry) pairs, ascending node
+  out.rptr.assign(size_t(n) + 1, 0);
+  for (int a : out.pagg) out.rptr[size_t(a) + 1]++;
+  for (int a = 0; a < n; a++) out.rptr[size_t(a) + 1] += out.rptr[size_t(a)];
+  out.rnode.assign(out.pagg.size(), 0);
+  out.rpos.assign(out.pagg.size(), 0);
+  std::vector<int> fill(out.rptr.begin(), out.rptr.end() - 1);
+  for (int i = 0; i < N; i++)
+    for (int q = out.pptr[size_t(i)]; q < out.pptr[size_t(i) + 1]; q++) {
+      const int a = out.pagg[size_t(q)];
+      out.rnode[size_t(fill[size_t(a)])] = i;
+      out.rpos[size_t(fill[size_t(a)]++)] = q;
+    }
+  // coarse pattern: row a = union of the two-ring patterns of a's restriction nodes
+  out.cptr.assign(size_t(n) + 1, 0);
+  out.cagg.clear();
+  for (int a = 0; a < n; a++) {
+    tmp.clear();
+    for (int t = out.rptr[size_t(a)]; t < out.rptr[size_t(a) + 1]; t++) {
+      const int i = out.rnode[size_t(t)];
+      for (int q = out.qptr[size_t(i)]; q < out.qptr[size_t(i) + 1]; q++) tmp.push_back(out.qagg[size_t(q)]);
+    }
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    out.cagg.insert(out.cagg.end(), tmp.begin(), tmp.end());
+    out.cptr[size_t(a) + 1] = int(out.cagg.size());
+  }
+}
+
 }  // namespace h33

@@ -141,4 +141,29 @@ int factor_bilu_fill(const FilledProfile &f, int level, const double *D, const d
 void level_schedule(const Profile &p, bool lower, std::vector<int> &order,
                     std::vector<int> &level_ptr);
 
+// Aggregates of the node graph for the coarse space of the learned two-level
+// preconditioner (no counterpart in the reference solver).  One pass: nodes in index
+// order; a node whose closed neighbourhood is still free roots a new aggregate of that
+// neighbourhood; every node left joins the aggregate of its first neighbour that a
+// root took.  Passes repeat on the graph of aggregates while there are more than
+// max_aggregates and a pass at least halves the count, so on a 27-point mesh one pass
+// gives 3x3x3-node aggregates and two give 9x9x9.  Also:
+//   pptr/pagg: for node i the aggregates of its closed neighbourhood, ascending
+//              (the block pattern of the smoothed prolongator's row i);
+//   rptr/rnode/rpos: for aggregate a the entries p of pagg with pagg[p] == a, as
+//              (node, p) pairs in ascending node order (the restriction's gather).
+//   qptr/qagg: for node i the aggregates of its two-ring (the union of pagg over the
+//              closed neighbourhood), ascending: the pattern of row i of A P;
+//   cptr/cagg: for aggregate a the aggregates b with a nonzero coarse block (a, b),
+//              ascending: the union of qagg over the nodes of a's restriction.
+struct Aggregation {
+  int n_agg = 0;
+  std::vector<int> agg;
+  std::vector<int> pptr, pagg;
+  std::vector<int> rptr, rnode, rpos;
+  std::vector<int> qptr, qagg;
+  std::vector<int> cptr, cagg;
+};
+void aggregate_nodes(const Profile &p, int max_aggregates, Aggregation &out);
+
 }  // namespace h33
