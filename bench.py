@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision variant")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner variants")
-    ap.add_argument("--train-steps", type=int, default=60)
+    ap.add_argument("--train-steps", type=int, default=40)
+    ap.add_argument("--train-lr", type=float, default=5e-3)
     ap.add_argument("--no-multi", action="store_true", help="skip the 16-load-case multi-RHS measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-system batched measurement")
     ap.add_argument("--no-assembly", action="store_true", help="skip the HEX8 assembly measurement")
@@ -72,6 +73,8 @@ def parse():
     ap.add_argument("--newton-mesh", default="64,64,64")
     ap.add_argument("--profile-solve", action="store_true",
                     help="one solve capped at 5 CG iterations, nothing printed (profiling)")
+    ap.add_argument("--profile-mode", type=int, default=0,
+                    help="precision mode (Iarray(42)) of the --profile-solve solve")
     ap.add_argument("--profile-multi", action="store_true",
                     help="one 16-load-case solve capped at 3 CG iterations, nothing printed (profiling)")
     ap.add_argument("--profile-batch", action="store_true",
@@ -523,7 +526,7 @@ def bench_learned_newton(args):
         if inc == 5 and it == 1 and not train:
             n = s.learn_record(0)
             t0 = time.perf_counter()
-            l0, l1 = s.learn_train(steps=args.train_steps, lr=2e-3)
+            l0, l1 = s.learn_train(steps=args.train_steps, lr=args.train_lr)
             train.update(pairs=n, steps=args.train_steps, loss_before=l0, loss_after=l1,
                          train_s=time.perf_counter() - t0)
         rec = {"increment": inc, "newton": it}
@@ -737,6 +740,7 @@ def main():
     if args.profile_solve:
         mm = m.copy()
         mm.set_iter(5)
+        mm.Iarray[41] = args.profile_mode
         rec = solver.solve(mm)
         if rec["error"] not in (0, 3001):
             raise SystemExit("solve failed: %r" % rec)
@@ -783,7 +787,7 @@ def main():
             assert rec["error"] == 0
         npairs = solver.learn_record(0)
         t1 = time.perf_counter()
-        loss0, loss1 = solver.learn_train(steps=args.train_steps, lr=2e-3)
+        loss0, loss1 = solver.learn_train(steps=args.train_steps, lr=args.train_lr)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
         train = {"pairs": npairs, "record_s": t1 - t0, "train_s": t2 - t1, "steps": args.train_steps,
@@ -792,12 +796,13 @@ def main():
     class VariantFailed(Exception):
         pass
 
-    def step(mode, learned=0):
+    def step(mode, learned=0, coarse=0):
         dX.zero_()
         torch.cuda.synchronize()
         iam = ia.copy()
         iam[41] = mode
         iam[42] = learned
+        iam[43] = coarse
         rec = solver.solve_resident_device(dB.data_ptr(), dX.data_ptr(), iam, ra.copy())
         if rec["error"] != 0:
             if mode == 0 and learned == 0:
@@ -806,22 +811,27 @@ def main():
         return rec
 
     variants = {}
-    modes = [("fp64", 0, 0)] + ([] if args.no_mixed else [("mixed", 1, 0)])
+    modes = [("fp64", 0, 0, 0)] + ([] if args.no_mixed else [("mixed", 1, 0, 0)])
     if train is not None:
-        modes += [("learned_fp64", 0, 1), ("learned_mixed", 1, 1)]
+        modes += [("learned_fp64", 0, 1, 0), ("learned_mixed", 1, 1, 0)]
+    if not args.no_learned and not args.no_mixed:
+        # ablations of the learned two-level preconditioner (not headline candidates):
+        # the same coarse space without the network's smoothing weights, and with the
+        # untrained network's weights (1/2 everywhere)
+        modes += [("twolevel_unsmoothed_mixed", 1, 1, 1), ("twolevel_uniform_mixed", 1, 1, 2)]
     clocks = Clocks(uuid)
     sols = {}
     failed = {}
     clocks.start()  # sampled over every variant's solves, the headline's among them
-    for name, mode, learned in modes:
+    for name, mode, learned, coarse in modes:
         # every rank runs the same steps; a variant that fails (non-FP64 only) is
         # reported and left out of the headline
         try:
             for _ in range(args.warmup):
-                step(mode, learned)
+                step(mode, learned, coarse)
             barrier()
             t0 = time.perf_counter()
-            recs = [step(mode, learned) for _ in range(args.steps)]
+            recs = [step(mode, learned, coarse) for _ in range(args.steps)]
         except VariantFailed as exc:
             barrier()
             r = exc.args[0]
@@ -840,7 +850,7 @@ def main():
         variants[name]["rel_err_vs_fp64"] = float(np.linalg.norm(sols[name] - sols["fp64"]) /
                                                   np.linalg.norm(sols["fp64"]))
     # headline: the fastest variant whose FP64 true residual meets the tolerance
-    ok = [k for k, v in variants.items() if v["true_resid"] <= args.tol]
+    ok = [k for k, v in variants.items() if v["true_resid"] <= args.tol and not k.startswith("twolevel_")]
     head = min(ok, key=lambda k: variants[k]["s"]) if ok else "fp64"
     variants.update({k: {"failed": v} for k, v in failed.items()})
     dev_s = variants[head]["s"]
@@ -942,9 +952,10 @@ def main():
         cfg = config_dict(nx, ny, nz, m, args)
         cfg["solver"] = {"fp64": "plain FP64 CG + SSOR (drop-in)",
                          "mixed": "FP64 CG + SSOR with BF16-stored factors (Iarray(42)=1)",
-                         "learned_fp64": "flexible CG, SSOR + learned network, FP64 (Iarray(43)=1)",
-                         "learned_mixed": "flexible CG, BF16-stored SSOR + learned network, FP64 iterations "
-                                          "(Iarray(42)=1, Iarray(43)=1)"}[head]
+                         "learned_fp64": "flexible CG, learned two-level preconditioner (SSOR two-grid cycle with "
+                                         "the coarse space the network shapes), FP64 (Iarray(43)=1)",
+                         "learned_mixed": "flexible CG, learned two-level preconditioner with BF16-stored SSOR and "
+                                          "FP32 inner residuals, FP64 iterations (Iarray(42)=1, Iarray(43)=1)"}[head]
         line = {
             "metric": METRIC, "value": dev_s, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_s * 1e3, "higher_is_better": False,

@@ -435,7 +435,28 @@ __global__ void coarse_prolong_kernel(CoarseView c, const double *__restrict__ y
   }
 }
 
+// End of the symmetric two-grid application: z = zc + z (z the post-smoothing SSOR
+// step), or z = zs once the correction is off (SSOR-CG).
+template <class R>
+__global__ void coarse_post_kernel(const R *__restrict__ zc, const R *__restrict__ zs, R *__restrict__ z, int n3,
+                                   const CgState *st) {
+  pdl_entry();
+  if (st && st->done) return;
+  const bool on = !st || st->use_gnn;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += gridDim.x * blockDim.x)
+    z[k] = on ? z[k] + zc[k] : zs[k];
+}
+
 // ---- training -----------------------------------------------------------------
+// out = double(a) (- b when given): a recorded FP32 pair vector widened, optionally
+// less an FP64 vector.
+__global__ void coarse_widen_kernel(const float *__restrict__ a, const double *__restrict__ b, double *__restrict__ out,
+                                    int n) {
+  pdl_entry();
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    out[k] = double(a[k]) - (b ? b[k] : 0.0);
+}
+
 // Loss of one recorded pair (r = A e): the energy of e outside the coarse space,
 //   L = (e^T r - bc^T y) / (e^T r),   y = Ac^-1 P^T r,
 // whose gradient in P is -2 (r - A P y) y^T / (e^T r), so in omega (dP/domega = -T0):

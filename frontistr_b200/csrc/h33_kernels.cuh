@@ -401,8 +401,10 @@ __global__ void alu_kernel(const double *__restrict__ blocks, const int *__restr
 
 // y = A x (MODE 0), r = b - A x (MODE 1); MODE 2: q = A p with the {p}{q} partial
 // and the ALPHA finisher.
-template <class R, int MODE>
-__global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<R> A, const R *__restrict__ x,
+// TV: the stored values (R by default; FP32 for the residuals inside the learned
+// preconditioner of precision mode 1).
+template <class R, int MODE, class TV = R>
+__global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<TV> A, const R *__restrict__ x,
                                                         R *__restrict__ y, const R *__restrict__ b,
                                                         CgState *st, double *partials) {
   pdl_entry();
@@ -416,7 +418,7 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView<R> A, const R *
     const int row = A.row0[s] + lane;
     const int len = active ? A.rowlen[s * 32 + lane] : 0;
     R y0 = 0, y1 = 0, y2 = 0;
-    row_gemv<R, R, 1, false>(A, s, lane, len, x, y0, y1, y2);
+    row_gemv<R, TV, 1, false>(A, s, lane, len, x, y0, y1, y2);
     if (active) {
       if (MODE == 1) {
         y0 = b[3 * row] - y0;

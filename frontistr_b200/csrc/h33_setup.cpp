@@ -812,7 +812,7 @@ void aggregate_nodes(const Profile &p, int max_aggregates, Aggregation &out) {
   for (int i = 0; i < N; i++) agg[size_t(i)] = i;
   int n = N;
   std::vector<std::vector<int>> g = adj;
-  while (n > max_aggregates) {
+  for (int pass = 0; pass == 0 || n > max_aggregates; pass++) {
     std::vector<int> a;
     const int na = aggregate_pass(n, g, a);
     if (2 * na > n) break;  // no longer coarsening

@@ -145,9 +145,10 @@ void level_schedule(const Profile &p, bool lower, std::vector<int> &order,
 // preconditioner (no counterpart in the reference solver).  One pass: nodes in index
 // order; a node whose closed neighbourhood is still free roots a new aggregate of that
 // neighbourhood; every node left joins the aggregate of its first neighbour that a
-// root took.  Passes repeat on the graph of aggregates while there are more than
-// max_aggregates and a pass at least halves the count, so on a 27-point mesh one pass
-// gives 3x3x3-node aggregates and two give 9x9x9.  Also:
+// root took.  The first pass always runs; passes then repeat on the graph of
+// aggregates while there are more than max_aggregates and a pass at least halves the
+// count, so on a 27-point mesh one pass gives 3x3x3-node aggregates and two give
+// 9x9x9.  Also:
 //   pptr/pagg: for node i the aggregates of its closed neighbourhood, ascending
 //              (the block pattern of the smoothed prolongator's row i);
 //   rptr/rnode/rpos: for aggregate a the entries p of pagg with pagg[p] == a, as

@@ -1156,6 +1156,54 @@ void ensure_bicg(Solver &S) {
 template <class R>
 void launch_coarse(Solver &S, const R *zs, const R *r, R *z, CgState *st);
 
+// HECMW33_COARSE_FORM: 0 (default) the symmetric two-grid form, 1 the additive form.
+// Measured on the 100^3 cube (BF16-stored SSOR, omega = 1/2): two-grid 62 iterations,
+// additive 115; the two-grid form is the one whose convergence the training loss
+// (the error energy left outside the coarse space after one SSOR step) measures.
+int coarse_form() {
+  static const int v = [] {
+    const char *e = std::getenv("HECMW33_COARSE_FORM");
+    return e ? std::atoi(e) : 0;
+  }();
+  return v;
+}
+
+// y = r - A x inside the preconditioner: with the FP32 copy of A when the SSOR is
+// BF16-stored (precision mode 1), else in the working precision.
+template <class R>
+void precond_resid(Solver &S, const Views<R> &V, const R *x, R *y) {
+  if constexpr (std::is_same<R, double>::value) {
+    if (V.lowp) {
+      launch_k(S.stream, spmv_kernel<double, 1, float>, S.grid_spmv(), kThreads, S.A.view32(), x, y,
+               static_cast<const double *>(V.r), static_cast<CgState *>(nullptr), static_cast<double *>(nullptr));
+      return;
+    }
+  }
+  launch_k(S.stream, spmv_kernel<R, 1>, S.grid_spmv(), kThreads, V.A, x, y, static_cast<const R *>(V.r),
+           static_cast<CgState *>(nullptr), static_cast<double *>(nullptr));
+}
+
+// The learned two-level preconditioner z = M^-1 r.  Symmetric two-grid form:
+//   zs = SSOR(r);  zc = zs + P Ac^-1 P^T (r - A zs);  z = zc + SSOR(r - A zc)
+// (pre-smoothing, coarse correction, post-smoothing: symmetric because SSOR is);
+// additive form: z = SSOR(r) + P Ac^-1 P^T r.  With the correction off (fallback)
+// z = SSOR(r).
+template <class R>
+void launch_learned_precond(Solver &S, const Views<R> &V, CgState *st) {
+  cudaStream_t s = S.stream;
+  launch_sweep<R, false>(S, V, V.r, V.zs, st);
+  if (coarse_form() == 1) {
+    launch_coarse<R>(S, V.zs, V.r, V.z, st);
+    return;
+  }
+  precond_resid<R>(S, V, V.zs, V.w);
+  launch_coarse<R>(S, V.zs, V.w, V.zp, st);
+  precond_resid<R>(S, V, V.zp, V.w);
+  launch_sweep<R, false>(S, V, V.w, V.z, st);
+  launch_k(s, coarse_post_kernel<R>, S.grid_vec(), kThreads, static_cast<const R *>(V.zp),
+           static_cast<const R *>(V.zs), V.z, S.n3(), static_cast<const CgState *>(st));
+}
+
 // One flexible-CG iteration with the learned two-level preconditioner: SSOR, then the
 // coarse correction of the space the network shapes (iterPREmax = 1).  The correction
 // may be switched off on the device (fallback); its kernels then only copy the SSOR
@@ -1166,8 +1214,7 @@ void launch_iteration_flex(Solver &S, const Views<R> &V, cudaGraphConditionalHan
   CgState *st = S.state.p;
   const int n3 = S.n3();
   launch_k(s, iter_begin_kernel, 1, 32, st, h, use_cond);
-  launch_sweep<R, false>(S, V, V.r, V.zs, st);
-  launch_coarse<R>(S, V.zs, V.r, V.z, st);
+  launch_learned_precond<R>(S, V, st);
   launch_k(s, fcg_rho_kernel<R>, S.grid_vec(), kThreads, V.z, V.r, V.rold, n3, st, S.partials.p);
   launch_k(s, update_p_kernel<R>, S.grid_vec(), kThreads, V.z, V.p, n3, st);
   launch_k(s, spmv_kernel<R, 2>, S.grid_spmv(), kThreads, V.A, V.p, V.q, nullptr, st, S.partials.p);
@@ -1196,8 +1243,7 @@ void launch_iteration_reliable(Solver &S, int iterpremax, bool learned, cudaGrap
   const Views<float> V = views(S, 0.0f);
   launch_k(s, iter_begin_kernel, 1, 32, st, h, use_cond);
   if (learned) {
-    launch_sweep<float, false>(S, V, V.r, V.zs, st);
-    launch_coarse<float>(S, V.zs, V.r, V.z, st);
+    launch_learned_precond<float>(S, V, st);
     launch_k(s, fcg_rho_kernel<float>, S.grid_vec(), kThreads, V.z, V.r, V.rold, n3, st, S.partials.p);
   } else {
     launch_precond<float>(S, V, iterpremax, V.r, V.z, st);
@@ -1284,7 +1330,8 @@ float run_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels, int
   S.h_params->iterpremax = iterpremax;
   S.h_params->inner = inner || reliable;
   S.h_params->flexible = learned;
-  S.h_params->use_gnn = learned;
+  // a coarse matrix that was not positive definite leaves the correction off (SSOR-CG)
+  S.h_params->use_gnn = learned && S.L.C.ok;
   S.h_params->reliable = reliable;
   S.h_params->ru_delta = ru_delta;
   S.h_params->method = method;
@@ -1700,9 +1747,19 @@ void learned_prepare_inference(Solver &S) {
     throw Failure(HECMW33_ERR_INCONS_PC, "learned preconditioner requested but not trained");
   if (!(S.pc.valid && S.pc.kind == 1))
     throw Failure(HECMW33_ERR_INCONS_PC, "the learned preconditioner works after SSOR (PRECOND 1 or 2)");
+  if (S.dom.on)
+    throw Failure(HECMW33_ERR_INCONS_PC, "the learned preconditioner takes a whole mesh (one domain) only");
   learned_graph(S);
   coarse_structure(S);
   coarse_values(S);
+  if (S.a32_version != S.values_version) {  // FP32 A for the residuals of the mode-1 preconditioner
+    S.A.val32.alloc(S.A.val.n);
+    const size_t n = S.A.val.n;
+    launch_k(S.stream, convert_kernel<float>, int(std::min<size_t>((n + kThreads - 1) / kThreads, size_t(S.nsm) * 16)),
+             kThreads, static_cast<const double *>(S.A.val.p), S.A.val32.p, n);
+    H33_CUDA(cudaGetLastError());
+    S.a32_version = S.values_version;
+  }
   const int wv = L.coarse_mode == 0 ? L.weights_version : -1;
   if (C.op_precond != S.pc.numeric_version || C.op_weights != wv || C.op_mode != L.coarse_mode) {
     const float *omega = nullptr;
@@ -1884,9 +1941,9 @@ float record_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels) 
   return ms;
 }
 
-// Trains the network on the recorded pairs: Adam on the mean loss of
-// learned_coarse_pass.  loss[0] = mean loss before the first step, loss[1] = after
-// the last.
+// Trains the network on the recorded pairs, smoothed once by SSOR: Adam on the mean
+// loss of learned_coarse_pass.  loss[0] = mean loss before the first step, loss[1] =
+// after the last.
 void learned_train(Solver &S, int steps, double lr, double *loss) {
   Learned &L = S.L;
   const int np = int(L.pr.size());
@@ -1898,18 +1955,42 @@ void learned_train(Solver &S, int steps, double lr, double *loss) {
   coarse_structure(S);
   coarse_values(S);
   if (!L.have_weights) learned_init_weights(S, 12345);
+  // The coarse correction has to capture what SSOR leaves: each pair's error after
+  // one SSOR step, e' = e - SSOR(r), with r' = A e' (FP64, stored as FP32).
+  std::vector<DevArray<float>> sr(static_cast<size_t>(np));
+  std::vector<double> ser(static_cast<size_t>(np));
   std::vector<const float *> pr;
-  for (int k = 0; k < np; k++) pr.push_back(L.pr[size_t(k)].p);
+  {
+    auto &C = L.C;
+    const Views<double> V = views(S, 0.0);
+    const int gt = S.grid_vec(), n3 = S.n3();
+    for (int k = 0; k < np; k++) {
+      launch_k(S.stream, coarse_widen_kernel, gt, kThreads, static_cast<const float *>(L.pr[size_t(k)].p),
+               static_cast<const double *>(nullptr), S.w.p, n3);
+      launch_sweep<double, false>(S, V, S.w.p, C.v.p, nullptr);
+      launch_k(S.stream, coarse_widen_kernel, gt, kThreads, static_cast<const float *>(L.pe[size_t(k)].p),
+               static_cast<const double *>(C.v.p), C.t0y.p, n3);
+      launch_k(S.stream, spmv_kernel<double, 0>, S.grid_spmv(), kThreads, S.A.view(),
+               static_cast<const double *>(C.t0y.p), C.apy.p, static_cast<const double *>(nullptr),
+               static_cast<CgState *>(nullptr), static_cast<double *>(nullptr));
+      sr[size_t(k)].alloc(size_t(n3));
+      launch_k(S.stream, narrow_kernel, gt, kThreads, static_cast<const double *>(C.apy.p), sr[size_t(k)].p, n3);
+      H33_CUDA(cudaGetLastError());
+      ser[size_t(k)] = dot_device(S, C.t0y.p, C.apy.p);
+      if (!(ser[size_t(k)] > 0.0)) throw Failure(HECMW33_ERR_CUDA, "learned training: a smoothed pair lost its energy");
+      pr.push_back(sr[size_t(k)].p);
+    }
+  }
   const int nparam = GnnOffsets::make().total;
-  loss[0] = learned_coarse_pass(S, pr, L.per, false);
+  loss[0] = learned_coarse_pass(S, pr, ser, false);
   for (int it = 0; it < steps; it++) {
-    learned_coarse_pass(S, pr, L.per, true);
+    learned_coarse_pass(S, pr, ser, true);
     L.adam_step++;
     launch_k(S.stream, gnn_adam_kernel, (nparam + 255) / 256, 256, L.theta.p, static_cast<const float *>(L.gacc.p),
              L.m1.p, L.m2.p, nparam, float(lr), 0.9f, 0.999f, 1e-8f, L.adam_step, 1.0f, L.theta_bf16.p);
     H33_CUDA(cudaGetLastError());
   }
-  loss[1] = learned_coarse_pass(S, pr, L.per, false);
+  loss[1] = learned_coarse_pass(S, pr, ser, false);
   L.weights_version++;
 }
 
@@ -4143,6 +4224,21 @@ HECMW33_API void hecmw33_gpu_colour_schedule(const int *N, const int *indexL, co
   *ncolor = ordering_mc(prof, perm_rcm, *ncolor_in, ci, pm, ipm);
   for (int c = 0; c <= *ncolor; c++) colorindex[c] = ci[c];
   for (int i = 0; i < n; i++) perm[i] = pm[i] + 1;
+  H33_ENTRY_END
+}
+
+HECMW33_API void hecmw33_gpu_coarse_aggregates(const int *N, const int *indexL, const int *itemL,
+                                               const int *indexU, const int *itemU, const int *max_aggregates,
+                                               int *n_agg, int *agg, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  const int n = *N;
+  validate(n, n, indexL[n], indexU[n], indexL, itemL, indexU, itemU);
+  Profile prof{n, indexL, itemL, indexU, itemU};
+  Aggregation ag;
+  aggregate_nodes(prof, max_aggregates && *max_aggregates > 0 ? *max_aggregates : coarse_max_aggregates(), ag);
+  *n_agg = ag.n_agg;
+  for (int i = 0; i < n; i++) agg[i] = ag.agg[size_t(i)];
   H33_ENTRY_END
 }
 

@@ -481,3 +481,18 @@ def colour_schedule(m, ncolor_in=10):
     if err.value:
         raise HecmwSolverError(err.value, last_error())
     return ci[:nc.value + 1].copy(), perm
+
+
+def coarse_aggregates(m, max_aggregates=0):
+    """Host-only aggregates of the node graph of a HecMatrix profile (the coarse space of
+    the learned two-level preconditioner): (number of aggregates, 0-based id per node)."""
+    lib = gpu_lib()
+    n = m.N
+    na = ctypes.c_int(0)
+    agg = np.zeros(n, np.int32)
+    err = ctypes.c_int(0)
+    lib.hecmw33_gpu_coarse_aggregates(_i(n), _ip(m.indexL), _ip(m.itemL), _ip(m.indexU), _ip(m.itemU),
+                                      _i(max_aggregates), ctypes.byref(na), _ip(agg), ctypes.byref(err))
+    if err.value:
+        raise HecmwSolverError(err.value, last_error())
+    return na.value, agg

@@ -54,7 +54,8 @@
  *                       residual are folded into FP64 (x64 += x32, r = b - A x in FP64)
  *                       each time the FP32 residual has fallen by Rarray(42) (0 -> 0.1)
  *       Rarray(42)      inner tolerance (mode 2) / refinement factor (mode 3)
- *       Iarray(43) = 1  learned preconditioner after SSOR (see hecmw33_gpu_learn_*)
+ *       Iarray(43) = 1  learned two-level preconditioner around SSOR (see
+ *                       hecmw33_gpu_learn_*; Iarray(44) its coarse smoothing weights)
  *   - *ierr receives 0 or an error code: the reference's codes (1001, 2001, 2002,
  *     3001-3004; hecmw1/src/solver/init/hecmw_solve_error.f90:9-16) or the
  *     HECMW33_ERR_* codes below.  1001 and 2001 are fatal in the reference
@@ -242,16 +243,38 @@ HECMW33_API void hecmw33_gpu_colour_schedule(const int *N, const int *indexL, co
                                              const int *ncolor_in, int *ncolor, int *colorindex,
                                              int *perm, int *ierr);
 
+/* Host-only (no GPU needed; no counterpart in the reference): the aggregates of the
+ * node graph on which the learned two-level preconditioner (Iarray(43) = 1) builds its
+ * coarse space.  Greedy passes (a node whose closed neighbourhood is free roots an
+ * aggregate of it; the rest join a neighbour's), the first always, then repeated on the
+ * aggregate graph while more than *max_aggregates remain (<= 0: the library default,
+ * 2000, or HECMW33_COARSE_AGG) and a pass at least halves the count.  agg[0..N-1]
+ * receives 0-based aggregate ids, *n_agg their number. */
+HECMW33_API void hecmw33_gpu_coarse_aggregates(const int *N, const int *indexL, const int *itemL,
+                                               const int *indexU, const int *itemU, const int *max_aggregates,
+                                               int *n_agg, int *agg, int *ierr);
+
 /* ---- learned preconditioner (no counterpart in the reference) -------------------
- * Selected by Iarray(43) = 1 (with SSOR, PRECOND 1/2, iterPREmax 1): after the SSOR
- * sweep, a 3-layer message-passing network over the matrix graph (width 32, BF16
- * weights, FP32 accumulation) adds a correction; the solve becomes flexible CG
- * (BETA = z.(r - r_old)/RHO_old).  The network is switched off on the device --
- * SSOR-CG takes over, restarted -- when RHO <= 0 or when the residual falls by
- * less than 20 % over 25 iterations.  Works in FP64 (Iarray(42) = 0) and inside
- * mixed precision (Iarray(42) = 1).  Training data are (r, e) pairs recorded from
- * earlier FP64 SSOR-CG solves on the same handle (e.g. earlier Newton or load
- * increments): r_k = b - A x_k and e_k = x* - x_k at iterations 1, 2, 4, 8, ...
+ * Selected by Iarray(43) = 1 (with SSOR, PRECOND 1/2, iterPREmax 1, a whole mesh): a
+ * two-level preconditioner in flexible CG (BETA = z.(r - r_old)/RHO_old), the
+ * symmetric two-grid cycle
+ *     zs = SSOR(r);  zc = zs + P Ac^-1 P^T (r - A zs);  z = zc + SSOR(r - A zc),
+ * Ac = P^T A P, on aggregates of the node graph (hecmw33_gpu_coarse_aggregates).  The
+ * prolongator is a smoothed aggregation P = (I - Omega D^-1 A) P0 (P0: the aggregates'
+ * translations, zero on constrained DOFs; D: the diagonal blocks) whose per-DOF
+ * smoothing weights Omega = sigmoid(out) come from a 3-layer message-passing network
+ * over the matrix graph (width 32, edge features the scaled 3x3 blocks, BF16 weights,
+ * FP32 accumulation), run once per matrix.  Ac is formed on the device and inverted
+ * there (FP64, blocked Gauss-Jordan); a coarse correction is P^T r, one dense GEMV and
+ * P y.  Iarray(44) picks the smoothing weights: 0 the network's (default), 1 none
+ * (Omega = 0: plain aggregation), 2 one half everywhere (the untrained network).  The
+ * correction is switched off on the device -- SSOR-CG takes over, restarted -- when
+ * RHO <= 0 or the residual falls by less than 20 % over 25 iterations, and from the
+ * start when Ac is not positive definite.  Works in FP64 (Iarray(42) = 0) and with
+ * the BF16-stored SSOR of precision mode 1 (whose residuals inside the cycle use an
+ * FP32 copy of A).  Training data are (r, e) pairs recorded from earlier FP64 SSOR-CG
+ * solves on the same handle (earlier Newton or load increments): r_k = b - A x_k and
+ * e_k = x* - x_k at iterations 1, 2, 4, 8, ...
  *
  * enable: 1 record pairs during the following FP64 solves, 0 stop, -1 forget them;
  * max_pairs (optional, >0): keep the newest max_pairs pairs; *npairs: pairs held. */
@@ -259,9 +282,12 @@ HECMW33_API void hecmw33_gpu_learn_record(const int *handle, const int *enable, 
                                           int *npairs, int *ierr);
 
 /* Trains the network on the recorded pairs with the handle's GPU kernels (forward,
- * backward, Adam; FP32 master weights), minimising the mean energy-norm error of the
- * preconditioned step, (z - e)^T A (z - e) / (e^T r).  loss[0]/loss[1]: mean loss
- * before the first and after the last of `steps` steps (learning rate lr). */
+ * backward, Adam; FP32 master weights).  Each pair is first smoothed by one SSOR step
+ * (e' = e - SSOR(r), r' = A e': the error the coarse space has to capture); the loss
+ * is the mean share of a pair's error energy outside the coarse space,
+ * (e'^T r' - (P^T r')^T Ac^-1 P^T r') / (e'^T r'), with Ac rebuilt and inverted at
+ * every step.  loss[0]/loss[1]: mean loss before the first and after the last of
+ * `steps` steps (learning rate lr). */
 HECMW33_API void hecmw33_gpu_learn_train(const int *handle, const int *steps, const double *lr, double *loss,
                                          int *ierr);
 
@@ -270,10 +296,13 @@ HECMW33_API void hecmw33_gpu_learn_train(const int *handle, const int *steps, co
  * must match) and reset the optimiser.  Used to save and restore trained networks. */
 HECMW33_API void hecmw33_gpu_learn_weights(const int *handle, const int *mode, float *theta, int *n, int *ierr);
 
-/* One evaluation of the network for checking: with weights theta (FP32), residual R
- * and error E (host, 3*NP), returns z = SSOR(R) + network correction (Z), the loss
- * (z - E)^T A (z - E) / (E^T R) and its gradient with respect to theta (grad, may be
- * NULL), all in FP32 on the GPU.  Needs the SSOR preconditioner already built. */
+/* One evaluation of the network for checking: with weights theta (FP32) and one pair,
+ * residual R and error E (host, 3*NP, R = A E, kept in FP32 as recorded pairs are),
+ * returns the network's smoothing weights Omega (Z, 3*NP), the loss of that pair as
+ * hecmw33_gpu_learn_train defines it but without the SSOR smoothing,
+ * (E^T R - (P^T R)^T Ac^-1 P^T R) / (E^T R), and its gradient with respect to theta
+ * (grad, may be NULL): network in FP32, coarse algebra in FP64 on the GPU.  Needs the
+ * SSOR preconditioner already built. */
 HECMW33_API void hecmw33_gpu_learn_eval(const int *handle, const float *theta, const double *R, const double *E,
                                         double *Z, double *loss, float *grad, int *ierr);
 

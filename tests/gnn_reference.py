@@ -1,26 +1,33 @@
-"""CPU (numpy, float64) reference of the learned preconditioner's network.
+"""CPU (numpy/scipy, float64) reference of the learned two-level preconditioner.
 
-TEST INFRASTRUCTURE: the checker for the CUDA forward/backward kernels of the
-learned preconditioner (frontistr_b200/csrc/h33_gnn.cuh).  It has no counterpart
-in the reference solver; its own gradients are checked by finite differences in
+TEST INFRASTRUCTURE: the checker for the CUDA kernels of the learned preconditioner
+(frontistr_b200/csrc/h33_gnn.cuh, h33_coarse.cuh).  It has no counterpart in the
+reference solver; its own gradients are checked by finite differences in
 tests/test_gnn_reference.py.
 
-Network (3 message-passing layers, width 32, no biases so that it is odd in its
-input, and scaled so that it is positively homogeneous -- z(c r) = c z(r)):
+Coarse space: aggregates of the node graph (the library's aggregate_nodes, through the
+C ABI), Ac = P^T A P, the correction P Ac^-1 P^T.
 
-  per node i: s_i = (trace(D_i)/3)^(-1/2), zs = SSOR(r), gamma = sqrt(mean(zs^2))
-  x_i   = [zs_i / gamma, s_i^2 r_i / gamma]                       (6)
-  h0_i  = W_in x_i                                                  (32)
-  edge (i,j), j != i, of the matrix graph; e_ij = s_i A_ij s_j      (9, row-major)
-  w^l_ij = tanh(u_l . e_ij + c_l)                                   (l = 1..3)
-  m^l_i = sum_j w^l_ij h^{l-1}_j
+Prolongator, per node i and aggregate b of i's closed neighbourhood N[i]:
+  M_i     = diag of the DOF mask (1 where the row of A has an off-diagonal entry)
+  T0(i,b) = D_i^-1 sum_{j in N[i], agg(j) = b} A_ij M_j
+  P(i,b)  = [b == agg(i)] M_i - diag(omega_i) T0(i,b)
+
+Network (3 message-passing layers, width 32) producing omega:
+  x_i   = [1, (|aggregates of N[i]| - 1) / 7, share of neighbours outside agg(i), M_i]
+  s_i   = (trace(D_i)/3)^(-1/2);  e_ij = s_i A_ij s_j  (9 features, edge (i,j), j != i)
+  h0_i  = W_in x_i
+  w^l_ij = tanh(u_l . e_ij + c_l);  m^l_i = sum_j w^l_ij h^{l-1}_j
   h^l_i = tanh(Ws_l h^{l-1}_i + Wm_l m^l_i)
-  z_i   = zs_i + gamma * W_out h^3_i                                 (3)
+  out_i = W_out h^3_i;  omega_i = sigmoid(out_i)          (3 per node)
 
-Loss on (r, e) pairs with A e = r (e the error of an iterate):
-  L = (z - e)^T A (z - e) / (e^T r)       (energy norm, relative)
+Loss on pairs (r, e) with A e = r (e the error of an iterate): the energy of e outside
+the coarse space, relative to its energy:
+  L = (e^T r - b^T y) / (e^T r),  b = P^T r,  y = Ac^-1 b
+  dL/dP = -2 g y^T / (e^T r),  g = r - A P y;   dL/domega_(i,d) = 2 g_(i,d) (T0 y)_(i,d) / (e^T r)
 """
 import numpy as np
+import scipy.sparse as sp
 
 WIDTH = 32
 LAYERS = 3
@@ -49,7 +56,7 @@ def unpack(theta):
 
 
 def init_params(seed=0, scale_out=0.0):
-    """Xavier-like init; W_out starts at scale_out (0 -> the network starts as SSOR)."""
+    """Xavier-like init; W_out starts at scale_out (0 -> omega = 1/2 everywhere)."""
     rng = np.random.default_rng(seed)
     parts = []
     for name, shp in param_shapes():
@@ -82,46 +89,120 @@ class Graph:
         blocks = np.concatenate(blocks)
         order = np.lexsort((cols, rows))
         self.rows, self.cols = rows[order], cols[order]
+        self.blocks = blocks[order].reshape(-1, 3, 3)
         self.E = blocks[order] * (self.s[self.rows] * self.s[self.cols])[:, None]
+        self.D = D
         self.N = N
 
 
-def forward(theta, g, zs, r):
+class Coarse:
+    """Aggregates, DOF mask, network features and T0 of a matrix (agg from the library)."""
+
+    def __init__(self, m, g, agg):
+        N = m.N
+        self.N, self.agg = N, np.asarray(agg, dtype=np.int64)
+        self.nagg = int(self.agg.max()) + 1
+        A = m.to_scipy().tocsr()
+        self.A = A
+        # DOF mask: rows with an off-diagonal entry
+        offd = (A - sp.diags(A.diagonal())).tocsr()
+        offd.eliminate_zeros()
+        self.mask = (np.diff(offd.indptr) > 0).astype(np.float64)
+        M = self.mask.reshape(N, 3)
+        # closed-neighbourhood aggregates per node, ascending
+        nb = [[i] for i in range(N)]
+        for i, j in zip(g.rows, g.cols):
+            nb[i].append(j)
+        self.pat = [sorted(set(self.agg[nb[i]].tolist())) for i in range(N)]
+        # T0(i,b) = D_i^-1 sum_{j in N[i], agg(j)=b} A_ij M_j
+        self.T0 = [{b: np.zeros((3, 3)) for b in self.pat[i]} for i in range(N)]
+        for i in range(N):
+            self.T0[i][self.agg[i]] += g.D[i] * M[i][None, :]
+        for k, (i, j) in enumerate(zip(g.rows, g.cols)):
+            self.T0[i][self.agg[j]] += g.blocks[k] * M[j][None, :]
+        for i in range(N):
+            Di = np.linalg.inv(g.D[i])
+            for b in self.T0[i]:
+                self.T0[i][b] = Di @ self.T0[i][b]
+        # network features
+        nnb = np.bincount(g.rows, minlength=N)
+        nout = np.bincount(g.rows, weights=(self.agg[g.rows] != self.agg[g.cols]).astype(float), minlength=N)
+        self.x = np.zeros((N, 6))
+        self.x[:, 0] = 1.0
+        self.x[:, 1] = np.array([len(p) - 1 for p in self.pat]) / 7.0
+        self.x[:, 2] = np.where(nnb > 0, nout / np.maximum(nnb, 1), 0.0)
+        self.x[:, 3:] = M
+
+    def prolongator(self, omega, which="P"):
+        """P (or T0) as a scipy matrix (3N x 3 nagg) for per-DOF weights omega (3N)."""
+        N = self.N
+        rows, cols, vals = [], [], []
+        w = np.asarray(omega, dtype=np.float64).reshape(N, 3)
+        M = self.mask.reshape(N, 3)
+        for i in range(N):
+            for b in self.pat[i]:
+                t = self.T0[i][b]
+                if which == "T0":
+                    blk = t.copy()
+                else:
+                    blk = (np.diag(M[i]) if b == self.agg[i] else 0.0) - w[i][:, None] * t
+                for d in range(3):
+                    for c in range(3):
+                        if blk[d, c] != 0.0:
+                            rows.append(3 * i + d)
+                            cols.append(3 * b + c)
+                            vals.append(blk[d, c])
+        return sp.csr_matrix((vals, (rows, cols)), shape=(3 * N, 3 * self.nagg))
+
+    def loss_and_grad(self, omega, pairs):
+        """Mean loss over pairs (r, e) and dL/domega (3N)."""
+        P = self.prolongator(omega)
+        T0 = self.prolongator(omega, which="T0")
+        Ac = (P.T @ self.A @ P).toarray()
+        Ainv = np.linalg.inv(Ac)
+        L, grad = 0.0, np.zeros(3 * self.N)
+        for r, e in pairs:
+            er = float(e @ r)
+            b = P.T @ r
+            y = Ainv @ b
+            g = r - self.A @ (P @ y)
+            L += (er - b @ y) / er
+            grad += 2.0 * g * (T0 @ y) / er
+        return L / len(pairs), grad / len(pairs)
+
+
+def forward(theta, g, x):
+    """out (N x 3) and the activations for backward."""
     P = unpack(theta)
     N = g.N
-    zs = zs.reshape(N, 3)
-    r = r.reshape(N, 3)
-    gamma = np.sqrt(np.mean(zs ** 2))
-    x = np.concatenate([zs / gamma, (g.s ** 2)[:, None] * r / gamma], axis=1)
     h = x @ P["W_in"].T
-    cache = {"x": x, "gamma": gamma, "h": [h], "m": [], "w": [], "pre_w": []}
+    cache = {"x": x, "h": [h], "m": [], "w": []}
     for l in range(LAYERS):
-        pre_w = g.E @ P["u%d" % l] + P["c%d" % l][0]
-        w = np.tanh(pre_w)
+        w = np.tanh(g.E @ P["u%d" % l] + P["c%d" % l][0])
         m = np.zeros((N, WIDTH))
         np.add.at(m, g.rows, w[:, None] * h[g.cols])
         h = np.tanh(h @ P["Ws%d" % l].T + m @ P["Wm%d" % l].T)
         cache["m"].append(m)
         cache["w"].append(w)
-        cache["pre_w"].append(pre_w)
         cache["h"].append(h)
-    z = zs + gamma * (h @ P["W_out"].T)
-    return z.ravel(), cache
+    return h @ P["W_out"].T, cache
 
 
-def backward(theta, g, cache, dz):
-    """Gradient of a scalar loss with respect to theta, given dL/dz."""
+def omega_of(out):
+    return 1.0 / (1.0 + np.exp(-out))
+
+
+def backward(theta, g, cache, dout):
+    """Gradient of a scalar loss with respect to theta, given dL/dout (N x 3)."""
     P = unpack(theta)
     N = g.N
-    dz = dz.reshape(N, 3)
+    dout = dout.reshape(N, 3)
     grads = {name: np.zeros(shp) for name, shp in param_shapes()}
-    gamma = cache["gamma"]
-    h3 = cache["h"][-1]
-    grads["W_out"] = gamma * dz.T @ h3
-    dh = gamma * dz @ P["W_out"]
+    grads["W_out"] = dout.T @ cache["h"][-1]
+    dh = dout @ P["W_out"]
     for l in reversed(range(LAYERS)):
         h_prev, h_new = cache["h"][l], cache["h"][l + 1]
-        m, w, pre_w = cache["m"][l], cache["w"][l], cache["pre_w"][l]
+        m, w = cache["m"][l], cache["w"][l]
         delta = dh * (1.0 - h_new ** 2)
         grads["Ws%d" % l] = delta.T @ h_prev
         grads["Wm%d" % l] = delta.T @ m
@@ -137,9 +218,10 @@ def backward(theta, g, cache, dz):
     return np.concatenate([grads[name].ravel() for name, _ in param_shapes()])
 
 
-def energy_loss(A, z, e, r):
-    """L = (z-e)^T A (z-e) / (e^T r) and dL/dz."""
-    d = z - e
-    q = A @ d
-    den = float(e @ r)
-    return float(d @ q) / den, 2.0 * q / den
+def loss_and_theta_grad(theta, g, c, pairs):
+    """The whole chain: theta -> omega -> loss, dL/dtheta and omega."""
+    out, cache = forward(theta, g, c.x)
+    om = omega_of(out).ravel()
+    L, dom = c.loss_and_grad(om, pairs)
+    dout = dom * om * (1.0 - om)
+    return L, backward(theta, g, cache, dout), om
