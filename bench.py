@@ -75,6 +75,9 @@ def parse():
                     help="one solve capped at 5 CG iterations, nothing printed (profiling)")
     ap.add_argument("--profile-mode", type=int, default=0,
                     help="precision mode (Iarray(42)) of the --profile-solve solve")
+    ap.add_argument("--profile-coarse", type=int, default=-1,
+                    help="with --profile-solve: the two-level preconditioner with these smoothing weights "
+                         "(Iarray(44): 1 none, 2 one half; no training needed)")
     ap.add_argument("--profile-multi", action="store_true",
                     help="one 16-load-case solve capped at 3 CG iterations, nothing printed (profiling)")
     ap.add_argument("--profile-batch", action="store_true",
@@ -741,6 +744,9 @@ def main():
         mm = m.copy()
         mm.set_iter(5)
         mm.Iarray[41] = args.profile_mode
+        if args.profile_coarse >= 1:
+            mm.Iarray[42] = 1
+            mm.Iarray[43] = args.profile_coarse
         rec = solver.solve(mm)
         if rec["error"] not in (0, 3001):
             raise SystemExit("solve failed: %r" % rec)
