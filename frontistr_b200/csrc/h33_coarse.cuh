@@ -34,6 +34,15 @@ struct CoarseView {
   double *ac;                      // nc x nc, row-major: Ac, then Ac^-1
 };
 
+// FP32 copies of P, A P and Ac^-1 for the application inside a solve (the training
+// and the operator build keep FP64): the correction only shapes the preconditioner,
+// and the copies halve the bytes an application streams.
+struct CoarseApply {
+  int n, nagg, nc;
+  const int *pptr, *pagg, *qptr, *qagg, *rptr, *rnode, *rpos;
+  const float *p, *q, *ainv;
+};
+
 __device__ __forceinline__ double warp_sum_d(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
@@ -432,6 +441,117 @@ __global__ void coarse_prolong_kernel(CoarseView c, const double *__restrict__ y
       if (v) v[3 * i + d] = a[d];
       if (t0y) t0y[3 * i + d] = t[d];
     }
+  }
+}
+
+// bc = P^T r with the FP32 copy of P: one CTA per aggregate (an aggregate's
+// restriction gathers ~1,000 nodes on the 9x9x9 aggregates); per-thread sums in
+// entry order, then a fixed-order CTA sum.
+template <class R>
+__global__ void __launch_bounds__(256) coarse_restrict32_kernel(CoarseApply c, const R *__restrict__ r,
+                                                                double *__restrict__ bc, const CgState *st) {
+  pdl_entry();
+  if (st && (st->done || !st->use_gnn)) return;
+  __shared__ double sh[3][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int a = blockIdx.x; a < c.nagg; a += gridDim.x) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int t = c.rptr[a] + threadIdx.x; t < c.rptr[a + 1]; t += blockDim.x) {
+      const int i = c.rnode[t];
+      const float *p = c.p + 9 * size_t(c.rpos[t]);
+      const double r0 = double(r[3 * i]), r1 = double(r[3 * i + 1]), r2 = double(r[3 * i + 2]);
+      s0 += double(p[0]) * r0 + double(p[3]) * r1 + double(p[6]) * r2;
+      s1 += double(p[1]) * r0 + double(p[4]) * r1 + double(p[7]) * r2;
+      s2 += double(p[2]) * r0 + double(p[5]) * r1 + double(p[8]) * r2;
+    }
+    s0 = warp_sum_d(s0);
+    s1 = warp_sum_d(s1);
+    s2 = warp_sum_d(s2);
+    if (lane == 0) {
+      sh[0][warp] = s0;
+      sh[1][warp] = s1;
+      sh[2][warp] = s2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      double v = 0.0;
+      for (int w = 0; w < int(blockDim.x >> 5); w++) v += sh[threadIdx.x][w];
+      bc[3 * a + threadIdx.x] = v;
+    }
+    __syncthreads();
+  }
+}
+
+// y = Ainv bc with the FP32 copy of Ac^-1, FP64 accumulation (warp per coarse row)
+__global__ void __launch_bounds__(kThreads) coarse_gemv32_kernel(int nc, const float *__restrict__ ainv,
+                                                                 const double *__restrict__ bc, double *__restrict__ y,
+                                                                 const CgState *st) {
+  pdl_entry();
+  if (st && (st->done || !st->use_gnn)) return;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nc; row += nwarps) {
+    const float *a = ainv + size_t(row) * nc;
+    double s = 0.0;
+    for (int k = lane; k < nc; k += 32) s += double(__ldcs(a + k)) * bc[k];
+    s = warp_sum_d(s);
+    if (lane == 0) y[row] = s;
+  }
+}
+
+// The coarse correction inside the two-grid cycle: zc = zs + P y and, in place,
+// w = w - (A P) y with the stored A P (the residual after the correction without a
+// full SpMV: a row of A P has a few blocks, a row of A 27), FP32 copies.  With the
+// correction off zc = zs and w is left alone.
+template <class R>
+__global__ void coarse_prolong_resid32_kernel(CoarseApply c, const double *__restrict__ y, const R *__restrict__ zs,
+                                              R *__restrict__ zc, R *__restrict__ w, const CgState *st) {
+  pdl_entry();
+  if (st && st->done) return;
+  const bool on = !st || st->use_gnn;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
+    double a[3] = {0.0, 0.0, 0.0}, q[3] = {0.0, 0.0, 0.0};
+    if (on) {
+      for (int k = c.pptr[i]; k < c.pptr[i + 1]; k++) {
+        const float *p = c.p + 9 * size_t(k);
+        const int b = c.pagg[k];
+        const double y0 = y[3 * b], y1 = y[3 * b + 1], y2 = y[3 * b + 2];
+        for (int d = 0; d < 3; d++)
+          a[d] += double(p[3 * d]) * y0 + double(p[3 * d + 1]) * y1 + double(p[3 * d + 2]) * y2;
+      }
+      for (int k = c.qptr[i]; k < c.qptr[i + 1]; k++) {
+        const float *qb = c.q + 9 * size_t(k);
+        const int b = c.qagg[k];
+        const double y0 = y[3 * b], y1 = y[3 * b + 1], y2 = y[3 * b + 2];
+        for (int d = 0; d < 3; d++)
+          q[d] += double(qb[3 * d]) * y0 + double(qb[3 * d + 1]) * y1 + double(qb[3 * d + 2]) * y2;
+      }
+    }
+    for (int d = 0; d < 3; d++) {
+      zc[3 * i + d] = R(double(zs[3 * i + d]) + a[d]);
+      if (on) w[3 * i + d] = R(double(w[3 * i + d]) - q[d]);
+    }
+  }
+}
+
+// z = zs + P y with the FP32 copy of P (the additive form); z = zs once off.
+template <class R>
+__global__ void coarse_prolong32_kernel(CoarseApply c, const double *__restrict__ y, const R *__restrict__ zs,
+                                        R *__restrict__ z, const CgState *st) {
+  pdl_entry();
+  if (st && st->done) return;
+  const bool on = !st || st->use_gnn;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
+    double a[3] = {0.0, 0.0, 0.0};
+    if (on)
+      for (int k = c.pptr[i]; k < c.pptr[i + 1]; k++) {
+        const float *p = c.p + 9 * size_t(k);
+        const int b = c.pagg[k];
+        const double y0 = y[3 * b], y1 = y[3 * b + 1], y2 = y[3 * b + 2];
+        for (int d = 0; d < 3; d++)
+          a[d] += double(p[3 * d]) * y0 + double(p[3 * d + 1]) * y1 + double(p[3 * d + 2]) * y2;
+      }
+    for (int d = 0; d < 3; d++) z[3 * i + d] = R(double(zs[3 * i + d]) + a[d]);
   }
 }
 

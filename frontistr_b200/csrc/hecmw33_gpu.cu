@@ -283,9 +283,14 @@ struct Learned {
     DevArray<int> agg, pptr, pagg, rptr, rnode, rpos, qptr, qagg, cptr, cagg, uptr, ucol, usrc;
     DevArray<float> mask, x, out, omega, dout;
     DevArray<double> t0, p, q, ac, gjc, gjd, bc, y, v, t0y, apy, dots;
+    DevArray<float> p32, q32, ainv32;  // FP32 copies for the application in a solve
     DevArray<int> err;
     float *one = nullptr;  // device 1.0f (the decode scale of the backward pass)
     DevArray<float> one_buf;
+    CoarseApply apply_view() {
+      return CoarseApply{n, nagg, nc, pptr.p, pagg.p, qptr.p, qagg.p, rptr.p, rnode.p, rpos.p,
+                         p32.p, q32.p, ainv32.p};
+    }
     CoarseView view() {
       return CoarseView{n,      nagg,   nc,     agg.p,  pptr.p, pagg.p, rptr.p, rnode.p, rpos.p,
                         qptr.p, qagg.p, cptr.p, cagg.p, uptr.p, ucol.p, usrc.p, mask.p,  t0.p,
@@ -1156,6 +1161,11 @@ void ensure_bicg(Solver &S) {
 template <class R>
 void launch_coarse(Solver &S, const R *zs, const R *r, R *z, CgState *st);
 
+// The coarse correction inside the two-grid cycle: zc = zs + P Ac^-1 P^T w and
+// w -= A P Ac^-1 P^T w (defined with the coarse space below).
+template <class R>
+void launch_coarse_cycle(Solver &S, const R *zs, R *w, R *zc, CgState *st);
+
 // HECMW33_COARSE_FORM: 0 (default) the symmetric two-grid form, 1 the additive form.
 // Measured on the 100^3 cube (BF16-stored SSOR, omega = 1/2): two-grid 62 iterations,
 // additive 115; the two-grid form is the one whose convergence the training loss
@@ -1185,7 +1195,8 @@ void precond_resid(Solver &S, const Views<R> &V, const R *x, R *y) {
 
 // The learned two-level preconditioner z = M^-1 r.  Symmetric two-grid form:
 //   zs = SSOR(r);  zc = zs + P Ac^-1 P^T (r - A zs);  z = zc + SSOR(r - A zc)
-// (pre-smoothing, coarse correction, post-smoothing: symmetric because SSOR is);
+// (pre-smoothing, coarse correction, post-smoothing: symmetric because SSOR is); the
+// residual r - A zc comes from r - A zs less (A P) y with the stored A P;
 // additive form: z = SSOR(r) + P Ac^-1 P^T r.  With the correction off (fallback)
 // z = SSOR(r).
 template <class R>
@@ -1197,8 +1208,7 @@ void launch_learned_precond(Solver &S, const Views<R> &V, CgState *st) {
     return;
   }
   precond_resid<R>(S, V, V.zs, V.w);
-  launch_coarse<R>(S, V.zs, V.w, V.zp, st);
-  precond_resid<R>(S, V, V.zp, V.w);
+  launch_coarse_cycle<R>(S, V.zs, V.w, V.zp, st);  // zp = zc, w = r - A zc
   launch_sweep<R, false>(S, V, V.w, V.z, st);
   launch_k(s, coarse_post_kernel<R>, S.grid_vec(), kThreads, static_cast<const R *>(V.zp),
            static_cast<const R *>(V.zs), V.z, S.n3(), static_cast<const CgState *>(st));
@@ -1662,6 +1672,15 @@ bool coarse_operator(Solver &S, const float *omega) {
     gj_update_kernel<<<dim3(unsigned(tiles), unsigned(tiles)), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjc.p);
     gj_col_kernel<<<std::max(1, (n + 255) / 256), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjc.p, C.gjd.p);
   }
+  // FP32 copies for the application
+  auto conv = [&](const DevArray<double> &a, DevArray<float> &b) {
+    b.alloc(a.n);
+    const int grid = int(std::min<size_t>((a.n + kThreads - 1) / kThreads, size_t(S.nsm) * 16));
+    launch_k(s, convert_kernel<float>, std::max(grid, 1), kThreads, static_cast<const double *>(a.p), b.p, a.n);
+  };
+  conv(C.p, C.p32);
+  conv(C.q, C.q32);
+  conv(C.ac, C.ainv32);
   H33_CUDA(cudaGetLastError());
   int err = 0;
   H33_CUDA(cudaMemcpyAsync(&err, C.err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1671,19 +1690,35 @@ bool coarse_operator(Solver &S, const float *omega) {
 }
 
 // z = zs + P Ac^-1 P^T r (or z = zs when the correction is off), in the solve's stream.
+// z = zs + P Ac^-1 P^T r (additive form), with the FP32 copies.
 template <class R>
 void launch_coarse(Solver &S, const R *zs, const R *r, R *z, CgState *st) {
   auto &C = S.L.C;
   cudaStream_t s = S.stream;
-  const CoarseView cv = C.view();
+  const CoarseApply ca = C.apply_view();
   const int gt = std::max(1, std::min((S.N + kThreads - 1) / kThreads, S.nsm * 8));
-  launch_k(s, coarse_restrict_kernel<R>, std::max(1, std::min((C.nagg + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8)),
-           kThreads, cv, r, C.bc.p, static_cast<const CgState *>(st));
-  launch_k(s, coarse_gemv_kernel, std::max(1, std::min((C.nc + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8)),
-           kThreads, C.nc, static_cast<const double *>(C.ac.p), static_cast<const double *>(C.bc.p), C.y.p,
+  launch_k(s, coarse_restrict32_kernel<R>, std::max(1, C.nagg), 256, ca, r, C.bc.p,
            static_cast<const CgState *>(st));
-  launch_k(s, coarse_prolong_kernel<R>, gt, kThreads, cv, static_cast<const double *>(C.y.p), zs, z,
-           static_cast<double *>(nullptr), static_cast<double *>(nullptr), static_cast<const CgState *>(st));
+  launch_k(s, coarse_gemv32_kernel, std::max(1, std::min((C.nc + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8)),
+           kThreads, C.nc, static_cast<const float *>(C.ainv32.p), static_cast<const double *>(C.bc.p), C.y.p,
+           static_cast<const CgState *>(st));
+  launch_k(s, coarse_prolong32_kernel<R>, gt, kThreads, ca, static_cast<const double *>(C.y.p), zs, z,
+           static_cast<const CgState *>(st));
+}
+
+template <class R>
+void launch_coarse_cycle(Solver &S, const R *zs, R *w, R *zc, CgState *st) {
+  auto &C = S.L.C;
+  cudaStream_t s = S.stream;
+  const CoarseApply ca = C.apply_view();
+  const int gt = std::max(1, std::min((S.N + kThreads - 1) / kThreads, S.nsm * 8));
+  launch_k(s, coarse_restrict32_kernel<R>, std::max(1, C.nagg), 256, ca, static_cast<const R *>(w), C.bc.p,
+           static_cast<const CgState *>(st));
+  launch_k(s, coarse_gemv32_kernel, std::max(1, std::min((C.nc + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8)),
+           kThreads, C.nc, static_cast<const float *>(C.ainv32.p), static_cast<const double *>(C.bc.p), C.y.p,
+           static_cast<const CgState *>(st));
+  launch_k(s, coarse_prolong_resid32_kernel<R>, gt, kThreads, ca, static_cast<const double *>(C.y.p), zs, zc, w,
+           static_cast<const CgState *>(st));
 }
 
 void learned_set_weights(Solver &S, const float *theta_host, bool reset_adam) {
