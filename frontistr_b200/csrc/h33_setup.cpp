@@ -746,140 +746,196 @@ void level_schedule(const Profile &p, bool lower, std::vector<int> &order,
 
 namespace {
 
-// Symmetric adjacency (no self loops) of a graph given by CSR rows with possibly
-// repeated entries: sorted and unique per row.
-void sym_unique(int n, std::vector<std::vector<int>> &adj) {
-  for (int i = 0; i < n; i++) {
-    auto &a = adj[size_t(i)];
-    std::sort(a.begin(), a.end());
-    a.erase(std::unique(a.begin(), a.end()), a.end());
-  }
-}
+// Compressed adjacency lists (row r: col[ptr[r] .. ptr[r+1]), ascending, no self).
+struct Csr {
+  std::vector<int64_t> ptr;
+  std::vector<int> col;
+  int n() const { return int(ptr.size()) - 1; }
+};
 
-// One greedy distance-1 aggregation pass over a graph (adjacency lists, no self).
-int aggregate_pass(int n, const std::vector<std::vector<int>> &adj, std::vector<int> &agg) {
+// One greedy distance-1 aggregation pass.
+int aggregate_pass(const Csr &g, std::vector<int> &agg) {
+  const int n = g.n();
   agg.assign(size_t(n), -1);
   int na = 0;
   for (int i = 0; i < n; i++) {
     if (agg[size_t(i)] >= 0) continue;
     bool free_nbhd = true;
-    for (int j : adj[size_t(i)])
-      if (agg[size_t(j)] >= 0) {
+    for (int64_t k = g.ptr[size_t(i)]; k < g.ptr[size_t(i) + 1]; k++)
+      if (agg[size_t(g.col[size_t(k)])] >= 0) {
         free_nbhd = false;
         break;
       }
     if (!free_nbhd) continue;
     agg[size_t(i)] = na;
-    for (int j : adj[size_t(i)]) agg[size_t(j)] = na;
+    for (int64_t k = g.ptr[size_t(i)]; k < g.ptr[size_t(i) + 1]; k++) agg[size_t(g.col[size_t(k)])] = na;
     na++;
   }
   std::vector<int> root_agg(agg);  // the aggregates the roots formed
   for (int i = 0; i < n; i++) {
     if (agg[size_t(i)] >= 0) continue;
-    for (int j : adj[size_t(i)])
-      if (root_agg[size_t(j)] >= 0) {
-        agg[size_t(i)] = root_agg[size_t(j)];
+    for (int64_t k = g.ptr[size_t(i)]; k < g.ptr[size_t(i) + 1]; k++)
+      if (root_agg[size_t(g.col[size_t(k)])] >= 0) {
+        agg[size_t(i)] = root_agg[size_t(g.col[size_t(k)])];
         break;
       }
-    if (agg[size_t(i)] < 0) agg[size_t(i)] = na++;  // unreachable for a connected graph; kept safe
+    if (agg[size_t(i)] < 0) agg[size_t(i)] = na++;  // no aggregated neighbour (isolated node)
   }
   return na;
+}
+
+// The graph of aggregates: a ~ b when a node of a neighbours a node of b.
+Csr coarse_graph(const Csr &g, const std::vector<int> &a, int na) {
+  const int n = g.n();
+  std::vector<int64_t> mptr(size_t(na) + 1, 0);
+  for (int u = 0; u < n; u++) mptr[size_t(a[size_t(u)]) + 1]++;
+  for (int c = 0; c < na; c++) mptr[size_t(c) + 1] += mptr[size_t(c)];
+  std::vector<int> members(static_cast<size_t>(n));
+  {
+    std::vector<int64_t> fill(mptr.begin(), mptr.end() - 1);
+    for (int u = 0; u < n; u++) members[size_t(fill[size_t(a[size_t(u)])]++)] = u;
+  }
+  Csr h;
+  h.ptr.assign(size_t(na) + 1, 0);
+  std::vector<int> mark(size_t(na), -1);
+  for (int c = 0; c < na; c++) {
+    for (int64_t m = mptr[size_t(c)]; m < mptr[size_t(c) + 1]; m++) {
+      const int u = members[size_t(m)];
+      for (int64_t k = g.ptr[size_t(u)]; k < g.ptr[size_t(u) + 1]; k++) {
+        const int b = a[size_t(g.col[size_t(k)])];
+        if (b != c && mark[size_t(b)] != c) {
+          mark[size_t(b)] = c;
+          h.col.push_back(b);
+        }
+      }
+    }
+    h.ptr[size_t(c) + 1] = int64_t(h.col.size());
+  }
+  for (int c = 0; c < na; c++) std::sort(h.col.begin() + h.ptr[size_t(c)], h.col.begin() + h.ptr[size_t(c) + 1]);
+  return h;
+}
+
+// For every row r: the sorted union of the values lists[q] (each in 0 .. nvals-1) over
+// q in items(r); distinct values found with a marker array per thread; two passes
+// (count, fill), rows in parallel.
+template <class Items, class Lists>
+void row_unions(int nrows, int nvals, Items items, Lists lists, std::vector<int> &ptr, std::vector<int> &out) {
+  std::vector<int> cnt(size_t(nrows) + 1, 0);
+  ptr.assign(size_t(nrows) + 1, 0);
+  for (int pass = 0; pass < 2; pass++) {
+#pragma omp parallel
+    {
+      std::vector<int> tmp, mark(size_t(nvals), -1);
+#pragma omp for schedule(dynamic, 1024)
+      for (int r = 0; r < nrows; r++) {
+        tmp.clear();
+        items(r, [&](int q) {
+          lists(q, [&](int v) {
+            if (mark[size_t(v)] != r) {
+              mark[size_t(v)] = r;
+              tmp.push_back(v);
+            }
+          });
+        });
+        if (pass == 0) {
+          cnt[size_t(r) + 1] = int(tmp.size());
+        } else {
+          std::sort(tmp.begin(), tmp.end());
+          std::copy(tmp.begin(), tmp.end(), out.begin() + ptr[size_t(r)]);
+        }
+      }
+    }
+    if (pass == 0) {
+      for (int r = 0; r < nrows; r++) ptr[size_t(r) + 1] = ptr[size_t(r)] + cnt[size_t(r) + 1];
+      out.assign(size_t(ptr[size_t(nrows)]), 0);
+    }
+  }
 }
 
 }  // namespace
 
 void aggregate_nodes(const Profile &p, int max_aggregates, Aggregation &out) {
   const int N = p.N;
-  std::vector<std::vector<int>> adj(static_cast<size_t>(N));
+  // the node graph: row i's own neighbours (its L and U items, ascending; the blocks
+  // the device kernels read for row i), in-range and not i
+  Csr adj;
+  adj.ptr.assign(size_t(N) + 1, 0);
+  auto keep = [&](int i, int c) { return c >= 0 && c < N && c != i; };
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < N; i++) {
-    for (int j = p.indexL[i]; j < p.indexL[i + 1]; j++) {
-      const int c = p.itemL[j] - 1;
-      if (c >= 0 && c < N && c != i) {
-        adj[size_t(i)].push_back(c);
-        adj[size_t(c)].push_back(i);
-      }
-    }
-    for (int j = p.indexU[i]; j < p.indexU[i + 1]; j++) {
-      const int c = p.itemU[j] - 1;
-      if (c >= 0 && c < N && c != i) {
-        adj[size_t(i)].push_back(c);
-        adj[size_t(c)].push_back(i);
-      }
-    }
+    int64_t k = 0;
+    for (int j = p.indexL[i]; j < p.indexL[i + 1]; j++) k += keep(i, p.itemL[j] - 1);
+    for (int j = p.indexU[i]; j < p.indexU[i + 1]; j++) k += keep(i, p.itemU[j] - 1);
+    adj.ptr[size_t(i) + 1] = k;
   }
-  sym_unique(N, adj);
+  for (int i = 0; i < N; i++) adj.ptr[size_t(i) + 1] += adj.ptr[size_t(i)];
+  adj.col.assign(size_t(adj.ptr[size_t(N)]), 0);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < N; i++) {
+    int64_t w = adj.ptr[size_t(i)];
+    for (int j = p.indexL[i]; j < p.indexL[i + 1]; j++)
+      if (keep(i, p.itemL[j] - 1)) adj.col[size_t(w++)] = p.itemL[j] - 1;
+    for (int j = p.indexU[i]; j < p.indexU[i + 1]; j++)
+      if (keep(i, p.itemU[j] - 1)) adj.col[size_t(w++)] = p.itemU[j] - 1;
+  }
   std::vector<int> agg(static_cast<size_t>(N));
   for (int i = 0; i < N; i++) agg[size_t(i)] = i;
   int n = N;
-  std::vector<std::vector<int>> g = adj;
+  Csr g = adj;
   for (int pass = 0; pass == 0 || n > max_aggregates; pass++) {
     std::vector<int> a;
-    const int na = aggregate_pass(n, g, a);
+    const int na = aggregate_pass(g, a);
     if (2 * na > n) break;  // no longer coarsening
     for (int i = 0; i < N; i++) agg[size_t(i)] = a[size_t(agg[size_t(i)])];
-    std::vector<std::vector<int>> h(static_cast<size_t>(na));
-    for (int u = 0; u < n; u++)
-      for (int v : g[size_t(u)])
-        if (a[size_t(u)] != a[size_t(v)]) h[size_t(a[size_t(u)])].push_back(a[size_t(v)]);
-    sym_unique(na, h);
-    g.swap(h);
+    g = coarse_graph(g, a, na);
     n = na;
   }
   out.n_agg = n;
   out.agg = agg;
   // prolongator pattern: aggregates of each closed neighbourhood
-  out.pptr.assign(size_t(N) + 1, 0);
-  out.pagg.clear();
-  std::vector<int> tmp;
-  for (int i = 0; i < N; i++) {
-    tmp.clear();
-    tmp.push_back(agg[size_t(i)]);
-    for (int j : adj[size_t(i)]) tmp.push_back(agg[size_t(j)]);
-    std::sort(tmp.begin(), tmp.end());
-    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-    out.pagg.insert(out.pagg.end(), tmp.begin(), tmp.end());
-    out.pptr[size_t(i) + 1] = int(out.pagg.size());
-  }
-  // two-ring pattern (rows of A P)
-  out.qptr.assign(size_t(N) + 1, 0);
-  out.qagg.clear();
-  for (int i = 0; i < N; i++) {
-    tmp.clear();
-    for (int q = out.pptr[size_t(i)]; q < out.pptr[size_t(i) + 1]; q++) tmp.push_back(out.pagg[size_t(q)]);
-    for (int j : adj[size_t(i)])
-      for (int q = out.pptr[size_t(j)]; q < out.pptr[size_t(j) + 1]; q++) tmp.push_back(out.pagg[size_t(q)]);
-    std::sort(tmp.begin(), tmp.end());
-    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-    out.qagg.insert(out.qagg.end(), tmp.begin(), tmp.end());
-    out.qptr[size_t(i) + 1] = int(out.qagg.size());
-  }
+  row_unions(
+      N, n,
+      [&](int i, auto f) {
+        f(i);
+        for (int64_t k = adj.ptr[size_t(i)]; k < adj.ptr[size_t(i) + 1]; k++) f(adj.col[size_t(k)]);
+      },
+      [&](int j, auto f) { f(agg[size_t(j)]); }, out.pptr, out.pagg);
+  // two-ring pattern (rows of A P): the union of the neighbours' prolongator patterns
+  row_unions(
+      N, n,
+      [&](int i, auto f) {
+        f(i);
+        for (int64_t k = adj.ptr[size_t(i)]; k < adj.ptr[size_t(i) + 1]; k++) f(adj.col[size_t(k)]);
+      },
+      [&](int j, auto f) {
+        for (int q = out.pptr[size_t(j)]; q < out.pptr[size_t(j) + 1]; q++) f(out.pagg[size_t(q)]);
+      },
+      out.qptr, out.qagg);
   // restriction gather: per aggregate its (node, entry) pairs, ascending node
   out.rptr.assign(size_t(n) + 1, 0);
   for (int a : out.pagg) out.rptr[size_t(a) + 1]++;
   for (int a = 0; a < n; a++) out.rptr[size_t(a) + 1] += out.rptr[size_t(a)];
   out.rnode.assign(out.pagg.size(), 0);
   out.rpos.assign(out.pagg.size(), 0);
-  std::vector<int> fill(out.rptr.begin(), out.rptr.end() - 1);
-  for (int i = 0; i < N; i++)
-    for (int q = out.pptr[size_t(i)]; q < out.pptr[size_t(i) + 1]; q++) {
-      const int a = out.pagg[size_t(q)];
-      out.rnode[size_t(fill[size_t(a)])] = i;
-      out.rpos[size_t(fill[size_t(a)]++)] = q;
-    }
-  // coarse pattern: row a = union of the two-ring patterns of a's restriction nodes
-  out.cptr.assign(size_t(n) + 1, 0);
-  out.cagg.clear();
-  for (int a = 0; a < n; a++) {
-    tmp.clear();
-    for (int t = out.rptr[size_t(a)]; t < out.rptr[size_t(a) + 1]; t++) {
-      const int i = out.rnode[size_t(t)];
-      for (int q = out.qptr[size_t(i)]; q < out.qptr[size_t(i) + 1]; q++) tmp.push_back(out.qagg[size_t(q)]);
-    }
-    std::sort(tmp.begin(), tmp.end());
-    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-    out.cagg.insert(out.cagg.end(), tmp.begin(), tmp.end());
-    out.cptr[size_t(a) + 1] = int(out.cagg.size());
+  {
+    std::vector<int> fill(out.rptr.begin(), out.rptr.end() - 1);
+    for (int i = 0; i < N; i++)
+      for (int q = out.pptr[size_t(i)]; q < out.pptr[size_t(i) + 1]; q++) {
+        const int a = out.pagg[size_t(q)];
+        out.rnode[size_t(fill[size_t(a)])] = i;
+        out.rpos[size_t(fill[size_t(a)]++)] = q;
+      }
   }
+  // coarse pattern: row a = union of the two-ring patterns of a's restriction nodes
+  row_unions(
+      n, n,
+      [&](int a, auto f) {
+        for (int t = out.rptr[size_t(a)]; t < out.rptr[size_t(a) + 1]; t++) f(out.rnode[size_t(t)]);
+      },
+      [&](int i, auto f) {
+        for (int q = out.qptr[size_t(i)]; q < out.qptr[size_t(i) + 1]; q++) f(out.qagg[size_t(q)]);
+      },
+      out.cptr, out.cagg);
 }
 
 }  // namespace h33
