@@ -167,11 +167,14 @@ int ordering_mc(const Profile &p, const std::vector<int> &perm_cur, int ncolor_i
   std::vector<int> mark(N, 0);           // >0 colour, -1 neighbour of this colour
   perm.assign(N, 0);
   colorindex.assign(1, 0);
+  // the nodes not yet coloured, in perm_cur order: every colour scans them from the
+  // start as the reference scans perm_cur (coloured nodes, which it skips, are left
+  // out), so the same nodes are taken in the same order
+  std::vector<int> rest(perm_cur.begin(), perm_cur.end());
   int done = 0, ncolor = 0;
   for (int colour = 1; colour <= N; colour++) {
     int taken = 0;
-    for (int i = 0; i < N; i++) {
-      const int node = perm_cur[i];
+    for (const int node : rest) {
       if (mark[node] != 0) continue;
       mark[node] = colour;
       perm[done++] = node;
@@ -192,8 +195,14 @@ int ordering_mc(const Profile &p, const std::vector<int> &perm_cur, int ncolor_i
       ncolor = colour;
       break;
     }
-    for (int i = 0; i < N; i++)
-      if (mark[i] == -1) mark[i] = 0;
+    // only uncoloured nodes carry -1 marks: clear them and drop the coloured ones
+    size_t w = 0;
+    for (const int node : rest) {
+      if (mark[node] > 0) continue;
+      mark[node] = 0;
+      rest[w++] = node;
+    }
+    rest.resize(w);
   }
   iperm.assign(N, 0);
   for (int i = 0; i < N; i++) iperm[perm[i]] = i;
@@ -230,6 +239,7 @@ void reordered_rows(const Profile &p, const std::vector<int> &perm, const std::v
   lower.ptr.assign(size_t(N) + 1, 0);
   upper.ptr.assign(size_t(N) + 1, 0);
   // counts per new row
+#pragma omp parallel for schedule(static)
   for (int inew = 0; inew < N; inew++) {
     const int iold = perm[inew];
     int nl = 0, nu = 0;
@@ -239,8 +249,12 @@ void reordered_rows(const Profile &p, const std::vector<int> &perm, const std::v
       if (p.itemU[j] > N) continue;
       (iperm[p.itemU[j] - 1] < inew ? nl : nu)++;
     }
-    lower.ptr[inew + 1] = lower.ptr[inew] + nl;
-    upper.ptr[inew + 1] = upper.ptr[inew] + nu;
+    lower.ptr[inew + 1] = nl;
+    upper.ptr[inew + 1] = nu;
+  }
+  for (int inew = 0; inew < N; inew++) {
+    lower.ptr[inew + 1] += lower.ptr[inew];
+    upper.ptr[inew + 1] += upper.ptr[inew];
   }
   lower.col.resize(size_t(lower.ptr[N]));
   lower.src.resize(size_t(lower.ptr[N]));
@@ -452,13 +466,25 @@ void order_rows_by_length(const BlockRows &lower, const BlockRows &upper, const 
                           int lanes, std::vector<int> &order) {
   const int n = int(lower.ptr.size()) - 1;
   order.resize(size_t(n));
-  for (int i = 0; i < n; i++) order[size_t(i)] = i;
   auto cls = [lanes](const BlockRows &br, int r) { return int((br.ptr[r + 1] - br.ptr[r] + lanes - 1) / lanes); };
-  for (size_t g = 0; g + 1 < group_rows.size(); g++)
-    std::stable_sort(order.begin() + group_rows[g], order.begin() + group_rows[g + 1], [&](int a, int b) {
-      const int la = cls(lower, a), lb = cls(lower, b);
-      return la != lb ? la < lb : cls(upper, a) < cls(upper, b);
-    });
+  int maxu = 0;
+  for (int r = 0; r < n; r++) maxu = std::max(maxu, cls(upper, r));
+  // a stable counting sort of each group by the key (lower slots, upper slots)
+  const int ng = int(group_rows.size()) - 1;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int g = 0; g < ng; g++) {
+    const int r0 = group_rows[size_t(g)], r1 = group_rows[size_t(g) + 1];
+    std::vector<int> key(size_t(r1 - r0));
+    int kmax = 0;
+    for (int r = r0; r < r1; r++) {
+      key[size_t(r - r0)] = cls(lower, r) * (maxu + 1) + cls(upper, r);
+      kmax = std::max(kmax, key[size_t(r - r0)]);
+    }
+    std::vector<int> start(size_t(kmax) + 2, 0);
+    for (int k : key) start[size_t(k) + 1]++;
+    for (int k = 0; k <= kmax; k++) start[size_t(k) + 1] += start[size_t(k)];
+    for (int r = r0; r < r1; r++) order[size_t(r0 + start[size_t(key[size_t(r - r0)])]++)] = r;
+  }
 }
 
 void permute_rows(const BlockRows &in, const std::vector<int> &order, const std::vector<int> &iorder,
