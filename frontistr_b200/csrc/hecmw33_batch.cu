@@ -611,15 +611,13 @@ void store_x(Batch &B, double *X, bool device) {
 
 // Autotune on the caller's B/X: one warm solve (it sets the per-system iteration
 // counts that order the queues), then one timed solve per schedule, each from the
-// same X (X itself is not modified); the fastest is kept.  Coordinate search:
-// cluster size and team share at the current lanes, then the lanes at the best of
-// those.  Layout rebuilds and graph captures happen outside the timed region.
+// same X (X itself is not modified); the fastest is kept.  Coordinate search: the
+// cluster size with every system given to teams, the team share at the best size,
+// then the lanes at the best of those (9 timed solves; the full grid of sizes and
+// shares took 13).  Layout rebuilds and graph captures happen outside the timed
+// region.
 double autotune(Batch &B, const Flags &f, const double *Bv, const double *X, bool device) {
-  std::vector<Schedule> cands;
   const int L0 = B.sched.lanes;
-  cands.push_back(Schedule{L0, 1, 0.0});
-  for (int c : {2, 4, 8})
-    for (double bf : {0.1, 0.25, 0.5, 1.0}) cands.push_back(Schedule{L0, c, bf});
   auto note_iters = [&]() {
     for (int s = 0; s < B.nsys; s++)
       if (!B.sys_h[s].skip) B.last_iter[s] = B.h_out[s].iter;
@@ -637,7 +635,12 @@ double autotune(Batch &B, const Flags &f, const double *Bv, const double *X, boo
       best = sc;
     }
   };
-  for (const Schedule &sc : cands) trial(sc);
+  trial(Schedule{L0, 1, 0.0});
+  for (int c : {2, 4, 8}) trial(Schedule{L0, c, 1.0});
+  if (best.cluster > 1) {
+    const int c = best.cluster;
+    for (double bf : {0.1, 0.25, 0.5}) trial(Schedule{L0, c, bf});
+  }
   for (int L : {4, 8, 16}) {
     if (L == L0) continue;
     Schedule sc = best;
