@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--no-config3", action="store_true",
                     help="skip the mixed-precision measurement on the jittered heterogeneous 80^3 system")
     ap.add_argument("--no-ilu0", action="store_true", help="skip the CG + ILU(0) measurement")
+    ap.add_argument("--no-newton", action="store_true",
+                    help="skip the learned preconditioner's Neo-Hookean Newton sequence (--learned-newton alone)")
     ap.add_argument("--batch-systems", type=int, default=256)
     ap.add_argument("--batch-edges", default="8,40", help="element range per box edge of the batch")
     ap.add_argument("--spmv-only", type=int, default=0,
@@ -948,6 +950,12 @@ def main():
     assembly = None if args.no_assembly else bench_assembly()
     batched = None if args.no_batched else bench_batched(args)
     domains = None if args.no_domains else bench_domains(m, solver)
+    newton = None
+    if not (args.no_newton or args.no_learned or world > 1):
+        # the learned preconditioner in the Newton sequence of the 64^3 Neo-Hookean block
+        newton = bench_learned_newton(args)
+        newton.pop("systems", None)
+        newton.pop("impl", None)
 
     ilu0 = None if (args.no_ilu0 or world > 1) else bench_ilu0(m, args, peak)
 
@@ -1013,6 +1021,7 @@ def main():
             "assembly": assembly,
             "batched": batched,
             "domains": domains,
+            "learned_newton": newton,
         }
         print(json.dumps(line))
     solver.close()
