@@ -238,6 +238,15 @@ __global__ void __launch_bounds__(kThreads) coarse_ac_kernel(CoarseView c) {
   }
 }
 
+// A coarse DOF whose basis vector is zero (every DOF of that direction in the
+// aggregate constrained) has a zero row and column in Ac (p^T A p = 0 only for p = 0,
+// A being SPD): its diagonal is set to 1, so that Ac stays invertible and the DOF's
+// correction, from a zero restriction, stays zero.
+__global__ void coarse_zero_diag_kernel(double *__restrict__ ac, int nc) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x)
+    if (ac[size_t(k) * nc + k] == 0.0) ac[size_t(k) * nc + k] = 1.0;
+}
+
 // ---- in-place inversion of the SPD coarse matrix: blocked Gauss-Jordan ----------
 // For each block K of kGjBlock pivots (no pivoting: Ac is SPD):
 //   Dinv = M_KK^-1;  C = M_:K (saved);  M_Kj = Dinv M_Kj (j not in K);

@@ -1662,6 +1662,7 @@ bool coarse_operator(Solver &S, const float *omega) {
   C.ac.zero(s);
   C.err.zero(s);
   launch_k(s, coarse_ac_kernel, std::max(1, S.nsm * 8), kThreads, cv);
+  coarse_zero_diag_kernel<<<std::max(1, (C.nc + 255) / 256), 256, 0, s>>>(C.ac.p, C.nc);
   const int n = C.nc;
   const int tiles = (n + 63) / 64;
   for (int k0 = 0; k0 < n; k0 += kGjBlock) {

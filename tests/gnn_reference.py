@@ -159,6 +159,8 @@ class Coarse:
         P = self.prolongator(omega)
         T0 = self.prolongator(omega, which="T0")
         Ac = (P.T @ self.A @ P).toarray()
+        zero = np.diag(Ac) == 0.0  # a zero basis vector (its DOFs all constrained)
+        Ac[zero, zero] = 1.0
         Ainv = np.linalg.inv(Ac)
         L, grad = 0.0, np.zeros(3 * self.N)
         for r, e in pairs:
