@@ -121,3 +121,27 @@ def test_training_gain_and_mixed():
         g, info, rec = _solve(s, mm, learned=1)
         assert info["error"] == 0
         assert Oracle(mm).rel_resid(g.X, mm.B) <= 1e-8
+
+
+def test_fixed_weights_need_no_training_and_errors():
+    """Iarray(44) = 1 / 2 (no smoothing / omega = 1/2) run without a trained network;
+    the network's weights without training, and the two-level preconditioner around a
+    preconditioner other than SSOR, are refused with 1001 as the reference refuses an
+    inconsistent PRECOND."""
+    from frontistr_b200.solver import HecmwSolverError
+    m = box_system(8, 8, 16, jitter=0.1, seed=5)
+    with GpuSolver() as s:
+        _, info_plain, _ = _solve(s, m)
+        for coarse in (1, 2):
+            g, info, rec = _solve(s, m, learned=1, coarse=coarse)
+            assert info["error"] == 0 and rec["learned"] == 1
+            assert info["iter"] < info_plain["iter"]
+            assert Oracle(m).rel_resid(g.X, m.B) <= 1e-8
+        with pytest.raises(HecmwSolverError) as e:
+            _solve(s, m, learned=1, coarse=0)
+        assert e.value.code == 1001
+        d = m.copy()
+        d.set_precond(3)
+        with pytest.raises(HecmwSolverError) as e:
+            _solve(s, d, learned=1, coarse=2)
+        assert e.value.code == 1001
