@@ -14,8 +14,9 @@ public dataset).  One step = one solve to relative residual 1e-8 with CG + SSOR
                (hecmw33_gpu_solve: matrix values + B + X uploaded, numeric
                preconditioner rebuild, solve, X downloaded), wall clock
   roofline     the dominant kernel of the headline solve, one SSOR application (the
-               forward + backward colour sweeps), against measured HBM bandwidth;
-               roofline_spmv the plain FP64 SpMV (spmv_kernel)
+               forward + backward colour sweeps; for the learned variants the two-grid
+               cycle's smoother, the same SSOR in first-fit colour order), against
+               measured HBM bandwidth; roofline_spmv the plain FP64 SpMV (spmv_kernel)
   cpu_baseline the CPU oracle (C restatement of the reference's CG + SSOR,
                OpenMP over all host cores) solving the same system to the same
                tolerance, measured (setup reported separately)
@@ -654,14 +655,26 @@ def bench_batched(args):
 
 def roofline_sweeps(sweeps, head, peak, peak_kind, tag):
     """The roofline object for one SSOR application (forward + backward colour
-    sweeps), in the storage of the headline variant."""
-    key = "bf16" if (head.endswith("mixed") and "bf16" in sweeps) else "fp64"
+    sweeps), in the storage of the headline variant; the learned variants apply the
+    two-grid cycle's smoother (the same SSOR on its own layouts, first-fit colours)."""
+    store = "bf16" if head.endswith("mixed") else "fp64"
+    smoother = head.startswith("learned") and ("smoother_" + store) in sweeps
+    key = ("smoother_" if smoother else "") + store
+    if key not in sweeps:
+        key = "fp64"
+        store = "fp64"
     sw = sweeps[key]
-    return {"bound": "hbm",
-            "kernel": "sweep_fwd_uni_kernel + sweep_bwd_uni_kernel: one SSOR application, all colours, %s"
-                      % ("BF16-stored values, FP32 diagonal LU" if key == "bf16" else "FP64"),
+    what = "BF16-stored values, FP32 diagonal LU" if store == "bf16" else "FP64"
+    if smoother:
+        kernel = ("sweep_fwd_uni_kernel + sweep_bwd_uni_kernel: one application of the learned preconditioner's "
+                  "SSOR smoother (first-fit colour order), all colours, %s" % what)
+        prof = "ssor_smoother_sweeps_%s.txt" % tag
+    else:
+        kernel = "sweep_fwd_uni_kernel + sweep_bwd_uni_kernel: one SSOR application, all colours, %s" % what
+        prof = "ssor_sweeps_%s.txt" % tag
+    return {"bound": "hbm", "kernel": kernel,
             "achieved": sw["achieved"], "peak": peak, "unit": "GB/s", "frac": sw["frac"], "peak_kind": peak_kind,
-            "traffic": traffic_from_profile("ssor_sweeps_%s.txt" % tag, "dram_bytes_per_apply_%s" % key),
+            "traffic": traffic_from_profile(prof, "dram_bytes_per_apply_%s" % store),
             "algorithmic_bytes": sw["algorithmic_bytes"], "ms_per_apply": sw["ms_per_apply"]}
 
 
@@ -897,10 +910,11 @@ def main():
     # the dominant kernels of an iteration: one preconditioner application (SSOR: the
     # forward + backward colour sweeps), FP64 and BF16-stored, timed live the same way
     sweeps = {}
-    for key, lp in (("fp64", 0), ("bf16", 1)):
-        if lp and args.no_mixed:
+    for key, lp, sm in (("fp64", 0, False), ("bf16", 1, False), ("smoother_fp64", 0, True),
+                        ("smoother_bf16", 1, True)):
+        if (lp and args.no_mixed) or (sm and train is None):
             continue
-        ms, nbytes = solver.time_precond(20, lp)
+        ms, nbytes = solver.time_precond(20, lp, smoother=sm)
         sweeps[key] = {"ms_per_apply": ms, "algorithmic_bytes": nbytes, "achieved": nbytes / (ms * 1e-3) / 1e9,
                        "frac": nbytes / (ms * 1e-3) / 1e9 / peak}
 

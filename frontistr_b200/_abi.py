@@ -25,6 +25,7 @@ SIGNATURES = {
     "hecmw33_gpu_precond_apply": [_i, _d, _d, _i, _d, _i],
     "hecmw33_gpu_get_colouring": [_i, _i, _i, _i, _i],
     "hecmw33_gpu_colour_schedule": [_i, _i, _i, _i, _i, _i, _i, _i, _i, _i],
+    "hecmw33_gpu_smoother_schedule": [_i, _i, _i, _i, _i, _i, _i, _i, _i],
     "hecmw33_gpu_coarse_aggregates": [_i, _i, _i, _i, _i, _i, _i, _i, _i],
     "hecmw33_gpu_last_solve_info": [_i, _i, _d, _i],
     "hecmw33_gpu_condition_estimate": [_i, _i, _d, _d, _i],

@@ -48,19 +48,25 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   return v;
 }
 
-// mask[3i+d] = 1 when row 3i+d of A has a nonzero off-diagonal entry (thread per node).
-__global__ void coarse_mask_kernel(CoarseView c, const double *__restrict__ raw) {
+// mask[3i+d] = 1 when row 3i+d of A has a nonzero off-diagonal entry (warp per node,
+// lane k over block k of the row).
+__global__ void __launch_bounds__(kThreads) coarse_mask_kernel(CoarseView c, const double *__restrict__ raw) {
   pdl_entry();
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < c.n; i += nwarps) {
     bool cpl[3] = {false, false, false};
-    for (int k = c.uptr[i]; k < c.uptr[i + 1]; k++) {
+    for (int k = c.uptr[i] + lane; k < c.uptr[i + 1]; k += 32) {
       const double *a = raw + 9 * size_t(c.usrc[k]);
       const bool diag = c.ucol[k] == i;
       for (int d = 0; d < 3; d++)
         for (int e = 0; e < 3; e++)
           if (!(diag && d == e) && a[3 * d + e] != 0.0) cpl[d] = true;
     }
-    for (int d = 0; d < 3; d++) c.mask[3 * i + d] = cpl[d] ? 1.0f : 0.0f;
+    for (int d = 0; d < 3; d++) {
+      const bool any = __any_sync(0xffffffffu, cpl[d]);
+      if (lane == 0) c.mask[3 * i + d] = any ? 1.0f : 0.0f;
+    }
   }
 }
 
@@ -100,26 +106,17 @@ __global__ void coarse_dot_kernel(int n, const double *__restrict__ a, const dou
   }
 }
 
-// T0(i,b) = D_i^-1 sum_{j in N[i], agg(j) = b} A_ij M_j   (thread per node; the node's
-// entries are its own, so no two threads write one entry).  A singular D_i (no such
-// block in an assembled stiffness) leaves the node's T0 at zero.
-__global__ void coarse_t0_kernel(CoarseView c, const double *__restrict__ raw) {
+// T0(i,b) = D_i^-1 sum_{j in N[i], agg(j) = b} A_ij M_j   (warp per node: per entry b
+// of the node's pattern, lane k sums block k of the row, then a warp sum; lane 0
+// writes the entry).  A singular D_i (no such block in an assembled stiffness) leaves
+// the node's T0 at zero.
+__global__ void __launch_bounds__(kThreads) coarse_t0_kernel(CoarseView c, const double *__restrict__ raw) {
   pdl_entry();
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
-    const int q0 = c.pptr[i], q1 = c.pptr[i + 1];
-    for (int q = q0; q < q1; q++)
-      for (int e = 0; e < 9; e++) c.t0[9 * size_t(q) + e] = 0.0;
-    for (int k = c.uptr[i]; k < c.uptr[i + 1]; k++) {
-      const int j = c.ucol[k];
-      const int b = c.agg[j];
-      int q = q0;
-      while (q < q1 && c.pagg[q] != b) q++;
-      if (q == q1) continue;  // not in the pattern (cannot happen for a closed neighbourhood)
-      const double *a = raw + 9 * size_t(c.usrc[k]);
-      double *t = c.t0 + 9 * size_t(q);
-      for (int d = 0; d < 3; d++)
-        for (int e = 0; e < 3; e++) t[3 * d + e] += a[3 * d + e] * double(c.mask[3 * j + e]);
-    }
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < c.n; i += nwarps) {
+    const int k0 = c.uptr[i], k1 = c.uptr[i + 1];
+    // D_i^-1 by the adjugate (every lane; lane 0 uses it)
     const double *D = raw + 9 * size_t(i);
     const double c00 = D[4] * D[8] - D[5] * D[7], c01 = D[5] * D[6] - D[3] * D[8], c02 = D[3] * D[7] - D[4] * D[6];
     const double det = D[0] * c00 + D[1] * c01 + D[2] * c02;
@@ -138,12 +135,25 @@ __global__ void coarse_t0_kernel(CoarseView c, const double *__restrict__ raw) {
     } else {
       for (int e = 0; e < 9; e++) inv[e] = 0.0;
     }
-    for (int q = q0; q < q1; q++) {
-      double *t = c.t0 + 9 * size_t(q);
-      double o[9];
-      for (int d = 0; d < 3; d++)
-        for (int e = 0; e < 3; e++) o[3 * d + e] = inv[3 * d] * t[e] + inv[3 * d + 1] * t[3 + e] + inv[3 * d + 2] * t[6 + e];
-      for (int e = 0; e < 9; e++) t[e] = o[e];
+    for (int q = c.pptr[i]; q < c.pptr[i + 1]; q++) {
+      const int b = c.pagg[q];
+      double t[9];
+      for (int e = 0; e < 9; e++) t[e] = 0.0;
+      for (int k = k0 + lane; k < k1; k += 32) {
+        const int j = c.ucol[k];
+        if (c.agg[j] != b) continue;
+        const double *a = raw + 9 * size_t(c.usrc[k]);
+        const double m[3] = {double(c.mask[3 * j]), double(c.mask[3 * j + 1]), double(c.mask[3 * j + 2])};
+        for (int d = 0; d < 3; d++)
+          for (int e = 0; e < 3; e++) t[3 * d + e] += a[3 * d + e] * m[e];
+      }
+      for (int e = 0; e < 9; e++) t[e] = warp_sum_d(t[e]);
+      if (lane == 0) {
+        double *o = c.t0 + 9 * size_t(q);
+        for (int d = 0; d < 3; d++)
+          for (int e = 0; e < 3; e++)
+            o[3 * d + e] = inv[3 * d] * t[e] + inv[3 * d + 1] * t[3 + e] + inv[3 * d + 2] * t[6 + e];
+      }
     }
   }
 }
@@ -248,131 +258,179 @@ __global__ void coarse_zero_diag_kernel(double *__restrict__ ac, int nc) {
 }
 
 // ---- in-place inversion of the SPD coarse matrix: blocked Gauss-Jordan ----------
-// For each block K of kGjBlock pivots (no pivoting: Ac is SPD):
-//   Dinv = M_KK^-1;  C = M_:K (saved);  M_Kj = Dinv M_Kj (j not in K);
-//   M_ij -= C_iK M_Kj (i, j not in K);  M_iK = -C_iK Dinv (i not in K);  M_KK = Dinv.
+// For each block K of kGjBlock pivots (no pivoting: Ac is SPD), with A = M_KK,
+// B = M_Kj, C = M_iK, E = M_ij (i, j not in K):
+//   gj_diag:   Dinv = A^-1                                   (one CTA)
+//   gj_col:    G = C Dinv (saved);  M_iK = -G;  M_KK = Dinv
+//   gj_update: M_ij -= G_i B_j                               (B still the old row panel)
+//   gj_row:    M_Kj = Dinv B_j
 // After the last block M holds Ac^-1.
-constexpr int kGjBlock = 32;
+constexpr int kGjBlock = 64;
 
-// Dinv = M_KK^-1 by unblocked Gauss-Jordan in shared memory (one CTA).  A pivot that
-// is not positive sets *err (the coarse operator is then not used).
-__global__ void gj_diag_kernel(double *__restrict__ M, int n, int k0, int nb, double *__restrict__ dinv,
-                               int *err) {
+// Dinv = M_KK^-1 by unblocked Gauss-Jordan in shared memory (one CTA of 1024
+// threads; thread t owns row t / 16, columns t % 16 + 16 v).  A pivot that is not
+// positive sets *err (the coarse operator is then not used).
+__global__ void __launch_bounds__(1024) gj_diag_kernel(double *__restrict__ M, int n, int k0, int nb,
+                                                       double *__restrict__ dinv, int *err) {
   __shared__ double s[kGjBlock][kGjBlock + 1];
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) s[t / nb][t % nb] = M[size_t(k0 + t / nb) * n + k0 + t % nb];
+  const int i = threadIdx.x >> 4, jl = threadIdx.x & 15;
+#pragma unroll
+  for (int v = 0; v < 4; v++) {
+    const int j = jl + 16 * v;
+    s[i][j] = (i < nb && j < nb) ? M[size_t(k0 + i) * n + k0 + j] : 0.0;
+  }
   __syncthreads();
   for (int k = 0; k < nb; k++) {
+    // row and column k are not written before the barrier below, so every thread
+    // reads the same pivot
     const double piv = s[k][k];
-    __syncthreads();
     if (!(piv > 0.0)) {
       if (threadIdx.x == 0) atomicOr(err, 1);
-      return;  // uniform: every thread read the same pivot
+      return;  // uniform
     }
     const double d = 1.0 / piv;
-    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-      const int i = t / nb, j = t % nb;
-      if (i != k && j != k) s[i][j] -= s[i][k] * s[k][j] * d;
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
-      if (t != k) {
-        s[k][t] *= d;
-        s[t][k] *= -d;
+    if (i != k) {
+      const double sik = s[i][k];
+#pragma unroll
+      for (int v = 0; v < 4; v++) {
+        const int j = jl + 16 * v;
+        if (j != k) s[i][j] -= sik * s[k][j] * d;
       }
     }
     __syncthreads();
-    if (threadIdx.x == 0) s[k][k] = d;
+    const int t = threadIdx.x;
+    if (t < nb && t != k) {
+      s[k][t] *= d;
+      s[t][k] *= -d;
+    }
+    if (t == 0) s[k][k] = d;
     __syncthreads();
   }
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) dinv[t] = s[t / nb][t % nb];
-}
-
-// C(i, t) = M(i, k0 + t) for all rows i (n x nb, row-major with stride kGjBlock).
-__global__ void gj_save_col_kernel(const double *__restrict__ M, int n, int k0, int nb, double *__restrict__ C) {
-  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n * nb; x += gridDim.x * blockDim.x) {
-    const int i = x / nb, t = x % nb;
-    C[size_t(i) * kGjBlock + t] = M[size_t(i) * n + k0 + t];
+#pragma unroll
+  for (int v = 0; v < 4; v++) {
+    const int j = jl + 16 * v;
+    if (i < nb && j < nb) dinv[i * nb + j] = s[i][j];
   }
 }
 
-// M(K, j) = Dinv M(K, j) for columns j outside K (thread per column).
-__global__ void gj_row_kernel(double *__restrict__ M, int n, int k0, int nb, const double *__restrict__ dinv) {
-  __shared__ double D[kGjBlock * kGjBlock];
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) D[t] = dinv[t];
+// G(i, :) = M(i, K) Dinv and M(i, K) = -G(i, :) for rows i outside K; M(K, K) = Dinv
+// and G = 0 on the rows of K.  Warp per row: lane l holds M(i, k0 + l) and
+// M(i, k0 + 32 + l), broadcast by shuffles; lane l computes columns l and l + 32.
+// G is n x kGjBlock, row-major.
+__global__ void __launch_bounds__(256) gj_col_kernel(double *__restrict__ M, int n, int k0, int nb,
+                                                     const double *__restrict__ dinv, double *__restrict__ G) {
+  __shared__ double D[kGjBlock][kGjBlock];
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) D[t / nb][t % nb] = dinv[t];
   __syncthreads();
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    if (j >= k0 && j < k0 + nb) continue;
-    double v[kGjBlock];
-    for (int t = 0; t < nb; t++) v[t] = M[size_t(k0 + t) * n + j];
-    for (int s = 0; s < nb; s++) {
-      double a = 0.0;
-      for (int t = 0; t < nb; t++) a += D[s * nb + t] * v[t];
-      M[size_t(k0 + s) * n + j] = a;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+    double *row = M + size_t(i) * n + k0;
+    double *g = G + size_t(i) * kGjBlock;
+    if (i >= k0 && i < k0 + nb) {
+      for (int s = lane; s < nb; s += 32) {
+        row[s] = D[i - k0][s];
+        g[s] = 0.0;
+      }
+      continue;
+    }
+    const double m0 = lane < nb ? row[lane] : 0.0;
+    const double m1 = lane + 32 < nb ? row[lane + 32] : 0.0;
+    double g0 = 0.0, g1 = 0.0;
+    const int s1 = min(lane + 32, kGjBlock - 1);
+    for (int t = 0; t < nb; t++) {
+      const double mt = __shfl_sync(0xffffffffu, t < 32 ? m0 : m1, t & 31);
+      g0 += mt * D[t][lane];
+      g1 += mt * D[t][s1];
+    }
+    if (lane < nb) {
+      g[lane] = g0;
+      row[lane] = -g0;
+    }
+    if (lane + 32 < nb) {
+      g[lane + 32] = g1;
+      row[lane + 32] = -g1;
     }
   }
 }
 
-// M(i, j) -= C(i, :) M(K, j) for i, j outside K: 64 x 64 tiles, the tile's panels in
-// shared memory, 4 x 4 outputs per thread (256 threads).
+// M(i, j) -= G(i, :) M(K, j) for i, j outside K (M(K, j) is still the old row panel).
+// Tiles of 128 rows x 64 columns, 256 threads with 8 x 4 outputs each; the panels
+// go through shared memory 16 pivots at a time.
+constexpr int kGjTileI = 128, kGjTileJ = 64, kGjChunk = 16;
 __global__ void __launch_bounds__(256) gj_update_kernel(double *__restrict__ M, int n, int k0, int nb,
-                                                        const double *__restrict__ C) {
-  __shared__ double Cs[64][kGjBlock + 1];
-  __shared__ double Rs[kGjBlock][64 + 1];
-  const int i0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
-  for (int t = threadIdx.x; t < 64 * kGjBlock; t += blockDim.x) {
-    const int r = t / kGjBlock, k = t % kGjBlock;
-    const int i = i0 + r;
-    Cs[r][k] = (i < n && k < nb) ? C[size_t(i) * kGjBlock + k] : 0.0;
-  }
-  for (int t = threadIdx.x; t < kGjBlock * 64; t += blockDim.x) {
-    const int k = t / 64, cc = t % 64;
-    const int j = j0 + cc;
-    Rs[k][cc] = (j < n && k < nb) ? M[size_t(k0 + k) * n + j] : 0.0;
-  }
-  __syncthreads();
-  const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
-  double acc[4][4] = {};
-  for (int k = 0; k < nb; k++) {
-    double a[4], b[4];
+                                                        const double *__restrict__ G) {
+  __shared__ __align__(16) double Gs[kGjChunk][kGjTileI + 4];  // Gs[k][i] = G(i0 + i, kc + k)
+  __shared__ __align__(16) double Bs[kGjChunk][kGjTileJ];      // Bs[k][j] = M(k0 + kc + k, j0 + j)
+  const int i0 = blockIdx.y * kGjTileI, j0 = blockIdx.x * kGjTileJ;
+  // a tile inside the pivot rows or columns has nothing to update
+  if ((i0 >= k0 && i0 + kGjTileI <= k0 + nb) || (j0 >= k0 && j0 + kGjTileJ <= k0 + nb)) return;
+  const int tr = threadIdx.x >> 4, tc = threadIdx.x & 15;
+  double acc[8][4];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      a[u] = Cs[tr + 16 * u][k];
-      b[u] = Rs[k][tc + 16 * u];
+  for (int u = 0; u < 8; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) acc[u][v] = 0.0;
+  for (int kc = 0; kc < nb; kc += kGjChunk) {
+    for (int e = threadIdx.x; e < kGjTileI * kGjChunk; e += blockDim.x) {
+      const int i = e / kGjChunk, k = e % kGjChunk;
+      Gs[k][i] = (i0 + i < n && kc + k < nb) ? G[size_t(i0 + i) * kGjBlock + kc + k] : 0.0;
     }
+    for (int e = threadIdx.x; e < kGjChunk * kGjTileJ; e += blockDim.x) {
+      const int k = e / kGjTileJ, j = e % kGjTileJ;
+      Bs[k][j] = (j0 + j < n && kc + k < nb) ? M[size_t(k0 + kc + k) * n + j0 + j] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < kGjChunk; k++) {
+      const double2 a01 = *reinterpret_cast<const double2 *>(&Gs[k][tr * 8]);
+      const double2 a23 = *reinterpret_cast<const double2 *>(&Gs[k][tr * 8 + 2]);
+      const double2 a45 = *reinterpret_cast<const double2 *>(&Gs[k][tr * 8 + 4]);
+      const double2 a67 = *reinterpret_cast<const double2 *>(&Gs[k][tr * 8 + 6]);
+      const double2 b01 = *reinterpret_cast<const double2 *>(&Bs[k][tc * 4]);
+      const double2 b23 = *reinterpret_cast<const double2 *>(&Bs[k][tc * 4 + 2]);
+      const double a[8] = {a01.x, a01.y, a23.x, a23.y, a45.x, a45.y, a67.x, a67.y};
+      const double b[4] = {b01.x, b01.y, b23.x, b23.y};
 #pragma unroll
-    for (int u = 0; u < 4; u++)
+      for (int u = 0; u < 8; u++)
 #pragma unroll
-      for (int v = 0; v < 4; v++) acc[u][v] += a[u] * b[v];
+        for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+    __syncthreads();
   }
 #pragma unroll
-  for (int u = 0; u < 4; u++) {
-    const int i = i0 + tr + 16 * u;
+  for (int u = 0; u < 8; u++) {
+    const int i = i0 + tr * 8 + u;
     if (i >= n || (i >= k0 && i < k0 + nb)) continue;
 #pragma unroll
     for (int v = 0; v < 4; v++) {
-      const int j = j0 + tc + 16 * v;
+      const int j = j0 + tc * 4 + v;
       if (j >= n || (j >= k0 && j < k0 + nb)) continue;
       M[size_t(i) * n + j] -= acc[u][v];
     }
   }
 }
 
-// M(i, K) = -C(i, :) Dinv for rows i outside K, M(K, K) = Dinv (thread per row).
-__global__ void gj_col_kernel(double *__restrict__ M, int n, int k0, int nb, const double *__restrict__ C,
-                              const double *__restrict__ dinv) {
-  __shared__ double D[kGjBlock * kGjBlock];
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) D[t] = dinv[t];
+// M(K, j) = Dinv M(K, j) for columns j outside K: a CTA of 128 threads takes 16
+// columns (the panel in shared memory), thread (c, g) rows g*8 .. g*8+7 of column c.
+__global__ void __launch_bounds__(128) gj_row_kernel(double *__restrict__ M, int n, int k0, int nb,
+                                                     const double *__restrict__ dinv) {
+  __shared__ double D[kGjBlock][kGjBlock];
+  __shared__ double V[kGjBlock][16];
+  const int j0 = blockIdx.x * 16;
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) D[t / nb][t % nb] = dinv[t];
+  for (int t = threadIdx.x; t < nb * 16; t += blockDim.x) {
+    const int k = t / 16, c = t % 16;
+    V[k][c] = j0 + c < n ? M[size_t(k0 + k) * n + j0 + c] : 0.0;
+  }
   __syncthreads();
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (i >= k0 && i < k0 + nb) {
-      for (int s = 0; s < nb; s++) M[size_t(i) * n + k0 + s] = D[(i - k0) * nb + s];
-      continue;
-    }
-    for (int s = 0; s < nb; s++) {
-      double a = 0.0;
-      for (int t = 0; t < nb; t++) a += C[size_t(i) * kGjBlock + t] * D[t * nb + s];
-      M[size_t(i) * n + k0 + s] = -a;
-    }
+  const int c = threadIdx.x & 15, g = threadIdx.x >> 4;
+  const int j = j0 + c;
+  if (j >= n || (j >= k0 && j < k0 + nb)) return;
+  for (int s = g * 8; s < min(g * 8 + 8, nb); s++) {
+    double a = 0.0;
+    for (int t = 0; t < nb; t++) a += D[s][t] * V[t][c];
+    M[size_t(k0 + s) * n + j] = a;
   }
 }
 

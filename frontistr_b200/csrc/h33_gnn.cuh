@@ -128,7 +128,12 @@ __global__ void gnn_encode_kernel(GnnGraph g, const W *__restrict__ theta, const
   }
 }
 
-// One message-passing layer (warp per node, lane = channel).
+// One message-passing layer (warp per node, lane = channel).  The weights sit
+// transposed in shared memory (WsT[k][j] = Ws[j][k]), so lane j's reads of column k
+// fall in distinct banks.  The node's edges are taken 32 at a time: lane e loads
+// edge e's column and weight, then every lane receives them by shuffles, so only
+// the h gathers (128 contiguous bytes per edge) touch memory; the sum over the
+// edges keeps their order.
 template <class W>
 __global__ void __launch_bounds__(kThreads) gnn_layer_kernel(GnnGraph g, const W *__restrict__ theta, int l,
                                                              const float *__restrict__ w,
@@ -138,10 +143,11 @@ __global__ void __launch_bounds__(kThreads) gnn_layer_kernel(GnnGraph g, const W
   pdl_entry();
   if (st && (st->done || !st->use_gnn)) return;
   const GnnOffsets o = GnnOffsets::make();
-  __shared__ float Ws[kGnnWidth * kGnnWidth], Wm[kGnnWidth * kGnnWidth];
+  __shared__ float WsT[kGnnWidth * kGnnWidth], WmT[kGnnWidth * kGnnWidth];
   for (int k = threadIdx.x; k < kGnnWidth * kGnnWidth; k += blockDim.x) {
-    Ws[k] = wload(theta + o.Ws[l] + k);
-    Wm[k] = wload(theta + o.Wm[l] + k);
+    const int j = k / kGnnWidth, c = k % kGnnWidth;
+    WsT[c * kGnnWidth + j] = wload(theta + o.Ws[l] + k);
+    WmT[c * kGnnWidth + j] = wload(theta + o.Wm[l] + k);
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -149,14 +155,29 @@ __global__ void __launch_bounds__(kThreads) gnn_layer_kernel(GnnGraph g, const W
   const float *wl = w + size_t(l) * g.nedges;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < g.n; i += nwarps) {
     float m = 0.0f;
-    for (int e = g.ptr[i]; e < g.ptr[i + 1]; e++) m += wl[e] * h_prev[size_t(g.col[e]) * kGnnWidth + lane];
+    const int e1 = g.ptr[i + 1];
+    for (int e0 = g.ptr[i]; e0 < e1; e0 += 32) {
+      const int ne = min(32, e1 - e0);
+      int myc = 0;
+      float myw = 0.0f;
+      if (lane < ne) {
+        myc = g.col[e0 + lane];
+        myw = wl[e0 + lane];
+      }
+#pragma unroll 8
+      for (int k = 0; k < ne; k++) {
+        const int c = __shfl_sync(0xffffffffu, myc, k);
+        const float wk = __shfl_sync(0xffffffffu, myw, k);
+        m += wk * h_prev[size_t(c) * kGnnWidth + lane];
+      }
+    }
     const float hs = h_prev[size_t(i) * kGnnWidth + lane];
     float a = 0.0f;
 #pragma unroll
     for (int k = 0; k < kGnnWidth; k++) {
       const float hk = __shfl_sync(0xffffffffu, hs, k);
       const float mk = __shfl_sync(0xffffffffu, m, k);
-      a += Ws[lane * kGnnWidth + k] * hk + Wm[lane * kGnnWidth + k] * mk;
+      a += WsT[k * kGnnWidth + lane] * hk + WmT[k * kGnnWidth + lane] * mk;
     }
     if (m_out) m_out[size_t(i) * kGnnWidth + lane] = m;
     h_new[size_t(i) * kGnnWidth + lane] = tanhf(a);
@@ -441,13 +462,16 @@ __global__ void gnn_node_scale_kernel(const double *__restrict__ raw, int n, flo
   }
 }
 
-// feat_e = s_i A_ij s_j for edge e = (i, j), A_ij the raw block src[e]
+// feat_e = s_i A_ij s_j for edge e = (i, j), A_ij the raw block src[e] (thread per
+// entry, so that the writes are contiguous)
 __global__ void gnn_edge_feat_kernel(GnnGraph g, const int *__restrict__ row_of, const int *__restrict__ src,
                                      const double *__restrict__ raw, float *__restrict__ feat) {
   pdl_entry();
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.nedges; e += gridDim.x * blockDim.x) {
+  const size_t total = size_t(9) * size_t(g.nedges);
+  for (size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x; x < total; x += size_t(gridDim.x) * blockDim.x) {
+    const int e = int(x / 9), k = int(x % 9);
     const double f = double(g.s[row_of[e]]) * double(g.s[g.col[e]]);
-    for (int k = 0; k < 9; k++) feat[9 * size_t(e) + k] = float(raw[9 * size_t(src[e]) + k] * f);
+    feat[x] = float(raw[9 * size_t(src[e]) + k] * f);
   }
 }
 

@@ -18,6 +18,7 @@
 namespace h33 {
 
 constexpr int kMaxRhs = 16;
+constexpr int kMrLanes = 16;  // lanes per row of the SpMM's copy of A
 constexpr int kRhsStride = 3 * kMaxRhs;  // doubles per node
 
 // Loop control shared by all right-hand sides.
@@ -122,8 +123,10 @@ __device__ __forceinline__ bool mr_locate(const SellView<double> &A, int sb, int
 // y = A x (MODE 0); y = b - A x (MODE 1); MODE 2: q = A p with the per-RHS {p}{q}
 // and ALPHA; MODE 3: r = b - A x with the per-RHS DNRM2 for the RHS whose true
 // residual is due, then the per-RHS end-of-iteration control (resid_ctl_kernel's
-// logic for every RHS).
-template <int MODE>
+// logic for every RHS).  A has K lanes per row (32/K rows per slice): with K = 16 the
+// half-warp's 16 blocks of one chunk of its row sit in one slot, so each of the nine
+// value loads and the column load is one contiguous 128-byte segment.
+template <int MODE, int K>
 __global__ void __launch_bounds__(kThreads) mr_spmv_kernel(SellView<double> A, const double *__restrict__ x,
                                                            double *__restrict__ y, const double *__restrict__ b,
                                                            CgState *st, MultiCtl *ctl, double *partials) {
@@ -143,16 +146,17 @@ __global__ void __launch_bounds__(kThreads) mr_spmv_kernel(SellView<double> A, c
   }
   const int hw0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
   const int nhw = (gridDim.x * blockDim.x) >> 4;
-  const int nrows_total = A.nslices * 32;
+  constexpr int rps = 32 / K;  // rows per slice
+  const int nrows_total = A.nslices * rps;
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
   double dot = 0.0;
   for (int t = hw0; t < nrows_total; t += nhw) {
-    const int s = t >> 5, roff = t & 31;
+    const int s = t / rps, roff = t % rps;
     if (roff >= A.nrows[s]) continue;
     const int row = A.row0[s] + roff;
     const int len = A.rowlen[s * 32 + roff];
     double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-    mr_row<1>(A, s, roff, len, l, hmask, x, y0, y1, y2);
+    mr_row<K>(A, s, roff, len, l, hmask, x, y0, y1, y2);
     const size_t o = size_t(row) * kRhsStride + l;
     if (MODE == 1 || MODE == 3) {
       y0 = b[o] - y0;

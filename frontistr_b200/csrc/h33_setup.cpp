@@ -159,6 +159,40 @@ void ordering_rcm(const Profile &p, std::vector<int> &perm, std::vector<int> &ip
   }
 }
 
+int ordering_greedy(const Profile &p, std::vector<int> &colorindex, std::vector<int> &perm,
+                    std::vector<int> &iperm) {
+  const int N = p.N;
+  std::vector<int> colour(static_cast<size_t>(N), -1), seen;
+  int ncolor = 0;
+  for (int i = 0; i < N; i++) {
+    auto visit = [&](const int *index, const int *item) {
+      for (int k = index[i]; k < index[i + 1]; k++) {
+        const int c = colour[static_cast<size_t>(item[k] - 1)];
+        if (c >= 0) seen[static_cast<size_t>(c)] = i;
+      }
+    };
+    seen.resize(static_cast<size_t>(ncolor) + 1, -1);
+    visit(p.indexL, p.itemL);
+    visit(p.indexU, p.itemU);
+    int c = 0;
+    while (seen[static_cast<size_t>(c)] == i) c++;
+    colour[static_cast<size_t>(i)] = c;
+    ncolor = std::max(ncolor, c + 1);
+  }
+  colorindex.assign(static_cast<size_t>(ncolor) + 1, 0);
+  for (int i = 0; i < N; i++) colorindex[static_cast<size_t>(colour[static_cast<size_t>(i)]) + 1]++;
+  for (int c = 0; c < ncolor; c++) colorindex[static_cast<size_t>(c) + 1] += colorindex[static_cast<size_t>(c)];
+  perm.assign(static_cast<size_t>(N), 0);
+  iperm.assign(static_cast<size_t>(N), 0);
+  std::vector<int> at(colorindex.begin(), colorindex.end() - 1);
+  for (int i = 0; i < N; i++) {
+    const int pos = at[static_cast<size_t>(colour[static_cast<size_t>(i)])]++;
+    perm[static_cast<size_t>(pos)] = i;
+    iperm[static_cast<size_t>(i)] = pos;
+  }
+  return ncolor;
+}
+
 int ordering_mc(const Profile &p, const std::vector<int> &perm_cur, int ncolor_in,
                 std::vector<int> &colorindex, std::vector<int> &perm, std::vector<int> &iperm) {
   const int N = p.N;

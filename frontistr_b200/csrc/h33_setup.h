@@ -35,6 +35,13 @@ void ordering_rcm(const Profile &p, std::vector<int> &perm, std::vector<int> &ip
 int ordering_mc(const Profile &p, const std::vector<int> &perm_cur, int ncolor_in,
                 std::vector<int> &colorindex, std::vector<int> &perm, std::vector<int> &iperm);
 
+// First-fit colouring in the input order (each node takes the smallest colour none of
+// its already coloured neighbours has), rows then ordered by colour, by node number
+// inside a colour.  On a structured 27-point mesh numbered lexicographically this
+// gives the 8 parity colours.  Returns the number of colours.
+int ordering_greedy(const Profile &p, std::vector<int> &colorindex, std::vector<int> &perm,
+                    std::vector<int> &iperm);
+
 // A row-wise list of blocks: for row r, entries [ptr[r], ptr[r+1]) of (col, src),
 // col = 0-based node index gathered by the kernel, src = raw block id.
 struct BlockRows {

@@ -243,6 +243,7 @@ struct Precond {
   DevArray<float> alu32_fwd, alu32_bwd;
   int numeric_version = 0, fp32_version = -1, lowp_version = -1;
   bool pos_cols = false;  // lo/up columns are colour positions (multicolour SSOR)
+  double sigma = 0.0;     // SIGMA_DIAG of the last numeric setup
 };
 
 // The learned preconditioner: node graph of the matrix, weights, activations and
@@ -269,6 +270,11 @@ struct Learned {
   std::vector<double> per;
   DevArray<double> losses;
   GnnGraph graph() const { return GnnGraph{n, nedges, ptr.p, col.p, rev.p, feat.p, s.p}; }
+  // the smoother of the two-grid cycle: SSOR on its own layouts in first-fit colour
+  // order, rebuilt with the matrix structure (symbolic) and with every numeric setup
+  // of the solve's SSOR (same SIGMA_DIAG)
+  Precond sm;
+  int sm_built_for = -1, sm_numeric_for = -1;
   // the coarse space the network shapes (h33_coarse.cuh): aggregation and patterns
   // (per matrix structure), prolongator, A P, dense coarse inverse (per matrix values
   // and weights), application and training vectors
@@ -447,6 +453,11 @@ struct Solver {
   DevArray<int> mt_ptr, mt_cols;
   DevArray<uint16_t> mt_lidx;
   int mt_generation = -1, mt_maxcols = 0, mt_occ = 0, mt_ntiles = 0;
+  // A again with 16 lanes per row for the multi-RHS SpMM (mr_spmv_kernel<., 16>)
+  DevSell<double> Amr;
+  int amr_generation = -1, amr_values = -1;
+  SellView<double> amr_view() const { return Amr.view(); }
+  int grid_amr() const { return grid_mr(Amr.nslices * (32 / kMrLanes)); }
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int build_counter = 0;  // monotonic id of preconditioner builds (graph cache key)
   // last-solve record
@@ -700,13 +711,20 @@ void diag_alu(Solver &S, DevArray<double> &alu, const double *blocks, const int 
   H33_CUDA(cudaGetLastError());
 }
 
-void setup_ssor(Solver &S, int ncolor_in, double sigma, bool symbolic) {
-  Precond &P = S.pc;
+// SSOR in P: the reference's RCM + multicolour ordering (greedy = false, the drop-in),
+// or first-fit colours in the input order (greedy = true: the learned preconditioner's
+// smoother, which is not bound to the reference's schedule).
+void setup_ssor(Solver &S, Precond &P, int ncolor_in, double sigma, bool symbolic, bool greedy) {
+  P.sigma = sigma;
   if (symbolic) {
     Profile prof{S.N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
     std::vector<int> perm_rcm, iperm_rcm, perm, iperm, colorindex;
-    ordering_rcm(prof, perm_rcm, iperm_rcm);
-    P.ncolor = ordering_mc(prof, perm_rcm, ncolor_in, colorindex, perm, iperm);
+    if (greedy) {
+      P.ncolor = ordering_greedy(prof, colorindex, perm, iperm);
+    } else {
+      ordering_rcm(prof, perm_rcm, iperm_rcm);
+      P.ncolor = ordering_mc(prof, perm_rcm, ncolor_in, colorindex, perm, iperm);
+    }
     BlockRows lower_ref, upper_ref, lower, upper;
     reordered_rows(prof, perm, iperm, lower_ref, upper_ref);
     // the device sweeps gather from their colour-ordered intermediate: columns as
@@ -859,7 +877,7 @@ void precond_setup(Solver &S, int precond, int ncolor_in, double sigma, int *Iar
   }
   P.kind = kind;
   P.ncolor_in = ncolor_in;
-  if (kind == 1) setup_ssor(S, ncolor_in, sigma, symbolic);
+  if (kind == 1) setup_ssor(S, P, ncolor_in, sigma, symbolic, false);
   else if (kind == 3) diag_alu(S, P.alu_fwd, S.raw.p, nullptr, sigma, 0);
   else setup_bilu(S, level, sigma, symbolic);
   int err = 0;
@@ -875,6 +893,31 @@ void precond_setup(Solver &S, int precond, int ncolor_in, double sigma, int *Iar
   }
   Iarray[97] = 0;
   Iarray[96] = 0;
+}
+
+// The learned preconditioner's smoother (Learned::sm) for the current matrix and the
+// solve's SSOR setup.  First-fit colours give far fewer colour launches than the
+// reference's multicolouring (8 against 17 on a structured hexahedral mesh).
+void ensure_smoother(Solver &S) {
+  Learned &L = S.L;
+  Precond &P = L.sm;
+  const bool symbolic = !P.valid || L.sm_built_for != S.generation;
+  if (!symbolic && L.sm_numeric_for == S.pc.numeric_version) return;
+  if (symbolic) P = Precond();
+  P.kind = 1;
+  setup_ssor(S, P, 0, S.pc.sigma, symbolic, true);
+  int err = 0;
+  H33_CUDA(cudaMemcpyAsync(&err, S.d_err.p, sizeof(int), cudaMemcpyDeviceToHost, S.stream));
+  S.sync();
+  (void)err;  // as the solve's SSOR: a zero pivot gives Inf entries, not an error
+  P.valid = true;
+  P.numeric_version = ++S.build_counter;
+  if (symbolic) {
+    P.generation = ++S.build_counter;
+    S.drop_graph();
+  }
+  L.sm_built_for = S.generation;
+  L.sm_numeric_for = S.pc.numeric_version;
 }
 
 // ---------------------------------------------------------------------------
@@ -893,32 +936,33 @@ struct Views {
   SellView<__nv_bfloat16> lo16, up16;
   const float *alu32_f, *alu32_b;
   R *zpos;  // the sweeps' intermediate in colour-position order (multicolour SSOR)
+  const Precond *pc;  // whose schedule the sweeps follow
 };
 
-Views<double> views(Solver &S, double, int lowp = 0) {
-  Precond &P = S.pc;
+// Views of the solve's vectors and of the preconditioner pc (default: the drop-in's).
+Views<double> views(Solver &S, double, int lowp = 0, const Precond *pc = nullptr) {
+  const Precond &P = pc ? *pc : S.pc;
   return Views<double>{S.A.view(),   P.lo.view(),   P.up.view(), P.alu_fwd.p,
                        P.alu_shared ? P.alu_fwd.p : P.alu_bwd.p,
                        S.b.p, S.x.p, S.r.p, S.z.p, S.p.p, S.q.p, S.w.p, S.zp.p, S.zs.p, S.rold.p,
                        lowp, P.lo.view16(), P.up.view16(), P.alu32_fwd.p,
-                       P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p, S.zpos.p};
+                       P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p, S.zpos.p, &P};
 }
-Views<float> views(Solver &S, float, int lowp = 0) {
-  Precond &P = S.pc;
+Views<float> views(Solver &S, float, int lowp = 0, const Precond *pc = nullptr) {
+  const Precond &P = pc ? *pc : S.pc;
   return Views<float>{S.A.view32(),   P.lo.view32(),   P.up.view32(), P.alu32_fwd.p,
                       P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p,
                       S.bf.p, S.xf.p, S.rf.p, S.zf.p, S.pf.p, S.qf.p, S.wf.p, S.zpf.p, S.zsf.p, S.roldf.p,
                       lowp, P.lo.view16(), P.up.view16(), P.alu32_fwd.p,
-                      P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p, S.zposf.p};
+                      P.alu_shared ? P.alu32_fwd.p : P.alu32_bwd.p, S.zposf.p, &P};
 }
 
 // z = M^-1 r, one pass; FUSE_RHO adds the RHO reduction + finisher.  K = lanes per
 // row of the sweep layouts.
 // Node-order sweeps: the ILU(0) level schedules.
 template <class R, class TV, class TA, bool FUSE_RHO, int K>
-void launch_sweep_node(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f,
-                       const TA *alu_b, const R *rin, R *zout, CgState *st) {
-  Precond &P = S.pc;
+void launch_sweep_node(Solver &S, const Precond &P, const SellView<TV> &lo, const SellView<TV> &up,
+                       const TA *alu_f, const TA *alu_b, const R *rin, R *zout, CgState *st) {
   cudaStream_t s = S.stream;
   const int *perm_b = P.alu_shared ? P.perm_fwd.p : P.perm_bwd.p;
   const int pre = level_pre<TV>();
@@ -967,9 +1011,8 @@ RunShape run_shape(const DevSell<double> &D, int g) {
 }
 
 template <class R, class TV, class TA, bool FUSE_RHO, int K>
-void launch_sweep_uni(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f, const R *rin,
-                      R *zout, R *zpos, CgState *st) {
-  Precond &P = S.pc;
+void launch_sweep_uni(Solver &S, const Precond &P, const SellView<TV> &lo, const SellView<TV> &up,
+                      const TA *alu_f, const R *rin, R *zout, R *zpos, CgState *st) {
   cudaStream_t s = S.stream;
   const int gf = int(P.lo.group_slice.size()) - 1;
   for (int g = 0; g < gf; g++) {
@@ -997,9 +1040,8 @@ void launch_sweep_uni(Solver &S, const SellView<TV> &lo, const SellView<TV> &up,
 
 // Lanes per row are 4, 8 or 16 (sweep_lanes()).
 template <class R, class TV, class TA, bool FUSE_RHO>
-void launch_sweep_t(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, const TA *alu_f, const TA *alu_b,
-                    const R *rin, R *zout, R *zpos, CgState *st) {
-  Precond &P = S.pc;
+void launch_sweep_t(Solver &S, const Precond &P, const SellView<TV> &lo, const SellView<TV> &up,
+                    const TA *alu_f, const TA *alu_b, const R *rin, R *zout, R *zpos, CgState *st) {
   if (P.kind == 3) {
     launch_k(S.stream, diag_kernel<R, TA, FUSE_RHO>, S.grid_vec(), kThreads, alu_f, S.N, rin, zout, st,
              S.partials.p);
@@ -1007,25 +1049,25 @@ void launch_sweep_t(Solver &S, const SellView<TV> &lo, const SellView<TV> &up, c
   }
   if (P.pos_cols) {
     switch (P.lo.lanes) {
-      case 8: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 8>(S, lo, up, alu_f, rin, zout, zpos, st);
-      case 16: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 16>(S, lo, up, alu_f, rin, zout, zpos, st);
-      default: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 4>(S, lo, up, alu_f, rin, zout, zpos, st);
+      case 8: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 8>(S, P, lo, up, alu_f, rin, zout, zpos, st);
+      case 16: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 16>(S, P, lo, up, alu_f, rin, zout, zpos, st);
+      default: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 4>(S, P, lo, up, alu_f, rin, zout, zpos, st);
     }
   }
   switch (P.lo.lanes) {
-    case 8: return launch_sweep_node<R, TV, TA, FUSE_RHO, 8>(S, lo, up, alu_f, alu_b, rin, zout, st);
-    case 16: return launch_sweep_node<R, TV, TA, FUSE_RHO, 16>(S, lo, up, alu_f, alu_b, rin, zout, st);
-    default: return launch_sweep_node<R, TV, TA, FUSE_RHO, 4>(S, lo, up, alu_f, alu_b, rin, zout, st);
+    case 8: return launch_sweep_node<R, TV, TA, FUSE_RHO, 8>(S, P, lo, up, alu_f, alu_b, rin, zout, st);
+    case 16: return launch_sweep_node<R, TV, TA, FUSE_RHO, 16>(S, P, lo, up, alu_f, alu_b, rin, zout, st);
+    default: return launch_sweep_node<R, TV, TA, FUSE_RHO, 4>(S, P, lo, up, alu_f, alu_b, rin, zout, st);
   }
 }
 
 template <class R, bool FUSE_RHO>
 void launch_sweep(Solver &S, const Views<R> &V, const R *rin, R *zout, CgState *st) {
   if (V.lowp)
-    launch_sweep_t<R, __nv_bfloat16, float, FUSE_RHO>(S, V.lo16, V.up16, V.alu32_f, V.alu32_b, rin, zout, V.zpos,
-                                                      st);
+    launch_sweep_t<R, __nv_bfloat16, float, FUSE_RHO>(S, *V.pc, V.lo16, V.up16, V.alu32_f, V.alu32_b, rin, zout,
+                                                      V.zpos, st);
   else
-    launch_sweep_t<R, R, R, FUSE_RHO>(S, V.lo, V.up, V.alu_f, V.alu_b, rin, zout, V.zpos, st);
+    launch_sweep_t<R, R, R, FUSE_RHO>(S, *V.pc, V.lo, V.up, V.alu_f, V.alu_b, rin, zout, V.zpos, st);
 }
 
 // hecmw_precond_apply (hecmw_precond.f90:86-172): z = M^-1 r with iterPREmax passes.
@@ -1250,7 +1292,7 @@ void launch_iteration_reliable(Solver &S, int iterpremax, bool learned, cudaGrap
   cudaStream_t s = S.stream;
   CgState *st = S.state.p;
   const int n3 = S.n3();
-  const Views<float> V = views(S, 0.0f);
+  const Views<float> V = views(S, 0.0f, 0, learned ? &S.L.sm : nullptr);
   launch_k(s, iter_begin_kernel, 1, 32, st, h, use_cond);
   if (learned) {
     launch_learned_precond<float>(S, V, st);
@@ -1285,7 +1327,7 @@ void build_graph(Solver &S, int iterpremax, int mode = 0) {
                       mode + (flexible ? S.L.graph_generation * 4 : 0)};
   if (G.exec && std::equal(key, key + 5, G.key)) return;
   G.drop();
-  const Views<R> V = views(S, R(), lowp);
+  const Views<R> V = views(S, R(), lowp, flexible ? &S.L.sm : nullptr);
   cudaGraph_t g = nullptr;
   H33_CUDA(cudaGraphCreate(&g, 0));
   G.graph = g;
@@ -1333,7 +1375,7 @@ void build_graph(Solver &S, int iterpremax, int mode = 0) {
 template <class R>
 float run_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels, int inner = 0, int learned = 0,
              int reliable = 0, double ru_delta = 1e-4, int lowp = 0, int method = 1) {
-  const Views<R> V = views(S, R(), lowp);
+  const Views<R> V = views(S, R(), lowp, learned ? &S.L.sm : nullptr);
   const int mode = (learned ? 1 : 0) | (reliable ? 2 : 0) | (lowp ? 4 : 0) | (method == 2 ? 8 : 0);
   S.h_params->tol = tol;
   S.h_params->maxit = maxit;
@@ -1426,6 +1468,29 @@ double dot_device(Solver &S, const double *a, const double *b) {
   return v;
 }
 
+// FP32 copies of one preconditioner's values (same layouts).
+void ensure_fp32_pc(Solver &S, Precond &P) {
+  auto conv = [&](const double *a, float *b, size_t n) {
+    if (n == 0) return;
+    const int grid = int(std::min<size_t>((n + kThreads - 1) / kThreads, size_t(S.nsm) * 16));
+    launch_k(S.stream, convert_kernel<float>, grid, kThreads, a, b, n);
+    H33_CUDA(cudaGetLastError());
+  };
+  if (P.fp32_version != P.numeric_version) {
+    for (auto *d : {&P.lo, &P.up}) {
+      d->val32.alloc(d->val.n);
+      conv(d->val.p, d->val32.p, d->val.n);
+    }
+    P.alu32_fwd.alloc(P.alu_fwd.n);
+    conv(P.alu_fwd.p, P.alu32_fwd.p, P.alu_fwd.n);
+    if (!P.alu_shared) {
+      P.alu32_bwd.alloc(P.alu_bwd.n);
+      conv(P.alu_bwd.p, P.alu32_bwd.p, P.alu_bwd.n);
+    }
+    P.fp32_version = P.numeric_version;
+  }
+}
+
 // FP32 copies of the matrix and preconditioner values (same sliced layouts),
 // refreshed when the FP64 values changed.
 void ensure_fp32(Solver &S) {
@@ -1440,20 +1505,7 @@ void ensure_fp32(Solver &S) {
     conv(S.A.val.p, S.A.val32.p, S.A.val.n);
     S.a32_version = S.values_version;
   }
-  Precond &P = S.pc;
-  if (P.fp32_version != P.numeric_version) {
-    for (auto *d : {&P.lo, &P.up}) {
-      d->val32.alloc(d->val.n);
-      conv(d->val.p, d->val32.p, d->val.n);
-    }
-    P.alu32_fwd.alloc(P.alu_fwd.n);
-    conv(P.alu_fwd.p, P.alu32_fwd.p, P.alu_fwd.n);
-    if (!P.alu_shared) {
-      P.alu32_bwd.alloc(P.alu_bwd.n);
-      conv(P.alu_bwd.p, P.alu32_bwd.p, P.alu_bwd.n);
-    }
-    P.fp32_version = P.numeric_version;
-  }
+  ensure_fp32_pc(S, S.pc);
   const size_t n3 = size_t(S.n3());
   for (auto *v : {&S.bf, &S.xf, &S.rf, &S.zf, &S.pf, &S.qf, &S.wf, &S.zpf}) v->alloc(n3);
   if (S.zposf.n != n3) {
@@ -1514,7 +1566,8 @@ void learned_graph(Solver &S) {
   if (L.feat_version != S.values_version) {
     const int grid = std::max(1, std::min((N + kThreads - 1) / kThreads, S.nsm * 8));
     launch_k(S.stream, gnn_node_scale_kernel, grid, kThreads, S.raw.p, N, L.s.p);
-    const int ge = std::max(1, std::min((L.nedges + kThreads - 1) / kThreads, S.nsm * 16));
+    const int ge = int(std::max<int64_t>(1, std::min<int64_t>((int64_t(9) * L.nedges + kThreads - 1) / kThreads,
+                                                               int64_t(S.nsm) * 16)));
     launch_k(S.stream, gnn_edge_feat_kernel, ge, kThreads, L.graph(), L.row_of.p, L.src.p, S.raw.p, L.feat.p);
     H33_CUDA(cudaGetLastError());
     L.feat_version = S.values_version;
@@ -1608,9 +1661,10 @@ void coarse_values(Solver &S) {
   auto &C = S.L.C;
   if (C.t0_version == S.values_version) return;
   const int gt = std::max(1, std::min((S.N + kThreads - 1) / kThreads, S.nsm * 8));
-  launch_k(S.stream, coarse_mask_kernel, gt, kThreads, C.view(), static_cast<const double *>(S.raw.p));
+  const int gw = std::max(1, std::min((S.N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 16));
+  launch_k(S.stream, coarse_mask_kernel, gw, kThreads, C.view(), static_cast<const double *>(S.raw.p));
   launch_k(S.stream, coarse_features_kernel, gt, kThreads, C.view(), C.x.p);
-  launch_k(S.stream, coarse_t0_kernel, gt, kThreads, C.view(), static_cast<const double *>(S.raw.p));
+  launch_k(S.stream, coarse_t0_kernel, gw, kThreads, C.view(), static_cast<const double *>(S.raw.p));
   H33_CUDA(cudaGetLastError());
   C.t0_version = S.values_version;
 }
@@ -1664,14 +1718,13 @@ bool coarse_operator(Solver &S, const float *omega) {
   launch_k(s, coarse_ac_kernel, std::max(1, S.nsm * 8), kThreads, cv);
   coarse_zero_diag_kernel<<<std::max(1, (C.nc + 255) / 256), 256, 0, s>>>(C.ac.p, C.nc);
   const int n = C.nc;
-  const int tiles = (n + 63) / 64;
+  const dim3 tiles(unsigned((n + kGjTileJ - 1) / kGjTileJ), unsigned((n + kGjTileI - 1) / kGjTileI));
   for (int k0 = 0; k0 < n; k0 += kGjBlock) {
     const int nb = std::min(kGjBlock, n - k0);
-    gj_diag_kernel<<<1, 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p, C.err.p);
-    gj_save_col_kernel<<<std::max(1, std::min((n * nb + 255) / 256, S.nsm * 8)), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjc.p);
-    gj_row_kernel<<<std::max(1, (n + 255) / 256), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p);
-    gj_update_kernel<<<dim3(unsigned(tiles), unsigned(tiles)), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjc.p);
-    gj_col_kernel<<<std::max(1, (n + 255) / 256), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjc.p, C.gjd.p);
+    gj_diag_kernel<<<1, 1024, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p, C.err.p);
+    gj_col_kernel<<<std::max(1, (n + 7) / 8), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p, C.gjc.p);
+    gj_update_kernel<<<tiles, 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjc.p);
+    gj_row_kernel<<<std::max(1, (n + 15) / 16), 128, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p);
   }
   // FP32 copies for the application
   auto conv = [&](const DevArray<double> &a, DevArray<float> &b) {
@@ -1785,6 +1838,7 @@ void learned_prepare_inference(Solver &S) {
     throw Failure(HECMW33_ERR_INCONS_PC, "the learned preconditioner works after SSOR (PRECOND 1 or 2)");
   if (S.dom.on)
     throw Failure(HECMW33_ERR_INCONS_PC, "the learned preconditioner takes a whole mesh (one domain) only");
+  ensure_smoother(S);
   learned_graph(S);
   coarse_structure(S);
   coarse_values(S);
@@ -1977,7 +2031,8 @@ float record_cg(Solver &S, int iterpremax, double tol, int maxit, int *kernels) 
   return ms;
 }
 
-// Trains the network on the recorded pairs, smoothed once by SSOR: Adam on the mean
+// Trains the network on the recorded pairs, smoothed once by the two-grid cycle's
+// SSOR smoother (Learned::sm): Adam on the mean
 // loss of learned_coarse_pass.  loss[0] = mean loss before the first step, loss[1] =
 // after the last.
 void learned_train(Solver &S, int steps, double lr, double *loss) {
@@ -1998,7 +2053,8 @@ void learned_train(Solver &S, int steps, double lr, double *loss) {
   std::vector<const float *> pr;
   {
     auto &C = L.C;
-    const Views<double> V = views(S, 0.0);
+    ensure_smoother(S);
+    const Views<double> V = views(S, 0.0, 0, &S.L.sm);
     const int gt = S.grid_vec(), n3 = S.n3();
     for (int k = 0; k < np; k++) {
       launch_k(S.stream, coarse_widen_kernel, gt, kThreads, static_cast<const float *>(L.pr[size_t(k)].p),
@@ -2032,8 +2088,7 @@ void learned_train(Solver &S, int steps, double lr, double *loss) {
 
 // BF16 copies of the preconditioner's sweep values and FP32 copies of its diagonal
 // LU (same layouts), refreshed when the preconditioner's values changed.
-void ensure_lowp(Solver &S) {
-  Precond &P = S.pc;
+void ensure_lowp(Solver &S, Precond &P) {
   if (P.lowp_version == P.numeric_version) return;
   auto grid = [&](size_t n) { return int(std::max<size_t>(1, std::min<size_t>((n + kThreads - 1) / kThreads, size_t(S.nsm) * 16))); };
   for (auto *d : {&P.lo, &P.up}) {
@@ -2050,6 +2105,7 @@ void ensure_lowp(Solver &S) {
   P.lowp_version = P.numeric_version;
   P.fp32_version = -1;  // the FP32 ALU copy now follows the low-precision path
 }
+void ensure_lowp(Solver &S) { ensure_lowp(S, S.pc); }
 
 // Checks and preconditioner setup shared by the FP64 and mixed solves
 // (hecmw_solve + hecmw_solve_iterative up to the CG call).  Returns 0 to go on,
@@ -2948,8 +3004,12 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   S.rhist_on = Iarray[20] == 1 && (method == 1 || method == 2) && !learned;  // hecmw_mat_get_iterlog
   S.iterlog = Iarray[20] == 1;
   if (S.rhist_on) S.rhist_buf.alloc(size_t(std::max(MAXIT, 1)));
-  if (lowp && iterPREmax > 0) ensure_lowp(S);
-  else lowp = 0;
+  if (lowp && iterPREmax > 0) {
+    ensure_lowp(S);
+    if (learned) ensure_lowp(S, S.L.sm);
+  } else {
+    lowp = 0;
+  }
   const bool record = S.L.recording && !learned && method == 1;
   if (graph_mode() && !record && (method == 1 || method == 2))
     build_graph<double>(S, iterPREmax, learned | (lowp ? 4 : 0) | (method == 2 ? 8 : 0));
@@ -3150,7 +3210,10 @@ int solve_mixed_reliable(Solver &S, int *Iarray, double *Rarray, int *iter, doub
   const int learned = Iarray[42] == 1 ? 1 : 0;
   S.L.coarse_mode = (Iarray[43] >= 0 && Iarray[43] <= 2) ? Iarray[43] : 0;
   ensure_fp32(S);
-  if (learned) learned_prepare_inference(S);
+  if (learned) {
+    learned_prepare_inference(S);
+    ensure_fp32_pc(S, S.L.sm);
+  }
   if (graph_mode()) build_graph<float>(S, iterPREmax, 2 | learned);
   Range rs("hecmw33_solve_mixed");
   const double t1 = wall();
@@ -3243,7 +3306,7 @@ void launch_mr_sweep(Solver &S, const double *rin, double *zout) {
 // Largest number of CTAs one reduction of the multi-RHS loop uses.
 int mr_max_parts(Solver &S) {
   Precond &P = S.pc;
-  int m = std::max(S.grid_mr(S.A.nslices * 32), S.grid_mr(S.N));
+  int m = std::max(S.grid_amr(), S.grid_mr(S.N));
   if (S.mt_occ > 0) m = std::max(m, std::min(S.mt_ntiles, S.nsm * S.mt_occ));
   if (P.valid && P.kind != 3) {
     const int K = P.lo.lanes;
@@ -3276,7 +3339,7 @@ void launch_mr_precond(Solver &S, int iterpremax) {
     if (it == 1) launch_k(s, copy_kernel<double>, gv, kThreads, S.mzp.p, S.mz.p, n48, nullptr);
     else launch_k(s, add_kernel<double>, gv, kThreads, S.mzp.p, S.mz.p, n48, nullptr);
     if (it == iterpremax) break;
-    launch_k(s, mr_spmv_kernel<1>, S.grid_mr(S.A.nslices * 32), kThreads, S.A.view(), S.mz.p, S.mw.p, S.mr.p, S.mst.p,
+    launch_k(s, mr_spmv_kernel<1, kMrLanes>, S.grid_amr(), kThreads, S.amr_view(), S.mz.p, S.mw.p, S.mr.p, S.mst.p,
                                                                        S.mctl.p, S.mpart.p);
     in = S.mw.p;
   }
@@ -3285,16 +3348,16 @@ void launch_mr_precond(Solver &S, int iterpremax) {
 
 void launch_mr_prologue(Solver &S, int nrhs, cudaGraphConditionalHandle h, int use_cond) {
   cudaStream_t s = S.stream;
-  const int gs = S.grid_mr(S.A.nslices * 32);
+  const int gs = S.grid_amr();
   launch_k(s, mr_init_kernel, 1, 32, S.mst.p, S.mctl.p, S.params.p, nrhs);
-  launch_k(s, mr_spmv_kernel<1>, gs, kThreads, S.A.view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p, S.mpart.p);
+  launch_k(s, mr_spmv_kernel<1, kMrLanes>, gs, kThreads, S.amr_view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p, S.mpart.p);
   launch_k(s, mr_dot_kernel<0>, S.grid_mr(S.N), kThreads, S.mb.p, S.mb.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
   launch_k(s, mr_ctl_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
 }
 
 void launch_mr_iteration(Solver &S, int iterpremax, cudaGraphConditionalHandle h, int use_cond) {
   cudaStream_t s = S.stream;
-  const int gs = S.grid_mr(S.A.nslices * 32), gn = S.grid_mr(S.N);
+  const int gs = S.grid_amr(), gn = S.grid_mr(S.N);
   launch_k(s, mr_iter_begin_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
   launch_mr_precond(S, iterpremax);
   launch_k(s, mr_update_p_kernel, gn, kThreads, S.mz.p, S.mp.p, S.N, S.mst.p, S.mctl.p);
@@ -3303,9 +3366,9 @@ void launch_mr_iteration(Solver &S, int iterpremax, cudaGraphConditionalHandle h
               size_t(S.mt_maxcols) * kRhsStride * sizeof(double), S.A.view(), S.mt_ptr.p, S.mt_cols.p,
               S.mt_lidx.p, S.mt_ntiles, S.mp.p, S.mq.p, S.mst.p, S.mctl.p, S.mpart.p);
   else
-    launch_k(s, mr_spmv_kernel<2>, gs, kThreads, S.A.view(), S.mp.p, S.mq.p, nullptr, S.mst.p, S.mctl.p, S.mpart.p);
+    launch_k(s, mr_spmv_kernel<2, kMrLanes>, gs, kThreads, S.amr_view(), S.mp.p, S.mq.p, nullptr, S.mst.p, S.mctl.p, S.mpart.p);
   launch_k(s, mr_update_xr_kernel, gn, kThreads, S.mx.p, S.mp.p, S.mr.p, S.mq.p, S.N, S.mst.p, S.mctl.p, S.mpart.p);
-  launch_k(s, mr_spmv_kernel<3>, gs, kThreads, S.A.view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p, S.mpart.p);
+  launch_k(s, mr_spmv_kernel<3, kMrLanes>, gs, kThreads, S.amr_view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p, S.mpart.p);
   launch_k(s, mr_ctl_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
 }
 
@@ -3400,6 +3463,20 @@ void build_mr_tiles(Solver &S) {
 
 void ensure_multi_buffers(Solver &S) {
   if (mr_tiled_mode() && S.mt_generation != S.generation) build_mr_tiles(S);
+  if (S.amr_generation != S.generation) {
+    Profile prof{S.N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
+    BlockRows rows;
+    unified_rows(prof, rows);
+    SellLayout lay;
+    build_sell(rows, std::vector<int>{0, S.N}, lay, kMrLanes);
+    S.Amr.upload(lay, S.stream);
+    S.amr_generation = S.generation;
+    S.amr_values = -1;
+  }
+  if (S.amr_values != S.values_version) {
+    S.Amr.pack(S.raw.p, S.stream, S.nsm);
+    S.amr_values = S.values_version;
+  }
   const size_t n48 = size_t(S.N) * kRhsStride;
   for (auto *v : {&S.mb, &S.mx, &S.mr, &S.mz, &S.mp, &S.mq, &S.mw, &S.mzp, &S.mzpos}) v->alloc(n48);
   S.mst.alloc(kMaxRhs);
@@ -3448,7 +3525,7 @@ float run_multi_chunk(Solver &S, int nrhs, const double *dB, double *dX, int ite
   }
   H33_CUDA(cudaEventRecord(S.ev1, s));
   // final true residuals (hecmw_rel_resid_L2_33 per RHS) and the zero-RHS lanes
-  launch_k(s, mr_spmv_kernel<1>, S.grid_mr(S.A.nslices * 32), kThreads, S.A.view(), S.mx.p, S.mw.p, S.mb.p, S.mst.p,
+  launch_k(s, mr_spmv_kernel<1, kMrLanes>, S.grid_amr(), kThreads, S.amr_view(), S.mx.p, S.mw.p, S.mb.p, S.mst.p,
                                                                      S.mctl.p, S.mpart.p);
   launch_k(s, mr_dot_kernel<2>, S.grid_mr(n), kThreads, S.mw.p, S.mw.p, n, S.mst.p, S.mctl.p, S.mpart.p);
   launch_k(s, mr_zero_x_kernel, gp, kThreads, S.mx.p, n, S.mst.p);
@@ -4263,6 +4340,21 @@ HECMW33_API void hecmw33_gpu_colour_schedule(const int *N, const int *indexL, co
   H33_ENTRY_END
 }
 
+HECMW33_API void hecmw33_gpu_smoother_schedule(const int *N, const int *indexL, const int *itemL,
+                                               const int *indexU, const int *itemU, int *ncolor,
+                                               int *colorindex, int *perm, int *ierr) {
+  if (ierr) *ierr = 0;
+  H33_ENTRY_BEGIN
+  const int n = *N;
+  validate(n, n, indexL[n], indexU[n], indexL, itemL, indexU, itemU);
+  Profile prof{n, indexL, itemL, indexU, itemU};
+  std::vector<int> pm, ipm, ci;
+  *ncolor = ordering_greedy(prof, ci, pm, ipm);
+  for (int c = 0; c <= *ncolor; c++) colorindex[c] = ci[c];
+  for (int i = 0; i < n; i++) perm[i] = pm[i] + 1;
+  H33_ENTRY_END
+}
+
 HECMW33_API void hecmw33_gpu_coarse_aggregates(const int *N, const int *indexL, const int *itemL,
                                                const int *indexU, const int *itemU, const int *max_aggregates,
                                                int *n_agg, int *agg, int *ierr) {
@@ -4356,11 +4448,16 @@ HECMW33_API void hecmw33_gpu_time_precond(const int *handle, const int *reps, co
   Solver &S = get(handle);
   DeviceGuard dg(S.device);
   if (!S.has_matrix) throw Failure(HECMW33_ERR_NO_MATRIX, "no matrix");
-  Precond &P = S.pc;
-  if (!P.valid) throw Failure(HECMW33_ERR_BAD_INPUT, "no preconditioner: solve once first");
-  const int lp = (lowp && *lowp && P.kind != 3) ? 1 : 0;
-  if (lp) ensure_lowp(S);
-  const Views<double> V = views(S, 0.0, lp);
+  if (!S.pc.valid) throw Failure(HECMW33_ERR_BAD_INPUT, "no preconditioner: solve once first");
+  const bool smoother = lowp && (*lowp & 2);
+  if (smoother) {
+    if (S.pc.kind != 1) throw Failure(HECMW33_ERR_BAD_INPUT, "the learned smoother follows an SSOR setup");
+    ensure_smoother(S);
+  }
+  Precond &P = smoother ? S.L.sm : S.pc;
+  const int lp = (lowp && (*lowp & 1) && P.kind != 3) ? 1 : 0;
+  if (lp) ensure_lowp(S, P);
+  const Views<double> V = views(S, 0.0, lp, &P);
   const int n = std::max(1, *reps);
   // z = M^-1 r on the resident r (the last solve's residual), one pass (iterPREmax = 1)
   launch_sweep<double, false>(S, V, S.r.p, S.w.p, nullptr);

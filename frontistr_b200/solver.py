@@ -410,12 +410,14 @@ class GpuSolver:
         self._check(err.value, fatal_only=False)
         return ms.value
 
-    def time_precond(self, reps=20, lowp=0):
+    def time_precond(self, reps=20, lowp=0, smoother=False):
         """(ms per application, algorithmic bytes per application) of the resident
-        preconditioner, one pass z = M^-1 r, timed with device events."""
+        preconditioner, one pass z = M^-1 r, timed with device events; smoother=True
+        times the learned preconditioner's SSOR smoother (first-fit colour order)."""
         ms, nbytes = ctypes.c_double(0), ctypes.c_double(0)
         err = ctypes.c_int(0)
-        self.lib.hecmw33_gpu_time_precond(ctypes.byref(self.handle), _i(reps), _i(lowp), ctypes.byref(ms),
+        flags = (1 if lowp else 0) | (2 if smoother else 0)
+        self.lib.hecmw33_gpu_time_precond(ctypes.byref(self.handle), _i(reps), _i(flags), ctypes.byref(ms),
                                           ctypes.byref(nbytes), ctypes.byref(err))
         self._check(err.value, fatal_only=False)
         return ms.value, nbytes.value
@@ -478,6 +480,22 @@ def colour_schedule(m, ncolor_in=10):
     err = ctypes.c_int(0)
     lib.hecmw33_gpu_colour_schedule(_i(n), _ip(m.indexL), _ip(m.itemL), _ip(m.indexU), _ip(m.itemU),
                                     _i(ncolor_in), ctypes.byref(nc), _ip(ci), _ip(perm), ctypes.byref(err))
+    if err.value:
+        raise HecmwSolverError(err.value, last_error())
+    return ci[:nc.value + 1].copy(), perm
+
+
+def smoother_schedule(m):
+    """Host-only colour schedule of the learned preconditioner's SSOR smoother
+    (first-fit colours in node order): (colorindex, perm), as colour_schedule."""
+    lib = gpu_lib()
+    n = m.N
+    nc = ctypes.c_int(0)
+    ci = np.zeros(n + 1, np.int32)
+    perm = np.zeros(n, np.int32)
+    err = ctypes.c_int(0)
+    lib.hecmw33_gpu_smoother_schedule(_i(n), _ip(m.indexL), _ip(m.itemL), _ip(m.indexU), _ip(m.itemU),
+                                      ctypes.byref(nc), _ip(ci), _ip(perm), ctypes.byref(err))
     if err.value:
         raise HecmwSolverError(err.value, last_error())
     return ci[:nc.value + 1].copy(), perm

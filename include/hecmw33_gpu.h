@@ -243,6 +243,16 @@ HECMW33_API void hecmw33_gpu_colour_schedule(const int *N, const int *indexL, co
                                              const int *ncolor_in, int *ncolor, int *colorindex,
                                              int *perm, int *ierr);
 
+/* Host-only (no GPU needed; no counterpart in the reference): the colour schedule of
+ * the learned preconditioner's SSOR smoother (Iarray(43) = 1), first-fit colours in the
+ * node order (each node takes the smallest colour that none of its already coloured
+ * neighbours has; 8 colours on a lexicographically numbered structured hexahedral
+ * mesh), rows ordered by colour and by node inside a colour.  Outputs as
+ * hecmw33_gpu_colour_schedule (colorindex needs N+1 entries, perm N, 1-based ids). */
+HECMW33_API void hecmw33_gpu_smoother_schedule(const int *N, const int *indexL, const int *itemL,
+                                               const int *indexU, const int *itemU, int *ncolor,
+                                               int *colorindex, int *perm, int *ierr);
+
 /* Host-only (no GPU needed; no counterpart in the reference): the aggregates of the
  * node graph on which the learned two-level preconditioner (Iarray(43) = 1) builds its
  * coarse space.  Greedy passes (a node whose closed neighbourhood is free roots an
@@ -260,6 +270,9 @@ HECMW33_API void hecmw33_gpu_coarse_aggregates(const int *N, const int *indexL, 
  * symmetric two-grid cycle
  *     zs = SSOR(r);  zc = zs + P Ac^-1 P^T (r - A zs);  z = zc + SSOR(r - A zc),
  * Ac = P^T A P, on aggregates of the node graph (hecmw33_gpu_coarse_aggregates).  The
+ * smoother SSOR is the solve's (same blocks, same SIGMA_DIAG) on its own layouts in
+ * first-fit colour order (hecmw33_gpu_smoother_schedule): not bound to the reference's
+ * schedule, it needs far fewer colour launches per sweep.  The
  * prolongator is a smoothed aggregation P = (I - Omega D^-1 A) P0 (P0: the aggregates'
  * translations, zero on constrained DOFs; D: the diagonal blocks) whose per-DOF
  * smoothing weights Omega = sigmoid(out) come from a 3-layer message-passing network
@@ -282,8 +295,9 @@ HECMW33_API void hecmw33_gpu_learn_record(const int *handle, const int *enable, 
                                           int *npairs, int *ierr);
 
 /* Trains the network on the recorded pairs with the handle's GPU kernels (forward,
- * backward, Adam; FP32 master weights).  Each pair is first smoothed by one SSOR step
- * (e' = e - SSOR(r), r' = A e': the error the coarse space has to capture); the loss
+ * backward, Adam; FP32 master weights).  Each pair is first smoothed by one step of
+ * the smoother (e' = e - SSOR(r), r' = A e': the error the coarse space has to
+ * capture); the loss
  * is the mean share of a pair's error energy outside the coarse space,
  * (e'^T r' - (P^T r')^T Ac^-1 P^T r') / (e'^T r'), with Ac rebuilt and inverted at
  * every step.  loss[0]/loss[1]: mean loss before the first and after the last of
@@ -333,8 +347,10 @@ HECMW33_API void hecmw33_gpu_time_spmv(const int *handle, const int *reps, doubl
  * z = M^-1 r (hecmw_precond_apply with iterPREmax = 1, hecmw_precond.f90:86-172; for
  * SSOR the forward and backward colour sweeps of hecmw_precond_SSOR_33.F90:302-405, for
  * ILU(p) the level-scheduled sweeps of hecmw_precond_BILU_33.f90), on the last solve's
- * residual, with device events on the handle's stream.  *lowp = 1 times the
- * BF16-stored factors of precision mode 1.  *ms_per_apply receives the average;
+ * residual, with device events on the handle's stream.  *lowp bit 0 times the
+ * BF16-stored factors of precision mode 1; bit 1 times the learned preconditioner's
+ * smoother (the same SSOR on its own layouts in first-fit colour order, Iarray(43) = 1)
+ * instead of the solve's SSOR.  *ms_per_apply receives the average;
  * *bytes_per_apply (may be NULL) the algorithmic bytes of one application:
  * 76 B per off-diagonal block (22 B with *lowp), the diagonal LU read by both sweeps
  * (72 B per node each, 36 B with *lowp), both triangles' row pointers and 96 B of

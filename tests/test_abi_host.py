@@ -13,7 +13,7 @@ from frontistr_b200 import _abi
 from frontistr_b200._lib import gpu_lib
 from frontistr_b200.matrix import HecMatrix
 from frontistr_b200.mesh import box_system
-from frontistr_b200.solver import HecmwSolverError, colour_schedule, last_error
+from frontistr_b200.solver import HecmwSolverError, colour_schedule, last_error, smoother_schedule
 from oracle_ctypes import Oracle
 from test_oracle_golden import golden_system
 
@@ -97,6 +97,42 @@ def test_single_node_and_disconnected_profiles():
     ci, perm = colour_schedule(m2)
     ci_o, perm_o = oracle_schedule(m2, 10)
     assert np.array_equal(ci, ci_o) and np.array_equal(perm, perm_o)
+
+
+def _neighbours(m):
+    nb = [set() for _ in range(m.N)]
+    for index, item in ((m.indexL, m.itemL), (m.indexU, m.itemU)):
+        for i in range(m.N):
+            for k in range(index[i], index[i + 1]):
+                nb[i].add(int(item[k]) - 1)
+    return nb
+
+
+@pytest.mark.parametrize("case", ["tet4", "box_small", "box_jitter"])
+def test_smoother_schedule_is_a_first_fit_colouring(case):
+    """The learned preconditioner's smoother colours: every node has the smallest
+    colour none of its lower-numbered neighbours has, no two neighbours share one,
+    rows by colour then node; 8 colours on a structured box."""
+    if case == "tet4":
+        _, m = golden_system()
+    elif case == "box_small":
+        m = box_system(6, 5, 7)
+    else:
+        m = box_system(5, 6, 4, jitter=0.2, seed=3)
+    ci, perm = smoother_schedule(m)
+    nc = len(ci) - 1
+    colour = np.empty(m.N, np.int64)
+    for c in range(nc):
+        colour[perm[ci[c]:ci[c + 1]] - 1] = c
+        assert np.all(np.diff(perm[ci[c]:ci[c + 1]]) > 0)  # node order inside a colour
+    assert sorted(perm.tolist()) == list(range(1, m.N + 1))
+    nb = _neighbours(m)
+    for i in range(m.N):
+        assert all(colour[j] != colour[i] for j in nb[i] if j != i)
+        lower = {int(colour[j]) for j in nb[i] if j < i}
+        assert colour[i] == min(set(range(len(lower) + 1)) - lower)
+    if case.startswith("box"):
+        assert nc == 8
 
 
 def test_rel_resid_noalloc_rejects_null_pointers():
