@@ -81,6 +81,10 @@ def parse():
     ap.add_argument("--profile-coarse", type=int, default=-1,
                     help="with --profile-solve: the two-level preconditioner with these smoothing weights "
                          "(Iarray(44): 1 none, 2 one half; no training needed)")
+    ap.add_argument("--profile-e2e", action="store_true",
+                    help="one drop-in call with host buffers and a forced numeric rebuild (learned + mode 1, "
+                         "network trained for 2 steps on 1 recorded solve), the last of 3 inside "
+                         "cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--profile-multi", action="store_true",
                     help="one 16-load-case solve capped at 3 CG iterations, nothing printed (profiling)")
     ap.add_argument("--profile-batch", action="store_true",
@@ -774,6 +778,27 @@ def main():
         with BatchSolver() as bs:
             bs.set_matrix(big, sys_ptr, ia, ra)
             bs.solve(big.B, np.zeros(3 * big.N), ia, ra)
+        return
+    if args.profile_e2e:
+        solver.learn_record(1, max_pairs=4)
+        rec = solver.solve(m.copy())
+        solver.learn_record(0)
+        solver.learn_train(steps=2, lr=5e-3)
+        for i in range(3):
+            mm = m.copy()
+            mm.Iarray[97] = 0
+            mm.Iarray[96] = 2  # numeric rebuild, as at a new Newton increment
+            mm.Iarray[41] = 1
+            mm.Iarray[42] = 1
+            torch.cuda.synchronize()
+            if i == 2:
+                torch.cuda.profiler.start()
+            rec = solver.solve(mm)
+            torch.cuda.synchronize()
+            if i == 2:
+                torch.cuda.profiler.stop()
+            if rec["error"] != 0:
+                raise SystemExit("solve failed: %r" % rec)
         return
     if args.profile_solve:
         mm = m.copy()
