@@ -316,7 +316,8 @@ __global__ void __launch_bounds__(1024) gj_diag_kernel(double *__restrict__ M, i
 // G(i, :) = M(i, K) Dinv and M(i, K) = -G(i, :) for rows i outside K; M(K, K) = Dinv
 // and G = 0 on the rows of K.  Warp per row: lane l holds M(i, k0 + l) and
 // M(i, k0 + 32 + l), broadcast by shuffles; lane l computes columns l and l + 32.
-// G is n x kGjBlock, row-major.
+// G is stored transposed, GT(s, i) = G(i, s) at GT[s * n + i], so that the update
+// kernel's panel loads run along i.
 __global__ void __launch_bounds__(256) gj_col_kernel(double *__restrict__ M, int n, int k0, int nb,
                                                      const double *__restrict__ dinv, double *__restrict__ G) {
   __shared__ double D[kGjBlock][kGjBlock];
@@ -326,11 +327,11 @@ __global__ void __launch_bounds__(256) gj_col_kernel(double *__restrict__ M, int
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
     double *row = M + size_t(i) * n + k0;
-    double *g = G + size_t(i) * kGjBlock;
+    double *g = G + i;  // column i of GT
     if (i >= k0 && i < k0 + nb) {
       for (int s = lane; s < nb; s += 32) {
         row[s] = D[i - k0][s];
-        g[s] = 0.0;
+        g[size_t(s) * n] = 0.0;
       }
       continue;
     }
@@ -344,59 +345,68 @@ __global__ void __launch_bounds__(256) gj_col_kernel(double *__restrict__ M, int
       g1 += mt * D[t][s1];
     }
     if (lane < nb) {
-      g[lane] = g0;
+      g[size_t(lane) * n] = g0;
       row[lane] = -g0;
     }
     if (lane + 32 < nb) {
-      g[lane + 32] = g1;
+      g[size_t(lane + 32) * n] = g1;
       row[lane + 32] = -g1;
     }
   }
 }
 
 // M(i, j) -= G(i, :) M(K, j) for i, j outside K (M(K, j) is still the old row panel).
-// Tiles of 128 rows x 64 columns, 256 threads with 8 x 4 outputs each; the panels
-// go through shared memory 16 pivots at a time.
-constexpr int kGjTileI = 128, kGjTileJ = 64, kGjChunk = 16;
-__global__ void __launch_bounds__(256) gj_update_kernel(double *__restrict__ M, int n, int k0, int nb,
-                                                        const double *__restrict__ G) {
-  __shared__ __align__(16) double Gs[kGjChunk][kGjTileI + 4];  // Gs[k][i] = G(i0 + i, kc + k)
-  __shared__ __align__(16) double Bs[kGjChunk][kGjTileJ];      // Bs[k][j] = M(k0 + kc + k, j0 + j)
+// Tiles of 128 rows x 64 columns, 256 threads with 8 x 4 outputs each, two CTAs per
+// SM: the tile's values are loaded into the accumulators first, then both panels of
+// the whole pivot block go to shared memory at once (GT along i, the row panel along
+// j: contiguous loads and conflict-free stores), one barrier, nb rank-1 steps.
+constexpr int kGjTileI = 128, kGjTileJ = 64;
+constexpr int kGjGs = kGjTileI + 4, kGjBs = kGjTileJ + 4;  // padded panel rows (doubles)
+constexpr size_t kGjUpdateSmem = sizeof(double) * size_t(kGjBlock) * (kGjGs + kGjBs);
+__global__ void __launch_bounds__(256, 2) gj_update_kernel(double *__restrict__ M, int n, int k0, int nb,
+                                                           const double *__restrict__ GT) {
+  extern __shared__ __align__(16) double gj_smem[];
+  double *Gs = gj_smem;                          // Gs[k][i] = G(i0 + i, k)
+  double *Bs = gj_smem + kGjBlock * kGjGs;       // Bs[k][j] = M(k0 + k, j0 + j)
   const int i0 = blockIdx.y * kGjTileI, j0 = blockIdx.x * kGjTileJ;
   // a tile inside the pivot rows or columns has nothing to update
   if ((i0 >= k0 && i0 + kGjTileI <= k0 + nb) || (j0 >= k0 && j0 + kGjTileJ <= k0 + nb)) return;
   const int tr = threadIdx.x >> 4, tc = threadIdx.x & 15;
   double acc[8][4];
 #pragma unroll
-  for (int u = 0; u < 8; u++)
+  for (int u = 0; u < 8; u++) {
+    const int i = i0 + tr * 8 + u;
 #pragma unroll
-    for (int v = 0; v < 4; v++) acc[u][v] = 0.0;
-  for (int kc = 0; kc < nb; kc += kGjChunk) {
-    for (int e = threadIdx.x; e < kGjTileI * kGjChunk; e += blockDim.x) {
-      const int i = e / kGjChunk, k = e % kGjChunk;
-      Gs[k][i] = (i0 + i < n && kc + k < nb) ? G[size_t(i0 + i) * kGjBlock + kc + k] : 0.0;
+    for (int v = 0; v < 4; v++) {
+      const int j = j0 + tc * 4 + v;
+      acc[u][v] = (i < n && j < n) ? M[size_t(i) * n + j] : 0.0;
     }
-    for (int e = threadIdx.x; e < kGjChunk * kGjTileJ; e += blockDim.x) {
-      const int k = e / kGjTileJ, j = e % kGjTileJ;
-      Bs[k][j] = (j0 + j < n && kc + k < nb) ? M[size_t(k0 + kc + k) * n + j0 + j] : 0.0;
-    }
-    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < kGjBlock * kGjTileI; e += blockDim.x) {
+    const int k = e / kGjTileI, i = e % kGjTileI;
+    Gs[k * kGjGs + i] = (i0 + i < n && k < nb) ? GT[size_t(k) * n + i0 + i] : 0.0;
+  }
+  for (int e = threadIdx.x; e < kGjBlock * kGjTileJ; e += blockDim.x) {
+    const int k = e / kGjTileJ, j = e % kGjTileJ;
+    Bs[k * kGjBs + j] = (j0 + j < n && k < nb) ? M[size_t(k0 + k) * n + j0 + j] : 0.0;
+  }
+  __syncthreads();
 #pragma unroll 4
-    for (int k = 0; k < kGjChunk; k++) {
-      const double2 a01 = *reinterpret_cast<const double2 *>(&Gs[k][tr * 8]);
-      const double2 a23 = *reinterpret_cast<const double2 *>(&Gs[k][tr * 8 + 2]);
-      const double2 a45 = *reinterpret_cast<const double2 *>(&Gs[k][tr * 8 + 4]);
-      const double2 a67 = *reinterpret_cast<const double2 *>(&Gs[k][tr * 8 + 6]);
-      const double2 b01 = *reinterpret_cast<const double2 *>(&Bs[k][tc * 4]);
-      const double2 b23 = *reinterpret_cast<const double2 *>(&Bs[k][tc * 4 + 2]);
-      const double a[8] = {a01.x, a01.y, a23.x, a23.y, a45.x, a45.y, a67.x, a67.y};
-      const double b[4] = {b01.x, b01.y, b23.x, b23.y};
+  for (int k = 0; k < nb; k++) {
+    const double *gk = Gs + k * kGjGs + tr * 8;
+    const double *bk = Bs + k * kGjBs + tc * 4;
+    const double2 a01 = *reinterpret_cast<const double2 *>(gk);
+    const double2 a23 = *reinterpret_cast<const double2 *>(gk + 2);
+    const double2 a45 = *reinterpret_cast<const double2 *>(gk + 4);
+    const double2 a67 = *reinterpret_cast<const double2 *>(gk + 6);
+    const double2 b01 = *reinterpret_cast<const double2 *>(bk);
+    const double2 b23 = *reinterpret_cast<const double2 *>(bk + 2);
+    const double a[8] = {a01.x, a01.y, a23.x, a23.y, a45.x, a45.y, a67.x, a67.y};
+    const double b[4] = {b01.x, b01.y, b23.x, b23.y};
 #pragma unroll
-      for (int u = 0; u < 8; u++)
+    for (int u = 0; u < 8; u++)
 #pragma unroll
-        for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], b[v], acc[u][v]);
-    }
-    __syncthreads();
+      for (int v = 0; v < 4; v++) acc[u][v] = fma(-a[u], b[v], acc[u][v]);
   }
 #pragma unroll
   for (int u = 0; u < 8; u++) {
@@ -406,7 +416,7 @@ __global__ void __launch_bounds__(256) gj_update_kernel(double *__restrict__ M, 
     for (int v = 0; v < 4; v++) {
       const int j = j0 + tc * 4 + v;
       if (j >= n || (j >= k0 && j < k0 + nb)) continue;
-      M[size_t(i) * n + j] -= acc[u][v];
+      M[size_t(i) * n + j] = acc[u][v];
     }
   }
 }

@@ -673,13 +673,15 @@ __global__ void __launch_bounds__(kThreads) sweep_fwd_uni_kernel(SellView<TV> L,
 // Backward sweep of one colour: zpos(pos) -= LU^-1 ( sum_upper A zpos(col) ), the
 // finished rows also written to z in node order; FUSE_RHO accumulates {r}{z} and the
 // last launch's last CTA runs the RHO finisher (hecmw_precond_SSOR_33.F90:353-405).
+// dpos (may be null): the row's correction LU^-1 (...) = y - z (y the forward value),
+// in colour-position order, for lower_resid_kernel.
 template <class R, class TV, class TA, int K, bool FUSE_RHO>
 __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U, const int *__restrict__ perm,
                                                                  const TA *__restrict__ alu, int npos,
                                                                  const R *__restrict__ r, R *__restrict__ z,
                                                                  R *__restrict__ zpos, int nslices, RunShape sh,
                                                                  CgState *st, double *partials, int part_base,
-                                                                 int part_total, int pre) {
+                                                                 int part_total, int pre, R *__restrict__ dpos) {
   colour_prologue<TV, TA, K>(U, alu, npos, nslices, sh, pre);
   if (st && st->done) return;
   const int lane = threadIdx.x & 31;
@@ -711,6 +713,11 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U,
       z[3 * node] = z0;
       z[3 * node + 1] = z1;
       z[3 * node + 2] = z2;
+      if (dpos) {
+        dpos[3 * row] = x1;
+        dpos[3 * row + 1] = x2;
+        dpos[3 * row + 2] = x3;
+      }
       if (FUSE_RHO)
         dot += double(r[3 * node]) * double(z0) + double(r[3 * node + 1]) * double(z1) +
                double(r[3 * node + 2]) * double(z2);
@@ -719,6 +726,34 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U,
   if (FUSE_RHO)
     reduce_finish(dot, partials, part_base + blockIdx.x, part_total, &st->ticket[0],
                   [&](double v) { fin_rho(st, v); });
+}
+
+// w = r - A z for z = SSOR(r) from a zero start with unit SIGMA_DIAG, without A: the
+// forward sweep solves (D + L) y = r, the backward (D + U) z = D y, so
+// r - A z = (D + L) y - L z - (D + U) z = L (y - z), and the backward sweep wrote
+// d = y - z (dpos).  One pass over the lower layout (all colours), warp per slice;
+// w in node order.
+template <class R, class TV, int K>
+__global__ void __launch_bounds__(kThreads) lower_resid_kernel(SellView<TV> L, const int *__restrict__ perm,
+                                                               const R *__restrict__ dpos, R *__restrict__ w,
+                                                               const CgState *st) {
+  pdl_entry();
+  if (st && st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int roff = lane / K;
+  const bool leader = (lane & (K - 1)) == 0;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < L.nslices; s += nwarps) {
+    const bool act = roff < L.nrows[s] && leader;
+    R y0 = R(0), y1 = R(0), y2 = R(0);
+    slice_gemv_u<R, TV, K, false>(L, L.slot0[s], L.len[s], lane, dpos, y0, y1, y2);
+    if (act) {
+      const int node = perm[L.row0[s] + roff];
+      w[3 * node] = y0;
+      w[3 * node + 1] = y1;
+      w[3 * node + 2] = y2;
+    }
+  }
 }
 
 // ---- symmetric diagonal scaling (SCALING=YES, hecmw_solver_scaling_33.f90) ----

@@ -380,6 +380,7 @@ struct Solver {
   DevSell<double> A;
   // vectors and scalars
   DevArray<double> b, x, r, z, p, q, w, zp;
+  DevArray<double> dpos;  // the learned smoother's y - z per colour position (lower_resid_kernel)
   DevArray<double> partials;
   DevArray<CgState> state;
   DevArray<CgParams> params;
@@ -1012,7 +1013,7 @@ RunShape run_shape(const DevSell<double> &D, int g) {
 
 template <class R, class TV, class TA, bool FUSE_RHO, int K>
 void launch_sweep_uni(Solver &S, const Precond &P, const SellView<TV> &lo, const SellView<TV> &up,
-                      const TA *alu_f, const R *rin, R *zout, R *zpos, CgState *st) {
+                      const TA *alu_f, const R *rin, R *zout, R *zpos, CgState *st, R *dpos = nullptr) {
   cudaStream_t s = S.stream;
   const int gf = int(P.lo.group_slice.size()) - 1;
   for (int g = 0; g < gf; g++) {
@@ -1033,7 +1034,8 @@ void launch_sweep_uni(Solver &S, const Precond &P, const SellView<TV> &lo, const
     // ticket count stays exact
     constexpr int pre = sweep_pre<TV>();
     launch_kp(s, true, sweep_bwd_uni_kernel<R, TV, TA, K, FUSE_RHO>, grid, kThreads, up,
-              P.perm_fwd.p, alu_f, S.N, rin, zout, zpos, ns, run_shape(P.up, g), st, S.partials.p, base, total, pre);
+              P.perm_fwd.p, alu_f, S.N, rin, zout, zpos, ns, run_shape(P.up, g), st, S.partials.p, base, total, pre,
+              dpos);
     base += grid;
   }
 }
@@ -1041,7 +1043,8 @@ void launch_sweep_uni(Solver &S, const Precond &P, const SellView<TV> &lo, const
 // Lanes per row are 4, 8 or 16 (sweep_lanes()).
 template <class R, class TV, class TA, bool FUSE_RHO>
 void launch_sweep_t(Solver &S, const Precond &P, const SellView<TV> &lo, const SellView<TV> &up,
-                    const TA *alu_f, const TA *alu_b, const R *rin, R *zout, R *zpos, CgState *st) {
+                    const TA *alu_f, const TA *alu_b, const R *rin, R *zout, R *zpos, CgState *st,
+                    R *dpos = nullptr) {
   if (P.kind == 3) {
     launch_k(S.stream, diag_kernel<R, TA, FUSE_RHO>, S.grid_vec(), kThreads, alu_f, S.N, rin, zout, st,
              S.partials.p);
@@ -1049,9 +1052,9 @@ void launch_sweep_t(Solver &S, const Precond &P, const SellView<TV> &lo, const S
   }
   if (P.pos_cols) {
     switch (P.lo.lanes) {
-      case 8: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 8>(S, P, lo, up, alu_f, rin, zout, zpos, st);
-      case 16: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 16>(S, P, lo, up, alu_f, rin, zout, zpos, st);
-      default: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 4>(S, P, lo, up, alu_f, rin, zout, zpos, st);
+      case 8: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 8>(S, P, lo, up, alu_f, rin, zout, zpos, st, dpos);
+      case 16: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 16>(S, P, lo, up, alu_f, rin, zout, zpos, st, dpos);
+      default: return launch_sweep_uni<R, TV, TA, FUSE_RHO, 4>(S, P, lo, up, alu_f, rin, zout, zpos, st, dpos);
     }
   }
   switch (P.lo.lanes) {
@@ -1061,13 +1064,29 @@ void launch_sweep_t(Solver &S, const Precond &P, const SellView<TV> &lo, const S
   }
 }
 
+// dpos (may be null; multicolour layouts only): the backward sweep's correction y - z
+// per colour position, for lower_resid_kernel.
 template <class R, bool FUSE_RHO>
-void launch_sweep(Solver &S, const Views<R> &V, const R *rin, R *zout, CgState *st) {
+void launch_sweep(Solver &S, const Views<R> &V, const R *rin, R *zout, CgState *st, R *dpos = nullptr) {
   if (V.lowp)
     launch_sweep_t<R, __nv_bfloat16, float, FUSE_RHO>(S, *V.pc, V.lo16, V.up16, V.alu32_f, V.alu32_b, rin, zout,
-                                                      V.zpos, st);
+                                                      V.zpos, st, dpos);
   else
-    launch_sweep_t<R, R, R, FUSE_RHO>(S, *V.pc, V.lo, V.up, V.alu_f, V.alu_b, rin, zout, V.zpos, st);
+    launch_sweep_t<R, R, R, FUSE_RHO>(S, *V.pc, V.lo, V.up, V.alu_f, V.alu_b, rin, zout, V.zpos, st, dpos);
+}
+
+// w = r - A z after z = launch_sweep(r) with dpos: lower_resid_kernel over the
+// preconditioner's lower layout, in its storage (BF16 values in precision mode 1).
+template <class TV>
+void launch_lower_resid(Solver &S, const Precond &P, const SellView<TV> &lo, const double *dpos, double *w,
+                        CgState *st) {
+  const int grid = std::max(1, std::min((P.lo.nslices + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * S.occ_sweep_uni));
+  const CgState *cst = st;
+  switch (P.lo.lanes) {
+    case 8: launch_k(S.stream, lower_resid_kernel<double, TV, 8>, grid, kThreads, lo, P.perm_fwd.p, dpos, w, cst); break;
+    case 16: launch_k(S.stream, lower_resid_kernel<double, TV, 16>, grid, kThreads, lo, P.perm_fwd.p, dpos, w, cst); break;
+    default: launch_k(S.stream, lower_resid_kernel<double, TV, 4>, grid, kThreads, lo, P.perm_fwd.p, dpos, w, cst); break;
+  }
 }
 
 // hecmw_precond_apply (hecmw_precond.f90:86-172): z = M^-1 r with iterPREmax passes.
@@ -1208,6 +1227,16 @@ void launch_coarse(Solver &S, const R *zs, const R *r, R *z, CgState *st);
 template <class R>
 void launch_coarse_cycle(Solver &S, const R *zs, R *w, R *zc, CgState *st);
 
+// HECMW33_LOWER_RESID=0: the two-grid cycle's residual r - A zs by an SpMV (with the
+// FP32 copy of A in precision mode 1) instead of lower_resid_kernel.
+bool lower_resid_mode() {
+  static const bool v = [] {
+    const char *e = std::getenv("HECMW33_LOWER_RESID");
+    return !(e && e[0] == '0');
+  }();
+  return v;
+}
+
 // HECMW33_COARSE_FORM: 0 (default) the symmetric two-grid form, 1 the additive form.
 // Measured on the 100^3 cube (BF16-stored SSOR, omega = 1/2): two-grid 62 iterations,
 // additive 115; the two-grid form is the one whose convergence the training loss
@@ -1244,12 +1273,28 @@ void precond_resid(Solver &S, const Views<R> &V, const R *x, R *y) {
 template <class R>
 void launch_learned_precond(Solver &S, const Views<R> &V, CgState *st) {
   cudaStream_t s = S.stream;
-  launch_sweep<R, false>(S, V, V.r, V.zs, st);
   if (coarse_form() == 1) {
+    launch_sweep<R, false>(S, V, V.r, V.zs, st);
     launch_coarse<R>(S, V.zs, V.r, V.z, st);
     return;
   }
-  precond_resid<R>(S, V, V.zs, V.w);
+  // w = r - A zs: from the pre-smoothing sweep's correction and the smoother's lower
+  // triangle when the identity holds with A's own values (multicolour layout, unit
+  // SIGMA_DIAG, FP64 smoother), else by an SpMV.  With the BF16-stored smoother the
+  // identity would give the residual of the BF16 operator instead (measured: 3 more
+  // iterations on a 16x16x32 box), so precision mode 1 keeps the SpMV.
+  bool lower = false;
+  if constexpr (std::is_same<R, double>::value)
+    lower = !V.lowp && V.pc->pos_cols && V.pc->sigma == 1.0 && S.dpos.n == size_t(S.n3()) && lower_resid_mode();
+  if (lower) {
+    if constexpr (std::is_same<R, double>::value) {
+      launch_sweep<R, false>(S, V, V.r, V.zs, st, S.dpos.p);
+      launch_lower_resid(S, *V.pc, V.lo, S.dpos.p, V.w, st);
+    }
+  } else {
+    launch_sweep<R, false>(S, V, V.r, V.zs, st);
+    precond_resid<R>(S, V, V.zs, V.w);
+  }
   launch_coarse_cycle<R>(S, V.zs, V.w, V.zp, st);  // zp = zc, w = r - A zc
   launch_sweep<R, false>(S, V, V.w, V.z, st);
   launch_k(s, coarse_post_kernel<R>, S.grid_vec(), kThreads, static_cast<const R *>(V.zp),
@@ -1718,12 +1763,13 @@ bool coarse_operator(Solver &S, const float *omega) {
   launch_k(s, coarse_ac_kernel, std::max(1, S.nsm * 8), kThreads, cv);
   coarse_zero_diag_kernel<<<std::max(1, (C.nc + 255) / 256), 256, 0, s>>>(C.ac.p, C.nc);
   const int n = C.nc;
+  H33_CUDA(cudaFuncSetAttribute(gj_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGjUpdateSmem)));
   const dim3 tiles(unsigned((n + kGjTileJ - 1) / kGjTileJ), unsigned((n + kGjTileI - 1) / kGjTileI));
   for (int k0 = 0; k0 < n; k0 += kGjBlock) {
     const int nb = std::min(kGjBlock, n - k0);
     gj_diag_kernel<<<1, 1024, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p, C.err.p);
     gj_col_kernel<<<std::max(1, (n + 7) / 8), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p, C.gjc.p);
-    gj_update_kernel<<<tiles, 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjc.p);
+    gj_update_kernel<<<tiles, 256, kGjUpdateSmem, s>>>(C.ac.p, n, k0, nb, C.gjc.p);
     gj_row_kernel<<<std::max(1, (n + 15) / 16), 128, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p);
   }
   // FP32 copies for the application
@@ -1868,6 +1914,7 @@ void learned_prepare_inference(Solver &S) {
   }
   const size_t n3 = size_t(S.n3());
   S.zs.alloc(n3);
+  S.dpos.alloc(n3);
   S.rold.alloc(n3);
   S.zsf.alloc(n3);
   S.roldf.alloc(n3);
@@ -3251,29 +3298,30 @@ int solve_mixed_reliable(Solver &S, int *Iarray, double *Rarray, int *iter, doub
 // Multi-RHS CG: up to kMaxRhs load cases per pass over the matrix (h33_multi.cuh).
 
 template <int K, bool FUSE_RHO, bool POS>
-void launch_mr_sweep_k(Solver &S, const double *rin, double *zout) {
+void launch_mr_sweep_k(Solver &S, const DevSell<double> &Lo, const DevSell<double> &Up, const double *rin,
+                       double *zout) {
   Precond &P = S.pc;
   cudaStream_t s = S.stream;
   const int *perm_b = P.alu_shared ? P.perm_fwd.p : P.perm_bwd.p;
   const double *alu_b = P.alu_shared ? P.alu_fwd.p : P.alu_bwd.p;
   MultiCtl *ctl = S.mctl.p;
-  const SellView<double> lo = P.lo.view(), up = P.up.view();
-  const int gf = int(P.lo.group_slice.size()) - 1;
+  const SellView<double> lo = Lo.view(), up = Up.view();
+  const int gf = int(Lo.group_slice.size()) - 1;
   for (int g = 0; g < gf; g++) {
-    const int sb = P.lo.group_slice[g], se = P.lo.group_slice[g + 1];
+    const int sb = Lo.group_slice[g], se = Lo.group_slice[g + 1];
     if (se <= sb) continue;
     launch_k(s, mr_sweep_fwd_kernel<K, POS>, S.grid_mr((se - sb) * (32 / K)), kThreads, 
         lo, P.perm_fwd.p, P.alu_fwd.p, S.N, rin, zout, S.mzpos.p, sb, se, ctl);
   }
-  const int gb = int(P.up.group_slice.size()) - 1;
+  const int gb = int(Up.group_slice.size()) - 1;
   int total = 0;
   for (int g = gb - 1; g >= 0; g--) {
-    const int sb = P.up.group_slice[g], se = P.up.group_slice[g + 1];
+    const int sb = Up.group_slice[g], se = Up.group_slice[g + 1];
     total += S.grid_mr(std::max(se - sb, 1) * (32 / K));
   }
   int base = 0;
   for (int g = gb - 1; g >= 0; g--) {
-    const int sb = P.up.group_slice[g], se = P.up.group_slice[g + 1];
+    const int sb = Up.group_slice[g], se = Up.group_slice[g + 1];
     const int grid = S.grid_mr(std::max(se - sb, 1) * (32 / K));
     launch_k(s, mr_sweep_bwd_kernel<K, FUSE_RHO, POS>, grid, kThreads, up, perm_b, alu_b, S.N, rin, zout, S.mzpos.p,
                                                                      sb, se, S.mst.p, ctl, S.mpart.p, base, total);
@@ -3291,15 +3339,15 @@ void launch_mr_sweep(Solver &S, const double *rin, double *zout) {
   }
   if (P.pos_cols) {
     switch (P.lo.lanes) {
-      case 4: return launch_mr_sweep_k<4, FUSE_RHO, true>(S, rin, zout);
-      case 16: return launch_mr_sweep_k<16, FUSE_RHO, true>(S, rin, zout);
-      default: return launch_mr_sweep_k<8, FUSE_RHO, true>(S, rin, zout);
+      case 4: return launch_mr_sweep_k<4, FUSE_RHO, true>(S, P.lo, P.up, rin, zout);
+      case 16: return launch_mr_sweep_k<16, FUSE_RHO, true>(S, P.lo, P.up, rin, zout);
+      default: return launch_mr_sweep_k<8, FUSE_RHO, true>(S, P.lo, P.up, rin, zout);
     }
   }
   switch (P.lo.lanes) {
-    case 4: return launch_mr_sweep_k<4, FUSE_RHO, false>(S, rin, zout);
-    case 16: return launch_mr_sweep_k<16, FUSE_RHO, false>(S, rin, zout);
-    default: return launch_mr_sweep_k<8, FUSE_RHO, false>(S, rin, zout);
+    case 4: return launch_mr_sweep_k<4, FUSE_RHO, false>(S, P.lo, P.up, rin, zout);
+    case 16: return launch_mr_sweep_k<16, FUSE_RHO, false>(S, P.lo, P.up, rin, zout);
+    default: return launch_mr_sweep_k<8, FUSE_RHO, false>(S, P.lo, P.up, rin, zout);
   }
 }
 
@@ -3309,11 +3357,12 @@ int mr_max_parts(Solver &S) {
   int m = std::max(S.grid_amr(), S.grid_mr(S.N));
   if (S.mt_occ > 0) m = std::max(m, std::min(S.mt_ntiles, S.nsm * S.mt_occ));
   if (P.valid && P.kind != 3) {
-    const int K = P.lo.lanes;
+    const DevSell<double> &U = P.up;
+    const int K = U.lanes;
     int total = 0;
-    const int gb = int(P.up.group_slice.size()) - 1;
+    const int gb = int(U.group_slice.size()) - 1;
     for (int g = 0; g < gb; g++)
-      total += S.grid_mr(std::max(P.up.group_slice[g + 1] - P.up.group_slice[g], 1) * (32 / K));
+      total += S.grid_mr(std::max(U.group_slice[g + 1] - U.group_slice[g], 1) * (32 / K));
     m = std::max(m, total);
   }
   return m;
