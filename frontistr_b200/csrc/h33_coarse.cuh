@@ -259,12 +259,19 @@ __global__ void coarse_zero_diag_kernel(double *__restrict__ ac, int nc) {
 
 // ---- in-place inversion of the SPD coarse matrix: blocked Gauss-Jordan ----------
 // For each block K of kGjBlock pivots (no pivoting: Ac is SPD), with A = M_KK,
-// B = M_Kj, C = M_iK, E = M_ij (i, j not in K):
-//   gj_diag:   Dinv = A^-1                                   (one CTA)
-//   gj_col:    G = C Dinv (saved);  M_iK = -G;  M_KK = Dinv
-//   gj_update: M_ij -= G_i B_j                               (B still the old row panel)
-//   gj_row:    M_Kj = Dinv B_j
-// After the last block M holds Ac^-1.
+// B = M_Kj, C = M_iK, E = M_ij (i, j not in K), Gauss-Jordan makes
+//   M_KK = A^-1,  M_Kj = A^-1 B,  M_iK = -C A^-1,  M_ij = E - C A^-1 B.
+// For symmetric A the matrix stays symmetric, except that the blocks between pivoted
+// and not yet pivoted indices are antisymmetric (M_ab = -M_ba^T for a pivoted, b not).
+// Only the lower triangle is kept up to date (half the update work); an upper entry
+// is read from its mirror with that sign:
+//   gj_diag:   Dinv = A^-1, A read from the lower triangle     (one CTA)
+//   gj_col:    C_i from the lower triangle (row K for i before K, sign -1), G_i = C_i Dinv,
+//              B_j = s_j C_j (s_j = -1 before K, +1 after: the old row panel), the new
+//              column panel -G into the lower triangle (row K for i before K), M_KK = Dinv
+//   gj_update: M_ij -= G_i B_j for i >= j outside K
+// and after the last block (all pivoted, symmetric again) gj_mirror copies the lower
+// triangle onto the upper.  Then M holds Ac^-1.
 constexpr int kGjBlock = 64;
 
 // Dinv = M_KK^-1 by unblocked Gauss-Jordan in shared memory (one CTA of 1024
@@ -277,7 +284,8 @@ __global__ void __launch_bounds__(1024) gj_diag_kernel(double *__restrict__ M, i
 #pragma unroll
   for (int v = 0; v < 4; v++) {
     const int j = jl + 16 * v;
-    s[i][j] = (i < nb && j < nb) ? M[size_t(k0 + i) * n + k0 + j] : 0.0;
+    const int a = max(i, j), b = min(i, j);  // the lower-triangle copy
+    s[i][j] = (i < nb && j < nb) ? M[size_t(k0 + a) * n + k0 + b] : 0.0;
   }
   __syncthreads();
   for (int k = 0; k < nb; k++) {
@@ -313,64 +321,80 @@ __global__ void __launch_bounds__(1024) gj_diag_kernel(double *__restrict__ M, i
   }
 }
 
-// G(i, :) = M(i, K) Dinv and M(i, K) = -G(i, :) for rows i outside K; M(K, K) = Dinv
-// and G = 0 on the rows of K.  Warp per row: lane l holds M(i, k0 + l) and
-// M(i, k0 + 32 + l), broadcast by shuffles; lane l computes columns l and l + 32.
-// G is stored transposed, GT(s, i) = G(i, s) at GT[s * n + i], so that the update
-// kernel's panel loads run along i.
+// Warp per row i.  Rows of K: M(i, k0 + s) = Dinv(i - k0, s) for s <= i - k0, G = B = 0.
+// Other rows: lane l holds C(i, l) and C(i, l + 32) (after K: M(i, k0 + t); before K:
+// -M(k0 + t, i)), broadcast by shuffles; lane l computes G(i, l) and G(i, l + 32).
+// G and B are stored transposed (GT[t * n + i], BT[t * n + j]) so that the update
+// kernel's panel loads run along i and j.
 __global__ void __launch_bounds__(256) gj_col_kernel(double *__restrict__ M, int n, int k0, int nb,
-                                                     const double *__restrict__ dinv, double *__restrict__ G) {
+                                                     const double *__restrict__ dinv, double *__restrict__ GT,
+                                                     double *__restrict__ BT) {
   __shared__ double D[kGjBlock][kGjBlock];
   for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) D[t / nb][t % nb] = dinv[t];
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
-    double *row = M + size_t(i) * n + k0;
-    double *g = G + i;  // column i of GT
     if (i >= k0 && i < k0 + nb) {
+      for (int s = lane; s <= i - k0; s += 32) M[size_t(i) * n + k0 + s] = D[i - k0][s];
       for (int s = lane; s < nb; s += 32) {
-        row[s] = D[i - k0][s];
-        g[size_t(s) * n] = 0.0;
+        GT[size_t(s) * n + i] = 0.0;
+        BT[size_t(s) * n + i] = 0.0;
       }
       continue;
     }
-    const double m0 = lane < nb ? row[lane] : 0.0;
-    const double m1 = lane + 32 < nb ? row[lane + 32] : 0.0;
+    const bool before = i < k0;
+    double c0 = 0.0, c1 = 0.0;
+    if (before) {
+      if (lane < nb) c0 = -M[size_t(k0 + lane) * n + i];
+      if (lane + 32 < nb) c1 = -M[size_t(k0 + lane + 32) * n + i];
+    } else {
+      const double *row = M + size_t(i) * n + k0;
+      if (lane < nb) c0 = row[lane];
+      if (lane + 32 < nb) c1 = row[lane + 32];
+    }
     double g0 = 0.0, g1 = 0.0;
     const int s1 = min(lane + 32, kGjBlock - 1);
     for (int t = 0; t < nb; t++) {
-      const double mt = __shfl_sync(0xffffffffu, t < 32 ? m0 : m1, t & 31);
-      g0 += mt * D[t][lane];
-      g1 += mt * D[t][s1];
+      const double ct = __shfl_sync(0xffffffffu, t < 32 ? c0 : c1, t & 31);
+      g0 += ct * D[t][lane];
+      g1 += ct * D[t][s1];
     }
+    const double sg = before ? -1.0 : 1.0;
     if (lane < nb) {
-      g[size_t(lane) * n] = g0;
-      row[lane] = -g0;
+      GT[size_t(lane) * n + i] = g0;
+      BT[size_t(lane) * n + i] = sg * c0;
+      if (before) M[size_t(k0 + lane) * n + i] = -g0;
+      else M[size_t(i) * n + k0 + lane] = -g0;
     }
     if (lane + 32 < nb) {
-      g[size_t(lane + 32) * n] = g1;
-      row[lane + 32] = -g1;
+      GT[size_t(lane + 32) * n + i] = g1;
+      BT[size_t(lane + 32) * n + i] = sg * c1;
+      if (before) M[size_t(k0 + lane + 32) * n + i] = -g1;
+      else M[size_t(i) * n + k0 + lane + 32] = -g1;
     }
   }
 }
 
-// M(i, j) -= G(i, :) M(K, j) for i, j outside K (M(K, j) is still the old row panel).
-// Tiles of 128 rows x 64 columns, 256 threads with 8 x 4 outputs each, two CTAs per
-// SM: the tile's values are loaded into the accumulators first, then both panels of
-// the whole pivot block go to shared memory at once (GT along i, the row panel along
-// j: contiguous loads and conflict-free stores), one barrier, nb rank-1 steps.
+// M(i, j) -= G(i, :) B(j, :) for i >= j outside K.  Tiles of 128 rows x 64 columns
+// (tiles wholly above the diagonal leave at once), 256 threads with 8 x 4 outputs
+// each, two CTAs per SM: the tile's values are loaded into the accumulators first,
+// then both panels of the whole pivot block go to shared memory at once (contiguous
+// loads along i and j, conflict-free stores), one barrier, nb rank-1 steps.
 constexpr int kGjTileI = 128, kGjTileJ = 64;
 constexpr int kGjGs = kGjTileI + 4, kGjBs = kGjTileJ + 4;  // padded panel rows (doubles)
 constexpr size_t kGjUpdateSmem = sizeof(double) * size_t(kGjBlock) * (kGjGs + kGjBs);
 __global__ void __launch_bounds__(256, 2) gj_update_kernel(double *__restrict__ M, int n, int k0, int nb,
-                                                           const double *__restrict__ GT) {
+                                                           const double *__restrict__ GT,
+                                                           const double *__restrict__ BT) {
   extern __shared__ __align__(16) double gj_smem[];
-  double *Gs = gj_smem;                          // Gs[k][i] = G(i0 + i, k)
-  double *Bs = gj_smem + kGjBlock * kGjGs;       // Bs[k][j] = M(k0 + k, j0 + j)
+  double *Gs = gj_smem;                     // Gs[k][i] = G(i0 + i, k)
+  double *Bs = gj_smem + kGjBlock * kGjGs;  // Bs[k][j] = B(j0 + j, k)
   const int i0 = blockIdx.y * kGjTileI, j0 = blockIdx.x * kGjTileJ;
-  // a tile inside the pivot rows or columns has nothing to update
-  if ((i0 >= k0 && i0 + kGjTileI <= k0 + nb) || (j0 >= k0 && j0 + kGjTileJ <= k0 + nb)) return;
+  // nothing to update: the tile lies above the diagonal, or inside the pivot rows or
+  // columns
+  if (i0 + kGjTileI <= j0 || (i0 >= k0 && i0 + kGjTileI <= k0 + nb) || (j0 >= k0 && j0 + kGjTileJ <= k0 + nb))
+    return;
   const int tr = threadIdx.x >> 4, tc = threadIdx.x & 15;
   double acc[8][4];
 #pragma unroll
@@ -379,7 +403,7 @@ __global__ void __launch_bounds__(256, 2) gj_update_kernel(double *__restrict__ 
 #pragma unroll
     for (int v = 0; v < 4; v++) {
       const int j = j0 + tc * 4 + v;
-      acc[u][v] = (i < n && j < n) ? M[size_t(i) * n + j] : 0.0;
+      acc[u][v] = (i < n && j <= i) ? M[size_t(i) * n + j] : 0.0;
     }
   }
   for (int e = threadIdx.x; e < kGjBlock * kGjTileI; e += blockDim.x) {
@@ -388,7 +412,7 @@ __global__ void __launch_bounds__(256, 2) gj_update_kernel(double *__restrict__ 
   }
   for (int e = threadIdx.x; e < kGjBlock * kGjTileJ; e += blockDim.x) {
     const int k = e / kGjTileJ, j = e % kGjTileJ;
-    Bs[k * kGjBs + j] = (j0 + j < n && k < nb) ? M[size_t(k0 + k) * n + j0 + j] : 0.0;
+    Bs[k * kGjBs + j] = (j0 + j < n && k < nb) ? BT[size_t(k) * n + j0 + j] : 0.0;
   }
   __syncthreads();
 #pragma unroll 4
@@ -415,32 +439,27 @@ __global__ void __launch_bounds__(256, 2) gj_update_kernel(double *__restrict__ 
 #pragma unroll
     for (int v = 0; v < 4; v++) {
       const int j = j0 + tc * 4 + v;
-      if (j >= n || (j >= k0 && j < k0 + nb)) continue;
+      if (j > i || (j >= k0 && j < k0 + nb)) continue;
       M[size_t(i) * n + j] = acc[u][v];
     }
   }
 }
 
-// M(K, j) = Dinv M(K, j) for columns j outside K: a CTA of 128 threads takes 16
-// columns (the panel in shared memory), thread (c, g) rows g*8 .. g*8+7 of column c.
-__global__ void __launch_bounds__(128) gj_row_kernel(double *__restrict__ M, int n, int k0, int nb,
-                                                     const double *__restrict__ dinv) {
-  __shared__ double D[kGjBlock][kGjBlock];
-  __shared__ double V[kGjBlock][16];
-  const int j0 = blockIdx.x * 16;
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) D[t / nb][t % nb] = dinv[t];
-  for (int t = threadIdx.x; t < nb * 16; t += blockDim.x) {
-    const int k = t / 16, c = t % 16;
-    V[k][c] = j0 + c < n ? M[size_t(k0 + k) * n + j0 + c] : 0.0;
+// M(j, i) = M(i, j) for i > j: 32 x 32 tiles of the lower triangle through shared
+// memory, written transposed (both sides contiguous).
+__global__ void __launch_bounds__(256) gj_mirror_kernel(double *__restrict__ M, int n) {
+  __shared__ double t[32][33];
+  const int bi = blockIdx.y, bj = blockIdx.x;
+  if (bj > bi) return;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int r = ty; r < 32; r += 8) {
+    const int i = bi * 32 + r, j = bj * 32 + tx;
+    t[r][tx] = (i < n && j < n) ? M[size_t(i) * n + j] : 0.0;
   }
   __syncthreads();
-  const int c = threadIdx.x & 15, g = threadIdx.x >> 4;
-  const int j = j0 + c;
-  if (j >= n || (j >= k0 && j < k0 + nb)) return;
-  for (int s = g * 8; s < min(g * 8 + 8, nb); s++) {
-    double a = 0.0;
-    for (int t = 0; t < nb; t++) a += D[s][t] * V[t][c];
-    M[size_t(k0 + s) * n + j] = a;
+  for (int r = ty; r < 32; r += 8) {
+    const int j = bj * 32 + r, i = bi * 32 + tx;  // write M(j, i) = M(i, j) for i > j
+    if (i < n && j < n && i > j) M[size_t(j) * n + i] = t[tx][r];
   }
 }
 

@@ -673,9 +673,11 @@ __global__ void __launch_bounds__(kThreads) sweep_fwd_uni_kernel(SellView<TV> L,
 // Backward sweep of one colour: zpos(pos) -= LU^-1 ( sum_upper A zpos(col) ), the
 // finished rows also written to z in node order; FUSE_RHO accumulates {r}{z} and the
 // last launch's last CTA runs the RHO finisher (hecmw_precond_SSOR_33.F90:353-405).
-// dpos (may be null): the row's correction LU^-1 (...) = y - z (y the forward value),
-// in colour-position order, for lower_resid_kernel.
-template <class R, class TV, class TA, int K, bool FUSE_RHO>
+// DPOS: dpos receives the row's correction LU^-1 (...) = y - z (y the forward value),
+// in colour-position order, for lower_resid_kernel.  A compile-time choice: the extra
+// store changes how the compiler contracts z = c - x, so the kernel without it keeps
+// the drop-in's arithmetic bit for bit.
+template <class R, class TV, class TA, int K, bool FUSE_RHO, bool DPOS = false>
 __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U, const int *__restrict__ perm,
                                                                  const TA *__restrict__ alu, int npos,
                                                                  const R *__restrict__ r, R *__restrict__ z,
@@ -713,7 +715,7 @@ __global__ void __launch_bounds__(kThreads) sweep_bwd_uni_kernel(SellView<TV> U,
       z[3 * node] = z0;
       z[3 * node + 1] = z1;
       z[3 * node + 2] = z2;
-      if (dpos) {
+      if constexpr (DPOS) {
         dpos[3 * row] = x1;
         dpos[3 * row + 1] = x2;
         dpos[3 * row + 2] = x3;

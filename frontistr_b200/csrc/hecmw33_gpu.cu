@@ -288,7 +288,7 @@ struct Learned {
     int n = 0, nagg = 0, nc = 0;
     DevArray<int> agg, pptr, pagg, rptr, rnode, rpos, qptr, qagg, cptr, cagg, uptr, ucol, usrc;
     DevArray<float> mask, x, out, omega, dout;
-    DevArray<double> t0, p, q, ac, gjc, gjd, bc, y, v, t0y, apy, dots;
+    DevArray<double> t0, p, q, ac, gjc, gjb, gjd, bc, y, v, t0y, apy, dots;
     DevArray<float> p32, q32, ainv32;  // FP32 copies for the application in a solve
     DevArray<int> err;
     float *one = nullptr;  // device 1.0f (the decode scale of the backward pass)
@@ -1033,9 +1033,18 @@ void launch_sweep_uni(Solver &S, const Precond &P, const SellView<TV> &lo, const
     // a colour without slices still launches (one idle CTA) so that the reduction
     // ticket count stays exact
     constexpr int pre = sweep_pre<TV>();
-    launch_kp(s, true, sweep_bwd_uni_kernel<R, TV, TA, K, FUSE_RHO>, grid, kThreads, up,
-              P.perm_fwd.p, alu_f, S.N, rin, zout, zpos, ns, run_shape(P.up, g), st, S.partials.p, base, total, pre,
-              dpos);
+    bool done = false;
+    if constexpr (!FUSE_RHO && std::is_same<R, double>::value && std::is_same<TV, double>::value) {
+      if (dpos) {  // the learned FP64 smoother's pre-smoothing (lower_resid_kernel)
+        launch_kp(s, true, sweep_bwd_uni_kernel<R, TV, TA, K, FUSE_RHO, true>, grid, kThreads, up, P.perm_fwd.p,
+                  alu_f, S.N, rin, zout, zpos, ns, run_shape(P.up, g), st, S.partials.p, base, total, pre, dpos);
+        done = true;
+      }
+    }
+    if (!done)
+      launch_kp(s, true, sweep_bwd_uni_kernel<R, TV, TA, K, FUSE_RHO, false>, grid, kThreads, up, P.perm_fwd.p,
+                alu_f, S.N, rin, zout, zpos, ns, run_shape(P.up, g), st, S.partials.p, base, total, pre,
+                static_cast<R *>(nullptr));
     base += grid;
   }
 }
@@ -1681,6 +1690,7 @@ void coarse_structure(Solver &S) {
   C.q.alloc(9 * nnzq);
   C.ac.alloc(nc * nc);
   C.gjc.alloc(nc * kGjBlock);
+  C.gjb.alloc(nc * kGjBlock);
   C.gjd.alloc(size_t(kGjBlock) * kGjBlock);
   C.bc.alloc(nc);
   C.y.alloc(nc);
@@ -1768,10 +1778,11 @@ bool coarse_operator(Solver &S, const float *omega) {
   for (int k0 = 0; k0 < n; k0 += kGjBlock) {
     const int nb = std::min(kGjBlock, n - k0);
     gj_diag_kernel<<<1, 1024, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p, C.err.p);
-    gj_col_kernel<<<std::max(1, (n + 7) / 8), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p, C.gjc.p);
-    gj_update_kernel<<<tiles, 256, kGjUpdateSmem, s>>>(C.ac.p, n, k0, nb, C.gjc.p);
-    gj_row_kernel<<<std::max(1, (n + 15) / 16), 128, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p);
+    gj_col_kernel<<<std::max(1, (n + 7) / 8), 256, 0, s>>>(C.ac.p, n, k0, nb, C.gjd.p, C.gjc.p, C.gjb.p);
+    gj_update_kernel<<<tiles, 256, kGjUpdateSmem, s>>>(C.ac.p, n, k0, nb, C.gjc.p, C.gjb.p);
   }
+  const unsigned nt = unsigned((n + 31) / 32);
+  gj_mirror_kernel<<<dim3(nt, nt), 256, 0, s>>>(C.ac.p, n);
   // FP32 copies for the application
   auto conv = [&](const DevArray<double> &a, DevArray<float> &b) {
     b.alloc(a.n);
