@@ -198,30 +198,49 @@ int ordering_mc(const Profile &p, const std::vector<int> &perm_cur, int ncolor_i
   const int N = p.N;
   if (ncolor_in < 1) ncolor_in = 1;
   const int per_colour = N / ncolor_in;  // colour size cap (0 = no cap)
-  std::vector<int> mark(N, 0);           // >0 colour, -1 neighbour of this colour
-  perm.assign(N, 0);
+  // Everything below works on positions in perm_cur (the order the reference scans):
+  // a node's neighbours are near it in that (banded) order, so the marks stay in cache.
+  std::vector<int> pos_of(static_cast<size_t>(N));
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < N; k++) pos_of[static_cast<size_t>(perm_cur[static_cast<size_t>(k)])] = k;
+  std::vector<int64_t> aptr(static_cast<size_t>(N) + 1, 0);
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < N; k++) {
+    const int node = perm_cur[static_cast<size_t>(k)];
+    int c = p.indexL[node + 1] - p.indexL[node];
+    for (int j = p.indexU[node]; j < p.indexU[node + 1]; j++) c += p.itemU[j] <= N;
+    aptr[static_cast<size_t>(k) + 1] = c;
+  }
+  for (int k = 0; k < N; k++) aptr[static_cast<size_t>(k) + 1] += aptr[static_cast<size_t>(k)];
+  std::vector<int> adj(static_cast<size_t>(aptr[static_cast<size_t>(N)]));
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < N; k++) {
+    const int node = perm_cur[static_cast<size_t>(k)];
+    int64_t w = aptr[static_cast<size_t>(k)];
+    for (int j = p.indexL[node]; j < p.indexL[node + 1]; j++) adj[static_cast<size_t>(w++)] = pos_of[static_cast<size_t>(p.itemL[j] - 1)];
+    for (int j = p.indexU[node]; j < p.indexU[node + 1]; j++)
+      if (p.itemU[j] <= N) adj[static_cast<size_t>(w++)] = pos_of[static_cast<size_t>(p.itemU[j] - 1)];
+  }
+  std::vector<int> mark(static_cast<size_t>(N), 0);  // >0 colour, -1 neighbour of this colour
+  perm.assign(static_cast<size_t>(N), 0);
   colorindex.assign(1, 0);
-  // the nodes not yet coloured, in perm_cur order: every colour scans them from the
-  // start as the reference scans perm_cur (coloured nodes, which it skips, are left
-  // out), so the same nodes are taken in the same order
-  std::vector<int> rest(perm_cur.begin(), perm_cur.end());
+  // the positions not yet coloured, ascending: every colour scans them from the start
+  // as the reference scans perm_cur (coloured nodes, which it skips, are left out), so
+  // the same nodes are taken in the same order
+  std::vector<int> rest(static_cast<size_t>(N));
+  for (int k = 0; k < N; k++) rest[static_cast<size_t>(k)] = k;
   int done = 0, ncolor = 0;
   for (int colour = 1; colour <= N; colour++) {
     int taken = 0;
-    for (const int node : rest) {
-      if (mark[node] != 0) continue;
-      mark[node] = colour;
-      perm[done++] = node;
+    for (const int k : rest) {
+      if (mark[static_cast<size_t>(k)] != 0) continue;
+      mark[static_cast<size_t>(k)] = colour;
+      perm[static_cast<size_t>(done++)] = perm_cur[static_cast<size_t>(k)];
       taken++;
       if (taken == per_colour || done == N) break;
-      for (int k = p.indexL[node]; k < p.indexL[node + 1]; k++) {
-        const int nb = p.itemL[k] - 1;
-        if (mark[nb] == 0) mark[nb] = -1;
-      }
-      for (int k = p.indexU[node]; k < p.indexU[node + 1]; k++) {
-        const int nb1 = p.itemU[k];
-        if (nb1 > N) continue;
-        if (mark[nb1 - 1] == 0) mark[nb1 - 1] = -1;
+      for (int64_t e = aptr[static_cast<size_t>(k)]; e < aptr[static_cast<size_t>(k) + 1]; e++) {
+        int &m = mark[static_cast<size_t>(adj[static_cast<size_t>(e)])];
+        if (m == 0) m = -1;
       }
     }
     colorindex.push_back(done);
@@ -229,17 +248,17 @@ int ordering_mc(const Profile &p, const std::vector<int> &perm_cur, int ncolor_i
       ncolor = colour;
       break;
     }
-    // only uncoloured nodes carry -1 marks: clear them and drop the coloured ones
+    // only uncoloured positions carry -1 marks: clear them and drop the coloured ones
     size_t w = 0;
-    for (const int node : rest) {
-      if (mark[node] > 0) continue;
-      mark[node] = 0;
-      rest[w++] = node;
+    for (const int k : rest) {
+      if (mark[static_cast<size_t>(k)] > 0) continue;
+      mark[static_cast<size_t>(k)] = 0;
+      rest[w++] = k;
     }
     rest.resize(w);
   }
-  iperm.assign(N, 0);
-  for (int i = 0; i < N; i++) iperm[perm[i]] = i;
+  iperm.assign(static_cast<size_t>(N), 0);
+  for (int i = 0; i < N; i++) iperm[static_cast<size_t>(perm[static_cast<size_t>(i)])] = i;
   return ncolor;
 }
 
@@ -272,10 +291,12 @@ void reordered_rows(const Profile &p, const std::vector<int> &perm, const std::v
   const int N = p.N, NPL = p.NPL();
   lower.ptr.assign(size_t(N) + 1, 0);
   upper.ptr.assign(size_t(N) + 1, 0);
+  // rows are visited in their old (input) order, so the profile and the neighbours'
+  // new indices are read from nearby memory; each finished row goes to its new place
   // counts per new row
 #pragma omp parallel for schedule(static)
-  for (int inew = 0; inew < N; inew++) {
-    const int iold = perm[inew];
+  for (int iold = 0; iold < N; iold++) {
+    const int inew = iperm[iold];
     int nl = 0, nu = 0;
     for (int j = p.indexL[iold]; j < p.indexL[iold + 1]; j++)
       (iperm[p.itemL[j] - 1] < inew ? nl : nu)++;
@@ -294,34 +315,39 @@ void reordered_rows(const Profile &p, const std::vector<int> &perm, const std::v
   lower.src.resize(size_t(lower.ptr[N]));
   upper.col.resize(size_t(upper.ptr[N]));
   upper.src.resize(size_t(upper.ptr[N]));
+  struct Entry {
+    int jnew, src, jold;  // new column, raw block, old column (the node id kept in col)
+  };
 #pragma omp parallel
   {
-    std::vector<std::pair<int, int>> lo, up;  // (new column, raw block)
+    std::vector<Entry> lo, up;
 #pragma omp for schedule(static)
-    for (int inew = 0; inew < N; inew++) {
-      const int iold = perm[inew];
+    for (int iold = 0; iold < N; iold++) {
+      const int inew = iperm[iold];
       lo.clear();
       up.clear();
       for (int j = p.indexL[iold]; j < p.indexL[iold + 1]; j++) {
-        const int jnew = iperm[p.itemL[j] - 1];
-        (jnew < inew ? lo : up).emplace_back(jnew, N + j);
+        const int jold = p.itemL[j] - 1, jnew = iperm[jold];
+        (jnew < inew ? lo : up).push_back(Entry{jnew, N + j, jold});
       }
       for (int j = p.indexU[iold]; j < p.indexU[iold + 1]; j++) {
         if (p.itemU[j] > N) continue;
-        const int jnew = iperm[p.itemU[j] - 1];
-        (jnew < inew ? lo : up).emplace_back(jnew, N + NPL + j);
+        const int jold = p.itemU[j] - 1, jnew = iperm[jold];
+        (jnew < inew ? lo : up).push_back(Entry{jnew, N + NPL + j, jold});
       }
-      std::sort(lo.begin(), lo.end());
-      std::sort(up.begin(), up.end());
+      // new columns are distinct within a row: the order is total
+      auto by_new = [](const Entry &a, const Entry &b) { return a.jnew < b.jnew; };
+      std::sort(lo.begin(), lo.end(), by_new);
+      std::sort(up.begin(), up.end(), by_new);
       int64_t w = lower.ptr[inew];
-      for (auto &e : lo) {
-        lower.col[w] = perm[e.first];  // column renumbered to the old node id
-        lower.src[w++] = e.second;
+      for (const Entry &e : lo) {
+        lower.col[w] = e.jold;
+        lower.src[w++] = e.src;
       }
       w = upper.ptr[inew];
-      for (auto &e : up) {
-        upper.col[w] = perm[e.first];
-        upper.src[w++] = e.second;
+      for (const Entry &e : up) {
+        upper.col[w] = e.jold;
+        upper.src[w++] = e.src;
       }
     }
   }
