@@ -159,26 +159,85 @@ void ordering_rcm(const Profile &p, std::vector<int> &perm, std::vector<int> &ip
   }
 }
 
-int ordering_greedy(const Profile &p, std::vector<int> &colorindex, std::vector<int> &perm,
-                    std::vector<int> &iperm) {
+namespace {
+
+// First-fit colouring in `order` (null: the input order): each node takes the smallest
+// colour that none of its already coloured neighbours has.  Returns the colour count.
+int first_fit(const Profile &p, const std::vector<int> *order, std::vector<int> &colour) {
   const int N = p.N;
-  std::vector<int> colour(static_cast<size_t>(N), -1), seen;
+  colour.assign(static_cast<size_t>(N), -1);
+  std::vector<int> seen;
   int ncolor = 0;
-  for (int i = 0; i < N; i++) {
-    auto visit = [&](const int *index, const int *item) {
-      for (int k = index[i]; k < index[i + 1]; k++) {
-        const int c = colour[static_cast<size_t>(item[k] - 1)];
-        if (c >= 0) seen[static_cast<size_t>(c)] = i;
-      }
-    };
+  for (int t = 0; t < N; t++) {
+    const int i = order ? (*order)[static_cast<size_t>(t)] : t;
     seen.resize(static_cast<size_t>(ncolor) + 1, -1);
-    visit(p.indexL, p.itemL);
-    visit(p.indexU, p.itemU);
+    for (int k = p.indexL[i]; k < p.indexL[i + 1]; k++) {
+      const int c = colour[static_cast<size_t>(p.itemL[k] - 1)];
+      if (c >= 0) seen[static_cast<size_t>(c)] = t;
+    }
+    for (int k = p.indexU[i]; k < p.indexU[i + 1]; k++) {
+      const int c = colour[static_cast<size_t>(p.itemU[k] - 1)];
+      if (c >= 0) seen[static_cast<size_t>(c)] = t;
+    }
     int c = 0;
-    while (seen[static_cast<size_t>(c)] == i) c++;
+    while (seen[static_cast<size_t>(c)] == t) c++;
     colour[static_cast<size_t>(i)] = c;
     ncolor = std::max(ncolor, c + 1);
   }
+  return ncolor;
+}
+
+// Smallest-last order (Matula and Beck, 1983): repeatedly remove a node of least
+// remaining degree; the reverse of the removal order.  Bucket queue with lazy entries.
+std::vector<int> smallest_last(const Profile &p) {
+  const int N = p.N;
+  std::vector<int> deg(static_cast<size_t>(N));
+  std::vector<char> removed(static_cast<size_t>(N), 0);
+  int maxd = 0;
+  for (int i = 0; i < N; i++) {
+    deg[static_cast<size_t>(i)] = (p.indexL[i + 1] - p.indexL[i]) + (p.indexU[i + 1] - p.indexU[i]);
+    maxd = std::max(maxd, deg[static_cast<size_t>(i)]);
+  }
+  std::vector<std::vector<int>> bucket(static_cast<size_t>(maxd) + 1);
+  for (int i = 0; i < N; i++) bucket[static_cast<size_t>(deg[static_cast<size_t>(i)])].push_back(i);
+  std::vector<int> order;
+  order.reserve(static_cast<size_t>(N));
+  int d = 0;
+  for (int cnt = 0; cnt < N; cnt++) {
+    d = std::max(0, d - 1);  // a removal lowers a neighbour's degree by one at most
+    int v;
+    for (;;) {
+      while (bucket[static_cast<size_t>(d)].empty()) d++;
+      v = bucket[static_cast<size_t>(d)].back();
+      bucket[static_cast<size_t>(d)].pop_back();
+      if (!removed[static_cast<size_t>(v)] && deg[static_cast<size_t>(v)] == d) break;  // else stale
+    }
+    removed[static_cast<size_t>(v)] = 1;
+    order.push_back(v);
+    auto drop = [&](int u) {
+      if (removed[static_cast<size_t>(u)]) return;
+      const int du = --deg[static_cast<size_t>(u)];
+      bucket[static_cast<size_t>(du)].push_back(u);
+    };
+    for (int k = p.indexL[v]; k < p.indexL[v + 1]; k++) drop(p.itemL[k] - 1);
+    for (int k = p.indexU[v]; k < p.indexU[v + 1]; k++) drop(p.itemU[k] - 1);
+  }
+  std::reverse(order.begin(), order.end());
+  return order;
+}
+
+}  // namespace
+
+int ordering_greedy(const Profile &p, std::vector<int> &colorindex, std::vector<int> &perm,
+                    std::vector<int> &iperm) {
+  const int N = p.N;
+  std::vector<int> c_in, c_sl;
+  const int n_in = first_fit(p, nullptr, c_in);
+  const std::vector<int> sl = smallest_last(p);
+  const int n_sl = first_fit(p, &sl, c_sl);
+  const bool use_sl = n_sl < n_in;
+  const std::vector<int> &colour = use_sl ? c_sl : c_in;
+  const int ncolor = use_sl ? n_sl : n_in;
   colorindex.assign(static_cast<size_t>(ncolor) + 1, 0);
   for (int i = 0; i < N; i++) colorindex[static_cast<size_t>(colour[static_cast<size_t>(i)]) + 1]++;
   for (int c = 0; c < ncolor; c++) colorindex[static_cast<size_t>(c) + 1] += colorindex[static_cast<size_t>(c)];

@@ -35,10 +35,12 @@ void ordering_rcm(const Profile &p, std::vector<int> &perm, std::vector<int> &ip
 int ordering_mc(const Profile &p, const std::vector<int> &perm_cur, int ncolor_in,
                 std::vector<int> &colorindex, std::vector<int> &perm, std::vector<int> &iperm);
 
-// First-fit colouring in the input order (each node takes the smallest colour none of
-// its already coloured neighbours has), rows then ordered by colour, by node number
-// inside a colour.  On a structured 27-point mesh numbered lexicographically this
-// gives the 8 parity colours.  Returns the number of colours.
+// First-fit colouring (each node takes the smallest colour none of its already
+// coloured neighbours has) in the input order and in smallest-last order (Matula and
+// Beck), whichever needs fewer colours (ties: the input order); rows then ordered by
+// colour, by node number inside a colour.  On a structured 27-point mesh numbered
+// lexicographically the input order gives the 8 parity colours; on other numberings
+// smallest-last usually needs fewer.  Returns the number of colours.
 int ordering_greedy(const Profile &p, std::vector<int> &colorindex, std::vector<int> &perm,
                     std::vector<int> &iperm);
 

@@ -244,11 +244,12 @@ HECMW33_API void hecmw33_gpu_colour_schedule(const int *N, const int *indexL, co
                                              int *perm, int *ierr);
 
 /* Host-only (no GPU needed; no counterpart in the reference): the colour schedule of
- * the learned preconditioner's SSOR smoother (Iarray(43) = 1), first-fit colours in the
- * node order (each node takes the smallest colour that none of its already coloured
- * neighbours has; 8 colours on a lexicographically numbered structured hexahedral
- * mesh), rows ordered by colour and by node inside a colour.  Outputs as
- * hecmw33_gpu_colour_schedule (colorindex needs N+1 entries, perm N, 1-based ids). */
+ * the learned preconditioner's SSOR smoother (Iarray(43) = 1): first-fit colours (each
+ * node takes the smallest colour that none of its already coloured neighbours has) in
+ * the node order and in smallest-last order, whichever needs fewer (8 colours on a
+ * lexicographically numbered structured hexahedral mesh); rows ordered by colour and by
+ * node inside a colour.  Outputs as hecmw33_gpu_colour_schedule (colorindex needs N+1
+ * entries, perm N, 1-based ids). */
 HECMW33_API void hecmw33_gpu_smoother_schedule(const int *N, const int *indexL, const int *itemL,
                                                const int *indexU, const int *itemU, int *ncolor,
                                                int *colorindex, int *perm, int *ierr);

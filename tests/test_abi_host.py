@@ -108,17 +108,30 @@ def _neighbours(m):
     return nb
 
 
-@pytest.mark.parametrize("case", ["tet4", "box_small", "box_jitter"])
-def test_smoother_schedule_is_a_first_fit_colouring(case):
-    """The learned preconditioner's smoother colours: every node has the smallest
-    colour none of its lower-numbered neighbours has, no two neighbours share one,
-    rows by colour then node; 8 colours on a structured box."""
+def _first_fit(nb, order):
+    colour = {}
+    for i in order:
+        used = {colour[j] for j in nb[i] if j in colour and j != i}
+        colour[i] = min(set(range(len(used) + 1)) - used)
+    return 1 + max(colour.values())
+
+
+@pytest.mark.parametrize("case", ["tet4", "box_small", "box_jitter", "box_renumbered"])
+def test_smoother_schedule_is_a_greedy_colouring(case):
+    """The learned preconditioner's smoother colours: a valid colouring (no two
+    neighbours share a colour), rows by colour then node, and no more colours than
+    first-fit in the node order (the library keeps the better of that and smallest-last
+    order): 8 on a lexicographically numbered box, fewer than first-fit on a randomly
+    renumbered one."""
     if case == "tet4":
         _, m = golden_system()
     elif case == "box_small":
         m = box_system(6, 5, 7)
-    else:
+    elif case == "box_jitter":
         m = box_system(5, 6, 4, jitter=0.2, seed=3)
+    else:
+        from test_gpu_learned import _renumbered_box
+        m = _renumbered_box(6, 5, 7, seed=2)
     ci, perm = smoother_schedule(m)
     nc = len(ci) - 1
     colour = np.empty(m.N, np.int64)
@@ -129,10 +142,12 @@ def test_smoother_schedule_is_a_first_fit_colouring(case):
     nb = _neighbours(m)
     for i in range(m.N):
         assert all(colour[j] != colour[i] for j in nb[i] if j != i)
-        lower = {int(colour[j]) for j in nb[i] if j < i}
-        assert colour[i] == min(set(range(len(lower) + 1)) - lower)
-    if case.startswith("box"):
+    natural = _first_fit(nb, range(m.N))
+    assert nc <= natural
+    if case in ("box_small", "box_jitter"):
         assert nc == 8
+    if case == "box_renumbered":
+        assert nc < natural, (nc, natural)
 
 
 def test_rel_resid_noalloc_rejects_null_pointers():
