@@ -3063,8 +3063,10 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   S.iterlog = Iarray[20] == 1;
   if (S.rhist_on) S.rhist_buf.alloc(size_t(std::max(MAXIT, 1)));
   if (lowp && iterPREmax > 0) {
-    ensure_lowp(S);
+    // a learned solve sweeps with its smoother only: the solve's SSOR needs its BF16
+    // copy when a plain solve (or the METHOD2 hand-over below) uses it
     if (learned) ensure_lowp(S, S.L.sm);
+    else ensure_lowp(S);
   } else {
     lowp = 0;
   }
@@ -3125,6 +3127,7 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
         if (auto_sigma) sigma = 1.0;
         method = METHOD2;
         learned = 0;
+        if (lowp) ensure_lowp(S);
         continue;
       }
     }
