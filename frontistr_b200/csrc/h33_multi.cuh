@@ -13,6 +13,7 @@
 // as converged.
 #pragma once
 
+#include "h33_coarse.cuh"
 #include "h33_kernels.cuh"
 
 namespace h33 {
@@ -517,7 +518,9 @@ __global__ void mr_init_kernel(CgState *st, MultiCtl *ctl, const CgParams *prm, 
     s->done = s->error = s->n_indef = s->recompute = s->converged = s->zero_rhs = 0;
     s->guard = 0;
     s->inner = 0;
-    s->flexible = s->use_gnn = s->restart = s->fallback = 0;
+    s->flexible = prm->flexible;
+    s->use_gnn = prm->use_gnn;
+    s->restart = s->fallback = 0;
     s->resid_mark = 1.0;
     s->gamma = 1.0f;
     s->reliable = s->ru_pending = s->ru_count = 0;
@@ -563,6 +566,242 @@ __global__ void mr_ctl_kernel(const CgState *st, MultiCtl *ctl, cudaGraphConditi
   if (ctl->guard > maxit + 1) any = 0;
   ctl->all_done = !any;
   set_loop(h, use_cond, any);
+}
+
+// ---- the learned two-level preconditioner for 16 RHS ---------------------------
+// The single-RHS cycle (zs = SSOR(r); zc = zs + P Ac^-1 P^T (r - A zs); z = zc +
+// SSOR(r - A zc)) in flexible CG, with the smoother's sweeps and A streamed once for
+// all RHS, and Ac^-1 (FP32 copy) read once per iteration for all of them (a GEMM with
+// 16 columns instead of 16 GEMVs).  Coarse vectors are RHS-minor: bc[(3a+c)*16 + l].
+// A RHS whose correction was switched off (st.use_gnn = 0: the stagnation fallback)
+// keeps zc = zs and w, so its cycle is SSOR + SSOR of the unchanged residual ... as in
+// the single solve, the fallback leaves only the smoother.
+
+// Deterministic per-RHS reduction of two values (as mr_reduce_finish); partials hold
+// 32 doubles per CTA.
+template <class Fin>
+__device__ __forceinline__ void mr_reduce_finish2(double va, double vb, double *partials, int part, int total,
+                                                  unsigned int *ticket, Fin fin) {
+  __shared__ double sha[kThreads / 16][kMaxRhs], shb[kThreads / 16][kMaxRhs];
+  __shared__ int is_last;
+  const int l = threadIdx.x & 15, hw = threadIdx.x >> 4;
+  sha[hw][l] = va;
+  shb[hw][l] = vb;
+  __syncthreads();
+  if (threadIdx.x < kMaxRhs) {
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < kThreads / 16; k++) {
+      a += sha[k][threadIdx.x];
+      b += shb[k][threadIdx.x];
+    }
+    partials[size_t(part) * 2 * kMaxRhs + threadIdx.x] = a;
+    partials[size_t(part) * 2 * kMaxRhs + kMaxRhs + threadIdx.x] = b;
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int t = atomicAdd(ticket, 1u);
+    is_last = (t == unsigned(total) - 1u);
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  double a = 0.0, b = 0.0;
+  for (int i = hw; i < total; i += kThreads / 16) {
+    a += __ldcg(&partials[size_t(i) * 2 * kMaxRhs + l]);
+    b += __ldcg(&partials[size_t(i) * 2 * kMaxRhs + kMaxRhs + l]);
+  }
+  __syncthreads();
+  sha[hw][l] = a;
+  shb[hw][l] = b;
+  __syncthreads();
+  if (threadIdx.x < kMaxRhs) {
+    double ta = 0.0, tb = 0.0;
+    for (int k = 0; k < kThreads / 16; k++) {
+      ta += sha[k][threadIdx.x];
+      tb += shb[k][threadIdx.x];
+    }
+    fin(int(threadIdx.x), ta, tb);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// RHO = {z}{r} and DELTA = {z}{r_old} per RHS in one pass, then fin_rho_flex.
+__global__ void __launch_bounds__(kThreads) mr_fcg_rho_kernel(const double *__restrict__ z,
+                                                              const double *__restrict__ r,
+                                                              const double *__restrict__ r_old, int n, CgState *st,
+                                                              MultiCtl *ctl, double *partials) {
+  pdl_entry();
+  if (ctl->all_done) return;
+  const int l = threadIdx.x & 15;
+  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  double a = 0.0, b = 0.0;
+  if (!st[l].done) {
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < n; i += nhw) {
+      const size_t o = size_t(i) * kRhsStride + l;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const double zi = z[o + 16 * c];
+        a += zi * r[o + 16 * c];
+        b += zi * r_old[o + 16 * c];
+      }
+    }
+  }
+  mr_reduce_finish2(a, b, partials, blockIdx.x, gridDim.x, &ctl->ticket[0], [&](int k, double rho, double delta) {
+    if (!st[k].done) fin_rho_flex(&st[k], rho, delta);
+  });
+}
+
+// Flexible CG update per RHS: r_old = r, x += ALPHA p, r -= ALPHA q with the DNRM2
+// (every 50th iteration r is recomputed from b - A x instead).
+__global__ void __launch_bounds__(kThreads) mr_update_xr_flex_kernel(double *__restrict__ x,
+                                                                     const double *__restrict__ p,
+                                                                     double *__restrict__ r,
+                                                                     double *__restrict__ r_old,
+                                                                     const double *__restrict__ q, int n, CgState *st,
+                                                                     MultiCtl *ctl, double *partials) {
+  pdl_entry();
+  if (ctl->all_done) return;
+  const int l = threadIdx.x & 15;
+  const bool act = !st[l].done;
+  const double alpha = st[l].alpha;
+  const bool refresh = (st[l].iter % kIterRecomputeR) == 0;
+  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  double dot = 0.0;
+  if (act) {
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < n; i += nhw) {
+      const size_t o = size_t(i) * kRhsStride + l;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        x[o + 16 * c] = alpha * p[o + 16 * c] + x[o + 16 * c];
+        const double ri = r[o + 16 * c];
+        r_old[o + 16 * c] = ri;
+        if (!refresh) {
+          const double rn = -alpha * q[o + 16 * c] + ri;
+          r[o + 16 * c] = rn;
+          dot += rn * rn;
+        }
+      }
+    }
+  }
+  mr_reduce_finish(dot, partials, blockIdx.x, gridDim.x, &ctl->ticket[2], [&](int k, double v) {
+    CgState *s = &st[k];
+    if (!s->done && (s->iter % kIterRecomputeR) != 0) fin_rr(s, v);
+  });
+}
+
+// bc = P^T w for 16 RHS: a CTA per aggregate, 16 groups of 16 lanes (lane = RHS) over
+// the aggregate's restriction entries, group partial sums added in group order.
+__global__ void __launch_bounds__(kThreads) mr_coarse_restrict_kernel(CoarseApply c, const double *__restrict__ w,
+                                                                      double *__restrict__ bc, const MultiCtl *ctl) {
+  pdl_entry();
+  if (ctl->all_done) return;
+  __shared__ double sh[kThreads / 16][3][kMaxRhs];
+  const int l = threadIdx.x & 15, g = threadIdx.x >> 4;
+  for (int a = blockIdx.x; a < c.nagg; a += gridDim.x) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int e = c.rptr[a] + g; e < c.rptr[a + 1]; e += kThreads / 16) {
+      const size_t o = size_t(c.rnode[e]) * kRhsStride + l;
+      const float *pb = c.p + 9 * size_t(c.rpos[e]);
+      const double w0 = w[o], w1 = w[o + 16], w2 = w[o + 32];
+#pragma unroll
+      for (int k = 0; k < 3; k++)  // (P^T w)_k = sum_d P(d, k) w_d
+        acc[k] += double(pb[k]) * w0 + double(pb[3 + k]) * w1 + double(pb[6 + k]) * w2;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) sh[g][k][l] = acc[k];
+    __syncthreads();
+    if (threadIdx.x < 3 * kMaxRhs) {
+      const int k = threadIdx.x >> 4, ll = threadIdx.x & 15;
+      double s = 0.0;
+      for (int gg = 0; gg < kThreads / 16; gg++) s += sh[gg][k][ll];
+      bc[size_t(3 * a + k) * kMaxRhs + ll] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// y = Ac^-1 bc for 16 RHS (FP32 copy of Ac^-1, FP64 sums): a warp per row, 8 rows per
+// CTA sharing the bc chunk staged in shared memory; lane t takes columns t, t + 32, ...
+// of its row, then a butterfly sum per RHS.
+constexpr int kMrGemmChunk = 256;
+__global__ void __launch_bounds__(kThreads) mr_coarse_gemm_kernel(int nc, const float *__restrict__ ainv,
+                                                                  const double *__restrict__ bc,
+                                                                  double *__restrict__ y, const MultiCtl *ctl) {
+  pdl_entry();
+  if (ctl->all_done) return;
+  __shared__ double bs[kMrGemmChunk][kMaxRhs + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int r0 = blockIdx.x * kWarpsPerCta; r0 < nc; r0 += gridDim.x * kWarpsPerCta) {
+    const int row = r0 + warp;
+    double acc[kMaxRhs];
+#pragma unroll
+    for (int l = 0; l < kMaxRhs; l++) acc[l] = 0.0;
+    for (int k0 = 0; k0 < nc; k0 += kMrGemmChunk) {
+      const int kn = min(kMrGemmChunk, nc - k0);
+      __syncthreads();
+      for (int t = threadIdx.x; t < kn * kMaxRhs; t += blockDim.x) bs[t / kMaxRhs][t % kMaxRhs] = bc[size_t(k0) * kMaxRhs + t];
+      __syncthreads();
+      if (row < nc) {
+        const float *ar = ainv + size_t(row) * nc + k0;
+        for (int k = lane; k < kn; k += 32) {
+          const double a = double(ar[k]);
+#pragma unroll
+          for (int l = 0; l < kMaxRhs; l++) acc[l] += a * bs[k][l];
+        }
+      }
+    }
+    if (row < nc) {
+#pragma unroll
+      for (int l = 0; l < kMaxRhs; l++) {
+        double v = acc[l];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == l) y[size_t(row) * kMaxRhs + l] = v;
+      }
+    }
+  }
+}
+
+// zc = zs + P y and w -= (A P) y per RHS (a half-warp per node, lane = RHS); a RHS whose
+// correction is off keeps zc = zs and w.
+__global__ void __launch_bounds__(kThreads) mr_coarse_prolong_resid_kernel(CoarseApply c, const double *__restrict__ y,
+                                                                           const double *__restrict__ zs,
+                                                                           double *__restrict__ zc,
+                                                                           double *__restrict__ w, const CgState *st,
+                                                                           const MultiCtl *ctl) {
+  pdl_entry();
+  if (ctl->all_done) return;
+  const int l = threadIdx.x & 15;
+  const bool on = !st[l].done && st[l].use_gnn;
+  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < c.n; i += nhw) {
+    const size_t o = size_t(i) * kRhsStride + l;
+    double a[3] = {0.0, 0.0, 0.0}, q[3] = {0.0, 0.0, 0.0};
+    if (on) {
+      for (int k = c.pptr[i]; k < c.pptr[i + 1]; k++) {
+        const float *pb = c.p + 9 * size_t(k);
+        const size_t b = size_t(3 * c.pagg[k]) * kMaxRhs + l;
+        const double y0 = y[b], y1 = y[b + 16], y2 = y[b + 32];
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+          a[d] += double(pb[3 * d]) * y0 + double(pb[3 * d + 1]) * y1 + double(pb[3 * d + 2]) * y2;
+      }
+      for (int k = c.qptr[i]; k < c.qptr[i + 1]; k++) {
+        const float *qb = c.q + 9 * size_t(k);
+        const size_t b = size_t(3 * c.qagg[k]) * kMaxRhs + l;
+        const double y0 = y[b], y1 = y[b + 16], y2 = y[b + 32];
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+          q[d] += double(qb[3 * d]) * y0 + double(qb[3 * d + 1]) * y1 + double(qb[3 * d + 2]) * y2;
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      zc[o + 16 * d] = zs[o + 16 * d] + a[d];
+      if (on) w[o + 16 * d] -= q[d];
+    }
+  }
 }
 
 // Column-major host layout (n3 x nrhs) <-> node-major RHS-minor layout.

@@ -443,6 +443,7 @@ struct Solver {
   GraphSlot g64, g32;
   // multi-RHS CG: node-major RHS-minor vectors (48 doubles per node), per-RHS states
   DevArray<double> mb, mx, mr, mz, mp, mq, mw, mzp, mzpos, mpart;
+  DevArray<double> mzs, mrold, mbc, my;  // the learned multi-RHS cycle (zs, r_old, P^T w, Ac^-1 P^T w)
   DevArray<CgState> mst;
   DevArray<MultiCtl> mctl;
   CgState *h_mst = nullptr;
@@ -3312,9 +3313,8 @@ int solve_mixed_reliable(Solver &S, int *Iarray, double *Rarray, int *iter, doub
 // Multi-RHS CG: up to kMaxRhs load cases per pass over the matrix (h33_multi.cuh).
 
 template <int K, bool FUSE_RHO, bool POS>
-void launch_mr_sweep_k(Solver &S, const DevSell<double> &Lo, const DevSell<double> &Up, const double *rin,
-                       double *zout) {
-  Precond &P = S.pc;
+void launch_mr_sweep_k(Solver &S, const Precond &P, const DevSell<double> &Lo, const DevSell<double> &Up,
+                       const double *rin, double *zout) {
   cudaStream_t s = S.stream;
   const int *perm_b = P.alu_shared ? P.perm_fwd.p : P.perm_bwd.p;
   const double *alu_b = P.alu_shared ? P.alu_fwd.p : P.alu_bwd.p;
@@ -3353,15 +3353,15 @@ void launch_mr_sweep(Solver &S, const double *rin, double *zout) {
   }
   if (P.pos_cols) {
     switch (P.lo.lanes) {
-      case 4: return launch_mr_sweep_k<4, FUSE_RHO, true>(S, P.lo, P.up, rin, zout);
-      case 16: return launch_mr_sweep_k<16, FUSE_RHO, true>(S, P.lo, P.up, rin, zout);
-      default: return launch_mr_sweep_k<8, FUSE_RHO, true>(S, P.lo, P.up, rin, zout);
+      case 4: return launch_mr_sweep_k<4, FUSE_RHO, true>(S, P, P.lo, P.up, rin, zout);
+      case 16: return launch_mr_sweep_k<16, FUSE_RHO, true>(S, P, P.lo, P.up, rin, zout);
+      default: return launch_mr_sweep_k<8, FUSE_RHO, true>(S, P, P.lo, P.up, rin, zout);
     }
   }
   switch (P.lo.lanes) {
-    case 4: return launch_mr_sweep_k<4, FUSE_RHO, false>(S, P.lo, P.up, rin, zout);
-    case 16: return launch_mr_sweep_k<16, FUSE_RHO, false>(S, P.lo, P.up, rin, zout);
-    default: return launch_mr_sweep_k<8, FUSE_RHO, false>(S, P.lo, P.up, rin, zout);
+    case 4: return launch_mr_sweep_k<4, FUSE_RHO, false>(S, P, P.lo, P.up, rin, zout);
+    case 16: return launch_mr_sweep_k<16, FUSE_RHO, false>(S, P, P.lo, P.up, rin, zout);
+    default: return launch_mr_sweep_k<8, FUSE_RHO, false>(S, P, P.lo, P.up, rin, zout);
   }
 }
 
@@ -3435,10 +3435,57 @@ void launch_mr_iteration(Solver &S, int iterpremax, cudaGraphConditionalHandle h
   launch_k(s, mr_ctl_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
 }
 
+// One flexible-CG iteration of the multi-RHS loop with the learned two-level
+// preconditioner (launch_learned_precond's symmetric cycle, FP64 smoother): zs =
+// SSOR(r); w = r - A zs; bc = P^T w; y = Ac^-1 bc; zc = zs + P y, w -= (A P) y;
+// z = zc + SSOR(w).
+void launch_mr_iteration_learned(Solver &S, cudaGraphConditionalHandle h, int use_cond) {
+  cudaStream_t s = S.stream;
+  Precond &P = S.L.sm;
+  auto &C = S.L.C;
+  const CoarseApply ca = C.apply_view();
+  const int gs = S.grid_amr(), gn = S.grid_mr(S.N);
+  const int n48 = S.N * kRhsStride;
+  auto smooth = [&](const double *rin, double *zout) {
+    switch (P.lo.lanes) {
+      case 8: return launch_mr_sweep_k<8, false, true>(S, P, P.lo, P.up, rin, zout);
+      case 16: return launch_mr_sweep_k<16, false, true>(S, P, P.lo, P.up, rin, zout);
+      default: return launch_mr_sweep_k<4, false, true>(S, P, P.lo, P.up, rin, zout);
+    }
+  };
+  launch_k(s, mr_iter_begin_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
+  smooth(S.mr.p, S.mzs.p);
+  launch_k(s, mr_spmv_kernel<1, kMrLanes>, gs, kThreads, S.amr_view(), static_cast<const double *>(S.mzs.p), S.mw.p,
+           static_cast<const double *>(S.mr.p), S.mst.p, S.mctl.p, S.mpart.p);
+  launch_k(s, mr_coarse_restrict_kernel, std::max(1, C.nagg), kThreads, ca, static_cast<const double *>(S.mw.p),
+           S.mbc.p, static_cast<const MultiCtl *>(S.mctl.p));
+  launch_k(s, mr_coarse_gemm_kernel, std::max(1, (C.nc + kWarpsPerCta - 1) / kWarpsPerCta), kThreads, C.nc,
+           static_cast<const float *>(C.ainv32.p), static_cast<const double *>(S.mbc.p), S.my.p,
+           static_cast<const MultiCtl *>(S.mctl.p));
+  launch_k(s, mr_coarse_prolong_resid_kernel, gn, kThreads, ca, static_cast<const double *>(S.my.p),
+           static_cast<const double *>(S.mzs.p), S.mzp.p, S.mw.p, static_cast<const CgState *>(S.mst.p),
+           static_cast<const MultiCtl *>(S.mctl.p));
+  smooth(S.mw.p, S.mz.p);
+  const int gv = std::max(1, std::min((n48 + kThreads - 1) / kThreads, S.nsm * S.occ_vec));
+  launch_k(s, add_kernel<double>, gv, kThreads, static_cast<const double *>(S.mzp.p), S.mz.p, n48,
+           static_cast<const CgState *>(nullptr));
+  launch_k(s, mr_fcg_rho_kernel, gn, kThreads, static_cast<const double *>(S.mz.p),
+           static_cast<const double *>(S.mr.p), static_cast<const double *>(S.mrold.p), S.N, S.mst.p, S.mctl.p,
+           S.mpart.p);
+  launch_k(s, mr_update_p_kernel, gn, kThreads, S.mz.p, S.mp.p, S.N, S.mst.p, S.mctl.p);
+  launch_k(s, mr_spmv_kernel<2, kMrLanes>, gs, kThreads, S.amr_view(), S.mp.p, S.mq.p, nullptr, S.mst.p, S.mctl.p,
+           S.mpart.p);
+  launch_k(s, mr_update_xr_flex_kernel, gn, kThreads, S.mx.p, static_cast<const double *>(S.mp.p), S.mr.p,
+           S.mrold.p, static_cast<const double *>(S.mq.p), S.N, S.mst.p, S.mctl.p, S.mpart.p);
+  launch_k(s, mr_spmv_kernel<3, kMrLanes>, gs, kThreads, S.amr_view(), S.mx.p, S.mr.p, S.mb.p, S.mst.p, S.mctl.p,
+           S.mpart.p);
+  launch_k(s, mr_ctl_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
+}
+
 // Graph of the whole multi-RHS loop (prologue + WHILE node), as build_graph.
-void build_graph_multi(Solver &S, int iterpremax, int nrhs) {
+void build_graph_multi(Solver &S, int iterpremax, int nrhs, bool learned = false) {
   GraphSlot &G = S.gm;
-  const int key[5] = {S.generation, S.pc.generation, S.pc.kind, iterpremax, nrhs};
+  const int key[5] = {S.generation, S.pc.generation, S.pc.kind, 2 * iterpremax + (learned ? 1 : 0), nrhs};
   if (G.exec && std::equal(key, key + 5, G.key)) return;
   G.drop();
   cudaGraph_t g = nullptr;
@@ -3464,7 +3511,8 @@ void build_graph_multi(Solver &S, int iterpremax, int nrhs) {
   H33_CUDA(cudaGraphAddNode(&cnode, g, dep.data(), dep.size(), &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   H33_CUDA(cudaStreamBeginCaptureToGraph(S.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  launch_mr_iteration(S, iterpremax, h, 1);
+  if (learned) launch_mr_iteration_learned(S, h, 1);
+  else launch_mr_iteration(S, iterpremax, h, 1);
   cudaGraph_t b2 = nullptr;
   H33_CUDA(cudaStreamEndCapture(S.stream, &b2));
   H33_CUDA(cudaGraphInstantiate(&G.exec, g, 0));
@@ -3544,14 +3592,14 @@ void ensure_multi_buffers(Solver &S) {
   for (auto *v : {&S.mb, &S.mx, &S.mr, &S.mz, &S.mp, &S.mq, &S.mw, &S.mzp, &S.mzpos}) v->alloc(n48);
   S.mst.alloc(kMaxRhs);
   S.mctl.alloc(1);
-  S.mpart.alloc(size_t(mr_max_parts(S)) * kMaxRhs + 1024);
+  S.mpart.alloc(size_t(mr_max_parts(S)) * 2 * kMaxRhs + 1024);  // two values per CTA (mr_fcg_rho_kernel)
 }
 
 // Solves nrhs <= kMaxRhs systems A X(:, k) = B(:, k); dB and dX are device arrays in
 // the column-major hecmwST layout (3N x nrhs).  Per-RHS results in iter/resid/error/
 // true_resid; returns the device time in ms and counts the kernels launched.
 float run_multi_chunk(Solver &S, int nrhs, const double *dB, double *dX, int iterpremax, double tol, int maxit,
-                      int *iter, double *resid, int *error, double *true_resid, int *kernels) {
+                      int *iter, double *resid, int *error, double *true_resid, int *kernels, bool learned = false) {
   cudaStream_t s = S.stream;
   const int n = S.N;
   const size_t n48 = size_t(n) * kRhsStride;
@@ -3562,8 +3610,8 @@ float run_multi_chunk(Solver &S, int nrhs, const double *dB, double *dX, int ite
   S.h_params->maxit = maxit;
   S.h_params->iterpremax = iterpremax;
   S.h_params->inner = 0;
-  S.h_params->flexible = 0;
-  S.h_params->use_gnn = 0;
+  S.h_params->flexible = learned ? 1 : 0;
+  S.h_params->use_gnn = learned ? 1 : 0;
   S.h_params->reliable = 0;
   S.h_params->ru_delta = 0.0;
   S.h_params->method = 1;
@@ -3574,12 +3622,15 @@ float run_multi_chunk(Solver &S, int nrhs, const double *dB, double *dX, int ite
   H33_CUDA(cudaMemcpyAsync(S.params.p, S.h_params, sizeof(CgParams), cudaMemcpyHostToDevice, s));
   H33_CUDA(cudaEventRecord(S.ev0, s));
   if (graph_mode()) {
-    build_graph_multi(S, iterpremax, nrhs);
+    build_graph_multi(S, iterpremax, nrhs, learned);
     H33_CUDA(cudaGraphLaunch(S.gm.exec, s));
   } else {
     launch_mr_prologue(S, nrhs, 0, 0);
     for (int it = 0; it <= maxit + kStreamChunk; it += kStreamChunk) {
-      for (int k = 0; k < kStreamChunk; k++) launch_mr_iteration(S, iterpremax, 0, 0);
+      for (int k = 0; k < kStreamChunk; k++) {
+        if (learned) launch_mr_iteration_learned(S, 0, 0);
+        else launch_mr_iteration(S, iterpremax, 0, 0);
+      }
       H33_CUDA(cudaGetLastError());
       H33_CUDA(cudaMemcpyAsync(S.h_mctl, S.mctl.p, sizeof(MultiCtl), cudaMemcpyDeviceToHost, s));
       S.sync();
@@ -3635,6 +3686,24 @@ int solve_multi(Solver &S, int nrhs, const double *dB, double *dX, int *Iarray, 
   recycle_precond_setting(Iarray);
   if (iterPREmax > 0) precond_setup(S, PRECOND, Iarray[33], sigma, Iarray);
   ensure_multi_buffers(S);
+  // Iarray(43) = 1: the learned two-level preconditioner for every load case (FP64
+  // smoother and recurrences; precision modes do not apply to multi-RHS solves)
+  bool learned = Iarray[42] == 1;
+  if (learned) {
+    if (iterPREmax != 1)
+      throw Failure(HECMW33_ERR_INCONS_PC, "the learned preconditioner applies one cycle per iteration (iterPREmax 1)");
+    S.L.coarse_mode = (Iarray[43] >= 0 && Iarray[43] <= 2) ? Iarray[43] : 0;
+    learned_prepare_inference(S);
+    learned = S.L.C.ok;  // a coarse matrix that is not positive definite: plain CG for all cases
+    const size_t n48 = size_t(S.N) * kRhsStride, nc16 = size_t(std::max(S.L.C.nc, 1)) * kMaxRhs;
+    S.mzs.alloc(n48);
+    if (S.mrold.n != n48) {
+      S.mrold.alloc(n48);
+      S.mrold.zero(S.stream);
+    }
+    S.mbc.alloc(nc16);
+    S.my.alloc(nc16);
+  }
   const double t1 = wall();
   Range rs("hecmw33_solve_multi");
   float ms = 0.0f;
@@ -3643,7 +3712,7 @@ int solve_multi(Solver &S, int nrhs, const double *dB, double *dX, int *Iarray, 
   for (int k0 = 0; k0 < nrhs; k0 += kMaxRhs) {
     const int m = std::min(kMaxRhs, nrhs - k0);
     ms += run_multi_chunk(S, m, dB + n3 * k0, dX + n3 * k0, iterPREmax, TOL, MAXIT, iter + k0, resid + k0,
-                          error + k0, true_resid + k0, &kernels);
+                          error + k0, true_resid + k0, &kernels, learned);
     for (int k = k0; k < k0 + m; k++) {
       if (!rc && error[k] != 0 && error[k] != HECMW33_ERR_ZERO_RHS) rc = error[k];
       if (!(error[k] == HECMW33_ERR_ZERO_RHS || true_resid[k] < TOL)) conv = 0;
@@ -3660,7 +3729,7 @@ int solve_multi(Solver &S, int nrhs, const double *dB, double *dX, int *Iarray, 
   S.last_solve_s = ms * 1e-3;
   S.last_setup_s = t1 - t0;
   S.last_true_resid = *std::max_element(true_resid, true_resid + nrhs);
-  S.last_learned = 0;
+  S.last_learned = learned ? 1 : 0;
   S.last_fallback = 0;
   if (times) {
     times[0] = t1 - t0;

@@ -206,7 +206,12 @@ HECMW33_API void hecmw33_gpu_solve(const int *handle, const int *N, const int *N
  * hecmw_solve_CG code of case k (2002 for a zero column, whose solution is 0);
  * true_resid[k] (may be NULL): ||b - A x|| / ||b|| after the solve.
  * Iarray(81) = 1 when every case reached Rarray(1); Iarray(82) = 1 when one diverged.
- * ierr: the first non-zero code of a case other than 2002, or 0. */
+ * ierr: the first non-zero code of a case other than 2002, or 0.
+ * Iarray(43) = 1 (no counterpart in the reference): every case runs the learned
+ * two-level preconditioner's flexible CG instead (see hecmw33_gpu_learn_record; FP64
+ * smoother and recurrences, Iarray(44) as for one solve, iterPREmax 1), with Ac^-1 read
+ * once per iteration for all cases; a coarse matrix that is not positive definite
+ * leaves every case on SSOR-CG.  Precision modes (Iarray(42)) do not apply here. */
 HECMW33_API void hecmw33_gpu_solve_multi(const int *handle, const int *nrhs, const double *B,
                                          double *X, int *Iarray, double *Rarray, int *iter,
                                          double *resid, int *error, double *true_resid,
