@@ -308,9 +308,11 @@ def face_load_cases(m, k, seed):
     return out
 
 
-def bench_multi(solver, m, nrhs=16):
+def bench_multi(solver, m, nrhs=16, learned=False):
     """16 load cases on the resident matrix: one multi-RHS solve (SpMM + 16-vector
-    sweeps) against the same 16 cases solved one after another (device times)."""
+    sweeps) against the same 16 cases solved one after another (device times).
+    learned: the same with the learned two-level preconditioner (Iarray(43) = 1, the
+    network trained above; FP64), against 16 learned solves one after another."""
     import numpy as np
     B = face_load_cases(m, nrhs, seed=11)
     ia, ra = m.Iarray.copy(), m.Rarray.copy()
@@ -327,13 +329,35 @@ def bench_multi(solver, m, nrhs=16):
         r1 = solver.solve_resident(B[k].copy(), x, ia.copy(), ra.copy())
         t_seq += r1["t_solve"]
         it_seq.append(int(r1["iter"]))
-    return {"load_cases": nrhs, "s": t_multi, "rhs_per_s": nrhs / t_multi, "sequential_s": t_seq,
-            "sequential_rhs_per_s": nrhs / t_seq, "speedup_vs_sequential": t_seq / t_multi,
-            "iterations": [int(v) for v in rec["iter"]], "sequential_iterations": it_seq,
-            "max_true_resid": float(np.max(rec["true_resid"])),
-            "errors": sorted(set(int(v) for v in rec["errors"])), "gpu_launches": kernels,
-            "workload": "%d random unit-norm tractions on the loaded face of the same matrix, CG+SSOR to 1e-8"
-                        % nrhs}
+    out = {"load_cases": nrhs, "s": t_multi, "rhs_per_s": nrhs / t_multi, "sequential_s": t_seq,
+           "sequential_rhs_per_s": nrhs / t_seq, "speedup_vs_sequential": t_seq / t_multi,
+           "iterations": [int(v) for v in rec["iter"]], "sequential_iterations": it_seq,
+           "max_true_resid": float(np.max(rec["true_resid"])),
+           "errors": sorted(set(int(v) for v in rec["errors"])), "gpu_launches": kernels,
+           "workload": "%d random unit-norm tractions on the loaded face of the same matrix, CG+SSOR to 1e-8"
+                       % nrhs}
+    if learned:
+        il = ia.copy()
+        il[42] = 1
+        X = np.zeros_like(B)
+        solver.solve_multi(B, X, il.copy(), ra.copy())  # warm
+        X = np.zeros_like(B)
+        rl = solver.solve_multi(B, X, il.copy(), ra.copy())
+        t_l = rl["t_solve"]
+        t_lseq, it_lseq = 0.0, []
+        for k in range(nrhs):
+            x = np.zeros(3 * m.N)
+            r1 = solver.solve_resident(B[k].copy(), x, il.copy(), ra.copy())
+            t_lseq += r1["t_solve"]
+            it_lseq.append(int(r1["iter"]))
+        out["learned"] = {"s": t_l, "rhs_per_s": nrhs / t_l, "speedup_vs_cg_ssor_multi": t_multi / t_l,
+                          "sequential_learned_s": t_lseq, "speedup_vs_sequential_learned": t_lseq / t_l,
+                          "iterations": [int(v) for v in rl["iter"]], "sequential_iterations": it_lseq,
+                          "max_true_resid": float(np.max(rl["true_resid"])),
+                          "errors": sorted(set(int(v) for v in rl["errors"])),
+                          "workload": "the same 16 cases, Iarray(43) = 1: flexible CG with the learned two-level "
+                                      "preconditioner (trained network, FP64 smoother), to 1e-8"}
+    return out
 
 
 def bench_config3(tol=1e-10):
@@ -984,7 +1008,7 @@ def main():
         # the 16-load-case, batched and config-3 figures are single-GPU measurements
         # reported at N = 1; replicas only repeat the headline
         args.no_multi = args.no_batched = args.no_config3 = args.no_assembly = args.no_domains = True
-    multi = None if args.no_multi else bench_multi(solver, m)
+    multi = None if args.no_multi else bench_multi(solver, m, learned=train is not None)
     config3 = None if args.no_config3 else bench_config3()
     assembly = None if args.no_assembly else bench_assembly()
     batched = None if args.no_batched else bench_batched(args)
