@@ -353,13 +353,15 @@ __global__ void __launch_bounds__(kThreads) mr_sweep_fwd_kernel(SellView<double>
 // Backward sweep; FUSE_RHO: per-RHS {r}{z} of the finished rows and, in the last
 // launch's last CTA, the RHO finisher of every RHS.  POS: updates zpos and writes the
 // finished rows to z in node order.
-template <int K, bool FUSE_RHO, bool POS>
+// DPOS (POS layouts): dpos receives each row's correction y - z per RHS, in position
+// order, for mr_lower_resid_kernel (a compile-time choice, as in sweep_bwd_uni_kernel).
+template <int K, bool FUSE_RHO, bool POS, bool DPOS = false>
 __global__ void __launch_bounds__(kThreads) mr_sweep_bwd_kernel(SellView<double> U, const int *__restrict__ perm,
                                                                 const double *__restrict__ alu, int npos,
                                                                 const double *__restrict__ r, double *__restrict__ z,
                                                                 double *__restrict__ zpos, int sb, int se, CgState *st,
                                                                 MultiCtl *ctl, double *partials, int part_base,
-                                                                int part_total) {
+                                                                int part_total, double *__restrict__ dpos) {
   pdl_entry();
   if (ctl && ctl->all_done) return;
   const int l = threadIdx.x & 15;
@@ -389,12 +391,43 @@ __global__ void __launch_bounds__(kThreads) mr_sweep_bwd_kernel(SellView<double>
     z[o] = z0;
     z[o + 16] = z1;
     z[o + 32] = z2;
+    if constexpr (DPOS) {
+      dpos[op] = x1;
+      dpos[op + 16] = x2;
+      dpos[op + 32] = x3;
+    }
     if (FUSE_RHO) dot += r[o] * z0 + r[o + 16] * z1 + r[o + 32] * z2;
   }
   if (FUSE_RHO)
     mr_reduce_finish(dot, partials, part_base + blockIdx.x, part_total, &ctl->ticket[0], [&](int k, double v) {
       if (!st[k].done) fin_rho(&st[k], v);
     });
+}
+
+// w = r - A z per RHS after z = SSOR(r) with dpos (unit SIGMA_DIAG): L (y - z) over the
+// smoother's lower layout (all colours, a half-warp per row), w in node order.
+template <int K>
+__global__ void __launch_bounds__(kThreads) mr_lower_resid_kernel(SellView<double> L, const int *__restrict__ perm,
+                                                                  const double *__restrict__ dpos,
+                                                                  double *__restrict__ w, const MultiCtl *ctl) {
+  pdl_entry();
+  if (ctl && ctl->all_done) return;
+  const int l = threadIdx.x & 15;
+  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  const int total = L.nslices * (32 / K);
+  const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; t < total; t += nhw) {
+    int s, roff;
+    if (!mr_locate<K>(L, 0, L.nslices, t, s, roff)) continue;
+    const int row = L.row0[s] + roff;
+    const int len = L.rowlen[s * 32 + roff];
+    double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+    mr_row<K>(L, s, roff, len, l, hmask, dpos, y0, y1, y2);
+    const size_t o = size_t(perm[row]) * kRhsStride + l;
+    w[o] = y0;
+    w[o + 16] = y1;
+    w[o + 32] = y2;
+  }
 }
 
 // Block-diagonal preconditioner for 16 RHS (optionally with the fused RHO).

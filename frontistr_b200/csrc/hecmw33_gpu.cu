@@ -443,7 +443,7 @@ struct Solver {
   GraphSlot g64, g32;
   // multi-RHS CG: node-major RHS-minor vectors (48 doubles per node), per-RHS states
   DevArray<double> mb, mx, mr, mz, mp, mq, mw, mzp, mzpos, mpart;
-  DevArray<double> mzs, mrold, mbc, my;  // the learned multi-RHS cycle (zs, r_old, P^T w, Ac^-1 P^T w)
+  DevArray<double> mzs, mrold, mbc, my, mdpos;  // the learned multi-RHS cycle (zs, r_old, P^T w, Ac^-1 P^T w, y - zs)
   DevArray<CgState> mst;
   DevArray<MultiCtl> mctl;
   CgState *h_mst = nullptr;
@@ -3314,7 +3314,7 @@ int solve_mixed_reliable(Solver &S, int *Iarray, double *Rarray, int *iter, doub
 
 template <int K, bool FUSE_RHO, bool POS>
 void launch_mr_sweep_k(Solver &S, const Precond &P, const DevSell<double> &Lo, const DevSell<double> &Up,
-                       const double *rin, double *zout) {
+                       const double *rin, double *zout, double *dpos = nullptr) {
   cudaStream_t s = S.stream;
   const int *perm_b = P.alu_shared ? P.perm_fwd.p : P.perm_bwd.p;
   const double *alu_b = P.alu_shared ? P.alu_fwd.p : P.alu_bwd.p;
@@ -3337,8 +3337,17 @@ void launch_mr_sweep_k(Solver &S, const Precond &P, const DevSell<double> &Lo, c
   for (int g = gb - 1; g >= 0; g--) {
     const int sb = Up.group_slice[g], se = Up.group_slice[g + 1];
     const int grid = S.grid_mr(std::max(se - sb, 1) * (32 / K));
-    launch_k(s, mr_sweep_bwd_kernel<K, FUSE_RHO, POS>, grid, kThreads, up, perm_b, alu_b, S.N, rin, zout, S.mzpos.p,
-                                                                     sb, se, S.mst.p, ctl, S.mpart.p, base, total);
+    bool done = false;
+    if constexpr (POS && !FUSE_RHO) {
+      if (dpos) {
+        launch_k(s, mr_sweep_bwd_kernel<K, FUSE_RHO, POS, true>, grid, kThreads, up, perm_b, alu_b, S.N, rin, zout,
+                 S.mzpos.p, sb, se, S.mst.p, ctl, S.mpart.p, base, total, dpos);
+        done = true;
+      }
+    }
+    if (!done)
+      launch_k(s, mr_sweep_bwd_kernel<K, FUSE_RHO, POS, false>, grid, kThreads, up, perm_b, alu_b, S.N, rin, zout,
+               S.mzpos.p, sb, se, S.mst.p, ctl, S.mpart.p, base, total, static_cast<double *>(nullptr));
     base += grid;
   }
 }
@@ -3446,17 +3455,31 @@ void launch_mr_iteration_learned(Solver &S, cudaGraphConditionalHandle h, int us
   const CoarseApply ca = C.apply_view();
   const int gs = S.grid_amr(), gn = S.grid_mr(S.N);
   const int n48 = S.N * kRhsStride;
-  auto smooth = [&](const double *rin, double *zout) {
+  auto smooth = [&](const double *rin, double *zout, double *dpos) {
     switch (P.lo.lanes) {
-      case 8: return launch_mr_sweep_k<8, false, true>(S, P, P.lo, P.up, rin, zout);
-      case 16: return launch_mr_sweep_k<16, false, true>(S, P, P.lo, P.up, rin, zout);
-      default: return launch_mr_sweep_k<4, false, true>(S, P, P.lo, P.up, rin, zout);
+      case 8: return launch_mr_sweep_k<8, false, true>(S, P, P.lo, P.up, rin, zout, dpos);
+      case 16: return launch_mr_sweep_k<16, false, true>(S, P, P.lo, P.up, rin, zout, dpos);
+      default: return launch_mr_sweep_k<4, false, true>(S, P, P.lo, P.up, rin, zout, dpos);
     }
   };
   launch_k(s, mr_iter_begin_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
-  smooth(S.mr.p, S.mzs.p);
-  launch_k(s, mr_spmv_kernel<1, kMrLanes>, gs, kThreads, S.amr_view(), static_cast<const double *>(S.mzs.p), S.mw.p,
-           static_cast<const double *>(S.mr.p), S.mst.p, S.mctl.p, S.mpart.p);
+  // w = r - A zs: L (y - zs) from the pre-smoothing's correction when SIGMA_DIAG is 1
+  // (as launch_learned_precond), else the SpMM
+  if (P.sigma == 1.0 && lower_resid_mode()) {
+    smooth(S.mr.p, S.mzs.p, S.mdpos.p);
+    const SellView<double> lo = P.lo.view();
+    const MultiCtl *cctl = S.mctl.p;
+    const int gl = S.grid_mr(P.lo.nslices * (32 / P.lo.lanes));
+    switch (P.lo.lanes) {
+      case 8: launch_k(s, mr_lower_resid_kernel<8>, gl, kThreads, lo, P.perm_fwd.p, static_cast<const double *>(S.mdpos.p), S.mw.p, cctl); break;
+      case 16: launch_k(s, mr_lower_resid_kernel<16>, gl, kThreads, lo, P.perm_fwd.p, static_cast<const double *>(S.mdpos.p), S.mw.p, cctl); break;
+      default: launch_k(s, mr_lower_resid_kernel<4>, gl, kThreads, lo, P.perm_fwd.p, static_cast<const double *>(S.mdpos.p), S.mw.p, cctl); break;
+    }
+  } else {
+    smooth(S.mr.p, S.mzs.p, nullptr);
+    launch_k(s, mr_spmv_kernel<1, kMrLanes>, gs, kThreads, S.amr_view(), static_cast<const double *>(S.mzs.p),
+             S.mw.p, static_cast<const double *>(S.mr.p), S.mst.p, S.mctl.p, S.mpart.p);
+  }
   launch_k(s, mr_coarse_restrict_kernel, std::max(1, C.nagg), kThreads, ca, static_cast<const double *>(S.mw.p),
            S.mbc.p, static_cast<const MultiCtl *>(S.mctl.p));
   launch_k(s, mr_coarse_gemm_kernel, std::max(1, (C.nc + kWarpsPerCta - 1) / kWarpsPerCta), kThreads, C.nc,
@@ -3465,7 +3488,7 @@ void launch_mr_iteration_learned(Solver &S, cudaGraphConditionalHandle h, int us
   launch_k(s, mr_coarse_prolong_resid_kernel, gn, kThreads, ca, static_cast<const double *>(S.my.p),
            static_cast<const double *>(S.mzs.p), S.mzp.p, S.mw.p, static_cast<const CgState *>(S.mst.p),
            static_cast<const MultiCtl *>(S.mctl.p));
-  smooth(S.mw.p, S.mz.p);
+  smooth(S.mw.p, S.mz.p, nullptr);
   const int gv = std::max(1, std::min((n48 + kThreads - 1) / kThreads, S.nsm * S.occ_vec));
   launch_k(s, add_kernel<double>, gv, kThreads, static_cast<const double *>(S.mzp.p), S.mz.p, n48,
            static_cast<const CgState *>(nullptr));
@@ -3697,6 +3720,7 @@ int solve_multi(Solver &S, int nrhs, const double *dB, double *dX, int *Iarray, 
     learned = S.L.C.ok;  // a coarse matrix that is not positive definite: plain CG for all cases
     const size_t n48 = size_t(S.N) * kRhsStride, nc16 = size_t(std::max(S.L.C.nc, 1)) * kMaxRhs;
     S.mzs.alloc(n48);
+    S.mdpos.alloc(n48);
     if (S.mrold.n != n48) {
       S.mrold.alloc(n48);
       S.mrold.zero(S.stream);
