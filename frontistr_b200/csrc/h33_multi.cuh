@@ -606,9 +606,9 @@ __global__ void mr_ctl_kernel(const CgState *st, MultiCtl *ctl, cudaGraphConditi
 // SSOR(r - A zc)) in flexible CG, with the smoother's sweeps and A streamed once for
 // all RHS, and Ac^-1 (FP32 copy) read once per iteration for all of them (a GEMM with
 // 16 columns instead of 16 GEMVs).  Coarse vectors are RHS-minor: bc[(3a+c)*16 + l].
-// A RHS whose correction was switched off (st.use_gnn = 0: the stagnation fallback)
-// keeps zc = zs and w, so its cycle is SSOR + SSOR of the unchanged residual ... as in
-// the single solve, the fallback leaves only the smoother.
+// A RHS whose correction was switched off (st.use_gnn = 0: the stagnation fallback of
+// loop_ctl, or a non-positive RHO) gets zc = zs and an unchanged w, so its
+// preconditioner is the two smoother steps alone, as the single solve's fallback.
 
 // Deterministic per-RHS reduction of two values (as mr_reduce_finish); partials hold
 // 32 doubles per CTA.
