@@ -607,8 +607,8 @@ __global__ void mr_ctl_kernel(const CgState *st, MultiCtl *ctl, cudaGraphConditi
 // all RHS, and Ac^-1 (FP32 copy) read once per iteration for all of them (a GEMM with
 // 16 columns instead of 16 GEMVs).  Coarse vectors are RHS-minor: bc[(3a+c)*16 + l].
 // A RHS whose correction was switched off (st.use_gnn = 0: the stagnation fallback of
-// loop_ctl, or a non-positive RHO) gets zc = zs and an unchanged w, so its
-// preconditioner is the two smoother steps alone, as the single solve's fallback.
+// loop_ctl, or a non-positive RHO) gets zc = zs and w = 0, so the post-smoothing adds
+// exactly nothing and z = zs = SSOR(r): SSOR-CG, as the single solve's fallback.
 
 // Deterministic per-RHS reduction of two values (as mr_reduce_finish); partials hold
 // 32 doubles per CTA.
@@ -797,7 +797,7 @@ __global__ void __launch_bounds__(kThreads) mr_coarse_gemm_kernel(int nc, const 
 }
 
 // zc = zs + P y and w -= (A P) y per RHS (a half-warp per node, lane = RHS); a RHS whose
-// correction is off keeps zc = zs and w.
+// correction is off gets zc = zs and w = 0.
 __global__ void __launch_bounds__(kThreads) mr_coarse_prolong_resid_kernel(CoarseApply c, const double *__restrict__ y,
                                                                            const double *__restrict__ zs,
                                                                            double *__restrict__ zc,
@@ -832,7 +832,7 @@ __global__ void __launch_bounds__(kThreads) mr_coarse_prolong_resid_kernel(Coars
 #pragma unroll
     for (int d = 0; d < 3; d++) {
       zc[o + 16 * d] = zs[o + 16 * d] + a[d];
-      if (on) w[o + 16 * d] -= q[d];
+      w[o + 16 * d] = on ? w[o + 16 * d] - q[d] : 0.0;
     }
   }
 }
