@@ -79,8 +79,8 @@ def parse():
     ap.add_argument("--profile-mode", type=int, default=0,
                     help="precision mode (Iarray(42)) of the --profile-solve solve")
     ap.add_argument("--profile-coarse", type=int, default=-1,
-                    help="with --profile-solve: the two-level preconditioner with these smoothing weights "
-                         "(Iarray(44): 1 none, 2 one half; no training needed)")
+                    help="with --profile-solve or --profile-multi: the two-level preconditioner with these "
+                         "smoothing weights (Iarray(44): 1 none, 2 one half; no training needed)")
     ap.add_argument("--profile-e2e", action="store_true",
                     help="one drop-in call with host buffers and a forced numeric rebuild (learned + mode 1, "
                          "network trained for 2 steps on 1 recorded solve), the last of 3 inside "
@@ -789,6 +789,9 @@ def main():
         B = face_load_cases(m, 16, seed=11)
         ia, ra = m.Iarray.copy(), m.Rarray.copy()
         ia[0] = 3
+        if args.profile_coarse >= 1:
+            ia[42] = 1
+            ia[43] = args.profile_coarse
         solver.solve_multi(B, np.zeros_like(B), ia, ra)
         return
     if args.profile_batch:

@@ -660,8 +660,14 @@ __device__ __forceinline__ void mr_reduce_finish2(double va, double vb, double *
   if (threadIdx.x == 0) *ticket = 0u;
 }
 
-// RHO = {z}{r} and DELTA = {z}{r_old} per RHS in one pass, then fin_rho_flex.
-__global__ void __launch_bounds__(kThreads) mr_fcg_rho_kernel(const double *__restrict__ z,
+// z = z + (zs + P y): the two-grid cycle's post-smoothing plus its coarse-corrected
+// part, the prolongation done here so that zc never goes through memory (P y is added
+// only for a RHS whose correction is on, in the order of
+// mr_coarse_resid_kernel's (A P) y); stored back into z.  Then RHO = {z}{r} and DELTA
+// = {z}{r_old} per RHS in the same pass and fin_rho_flex.
+__global__ void __launch_bounds__(kThreads) mr_fcg_rho_kernel(double *__restrict__ z,
+                                                              const double *__restrict__ zs, CoarseApply c,
+                                                              const double *__restrict__ y,
                                                               const double *__restrict__ r,
                                                               const double *__restrict__ r_old, int n, CgState *st,
                                                               MultiCtl *ctl, double *partials) {
@@ -669,15 +675,37 @@ __global__ void __launch_bounds__(kThreads) mr_fcg_rho_kernel(const double *__re
   if (ctl->all_done) return;
   const int l = threadIdx.x & 15;
   const int nhw = (gridDim.x * blockDim.x) >> 4;
+  const bool on = st[l].use_gnn;
   double a = 0.0, b = 0.0;
   if (!st[l].done) {
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < n; i += nhw) {
       const size_t o = size_t(i) * kRhsStride + l;
+      // the streamed operands first, so that their loads overlap the P y gathers
+      double zv[3], zsv[3], rv[3], rov[3];
 #pragma unroll
-      for (int c = 0; c < 3; c++) {
-        const double zi = z[o + 16 * c];
-        a += zi * r[o + 16 * c];
-        b += zi * r_old[o + 16 * c];
+      for (int d = 0; d < 3; d++) {
+        zv[d] = z[o + 16 * d];
+        zsv[d] = zs[o + 16 * d];
+        rv[d] = r[o + 16 * d];
+        rov[d] = r_old[o + 16 * d];
+      }
+      double py[3] = {0.0, 0.0, 0.0};
+      if (on) {
+        for (int k = c.pptr[i]; k < c.pptr[i + 1]; k++) {
+          const float *pb = c.p + 9 * size_t(k);
+          const size_t bo = size_t(3 * c.pagg[k]) * kMaxRhs + l;
+          const double y0 = y[bo], y1 = y[bo + 16], y2 = y[bo + 32];
+#pragma unroll
+          for (int d = 0; d < 3; d++)
+            py[d] += double(pb[3 * d]) * y0 + double(pb[3 * d + 1]) * y1 + double(pb[3 * d + 2]) * y2;
+        }
+      }
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double zi = zv[d] + (zsv[d] + py[d]);
+        z[o + 16 * d] = zi;
+        a += zi * rv[d];
+        b += zi * rov[d];
       }
     }
   }
@@ -755,54 +783,109 @@ __global__ void __launch_bounds__(kThreads) mr_coarse_restrict_kernel(CoarseAppl
   }
 }
 
-// y = Ac^-1 bc for 16 RHS (FP32 copy of Ac^-1, FP64 sums): a warp per row, 8 rows per
-// CTA sharing the bc chunk staged in shared memory; lane t takes columns t, t + 32, ...
-// of its row, then a butterfly sum per RHS.
-constexpr int kMrGemmChunk = 256;
-__global__ void __launch_bounds__(kThreads) mr_coarse_gemm_kernel(int nc, const float *__restrict__ ainv,
-                                                                  const double *__restrict__ bc,
-                                                                  double *__restrict__ y, const MultiCtl *ctl) {
+// y = Ac^-1 bc for 16 RHS (FP32 copy of Ac^-1, FP64 sums).  A CTA takes 16 rows:
+// each step stages a 16 x 128 tile of Ac^-1 and the matching 128 x 16 rows of bc in
+// shared memory, and every thread accumulates a 4-row x 4-RHS tile over the columns
+// k = s (mod 16) of its slice s; the 16 slices are then added in a fixed order (pairs
+// in the warp, then the 8 warps in order), so y does not depend on the grid.  The next
+// step's tiles are loaded into registers while the current one is multiplied.  Ac^-1
+// is read once per launch and bc once per CTA.
+constexpr int kMrGemmRows = 16;
+constexpr int kMrGemmChunk = 128;
+constexpr int kMrGemmSlices = kThreads / kMrGemmRows;
+constexpr int kMrGemmAPer = kMrGemmRows * kMrGemmChunk / kThreads;        // floats of Ac^-1 per thread and step
+constexpr int kMrGemmBPer = kMrGemmChunk * (kMaxRhs / 2) / kThreads;      // double2 of bc per thread and step
+static_assert(kMrGemmSlices == 16 && kMaxRhs == 16, "4 x 4 thread tiles of a 16 x 16 output block");
+static_assert(kMrGemmAPer * kThreads == kMrGemmRows * kMrGemmChunk && kMrGemmBPer * kThreads == kMrGemmChunk * 8,
+              "whole tiles per thread");
+__global__ void __launch_bounds__(kThreads, 3) mr_coarse_gemm_kernel(int nc, const float *__restrict__ ainv,
+                                                                     const double *__restrict__ bc,
+                                                                     double *__restrict__ y, const MultiCtl *ctl) {
   pdl_entry();
   if (ctl->all_done) return;
-  __shared__ double bs[kMrGemmChunk][kMaxRhs + 1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int r0 = blockIdx.x * kWarpsPerCta; r0 < nc; r0 += gridDim.x * kWarpsPerCta) {
-    const int row = r0 + warp;
-    double acc[kMaxRhs];
+  // row stride 129: the 8 (row, slice) pairs a load of a warp touches sit in 8 banks
+  __shared__ float as[kMrGemmRows][kMrGemmChunk + 1];
+  // row stride 18 doubles (144 bytes): the two slices of a warp read adjacent rows in
+  // disjoint banks
+  __shared__ __align__(16) double bs[kMrGemmChunk][kMaxRhs + 2];
+  __shared__ double red[kWarpsPerCta][kMrGemmRows][kMaxRhs];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int s = t >> 4, rg = (t >> 2) & 3, q = t & 3;
+  float ra[kMrGemmAPer];
+  double2 rb[kMrGemmBPer];
+  auto fetch = [&](int r0, int k0) {
+    const int kn = min(kMrGemmChunk, nc - k0);
 #pragma unroll
-    for (int l = 0; l < kMaxRhs; l++) acc[l] = 0.0;
+    for (int m = 0; m < kMrGemmAPer; m++) {
+      const int e = t + kThreads * m, r = e / kMrGemmChunk, k = e % kMrGemmChunk;
+      ra[m] = (r0 + r < nc && k < kn) ? __ldcs(ainv + size_t(r0 + r) * nc + k0 + k) : 0.0f;
+    }
+#pragma unroll
+    for (int m = 0; m < kMrGemmBPer; m++) {
+      const int e = t + kThreads * m, k = e / (kMaxRhs / 2), c2 = e % (kMaxRhs / 2);
+      rb[m] = k < kn ? reinterpret_cast<const double2 *>(bc + size_t(k0 + k) * kMaxRhs)[c2] : make_double2(0.0, 0.0);
+    }
+  };
+  for (int r0 = blockIdx.x * kMrGemmRows; r0 < nc; r0 += gridDim.x * kMrGemmRows) {
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) acc[i][c] = 0.0;
+    fetch(r0, 0);
     for (int k0 = 0; k0 < nc; k0 += kMrGemmChunk) {
-      const int kn = min(kMrGemmChunk, nc - k0);
-      __syncthreads();
-      for (int t = threadIdx.x; t < kn * kMaxRhs; t += blockDim.x) bs[t / kMaxRhs][t % kMaxRhs] = bc[size_t(k0) * kMaxRhs + t];
-      __syncthreads();
-      if (row < nc) {
-        const float *ar = ainv + size_t(row) * nc + k0;
-        for (int k = lane; k < kn; k += 32) {
-          const double a = double(ar[k]);
+      __syncthreads();  // the previous step's reads of as and bs are done
 #pragma unroll
-          for (int l = 0; l < kMaxRhs; l++) acc[l] += a * bs[k][l];
+      for (int m = 0; m < kMrGemmAPer; m++) {
+        const int e = t + kThreads * m;
+        as[e / kMrGemmChunk][e % kMrGemmChunk] = ra[m];
+      }
+#pragma unroll
+      for (int m = 0; m < kMrGemmBPer; m++) {
+        const int e = t + kThreads * m;
+        *reinterpret_cast<double2 *>(&bs[e / (kMaxRhs / 2)][2 * (e % (kMaxRhs / 2))]) = rb[m];
+      }
+      __syncthreads();
+      if (k0 + kMrGemmChunk < nc) fetch(r0, k0 + kMrGemmChunk);
+#pragma unroll 2
+      for (int j = 0; j < kMrGemmChunk / kMrGemmSlices; j++) {
+        const int k = s + kMrGemmSlices * j;
+        const double2 b01 = *reinterpret_cast<const double2 *>(&bs[k][4 * q]);
+        const double2 b23 = *reinterpret_cast<const double2 *>(&bs[k][4 * q + 2]);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const double a = double(as[4 * rg + i][k]);
+          acc[i][0] += a * b01.x;
+          acc[i][1] += a * b01.y;
+          acc[i][2] += a * b23.x;
+          acc[i][3] += a * b23.y;
         }
       }
     }
-    if (row < nc) {
 #pragma unroll
-      for (int l = 0; l < kMaxRhs; l++) {
-        double v = acc[l];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == l) y[size_t(row) * kMaxRhs + l] = v;
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const double v = acc[i][c] + __shfl_xor_sync(0xffffffffu, acc[i][c], 16);
+        if (lane < 16) red[warp][4 * rg + i][4 * q + c] = v;
       }
+    __syncthreads();
+    {
+      const int row = t >> 4, l = t & 15;
+      double v = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWarpsPerCta; w++) v += red[w][row][l];
+      if (r0 + row < nc) y[size_t(r0 + row) * kMaxRhs + l] = v;
     }
   }
 }
 
-// zc = zs + P y and w -= (A P) y per RHS (a half-warp per node, lane = RHS); a RHS whose
-// correction is off gets zc = zs and w = 0.
-__global__ void __launch_bounds__(kThreads) mr_coarse_prolong_resid_kernel(CoarseApply c, const double *__restrict__ y,
-                                                                           const double *__restrict__ zs,
-                                                                           double *__restrict__ zc,
-                                                                           double *__restrict__ w, const CgState *st,
-                                                                           const MultiCtl *ctl) {
+// w -= (A P) y per RHS (a half-warp per node, lane = RHS), the residual after the
+// coarse correction; a RHS whose correction is off gets w = 0 (its cycle is the plain
+// smoother).  The correction zs + P y itself is formed in mr_fcg_rho_kernel.
+__global__ void __launch_bounds__(kThreads) mr_coarse_resid_kernel(CoarseApply c, const double *__restrict__ y,
+                                                                   double *__restrict__ w, const CgState *st,
+                                                                   const MultiCtl *ctl) {
   pdl_entry();
   if (ctl->all_done) return;
   const int l = threadIdx.x & 15;
@@ -810,16 +893,15 @@ __global__ void __launch_bounds__(kThreads) mr_coarse_prolong_resid_kernel(Coars
   const int nhw = (gridDim.x * blockDim.x) >> 4;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < c.n; i += nhw) {
     const size_t o = size_t(i) * kRhsStride + l;
-    double a[3] = {0.0, 0.0, 0.0}, q[3] = {0.0, 0.0, 0.0};
-    if (on) {
-      for (int k = c.pptr[i]; k < c.pptr[i + 1]; k++) {
-        const float *pb = c.p + 9 * size_t(k);
-        const size_t b = size_t(3 * c.pagg[k]) * kMaxRhs + l;
-        const double y0 = y[b], y1 = y[b + 16], y2 = y[b + 32];
+    if (!on) {
 #pragma unroll
-        for (int d = 0; d < 3; d++)
-          a[d] += double(pb[3 * d]) * y0 + double(pb[3 * d + 1]) * y1 + double(pb[3 * d + 2]) * y2;
-      }
+      for (int d = 0; d < 3; d++) w[o + 16 * d] = 0.0;
+      continue;
+    }
+    double wv[3], q[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < 3; d++) wv[d] = w[o + 16 * d];  // overlaps the (A P) y gathers
+    {
       for (int k = c.qptr[i]; k < c.qptr[i + 1]; k++) {
         const float *qb = c.q + 9 * size_t(k);
         const size_t b = size_t(3 * c.qagg[k]) * kMaxRhs + l;
@@ -830,10 +912,7 @@ __global__ void __launch_bounds__(kThreads) mr_coarse_prolong_resid_kernel(Coars
       }
     }
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
-      zc[o + 16 * d] = zs[o + 16 * d] + a[d];
-      w[o + 16 * d] = on ? w[o + 16 * d] - q[d] : 0.0;
-    }
+    for (int d = 0; d < 3; d++) w[o + 16 * d] = wv[d] - q[d];
   }
 }
 

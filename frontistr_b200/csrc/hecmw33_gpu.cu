@@ -450,6 +450,9 @@ struct Solver {
   MultiCtl *h_mctl = nullptr;
   GraphSlot gm;
   int occ_mr = 4;
+  // the multi-RHS vector kernels of the learned iteration (fewer registers than the sweeps):
+  // the reductions (mr_fcg_rho_kernel) and the (A P) y residual
+  int occ_mrv = 4, occ_mrq = 4;
   // tiled SpMM of the multi-RHS loop: per 16-row tile its distinct columns, and each
   // block's place in that list
   DevArray<int> mt_ptr, mt_cols;
@@ -476,10 +479,14 @@ struct Solver {
     occ_sweep_uni = std::max(occ_sweep_uni, 1);
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_vec, update_xr_kernel<double>, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mr, mr_sweep_bwd_kernel<8, true, true>, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mrv, mr_fcg_rho_kernel, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mrq, mr_coarse_resid_kernel, kThreads, 0));
     occ_spmv = std::max(occ_spmv, 1);
     occ_sweep = std::max(occ_sweep, 1);
     occ_vec = std::max(occ_vec, 1);
     occ_mr = std::max(occ_mr, 1);
+    occ_mrv = std::max(occ_mrv, 1);
+    occ_mrq = std::max(occ_mrq, 1);
     H33_CUDA(cudaMallocHost(&h_params, sizeof(CgParams)));
     std::memset(h_params, 0, sizeof(CgParams));
     H33_CUDA(cudaMallocHost(&h_state, sizeof(CgState)));
@@ -525,6 +532,7 @@ struct Solver {
   }
   // multi-RHS kernels: one half-warp per block row
   int grid_mr(int rows) const { return std::max(1, std::min((rows + 15) / 16, nsm * occ_mr)); }
+  int grid_mrv(int rows) const { return std::max(1, std::min((rows + 15) / 16, nsm * occ_mrv)); }
   void sync() { H33_CUDA(cudaStreamSynchronize(stream)); }
 };
 
@@ -2570,7 +2578,6 @@ float run_gmres(Solver &S, int iterpremax, double tol, int maxit, int nrest, int
     H33_CUDA(cudaMemcpyAsync(g.s + 1, &rnorm, sizeof(double), cudaMemcpyHostToDevice, s));
     H33_CUDA(cudaMemsetAsync(S.g_flag.p, 0, sizeof(int), s));
     launched++;
-    bool broke = false;
     for (I = 1; I <= m; I++) {
       (*iter)++;
       precond(vec(I - 1), S.g_zq.p);
@@ -2593,10 +2600,7 @@ float run_gmres(Solver &S, int iterpremax, double tol, int maxit, int nrest, int
       H33_CUDA(cudaMemcpyAsync(&brk, S.g_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
       H33_CUDA(cudaMemcpyAsync(&rs, g.resid, sizeof(double), cudaMemcpyDeviceToHost, s));
       S.sync();
-      if (brk) {  // {w} = 0: the reference leaves the inner loop (:231)
-        broke = true;
-        break;
-      }
+      if (brk) break;  // {w} = 0: the reference leaves the inner loop (:231)
       *resid = rs;
       if (S.iterlog) std::printf("%8d%8d%16.6E\n", *iter, I + 1, rs);  // :286-287
       if (estcond > 0 && *iter % estcond == 0) gmres_condition(S, g.H, ld, I);  // :290-291
@@ -2612,7 +2616,6 @@ float run_gmres(Solver &S, int iterpremax, double tol, int maxit, int nrest, int
       }
     }
     if (exit_outer) break;
-    (void)broke;
     // current solution and the true residual of the restart (:331-377)
     finish(m);
     launch_k(s, spmv_kernel<double, 1>, S.grid_spmv(), kThreads, V.A, V.x, V.r, V.b, nullptr, nullptr);
@@ -3377,7 +3380,7 @@ void launch_mr_sweep(Solver &S, const double *rin, double *zout) {
 // Largest number of CTAs one reduction of the multi-RHS loop uses.
 int mr_max_parts(Solver &S) {
   Precond &P = S.pc;
-  int m = std::max(S.grid_amr(), S.grid_mr(S.N));
+  int m = std::max({S.grid_amr(), S.grid_mr(S.N), S.grid_mrv(S.N)});
   if (S.mt_occ > 0) m = std::max(m, std::min(S.mt_ntiles, S.nsm * S.mt_occ));
   if (P.valid && P.kind != 3) {
     const DevSell<double> &U = P.up;
@@ -3453,8 +3456,8 @@ void launch_mr_iteration_learned(Solver &S, cudaGraphConditionalHandle h, int us
   Precond &P = S.L.sm;
   auto &C = S.L.C;
   const CoarseApply ca = C.apply_view();
-  const int gs = S.grid_amr(), gn = S.grid_mr(S.N);
-  const int n48 = S.N * kRhsStride;
+  // gn: the vector kernels, sized by their own occupancy rather than the sweeps'
+  const int gs = S.grid_amr(), gn = S.grid_mrv(S.N);
   auto smooth = [&](const double *rin, double *zout, double *dpos) {
     switch (P.lo.lanes) {
       case 8: return launch_mr_sweep_k<8, false, true>(S, P, P.lo, P.up, rin, zout, dpos);
@@ -3482,18 +3485,15 @@ void launch_mr_iteration_learned(Solver &S, cudaGraphConditionalHandle h, int us
   }
   launch_k(s, mr_coarse_restrict_kernel, std::max(1, C.nagg), kThreads, ca, static_cast<const double *>(S.mw.p),
            S.mbc.p, static_cast<const MultiCtl *>(S.mctl.p));
-  launch_k(s, mr_coarse_gemm_kernel, std::max(1, (C.nc + kWarpsPerCta - 1) / kWarpsPerCta), kThreads, C.nc,
+  launch_k(s, mr_coarse_gemm_kernel, std::max(1, (C.nc + kMrGemmRows - 1) / kMrGemmRows), kThreads, C.nc,
            static_cast<const float *>(C.ainv32.p), static_cast<const double *>(S.mbc.p), S.my.p,
            static_cast<const MultiCtl *>(S.mctl.p));
-  launch_k(s, mr_coarse_prolong_resid_kernel, gn, kThreads, ca, static_cast<const double *>(S.my.p),
-           static_cast<const double *>(S.mzs.p), S.mzp.p, S.mw.p, static_cast<const CgState *>(S.mst.p),
-           static_cast<const MultiCtl *>(S.mctl.p));
+  launch_k(s, mr_coarse_resid_kernel, std::max(1, std::min((S.N + 15) / 16, S.nsm * S.occ_mrq)), kThreads, ca, static_cast<const double *>(S.my.p), S.mw.p,
+           static_cast<const CgState *>(S.mst.p), static_cast<const MultiCtl *>(S.mctl.p));
   smooth(S.mw.p, S.mz.p, nullptr);
-  const int gv = std::max(1, std::min((n48 + kThreads - 1) / kThreads, S.nsm * S.occ_vec));
-  launch_k(s, add_kernel<double>, gv, kThreads, static_cast<const double *>(S.mzp.p), S.mz.p, n48,
-           static_cast<const CgState *>(nullptr));
-  launch_k(s, mr_fcg_rho_kernel, gn, kThreads, static_cast<const double *>(S.mz.p),
-           static_cast<const double *>(S.mr.p), static_cast<const double *>(S.mrold.p), S.N, S.mst.p, S.mctl.p,
+  // z = SSOR(w) + (zs + P y), formed inside the RHO/DELTA pass
+  launch_k(s, mr_fcg_rho_kernel, gn, kThreads, S.mz.p, static_cast<const double *>(S.mzs.p), ca,
+           static_cast<const double *>(S.my.p), static_cast<const double *>(S.mr.p), static_cast<const double *>(S.mrold.p), S.N, S.mst.p, S.mctl.p,
            S.mpart.p);
   launch_k(s, mr_update_p_kernel, gn, kThreads, S.mz.p, S.mp.p, S.N, S.mst.p, S.mctl.p);
   launch_k(s, mr_spmv_kernel<2, kMrLanes>, gs, kThreads, S.amr_view(), S.mp.p, S.mq.p, nullptr, S.mst.p, S.mctl.p,
