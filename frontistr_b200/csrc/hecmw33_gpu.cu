@@ -450,9 +450,10 @@ struct Solver {
   MultiCtl *h_mctl = nullptr;
   GraphSlot gm;
   int occ_mr = 4;
-  // the multi-RHS vector kernels of the learned iteration (fewer registers than the sweeps):
-  // the reductions (mr_fcg_rho_kernel) and the (A P) y residual
-  int occ_mrv = 4, occ_mrq = 4;
+  // the multi-RHS vector kernels (fewer registers than the sweeps): the streamed updates
+  // (mr_update_xr_kernel), the learned iteration's RHO pass with its P y gathers and its
+  // (A P) y residual
+  int occ_mru = 4, occ_mrv = 4, occ_mrq = 4;
   // tiled SpMM of the multi-RHS loop: per 16-row tile its distinct columns, and each
   // block's place in that list
   DevArray<int> mt_ptr, mt_cols;
@@ -479,12 +480,14 @@ struct Solver {
     occ_sweep_uni = std::max(occ_sweep_uni, 1);
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_vec, update_xr_kernel<double>, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mr, mr_sweep_bwd_kernel<8, true, true>, kThreads, 0));
+    H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mru, mr_update_xr_kernel, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mrv, mr_fcg_rho_kernel, kThreads, 0));
     H33_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mrq, mr_coarse_resid_kernel, kThreads, 0));
     occ_spmv = std::max(occ_spmv, 1);
     occ_sweep = std::max(occ_sweep, 1);
     occ_vec = std::max(occ_vec, 1);
     occ_mr = std::max(occ_mr, 1);
+    occ_mru = std::max(occ_mru, 1);
     occ_mrv = std::max(occ_mrv, 1);
     occ_mrq = std::max(occ_mrq, 1);
     H33_CUDA(cudaMallocHost(&h_params, sizeof(CgParams)));
@@ -532,7 +535,8 @@ struct Solver {
   }
   // multi-RHS kernels: one half-warp per block row
   int grid_mr(int rows) const { return std::max(1, std::min((rows + 15) / 16, nsm * occ_mr)); }
-  int grid_mrv(int rows) const { return std::max(1, std::min((rows + 15) / 16, nsm * occ_mrv)); }
+  // a half-warp per row, at most occ resident CTAs per SM
+  int grid_rows(int rows, int occ) const { return std::max(1, std::min((rows + 15) / 16, nsm * occ)); }
   void sync() { H33_CUDA(cudaStreamSynchronize(stream)); }
 };
 
@@ -3380,7 +3384,7 @@ void launch_mr_sweep(Solver &S, const double *rin, double *zout) {
 // Largest number of CTAs one reduction of the multi-RHS loop uses.
 int mr_max_parts(Solver &S) {
   Precond &P = S.pc;
-  int m = std::max({S.grid_amr(), S.grid_mr(S.N), S.grid_mrv(S.N)});
+  int m = std::max({S.grid_amr(), S.grid_mr(S.N), S.grid_rows(S.N, S.occ_mru), S.grid_rows(S.N, S.occ_mrv)});
   if (S.mt_occ > 0) m = std::max(m, std::min(S.mt_ntiles, S.nsm * S.mt_occ));
   if (P.valid && P.kind != 3) {
     const DevSell<double> &U = P.up;
@@ -3432,7 +3436,7 @@ void launch_mr_prologue(Solver &S, int nrhs, cudaGraphConditionalHandle h, int u
 
 void launch_mr_iteration(Solver &S, int iterpremax, cudaGraphConditionalHandle h, int use_cond) {
   cudaStream_t s = S.stream;
-  const int gs = S.grid_amr(), gn = S.grid_mr(S.N);
+  const int gs = S.grid_amr(), gn = S.grid_rows(S.N, S.occ_mru);
   launch_k(s, mr_iter_begin_kernel, 1, 32, S.mst.p, S.mctl.p, h, use_cond);
   launch_mr_precond(S, iterpremax);
   launch_k(s, mr_update_p_kernel, gn, kThreads, S.mz.p, S.mp.p, S.N, S.mst.p, S.mctl.p);
@@ -3456,8 +3460,8 @@ void launch_mr_iteration_learned(Solver &S, cudaGraphConditionalHandle h, int us
   Precond &P = S.L.sm;
   auto &C = S.L.C;
   const CoarseApply ca = C.apply_view();
-  // gn: the vector kernels, sized by their own occupancy rather than the sweeps'
-  const int gs = S.grid_amr(), gn = S.grid_mrv(S.N);
+  // the vector kernels' grids from their own occupancy, not the sweeps'
+  const int gs = S.grid_amr(), gn = S.grid_rows(S.N, S.occ_mru), grho = S.grid_rows(S.N, S.occ_mrv);
   auto smooth = [&](const double *rin, double *zout, double *dpos) {
     switch (P.lo.lanes) {
       case 8: return launch_mr_sweep_k<8, false, true>(S, P, P.lo, P.up, rin, zout, dpos);
@@ -3488,11 +3492,11 @@ void launch_mr_iteration_learned(Solver &S, cudaGraphConditionalHandle h, int us
   launch_k(s, mr_coarse_gemm_kernel, std::max(1, (C.nc + kMrGemmRows - 1) / kMrGemmRows), kThreads, C.nc,
            static_cast<const float *>(C.ainv32.p), static_cast<const double *>(S.mbc.p), S.my.p,
            static_cast<const MultiCtl *>(S.mctl.p));
-  launch_k(s, mr_coarse_resid_kernel, std::max(1, std::min((S.N + 15) / 16, S.nsm * S.occ_mrq)), kThreads, ca, static_cast<const double *>(S.my.p), S.mw.p,
+  launch_k(s, mr_coarse_resid_kernel, S.grid_rows(S.N, S.occ_mrq), kThreads, ca, static_cast<const double *>(S.my.p), S.mw.p,
            static_cast<const CgState *>(S.mst.p), static_cast<const MultiCtl *>(S.mctl.p));
   smooth(S.mw.p, S.mz.p, nullptr);
   // z = SSOR(w) + (zs + P y), formed inside the RHO/DELTA pass
-  launch_k(s, mr_fcg_rho_kernel, gn, kThreads, S.mz.p, static_cast<const double *>(S.mzs.p), ca,
+  launch_k(s, mr_fcg_rho_kernel, grho, kThreads, S.mz.p, static_cast<const double *>(S.mzs.p), ca,
            static_cast<const double *>(S.my.p), static_cast<const double *>(S.mr.p), static_cast<const double *>(S.mrold.p), S.N, S.mst.p, S.mctl.p,
            S.mpart.p);
   launch_k(s, mr_update_p_kernel, gn, kThreads, S.mz.p, S.mp.p, S.N, S.mst.p, S.mctl.p);
