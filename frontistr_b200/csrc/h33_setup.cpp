@@ -412,8 +412,7 @@ void reordered_rows(const Profile &p, const std::vector<int> &perm, const std::v
   }
 }
 
-void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out, int lanes,
-                int max_runs) {
+void sell_shape(const int *count, const std::vector<int> &group_rows, SellLayout &out, int lanes, int max_runs) {
   if (lanes < 1 || lanes > 32 || (32 % lanes) != 0) throw std::runtime_error("lanes per row must divide 32");
   out = SellLayout();
   out.lanes = lanes;
@@ -428,10 +427,7 @@ void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellL
     for (int r0 = group_rows[g]; r0 < group_rows[g + 1]; r0 += per_slice) {
       const int nr = std::min(per_slice, group_rows[g + 1] - r0);
       int len = 0;
-      for (int l = 0; l < nr; l++) {
-        const int n = int(rows.ptr[r0 + l + 1] - rows.ptr[r0 + l]);
-        len = std::max(len, (n + lanes - 1) / lanes);
-      }
+      for (int l = 0; l < nr; l++) len = std::max(len, (count[r0 + l] + lanes - 1) / lanes);
       lens.push_back(len);
     }
     if (max_runs > 0) {
@@ -485,6 +481,16 @@ void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellL
   }
   out.nslices = int(out.row0.size());
   out.rowlen.assign(size_t(out.nslices) * 32, 0);
+  for (int s = 0; s < out.nslices; s++)
+    for (int r = 0; r < out.nrows[s]; r++) out.rowlen[size_t(s) * 32 + r] = count[out.row0[s] + r];
+}
+
+void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out, int lanes,
+                int max_runs) {
+  const int nrows = int(rows.ptr.size()) - 1;
+  std::vector<int> count(size_t(std::max(nrows, 0)));
+  for (int r = 0; r < nrows; r++) count[size_t(r)] = int(rows.ptr[r + 1] - rows.ptr[r]);
+  sell_shape(count.data(), group_rows, out, lanes, max_runs);
   out.col.assign(size_t(out.nslots) * 32, 0);
   out.src.assign(size_t(out.nslots) * 32, -1);
   // block k of the row at offset r of slice s sits in slot k / lanes, lane r*lanes + k % lanes
@@ -494,7 +500,6 @@ void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellL
       const int row = out.row0[s] + r;
       const int64_t b = rows.ptr[row];
       const int n = int(rows.ptr[row + 1] - b);
-      out.rowlen[size_t(s) * 32 + r] = n;
       for (int k = 0; k < n; k++) {
         const size_t at = (size_t(out.slot0[s]) + k / lanes) * 32 + size_t(r) * lanes + k % lanes;
         out.col[at] = rows.col[b + k];
@@ -584,10 +589,20 @@ void element_contributions(int n_node, int n_elem, int nn, const int *conn, cons
 void order_rows_by_length(const BlockRows &lower, const BlockRows &upper, const std::vector<int> &group_rows,
                           int lanes, std::vector<int> &order) {
   const int n = int(lower.ptr.size()) - 1;
+  std::vector<int> nl(size_t(std::max(n, 0))), nu(size_t(std::max(n, 0)));
+  for (int r = 0; r < n; r++) {
+    nl[size_t(r)] = int(lower.ptr[r + 1] - lower.ptr[r]);
+    nu[size_t(r)] = int(upper.ptr[r + 1] - upper.ptr[r]);
+  }
+  order_rows_by_counts(nl.data(), nu.data(), n, group_rows, lanes, order);
+}
+
+void order_rows_by_counts(const int *nl, const int *nu, int n, const std::vector<int> &group_rows, int lanes,
+                          std::vector<int> &order) {
   order.resize(size_t(n));
-  auto cls = [lanes](const BlockRows &br, int r) { return int((br.ptr[r + 1] - br.ptr[r] + lanes - 1) / lanes); };
+  auto cls = [lanes](const int *c, int r) { return (c[r] + lanes - 1) / lanes; };
   int maxu = 0;
-  for (int r = 0; r < n; r++) maxu = std::max(maxu, cls(upper, r));
+  for (int r = 0; r < n; r++) maxu = std::max(maxu, cls(nu, r));
   // a stable counting sort of each group by the key (lower slots, upper slots)
   const int ng = int(group_rows.size()) - 1;
 #pragma omp parallel for schedule(dynamic, 1)
@@ -596,7 +611,7 @@ void order_rows_by_length(const BlockRows &lower, const BlockRows &upper, const 
     std::vector<int> key(size_t(r1 - r0));
     int kmax = 0;
     for (int r = r0; r < r1; r++) {
-      key[size_t(r - r0)] = cls(lower, r) * (maxu + 1) + cls(upper, r);
+      key[size_t(r - r0)] = cls(nl, r) * (maxu + 1) + cls(nu, r);
       kmax = std::max(kmax, key[size_t(r - r0)]);
     }
     std::vector<int> start(size_t(kmax) + 2, 0);

@@ -86,6 +86,12 @@ struct SellLayout {
 // finds a slice's first slot and slot count from its index and the group's table.
 void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellLayout &out,
                 int lanes = 1, int max_runs = 0);
+// The same layout from the rows' block counts alone (count[r] blocks in row r): every
+// field but col and src, which the device fills (block k of the row at offset r of
+// slice s goes to slot slot0[s] + k / lanes, lane r * lanes + k % lanes; padding col
+// 0, src -1).
+void sell_shape(const int *count, const std::vector<int> &group_rows, SellLayout &out, int lanes = 1,
+                int max_runs = 0);
 
 // Order of the rows inside each group for the sliced layouts of a lower and an upper
 // part with the same rows: sorted by (lower slot count, upper slot count) at `lanes`
@@ -93,6 +99,9 @@ void build_sell(const BlockRows &rows, const std::vector<int> &group_rows, SellL
 // distinct slot counts.  order[new] = old row; rows never leave their group.
 void order_rows_by_length(const BlockRows &lower, const BlockRows &upper, const std::vector<int> &group_rows,
                           int lanes, std::vector<int> &order);
+// The same from the rows' lower and upper block counts (n rows).
+void order_rows_by_counts(const int *nl, const int *nu, int n, const std::vector<int> &group_rows, int lanes,
+                          std::vector<int> &order);
 
 // Rows of `in` taken in the order `order` (order[new] = old row) and columns renamed
 // by iorder (iorder[old] = new); the blocks of each row keep their order.

@@ -39,6 +39,7 @@
 #include "h33_gmres.cuh"
 #include "h33_gnn.cuh"
 #include "h33_kernels.cuh"
+#include "h33_layout.cuh"
 #include "h33_multi.cuh"
 #include "h33_setup.h"
 #include "h33_vecops.cuh"
@@ -173,6 +174,22 @@ double wall() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// HECMW33_SETUP_TRACE=1 prints the wall time of each setup phase (host orderings,
+// layouts, uploads, device packing, graph capture) on stderr, the device synchronised
+// at every mark so that a phase owns its own device work.  Off: one branch per mark.
+void setup_mark(const char *what) {
+  static const bool on = [] {
+    const char *e = std::getenv("HECMW33_SETUP_TRACE");
+    return e && e[0] == '1';
+  }();
+  static double last = 0.0;
+  if (!on) return;
+  cudaDeviceSynchronize();
+  const double t = wall();
+  std::fprintf(stderr, "[setup] %-36s %9.1f ms\n", what, last > 0.0 ? 1e3 * (t - last) : 0.0);
+  last = t;
+}
+
 // Device copy of a sliced layout plus its values.
 template <class T>
 struct DevSell {
@@ -186,6 +203,13 @@ struct DevSell {
 
   int lanes = 1;
   void upload(const SellLayout &L, cudaStream_t s) {
+    upload_shape(L, s);
+    H33_CUDA(cudaMemcpyAsync(col.p, L.col.data(), col.bytes(), cudaMemcpyHostToDevice, s));
+    H33_CUDA(cudaMemcpyAsync(src.p, L.src.data(), src.bytes(), cudaMemcpyHostToDevice, s));
+  }
+  // Everything but the blocks' columns and raw ids, which a fill kernel writes into
+  // col and src (cleared here to the padding: column 0, raw id -1).
+  void upload_shape(const SellLayout &L, cudaStream_t s) {
     nslices = L.nslices;
     lanes = L.lanes;
     nslots = int(L.nslots);
@@ -194,8 +218,10 @@ struct DevSell {
     slot0.upload(L.slot0, s);
     len.upload(L.len, s);
     rowlen.upload(L.rowlen, s);
-    col.upload(L.col, s);
-    src.upload(L.src, s);
+    col.alloc(size_t(nslots) * 32);
+    src.alloc(size_t(nslots) * 32);
+    col.zero(s);
+    if (src.n) H33_CUDA(cudaMemsetAsync(src.p, 0xff, src.bytes(), s));
     val.alloc(size_t(nslots) * 288);
     group_slice = L.group_slice;
     run_ptr = L.run_ptr;
@@ -376,6 +402,7 @@ struct Solver {
   int generation = 0;
   bool zero_diag = false;
   std::vector<int> indexL, itemL, indexU, itemU;
+  DevArray<int> d_indexL, d_itemL, d_indexU, d_itemU;  // the same profile on the device (layout fills)
   DevArray<double> raw;
   DevSell<double> A;
   // vectors and scalars
@@ -575,6 +602,44 @@ void validate(int N, int NP, int NPL, int NPU, const int *indexL, const int *ite
 }
 
 // Symbolic part of set_matrix: host copy of the profile, SpMV layout, vectors.
+// HECMW33_HOST_LAYOUT=1 builds the sliced layouts wholly on the host (unified_rows,
+// reordered_rows, build_sell: the reference for the device fill, which gives the same
+// layouts entry for entry); read at every symbolic setup.
+bool host_layouts() {
+  const char *e = std::getenv("HECMW33_HOST_LAYOUT");
+  return e && e[0] == '1';
+}
+
+DevProfile dev_profile(const Solver &S) {
+  return DevProfile{S.N, S.NPL, S.d_indexL.p, S.d_itemL.p, S.d_indexU.p, S.d_itemU.p};
+}
+
+// The matrix's unified rows (L, D, U of each row) in a sliced layout of `lanes` lanes
+// per row, rows in input order as one group: the shape from the rows' block counts on
+// the host, the blocks placed by fill_unified_kernel.
+void build_unified(Solver &S, DevSell<double> &D, int lanes) {
+  const int N = S.N;
+  if (host_layouts()) {
+    Profile prof{N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
+    BlockRows rows;
+    unified_rows(prof, rows);
+    SellLayout lay;
+    build_sell(rows, std::vector<int>{0, N}, lay, lanes);
+    D.upload(lay, S.stream);
+    return;
+  }
+  std::vector<int> count(static_cast<size_t>(N));
+  for (int i = 0; i < N; i++)
+    count[size_t(i)] = (S.indexL[size_t(i) + 1] - S.indexL[size_t(i)]) + 1 + (S.indexU[size_t(i) + 1] - S.indexU[size_t(i)]);
+  SellLayout lay;
+  sell_shape(count.data(), std::vector<int>{0, N}, lay, lanes);
+  D.upload_shape(lay, S.stream);
+  const int grid = std::max(1, std::min((N + kThreads - 1) / kThreads, S.nsm * 8));
+  launch_k(S.stream, fill_unified_kernel, grid, kThreads, dev_profile(S), lanes, static_cast<const int *>(D.slot0.p),
+           D.col.p, D.src.p);
+  H33_CUDA(cudaGetLastError());
+}
+
 void set_profile(Solver &S, int N, int NPL, int NPU, const int *indexL, const int *itemL, const int *indexU,
                  const int *itemU) {
   S.has_matrix = false;
@@ -586,12 +651,12 @@ void set_profile(Solver &S, int N, int NPL, int NPU, const int *indexL, const in
   S.itemL.assign(itemL, itemL + NPL);
   S.indexU.assign(indexU, indexU + N + 1);
   S.itemU.assign(itemU, itemU + NPU);
-  Profile prof{N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
-  BlockRows rows;
-  unified_rows(prof, rows);
-  SellLayout lay;
-  build_sell(rows, std::vector<int>{0, N}, lay);
-  S.A.upload(lay, S.stream);
+  S.d_indexL.upload(S.indexL, S.stream);
+  S.d_itemL.upload(S.itemL, S.stream);
+  S.d_indexU.upload(S.indexU, S.stream);
+  S.d_itemU.upload(S.itemU, S.stream);
+  setup_mark("set_matrix: profile up");
+  build_unified(S, S.A, 1);
   const size_t n3 = size_t(3) * N;
   for (auto *v : {&S.b, &S.x, &S.r, &S.z, &S.p, &S.q, &S.w, &S.zp}) v->alloc(n3);
   S.partials.alloc(size_t(std::max(N / 32 + 64, S.nsm * 16)) + 1024);
@@ -695,7 +760,9 @@ void set_matrix_square(Solver &S, int N, int NPL, int NPU, const int *indexL, co
                        const int *Iarray) {
   const bool symbolic = !S.has_matrix || N != S.N || NPL != S.NPL || NPU != S.NPU || Iarray == nullptr ||
                         Iarray[97] != 0;
+  setup_mark("set_matrix: start");
   if (symbolic) set_profile(S, N, NPL, NPU, indexL, itemL, indexU, itemU);
+  setup_mark("set_matrix: profile + SpMV layout");
   const size_t nb = size_t(N) + NPL + NPU;
   S.raw.alloc(9 * nb);
   H33_CUDA(cudaMemcpyAsync(S.raw.p, D, sizeof(double) * 9 * N, cudaMemcpyHostToDevice, S.stream));
@@ -712,6 +779,7 @@ void set_matrix_square(Solver &S, int N, int NPL, int NPU, const int *indexL, co
       if (std::fabs(D[9 * size_t(i) + 4 * j]) == 0.0) S.zero_diag = true;
   S.has_matrix = true;
   S.sync();
+  setup_mark("set_matrix: values up + packed");
 }
 
 // ---------------------------------------------------------------------------
@@ -733,41 +801,107 @@ void setup_ssor(Solver &S, Precond &P, int ncolor_in, double sigma, bool symboli
   if (symbolic) {
     Profile prof{S.N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
     std::vector<int> perm_rcm, iperm_rcm, perm, iperm, colorindex;
+    setup_mark("ssor: start");
     if (greedy) {
       P.ncolor = ordering_greedy(prof, colorindex, perm, iperm);
+      setup_mark("ssor: first-fit colouring");
     } else {
       ordering_rcm(prof, perm_rcm, iperm_rcm);
+      setup_mark("ssor: RCM");
       P.ncolor = ordering_mc(prof, perm_rcm, ncolor_in, colorindex, perm, iperm);
+      setup_mark("ssor: multicolouring");
     }
-    BlockRows lower_ref, upper_ref, lower, upper;
-    reordered_rows(prof, perm, iperm, lower_ref, upper_ref);
-    // the device sweeps gather from their colour-ordered intermediate: columns as
-    // positions (the same blocks in the same order; only the index names change)
-    for (auto *br : {&lower_ref, &upper_ref})
-      for (int &c : br->col) c = iperm[c];
-    // inside each colour the device places its rows by slot count (rows of one
-    // colour never read each other, so the sweep's arithmetic per row is unchanged):
-    // the slices of a colour then need few distinct slot counts and little padding
     const int lanes = sweep_lanes();
-    std::vector<int> order, iorder(size_t(S.N));
-    order_rows_by_length(lower_ref, upper_ref, colorindex, lanes, order);
-    for (int i = 0; i < S.N; i++) iorder[size_t(order[size_t(i)])] = i;
-    permute_rows(lower_ref, order, iorder, lower);
-    permute_rows(upper_ref, order, iorder, upper);
-    std::vector<int> perm_dev(size_t(S.N));
-    for (int i = 0; i < S.N; i++) perm_dev[size_t(i)] = perm[size_t(order[size_t(i)])];
-    SellLayout lo, up;
-    build_sell(lower, colorindex, lo, lanes, kMaxRuns);
-    build_sell(upper, colorindex, up, lanes, kMaxRuns);
+    if (host_layouts()) {
+      BlockRows lower_ref, upper_ref, lower, upper;
+      reordered_rows(prof, perm, iperm, lower_ref, upper_ref);
+      // the device sweeps gather from their colour-ordered intermediate: columns as
+      // positions (the same blocks in the same order; only the index names change)
+      for (auto *br : {&lower_ref, &upper_ref})
+        for (int &c : br->col) c = iperm[c];
+      // inside each colour the device places its rows by slot count (rows of one
+      // colour never read each other, so the sweep's arithmetic per row is unchanged):
+      // the slices of a colour then need few distinct slot counts and little padding
+      std::vector<int> order, iorder(size_t(S.N));
+      order_rows_by_length(lower_ref, upper_ref, colorindex, lanes, order);
+      for (int i = 0; i < S.N; i++) iorder[size_t(order[size_t(i)])] = i;
+      permute_rows(lower_ref, order, iorder, lower);
+      permute_rows(upper_ref, order, iorder, upper);
+      std::vector<int> perm_dev(size_t(S.N));
+      for (int i = 0; i < S.N; i++) perm_dev[size_t(i)] = perm[size_t(order[size_t(i)])];
+      SellLayout lo, up;
+      build_sell(lower, colorindex, lo, lanes, kMaxRuns);
+      build_sell(upper, colorindex, up, lanes, kMaxRuns);
+      P.lo.upload(lo, S.stream);
+      P.up.upload(up, S.stream);
+      P.perm_fwd.upload(perm_dev, S.stream);
+    } else {
+      // the same layouts with the O(blocks) work on the device: the rows' lower and
+      // upper block counts in the new order (count_parts_kernel), the row order inside
+      // each colour and the layouts' shape from those counts on the host, the blocks
+      // placed by fill_reordered_kernel
+      const int N = S.N;
+      const DevProfile dp = dev_profile(S);
+      DevArray<int> d_perm, d_iperm, d_nl, d_nu, d_order, d_iorder, d_row_slice;
+      d_perm.upload(perm, S.stream);
+      d_iperm.upload(iperm, S.stream);
+      d_nl.alloc(size_t(N));
+      d_nu.alloc(size_t(N));
+      const int grid = std::max(1, std::min((N + kThreads - 1) / kThreads, S.nsm * 8));
+      launch_k(S.stream, count_parts_kernel, grid, kThreads, dp, static_cast<const int *>(d_iperm.p), d_nl.p, d_nu.p);
+      H33_CUDA(cudaGetLastError());
+      std::vector<int> nl(static_cast<size_t>(N)), nu(static_cast<size_t>(N));
+      H33_CUDA(cudaMemcpyAsync(nl.data(), d_nl.p, sizeof(int) * size_t(N), cudaMemcpyDeviceToHost, S.stream));
+      H33_CUDA(cudaMemcpyAsync(nu.data(), d_nu.p, sizeof(int) * size_t(N), cudaMemcpyDeviceToHost, S.stream));
+      S.sync();
+      setup_mark("  ssor layouts: row counts (device)");
+      const size_t nn = static_cast<size_t>(N);
+      std::vector<int> order, iorder(nn), cl(nn), cu(nn), perm_dev(nn);
+      order_rows_by_counts(nl.data(), nu.data(), N, colorindex, lanes, order);
+      for (int q = 0; q < N; q++) {
+        const int i = order[size_t(q)];
+        iorder[size_t(i)] = q;
+        cl[size_t(q)] = nl[size_t(i)];
+        cu[size_t(q)] = nu[size_t(i)];
+        perm_dev[size_t(q)] = perm[size_t(i)];
+      }
+      SellLayout lo, up;
+      sell_shape(cl.data(), colorindex, lo, lanes, kMaxRuns);
+      sell_shape(cu.data(), colorindex, up, lanes, kMaxRuns);
+      // both parts cut the colours into the same slices (same groups, same rows per slice)
+      std::vector<int> row_slice(nn);
+      for (int sl = 0; sl < lo.nslices; sl++)
+        for (int r = 0; r < lo.nrows[size_t(sl)]; r++) row_slice[size_t(lo.row0[size_t(sl)] + r)] = sl;
+      setup_mark("  ssor layouts: row order, shape (host)");
+      P.lo.upload_shape(lo, S.stream);
+      P.up.upload_shape(up, S.stream);
+      setup_mark("  ssor layouts: shape up, arrays allocated");
+      d_order.upload(order, S.stream);
+      d_iorder.upload(iorder, S.stream);
+      d_row_slice.upload(row_slice, S.stream);
+      const int gw = std::max(1, std::min((N + kWarpsPerCta - 1) / kWarpsPerCta, S.nsm * 8));
+      launch_k(S.stream, fill_reordered_kernel<true>, gw, kThreads, dp, static_cast<const int *>(d_perm.p),
+               static_cast<const int *>(d_iperm.p), static_cast<const int *>(d_order.p),
+               static_cast<const int *>(d_iorder.p), static_cast<const int *>(d_row_slice.p),
+               static_cast<const int *>(P.lo.row0.p), static_cast<const int *>(P.lo.slot0.p), lanes, P.lo.col.p,
+               P.lo.src.p);
+      launch_k(S.stream, fill_reordered_kernel<false>, gw, kThreads, dp, static_cast<const int *>(d_perm.p),
+               static_cast<const int *>(d_iperm.p), static_cast<const int *>(d_order.p),
+               static_cast<const int *>(d_iorder.p), static_cast<const int *>(d_row_slice.p),
+               static_cast<const int *>(P.up.row0.p), static_cast<const int *>(P.up.slot0.p), lanes, P.up.col.p,
+               P.up.src.p);
+      H33_CUDA(cudaGetLastError());
+      P.perm_fwd.upload(perm_dev, S.stream);
+      S.sync();  // the fills read the temporaries above
+      setup_mark("  ssor layouts: blocks placed (device)");
+    }
+    setup_mark("ssor: layouts");
     P.pos_cols = true;
     // padding blocks gather zpos[0]: it must hold finite values from the start
     S.zpos.alloc(size_t(3) * S.N);
     S.zpos.zero(S.stream);
-    P.lo.upload(lo, S.stream);
-    P.up.upload(up, S.stream);
     P.lo.group_rows = colorindex;
     P.up.group_rows = colorindex;
-    P.perm_fwd.upload(perm_dev, S.stream);
     P.colorindex = colorindex;
     P.perm = perm;  // the reference's ordering (reported); the device uses perm_dev
     P.alu_shared = true;
@@ -775,6 +909,7 @@ void setup_ssor(Solver &S, Precond &P, int ncolor_in, double sigma, bool symboli
   P.lo.pack(S.raw.p, S.stream, S.nsm);
   P.up.pack(S.raw.p, S.stream, S.nsm);
   diag_alu(S, P.alu_fwd, S.raw.p, P.perm_fwd.p, sigma, 0);
+  setup_mark("ssor: value packing + diagonal LU");
 }
 
 // Block ILU(p) (hecmw_precond_BILU_33.f90): p = 0 on the matrix's own pattern
@@ -1591,37 +1726,53 @@ void learned_graph(Solver &S) {
   const int N = S.N;
   if (L.graph_generation < 0 || L.built_for != S.generation) {
     const int NPL = S.NPL;
-    std::vector<int> ptr(size_t(N) + 1, 0), col, src, row_of, rev;
-    col.reserve(size_t(S.NPL) + S.NPU);
-    for (int i = 0; i < N; i++) {
-      for (int j = S.indexL[i]; j < S.indexL[i + 1]; j++) {
-        col.push_back(S.itemL[j] - 1);
-        src.push_back(N + j);
-        row_of.push_back(i);
-      }
-      for (int j = S.indexU[i]; j < S.indexU[i + 1]; j++) {
-        col.push_back(S.itemU[j] - 1);
-        src.push_back(N + NPL + j);
-        row_of.push_back(i);
-      }
-      ptr[i + 1] = int(col.size());
-    }
-    const int ne = int(col.size());
-    rev.assign(size_t(ne), 0);
-#pragma omp parallel for schedule(static)
-    for (int e = 0; e < ne; e++) {
-      const int i = row_of[e], j = col[e];
-      const int *b = col.data() + ptr[j], *en = col.data() + ptr[j + 1];
-      const int *f = std::lower_bound(b, en, i);
-      rev[e] = (f != en && *f == i) ? int(f - col.data()) : e;
-    }
+    std::vector<int> ptr(size_t(N) + 1, 0);
+    for (int i = 0; i < N; i++)
+      ptr[size_t(i) + 1] = ptr[size_t(i)] + (S.indexL[size_t(i) + 1] - S.indexL[size_t(i)]) +
+                           (S.indexU[size_t(i) + 1] - S.indexU[size_t(i)]);
+    const int ne = ptr[size_t(N)];
     L.n = N;
     L.nedges = ne;
     L.ptr.upload(ptr, S.stream);
-    L.col.upload(col, S.stream);
-    L.src.upload(src, S.stream);
-    L.row_of.upload(row_of, S.stream);
-    L.rev.upload(rev, S.stream);
+    if (host_layouts()) {
+      std::vector<int> col, src, row_of, rev;
+      col.reserve(size_t(ne));
+      for (int i = 0; i < N; i++) {
+        for (int j = S.indexL[i]; j < S.indexL[i + 1]; j++) {
+          col.push_back(S.itemL[j] - 1);
+          src.push_back(N + j);
+          row_of.push_back(i);
+        }
+        for (int j = S.indexU[i]; j < S.indexU[i + 1]; j++) {
+          col.push_back(S.itemU[j] - 1);
+          src.push_back(N + NPL + j);
+          row_of.push_back(i);
+        }
+      }
+      rev.assign(size_t(ne), 0);
+#pragma omp parallel for schedule(static)
+      for (int e = 0; e < ne; e++) {
+        const int i = row_of[e], j = col[e];
+        const int *b = col.data() + ptr[j], *en = col.data() + ptr[j + 1];
+        const int *f = std::lower_bound(b, en, i);
+        rev[e] = (f != en && *f == i) ? int(f - col.data()) : e;
+      }
+      L.col.upload(col, S.stream);
+      L.src.upload(src, S.stream);
+      L.row_of.upload(row_of, S.stream);
+      L.rev.upload(rev, S.stream);
+    } else {
+      // the edges, their raw ids, rows and reverses placed on the device from the
+      // resident profile
+      for (auto *a : {&L.col, &L.src, &L.row_of, &L.rev}) a->alloc(size_t(ne));
+      const int gr = std::max(1, std::min((N + kThreads - 1) / kThreads, S.nsm * 8));
+      launch_k(S.stream, fill_edges_kernel, gr, kThreads, dev_profile(S), static_cast<const int *>(L.ptr.p), L.col.p,
+               L.src.p, L.row_of.p);
+      const int ge = std::max(1, std::min((ne + kThreads - 1) / kThreads, S.nsm * 16));
+      launch_k(S.stream, edge_reverse_kernel, ge, kThreads, N, static_cast<const int *>(L.ptr.p),
+               static_cast<const int *>(L.col.p), static_cast<const int *>(L.row_of.p), ne, L.rev.p);
+      H33_CUDA(cudaGetLastError());
+    }
     L.feat.alloc(size_t(9) * std::max(ne, 1));
     L.s.alloc(size_t(N));
     L.w.alloc(size_t(kGnnLayers) * std::max(ne, 1));
@@ -1670,12 +1821,30 @@ void coarse_structure(Solver &S) {
   Profile prof{S.N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
   Aggregation ag;
   aggregate_nodes(prof, coarse_max_aggregates(), ag);
-  BlockRows u;
-  unified_rows(prof, u);
-  if (u.ptr.back() > int64_t(std::numeric_limits<int>::max()))
-    throw Failure(HECMW33_ERR_BAD_INPUT, "coarse space: too many blocks for 32-bit row pointers");
-  std::vector<int> uptr(u.ptr.size());
-  for (size_t k = 0; k < u.ptr.size(); k++) uptr[k] = int(u.ptr[k]);
+  // the unified rows (L, D, U per row) as CSR: the row pointers from the block counts,
+  // the blocks placed on the device (on the host with HECMW33_HOST_LAYOUT=1)
+  std::vector<int> uptr(size_t(S.N) + 1, 0);
+  int64_t nu = 0;
+  for (int i = 0; i < S.N; i++) {
+    nu += (S.indexL[size_t(i) + 1] - S.indexL[size_t(i)]) + 1 + (S.indexU[size_t(i) + 1] - S.indexU[size_t(i)]);
+    if (nu > int64_t(std::numeric_limits<int>::max()))
+      throw Failure(HECMW33_ERR_BAD_INPUT, "coarse space: too many blocks for 32-bit row pointers");
+    uptr[size_t(i) + 1] = int(nu);
+  }
+  C.uptr.upload(uptr, S.stream);
+  if (host_layouts()) {
+    BlockRows u;
+    unified_rows(prof, u);
+    C.ucol.upload(u.col, S.stream);
+    C.usrc.upload(u.src, S.stream);
+  } else {
+    C.ucol.alloc(size_t(nu));
+    C.usrc.alloc(size_t(nu));
+    const int gr = std::max(1, std::min((S.N + kThreads - 1) / kThreads, S.nsm * 8));
+    launch_k(S.stream, fill_unified_csr_kernel, gr, kThreads, dev_profile(S), static_cast<const int *>(C.uptr.p),
+             C.ucol.p, C.usrc.p);
+    H33_CUDA(cudaGetLastError());
+  }
   C.n = S.N;
   C.nagg = ag.n_agg;
   C.nc = 3 * ag.n_agg;
@@ -1689,9 +1858,6 @@ void coarse_structure(Solver &S) {
   C.qagg.upload(ag.qagg, S.stream);
   C.cptr.upload(ag.cptr, S.stream);
   C.cagg.upload(ag.cagg, S.stream);
-  C.uptr.upload(uptr, S.stream);
-  C.ucol.upload(u.col, S.stream);
-  C.usrc.upload(u.src, S.stream);
   const size_t n3 = size_t(S.n3()), nnzp = ag.pagg.size(), nnzq = ag.qagg.size(), nc = size_t(C.nc);
   C.mask.alloc(n3);
   C.x.alloc(size_t(S.N) * 6);
@@ -1909,9 +2075,14 @@ void learned_prepare_inference(Solver &S) {
   if (S.dom.on)
     throw Failure(HECMW33_ERR_INCONS_PC, "the learned preconditioner takes a whole mesh (one domain) only");
   ensure_smoother(S);
-  learned_graph(S);
+  if (L.coarse_mode == 0) {  // the network's graph and features (the fixed weights need neither)
+    learned_graph(S);
+    setup_mark("learned: network graph");
+  }
   coarse_structure(S);
+  setup_mark("learned: aggregates, P and A P structure");
   coarse_values(S);
+  setup_mark("learned: coarse values");
   if (S.a32_version != S.values_version) {  // FP32 A for the residuals of the mode-1 preconditioner
     S.A.val32.alloc(S.A.val.n);
     const size_t n = S.A.val.n;
@@ -1931,7 +2102,9 @@ void learned_prepare_inference(Solver &S) {
       C.omega.upload(half, S.stream);
       omega = C.omega.p;
     }
+    setup_mark("learned: FP32 A, omega");
     coarse_operator(S, omega);
+    setup_mark("learned: Ac and its inverse");
     C.op_precond = S.pc.numeric_version;
     C.op_weights = wv;
     C.op_mode = L.coarse_mode;
@@ -3050,18 +3223,23 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   if (times) times[0] = times[1] = times[2] = 0.0;
   double sigma;
   bool auto_sigma;
+  setup_mark("solve: start");
   ScaleScope scaling(S, Iarray[6] != 0);
   const int pre = prepare_solve(S, Iarray, Rarray, &sigma, &auto_sigma);
   if (pre) {
     scaling.restore();
     return pre;
   }
+  setup_mark("solve: precond_setup");
   const int MAXIT = Iarray[0], PRECOND = Iarray[2], iterPREmax = Iarray[4], METHOD2 = Iarray[7];
   const double TOL = Rarray[0];
   int method = Iarray[1];
   int learned = (Iarray[42] == 1 && method == 1) ? 1 : 0;  // the learned two-level preconditioner
   S.L.coarse_mode = (Iarray[43] >= 0 && Iarray[43] <= 2) ? Iarray[43] : 0;
-  if (learned) learned_prepare_inference(S);
+  if (learned) {
+    learned_prepare_inference(S);
+    setup_mark("solve: learned smoother + coarse space");
+  }
   const int ESTCOND = Iarray[13];  // hecmw_mat_get_estcond
   S.lanczos_on = ESTCOND > 0 && method == 1 && !learned;
   S.last_lanczos_n = 0;
@@ -3078,9 +3256,11 @@ int solve_fp64(Solver &S, int *Iarray, double *Rarray, int *iter, double *resid,
   } else {
     lowp = 0;
   }
+  setup_mark("solve: BF16 copies, buffers");
   const bool record = S.L.recording && !learned && method == 1;
   if (graph_mode() && !record && (method == 1 || method == 2))
     build_graph<double>(S, iterPREmax, learned | (lowp ? 4 : 0) | (method == 2 ? 8 : 0));
+  setup_mark("solve: graph capture + instantiate");
   Range rs("hecmw33_solve");
   const double t1 = wall();
   int error = 0, kernels = 1;
@@ -3602,12 +3782,7 @@ void build_mr_tiles(Solver &S) {
 void ensure_multi_buffers(Solver &S) {
   if (mr_tiled_mode() && S.mt_generation != S.generation) build_mr_tiles(S);
   if (S.amr_generation != S.generation) {
-    Profile prof{S.N, S.indexL.data(), S.itemL.data(), S.indexU.data(), S.itemU.data()};
-    BlockRows rows;
-    unified_rows(prof, rows);
-    SellLayout lay;
-    build_sell(rows, std::vector<int>{0, S.N}, lay, kMrLanes);
-    S.Amr.upload(lay, S.stream);
+    build_unified(S, S.Amr, kMrLanes);
     S.amr_generation = S.generation;
     S.amr_values = -1;
   }
