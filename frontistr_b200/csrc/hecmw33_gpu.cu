@@ -477,6 +477,9 @@ struct Solver {
   MultiCtl *h_mctl = nullptr;
   GraphSlot gm;
   int occ_mr = 4;
+  // pinned staging of pageable host -> device copies (upload_pageable)
+  void *stage[2] = {nullptr, nullptr};
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   // the multi-RHS vector kernels (fewer registers than the sweeps): the streamed updates
   // (mr_update_xr_kernel), the learned iteration's RHO pass with its P y gathers and its
   // (A P) y residual
@@ -539,6 +542,10 @@ struct Solver {
     if (stream) {
       cudaStreamSynchronize(stream);
       cudaStreamDestroy(stream);
+    }
+    for (int b = 0; b < 2; b++) {
+      if (stage_ev[b]) cudaEventDestroy(stage_ev[b]);
+      if (stage[b]) cudaFreeHost(stage[b]);
     }
   }
   void drop_graph() {
@@ -608,6 +615,46 @@ void validate(int N, int NP, int NPL, int NPU, const int *indexL, const int *ite
 bool host_layouts() {
   const char *e = std::getenv("HECMW33_HOST_LAYOUT");
   return e && e[0] == '1';
+}
+
+// Host -> device copy of a caller's buffer on S.stream.  Pinned (or registered) memory
+// goes straight to the DMA engine; pageable memory goes through two pinned staging
+// buffers, host threads filling one while the other's DMA runs (a pageable
+// cudaMemcpyAsync stages through one driver thread: about 11 GB/s for the cube's 2 GB
+// of values).  Returns once the last chunk is queued; the data are then stream-ordered.
+constexpr size_t kStageBytes = size_t(32) << 20;
+void upload_host(Solver &S, void *dst, const void *src, size_t bytes) {
+  if (bytes == 0) return;
+  cudaPointerAttributes attr{};
+  const bool pinned = cudaPointerGetAttributes(&attr, src) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+  (void)cudaGetLastError();  // an unregistered pointer may leave an error behind on older drivers
+  if (pinned || bytes < kStageBytes) {
+    H33_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, S.stream));
+    return;
+  }
+  for (int b = 0; b < 2; b++) {
+    if (!S.stage[b]) {
+      H33_CUDA(cudaHostAlloc(&S.stage[b], kStageBytes, cudaHostAllocDefault));
+      H33_CUDA(cudaEventCreateWithFlags(&S.stage_ev[b], cudaEventDisableTiming));
+    }
+  }
+  const char *from = static_cast<const char *>(src);
+  char *to = static_cast<char *>(dst);
+  constexpr size_t kPiece = size_t(1) << 20;
+  for (size_t off = 0, k = 0; off < bytes; off += kStageBytes, k++) {
+    const int b = int(k & 1);
+    const size_t n = std::min(kStageBytes, bytes - off);
+    H33_CUDA(cudaEventSynchronize(S.stage_ev[b]));  // the buffer's previous DMA is done
+    char *st = static_cast<char *>(S.stage[b]);
+    const int64_t np = int64_t((n + kPiece - 1) / kPiece);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < np; i++) {
+      const size_t o = size_t(i) * kPiece;
+      std::memcpy(st + o, from + off + o, std::min(kPiece, n - o));
+    }
+    H33_CUDA(cudaMemcpyAsync(to + off, st, n, cudaMemcpyHostToDevice, S.stream));
+    H33_CUDA(cudaEventRecord(S.stage_ev[b], S.stream));
+  }
 }
 
 DevProfile dev_profile(const Solver &S) {
@@ -765,12 +812,9 @@ void set_matrix_square(Solver &S, int N, int NPL, int NPU, const int *indexL, co
   setup_mark("set_matrix: profile + SpMV layout");
   const size_t nb = size_t(N) + NPL + NPU;
   S.raw.alloc(9 * nb);
-  H33_CUDA(cudaMemcpyAsync(S.raw.p, D, sizeof(double) * 9 * N, cudaMemcpyHostToDevice, S.stream));
-  if (NPL)
-    H33_CUDA(cudaMemcpyAsync(S.raw.p + 9 * size_t(N), AL, sizeof(double) * 9 * NPL, cudaMemcpyHostToDevice, S.stream));
-  if (NPU)
-    H33_CUDA(cudaMemcpyAsync(S.raw.p + 9 * (size_t(N) + NPL), AU, sizeof(double) * 9 * NPU,
-                             cudaMemcpyHostToDevice, S.stream));
+  upload_host(S, S.raw.p, D, sizeof(double) * 9 * size_t(N));
+  if (NPL) upload_host(S, S.raw.p + 9 * size_t(N), AL, sizeof(double) * 9 * size_t(NPL));
+  if (NPU) upload_host(S, S.raw.p + 9 * (size_t(N) + NPL), AU, sizeof(double) * 9 * size_t(NPU));
   S.A.pack(S.raw.p, S.stream, S.nsm);
   S.values_version++;
   S.zero_diag = false;
@@ -4496,8 +4540,10 @@ HECMW33_API void hecmw33_gpu_solve_multi(const int *handle, const int *nrhs, con
   if (!nrhs || *nrhs < 1) throw Failure(HECMW33_ERR_BAD_INPUT, "nrhs must be positive");
   const size_t total = size_t(S.n3()) * size_t(*nrhs);
   DevArray<double> dB, dX;
-  dB.upload(B, total, S.stream);
-  dX.upload(X, total, S.stream);
+  dB.alloc(total);
+  dX.alloc(total);
+  upload_host(S, dB.p, B, sizeof(double) * total);
+  upload_host(S, dX.p, X, sizeof(double) * total);
   std::vector<double> tr(static_cast<size_t>(*nrhs));
   const int rc = solve_multi(S, *nrhs, dB.p, dX.p, Iarray, Rarray, iter, resid, error, tr.data(), times);
   H33_CUDA(cudaMemcpyAsync(X, dX.p, sizeof(double) * total, cudaMemcpyDeviceToHost, S.stream));
