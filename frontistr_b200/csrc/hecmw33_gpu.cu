@@ -618,17 +618,22 @@ bool host_layouts() {
 }
 
 // Host -> device copy of a caller's buffer on S.stream.  Pinned (or registered) memory
-// goes straight to the DMA engine; pageable memory goes through two pinned staging
-// buffers, host threads filling one while the other's DMA runs (a pageable
-// cudaMemcpyAsync stages through one driver thread: about 11 GB/s for the cube's 2 GB
-// of values).  Returns once the last chunk is queued; the data are then stream-ordered.
+// goes straight to the DMA engine (device or managed memory as a plain copy); pageable
+// memory goes through two pinned staging buffers, host threads filling one while the
+// other's DMA runs (a pageable cudaMemcpyAsync stages through one driver thread: about
+// 11 GB/s for the cube's 2 GB of values).  Returns once the last chunk is queued; the
+// data are then stream-ordered.
 constexpr size_t kStageBytes = size_t(32) << 20;
 void upload_host(Solver &S, void *dst, const void *src, size_t bytes) {
   if (bytes == 0) return;
   cudaPointerAttributes attr{};
-  const bool pinned = cudaPointerGetAttributes(&attr, src) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+  const bool known = cudaPointerGetAttributes(&attr, src) == cudaSuccess;
   (void)cudaGetLastError();  // an unregistered pointer may leave an error behind on older drivers
-  if (pinned || bytes < kStageBytes) {
+  if (known && attr.type != cudaMemoryTypeUnregistered) {  // pinned, registered, managed or device memory
+    H33_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, S.stream));
+    return;
+  }
+  if (bytes < kStageBytes) {
     H33_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, S.stream));
     return;
   }
