@@ -1041,13 +1041,15 @@ void aggregate_nodes(const Profile &p, int max_aggregates, Aggregation &out) {
   std::vector<int> agg(static_cast<size_t>(N));
   for (int i = 0; i < N; i++) agg[size_t(i)] = i;
   int n = N;
-  Csr g = adj;
+  const Csr *g = &adj;  // the graph of the current level (the node graph itself first: no copy)
+  Csr level;
   for (int pass = 0; pass == 0 || n > max_aggregates; pass++) {
     std::vector<int> a;
-    const int na = aggregate_pass(g, a);
+    const int na = aggregate_pass(*g, a);
     if (2 * na > n) break;  // no longer coarsening
     for (int i = 0; i < N; i++) agg[size_t(i)] = a[size_t(agg[size_t(i)])];
-    g = coarse_graph(g, a, na);
+    level = coarse_graph(*g, a, na);
+    g = &level;
     n = na;
   }
   out.n_agg = n;
