@@ -9,6 +9,8 @@
 // Everything here is 0-based; node ids in the input profile are 1-based.
 #include "h33_setup.h"
 
+#include <omp.h>
+
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -688,36 +690,63 @@ int factor_bilu0(const Profile &p, const double *D, const double *AL, const doub
     Dlu0[9 * size_t(i) + 4] *= sigma_diag;
     Dlu0[9 * size_t(i) + 8] *= sigma_diag;
   }
-  if (N > 0 && lu33_inplace(Dlu0.data())) return 9001;
-  // position markers of row i's lower / upper entries (0 = absent)
-  std::vector<int> posL(N, 0), posU(N, 0);
-  double RHS[9];
-  for (int i = 1; i < N; i++) {
-    for (int k = p.indexL[i]; k < p.indexL[i + 1]; k++) posL[p.itemL[k] - 1] = k + 1;
-    for (int k = p.indexU[i]; k < p.indexU[i + 1]; k++)
-      if (p.itemU[k] <= N) posU[p.itemU[k] - 1] = k + 1;
-    for (int kk = p.indexL[i]; kk < p.indexL[i + 1]; kk++) {
-      const int k = p.itemL[kk] - 1;
-      double Aik[9];
-      std::memcpy(Aik, &ALlu0[9 * size_t(kk)], sizeof(Aik));
-      const double *Dk = &Dlu0[9 * size_t(k)];
-      for (int jj = p.indexU[k]; jj < p.indexU[k + 1]; jj++) {
-        const int j = p.itemU[jj] - 1;
-        if (j >= N) continue;
-        // a row's own id is in neither of its lists, so j == i never passes here and
-        // the diagonal block is left as it is (as in the reference)
-        if (posL[j] == 0 && posU[j] == 0) continue;
-        aik_dinv_akj(RHS, Dk, Aik, &AUlu0[9 * size_t(jj)]);
-        double *dst = j < i ? &ALlu0[9 * size_t(posL[j] - 1)] : &AUlu0[9 * size_t(posU[j] - 1)];
-        for (int e = 0; e < 9; e++) dst[e] = dst[e] - RHS[e];
+  // Row i reads only rows k of its lower list (their final U blocks and diagonal LU)
+  // and writes only its own blocks, so the rows of one level of the lower pattern are
+  // factored in parallel; each row's arithmetic is the natural-order sweep's, in the
+  // same order, so the factors are the serial ones bit for bit.  Level order reads the
+  // neighbours' rows from farther back than the natural order (on a 101^3 27-point
+  // profile one thread takes 5.5 s against 3.0 s in natural order), so with fewer
+  // than four threads the rows go in natural order.
+  std::vector<int> order, level_ptr;
+  if (omp_get_max_threads() >= 4) {
+    level_schedule(p, true, order, level_ptr);
+  } else {
+    order.resize(size_t(N));
+    for (int i = 0; i < N; i++) order[size_t(i)] = i;
+    level_ptr = {0, N};  // one "level": the loop below then runs the rows in order on one thread
+  }
+  const int nlev = int(level_ptr.size()) - 1;
+  const bool serial = nlev == 1 && omp_get_max_threads() < 4;
+  int bad = 0;
+#pragma omp parallel if (!serial)
+  {
+    // position markers of row i's lower / upper entries (0 = absent), per thread
+    std::vector<int> posL(static_cast<size_t>(N), 0), posU(static_cast<size_t>(N), 0);
+    double RHS[9];
+    for (int lv = 0; lv < nlev; lv++) {
+#pragma omp for schedule(static)
+      for (int t = level_ptr[size_t(lv)]; t < level_ptr[size_t(lv) + 1]; t++) {
+        const int i = order[size_t(t)];
+        for (int k = p.indexL[i]; k < p.indexL[i + 1]; k++) posL[size_t(p.itemL[k] - 1)] = k + 1;
+        for (int k = p.indexU[i]; k < p.indexU[i + 1]; k++)
+          if (p.itemU[k] <= N) posU[size_t(p.itemU[k] - 1)] = k + 1;
+        for (int kk = p.indexL[i]; kk < p.indexL[i + 1]; kk++) {
+          const int k = p.itemL[kk] - 1;
+          double Aik[9];
+          std::memcpy(Aik, &ALlu0[9 * size_t(kk)], sizeof(Aik));
+          const double *Dk = &Dlu0[9 * size_t(k)];
+          for (int jj = p.indexU[k]; jj < p.indexU[k + 1]; jj++) {
+            const int j = p.itemU[jj] - 1;
+            if (j >= N) continue;
+            // a row's own id is in neither of its lists, so j == i never passes here and
+            // the diagonal block is left as it is (as in the reference)
+            if (posL[size_t(j)] == 0 && posU[size_t(j)] == 0) continue;
+            aik_dinv_akj(RHS, Dk, Aik, &AUlu0[9 * size_t(jj)]);
+            double *dst = j < i ? &ALlu0[9 * size_t(posL[size_t(j)] - 1)] : &AUlu0[9 * size_t(posU[size_t(j)] - 1)];
+            for (int q = 0; q < 9; q++) dst[q] = dst[q] - RHS[q];
+          }
+        }
+        if (lu33_inplace(&Dlu0[9 * size_t(i)])) {
+#pragma omp atomic write
+          bad = 1;
+        }
+        for (int k = p.indexL[i]; k < p.indexL[i + 1]; k++) posL[size_t(p.itemL[k] - 1)] = 0;
+        for (int k = p.indexU[i]; k < p.indexU[i + 1]; k++)
+          if (p.itemU[k] <= N) posU[size_t(p.itemU[k] - 1)] = 0;
       }
     }
-    if (lu33_inplace(&Dlu0[9 * size_t(i)])) return 9001;
-    for (int k = p.indexL[i]; k < p.indexL[i + 1]; k++) posL[p.itemL[k] - 1] = 0;
-    for (int k = p.indexU[i]; k < p.indexU[i + 1]; k++)
-      if (p.itemU[k] <= N) posU[p.itemU[k] - 1] = 0;
   }
-  return 0;
+  return bad ? 9001 : 0;
 }
 
 void bilu_fill(const Profile &p, int level, FilledProfile &f) {
