@@ -681,10 +681,14 @@ void aik_dinv_akj(double *RHS, const double *Dk, const double *Aik, const double
 int factor_bilu0(const Profile &p, const double *D, const double *AL, const double *AU,
                  double sigma_diag, std::vector<double> &Dlu0, std::vector<double> &ALlu0,
                  std::vector<double> &AUlu0) {
-  const int N = p.N, NPL = p.NPL(), NPU = p.NPU();
-  Dlu0.assign(D, D + 9 * size_t(N));
-  ALlu0.assign(AL, AL + 9 * size_t(NPL));
-  AUlu0.assign(AU, AU + 9 * size_t(NPU));
+  Dlu0.assign(D, D + 9 * size_t(p.N));
+  ALlu0.assign(AL, AL + 9 * size_t(p.NPL()));
+  AUlu0.assign(AU, AU + 9 * size_t(p.NPU()));
+  return factor_bilu0_inplace(p, Dlu0.data(), ALlu0.data(), AUlu0.data(), sigma_diag);
+}
+
+int factor_bilu0_inplace(const Profile &p, double *Dlu0, double *ALlu0, double *AUlu0, double sigma_diag) {
+  const int N = p.N;
   for (int i = 0; i < N; i++) {
     Dlu0[9 * size_t(i)] *= sigma_diag;
     Dlu0[9 * size_t(i) + 4] *= sigma_diag;

@@ -128,6 +128,8 @@ void element_contributions(int n_node, int n_elem, int nn, const int *conn, cons
 int factor_bilu0(const Profile &p, const double *D, const double *AL, const double *AU,
                  double sigma_diag, std::vector<double> &Dlu0, std::vector<double> &ALlu0,
                  std::vector<double> &AUlu0);
+// The same in place on the D, AL, AU arrays (9 N, 9 NPL, 9 NPU doubles).
+int factor_bilu0_inplace(const Profile &p, double *D, double *AL, double *AU, double sigma_diag);
 
 // Fill pattern of the reference's block ILU(1) / ILU(2) (FORM_ILU1_33 / FORM_ILU2_33,
 // hecmw_precond_BILU_33.f90:371-739, 748-1337) on the internal rows of p: level-1

@@ -662,6 +662,52 @@ void upload_host(Solver &S, void *dst, const void *src, size_t bytes) {
   }
 }
 
+// Device -> host copy into a caller's or the library's pageable buffer, complete on
+// return: through the same two pinned staging buffers, the DMA of one chunk running
+// while host threads copy the previous one out (pinned or device destinations take a
+// plain copy).
+void download_host(Solver &S, void *dst, const void *src, size_t bytes) {
+  if (bytes == 0) return;
+  cudaPointerAttributes attr{};
+  const bool known = cudaPointerGetAttributes(&attr, dst) == cudaSuccess;
+  (void)cudaGetLastError();
+  if ((known && attr.type != cudaMemoryTypeUnregistered) || bytes < kStageBytes) {
+    H33_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, S.stream));
+    S.sync();
+    return;
+  }
+  for (int b = 0; b < 2; b++) {
+    if (!S.stage[b]) {
+      H33_CUDA(cudaHostAlloc(&S.stage[b], kStageBytes, cudaHostAllocDefault));
+      H33_CUDA(cudaEventCreateWithFlags(&S.stage_ev[b], cudaEventDisableTiming));
+    }
+  }
+  const char *from = static_cast<const char *>(src);
+  char *to = static_cast<char *>(dst);
+  const size_t nchunks = (bytes + kStageBytes - 1) / kStageBytes;
+  auto issue = [&](size_t k) {  // DMA of chunk k into its staging buffer (stream-ordered after its last use)
+    const int b = int(k & 1);
+    const size_t off = k * kStageBytes, n = std::min(kStageBytes, bytes - off);
+    H33_CUDA(cudaMemcpyAsync(S.stage[b], from + off, n, cudaMemcpyDeviceToHost, S.stream));
+    H33_CUDA(cudaEventRecord(S.stage_ev[b], S.stream));
+  };
+  constexpr size_t kPiece = size_t(1) << 20;
+  issue(0);
+  for (size_t k = 0; k < nchunks; k++) {
+    if (k + 1 < nchunks) issue(k + 1);
+    const int b = int(k & 1);
+    H33_CUDA(cudaEventSynchronize(S.stage_ev[b]));  // chunk k has landed
+    const size_t off = k * kStageBytes, n = std::min(kStageBytes, bytes - off);
+    const char *st = static_cast<const char *>(S.stage[b]);
+    const int64_t np = int64_t((n + kPiece - 1) / kPiece);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < np; i++) {
+      const size_t o = size_t(i) * kPiece;
+      std::memcpy(to + off + o, st + o, std::min(kPiece, n - o));
+    }
+  }
+}
+
 DevProfile dev_profile(const Solver &S) {
   return DevProfile{S.N, S.NPL, S.d_indexL.p, S.d_itemL.p, S.d_indexU.p, S.d_itemU.p};
 }
@@ -1016,19 +1062,24 @@ void setup_bilu(Solver &S, int level, double sigma, bool symbolic) {
   // numeric factorisation on the host, from the resident values
   const size_t nb = size_t(S.N) + S.NPL + S.NPU;
   std::vector<double> host(9 * nb);
-  H33_CUDA(cudaMemcpyAsync(host.data(), S.raw.p, sizeof(double) * host.size(), cudaMemcpyDeviceToHost, S.stream));
-  S.sync();
-  const double *D = host.data(), *AL = host.data() + 9 * size_t(S.N), *AU = host.data() + 9 * (size_t(S.N) + S.NPL);
-  std::vector<double> Dlu, ALlu, AUlu;
-  const int rc = level > 0 ? factor_bilu_fill(P.fill, level, D, AL, AU, sigma, Dlu, ALlu, AUlu)
-                           : factor_bilu0(prof0, D, AL, AU, sigma, Dlu, ALlu, AUlu);
-  if (rc) throw Failure(HECMW33_ERR_ILU_ZERO_PIVOT, "block ILU: zero pivot (the reference stops here)");
-  std::vector<double> fac;
-  fac.reserve(Dlu.size() + ALlu.size() + AUlu.size());
-  fac.insert(fac.end(), Dlu.begin(), Dlu.end());
-  fac.insert(fac.end(), ALlu.begin(), ALlu.end());
-  fac.insert(fac.end(), AUlu.begin(), AUlu.end());
-  P.ilu_raw.upload(fac.data(), fac.size(), S.stream);
+  download_host(S, host.data(), S.raw.p, sizeof(double) * host.size());
+  double *D = host.data(), *AL = host.data() + 9 * size_t(S.N), *AU = host.data() + 9 * (size_t(S.N) + S.NPL);
+  if (level == 0) {
+    // ILU(0) keeps the matrix's pattern: factored in place, uploaded in the raw layout
+    if (factor_bilu0_inplace(prof0, D, AL, AU, sigma))
+      throw Failure(HECMW33_ERR_ILU_ZERO_PIVOT, "block ILU: zero pivot (the reference stops here)");
+    P.ilu_raw.alloc(host.size());
+    upload_host(S, P.ilu_raw.p, host.data(), sizeof(double) * host.size());
+  } else {
+    std::vector<double> Dlu, ALlu, AUlu;
+    if (factor_bilu_fill(P.fill, level, D, AL, AU, sigma, Dlu, ALlu, AUlu))
+      throw Failure(HECMW33_ERR_ILU_ZERO_PIVOT, "block ILU: zero pivot (the reference stops here)");
+    P.ilu_raw.alloc(Dlu.size() + ALlu.size() + AUlu.size());
+    upload_host(S, P.ilu_raw.p, Dlu.data(), sizeof(double) * Dlu.size());
+    upload_host(S, P.ilu_raw.p + Dlu.size(), ALlu.data(), sizeof(double) * ALlu.size());
+    upload_host(S, P.ilu_raw.p + Dlu.size() + ALlu.size(), AUlu.data(), sizeof(double) * AUlu.size());
+    S.sync();  // the factors' vectors go at the end of this scope
+  }
   P.lo.pack(P.ilu_raw.p, S.stream, S.nsm);
   P.up.pack(P.ilu_raw.p, S.stream, S.nsm);
   diag_alu(S, P.alu_fwd, P.ilu_raw.p, P.perm_fwd.p, 1.0, 1);
