@@ -125,6 +125,27 @@ __global__ void fill_reordered_kernel(DevProfile p, const int *__restrict__ perm
   }
 }
 
+// The block ILU layouts (level order): layout row q holds row ord[q]'s L blocks (UPPER
+// false) or U blocks (UPPER true) as stored, columns as 0-based node ids, values by raw
+// block id.  A thread per row.
+template <bool UPPER>
+__global__ void fill_ordered_kernel(DevProfile p, const int *__restrict__ ord, const int *__restrict__ row_slice,
+                                    const int *__restrict__ row0, const int *__restrict__ slot0, int lanes,
+                                    int *__restrict__ col, int *__restrict__ src) {
+  pdl_entry();
+  const int *index = UPPER ? p.indexU : p.indexL, *item = UPPER ? p.itemU : p.itemL;
+  const int base = UPPER ? p.N + p.NPL : p.N;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < p.N; q += gridDim.x * blockDim.x) {
+    const int i = ord[q], s = row_slice[q], r = q - row0[s], s0 = slot0[s];
+    int k = 0;
+    for (int j = index[i]; j < index[i + 1]; j++, k++) {
+      const size_t at = sell_at(s0, r, k, lanes);
+      col[at] = item[j] - 1;
+      src[at] = base + j;
+    }
+  }
+}
+
 // The unified rows as CSR (ptr from the host's block counts): row i's L blocks, its
 // diagonal, its U blocks as stored; col 0-based, src the raw block id.  A thread per row.
 __global__ void fill_unified_csr_kernel(DevProfile p, const int *__restrict__ ptr, int *__restrict__ col,

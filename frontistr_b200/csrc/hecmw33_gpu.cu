@@ -1020,41 +1020,78 @@ void setup_bilu(Solver &S, int level, double sigma, bool symbolic) {
     std::vector<int> ord_f, lev_f, ord_b, lev_b;
     level_schedule(prof, true, ord_f, lev_f);
     level_schedule(prof, false, ord_b, lev_b);
-    BlockRows lower, upper;
-    const int N = S.N, NPL = prof.NPL();
-    lower.ptr.assign(size_t(N) + 1, 0);
-    upper.ptr.assign(size_t(N) + 1, 0);
-    for (int pos = 0; pos < N; pos++) {
-      const int i = ord_f[pos];
-      lower.ptr[pos + 1] = lower.ptr[pos] + (prof.indexL[i + 1] - prof.indexL[i]);
-      const int k = ord_b[pos];
-      upper.ptr[pos + 1] = upper.ptr[pos] + (prof.indexU[k + 1] - prof.indexU[k]);
-    }
-    lower.col.resize(size_t(lower.ptr[N]));
-    lower.src.resize(size_t(lower.ptr[N]));
-    upper.col.resize(size_t(upper.ptr[N]));
-    upper.src.resize(size_t(upper.ptr[N]));
-    for (int pos = 0; pos < N; pos++) {
-      const int i = ord_f[pos];
-      int64_t w = lower.ptr[pos];
-      for (int j = prof.indexL[i]; j < prof.indexL[i + 1]; j++) {
-        lower.col[w] = prof.itemL[j] - 1;
-        lower.src[w++] = N + j;
+    if (level == 0 && !host_layouts()) {
+      // the matrix's own pattern: the shapes from the rows' counts, the blocks placed
+      // on the device from the resident profile (fill_ordered_kernel)
+      const int N = S.N, lanes = sweep_lanes();
+      const size_t nn = static_cast<size_t>(N);
+      std::vector<int> cl(nn), cu(nn);
+      for (int q = 0; q < N; q++) {
+        cl[size_t(q)] = S.indexL[size_t(ord_f[size_t(q)]) + 1] - S.indexL[size_t(ord_f[size_t(q)])];
+        cu[size_t(q)] = S.indexU[size_t(ord_b[size_t(q)]) + 1] - S.indexU[size_t(ord_b[size_t(q)])];
       }
-      const int k = ord_b[pos];
-      w = upper.ptr[pos];
-      for (int j = prof.indexU[k]; j < prof.indexU[k + 1]; j++) {
-        upper.col[w] = prof.itemU[j] - 1;
-        upper.src[w++] = N + NPL + j;
+      SellLayout lo, up;
+      sell_shape(cl.data(), lev_f, lo, lanes);
+      sell_shape(cu.data(), lev_b, up, lanes);
+      std::vector<int> rs_f(nn), rs_b(nn);
+      for (int sl = 0; sl < lo.nslices; sl++)
+        for (int r = 0; r < lo.nrows[size_t(sl)]; r++) rs_f[size_t(lo.row0[size_t(sl)] + r)] = sl;
+      for (int sl = 0; sl < up.nslices; sl++)
+        for (int r = 0; r < up.nrows[size_t(sl)]; r++) rs_b[size_t(up.row0[size_t(sl)] + r)] = sl;
+      P.lo.upload_shape(lo, S.stream);
+      P.up.upload_shape(up, S.stream);
+      P.perm_fwd.upload(ord_f, S.stream);
+      P.perm_bwd.upload(ord_b, S.stream);
+      DevArray<int> d_rsf, d_rsb;
+      d_rsf.upload(rs_f, S.stream);
+      d_rsb.upload(rs_b, S.stream);
+      const DevProfile dp = dev_profile(S);
+      const int grid = std::max(1, std::min((N + kThreads - 1) / kThreads, S.nsm * 8));
+      launch_k(S.stream, fill_ordered_kernel<false>, grid, kThreads, dp, static_cast<const int *>(P.perm_fwd.p),
+               static_cast<const int *>(d_rsf.p), static_cast<const int *>(P.lo.row0.p),
+               static_cast<const int *>(P.lo.slot0.p), lanes, P.lo.col.p, P.lo.src.p);
+      launch_k(S.stream, fill_ordered_kernel<true>, grid, kThreads, dp, static_cast<const int *>(P.perm_bwd.p),
+               static_cast<const int *>(d_rsb.p), static_cast<const int *>(P.up.row0.p),
+               static_cast<const int *>(P.up.slot0.p), lanes, P.up.col.p, P.up.src.p);
+      H33_CUDA(cudaGetLastError());
+      S.sync();  // the fills read the row-slice tables above
+    } else {  // the filled pattern of ILU(1)/(2), or HECMW33_HOST_LAYOUT=1: on the host
+      BlockRows lower, upper;
+      const int N = S.N, NPL = prof.NPL();
+      lower.ptr.assign(size_t(N) + 1, 0);
+      upper.ptr.assign(size_t(N) + 1, 0);
+      for (int pos = 0; pos < N; pos++) {
+        const int i = ord_f[pos];
+        lower.ptr[pos + 1] = lower.ptr[pos] + (prof.indexL[i + 1] - prof.indexL[i]);
+        const int k = ord_b[pos];
+        upper.ptr[pos + 1] = upper.ptr[pos] + (prof.indexU[k + 1] - prof.indexU[k]);
       }
+      lower.col.resize(size_t(lower.ptr[N]));
+      lower.src.resize(size_t(lower.ptr[N]));
+      upper.col.resize(size_t(upper.ptr[N]));
+      upper.src.resize(size_t(upper.ptr[N]));
+      for (int pos = 0; pos < N; pos++) {
+        const int i = ord_f[pos];
+        int64_t w = lower.ptr[pos];
+        for (int j = prof.indexL[i]; j < prof.indexL[i + 1]; j++) {
+          lower.col[w] = prof.itemL[j] - 1;
+          lower.src[w++] = N + j;
+        }
+        const int k = ord_b[pos];
+        w = upper.ptr[pos];
+        for (int j = prof.indexU[k]; j < prof.indexU[k + 1]; j++) {
+          upper.col[w] = prof.itemU[j] - 1;
+          upper.src[w++] = N + NPL + j;
+        }
+      }
+      SellLayout lo, up;
+      build_sell(lower, lev_f, lo, sweep_lanes());
+      build_sell(upper, lev_b, up, sweep_lanes());
+      P.lo.upload(lo, S.stream);
+      P.up.upload(up, S.stream);
+      P.perm_fwd.upload(ord_f, S.stream);
+      P.perm_bwd.upload(ord_b, S.stream);
     }
-    SellLayout lo, up;
-    build_sell(lower, lev_f, lo, sweep_lanes());
-    build_sell(upper, lev_b, up, sweep_lanes());
-    P.lo.upload(lo, S.stream);
-    P.up.upload(up, S.stream);
-    P.perm_fwd.upload(ord_f, S.stream);
-    P.perm_bwd.upload(ord_b, S.stream);
     P.alu_shared = false;
     P.ncolor = 0;
     P.ilu_level = level;

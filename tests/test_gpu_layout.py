@@ -1,11 +1,11 @@
 """The sliced layouts filled on the device from the resident profile
-(fill_unified_kernel; count_parts_kernel + fill_reordered_kernel) against the host
-builders (HECMW33_HOST_LAYOUT=1: unified_rows, reordered_rows, build_sell): solves
-through either give the same iterations and the same X bit for bit -- the SpMV layout,
-the reference's RCM + multicolour SSOR schedule at several ncolor_in, the learned
-preconditioner's first-fit smoother, its network's graph and coarse space, and the
-16-lane copy of A of the multi-RHS solve, on a jittered box and on a box with randomly
-renumbered nodes."""
+(fill_unified_kernel; count_parts_kernel + fill_reordered_kernel; fill_ordered_kernel)
+against the host builders (HECMW33_HOST_LAYOUT=1: unified_rows, reordered_rows,
+build_sell): solves through either give the same iterations and the same X bit for
+bit -- the SpMV layout, the reference's RCM + multicolour SSOR schedule at several
+ncolor_in, block ILU(0)'s level-ordered layouts, the learned preconditioner's first-fit
+smoother, its network's graph and coarse space, and the 16-lane copy of A of the
+multi-RHS solve, on a jittered box and on a box with randomly renumbered nodes."""
 import numpy as np
 import pytest
 
@@ -48,7 +48,8 @@ def _solve(m, monkeypatch, host, settings):
     [(33, 40)],                      # ncolor_in 40
     [(41, 1)],                       # BF16-stored SSOR values
     [(42, 1), (43, 2)],              # learned two-level preconditioner (first-fit smoother)
-], ids=["ssor", "ncolor2", "ncolor40", "bf16", "learned"])
+    [(2, 10)],                       # block ILU(0): level-ordered layouts of the matrix's pattern
+], ids=["ssor", "ncolor2", "ncolor40", "bf16", "learned", "ilu0"])
 def test_device_layouts_equal_host(name, settings, monkeypatch):
     m = _system(name)
     m.set_iter(20000)
