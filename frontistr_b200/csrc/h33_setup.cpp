@@ -234,9 +234,18 @@ int ordering_greedy(const Profile &p, std::vector<int> &colorindex, std::vector<
                     std::vector<int> &iperm) {
   const int N = p.N;
   std::vector<int> c_in, c_sl;
-  const int n_in = first_fit(p, nullptr, c_in);
-  const std::vector<int> sl = smallest_last(p);
-  const int n_sl = first_fit(p, &sl, c_sl);
+  int n_in = 0, n_sl = 0;
+  // the two candidate colourings are independent: one thread each
+#pragma omp parallel sections num_threads(2)
+  {
+#pragma omp section
+    n_in = first_fit(p, nullptr, c_in);
+#pragma omp section
+    {
+      const std::vector<int> sl = smallest_last(p);
+      n_sl = first_fit(p, &sl, c_sl);
+    }
+  }
   const bool use_sl = n_sl < n_in;
   const std::vector<int> &colour = use_sl ? c_sl : c_in;
   const int ncolor = use_sl ? n_sl : n_in;
