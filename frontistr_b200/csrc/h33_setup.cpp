@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <numeric>
 #include <stdexcept>
 
@@ -282,7 +283,9 @@ int ordering_mc(const Profile &p, const std::vector<int> &perm_cur, int ncolor_i
     aptr[static_cast<size_t>(k) + 1] = c;
   }
   for (int k = 0; k < N; k++) aptr[static_cast<size_t>(k) + 1] += aptr[static_cast<size_t>(k)];
-  std::vector<int> adj(static_cast<size_t>(aptr[static_cast<size_t>(N)]));
+  // left uninitialised: the parallel fill below writes every entry (and first-touches
+  // the pages on many threads instead of one zero-filling pass)
+  std::unique_ptr<int[]> adj(new int[static_cast<size_t>(aptr[static_cast<size_t>(N)]) + 1]);
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < N; k++) {
     const int node = perm_cur[static_cast<size_t>(k)];
